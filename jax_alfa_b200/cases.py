@@ -1,0 +1,217 @@
+"""Workload definitions: run configurations and seeded initial conditions.
+
+Each case is a dict whose keys are the reference's ``Config.py`` option names
+(see ``src/config/ConfigLoader.py:70-157`` for the defaults and
+``examples/NBL_A94/runs/*/Config.py`` for a complete file), plus the seeded
+initial fields in the reference's input-file convention
+(``src/initialization/Initialization.py:58-100``: ``vel.npy`` holds total
+u, v, w as Fortran-flattened columns, ``TH.npy`` absolute theta).
+
+Cases (all FP64, 3/2-rule dealiased, FGR=1):
+  neutral     32x32x32, pressure-gradient-driven neutral ABL (log-law u,
+              u*=0.45 m/s, z0=0.1 m, Coriolis off), LASDD-SM, dt=0.5 s.
+              The large-scale forcing is the reference's advective tendency
+              (optAdvection=1, ``src/pde/NSE_AllTerms.py:86-88``) held at
+              Uadv = u*^2 / Lz.
+  neutral256  the same physics on 256^3 (the throughput workload).
+  convective  128^3 CBL: 0.24 K m/s surface flux, z0=0.16 m, inversion,
+              0.03 m/s velocity noise below 200 m.
+  stable      256x256x192 SBL: prescribed surface cooling 0.5 K/h from
+              265 K, geostrophic wind 8 m/s, LAD-SM (dynamic Smagorinsky).
+"""
+import numpy as np
+
+VONK = 0.4
+
+_BASE = dict(
+    use_double_precision=True, optGPU=1, GPU_ID=0,
+    istep=1, Ugal=0.0,
+    optSurfFlux=0, optSurfBC=0, z0m=0.1, z0T=0.1, zTemperature=0.0,
+    SensibleHeatFlux=0.0, SurfaceBCFile="input/SurfaceBC.npz",
+    optGeoWind=0, Ug2=0.0, Vg2=0.0, GeoWindFile="input/GeoWind.npz",
+    f_coriolis=0.0, inversion=0.0, optBuoyancy=1, T_0=300.0,
+    optSgs=1, dynamicSGS_call_time=1, FGR=1,
+    Cs2=0.1 ** 2, Cwl=0.1 ** 2, Cs2PrRatio=0.1 ** 2, CwlPrRatio=0.1 ** 2,
+    optDamping=0, RelaxTime=300.0,
+    SampleInterval_sec=1.0e9, OutputInterval_sec=1.0e9, Output3DInterval_sec=1.0e9,
+    optAdvection=0, AdvectionFile="input/AdvForcing.npz",
+    optMoisture=0, zMoisture=0.0, MoistureFlux=0.0, optMoistureSurfBC=0,
+    MoistureSurfaceBCFile="input/MoistureSurfaceBC.npz", q_inversion=0.0,
+    optPressureSolver=1,
+)
+
+USTAR_NEUTRAL = 0.45
+
+
+def neutral(nx=32, ny=32, nz=32, nsteps=200, **over):
+    cfg = dict(_BASE, l_x=2000.0, l_y=2000.0, l_z=1000.0, nx=nx, ny=ny, nz=nz,
+               dt=0.5, optSgs=1, z0m=0.1, z0T=0.1, optAdvection=1,
+               z_damping=800.0, optDamping=0)
+    cfg["SimTime"] = nsteps * cfg["dt"]
+    cfg["Uadv_const"] = USTAR_NEUTRAL ** 2 / cfg["l_z"]   # m s^-2
+    cfg["case"] = "neutral"
+    cfg.update(over)
+    return cfg
+
+
+def neutral256(nsteps=10, **over):
+    cfg = neutral(256, 256, 256, nsteps=nsteps, **over)
+    cfg["case"] = "neutral256"
+    return cfg
+
+
+def convective(nx=128, ny=128, nz=128, nsteps=2000, **over):
+    cfg = dict(_BASE, l_x=5120.0, l_y=5120.0, l_z=2048.0, nx=nx, ny=ny, nz=nz,
+               dt=0.5, optSgs=1, z0m=0.16, z0T=0.16, optSurfFlux=1,
+               SensibleHeatFlux=0.24, f_coriolis=1.0e-4, inversion=3.0 / 1000,
+               optDamping=1, z_damping=1650.0, RelaxTime=300.0)
+    cfg["SimTime"] = nsteps * cfg["dt"]
+    cfg["case"] = "convective"
+    cfg.update(over)
+    return cfg
+
+
+def stable(nx=256, ny=256, nz=192, nsteps=1000, **over):
+    cfg = dict(_BASE, l_x=400.0, l_y=400.0, l_z=400.0, nx=nx, ny=ny, nz=nz,
+               dt=0.1, optSgs=3, z0m=0.1, z0T=0.1, optSurfBC=2, Ug2=8.0,
+               Vg2=0.0, Ugal=5.0, f_coriolis=1.4e-4, T_0=265.0,
+               inversion=0.01, optDamping=1, z_damping=300.0, RelaxTime=60.0)
+    cfg["SimTime"] = nsteps * cfg["dt"]
+    cfg["case"] = "stable"
+    cfg.update(over)
+    return cfg
+
+
+CASES = {"neutral": neutral, "neutral256": neutral256,
+         "convective": convective, "stable": stable}
+
+
+def nsteps_of(cfg):
+    """``src/config/DerivedVars.py:90``."""
+    return int(np.ceil(cfg["SimTime"] / cfg["dt"]))
+
+
+def z_uvp(cfg):
+    """Cell-centre heights (m) as the reference's input generators use them
+    (``examples/NBL_A94/runs/*/CreateInputs_NBL_A94.py``: z_k=(k+1/2)dz,
+    dz=Lz/(nz-1))."""
+    dz = cfg["l_z"] / (cfg["nz"] - 1)
+    return (np.arange(cfg["nz"]) + 0.5) * dz
+
+
+def initial_fields(cfg, seed=0):
+    """Dimensional initial (u, v, w, theta), each (nx, ny, nz) C-order, u
+    total (Ugal included), theta absolute."""
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    z = z_uvp(cfg)
+    rng = np.random.default_rng(seed)
+    u = np.zeros((nx, ny, nz))
+    v = np.zeros((nx, ny, nz))
+    w = np.zeros((nx, ny, nz))
+    th = np.full((nx, ny, nz), float(cfg["T_0"]))
+    case = cfg["case"]
+    if case in ("neutral", "neutral256"):
+        prof = (USTAR_NEUTRAL / VONK) * np.log(z / cfg["z0m"])
+        u[:] = prof[None, None, :]
+        for k in range(nz):
+            if z[k] < 500.0:
+                u[:, :, k] += 0.005 * u[:, :, k] * rng.uniform(-1.0, 1.0, (nx, ny))
+                v[:, :, k] += 0.005 * u[:, :, k] * rng.uniform(-1.0, 1.0, (nx, ny))
+        th[:] = 300.0
+    elif case == "convective":
+        prof = np.where(z <= 1350.0, 300.0,
+                        np.where(z <= 1450.0, 300.0 + 5.0 * (z - 1350.0) / 100.0,
+                                 305.0 + 3.0e-3 * (z - 1450.0)))
+        th[:] = prof[None, None, :]
+        for k in range(nz):
+            if z[k] < 1000.0:
+                th[:, :, k] += 0.1 * rng.uniform(-1.0, 1.0, (nx, ny))
+        # u = v = 0 everywhere would make the near-surface wind speed zero and
+        # the reference's wall boundary value 0/0 (src/operations/
+        # Derivatives.py:224-229); like the reference's own CBL generator
+        # (examples/CBL_N91/runs/*/CreateInputs_CBL_N91.py) seed 0.03 m/s
+        # noise into u and w below 200 m.
+        for k in range(nz):
+            if z[k] <= 200.0:
+                r = 0.03 * rng.standard_normal((nx, ny))
+                u[:, :, k] += r
+                w[:, :, k] += r
+    elif case == "stable":
+        u[:] = cfg["Ug2"]
+        prof = np.where(z <= 100.0, 265.0, 265.0 + 0.01 * (z - 100.0))
+        th[:] = prof[None, None, :]
+        for k in range(nz):
+            if z[k] < 50.0:
+                th[:, :, k] += 0.1 * rng.uniform(-1.0, 1.0, (nx, ny))
+    else:
+        raise ValueError(case)
+    return u, v, w, th
+
+
+def surface_bc_series(cfg):
+    """Surface boundary series at every step, t=0..SimTime, in the
+    ``Initialization.py:107-160`` format: for ``optSurfBC=2`` the surface
+    temperature (K), cooling linearly at 0.5 K/h from 265 K; for
+    ``optSurfBC=1`` a heat flux (K m/s) oscillating about the case's
+    SensibleHeatFlux."""
+    n = nsteps_of(cfg) + 1
+    t = np.arange(n) * cfg["dt"]
+    if cfg["optSurfBC"] == 1:
+        return cfg["SensibleHeatFlux"] + 0.02 * np.sin(2 * np.pi * t / 3600.0)
+    return 265.0 - 0.5 * t / 3600.0
+
+
+def adv_forcing_series(cfg):
+    """(Uadv, Vadv, THadv) in m s^-2 / K s^-1 at every step and level
+    (``Initialization.py:253-323`` format)."""
+    n = nsteps_of(cfg) + 1
+    nz = cfg["nz"]
+    U = np.full((n, nz), cfg.get("Uadv_const", 0.0))
+    return U, np.zeros((n, nz)), np.zeros((n, nz))
+
+
+def to_reference_files(cfg, u, v, w, th):
+    """Arrays in the layout of the reference's ``vel.npy`` / ``TH.npy``."""
+    vel = np.column_stack([u.reshape(-1, order="F"), v.reshape(-1, order="F"),
+                           w.reshape(-1, order="F")])
+    return vel, th.reshape(-1, order="F")
+
+
+def config_py_text(cfg):
+    """A ``Config.py`` for the reference holding this case's options."""
+    lines = ["import numpy as np"]
+    skip = {"case", "Uadv_const"}
+    for k, v in cfg.items():
+        if k in skip:
+            continue
+        lines.append(f"{k} = {v!r}")
+    return "\n".join(lines) + "\n"
+
+
+def write_run_dir(cfg, path, seed=0):
+    """Write ``Config.py`` and ``input/`` files the reference's Main.py loads."""
+    import os
+    os.makedirs(os.path.join(path, "input"), exist_ok=True)
+    with open(os.path.join(path, "Config.py"), "w") as f:
+        f.write(config_py_text(cfg))
+    u, v, w, th = initial_fields(cfg, seed)
+    vel, thf = to_reference_files(cfg, u, v, w, th)
+    np.save(os.path.join(path, "input", "vel.npy"), vel)
+    np.save(os.path.join(path, "input", "TH.npy"), thf)
+    if cfg["optSurfBC"] >= 1:
+        np.savez(os.path.join(path, cfg["SurfaceBCFile"]), dt_surf=cfg["dt"],
+                 optSurfBC=np.int32(cfg["optSurfBC"]), data_series=surface_bc_series(cfg))
+    if cfg["optAdvection"] >= 1:
+        U, V, T = adv_forcing_series(cfg)
+        np.savez(os.path.join(path, cfg["AdvectionFile"]), dt_adv=cfg["dt"],
+                 optAdvection=np.int32(cfg["optAdvection"]),
+                 Uadv_series=U, Vadv_series=V, THadv_series=T)
+
+
+def gp_per_step(cfg):
+    return cfg["nx"] * cfg["ny"] * cfg["nz"]
+
+
+__all__ = ["CASES", "neutral", "neutral256", "convective", "stable",
+           "initial_fields", "write_run_dir", "nsteps_of", "surface_bc_series",
+           "adv_forcing_series", "gp_per_step"]
