@@ -1,0 +1,236 @@
+/*
+ * libalfa: B200 (sm_100a) FP64 implementation of the JAX-ALFA per-timestep
+ * LES hot path behind a plain C ABI.
+ *
+ * Conventions (identical to the reference's arrays, so no transposes at the
+ * boundary):
+ *   - every array pointer is a DEVICE pointer unless a comment says "host";
+ *   - real 3-D fields are (nx, ny, nz) C-order doubles, z fastest;
+ *   - spectra are (nx, ny/2+1, nz) interleaved complex doubles (re, im),
+ *     i.e. numpy.fft.rfft2(F, axes=(0, 1)) of such a field;
+ *   - padded fields (Dealias1 output) are (mx, my, nz), mx = 1.5 nx;
+ *   - the pressure system is (nx, ny/2+1, nz+1) real and imaginary parts;
+ *   - 2-D surface planes are (nx, ny); vertical profiles are (nz).
+ * All calls are asynchronous on the context's stream (alfa_set_stream) and
+ * return 0 or a negative ALFA_E_* code; alfa_last_error() describes it.
+ * Nothing here calls exit/abort or traps on the device.
+ *
+ * Static, configuration-derived reference arguments (kx2, ky2, the pressure
+ * wavenumbers, b_thomas, m_thomas, c_pressure, the Rayleigh damping arrays,
+ * the ZeRo* scratch arrays) live in the context and are not passed.
+ * Reference citations are path:line inside the JAX-ALFA project.
+ */
+#ifndef ALFA_H
+#define ALFA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALFA_OK 0
+#define ALFA_E_CONFIG (-1)   /* unsupported or inconsistent configuration */
+#define ALFA_E_SHAPE (-2)    /* a size or pointer argument is invalid      */
+#define ALFA_E_CUDA (-3)     /* a CUDA runtime call or launch failed       */
+#define ALFA_E_NUMERIC (-4)  /* non-finite state detected                  */
+#define ALFA_E_TIMEOUT (-5)  /* a bounded device wait gave up              */
+#define ALFA_E_STATE (-6)    /* call order (e.g. step before init_state)   */
+
+typedef struct alfa_ctx alfa_ctx;
+
+/* Option names and units of the reference's Config.py
+ * (src/config/ConfigLoader.py:70-157, examples/NBL_A94/runs/.../Config.py). */
+typedef struct alfa_config {
+  int nx, ny, nz;
+  double l_x, l_y, l_z;          /* m */
+  double dt;                     /* s */
+  int istep;
+  double Ugal;                   /* m/s */
+  int optSurfFlux;               /* 0 homogeneous, 1 heterogeneous */
+  int optSurfBC;                 /* 0 const flux, 1 flux series, 2 temperature series */
+  double z0m, z0T, zTemperature; /* m */
+  double SensibleHeatFlux;       /* K m/s */
+  double Ug2, Vg2;               /* m/s (optGeoWind = 0) */
+  double f_coriolis;             /* 1/s */
+  double inversion;              /* K/m */
+  int optBuoyancy;               /* 0: /T_0, 1: /<THv> */
+  double T_0;                    /* K */
+  int optSgs;                    /* 0 static, 1 LASDD-SM, 3 LAD-SM */
+  int dynamicSGS_call_time;
+  int FGR;                       /* 1 (3/2-rule dealiasing) */
+  double Cs2, Cs2PrRatio;        /* initial coefficients */
+  int optDamping;
+  double z_damping, RelaxTime;   /* m, s */
+  int optAdvection;
+  int optPressureSolver;         /* 1 Thomas, 0 dense (same tridiagonal system) */
+} alfa_config;
+
+/* Derived constants (src/config/DerivedVars.py:48-112, Preprocess.py:44-62). */
+typedef struct alfa_derived {
+  int mx, my, nx_rfft, ny_rfft;
+  double z_scale, g_nondim, f_coriolis_nondim, T_0_nondim, inversion_nondim;
+  double dx, dy, dz, L, dt_nondim, TFR;
+  int cut_explicit[2], cut_level1[2], cut_level2[2];
+} alfa_derived;
+
+/* Per-step diagnostics of the whole-step driver (host struct). */
+typedef struct alfa_diag {
+  int iteration;        /* next iteration number (Main.py loop variable) */
+  double CFL, CFLmax;   /* Main.py:534-540 */
+  double ustar_rms;     /* sqrt(mean(ustar^2)), Main.py:576 */
+  double qz_sfc_avg;    /* non-dimensional surface heat flux */
+} alfa_diag;
+
+/* ---- context ----------------------------------------------------------- */
+/* Replaces the static initialisation of src/Main.py:46-62 (Wavenumber,
+ * ThomasPressureInit / PressureInit) and DerivedVars. */
+int alfa_create(const alfa_config* cfg, alfa_ctx** out);
+void alfa_destroy(alfa_ctx* ctx);
+const char* alfa_last_error(const alfa_ctx* ctx);
+int alfa_set_stream(alfa_ctx* ctx, void* cuda_stream);
+int alfa_get_derived(const alfa_ctx* ctx, alfa_derived* out /* host */);
+size_t alfa_workspace_bytes(const alfa_ctx* ctx);
+
+/* ---- src/operations ---------------------------------------------------- */
+int alfa_FFT(alfa_ctx*, const double* F, double* F_fft);                 /* FFT.py:44 */
+int alfa_FFT_pad(alfa_ctx*, const double* F_pad, double* F_pad_fft);     /* FFT.py:68 */
+int alfa_Dealias1(alfa_ctx*, const double* F_fft, double* F_pad);        /* Dealiasing.py:51 */
+int alfa_Dealias2(alfa_ctx*, const double* F_pad_fft, double* F);        /* Dealiasing.py:86 */
+int alfa_Filtering_Explicit(alfa_ctx*, const double* F_fft, double* F_new,
+                            double* F_fft_new);                          /* Filtering.py:50 */
+int alfa_Filtering_Level1(alfa_ctx*, const double* F_fft, double* F_hat);  /* Filtering.py:97 */
+int alfa_Filtering_Level2(alfa_ctx*, const double* F_fft, double* F_hatd); /* Filtering.py:135 */
+/* axis 0: kx2, axis 1: ky2 */
+int alfa_Derivxy(alfa_ctx*, const double* F_fft, int axis, double* dFdxy); /* Derivatives.py:161 */
+/* out[9] = dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz */
+int alfa_velocityGradients(alfa_ctx*, const double* u, const double* v, const double* w,
+                           const double* u_fft, const double* v_fft, const double* w_fft,
+                           const double* ustar, const double* M_sfc_loc, const double* fi2D_m,
+                           double* const out[9]);                        /* Derivatives.py:47 */
+/* out[3] = dTHdx, dTHdy, dTHdz */
+int alfa_potentialTemperatureGradients(alfa_ctx*, const double* TH, const double* ustar,
+                                       const double* qz_sfc, const double* fi2D_h,
+                                       double* const out[3]);            /* Derivatives.py:107 */
+int alfa_Derivz_Generic_uvp(alfa_ctx*, const double* F, double* dFdz);  /* Derivatives.py:310 */
+int alfa_Derivz_Generic_w(alfa_ctx*, const double* F, double* dFdz);    /* Derivatives.py:340 */
+
+/* ---- src/utilities ----------------------------------------------------- */
+int alfa_PlanarMean(alfa_ctx*, const double* F, double* mean_nz);        /* Utilities.py:41 */
+/* every (x, y) plane of an (nx, ny, nz) field */
+int alfa_Imfilter(alfa_ctx*, const double* F, double* out);              /* Utilities.py:87 */
+/* Laguerre roots of nlev quintics from each of the 8 beta guesses, then the
+ * beta selection of ComputeBeta1/2: coeffs (6, nlev) = ff, ee, dd, cc, bb, aa */
+int alfa_ComputeBeta(alfa_ctx*, const double* coeffs, int nlev, double* beta);
+                                         /* DynamicSGS_LASDD_SM.py:53, Utilities.py:123 */
+
+/* ---- src/surface/SurfaceFlux.py:166-443 --------------------------------
+ * most_in / most_out: psi2D_m, psi2D_m0, psi2D_h, psi2D_h0, fi2D_m, fi2D_h.
+ * qz_sfc_avg is a device scalar; sfc_val is the series value of this step. */
+int alfa_SurfaceFlux_HomogeneousConstantFlux(alfa_ctx*, const double* u, const double* v,
+    const double* TH, const double* const most_in[6], double* M_sfc_loc, double* ustar,
+    double* qz_sfc_avg, double* invOB, double* const most_out[6]);          /* :166 */
+int alfa_SurfaceFlux_HeterogeneousConstantFlux(alfa_ctx*, const double* u, const double* v,
+    const double* TH, const double* const most_in[6], double* M_sfc_loc, double* ustar,
+    double* qz_sfc_avg, double* invOB, double* const most_out[6]);          /* :209 */
+int alfa_SurfaceFlux_HomogeneousVaryingFlux(alfa_ctx*, const double* u, const double* v,
+    const double* TH, double sfc_val, const double* const most_in[6], double* M_sfc_loc,
+    double* ustar, double* qz_sfc_2D, double* qz_sfc_avg, double* invOB,
+    double* const most_out[6]);                                              /* :246 */
+int alfa_SurfaceFlux_HeterogeneousVaryingFlux(alfa_ctx*, const double* u, const double* v,
+    const double* TH, double sfc_val, const double* const most_in[6], double* M_sfc_loc,
+    double* ustar, double* qz_sfc_2D, double* qz_sfc_avg, double* invOB,
+    double* const most_out[6]);                                              /* :290 */
+int alfa_SurfaceFlux_HomogeneousPrescribedTemperature(alfa_ctx*, const double* u,
+    const double* v, const double* TH, double sfc_val, const double* const most_in[6],
+    double* M_sfc_loc, double* ustar, double* qz_sfc_2D, double* qz_sfc_avg, double* invOB,
+    double* const most_out[6]);                                              /* :335 */
+int alfa_SurfaceFlux_HeterogeneousPrescribedTemperature(alfa_ctx*, const double* u,
+    const double* v, const double* TH, double sfc_val, const double* const most_in[6],
+    double* M_sfc_loc, double* ustar, double* qz_sfc_2D, double* qz_sfc_avg, double* invOB,
+    double* const most_out[6]);                                              /* :393 */
+
+/* ---- src/pde ------------------------------------------------------------ */
+int alfa_Advection(alfa_ctx*, const double* u, const double* v, const double* w,
+                   const double* dudy, const double* dudz, const double* dvdx,
+                   const double* dvdz, const double* dwdx, const double* dwdy,
+                   double* Cx, double* Cy, double* Cz);      /* NSE_AdvectionTerms.py:246 */
+int alfa_ScalarAdvection(alfa_ctx*, const double* u, const double* v, const double* w,
+                         const double* dsdx, const double* dsdy, const double* dsdz,
+                         double* out);                        /* SCL_AdvectionTerms.py:158 */
+int alfa_BuoyancyOpt1(alfa_ctx*, const double* TH, double* buoyancy); /* NSE_BuoyancyTerms.py:49 */
+int alfa_BuoyancyOpt2(alfa_ctx*, const double* TH, double* buoyancy); /* NSE_BuoyancyTerms.py:104 */
+
+/* grads[9] as velocityGradients' out.  mom[25] receives DynamicSGS's tuple
+ * (DynamicSGS_Main.py:323-331): txx, tyy, tzz, txy, txz, tyz, Cs2_1D_avg1,
+ * Cs2_1D_avg2, beta1_1D, Cs2_3D, u_, v_, w_, u_hat, v_hat, w_hat, u_hatd,
+ * v_hatd, w_hatd, S_uvp, S_uvp_pad (mx,my,nz), S_w, S_w_pad (mx,my,nz),
+ * S_uvp_hat, S_uvp_hatd.  Entries 6..9 may be NULL (they duplicate the
+ * dedicated outputs).                                  NSE_SGSTerms.py:113 */
+int alfa_DivStressDynamicSGS(alfa_ctx*, const double* const grads[9], const double* u,
+                             const double* v, const double* w, const double* M_sfc_loc,
+                             const double* psi2D_m, const double* psi2D_m0, double* divtx,
+                             double* divty, double* divtz, double* Cs2_1D_avg1,
+                             double* Cs2_1D_avg2, double* beta1_1D, double* Cs2_3D,
+                             double* const mom[25]);
+/* mom15 = mom[10..24] of the call above.               SCL_SGSTerms.py:97 */
+int alfa_DivFluxDynamicSGS(alfa_ctx*, const double* const mom15[15], const double* TH,
+                           const double* dTHdx, const double* dTHdy, const double* dTHdz,
+                           const double* qz_sfc, double* qz, double* divq,
+                           double* Cs2PrRatio_3D, double* Cs2PrRatio_1D, double* beta2_1D);
+/* mom[10] receives StaticSGS's tuple (StaticSGS_Main.py:248-250): txx, tyy,
+ * tzz, txy, txz, tyz, S_uvp, S_uvp_pad, S_w, S_w_pad.   NSE_SGSTerms.py:186 */
+int alfa_DivStressStaticSGS(alfa_ctx*, const double* const grads[9], const double* Cs2_3D,
+                            const double* u, const double* v, const double* M_sfc_loc,
+                            const double* psi2D_m, const double* psi2D_m0, double* divtx,
+                            double* divty, double* divtz, double* const mom[10]);
+/* mom4 = S_uvp, S_uvp_pad, S_w, S_w_pad.              SCL_SGSTerms.py:169 */
+int alfa_DivFluxStaticSGS(alfa_ctx*, const double* const mom4[4], const double* Cs2PrRatio_3D,
+                          const double* dTHdx, const double* dTHdy, const double* dTHdz,
+                          const double* qz_sfc, double* qz, double* divq);
+
+/* Ug, Vg, Uadv, Vadv, THadv are the (nz) profiles the reference broadcasts
+ * over (nx, ny, nz) (Main.py:82, 120-122, Initialization.py:163-170). */
+int alfa_RHS_Momentum(alfa_ctx*, const double* u, const double* v, const double* w,
+                      const double* Ug, const double* Vg, const double* Cx, const double* Cy,
+                      const double* Cz, const double* buoyancy, const double* divtx,
+                      const double* divty, const double* divtz, const double* Uadv,
+                      const double* Vadv, double* RHS_u, double* RHS_v,
+                      double* RHS_w);                          /* NSE_AllTerms.py:48 */
+int alfa_RHS_Scalar(alfa_ctx*, const double* TH, const double* THAdvectionSum,
+                    const double* divq, const double* THadv, double* RHS_TH); /* SCL_AllTerms.py:48 */
+int alfa_PressureRC(alfa_ctx*, const double* u, const double* v, const double* w,
+                    const double* RHS_u, const double* RHS_v, const double* RHS_w,
+                    const double* RHS_u_previous, const double* RHS_v_previous,
+                    const double* RHS_w_previous, const double* divtz, double* RC_real,
+                    double* RC_imag, double* fRz_real);        /* NSE_PressureTerms.py:109 */
+int alfa_ThomasPressureSolve(alfa_ctx*, const double* RC_real, const double* RC_imag,
+                             const double* fRz_real, double* p, double* dpdx, double* dpdy,
+                             double* dpdz);           /* NSE_PressureTerms_Thomas.py:218 */
+/* in place allowed (x_new == x) */
+int alfa_AB2_uvw(alfa_ctx*, const double* u, const double* v, const double* w,
+                 const double* RHS_u, const double* RHS_u_previous, const double* RHS_v,
+                 const double* RHS_v_previous, const double* RHS_w,
+                 const double* RHS_w_previous, double* u_new, double* v_new,
+                 double* w_new);                          /* NSE_TimeAdvancement.py:45 */
+int alfa_AB2_TH(alfa_ctx*, const double* TH, const double* RHS_TH,
+                const double* RHS_TH_previous, double* TH_new); /* SCL_TimeAdvancement.py:46 */
+
+/* ---- whole step: the loop body of src/Main.py:156-541 -------------------
+ * State is held in the context.  init_state takes non-dimensional fields as
+ * Main.py holds them after Initialize_uvw/TH (u without Ugal, TH - T_0).
+ * Series (host pointers, copied): Uadv/Vadv/THadv (nrows, nz) non-dimensional
+ * (Initialize_AdvForcing), sfc (nrows) non-dimensional (Initialize_SurfaceBC);
+ * row iteration-1 is used at each iteration, as in Main.py:179-188, 225. */
+int alfa_init_state(alfa_ctx*, const double* u, const double* v, const double* w,
+                    const double* TH);
+int alfa_set_series(alfa_ctx*, const double* Uadv, const double* Vadv, const double* THadv,
+                    const double* sfc, int nrows);
+int alfa_step(alfa_ctx*, int nsteps);
+int alfa_get_state(alfa_ctx*, double* u, double* v, double* w, double* TH, double* p);
+int alfa_get_diag(alfa_ctx*, alfa_diag* out /* host; synchronises the stream */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALFA_H */

@@ -1,0 +1,461 @@
+"""Host-side mirror of the reference's function-level API on libalfa.
+
+``Alfa(cfg)`` binds one configuration (the reference's Config.py option names,
+see ``jax_alfa_b200.cases``) to a libalfa context.  Its methods carry the
+names, argument order and return tuples of the functions the reference's
+``src/Main.py`` calls, operate on torch CUDA tensors in the reference layout
+(fields (nx, ny, nz) float64 z-fastest, spectra (nx, ny//2+1, nz)
+complex128) and launch on torch's current stream.  Static arguments the
+reference threads through (kx2, ky2, ZeRo* scratch, pressure factors,
+Rayleigh arrays) are accepted for signature compatibility and taken from the
+context.  PyTorch provides device memory and streams only; all arithmetic is
+in libalfa's kernels.
+
+``Simulation`` drives the whole step (``alfa_step``) with the state resident
+on the device.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+F64 = torch.float64
+C128 = torch.complex128
+
+CONFIG_KEYS = [f for f, _ in _lib.AlfaConfig._fields_]
+
+
+def make_config(cfg):
+    c = _lib.AlfaConfig()
+    for k in CONFIG_KEYS:
+        v = cfg[k]
+        setattr(c, k, int(v) if isinstance(getattr(c, k), int) else float(v))
+    return c
+
+
+class Alfa:
+    def __init__(self, cfg, device=None):
+        if not torch.cuda.is_available():
+            raise _lib.AlfaError("libalfa needs a CUDA device (no CPU path)")
+        self.lib = _lib.load()
+        self.cfg = dict(cfg)
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        ctx = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            rc = self.lib.alfa_create(ctypes.byref(make_config(cfg)), ctypes.byref(ctx))
+        if rc != 0:
+            msg = self.lib.alfa_last_error(None)
+            raise _lib.AlfaError(f"alfa_create failed ({rc}): {msg.decode() if msg else ''}")
+        self.ctx = ctx
+        d = _lib.AlfaDerived()
+        self.lib.alfa_get_derived(ctx, ctypes.byref(d))
+        self.derived = d
+        self.nx, self.ny, self.nz = cfg["nx"], cfg["ny"], cfg["nz"]
+        self.mx, self.my = d.mx, d.my
+        self.nx_rfft, self.ny_rfft = d.nx_rfft, d.ny_rfft
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.alfa_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- plumbing
+    def _call(self, name, *args):
+        self.lib.alfa_set_stream(self.ctx, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+        rc = getattr(self.lib, name)(self.ctx, *args)
+        if rc != 0:
+            raise _lib.AlfaError(f"{name} failed ({rc}): {self.lib.alfa_last_error(self.ctx).decode()}")
+
+    def _p(self, t, shape=None, dtype=F64):
+        if not isinstance(t, torch.Tensor):
+            raise TypeError("expected a torch tensor")
+        if t.device != self.device or t.dtype != dtype or not t.is_contiguous():
+            raise ValueError(f"expected contiguous {dtype} on {self.device}, got {t.dtype} "
+                             f"on {t.device} (contiguous={t.is_contiguous()})")
+        if shape is not None and tuple(t.shape) != tuple(shape):
+            raise ValueError(f"expected shape {tuple(shape)}, got {tuple(t.shape)}")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def _pp(self, tensors, shapes=None):
+        arr = (ctypes.c_void_p * len(tensors))()
+        for i, t in enumerate(tensors):
+            arr[i] = None if t is None else self._p(t, None if shapes is None else shapes[i]).value
+        return arr
+
+    def _new(self, shape, dtype=F64):
+        return torch.empty(shape, dtype=dtype, device=self.device)
+
+    @property
+    def N(self):
+        return (self.nx, self.ny, self.nz)
+
+    @property
+    def S(self):
+        return (self.nx, self.ny_rfft, self.nz)
+
+    @property
+    def P(self):
+        return (self.mx, self.my, self.nz)
+
+    @property
+    def H(self):
+        return (self.nx, self.ny)
+
+    def _f(self, t):
+        return self._p(t, self.N)
+
+    def _prof(self, a):
+        """(nz) profile of a horizontally uniform argument (the reference
+        passes broadcast (nx, ny, nz) arrays) or of an (nz) tensor.  The
+        result may be a new tensor: hold it in a variable while its pointer
+        is in use (a freed temporary's memory is reused by the next one)."""
+        if isinstance(a, torch.Tensor) and a.dim() == 3:
+            a = a[0, 0, :]
+        return torch.as_tensor(a, dtype=F64, device=self.device).contiguous().reshape(self.nz)
+
+    # ------------------------------------------------------------- operations
+    def Wavenumber(self):
+        """Preprocess.py:73-102 (for signature compatibility)."""
+        kx = torch.fft.fftfreq(self.nx, 1 / self.nx, dtype=F64)
+        ky = torch.fft.rfftfreq(self.ny, 1 / self.ny, dtype=F64)
+        kx[self.nx // 2] = 0
+        ky[self.ny // 2] = 0
+        kx2 = kx[:, None, None].expand(self.nx, self.ny_rfft, self.nz).to(self.device)
+        ky2 = ky[None, :, None].expand(self.nx, self.ny_rfft, self.nz).to(self.device)
+        self._kx2, self._ky2 = kx2, ky2
+        return kx2, ky2
+
+    def FFT(self, F):
+        out = self._new(self.S, C128)
+        self._call("alfa_FFT", self._f(F), self._p(out, dtype=C128))
+        return out
+
+    def FFT_pad(self, F_pad):
+        out = self._new((self.mx, self.my // 2 + 1, self.nz), C128)
+        self._call("alfa_FFT_pad", self._p(F_pad, self.P), self._p(out, dtype=C128))
+        return out
+
+    def Dealias1(self, F_fft, ZeRo3D_pad_fft=None):
+        out = self._new(self.P)
+        self._call("alfa_Dealias1", self._p(F_fft, self.S, C128), self._p(out))
+        return out
+
+    def Dealias2(self, F_pad_fft, ZeRo3D_fft=None):
+        out = self._new(self.N)
+        self._call("alfa_Dealias2", self._p(F_pad_fft, (self.mx, self.my // 2 + 1, self.nz), C128),
+                   self._p(out))
+        return out
+
+    def Filtering_Explicit(self, F_fft):
+        F = self._new(self.N)
+        Fn = self._new(self.S, C128)
+        self._call("alfa_Filtering_Explicit", self._p(F_fft, self.S, C128), self._p(F),
+                   self._p(Fn, dtype=C128))
+        return F, Fn
+
+    def Filtering_Level1(self, F_fft):
+        F = self._new(self.N)
+        self._call("alfa_Filtering_Level1", self._p(F_fft, self.S, C128), self._p(F))
+        return F
+
+    def Filtering_Level2(self, F_fft):
+        F = self._new(self.N)
+        self._call("alfa_Filtering_Level2", self._p(F_fft, self.S, C128), self._p(F))
+        return F
+
+    def _axis(self, kxy2):
+        if isinstance(kxy2, (int, np.integer)):
+            return int(kxy2)
+        if isinstance(kxy2, str):
+            return {"x": 0, "y": 1}[kxy2]
+        if kxy2 is getattr(self, "_kx2", None):
+            return 0
+        if kxy2 is getattr(self, "_ky2", None):
+            return 1
+        k = torch.as_tensor(kxy2)
+        # kx2 varies along axis 0, ky2 along axis 1
+        return 0 if k.shape[0] > 1 and bool((k[1:2, 0, 0] != k[0:1, 0, 0]).any()) else 1
+
+    def Derivxy(self, F_fft, kxy2):
+        out = self._new(self.N)
+        self._call("alfa_Derivxy", self._p(F_fft, self.S, C128), self._axis(kxy2), self._p(out))
+        return out
+
+    def velocityGradients(self, u, v, w, u_fft, v_fft, w_fft, kx2, ky2, ustar, M_sfc_loc,
+                          MOSTfunctions, ZeRo3D=None):
+        out = [self._new(self.N) for _ in range(9)]
+        self._call("alfa_velocityGradients", self._f(u), self._f(v), self._f(w),
+                   self._p(u_fft, self.S, C128), self._p(v_fft, self.S, C128),
+                   self._p(w_fft, self.S, C128), self._p(ustar, self.H), self._p(M_sfc_loc, self.H),
+                   self._p(MOSTfunctions[4], self.H), self._pp(out))
+        return tuple(out)
+
+    def potentialTemperatureGradients(self, TH, kx2, ky2, ustar, qz_sfc, MOSTfunctions,
+                                      ZeRo3D=None):
+        out = [self._new(self.N) for _ in range(3)]
+        self._call("alfa_potentialTemperatureGradients", self._f(TH), self._p(ustar, self.H),
+                   self._p(qz_sfc, self.H), self._p(MOSTfunctions[5], self.H), self._pp(out))
+        return tuple(out)
+
+    def Derivz_Generic_uvp(self, F, ZeRo3D=None):
+        out = self._new(self.N)
+        self._call("alfa_Derivz_Generic_uvp", self._f(F), self._p(out))
+        return out
+
+    def Derivz_Generic_w(self, F, ZeRo3D=None):
+        out = self._new(self.N)
+        self._call("alfa_Derivz_Generic_w", self._f(F), self._p(out))
+        return out
+
+    def PlanarMean(self, F):
+        out = self._new((self.nz,))
+        self._call("alfa_PlanarMean", self._f(F), self._p(out))
+        return out
+
+    def Imfilter(self, F):
+        """Utilities.py:87-115 applied to every (x, y) plane of a field."""
+        out = self._new(self.N)
+        self._call("alfa_Imfilter", self._f(F), self._p(out))
+        return out
+
+    def ComputeBeta1(self, ff, ee, dd, cc, bb, aa):
+        co = torch.stack([torch.as_tensor(x, dtype=F64, device=self.device)
+                          for x in (ff, ee, dd, cc, bb, aa)]).contiguous()
+        n = co.shape[1]
+        out = self._new((n,))
+        self._call("alfa_ComputeBeta", self._p(co), n, self._p(out))
+        return out
+
+    ComputeBeta2 = ComputeBeta1
+
+    # ---------------------------------------------------------------- surface
+    def _surface(self, name, u, v, TH, MOST, sfc_val=None):
+        M, us, inv = self._new(self.H), self._new(self.H), self._new(self.H)
+        q2 = self._new(self.H)
+        qavg = self._new(())
+        mo = [self._new(self.H) for _ in range(6)]
+        mi = self._pp(list(MOST), [self.H] * 6)
+        if sfc_val is None:
+            self._call(name, self._f(u), self._f(v), self._f(TH), mi, self._p(M), self._p(us),
+                       self._p(qavg), self._p(inv), self._pp(mo))
+            return M, us, qavg, inv, tuple(mo)
+        self._call(name, self._f(u), self._f(v), self._f(TH), ctypes.c_double(float(sfc_val)), mi,
+                   self._p(M), self._p(us), self._p(q2), self._p(qavg), self._p(inv), self._pp(mo))
+        return M, us, q2, qavg, inv, tuple(mo)
+
+    def SurfaceFlux_HomogeneousConstantFlux(self, u, v, TH, MOSTfunctions):
+        return self._surface("alfa_SurfaceFlux_HomogeneousConstantFlux", u, v, TH, MOSTfunctions)
+
+    def SurfaceFlux_HeterogeneousConstantFlux(self, u, v, TH, MOSTfunctions):
+        return self._surface("alfa_SurfaceFlux_HeterogeneousConstantFlux", u, v, TH, MOSTfunctions)
+
+    def SurfaceFlux_HomogeneousVaryingFlux(self, u, v, TH, qz_sfc_t, MOSTfunctions):
+        return self._surface("alfa_SurfaceFlux_HomogeneousVaryingFlux", u, v, TH, MOSTfunctions,
+                             qz_sfc_t)
+
+    def SurfaceFlux_HeterogeneousVaryingFlux(self, u, v, TH, qz_sfc_t, MOSTfunctions):
+        return self._surface("alfa_SurfaceFlux_HeterogeneousVaryingFlux", u, v, TH, MOSTfunctions,
+                             qz_sfc_t)
+
+    def SurfaceFlux_HomogeneousPrescribedTemperature(self, u, v, TH, TH_sfc_t, MOSTfunctions):
+        return self._surface("alfa_SurfaceFlux_HomogeneousPrescribedTemperature", u, v, TH,
+                             MOSTfunctions, TH_sfc_t)
+
+    def SurfaceFlux_HeterogeneousPrescribedTemperature(self, u, v, TH, TH_sfc_t, MOSTfunctions):
+        return self._surface("alfa_SurfaceFlux_HeterogeneousPrescribedTemperature", u, v, TH,
+                             MOSTfunctions, TH_sfc_t)
+
+    # -------------------------------------------------------------------- pde
+    def Advection(self, u, v, w, dudy, dudz, dvdx, dvdz, dwdx, dwdy, ZeRo3D=None, ZeRo3D_fft=None,
+                  ZeRo3D_pad=None, ZeRo3D_pad_fft=None):
+        out = [self._new(self.N) for _ in range(3)]
+        self._call("alfa_Advection", *[self._f(x) for x in (u, v, w, dudy, dudz, dvdx, dvdz, dwdx,
+                                                              dwdy)], *[self._p(x) for x in out])
+        return tuple(out)
+
+    def ScalarAdvection(self, u, v, w, dsdx, dsdy, dsdz, ZeRo3D=None, ZeRo3D_fft=None,
+                        ZeRo3D_pad=None, ZeRo3D_pad_fft=None):
+        out = self._new(self.N)
+        self._call("alfa_ScalarAdvection", *[self._f(x) for x in (u, v, w, dsdx, dsdy, dsdz)],
+                   self._p(out))
+        return out
+
+    def _check_dry(self, H):
+        if H is not None and bool(torch.as_tensor(H).abs().max() != 0):
+            raise NotImplementedError("moisture (H != 0) is not part of this build")
+
+    def BuoyancyOpt1(self, TH, H=None, ZeRo3D=None):
+        self._check_dry(H)
+        out = self._new(self.N)
+        self._call("alfa_BuoyancyOpt1", self._f(TH), self._p(out))
+        return out
+
+    def BuoyancyOpt2(self, TH, H=None, ZeRo3D=None):
+        self._check_dry(H)
+        out = self._new(self.N)
+        self._call("alfa_BuoyancyOpt2", self._f(TH), self._p(out))
+        return out
+
+    def _mom25(self):
+        return [None if 6 <= i <= 9 else self._new(self.P if i in (20, 22) else self.N)
+                for i in range(25)]
+
+    def DivStressDynamicSGS(self, dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz,
+                            u, v, w, M_sfc_loc, MOSTfunctions, ZeRo3D=None, ZeRo3D_fft=None,
+                            ZeRo3D_pad_fft=None, kx2=None, ky2=None):
+        g = self._pp([dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz], [self.N] * 9)
+        divt = [self._new(self.N) for _ in range(3)]
+        a1, a2, b1 = self._new((self.nz,)), self._new((self.nz,)), self._new((self.nz,))
+        cs2 = self._new(self.N)
+        mom = self._mom25()
+        self._call("alfa_DivStressDynamicSGS", g, self._f(u), self._f(v), self._f(w),
+                   self._p(M_sfc_loc, self.H), self._p(MOSTfunctions[0], self.H),
+                   self._p(MOSTfunctions[1], self.H), *[self._p(x) for x in divt], self._p(a1),
+                   self._p(a2), self._p(b1), self._p(cs2), self._pp(mom))
+        mom[6], mom[7], mom[8], mom[9] = a1, a2, b1, cs2
+        return (*divt, a1, a2, b1, cs2, tuple(mom))
+
+    def DivFluxDynamicSGS(self, dynamicSGSmomentum, TH, dTHdx, dTHdy, dTHdz, SHFX, ZeRo3D=None,
+                          ZeRo3D_fft=None, ZeRo3D_pad_fft=None, kx2=None, ky2=None):
+        m = list(dynamicSGSmomentum)
+        shapes = [self.P if i in (10, 12) else self.N for i in range(15)]
+        qz, divq, r3 = self._new(self.N), self._new(self.N), self._new(self.N)
+        r1, b2 = self._new((self.nz,)), self._new((self.nz,))
+        self._call("alfa_DivFluxDynamicSGS", self._pp(m, shapes), self._f(TH), self._f(dTHdx),
+                   self._f(dTHdy), self._f(dTHdz), self._p(SHFX.contiguous(), self.H), self._p(qz),
+                   self._p(divq), self._p(r3), self._p(r1), self._p(b2))
+        return qz, divq, r3, r1, b2
+
+    def DivStressStaticSGS(self, dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz, Cs2_3D,
+                           u, v, M_sfc_loc, MOSTfunctions, ZeRo3D=None, ZeRo3D_fft=None,
+                           ZeRo3D_pad_fft=None, kx2=None, ky2=None):
+        g = self._pp([dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz], [self.N] * 9)
+        divt = [self._new(self.N) for _ in range(3)]
+        mom = [self._new(self.P if i in (7, 9) else self.N) for i in range(10)]
+        self._call("alfa_DivStressStaticSGS", g, self._f(Cs2_3D), self._f(u), self._f(v),
+                   self._p(M_sfc_loc, self.H), self._p(MOSTfunctions[0], self.H),
+                   self._p(MOSTfunctions[1], self.H), *[self._p(x) for x in divt], self._pp(mom))
+        return (*divt, tuple(mom))
+
+    def DivFluxStaticSGS(self, staticSGSmomentum, Cs2PrRatio_3D, dTHdx, dTHdy, dTHdz, SHFX,
+                         ZeRo3D=None, ZeRo3D_fft=None, ZeRo3D_pad_fft=None, kx2=None, ky2=None):
+        m = list(staticSGSmomentum)
+        qz, divq = self._new(self.N), self._new(self.N)
+        self._call("alfa_DivFluxStaticSGS", self._pp(m, [self.N, self.P, self.N, self.P]),
+                   self._f(Cs2PrRatio_3D), self._f(dTHdx), self._f(dTHdy), self._f(dTHdz),
+                   self._p(SHFX.contiguous(), self.H), self._p(qz), self._p(divq))
+        return qz, divq
+
+    def RHS_Momentum(self, u, v, w, Ug, Vg, Cx, Cy, Cz, buoyancy, divtx, divty, divtz,
+                     RayleighDampCoeff=None, RayleighDampCoeff_stag=None, Uadv=None, Vadv=None):
+        out = [self._new(self.N) for _ in range(3)]
+        z = torch.zeros(self.nz, dtype=F64, device=self.device)
+        Ua = z if Uadv is None else self._prof(Uadv)
+        Va = z if Vadv is None else self._prof(Vadv)
+        ug, vg = self._prof(Ug), self._prof(Vg)
+        self._call("alfa_RHS_Momentum", self._f(u), self._f(v), self._f(w),
+                   self._p(ug), self._p(vg),
+                   *[self._f(x) for x in (Cx, Cy, Cz, buoyancy, divtx, divty, divtz)],
+                   self._p(Ua), self._p(Va), *[self._p(x) for x in out])
+        return tuple(out)
+
+    def RHS_Scalar(self, TH, THAdvectionSum, divq, RayleighDampCoeff_stag=None, THadv=None):
+        out = self._new(self.N)
+        Ta = torch.zeros(self.nz, dtype=F64, device=self.device) if THadv is None else self._prof(THadv)
+        self._call("alfa_RHS_Scalar", self._f(TH), self._f(THAdvectionSum), self._f(divq),
+                   self._p(Ta), self._p(out))
+        return out
+
+    def PressureRC(self, u, v, w, RHS_u, RHS_v, RHS_w, RHS_u_previous, RHS_v_previous,
+                   RHS_w_previous, divtz, kr2_pressure=None, kc2_pressure=None):
+        R = (self.nx, self.ny_rfft, self.nz + 1)
+        RCr, RCi, fRz = self._new(R), self._new(R), self._new(self.S)
+        self._call("alfa_PressureRC", *[self._f(x) for x in (u, v, w, RHS_u, RHS_v, RHS_w,
+                                                              RHS_u_previous, RHS_v_previous,
+                                                              RHS_w_previous, divtz)],
+                   self._p(RCr), self._p(RCi), self._p(fRz))
+        return RCr, RCi, fRz
+
+    def ThomasPressureSolve(self, RC_real, RC_imag, fRz_real, b_thomas=None, m_thomas=None,
+                            c_pressure=None):
+        R = (self.nx, self.ny_rfft, self.nz + 1)
+        out = [self._new(self.N) for _ in range(4)]
+        self._call("alfa_ThomasPressureSolve", self._p(RC_real, R), self._p(RC_imag, R),
+                   self._p(fRz_real, self.S), *[self._p(x) for x in out])
+        return tuple(out)
+
+    def AB2_uvw(self, u, v, w, RHS_u, RHS_u_previous, RHS_v, RHS_v_previous, RHS_w,
+                RHS_w_previous):
+        out = [self._new(self.N) for _ in range(3)]
+        self._call("alfa_AB2_uvw", *[self._f(x) for x in (u, v, w, RHS_u, RHS_u_previous, RHS_v,
+                                                           RHS_v_previous, RHS_w, RHS_w_previous)],
+                   *[self._p(x) for x in out])
+        return tuple(out)
+
+    def AB2_TH(self, TH, RHS_TH, RHS_TH_previous):
+        out = self._new(self.N)
+        self._call("alfa_AB2_TH", self._f(TH), self._f(RHS_TH), self._f(RHS_TH_previous),
+                   self._p(out))
+        return out
+
+
+class Simulation:
+    """The reference's time loop (``src/Main.py:156-541``) run by libalfa
+    with the state on the device.  Fields in: dimensional (u total incl.
+    Ugal, theta absolute) as the reference's input files hold them."""
+
+    def __init__(self, cfg, u, v, w, th, surface_series=None, adv_series=None, device=None):
+        self.alfa = Alfa(cfg, device)
+        a = self.alfa
+        z = a.derived.z_scale
+        dev = a.device
+        tt = lambda x: torch.as_tensor(np.ascontiguousarray(x), dtype=F64).to(dev)
+        self._call = a._call
+        # keep the device copies alive until the (asynchronous) call is enqueued
+        fields = (tt(u) - cfg["Ugal"], tt(v), tt(w), tt(th) - cfg["T_0"])
+        self._call("alfa_init_state", *[a._f(x) for x in fields])
+        torch.cuda.current_stream(dev).synchronize()
+        del fields
+        nrows = 0
+        ptr = lambda x: None if x is None else np.ascontiguousarray(x, dtype=np.float64).ctypes.data_as(_lib.c_double_p)
+        keep = []
+        U = V = T = S = None
+        if adv_series is not None:
+            U, V, T = [np.ascontiguousarray(x * z, dtype=np.float64) for x in adv_series]
+            nrows = U.shape[0]
+            keep += [U, V, T]
+        if surface_series is not None:
+            s = np.asarray(surface_series, dtype=np.float64)
+            S = np.ascontiguousarray(s if cfg["optSurfBC"] == 1 else s - cfg["T_0"])
+            nrows = max(nrows, S.shape[0]) if adv_series is None else nrows
+            keep.append(S)
+        if U is not None and S is not None and S.shape[0] != U.shape[0]:
+            raise ValueError("series lengths differ")
+        self._call("alfa_set_series", ptr(U), ptr(V), ptr(T), ptr(S), nrows)
+
+    def step(self, n=1):
+        self._call("alfa_step", int(n))
+        return self
+
+    def state(self):
+        a = self.alfa
+        out = [a._new(a.N) for _ in range(5)]
+        self._call("alfa_get_state", *[a._p(x) for x in out])
+        return dict(zip(("u", "v", "w", "TH", "p"), out))
+
+    def diag(self):
+        d = _lib.AlfaDiag()
+        a = self.alfa
+        a.lib.alfa_set_stream(a.ctx, ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream))
+        rc = a.lib.alfa_get_diag(a.ctx, ctypes.byref(d))
+        if rc != 0:
+            raise _lib.AlfaError(a.lib.alfa_last_error(a.ctx).decode())
+        return {k: getattr(d, k) for k, _ in d._fields_}

@@ -1,0 +1,1379 @@
+// Engine set-up, the reference-named C-ABI entry points and the whole-step
+// driver (the loop body of the reference's src/Main.py:156-541).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "alfa_internal.cuh"
+#include "alfa_physics.cuh"
+
+using namespace alfa;
+
+namespace alfa {
+
+// ---------------------------------------------------------------------------
+// Workspace: named field slots carved from one allocation
+// ---------------------------------------------------------------------------
+struct Work {
+  // model state (whole-step driver)
+  double *u, *v, *w, *TH, *p;
+  double *RHS[4], *RHSp[4];
+  double *Cs2, *Cs2Pr;
+  double *most[6], *most_new[6];
+  double *M, *ustar, *q2, *invOB, *qz_plane;
+  cd *ufft, *vfft, *wfft;
+  double* Ug;  // (nz) profiles
+  double* Vg;
+  double* zero_prof;
+  double* series_adv = nullptr;  // (nrows, 3, nz) non-dimensional Uadv, Vadv, THadv
+  int series_rows = 0;
+  std::vector<double> sfc_series;  // host
+  // step temporaries
+  double* g[9];
+  double* gT[3];
+  double *Cx, *Cy, *Cz, *THadv, *buoy;
+  double *divt[3], *divq, *qz;
+  double* mom[25];
+  // internal SGS temporaries
+  double *S12, *S13, *S23;
+  double *ph[6], *pd[6], *Sh[6], *Sd[6], *SSh[6], *SSd[6];
+  double *LM, *MM;
+  double *Th, *Td, *uTh[3], *uTd[3], *Gh[3], *Gd[3], *SGh[3], *SGd[3];
+  double *qx, *qy;
+  double* Pb[10];  // padded fields
+  // pressure
+  double *RCr, *RCi, *fRzr;
+  cd *fRx, *fRy, *fRz, *fp, *fb2;
+  double* planes2;
+  double *dp[3];
+  double* prof;  // small profiles scratch
+  int iteration = 1;
+  int have_state = 0;
+  double CFL = 0, CFLmax = 0;
+  double* d_cfl;  // 3 maxima
+  double* d_qavg;
+};
+
+}  // namespace alfa
+
+struct alfa_ctx {
+  Engine e;
+  Work w;
+  void* base = nullptr;
+  size_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// set-up
+// ---------------------------------------------------------------------------
+static bool factor_23(int n, int* rad, int* np) {
+  int m = n, k = 0;
+  const int rs[5] = {16, 8, 4, 3, 2};
+  for (int r : rs) {
+    while (m % r == 0 && m > 1) {
+      if (k >= 8) return false;
+      rad[k++] = r;
+      m /= r;
+    }
+  }
+  *np = k;
+  return m == 1 && n >= 2;
+}
+
+static int make_plan(Engine& e, int n, FftPlan* p) {
+  p->n = n;
+  if (!factor_23(n, p->rad, &p->npass)) return -1;
+  std::vector<cd> tw(n);
+  for (int q = 0; q < n; q++) {
+    const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)q / n;
+    tw[q] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  void* d = nullptr;
+  if (cudaMalloc(&d, n * sizeof(cd)) != cudaSuccess) return -2;
+  cudaMemcpy(d, tw.data(), n * sizeof(cd), cudaMemcpyHostToDevice);
+  e.allocs.push_back(d);
+  p->tw = (const cd*)d;
+  return 0;
+}
+
+static double* upload(Engine& e, const std::vector<double>& h) {
+  void* d = nullptr;
+  if (cudaMalloc(&d, h.size() * sizeof(double) + 8) != cudaSuccess) return nullptr;
+  cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+  e.allocs.push_back(d);
+  return (double*)d;
+}
+
+namespace alfa {
+
+int check_launch(Engine& e, const char* what) {
+  cudaError_t st = cudaGetLastError();
+  if (st != cudaSuccess) {
+    e.err = std::string(what) + ": " + cudaGetErrorString(st);
+    return ALFA_E_CUDA;
+  }
+  return ALFA_OK;
+}
+
+int engine_init(Engine& e, const alfa_config& c) {
+  e.cfg = c;
+  const double PI = 3.141592653589793;  // jnp.pi
+  e.nx = c.nx;
+  e.ny = c.ny;
+  e.nz = c.nz;
+  if (c.nx < 4 || c.ny < 4 || c.nz < 3 || (c.nx % 2) || (c.ny % 2))
+    return e.fail("grid must have even nx, ny >= 4 and nz >= 3", ALFA_E_CONFIG);
+  if (c.FGR != 1) return e.fail("only FGR = 1 (3/2-rule dealiasing) is implemented", ALFA_E_CONFIG);
+  if (!(c.optSgs == 0 || c.optSgs == 1 || c.optSgs == 3))
+    return e.fail("optSgs must be 0 (static), 1 (LASDD-SM) or 3 (LAD-SM)", ALFA_E_CONFIG);
+  if (c.dynamicSGS_call_time < 1) return e.fail("dynamicSGS_call_time must be >= 1", ALFA_E_CONFIG);
+  e.mx = (int)(1.5 * c.nx);
+  e.my = (int)(1.5 * c.ny);
+  e.nxh = c.nx / 2 + 1;
+  e.nyh = c.ny / 2 + 1;
+  e.mxh = e.mx / 2 + 1;
+  e.myh = e.my / 2 + 1;
+  // src/config/DerivedVars.py:48-112 (u_scale = TH_scale = 1)
+  e.z_scale = c.l_x / (2 * PI);
+  e.g_nondim = 9.81 * e.z_scale / 1.0;
+  e.f_nondim = c.f_coriolis * (e.z_scale / 1.0);
+  e.T0_nondim = c.T_0 / 1.0;
+  e.inversion_nondim = c.inversion * (e.z_scale / 1.0);
+  e.qz_sfc_const = c.SensibleHeatFlux * 1.0 / (1.0 * 1.0);
+  e.dx = 2 * PI / c.nx;
+  e.dy = 2 * PI / c.ny;
+  e.dz = (c.l_z / e.z_scale) / (c.nz - 1);
+  e.idz = 1.0 / e.dz;
+  e.L = c.FGR * std::pow(e.dx * e.dy * e.dz, 1.0 / 3.0);
+  e.dt_nondim = c.dt * 1.0 / e.z_scale;
+  e.TFR = 2;
+  e.optDealias = 1;
+  e.Cs2_init = c.Cs2;
+  e.Cs2PrRatio_init = c.Cs2PrRatio;
+  e.z_damping_nondim = c.z_damping / e.z_scale;
+  e.RelaxTime_nondim = c.RelaxTime * (1.0 / e.z_scale);
+  // Filtering.py cut-offs (Python round(): ties to even)
+  const double inv2fgr = 1.0 / (2.0 * c.FGR);
+  e.cut_e[0] = (int)std::nearbyint(c.nx * inv2fgr);
+  e.cut_e[1] = (int)std::nearbyint(c.ny * inv2fgr);
+  e.cut_1[0] = (int)std::nearbyint(c.nx / (2 * c.FGR * e.TFR));
+  e.cut_1[1] = (int)std::nearbyint(c.ny / (2 * c.FGR * e.TFR));
+  e.cut_2[0] = (int)std::nearbyint(c.nx / (2 * c.FGR * e.TFR * e.TFR));
+  e.cut_2[1] = (int)std::nearbyint(c.ny / (2 * c.FGR * e.TFR * e.TFR));
+  if (e.cut_2[0] < 1 || e.cut_2[1] < 1) return e.fail("grid too small for the test filters", ALFA_E_CONFIG);
+
+  if (make_plan(e, e.nx, &e.pnx) || make_plan(e, e.ny, &e.pny) || make_plan(e, e.mx, &e.pmx) ||
+      make_plan(e, e.my, &e.pmy))
+    return e.fail("nx and ny must be of the form 2^a 3^b (FFT radices 2, 3, 4, 8, 16)",
+                  ALFA_E_CONFIG);
+
+  // wavenumbers (Preprocess.py:89-94): fftfreq / rfftfreq with Nyquist 0
+  std::vector<double> kx(c.nx), ky(e.nyh), kr(c.nx);
+  for (int i = 0; i < c.nx; i++) {
+    kx[i] = (i < c.nx / 2) ? i : i - c.nx;
+    kr[i] = kx[i];  // pressure wavenumbers keep the Nyquist (NSE_PressureTerms.py:72-77)
+  }
+  kx[c.nx / 2] = 0.0;
+  for (int j = 0; j < e.nyh; j++) ky[j] = j;
+  ky[c.ny / 2] = 0.0;
+  e.d_kx = upload(e, kx);
+  e.d_ky = upload(e, ky);
+  e.d_kr = upload(e, kr);
+
+  // Thomas factors (NSE_PressureTerms_Thomas.py:151-214)
+  const int nz = c.nz, N1 = nz + 1;
+  const double dz = e.dz;
+  std::vector<double> a(N1, 1.0 / (dz * dz)), cc(N1, 1.0 / (dz * dz));
+  a[0] = 0;
+  a[nz] = -1;
+  cc[0] = 1;
+  cc[nz] = 0;
+  const size_t nm = (size_t)c.nx * e.nyh;
+  std::vector<double> bt(nm * N1), mt((size_t)nz * nm);
+  for (int i = 0; i < c.nx; i++) {
+    for (int j = 0; j < e.nyh; j++) {
+      const size_t m = (size_t)i * e.nyh + j;
+      double* b = &bt[m * N1];
+      const double kr2 = kr[i], kc2 = j;
+      const double bb = -(kr2 * kr2 + kc2 * kc2 + 2 / (dz * dz));
+      for (int k = 0; k < N1; k++) b[k] = bb;
+      b[0] = -1;
+      b[nz] = 1;
+      if (i == 0 && j == 0 && c.optPressureSolver == 1)
+        for (int k = 1; k < nz; k++) b[k] = -(1.0 + 2.0 / (dz * dz));
+      for (int k = 1; k < N1; k++) {
+        const double mk = a[k] / b[k - 1];
+        mt[(size_t)(k - 1) * nm + m] = mk;
+        b[k] = b[k] - mk * cc[k - 1];
+      }
+    }
+  }
+  e.d_b_thomas = upload(e, bt);
+  e.d_m_thomas = upload(e, mt);
+  e.d_c_p = upload(e, cc);
+
+  // Rayleigh damping profiles (Initialization.py:395-460)
+  {
+    const double inv = 1.0 / e.RelaxTime_nondim;
+    const double ztop = c.l_z / e.z_scale;
+    const double thick = ztop - e.z_damping_nondim;
+    std::vector<double> r1(nz), r2(nz);
+    for (int k = 0; k < nz; k++) {
+      const double z1 = k * dz, z2 = (k + 0.5) * dz;
+      r1[k] = (z1 >= e.z_damping_nondim && z1 <= ztop)
+                  ? 0.5 * inv * (1.0 - std::cos(PI * (z1 - e.z_damping_nondim) / thick))
+                  : 0.0;
+      r2[k] = (z2 >= e.z_damping_nondim && z2 <= ztop)
+                  ? 0.5 * inv * (1.0 - std::cos(PI * (z2 - e.z_damping_nondim) / thick))
+                  : 0.0;
+    }
+    e.d_rd = upload(e, r1);
+    e.d_rd_stag = upload(e, r2);
+  }
+  if (!e.d_kx || !e.d_b_thomas || !e.d_rd) return e.fail("device allocation failed", ALFA_E_CUDA);
+  return ALFA_OK;
+}
+
+void engine_free(Engine& e) {
+  for (void* p : e.allocs) cudaFree(p);
+  e.allocs.clear();
+}
+
+}  // namespace alfa
+
+// carve the workspace: counts first, then pointers
+struct Carver {
+  char* base;
+  size_t off = 0;
+  bool dry;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = dry ? nullptr : (T*)(base + off);
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+static void carve(alfa_ctx* c, Carver& k) {
+  Engine& e = c->e;
+  Work& w = c->w;
+  const size_t N = e.N(), P = e.P(), S = e.S(), H = e.H(), nz = e.nz;
+  const size_t R = (size_t)e.nx * e.nyh * (nz + 1);
+  w.u = k.take<double>(N);
+  w.v = k.take<double>(N);
+  w.w = k.take<double>(N);
+  w.TH = k.take<double>(N);
+  w.p = k.take<double>(N);
+  for (int i = 0; i < 4; i++) {
+    w.RHS[i] = k.take<double>(N);
+    w.RHSp[i] = k.take<double>(N);
+  }
+  w.Cs2 = k.take<double>(N);
+  w.Cs2Pr = k.take<double>(N);
+  for (int i = 0; i < 6; i++) {
+    w.most[i] = k.take<double>(H);
+    w.most_new[i] = k.take<double>(H);
+  }
+  w.M = k.take<double>(H);
+  w.ustar = k.take<double>(H);
+  w.q2 = k.take<double>(H);
+  w.invOB = k.take<double>(H);
+  w.qz_plane = k.take<double>(H);
+  w.ufft = k.take<cd>(S);
+  w.vfft = k.take<cd>(S);
+  w.wfft = k.take<cd>(S);
+  w.Ug = k.take<double>(nz);
+  w.Vg = k.take<double>(nz);
+  w.zero_prof = k.take<double>(nz);
+  for (int i = 0; i < 9; i++) w.g[i] = k.take<double>(N);
+  for (int i = 0; i < 3; i++) w.gT[i] = k.take<double>(N);
+  w.Cx = k.take<double>(N);
+  w.Cy = k.take<double>(N);
+  w.Cz = k.take<double>(N);
+  w.THadv = k.take<double>(N);
+  w.buoy = k.take<double>(N);
+  for (int i = 0; i < 3; i++) w.divt[i] = k.take<double>(N);
+  w.divq = k.take<double>(N);
+  w.qz = k.take<double>(N);
+  for (int i = 0; i < 25; i++) {
+    if (i >= 6 && i <= 9) {
+      w.mom[i] = nullptr;
+      continue;
+    }
+    w.mom[i] = (i == 20 || i == 22) ? k.take<double>(P) : k.take<double>(N);
+  }
+  w.S12 = k.take<double>(N);
+  w.S13 = k.take<double>(N);
+  w.S23 = k.take<double>(N);
+  for (int i = 0; i < 6; i++) {
+    w.ph[i] = k.take<double>(N);
+    w.pd[i] = k.take<double>(N);
+    w.Sh[i] = k.take<double>(N);
+    w.Sd[i] = k.take<double>(N);
+    w.SSh[i] = k.take<double>(N);
+    w.SSd[i] = k.take<double>(N);
+  }
+  w.LM = k.take<double>(N);
+  w.MM = k.take<double>(N);
+  w.Th = k.take<double>(N);
+  w.Td = k.take<double>(N);
+  for (int i = 0; i < 3; i++) {
+    w.uTh[i] = k.take<double>(N);
+    w.uTd[i] = k.take<double>(N);
+    w.Gh[i] = k.take<double>(N);
+    w.Gd[i] = k.take<double>(N);
+    w.SGh[i] = k.take<double>(N);
+    w.SGd[i] = k.take<double>(N);
+  }
+  w.qx = k.take<double>(N);
+  w.qy = k.take<double>(N);
+  for (int i = 0; i < 10; i++) w.Pb[i] = k.take<double>(P);
+  w.RCr = k.take<double>(R);
+  w.RCi = k.take<double>(R);
+  w.fRzr = k.take<double>(S);
+  w.fRx = k.take<cd>(S);
+  w.fRy = k.take<cd>(S);
+  w.fRz = k.take<cd>(S);
+  w.fp = k.take<cd>(S);
+  w.fb2 = k.take<cd>((size_t)e.nx * e.nyh * 2);
+  w.planes2 = k.take<double>(H * 2);
+  for (int i = 0; i < 3; i++) w.dp[i] = k.take<double>(N);
+  w.prof = k.take<double>(64 * nz + 64);
+  w.d_cfl = k.take<double>(4);
+  w.d_qavg = k.take<double>(4);
+  // engine scratch
+  e.T_elems = (size_t)e.mx * e.myh * nz;
+  for (int i = 0; i < 4; i++) e.T[i] = k.take<cd>(e.T_elems);
+  e.red_elems = (size_t)256 * 12 * nz + 1024;
+  e.red = k.take<double>(e.red_elems);
+  e.scal = k.take<double>(64 * nz + 256);
+  e.W_elems = N;
+  e.W = k.take<double>(N);
+}
+
+// ---------------------------------------------------------------------------
+// internal implementations shared by the C-ABI and the step driver
+// ---------------------------------------------------------------------------
+static Loader ld(const Engine& e, int kind, std::initializer_list<const double*> a,
+                 double c0 = 0.0, double c1 = 0.0, int sub = 0) {
+  Loader L{};
+  L.kind = kind;
+  L.sub = sub;
+  L.nz = e.nz;
+  int i = 0;
+  for (const double* p : a) L.a[i++] = p;
+  L.c[0] = c0;
+  L.c[1] = c1;
+  return L;
+}
+
+// Derivxy(FFT(field)) with per-output accumulate flags
+static void deriv_field_acc(Engine& e, const Loader& L, double* dx, int accx, double* dy,
+                            int accy) {
+  launch_y_fwd(e, L, e.nx, e.pny, e.nyh, e.T[0]);
+  XOut o[2];
+  int n = 0;
+  auto mk = [&](int map, cd* T) {
+    XOut x{};
+    x.kind = XO_INV;
+    x.map = map;
+    x.K = e.nyh;
+    x.rows = e.nx;
+    x.dst = T;
+    x.inv = e.pnx;
+    return x;
+  };
+  if (dx) o[n++] = mk(MAP_DX, e.T[1]);
+  if (dy) o[n++] = mk(MAP_DY, e.T[2]);
+  launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, n, o, e.nyh);
+  const double s = 1.0 / ((double)e.nx * e.ny);
+  if (dx) launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, s, dx, accx);
+  if (dy) launch_y_inv(e, e.T[2], e.nx, e.nyh, e.pny, s, dy, accy);
+}
+
+// NSE_SGSTerms.py:55-105
+static void div_stress(alfa_ctx* c, const double* txx, const double* tyy, const double* tzz,
+                       const double* txy, const double* txz, const double* tyz, double* dtx,
+                       double* dty, double* dtz) {
+  Engine& e = c->e;
+  deriv_field_acc(e, ld_field(e, txx), dtx, 0, nullptr, 0);
+  deriv_field_acc(e, ld_field(e, txy), dty, 0, dtx, 1);
+  deriv_field_acc(e, ld_field(e, tyy), nullptr, 0, dty, 1);
+  deriv_field_acc(e, ld_field(e, txz), dtz, 0, nullptr, 0);
+  deriv_field_acc(e, ld_field(e, tyz), nullptr, 0, dtz, 1);
+  divergence_finish(e, dtx, txz, 1);
+  divergence_finish(e, dty, tyz, 1);
+  divergence_finish(e, dtz, tzz, 0);
+}
+
+// SCL_SGSTerms.py:55-89
+static void div_flux(alfa_ctx* c, const double* qx, const double* qy, const double* qz,
+                     double* divq) {
+  Engine& e = c->e;
+  deriv_field_acc(e, ld_field(e, qx), divq, 0, nullptr, 0);
+  deriv_field_acc(e, ld_field(e, qy), nullptr, 0, divq, 1);
+  divergence_finish(e, divq, qz, 1);
+}
+
+static void advection(alfa_ctx* c, const double* u, const double* v, const double* w,
+                      const double* uy, const double* uz, const double* vx, const double* vz,
+                      const double* wx, const double* wy, double* Cx, double* Cy, double* Cz) {
+  Engine& e = c->e;
+  double* const* Pb = c->w.Pb;
+  const double* src[9] = {u, v, w, uy, uz, vx, vz, wx, wy};
+  for (int i = 0; i < 9; i++) op_pad(e, ld_field(e, src[i]), Pb[i]);
+  // Pb: 0 up 1 vp 2 wp 3 uy 4 uz 5 vx 6 vz 7 wx 8 wy
+  op_unpad(e, ld(e, LD_ADV_XY, {Pb[1], Pb[3], Pb[5], Pb[2], Pb[4], Pb[7]}), Cx);
+  op_unpad(e, ld(e, LD_ADV_XY, {Pb[0], Pb[5], Pb[3], Pb[2], Pb[6], Pb[8]}), Cy);
+  op_unpad(e, ld(e, LD_ADV_Z, {Pb[0], Pb[1], Pb[7], Pb[4], Pb[8], Pb[6]}), Cz);
+}
+
+// SCL_AdvectionTerms.py:57-106; reuse_uvw: Pb[0..2] already hold the padded
+// u, v, w of this step (the reference recomputes the identical values)
+static void scalar_advection(alfa_ctx* c, const double* u, const double* v, const double* w,
+                             const double* sx, const double* sy, const double* sz, double* out,
+                             bool reuse_uvw) {
+  Engine& e = c->e;
+  double* const* Pb = c->w.Pb;
+  if (!reuse_uvw) {
+    op_pad(e, ld_field(e, u), Pb[0]);
+    op_pad(e, ld_field(e, v), Pb[1]);
+    op_pad(e, ld_field(e, w), Pb[2]);
+  }
+  op_pad(e, ld_field(e, sx), Pb[3]);
+  op_pad(e, ld_field(e, sy), Pb[4]);
+  op_pad(e, ld_field(e, sz), Pb[5]);
+  op_unpad(e, ld(e, LD_SCALAR_ADV, {Pb[0], Pb[1], Pb[2], Pb[3], Pb[4], Pb[5]}), out);
+}
+
+// Stresses of StressesUVPnodes_Dealias / StressesWnodes_Dealias from the
+// strains (uvp padded components in Pb[0..3], |S|_pad), Cs2_pad in Pb[9];
+// then the w-node strains are padded into Pb[0..5].
+static void sgs_stresses(alfa_ctx* c, const double* const g[9], const double* S_uvp_pad,
+                         const double* u, const double* v, const double* M, const double* pm,
+                         const double* pm0, double* const t6[6], double* S_w, double* S_w_pad) {
+  Engine& e = c->e;
+  double* const* Pb = c->w.Pb;
+  const double cst = -2 * std::pow(e.L, 2.0);
+  for (int i = 0; i < 4; i++)
+    op_unpad(e, ld(e, LD_STRESS_UVP, {Pb[9], S_uvp_pad, Pb[i]}, cst), t6[i]);
+  Loader Lw = ld(e, LD_W_SXX, {g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8]});
+  for (int s = 0; s < 6; s++) {
+    Lw.sub = s;
+    op_pad(e, Lw, Pb[s]);
+  }
+  smag_w(e, g, S_w);
+  const double* q6[6] = {Pb[0], Pb[1], Pb[2], Pb[3], Pb[4], Pb[5]};
+  smag6(e, q6, e.P(), S_w_pad);
+  op_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[4]}, cst), t6[4]);
+  op_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[5]}, cst), t6[5]);
+  wall_override(e, u, v, M, pm, pm0, t6[4], t6[5]);
+}
+
+// uvp strains + their padded copies: S11..S33 alias dudx, dvdy, dwdz.
+static void uvp_strains_padded(alfa_ctx* c, const double* const g[9], const double* Sij[6],
+                               double* S_uvp, double* S_uvp_pad) {
+  Engine& e = c->e;
+  Work& w = c->w;
+  strains_uvp(e, g, w.S12, w.S13, w.S23, S_uvp);
+  Sij[0] = g[0];
+  Sij[1] = g[4];
+  Sij[2] = g[8];
+  Sij[3] = w.S12;
+  Sij[4] = w.S13;
+  Sij[5] = w.S23;
+  for (int i = 0; i < 6; i++) op_pad(e, ld_field(e, Sij[i]), w.Pb[i]);
+  const double* p6[6] = {w.Pb[0], w.Pb[1], w.Pb[2], w.Pb[3], w.Pb[4], w.Pb[5]};
+  smag6(e, p6, e.P(), S_uvp_pad);
+}
+
+__global__ void k_ones_ext(double* p, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 1.0;
+}
+
+// DynamicSGS (DynamicSGS_Main.py:85-331, SM, dealiased) + DivStress.
+// mom: 25 slots as in alfa.h (6..9 unused here)
+static int dynamic_sgs(alfa_ctx* c, const double* const g[9], const double* u, const double* v,
+                       const double* w, const double* M, const double* pm, const double* pm0,
+                       double* divt[3], double* avg1, double* avg2, double* beta1,
+                       double* Cs2, double* const mom[25]) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const double* Sij[6];
+  double* S_uvp = mom[19];
+  uvp_strains_padded(c, g, Sij, S_uvp, mom[20]);
+  // LASDD (DynamicSGS_LASDD_SM.py:178-367)
+  double *u_ = mom[10], *v_ = mom[11], *w_ = mom[12];
+  if (u_ != u) cudaMemcpyAsync(u_, u, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  if (v_ != v) cudaMemcpyAsync(v_, v, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  wstar(e, w, w_);
+  op_filter12(e, ld_field(e, u_), mom[13], mom[16]);
+  op_filter12(e, ld_field(e, v_), mom[14], mom[17]);
+  op_filter12(e, ld_field(e, w_), mom[15], mom[18]);
+  const double* pa[6] = {u_, v_, w_, u_, u_, v_};
+  const double* pb[6] = {u_, v_, w_, v_, w_, w_};
+  for (int i = 0; i < 6; i++) op_filter12(e, ld(e, LD_MUL, {pa[i], pb[i]}), W.ph[i], W.pd[i]);
+  for (int i = 0; i < 6; i++) op_filter12(e, ld_field(e, Sij[i]), W.Sh[i], W.Sd[i]);
+  for (int i = 0; i < 6; i++) op_filter12(e, ld(e, LD_MUL, {S_uvp, Sij[i]}), W.SSh[i], W.SSd[i]);
+  const double* sh6[6] = {W.Sh[0], W.Sh[1], W.Sh[2], W.Sh[3], W.Sh[4], W.Sh[5]};
+  const double* sd6[6] = {W.Sd[0], W.Sd[1], W.Sd[2], W.Sd[3], W.Sd[4], W.Sd[5]};
+  smag6_n(e, sh6, mom[23]);
+  smag6_n(e, sd6, mom[24]);
+  LasddFields f;
+  for (int i = 0; i < 3; i++) {
+    f.hat[i] = mom[13 + i];
+    f.hatd[i] = mom[16 + i];
+  }
+  for (int i = 0; i < 6; i++) {
+    f.ph[i] = W.ph[i];
+    f.pd[i] = W.pd[i];
+    f.Sh[i] = W.Sh[i];
+    f.Sd[i] = W.Sd[i];
+    f.SSh[i] = W.SSh[i];
+    f.SSd[i] = W.SSd[i];
+  }
+  f.S_hat = mom[23];
+  f.S_hatd = mom[24];
+  double* sums = W.prof;
+  double* co = W.prof + 10 * e.nz;
+  if (e.cfg.optSgs == 1) {
+    lasdd_sums(e, f, sums);
+    lasdd_poly(e, sums, 0, co);
+    compute_beta(e, co, e.nz, beta1);
+  } else {
+    k_ones_ext<<<1, 256, 0, e.stream>>>(beta1, e.nz);  // LAD: beta = 1 (:321-325)
+  }
+  lasdd_LM_MM(e, f, beta1, W.LM, W.MM);
+  clip_ratio(e, W.LM, W.MM, Cs2);
+  cs2_profiles(e, Cs2, avg1, avg2);
+  // stresses (SGSStresses_SM.py) with Cs2_3D_pad = Dealias1(FFT(Cs2_3D))
+  op_pad(e, ld_field(e, Cs2), W.Pb[9]);
+  double* t6[6] = {mom[0], mom[1], mom[2], mom[3], mom[4], mom[5]};
+  sgs_stresses(c, g, mom[20], u, v, M, pm, pm0, t6, mom[21], mom[22]);
+  div_stress(c, mom[0], mom[1], mom[2], mom[3], mom[4], mom[5], divt[0], divt[1], divt[2]);
+  return check_launch(e, "DivStressDynamicSGS");
+}
+
+// StaticSGS (StaticSGS_Main.py:76-250) + DivStress; mom10 as in alfa.h
+static int static_sgs(alfa_ctx* c, const double* const g[9], const double* Cs2, const double* u,
+                      const double* v, const double* M, const double* pm, const double* pm0,
+                      double* divt[3], double* const mom10[10]) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const double* Sij[6];
+  uvp_strains_padded(c, g, Sij, mom10[6], mom10[7]);
+  op_pad(e, ld_field(e, Cs2), W.Pb[9]);
+  double* t6[6] = {mom10[0], mom10[1], mom10[2], mom10[3], mom10[4], mom10[5]};
+  sgs_stresses(c, g, mom10[7], u, v, M, pm, pm0, t6, mom10[8], mom10[9]);
+  div_stress(c, mom10[0], mom10[1], mom10[2], mom10[3], mom10[4], mom10[5], divt[0], divt[1],
+             divt[2]);
+  return check_launch(e, "DivStressStaticSGS");
+}
+
+// StaticSGSscalar (StaticSGS_Main.py:258-360, dealiased SM) + DivFlux
+static void scalar_fluxes(alfa_ctx* c, const double* S_uvp_pad, const double* S_w_pad,
+                          const double* r3, const double* gx, const double* gy, const double* gz,
+                          const double* qz_sfc, double* qz, double* divq) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  op_pad(e, ld_field(e, gx), W.Pb[0]);
+  op_pad(e, ld_field(e, gy), W.Pb[1]);
+  op_pad(e, ld_field(e, gz), W.Pb[2]);
+  op_pad(e, ld_field(e, r3), W.Pb[3]);
+  const double cst = -2 * std::pow(e.L, 2.0);
+  op_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[0]}, cst), W.qx);
+  op_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[1]}, cst), W.qy);
+  op_unpad(e, ld(e, LD_STRESS_W, {W.Pb[3], S_w_pad, W.Pb[2]}, cst), qz);
+  set_plane0(e, qz_sfc, qz);
+  div_flux(c, W.qx, W.qy, qz, divq);
+}
+
+// DynamicSGSscalar (DynamicSGS_Main.py:339-478) + DivFlux; m15 = mom[10..24]
+static int dynamic_sgs_scalar(alfa_ctx* c, const double* const m15[15], const double* TH,
+                              const double* gx, const double* gy, const double* gz,
+                              const double* qz_sfc, double* qz, double* divq, double* r3,
+                              double* r1, double* beta2) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const double *u_ = m15[0], *v_ = m15[1], *w_ = m15[2];
+  const double* S = m15[9];
+  op_filter12(e, ld_field(e, TH), W.Th, W.Td);
+  const double* uv3[3] = {u_, v_, w_};
+  for (int i = 0; i < 3; i++) op_filter12(e, ld(e, LD_MUL, {uv3[i], TH}), W.uTh[i], W.uTd[i]);
+  op_filter12(e, ld_field(e, gx), W.Gh[0], W.Gd[0]);
+  op_filter12(e, ld_field(e, gy), W.Gh[1], W.Gd[1]);
+  op_filter12(e, ld(e, LD_THZ, {gz}), W.Gh[2], W.Gd[2]);
+  op_filter12(e, ld(e, LD_MUL, {S, gx}), W.SGh[0], W.SGd[0]);
+  op_filter12(e, ld(e, LD_MUL, {S, gy}), W.SGh[1], W.SGd[1]);
+  op_filter12(e, ld(e, LD_MUL_THZ, {S, gz}), W.SGh[2], W.SGd[2]);
+  ScalarLasddFields f;
+  for (int i = 0; i < 3; i++) {
+    f.hat[i] = m15[3 + i];
+    f.hatd[i] = m15[6 + i];
+    f.uTh[i] = W.uTh[i];
+    f.uTd[i] = W.uTd[i];
+    f.Gh[i] = W.Gh[i];
+    f.Gd[i] = W.Gd[i];
+    f.SGh[i] = W.SGh[i];
+    f.SGd[i] = W.SGd[i];
+  }
+  f.Th = W.Th;
+  f.Td = W.Td;
+  f.S_hat = m15[13];
+  f.S_hatd = m15[14];
+  double* sums = W.prof;
+  double* co = W.prof + 10 * e.nz;
+  if (e.cfg.optSgs == 1) {
+    scalar_lasdd_sums(e, f, sums);
+    lasdd_poly(e, sums, 1, co);
+    compute_beta(e, co, e.nz, beta2);
+  } else {
+    k_ones_ext<<<1, 256, 0, e.stream>>>(beta2, e.nz);
+  }
+  scalar_Tup_Tdn(e, f, beta2, W.LM, W.MM);
+  clip_ratio(e, W.LM, W.MM, r3);
+  const double* fr[1] = {r3};
+  plane_means(e, fr, 1, r1);
+  scalar_fluxes(c, m15[10], m15[12], r3, gx, gy, gz, qz_sfc, qz, divq);
+  return check_launch(e, "DivFluxDynamicSGS");
+}
+
+// PressureRC (NSE_PressureTerms.py:109-182)
+static int pressure_rc_fn(alfa_ctx* c, const double* u, const double* v, const double* w,
+                          const double* Ru, const double* Rv, const double* Rw, const double* Rup,
+                          const double* Rvp, const double* Rwp, const double* divtz, double* RCr,
+                          double* RCi, double* fRzr) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const double c0 = 1.0 / 3.0, c1 = 2.0 / (3.0 * e.dt_nondim);
+  op_rfft2(e, ld(e, LD_PRESSURE_R, {Ru, Rup, u}, c0, c1), W.fRx);
+  op_rfft2(e, ld(e, LD_PRESSURE_R, {Rv, Rvp, v}, c0, c1), W.fRy);
+  op_rfft2(e, ld(e, LD_PRESSURE_R, {Rw, Rwp, w}, c0, c1), W.fRz);
+  // rfft2 of the bottom and top planes of divtz, as a 2-level field
+  copy_planes_z(e, divtz, 0, e.nz - 1, W.planes2);
+  const int nz = e.nz;
+  e.nz = 2;
+  Loader L2 = ld_field(e, W.planes2);
+  op_rfft2(e, L2, W.fb2);
+  e.nz = nz;
+  pressure_rc(e, W.fRx, W.fRy, W.fRz, W.fb2, nullptr, RCr, RCi, fRzr);
+  return check_launch(e, "PressureRC");
+}
+
+// ThomasPressureSolve (NSE_PressureTerms_Thomas.py:218-292)
+static int pressure_solve_fn(alfa_ctx* c, const double* RCr, const double* RCi,
+                             const double* fRzr, double* p, double* dpdx, double* dpdy,
+                             double* dpdz) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  thomas_solve(e, RCr, RCi, fRzr, W.fp);
+  op_irfft2(e, W.fp, p);
+  deriv_field_acc(e, ld_field(e, p), dpdx, 0, dpdy, 0);
+  derivz_generic(e, p, 0, dpdz);
+  return check_launch(e, "ThomasPressureSolve");
+}
+
+static int surface_variant(const alfa_config& c) {
+  if (c.optSurfBC == 0) return c.optSurfFlux == 0 ? 0 : 1;
+  if (c.optSurfBC == 1) return c.optSurfFlux == 0 ? 2 : 3;
+  return c.optSurfFlux == 0 ? 4 : 5;
+}
+
+// ---------------------------------------------------------------------------
+// whole step: src/Main.py:156-541 (dry, constant geostrophic wind)
+// ---------------------------------------------------------------------------
+static int one_step(alfa_ctx* c) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const alfa_config& cf = e.cfg;
+  const int it = W.iteration;
+  const int nz = e.nz;
+  if (it > cf.istep)
+    for (int i = 0; i < 4; i++) std::swap(W.RHSp[i], W.RHS[i]);
+  const double *Uadv = W.zero_prof, *Vadv = W.zero_prof, *THadv = W.zero_prof;
+  if (cf.optAdvection >= 1) {
+    if (it - 1 >= W.series_rows) return e.fail("advection series exhausted", ALFA_E_STATE);
+    const double* row = W.series_adv + (size_t)(it - 1) * 3 * nz;
+    Uadv = row;
+    Vadv = row + nz;
+    THadv = row + 2 * nz;
+  }
+  // filtering (Main.py:193-197): the filtered field replaces the state, so
+  // filter into the (not yet used) gradient slot and swap the two N-sized
+  // buffers; the TH spectrum is discarded as in the reference.
+  op_filter_explicit(e, ld_field(e, W.u), W.g[0], W.ufft);
+  std::swap(W.u, W.g[0]);
+  op_filter_explicit(e, ld_field(e, W.v), W.g[0], W.vfft);
+  std::swap(W.v, W.g[0]);
+  op_filter_explicit(e, ld_field(e, W.w), W.g[0], W.wfft);
+  std::swap(W.w, W.g[0]);
+  op_filter_explicit(e, ld_field(e, W.TH), W.g[0], W.fp);
+  std::swap(W.TH, W.g[0]);
+  // surface fluxes (Main.py:213-243)
+  const int var = surface_variant(cf);
+  double sfc = 0.0;
+  if (cf.optSurfBC >= 1) {
+    if (it - 1 >= (int)W.sfc_series.size()) return e.fail("surface series exhausted", ALFA_E_STATE);
+    sfc = W.sfc_series[it - 1];
+  }
+  SurfaceIO io;
+  io.u = W.u;
+  io.v = W.v;
+  io.TH = W.TH;
+  for (int i = 0; i < 6; i++) {
+    io.most_in[i] = W.most[i];
+    io.most_out[i] = W.most_new[i];
+  }
+  io.M = W.M;
+  io.ustar = W.ustar;
+  io.q2 = W.q2;
+  io.qavg = W.d_qavg;
+  io.invOB = W.invOB;
+  surface_flux(e, var, sfc, io);
+  for (int i = 0; i < 6; i++) std::swap(W.most[i], W.most_new[i]);
+  const double* qz_step = (var <= 1) ? W.qz_plane : W.q2;
+  // gradients (Main.py:275-290)
+  op_deriv_spec(e, W.ufft, W.g[0], W.g[3]);
+  op_deriv_spec(e, W.vfft, W.g[1], W.g[4]);
+  op_deriv_spec(e, W.wfft, W.g[2], W.g[5]);
+  derivz_M(e, W.u, W.v, W.w, W.ustar, W.M, W.most[4], W.g[6], W.g[7], W.g[8]);
+  deriv_field_acc(e, ld_field(e, W.TH), W.gT[0], 0, W.gT[1], 0);
+  derivz_TH(e, W.TH, W.ustar, qz_step, W.most[5], W.gT[2]);
+  // advection (Main.py:301-311)
+  advection(c, W.u, W.v, W.w, W.g[3], W.g[6], W.g[1], W.g[7], W.g[2], W.g[5], W.Cx, W.Cy, W.Cz);
+  scalar_advection(c, W.u, W.v, W.w, W.gT[0], W.gT[1], W.gT[2], W.THadv, true);
+  // buoyancy (Main.py:323-327)
+  buoyancy(e, W.TH, cf.optBuoyancy == 0 ? 0 : 1, W.buoy);
+  // SGS (Main.py:333-455)
+  const double* g9[9] = {W.g[0], W.g[1], W.g[2], W.g[3], W.g[4], W.g[5], W.g[6], W.g[7], W.g[8]};
+  const bool dyn = (cf.optSgs >= 1 && cf.optSgs <= 4) &&
+                   (it == cf.istep || it % cf.dynamicSGS_call_time == 0);
+  int st;
+  if (dyn) {
+    double* mom[25];
+    for (int i = 0; i < 25; i++) mom[i] = W.mom[i];
+    mom[10] = W.u;  // u_ = u.copy(), v_ = v.copy(): aliases (never written)
+    mom[11] = W.v;
+    double* beta1 = W.prof + 20 * nz;
+    st = dynamic_sgs(c, g9, W.u, W.v, W.w, W.M, W.most[0], W.most[1], W.divt, W.prof + 21 * nz,
+                     W.prof + 22 * nz, beta1, W.Cs2, mom);
+    if (st) return st;
+    const double* m15[15];
+    for (int i = 0; i < 15; i++) m15[i] = mom[10 + i];
+    st = dynamic_sgs_scalar(c, m15, W.TH, W.gT[0], W.gT[1], W.gT[2], qz_step, W.qz, W.divq,
+                            W.Cs2Pr, W.prof + 23 * nz, W.prof + 24 * nz);
+    if (st) return st;
+  } else {
+    double* m10[10] = {W.mom[0], W.mom[1], W.mom[2], W.mom[3], W.mom[4],
+                       W.mom[5], W.mom[19], W.mom[20], W.mom[21], W.mom[22]};
+    st = static_sgs(c, g9, W.Cs2, W.u, W.v, W.M, W.most[0], W.most[1], W.divt, m10);
+    if (st) return st;
+    scalar_fluxes(c, m10[7], m10[9], W.Cs2Pr, W.gT[0], W.gT[1], W.gT[2], qz_step, W.qz, W.divq);
+  }
+  // RHS (Main.py:464-473)
+  double* bars = W.prof + 30 * nz;
+  if (cf.optDamping == 1) {
+    const double* f3[3] = {W.u, W.v, W.TH};
+    plane_means(e, f3, 3, bars);
+  }
+  rhs_momentum(e, W.u, W.v, W.w, W.Ug, W.Vg, W.Cx, W.Cy, W.Cz, W.buoy, W.divt[0], W.divt[1],
+               W.divt[2], Uadv, Vadv, bars, bars + nz, W.RHS[0], W.RHS[1], W.RHS[2]);
+  rhs_scalar(e, W.TH, W.THadv, W.divq, THadv, bars + 2 * nz, W.RHS[3]);
+  // pressure (Main.py:481-500)
+  st = pressure_rc_fn(c, W.u, W.v, W.w, W.RHS[0], W.RHS[1], W.RHS[2], W.RHSp[0], W.RHSp[1],
+                      W.RHSp[2], W.divt[2], W.RCr, W.RCi, W.fRzr);
+  if (st) return st;
+  st = pressure_solve_fn(c, W.RCr, W.RCi, W.fRzr, W.p, W.dp[0], W.dp[1], W.dp[2]);
+  if (st) return st;
+  subtract3(e, W.RHS[0], W.RHS[1], W.RHS[2], W.dp[0], W.dp[1], W.dp[2]);
+  // AB2 bootstrap and advance (Main.py:506-526)
+  const double* Rp[4];
+  for (int i = 0; i < 4; i++) Rp[i] = (it == cf.istep) ? W.RHS[i] : W.RHSp[i];
+  ab2_uvw(e, W.u, W.v, W.w, W.RHS[0], Rp[0], W.RHS[1], Rp[1], W.RHS[2], Rp[2], W.u, W.v, W.w);
+  ab2_th(e, W.TH, W.RHS[3], Rp[3], W.TH);
+  if (it == cf.istep)
+    for (int i = 0; i < 4; i++)
+      cudaMemcpyAsync(W.RHSp[i], W.RHS[i], e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  // CFL (Main.py:534-540): maxima stay on the device, read by alfa_get_diag
+  cfl_max(e, W.u, W.v, W.w, W.d_cfl);
+  W.iteration++;
+  return check_launch(e, "step");
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+#define CTX_CHECK(c)                                  \
+  do {                                                \
+    if (!(c)) return ALFA_E_STATE;                    \
+  } while (0)
+
+static thread_local std::string g_create_error;
+
+extern "C" {
+
+int alfa_create(const alfa_config* cfg, alfa_ctx** out) {
+  if (!cfg || !out) return ALFA_E_SHAPE;
+  *out = nullptr;
+  alfa_ctx* c = new alfa_ctx();
+  cudaGetDevice(&c->e.device);
+  int st = engine_init(c->e, *cfg);
+  if (st) {
+    g_create_error = c->e.err;
+    engine_free(c->e);
+    delete c;
+    return st;
+  }
+  Carver k{nullptr, 0, true};
+  carve(c, k);
+  c->bytes = k.off + 256;
+  if (cudaMalloc(&c->base, c->bytes) != cudaSuccess) {
+    g_create_error = "workspace allocation of " + std::to_string(c->bytes) + " bytes failed";
+    engine_free(c->e);
+    delete c;
+    return ALFA_E_CUDA;
+  }
+  cudaMemset(c->base, 0, c->bytes);
+  Carver k2{(char*)c->base, 0, false};
+  carve(c, k2);
+  *out = c;
+  return ALFA_OK;
+}
+
+void alfa_destroy(alfa_ctx* c) {
+  if (!c) return;
+  if (c->w.series_adv) cudaFree(c->w.series_adv);
+  cudaFree(c->base);
+  engine_free(c->e);
+  delete c;
+}
+
+// with a null context: the reason of the last failed alfa_create on this thread
+const char* alfa_last_error(const alfa_ctx* c) {
+  return c ? c->e.err.c_str() : g_create_error.c_str();
+}
+
+int alfa_set_stream(alfa_ctx* c, void* s) {
+  CTX_CHECK(c);
+  c->e.stream = (cudaStream_t)s;
+  return ALFA_OK;
+}
+
+size_t alfa_workspace_bytes(const alfa_ctx* c) { return c ? c->bytes : 0; }
+
+int alfa_get_derived(const alfa_ctx* c, alfa_derived* o) {
+  CTX_CHECK(c);
+  if (!o) return ALFA_E_SHAPE;
+  const Engine& e = c->e;
+  o->mx = e.mx;
+  o->my = e.my;
+  o->nx_rfft = e.nxh;
+  o->ny_rfft = e.nyh;
+  o->z_scale = e.z_scale;
+  o->g_nondim = e.g_nondim;
+  o->f_coriolis_nondim = e.f_nondim;
+  o->T_0_nondim = e.T0_nondim;
+  o->inversion_nondim = e.inversion_nondim;
+  o->dx = e.dx;
+  o->dy = e.dy;
+  o->dz = e.dz;
+  o->L = e.L;
+  o->dt_nondim = e.dt_nondim;
+  o->TFR = e.TFR;
+  for (int i = 0; i < 2; i++) {
+    o->cut_explicit[i] = e.cut_e[i];
+    o->cut_level1[i] = e.cut_1[i];
+    o->cut_level2[i] = e.cut_2[i];
+  }
+  return ALFA_OK;
+}
+
+#define NN(p) \
+  if (!(p)) return c->e.fail("null pointer argument: " #p, ALFA_E_SHAPE)
+
+int alfa_FFT(alfa_ctx* c, const double* F, double* F_fft) {
+  CTX_CHECK(c);
+  NN(F);
+  NN(F_fft);
+  op_rfft2(c->e, ld_field(c->e, F), (cd*)F_fft);
+  return check_launch(c->e, "FFT");
+}
+
+int alfa_FFT_pad(alfa_ctx* c, const double* F_pad, double* F_pad_fft) {
+  CTX_CHECK(c);
+  NN(F_pad);
+  NN(F_pad_fft);
+  op_rfft2_pad(c->e, ld_field(c->e, F_pad), (cd*)F_pad_fft);
+  return check_launch(c->e, "FFT_pad");
+}
+
+int alfa_Dealias1(alfa_ctx* c, const double* F_fft, double* F_pad) {
+  CTX_CHECK(c);
+  NN(F_fft);
+  NN(F_pad);
+  op_pad_spec(c->e, (const cd*)F_fft, F_pad);
+  return check_launch(c->e, "Dealias1");
+}
+
+int alfa_Dealias2(alfa_ctx* c, const double* F_pad_fft, double* F) {
+  CTX_CHECK(c);
+  NN(F_pad_fft);
+  NN(F);
+  op_unpad_spec(c->e, (const cd*)F_pad_fft, F);
+  return check_launch(c->e, "Dealias2");
+}
+
+int alfa_Filtering_Explicit(alfa_ctx* c, const double* F_fft, double* F_new, double* F_fft_new) {
+  CTX_CHECK(c);
+  NN(F_fft);
+  NN(F_new);
+  NN(F_fft_new);
+  Engine& e = c->e;
+  const int cx = e.cut_e[0], cy = e.cut_e[1];
+  XOut o[2];
+  o[0] = XOut{};
+  o[0].kind = XO_SPEC;
+  o[0].map = MAP_TRUNC;
+  o[0].cx = cx;
+  o[0].cy = cy;
+  o[0].K = e.nyh;
+  o[0].rows = e.nx;
+  o[0].dst = (cd*)F_fft_new;
+  o[1] = XOut{};
+  o[1].kind = XO_INV;
+  o[1].map = MAP_TRUNC;
+  o[1].cx = cx;
+  o[1].cy = cy;
+  o[1].K = cy;
+  o[1].rows = e.nx;
+  o[1].dst = e.T[1];
+  o[1].inv = e.pnx;
+  launch_x(e, (const cd*)F_fft, 1, e.nx, e.nyh, e.pnx, 2, o, e.nyh);
+  launch_y_inv(e, e.T[1], e.nx, cy, e.pny, 1.0 / ((double)e.nx * e.ny), F_new, 0);
+  return check_launch(e, "Filtering_Explicit");
+}
+
+int alfa_Filtering_Level1(alfa_ctx* c, const double* F_fft, double* F_hat) {
+  CTX_CHECK(c);
+  NN(F_fft);
+  NN(F_hat);
+  op_filter1_spec(c->e, (const cd*)F_fft, 1, F_hat);
+  return check_launch(c->e, "Filtering_Level1");
+}
+
+int alfa_Filtering_Level2(alfa_ctx* c, const double* F_fft, double* F_hatd) {
+  CTX_CHECK(c);
+  NN(F_fft);
+  NN(F_hatd);
+  op_filter1_spec(c->e, (const cd*)F_fft, 2, F_hatd);
+  return check_launch(c->e, "Filtering_Level2");
+}
+
+int alfa_Derivxy(alfa_ctx* c, const double* F_fft, int axis, double* d) {
+  CTX_CHECK(c);
+  NN(F_fft);
+  NN(d);
+  if (axis != 0 && axis != 1) return c->e.fail("axis must be 0 (x) or 1 (y)", ALFA_E_SHAPE);
+  op_deriv_spec(c->e, (const cd*)F_fft, axis == 0 ? d : nullptr, axis == 1 ? d : nullptr);
+  return check_launch(c->e, "Derivxy");
+}
+
+int alfa_velocityGradients(alfa_ctx* c, const double* u, const double* v, const double* w,
+                           const double* u_fft, const double* v_fft, const double* w_fft,
+                           const double* ustar, const double* M, const double* fi_m,
+                           double* const out[9]) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(u_fft); NN(v_fft); NN(w_fft); NN(ustar); NN(M); NN(fi_m); NN(out);
+  for (int i = 0; i < 9; i++) NN(out[i]);
+  Engine& e = c->e;
+  op_deriv_spec(e, (const cd*)u_fft, out[0], out[3]);
+  op_deriv_spec(e, (const cd*)v_fft, out[1], out[4]);
+  op_deriv_spec(e, (const cd*)w_fft, out[2], out[5]);
+  derivz_M(e, u, v, w, ustar, M, fi_m, out[6], out[7], out[8]);
+  return check_launch(e, "velocityGradients");
+}
+
+int alfa_potentialTemperatureGradients(alfa_ctx* c, const double* TH, const double* ustar,
+                                       const double* qz, const double* fi_h, double* const out[3]) {
+  CTX_CHECK(c);
+  NN(TH); NN(ustar); NN(qz); NN(fi_h); NN(out); NN(out[0]); NN(out[1]); NN(out[2]);
+  Engine& e = c->e;
+  deriv_field_acc(e, ld_field(e, TH), out[0], 0, out[1], 0);
+  derivz_TH(e, TH, ustar, qz, fi_h, out[2]);
+  return check_launch(e, "potentialTemperatureGradients");
+}
+
+int alfa_Derivz_Generic_uvp(alfa_ctx* c, const double* F, double* d) {
+  CTX_CHECK(c);
+  NN(F); NN(d);
+  derivz_generic(c->e, F, 0, d);
+  return check_launch(c->e, "Derivz_Generic_uvp");
+}
+
+int alfa_Derivz_Generic_w(alfa_ctx* c, const double* F, double* d) {
+  CTX_CHECK(c);
+  NN(F); NN(d);
+  derivz_generic(c->e, F, 1, d);
+  return check_launch(c->e, "Derivz_Generic_w");
+}
+
+int alfa_PlanarMean(alfa_ctx* c, const double* F, double* m) {
+  CTX_CHECK(c);
+  NN(F); NN(m);
+  const double* f[1] = {F};
+  plane_means(c->e, f, 1, m);
+  return check_launch(c->e, "PlanarMean");
+}
+
+int alfa_Imfilter(alfa_ctx* c, const double* F, double* out) {
+  CTX_CHECK(c);
+  NN(F); NN(out);
+  imfilter(c->e, F, out);
+  return check_launch(c->e, "Imfilter");
+}
+
+int alfa_ComputeBeta(alfa_ctx* c, const double* co, int nlev, double* beta) {
+  CTX_CHECK(c);
+  NN(co); NN(beta);
+  if (nlev <= 0) return c->e.fail("nlev must be positive", ALFA_E_SHAPE);
+  compute_beta(c->e, co, nlev, beta);
+  return check_launch(c->e, "ComputeBeta");
+}
+
+static int surf(alfa_ctx* c, int var, double sfc, const double* u, const double* v,
+                const double* TH, const double* const mi[6], double* M, double* ustar, double* q2,
+                double* qavg, double* invOB, double* const mo[6]) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(TH); NN(mi); NN(mo); NN(M); NN(ustar); NN(qavg); NN(invOB);
+  for (int i = 0; i < 6; i++) {
+    NN(mi[i]);
+    NN(mo[i]);
+  }
+  SurfaceIO io;
+  io.u = u;
+  io.v = v;
+  io.TH = TH;
+  for (int i = 0; i < 6; i++) {
+    io.most_in[i] = mi[i];
+    io.most_out[i] = mo[i];
+  }
+  io.M = M;
+  io.ustar = ustar;
+  io.q2 = q2 ? q2 : c->w.q2;
+  io.qavg = qavg;
+  io.invOB = invOB;
+  surface_flux(c->e, var, sfc, io);
+  return check_launch(c->e, "SurfaceFlux");
+}
+
+int alfa_SurfaceFlux_HomogeneousConstantFlux(alfa_ctx* c, const double* u, const double* v,
+    const double* TH, const double* const mi[6], double* M, double* ustar, double* qavg,
+    double* invOB, double* const mo[6]) {
+  return surf(c, 0, 0.0, u, v, TH, mi, M, ustar, nullptr, qavg, invOB, mo);
+}
+int alfa_SurfaceFlux_HeterogeneousConstantFlux(alfa_ctx* c, const double* u, const double* v,
+    const double* TH, const double* const mi[6], double* M, double* ustar, double* qavg,
+    double* invOB, double* const mo[6]) {
+  return surf(c, 1, 0.0, u, v, TH, mi, M, ustar, nullptr, qavg, invOB, mo);
+}
+int alfa_SurfaceFlux_HomogeneousVaryingFlux(alfa_ctx* c, const double* u, const double* v,
+    const double* TH, double s, const double* const mi[6], double* M, double* ustar,
+    double* q2, double* qavg, double* invOB, double* const mo[6]) {
+  return surf(c, 2, s, u, v, TH, mi, M, ustar, q2, qavg, invOB, mo);
+}
+int alfa_SurfaceFlux_HeterogeneousVaryingFlux(alfa_ctx* c, const double* u, const double* v,
+    const double* TH, double s, const double* const mi[6], double* M, double* ustar,
+    double* q2, double* qavg, double* invOB, double* const mo[6]) {
+  return surf(c, 3, s, u, v, TH, mi, M, ustar, q2, qavg, invOB, mo);
+}
+int alfa_SurfaceFlux_HomogeneousPrescribedTemperature(alfa_ctx* c, const double* u,
+    const double* v, const double* TH, double s, const double* const mi[6], double* M,
+    double* ustar, double* q2, double* qavg, double* invOB, double* const mo[6]) {
+  return surf(c, 4, s, u, v, TH, mi, M, ustar, q2, qavg, invOB, mo);
+}
+int alfa_SurfaceFlux_HeterogeneousPrescribedTemperature(alfa_ctx* c, const double* u,
+    const double* v, const double* TH, double s, const double* const mi[6], double* M,
+    double* ustar, double* q2, double* qavg, double* invOB, double* const mo[6]) {
+  return surf(c, 5, s, u, v, TH, mi, M, ustar, q2, qavg, invOB, mo);
+}
+
+int alfa_Advection(alfa_ctx* c, const double* u, const double* v, const double* w,
+                   const double* dudy, const double* dudz, const double* dvdx, const double* dvdz,
+                   const double* dwdx, const double* dwdy, double* Cx, double* Cy, double* Cz) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(dudy); NN(dudz); NN(dvdx); NN(dvdz); NN(dwdx); NN(dwdy);
+  NN(Cx); NN(Cy); NN(Cz);
+  advection(c, u, v, w, dudy, dudz, dvdx, dvdz, dwdx, dwdy, Cx, Cy, Cz);
+  return check_launch(c->e, "Advection");
+}
+
+int alfa_ScalarAdvection(alfa_ctx* c, const double* u, const double* v, const double* w,
+                         const double* sx, const double* sy, const double* sz, double* out) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(sx); NN(sy); NN(sz); NN(out);
+  scalar_advection(c, u, v, w, sx, sy, sz, out, false);
+  return check_launch(c->e, "ScalarAdvection");
+}
+
+int alfa_BuoyancyOpt1(alfa_ctx* c, const double* TH, double* b) {
+  CTX_CHECK(c);
+  NN(TH); NN(b);
+  buoyancy(c->e, TH, 0, b);
+  return check_launch(c->e, "BuoyancyOpt1");
+}
+
+int alfa_BuoyancyOpt2(alfa_ctx* c, const double* TH, double* b) {
+  CTX_CHECK(c);
+  NN(TH); NN(b);
+  buoyancy(c->e, TH, 1, b);
+  return check_launch(c->e, "BuoyancyOpt2");
+}
+
+int alfa_DivStressDynamicSGS(alfa_ctx* c, const double* const g[9], const double* u,
+                             const double* v, const double* w, const double* M, const double* pm,
+                             const double* pm0, double* dtx, double* dty, double* dtz,
+                             double* avg1, double* avg2, double* beta1, double* Cs2,
+                             double* const mom[25]) {
+  CTX_CHECK(c);
+  NN(g); NN(u); NN(v); NN(w); NN(M); NN(pm); NN(pm0); NN(dtx); NN(dty); NN(dtz);
+  NN(avg1); NN(avg2); NN(beta1); NN(Cs2); NN(mom);
+  for (int i = 0; i < 9; i++) NN(g[i]);
+  for (int i = 0; i < 25; i++)
+    if (!(i >= 6 && i <= 9)) NN(mom[i]);
+  if (c->e.cfg.optSgs != 1 && c->e.cfg.optSgs != 3)
+    return c->e.fail("DivStressDynamicSGS needs optSgs 1 or 3", ALFA_E_CONFIG);
+  double* divt[3] = {dtx, dty, dtz};
+  double* m[25];
+  for (int i = 0; i < 25; i++) m[i] = mom[i];
+  int st = dynamic_sgs(c, g, u, v, w, M, pm, pm0, divt, avg1, avg2, beta1, Cs2, m);
+  if (st) return st;
+  Engine& e = c->e;
+  if (mom[6]) cudaMemcpyAsync(mom[6], avg1, e.nz * 8, cudaMemcpyDeviceToDevice, e.stream);
+  if (mom[7]) cudaMemcpyAsync(mom[7], avg2, e.nz * 8, cudaMemcpyDeviceToDevice, e.stream);
+  if (mom[8]) cudaMemcpyAsync(mom[8], beta1, e.nz * 8, cudaMemcpyDeviceToDevice, e.stream);
+  if (mom[9]) cudaMemcpyAsync(mom[9], Cs2, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  return check_launch(e, "DivStressDynamicSGS");
+}
+
+int alfa_DivFluxDynamicSGS(alfa_ctx* c, const double* const m15[15], const double* TH,
+                           const double* gx, const double* gy, const double* gz,
+                           const double* qz_sfc, double* qz, double* divq, double* r3,
+                           double* r1, double* beta2) {
+  CTX_CHECK(c);
+  NN(m15); NN(TH); NN(gx); NN(gy); NN(gz); NN(qz_sfc); NN(qz); NN(divq); NN(r3); NN(r1);
+  NN(beta2);
+  for (int i = 0; i < 15; i++) NN(m15[i]);
+  if (c->e.cfg.optSgs != 1 && c->e.cfg.optSgs != 3)
+    return c->e.fail("DivFluxDynamicSGS needs optSgs 1 or 3", ALFA_E_CONFIG);
+  return dynamic_sgs_scalar(c, m15, TH, gx, gy, gz, qz_sfc, qz, divq, r3, r1, beta2);
+}
+
+int alfa_DivStressStaticSGS(alfa_ctx* c, const double* const g[9], const double* Cs2,
+                            const double* u, const double* v, const double* M, const double* pm,
+                            const double* pm0, double* dtx, double* dty, double* dtz,
+                            double* const mom10[10]) {
+  CTX_CHECK(c);
+  NN(g); NN(Cs2); NN(u); NN(v); NN(M); NN(pm); NN(pm0); NN(dtx); NN(dty); NN(dtz); NN(mom10);
+  for (int i = 0; i < 9; i++) NN(g[i]);
+  for (int i = 0; i < 10; i++) NN(mom10[i]);
+  double* divt[3] = {dtx, dty, dtz};
+  return static_sgs(c, g, Cs2, u, v, M, pm, pm0, divt, mom10);
+}
+
+int alfa_DivFluxStaticSGS(alfa_ctx* c, const double* const m4[4], const double* r3,
+                          const double* gx, const double* gy, const double* gz,
+                          const double* qz_sfc, double* qz, double* divq) {
+  CTX_CHECK(c);
+  NN(m4); NN(r3); NN(gx); NN(gy); NN(gz); NN(qz_sfc); NN(qz); NN(divq);
+  for (int i = 0; i < 4; i++) NN(m4[i]);
+  scalar_fluxes(c, m4[1], m4[3], r3, gx, gy, gz, qz_sfc, qz, divq);
+  return check_launch(c->e, "DivFluxStaticSGS");
+}
+
+int alfa_RHS_Momentum(alfa_ctx* c, const double* u, const double* v, const double* w,
+                      const double* Ug, const double* Vg, const double* Cx, const double* Cy,
+                      const double* Cz, const double* b, const double* dtx, const double* dty,
+                      const double* dtz, const double* Uadv, const double* Vadv, double* Ru,
+                      double* Rv, double* Rw) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(Ug); NN(Vg); NN(Cx); NN(Cy); NN(Cz); NN(b); NN(dtx); NN(dty); NN(dtz);
+  NN(Uadv); NN(Vadv); NN(Ru); NN(Rv); NN(Rw);
+  Engine& e = c->e;
+  double* bars = c->w.prof + 40 * e.nz;
+  if (e.cfg.optDamping == 1) {
+    const double* f2[2] = {u, v};
+    plane_means(e, f2, 2, bars);
+  }
+  rhs_momentum(e, u, v, w, Ug, Vg, Cx, Cy, Cz, b, dtx, dty, dtz, Uadv, Vadv, bars, bars + e.nz,
+               Ru, Rv, Rw);
+  return check_launch(e, "RHS_Momentum");
+}
+
+int alfa_RHS_Scalar(alfa_ctx* c, const double* TH, const double* adv, const double* divq,
+                    const double* THadv, double* R) {
+  CTX_CHECK(c);
+  NN(TH); NN(adv); NN(divq); NN(THadv); NN(R);
+  Engine& e = c->e;
+  double* bar = c->w.prof + 42 * e.nz;
+  if (e.cfg.optDamping == 1) {
+    const double* f1[1] = {TH};
+    plane_means(e, f1, 1, bar);
+  }
+  rhs_scalar(e, TH, adv, divq, THadv, bar, R);
+  return check_launch(e, "RHS_Scalar");
+}
+
+int alfa_PressureRC(alfa_ctx* c, const double* u, const double* v, const double* w,
+                    const double* Ru, const double* Rv, const double* Rw, const double* Rup,
+                    const double* Rvp, const double* Rwp, const double* divtz, double* RCr,
+                    double* RCi, double* fRzr) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(Ru); NN(Rv); NN(Rw); NN(Rup); NN(Rvp); NN(Rwp); NN(divtz);
+  NN(RCr); NN(RCi); NN(fRzr);
+  return pressure_rc_fn(c, u, v, w, Ru, Rv, Rw, Rup, Rvp, Rwp, divtz, RCr, RCi, fRzr);
+}
+
+int alfa_ThomasPressureSolve(alfa_ctx* c, const double* RCr, const double* RCi,
+                             const double* fRzr, double* p, double* dpdx, double* dpdy,
+                             double* dpdz) {
+  CTX_CHECK(c);
+  NN(RCr); NN(RCi); NN(fRzr); NN(p); NN(dpdx); NN(dpdy); NN(dpdz);
+  return pressure_solve_fn(c, RCr, RCi, fRzr, p, dpdx, dpdy, dpdz);
+}
+
+int alfa_AB2_uvw(alfa_ctx* c, const double* u, const double* v, const double* w,
+                 const double* Ru, const double* Rup, const double* Rv, const double* Rvp,
+                 const double* Rw, const double* Rwp, double* un, double* vn, double* wn) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(Ru); NN(Rup); NN(Rv); NN(Rvp); NN(Rw); NN(Rwp); NN(un); NN(vn); NN(wn);
+  ab2_uvw(c->e, u, v, w, Ru, Rup, Rv, Rvp, Rw, Rwp, un, vn, wn);
+  return check_launch(c->e, "AB2_uvw");
+}
+
+int alfa_AB2_TH(alfa_ctx* c, const double* TH, const double* R, const double* Rp, double* out) {
+  CTX_CHECK(c);
+  NN(TH); NN(R); NN(Rp); NN(out);
+  ab2_th(c->e, TH, R, Rp, out);
+  return check_launch(c->e, "AB2_TH");
+}
+
+__global__ void k_fill(double* p, double v, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
+}
+__global__ void k_fill_n(double* p, double v, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+int alfa_init_state(alfa_ctx* c, const double* u, const double* v, const double* w,
+                    const double* TH) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(TH);
+  Engine& e = c->e;
+  Work& W = c->w;
+  const size_t N = e.N(), H = e.H();
+  cudaMemcpyAsync(W.u, u, N * 8, cudaMemcpyDeviceToDevice, e.stream);
+  cudaMemcpyAsync(W.v, v, N * 8, cudaMemcpyDeviceToDevice, e.stream);
+  cudaMemcpyAsync(W.w, w, N * 8, cudaMemcpyDeviceToDevice, e.stream);
+  cudaMemcpyAsync(W.TH, TH, N * 8, cudaMemcpyDeviceToDevice, e.stream);
+  for (int i = 0; i < 4; i++) {
+    cudaMemsetAsync(W.RHS[i], 0, N * 8, e.stream);
+    cudaMemsetAsync(W.RHSp[i], 0, N * 8, e.stream);
+  }
+  for (int i = 0; i < 6; i++) k_fill_n<<<64, 256, 0, e.stream>>>(W.most[i], i >= 4 ? 1.0 : 0.0, H);
+  k_fill_n<<<64, 256, 0, e.stream>>>(W.qz_plane, e.qz_sfc_const, H);
+  k_fill_n<<<256, 256, 0, e.stream>>>(W.Cs2, e.Cs2_init, N);
+  k_fill_n<<<256, 256, 0, e.stream>>>(W.Cs2Pr, e.Cs2PrRatio_init, N);
+  k_fill<<<1, 256, 0, e.stream>>>(W.Ug, e.cfg.Ug2 / 1.0, e.nz);
+  k_fill<<<1, 256, 0, e.stream>>>(W.Vg, e.cfg.Vg2 / 1.0, e.nz);
+  k_fill<<<1, 256, 0, e.stream>>>(W.zero_prof, 0.0, e.nz);
+  W.iteration = e.cfg.istep;
+  W.have_state = 1;
+  W.CFLmax = 0;
+  return check_launch(e, "init_state");
+}
+
+int alfa_set_series(alfa_ctx* c, const double* Uadv, const double* Vadv, const double* THadv,
+                    const double* sfc, int nrows) {
+  CTX_CHECK(c);
+  if (nrows < 0) return ALFA_E_SHAPE;
+  Engine& e = c->e;
+  Work& W = c->w;
+  const int nz = e.nz;
+  if (W.series_adv) {
+    cudaFree(W.series_adv);
+    W.series_adv = nullptr;
+  }
+  W.series_rows = 0;
+  if (Uadv || Vadv || THadv) {
+    std::vector<double> h((size_t)nrows * 3 * nz, 0.0);
+    for (int r = 0; r < nrows; r++)
+      for (int k = 0; k < nz; k++) {
+        h[((size_t)r * 3 + 0) * nz + k] = Uadv ? Uadv[(size_t)r * nz + k] : 0.0;
+        h[((size_t)r * 3 + 1) * nz + k] = Vadv ? Vadv[(size_t)r * nz + k] : 0.0;
+        h[((size_t)r * 3 + 2) * nz + k] = THadv ? THadv[(size_t)r * nz + k] : 0.0;
+      }
+    if (cudaMalloc(&W.series_adv, h.size() * 8 + 8) != cudaSuccess)
+      return e.fail("series allocation failed", ALFA_E_CUDA);
+    cudaMemcpy(W.series_adv, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+    W.series_rows = nrows;
+  }
+  W.sfc_series.assign(sfc ? sfc : (const double*)nullptr, sfc ? sfc + nrows : (const double*)nullptr);
+  return ALFA_OK;
+}
+
+int alfa_step(alfa_ctx* c, int nsteps) {
+  CTX_CHECK(c);
+  if (!c->w.have_state) return c->e.fail("alfa_step before alfa_init_state", ALFA_E_STATE);
+  for (int s = 0; s < nsteps; s++) {
+    int st = one_step(c);
+    if (st) return st;
+  }
+  return ALFA_OK;
+}
+
+int alfa_get_state(alfa_ctx* c, double* u, double* v, double* w, double* TH, double* p) {
+  CTX_CHECK(c);
+  Engine& e = c->e;
+  Work& W = c->w;
+  const size_t N = e.N() * 8;
+  if (u) cudaMemcpyAsync(u, W.u, N, cudaMemcpyDeviceToDevice, e.stream);
+  if (v) cudaMemcpyAsync(v, W.v, N, cudaMemcpyDeviceToDevice, e.stream);
+  if (w) cudaMemcpyAsync(w, W.w, N, cudaMemcpyDeviceToDevice, e.stream);
+  if (TH) cudaMemcpyAsync(TH, W.TH, N, cudaMemcpyDeviceToDevice, e.stream);
+  if (p) cudaMemcpyAsync(p, W.p, N, cudaMemcpyDeviceToDevice, e.stream);
+  return check_launch(e, "get_state");
+}
+
+int alfa_get_diag(alfa_ctx* c, alfa_diag* o) {
+  CTX_CHECK(c);
+  if (!o) return ALFA_E_SHAPE;
+  Engine& e = c->e;
+  Work& W = c->w;
+  double m[3] = {0, 0, 0}, q = 0;
+  cudaMemcpyAsync(m, W.d_cfl, 3 * 8, cudaMemcpyDeviceToHost, e.stream);
+  cudaMemcpyAsync(&q, W.d_qavg, 8, cudaMemcpyDeviceToHost, e.stream);
+  std::vector<double> us(e.H());
+  cudaMemcpyAsync(us.data(), W.ustar, e.H() * 8, cudaMemcpyDeviceToHost, e.stream);
+  if (cudaStreamSynchronize(e.stream) != cudaSuccess) return e.fail("diag sync failed", ALFA_E_CUDA);
+  const double cfl = std::max(std::max(m[0] * e.dt_nondim / e.dx, m[1] * e.dt_nondim / e.dy),
+                              m[2] * e.dt_nondim / e.dz);
+  W.CFL = cfl;
+  if (cfl > W.CFLmax) W.CFLmax = cfl;
+  double s = 0;
+  for (double x : us) s += x * x;
+  o->iteration = W.iteration;
+  o->CFL = cfl;
+  o->CFLmax = W.CFLmax;
+  o->ustar_rms = std::sqrt(s / (double)e.H());
+  o->qz_sfc_avg = q;
+  if (!std::isfinite(cfl)) return e.fail("non-finite velocity", ALFA_E_NUMERIC);
+  return ALFA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,204 @@
+// FP64 batched FFT building blocks for sm_100a.
+//
+// A CTA transforms C independent columns at once: a tile of n rows x C
+// columns of complex doubles held in shared memory with the column index
+// fastest (element (row, c) at row*C + c), which is exactly the layout of a
+// run of C consecutive z levels of a field stored z-fastest.  The transform
+// is a mixed-radix Stockham sweep: each pass, every thread takes R elements
+// of one column into registers, applies the inter-pass twiddles from a
+// per-length table, runs an R-point DFT in registers and writes the R
+// results to the other shared-memory buffer (ping-pong, no bit reversal).
+// Radices 2, 3, 4, 8 and 16 cover every length 2^a 3^b used by the grids
+// (n, 3n/2 for the 3/2-rule padding).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace alfa {
+
+typedef double2 cd;
+
+__device__ __forceinline__ cd cadd(cd a, cd b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cd csub(cd a, cd b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cd cmul(cd a, cd b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ cd cscale(cd a, double s) { return make_double2(a.x * s, a.y * s); }
+// a * (S i): S = -1 forward (multiply by -i), S = +1 inverse (multiply by +i)
+template <int S>
+__device__ __forceinline__ cd rot90(cd a) {
+  return S < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+}
+
+// cos(m pi / 8) and sin(m pi / 8) for m = 0..15 (exact roots of unity of
+// order 16, correctly rounded).
+__device__ __forceinline__ cd w16(int m, int S) {
+  const double c1 = 0.92387953251128675613;  // cos(pi/8)
+  const double s1 = 0.38268343236508977173;  // sin(pi/8)
+  const double r2 = 0.70710678118654752440;  // sqrt(1/2)
+  double c, s;
+  switch (m & 15) {
+    case 0: c = 1.0; s = 0.0; break;
+    case 1: c = c1; s = s1; break;
+    case 2: c = r2; s = r2; break;
+    case 3: c = s1; s = c1; break;
+    case 4: c = 0.0; s = 1.0; break;
+    case 5: c = -s1; s = c1; break;
+    case 6: c = -r2; s = r2; break;
+    case 7: c = -c1; s = s1; break;
+    case 8: c = -1.0; s = 0.0; break;
+    case 9: c = -c1; s = -s1; break;
+    case 10: c = -r2; s = -r2; break;
+    case 11: c = -s1; s = -c1; break;
+    case 12: c = 0.0; s = -1.0; break;
+    case 13: c = s1; s = -c1; break;
+    case 14: c = r2; s = -r2; break;
+    default: c = c1; s = -s1; break;
+  }
+  return make_double2(c, S * s);
+}
+
+template <int S>
+__device__ __forceinline__ void dft2(cd& a, cd& b) {
+  cd t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+template <int S>
+__device__ __forceinline__ void dft3(cd& a, cd& b, cd& c) {
+  const double h = 0.86602540378443864676;  // sqrt(3)/2
+  cd t1 = cadd(b, c);
+  cd t2 = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  cd d = csub(b, c);
+  cd t3 = rot90<S>(cscale(d, h));
+  a = cadd(a, t1);
+  b = cadd(t2, t3);
+  c = csub(t2, t3);
+}
+
+template <int S>
+__device__ __forceinline__ void dft4(cd& v0, cd& v1, cd& v2, cd& v3) {
+  cd t0 = cadd(v0, v2), t1 = csub(v0, v2);
+  cd t2 = cadd(v1, v3), t3 = rot90<S>(csub(v1, v3));
+  v0 = cadd(t0, t2);
+  v2 = csub(t0, t2);
+  v1 = cadd(t1, t3);
+  v3 = csub(t1, t3);
+}
+
+template <int S>
+__device__ __forceinline__ void dft8(cd* v) {
+  // radix-2 over two 4-point DFTs (even and odd inputs)
+  cd e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  cd o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<S>(e0, e1, e2, e3);
+  dft4<S>(o0, o1, o2, o3);
+  const double r2 = 0.70710678118654752440;
+  o1 = cmul(o1, make_double2(r2, S * r2));
+  o2 = rot90<S>(o2);
+  o3 = cmul(o3, make_double2(-r2, S * r2));
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+template <int S>
+__device__ __forceinline__ void dft16(cd* v) {
+  // 4 x 4: inner 4-point DFTs over n2 (stride 4), twiddle W16^(n1 k2),
+  // outer 4-point DFTs over n1.
+#pragma unroll
+  for (int n1 = 0; n1 < 4; n1++) dft4<S>(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+#pragma unroll
+  for (int n1 = 1; n1 < 4; n1++) {
+#pragma unroll
+    for (int k2 = 1; k2 < 4; k2++) v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], w16(n1 * k2, S));
+  }
+  cd o[16];
+#pragma unroll
+  for (int k2 = 0; k2 < 4; k2++) {
+    cd a = v[4 * k2], b = v[4 * k2 + 1], c = v[4 * k2 + 2], d = v[4 * k2 + 3];
+    dft4<S>(a, b, c, d);
+    o[k2] = a; o[k2 + 4] = b; o[k2 + 8] = c; o[k2 + 12] = d;
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = o[i];
+}
+
+template <int R, int S>
+__device__ __forceinline__ void dftR(cd* v) {
+  if (R == 2) dft2<S>(v[0], v[1]);
+  else if (R == 3) dft3<S>(v[0], v[1], v[2]);
+  else if (R == 4) dft4<S>(v[0], v[1], v[2], v[3]);
+  else if (R == 8) dft8<S>(v);
+  else dft16<S>(v);
+}
+
+// Length-n transform plan: radices of the Stockham passes and the table
+// tw[q] = exp(-2 pi i q / n), q = 0..n-1 (computed on the host in long
+// double and rounded once).
+struct FftPlan {
+  int n;
+  int npass;
+  int rad[8];
+  const cd* tw;
+};
+
+// One Stockham pass of radix R over C columns (Govindaraju et al., "High
+// performance discrete Fourier transforms on graphics processors", SC 2008,
+// Stockham formulation).  src/dst are n x C shared-memory tiles.
+template <int R, int S>
+__device__ __forceinline__ void stockham_pass(const cd* __restrict__ src, cd* __restrict__ dst, int n,
+                                              int Ns, int C, const cd* __restrict__ tw) {
+  const int nR = n / R;
+  const int B = nR * C;
+  const int stride = n / (Ns * R);
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const int c = b % C;
+    const int j = b / C;
+    cd v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = src[(j + r * nR) * C + c];
+    const int k = j % Ns;
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        cd w = __ldg(&tw[k * r * stride]);
+        if (S > 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    dftR<R, S>(v);
+    const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) dst[(idxD + r * Ns) * C + c] = v[r];
+  }
+}
+
+// Full unnormalised transform of the n x C tile in buf[0]; buf[1] is
+// scratch of the same size.  Returns the index (0/1) of the buffer holding
+// the result.  S = -1 forward, +1 inverse.  Leaves a __syncthreads() behind.
+template <int S>
+__device__ int fft_tile(cd* buf0, cd* buf1, const FftPlan& p, int C) {
+  cd* src = buf0;
+  cd* dst = buf1;
+  int Ns = 1;
+  for (int i = 0; i < p.npass; i++) {
+    __syncthreads();
+    switch (p.rad[i]) {
+      case 16: stockham_pass<16, S>(src, dst, p.n, Ns, C, p.tw); break;
+      case 8: stockham_pass<8, S>(src, dst, p.n, Ns, C, p.tw); break;
+      case 4: stockham_pass<4, S>(src, dst, p.n, Ns, C, p.tw); break;
+      case 3: stockham_pass<3, S>(src, dst, p.n, Ns, C, p.tw); break;
+      default: stockham_pass<2, S>(src, dst, p.n, Ns, C, p.tw); break;
+    }
+    Ns *= p.rad[i];
+    cd* t = src;
+    src = dst;
+    dst = t;
+  }
+  __syncthreads();
+  return src == buf0 ? 0 : 1;
+}
+
+}  // namespace alfa

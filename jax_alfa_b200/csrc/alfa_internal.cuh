@@ -1,0 +1,138 @@
+// Engine state and internal interfaces of libalfa (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "alfa.h"
+#include "alfa_fft.cuh"
+
+namespace alfa {
+
+// ---------------------------------------------------------------------------
+// Physical-space value producers for the y-forward FFT stage.  Instead of
+// materialising a product or a staggered combination as a full field and
+// transforming it, the first FFT stage evaluates it while loading its tile.
+// Each kind restates one expression of the reference (cited at its use).
+// ---------------------------------------------------------------------------
+enum LoadKind {
+  LD_FIELD = 0,      // a0
+  LD_MUL,            // a0 * a1
+  LD_MUL3,           // a0 * a1 * a2   (left to right)
+  LD_PRESSURE_R,     // a0 - c0*a1 + c1*a2        (PressureRC R_i)
+  LD_ADV_XY,         // Cx/Cy rows (advection, padded space)
+  LD_ADV_Z,          // Cz rows
+  LD_SCALAR_ADV,     // scalar advection rows
+  LD_STRESS_UVP,     // -2L^2 Cs2 |S| S_ij, top row 0
+  LD_STRESS_W,       // interior -2L^2 stag(Cs2)|S_w| S_i3, rows 0 and top 0
+  LD_QZ,             // interior -2L^2 stag(r)|S_w| dTHdz, rows 0 and top 0
+  LD_WSTAR,          // w_ of LASDD: staggered w
+  LD_UVP_S13,        // S13/S23 on uvp nodes from gradients
+  LD_W_SXX,          // w-node strain components from gradients
+  LD_THZ,            // THz of ScalarLASDD
+  LD_MUL_THZ,        // a0 * THz(a1)
+};
+
+struct Loader {
+  int kind;
+  int sub;            // variant selector inside a kind
+  int nz;
+  const double* a[10];
+  double c[4];
+};
+
+// Output maps of the x-column stage.
+enum SpecMap { MAP_IDENT = 0, MAP_TRUNC, MAP_DX, MAP_DY, MAP_PAD, MAP_UNPAD };
+enum XOutKind { XO_SPEC = 0, XO_INV = 1 };
+
+struct XOut {
+  int kind;   // XO_SPEC: write the mapped spectrum column (nx, nyh layout)
+              // XO_INV : inverse-transform the mapped column, write T tile
+  int map;
+  int cx, cy; // truncation cut-offs (MAP_TRUNC)
+  int K;      // ky columns held by the destination
+  int rows;   // rows of the destination (transform length for XO_INV)
+  cd* dst;
+  FftPlan inv;
+};
+
+struct Engine;
+
+// ---------------------------------------------------------------------------
+// Engine: one configuration, one stream, its constants, tables, workspace.
+// ---------------------------------------------------------------------------
+struct Engine {
+  alfa_config cfg;
+  cudaStream_t stream = 0;
+  std::string err;
+  int device = 0;
+
+  // grid
+  int nx, ny, nz, mx, my, nxh, nyh, mxh, myh;
+  // DerivedVars (src/config/DerivedVars.py:48-112), in the reference's order
+  double z_scale, g_nondim, f_nondim, T0_nondim, inversion_nondim, qz_sfc_const;
+  double dx, dy, dz, idz, L, dt_nondim, TFR;
+  int optDealias;
+  double Cs2_init, Cs2PrRatio_init, z_damping_nondim, RelaxTime_nondim;
+  int cut_e[2], cut_1[2], cut_2[2];   // explicit / level-1 / level-2 cut-offs (x, y)
+
+  // device tables
+  double* d_kx = nullptr;   // (nx) with Nyquist zeroed
+  double* d_ky = nullptr;   // (nyh) with Nyquist zeroed
+  double* d_kr = nullptr;   // (nx) pressure x wavenumbers (Nyquist kept)
+  double* d_b_thomas = nullptr;  // (nx, nyh, nz+1)
+  double* d_m_thomas = nullptr;  // (nz, nx, nyh)
+  double* d_c_p = nullptr;       // (nz+1)
+  double* d_rd = nullptr;        // Rayleigh damping profile, full levels (nz)
+  double* d_rd_stag = nullptr;   // half levels (nz)
+  FftPlan pnx, pny, pmx, pmy;
+  std::vector<void*> allocs;
+
+  // workspace (complex tiles and fields)
+  cd* T[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t T_elems = 0;
+  double* red = nullptr;          // reduction partials
+  size_t red_elems = 0;
+  double* scal = nullptr;         // small device scalars / profiles
+  double* W = nullptr;            // field workspace arena
+  size_t W_elems = 0;
+
+  size_t N() const { return (size_t)nx * ny * nz; }
+  size_t P() const { return (size_t)mx * my * nz; }
+  size_t S() const { return (size_t)nx * nyh * nz; }
+  size_t H() const { return (size_t)nx * ny; }
+
+  int fail(const std::string& m, int code) {
+    err = m;
+    return code;
+  }
+};
+
+int engine_init(Engine& e, const alfa_config& c);
+void engine_free(Engine& e);
+int check_launch(Engine& e, const char* what);
+
+// spectral building blocks (alfa_spectral.cu)
+void launch_y_fwd(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T);
+void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const FftPlan& fwd,
+              int nout, const XOut* outs, int Kgrid);
+void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
+                  double* out, int accumulate);
+
+// composite transforms on regular/padded grids
+Loader ld_field(const Engine& e, const double* a);
+void op_rfft2(Engine& e, const Loader& L, cd* spec);                       // FFT
+void op_filter_explicit(Engine& e, const Loader& L, double* out, cd* spec); // Filtering_Explicit(FFT(.))
+void op_filter12(Engine& e, const Loader& L, double* out1, double* out2);   // Level1/Level2 of FFT(.)
+void op_deriv_spec(Engine& e, const cd* spec, double* dx, double* dy);      // Derivxy x/y of a spectrum
+void op_deriv_field(Engine& e, const Loader& L, double* dx, double* dy);    // Derivxy(FFT(.)) x/y
+void op_pad(Engine& e, const Loader& L, double* out_pad);                   // Dealias1(FFT(.))
+void op_unpad(Engine& e, const Loader& L_pad, double* out);                 // Dealias2(FFT_pad(.))
+void op_irfft2(Engine& e, const cd* spec, double* out);                     // irfft2 of a spectrum
+void op_pad_spec(Engine& e, const cd* spec, double* out_pad);               // Dealias1(spec)
+void op_unpad_spec(Engine& e, const cd* spec_pad, double* out);             // Dealias2(spec_pad)
+void op_rfft2_pad(Engine& e, const Loader& L, cd* spec_pad);                // FFT_pad
+void op_filter1_spec(Engine& e, const cd* spec, int level, double* out);    // Filtering_Level1/2(spec)
+
+}  // namespace alfa

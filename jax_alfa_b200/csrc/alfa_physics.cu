@@ -1,0 +1,1160 @@
+// Physical-space kernels of the LES step.  Each restates a reference
+// expression in the reference's evaluation order (cited per kernel); the
+// fields are (nx, ny, nz) z-fastest, so z stencils are unit-stride and a
+// warp reading consecutive z is coalesced.
+#include <cmath>
+
+#include "alfa_physics.cuh"
+
+namespace alfa {
+
+static constexpr int TPB = 256;
+
+static inline int nblocks(size_t n, int tpb = TPB) {
+  size_t b = (n + tpb - 1) / tpb;
+  return (int)(b > 148 * 16 ? 148 * 16 : b);
+}
+
+#define GRID_STRIDE(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); \
+                               i += (size_t)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------------------
+// plane reductions: partial sums over blocks of (x, y) rows, then a fixed
+// order sum of the partials (deterministic, independent of timing)
+// ---------------------------------------------------------------------------
+static constexpr int RED_BLOCKS = 256;
+static constexpr int RED_MAXQ = 12;
+
+struct RedArgs {
+  const double* f[RED_MAXQ];
+  int nq;
+};
+
+__global__ void k_plane_partial(RedArgs a, size_t H, int nz, double* __restrict__ part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int q = 0; q < a.nq; q++) {
+    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+      double s = 0.0;
+      for (size_t r = r0; r < r1; r++) s += a.f[q][r * nz + z];
+      part[((size_t)blockIdx.x * a.nq + q) * nz + z] = s;
+    }
+  }
+}
+
+__global__ void k_partial_finish(const double* __restrict__ part, int nblk, int nq, int nz,
+                                 double scale, double* __restrict__ out) {
+  GRID_STRIDE(t, (size_t)nq * nz) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; b++) s += part[(size_t)b * nq * nz + t];
+    out[t] = s * scale;
+  }
+}
+
+static int red_blocks(const Engine& e) {
+  return (int)(e.H() < (size_t)RED_BLOCKS ? e.H() : RED_BLOCKS);
+}
+
+void plane_sums(Engine& e, const double* const* fields, int nq, double* sums) {
+  RedArgs a{};
+  a.nq = nq;
+  for (int q = 0; q < nq; q++) a.f[q] = fields[q];
+  const int nb = red_blocks(e);
+  k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
+  k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(e.red, nb, nq, e.nz, 1.0,
+                                                                       sums);
+}
+
+void plane_means(Engine& e, const double* const* fields, int nq, double* means) {
+  RedArgs a{};
+  a.nq = nq;
+  for (int q = 0; q < nq; q++) a.f[q] = fields[q];
+  const int nb = red_blocks(e);
+  k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
+  k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(
+      e.red, nb, nq, e.nz, 1.0 / (double)e.H(), means);
+}
+
+// ---------------------------------------------------------------------------
+// surface layer: SurfaceFlux.py:53-443 (one block: three ordered passes
+// over the surface plane with block-level reductions in between)
+// ---------------------------------------------------------------------------
+struct SurfConst {
+  double Ugal, T0, vonk_g, log_m, log_h, half_dz, z0m_s, zT_s;
+  int variant;
+  double sfc_val, qz_const;
+  size_t H;
+  int nz;
+};
+
+__device__ double block_sum(double v, double* sh) {
+  // fixed-shape tree over the block (deterministic)
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] = sh[t] + sh[t + s];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__device__ void most_fn(double zL, bool stable, double* psi_m, double* psi_h, double* fi_m,
+                        double* fi_h) {
+  if (stable) {  // MOSTstable, SurfaceFlux.py:53-80
+    *psi_m = 5.0 * zL;
+    *psi_h = 5.0 * zL;
+    *fi_m = 1.0 + *psi_m;
+    *fi_h = 1.0 + *psi_h;
+  } else {  // MOSTunstable, SurfaceFlux.py:83-112
+    const double x = pow(1.0 - 15.0 * zL, 0.25);
+    *psi_m = -2.0 * log(0.5 * (1.0 + x)) - log(0.5 * (1.0 + x * x)) + 2.0 * atan(x) -
+             3.14159265358979323846 / 2.0;
+    *psi_h = -2.0 * log(0.5 * (1.0 + x * x));
+    const double ix = 1.0 / x;
+    *fi_m = ix;
+    *fi_h = ix * ix;
+  }
+}
+
+struct SurfPtr {
+  const double* u;
+  const double* v;
+  const double* TH;
+  const double* mi[6];
+  double* M;
+  double* ustar;
+  double* q2;
+  double* qavg;
+  double* invOB;
+  double* mo[6];
+};
+
+__global__ void k_surface(SurfConst c, SurfPtr p) {
+  __shared__ double sh[1024];
+  const size_t H = c.H;
+  const int nz = c.nz;
+  const bool hom = (c.variant == 0 || c.variant == 2 || c.variant == 4);
+  // pass 1: plane sums of the local wind speed and first-level theta
+  double sM = 0.0, sT = 0.0, sQ = 0.0;
+  for (size_t r = threadIdx.x; r < H; r += blockDim.x) {
+    const double uu = p.u[r * nz] + c.Ugal;
+    const double vv = p.v[r * nz];
+    sM += sqrt(uu * uu + vv * vv);
+    sT += p.TH[r * nz];
+    sQ += c.qz_const;
+  }
+  const double meanM = block_sum(sM, sh) / (double)H;
+  const double meanT = block_sum(sT, sh) / (double)H;
+  const double meanQc = block_sum(sQ, sh) / (double)H;
+  // pass 2: u*, diagnosed heat flux
+  double sq2 = 0.0;
+  for (size_t r = threadIdx.x; r < H; r += blockDim.x) {
+    double M;
+    if (hom) {
+      M = meanM;
+    } else {
+      const double uu = p.u[r * nz] + c.Ugal;
+      const double vv = p.v[r * nz];
+      M = sqrt(uu * uu + vv * vv);
+    }
+    const double denom_m = c.log_m + p.mi[0][r] - p.mi[1][r];
+    const double us = fmax(0.4 * M / denom_m, 1e-3);
+    p.M[r] = M;
+    p.ustar[r] = us;
+    if (c.variant >= 4) {
+      const double th_air = (c.variant == 4) ? meanT : p.TH[r * nz];
+      const double denom_h = c.log_h + p.mi[2][r] - p.mi[3][r];
+      const double q = (c.variant == 4) ? us * 0.4 * (c.sfc_val - th_air) * 1.0 / denom_h
+                                        : us * 0.4 * (c.sfc_val - th_air) / denom_h;
+      p.q2[r] = q;
+      sq2 += q;
+    } else if (c.variant >= 2) {
+      p.q2[r] = c.sfc_val * 1.0;
+    }
+  }
+  double qavg;
+  if (c.variant >= 4) {
+    qavg = block_sum(sq2, sh) / (double)H;
+  } else if (c.variant >= 2) {
+    qavg = c.sfc_val;
+  } else {
+    qavg = meanQc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *p.qavg = qavg;
+  // pass 3: Obukhov length and the lagged MOST functions
+  const bool stable = qavg <= 0.0;
+  for (size_t r = threadIdx.x; r < H; r += blockDim.x) {
+    double THref;
+    if (c.variant == 1 || c.variant == 3) {
+      THref = p.TH[r * nz] + c.T0;
+    } else {
+      THref = (meanT + c.T0) * 1.0;
+    }
+    const double us = p.ustar[r];
+    const double invOB = -(c.vonk_g * qavg) / ((us * us * us) * THref);
+    p.invOB[r] = invOB;
+    double pm, ph, fm, fh, d0, d1, d2;
+    most_fn(c.half_dz * invOB, stable, &pm, &ph, &fm, &fh);
+    double pm0, ph0;
+    most_fn(c.z0m_s * invOB, stable, &pm0, &d0, &d1, &d2);
+    most_fn(c.zT_s * invOB, stable, &d0, &ph0, &d1, &d2);
+    p.mo[0][r] = pm;
+    p.mo[1][r] = pm0;
+    p.mo[2][r] = ph;
+    p.mo[3][r] = ph0;
+    p.mo[4][r] = fm;
+    p.mo[5][r] = fh;
+  }
+}
+
+int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io) {
+  SurfConst c;
+  c.Ugal = e.cfg.Ugal;
+  c.T0 = e.T0_nondim;
+  c.vonk_g = 0.4 * e.g_nondim;
+  c.log_m = std::log(0.5 * e.dz * e.z_scale / e.cfg.z0m);
+  const double zref = e.cfg.zTemperature > 0.0 ? e.cfg.zTemperature : e.cfg.z0T;
+  c.log_h = std::log(0.5 * e.dz * e.z_scale / zref);
+  c.half_dz = 0.5 * e.dz;
+  c.z0m_s = e.cfg.z0m / e.z_scale;
+  c.zT_s = zref / e.z_scale;
+  c.variant = variant;
+  c.sfc_val = sfc_val;
+  c.qz_const = e.qz_sfc_const;
+  c.H = e.H();
+  c.nz = e.nz;
+  SurfPtr p;
+  p.u = io.u;
+  p.v = io.v;
+  p.TH = io.TH;
+  for (int i = 0; i < 6; i++) {
+    p.mi[i] = io.most_in[i];
+    p.mo[i] = io.most_out[i];
+  }
+  p.M = io.M;
+  p.ustar = io.ustar;
+  p.q2 = io.q2;
+  p.qavg = io.qavg;
+  p.invOB = io.invOB;
+  k_surface<<<1, 1024, 0, e.stream>>>(c, p);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// vertical derivatives: Derivatives.py:190-362
+// ---------------------------------------------------------------------------
+__global__ void k_derivz_M(const double* __restrict__ u, const double* __restrict__ v,
+                           const double* __restrict__ w, const double* __restrict__ ustar,
+                           const double* __restrict__ M, const double* __restrict__ fi,
+                           double* dudz, double* dvdz, double* dwdz, size_t n, int nz,
+                           double idz, double Ugal, double den_c) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const size_t r = i / nz;
+    if (z == 0) {
+      const double den = M[r] * 0.4 * 0.5 * den_c;
+      dudz[i] = fi[r] * ustar[r] * (u[i] + Ugal) / den;
+      dvdz[i] = fi[r] * ustar[r] * v[i] / den;
+    } else if (z < nz - 1) {
+      dudz[i] = (u[i] - u[i - 1]) * idz;
+      dvdz[i] = (v[i] - v[i - 1]) * idz;
+    } else {
+      dudz[i] = 0.0;
+      dvdz[i] = 0.0;
+    }
+    dwdz[i] = (z < nz - 1) ? (w[i + 1] - w[i]) * idz : 0.0;
+  }
+}
+
+void derivz_M(Engine& e, const double* u, const double* v, const double* w, const double* ustar,
+              const double* M, const double* fi_m, double* dudz, double* dvdz, double* dwdz) {
+  k_derivz_M<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, v, w, ustar, M, fi_m, dudz, dvdz, dwdz,
+                                                    e.N(), e.nz, e.idz, e.cfg.Ugal, e.dz);
+}
+
+__global__ void k_derivz_TH(const double* __restrict__ T, const double* __restrict__ ustar,
+                            const double* __restrict__ qz, const double* __restrict__ fi,
+                            double* out, size_t n, int nz, double idz, double den) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const size_t r = i / nz;
+    if (z == 0) {
+      out[i] = fi[r] * (-qz[r] / ustar[r]) / den;
+    } else {
+      out[i] = (T[i] - T[i - 1]) * idz;
+    }
+  }
+}
+
+void derivz_TH(Engine& e, const double* TH, const double* ustar, const double* qz,
+               const double* fi_h, double* dTHdz) {
+  k_derivz_TH<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, ustar, qz, fi_h, dTHdz, e.N(), e.nz,
+                                                     e.idz, 0.4 * 0.5 * e.dz);
+}
+
+__device__ __forceinline__ double dz_generic(const double* F, size_t i, int z, int nz, int w,
+                                             double idz) {
+  if (w) return (z < nz - 1) ? (F[i + 1] - F[i]) * idz : 0.0;  // Derivz_Generic_w
+  return (z > 0) ? (F[i] - F[i - 1]) * idz : 0.0;              // Derivz_Generic_uvp
+}
+
+__global__ void k_derivz_generic(const double* __restrict__ F, double* out, size_t n, int nz,
+                                 int w, double idz) {
+  GRID_STRIDE(i, n) { out[i] = dz_generic(F, i, (int)(i % nz), nz, w, idz); }
+}
+
+void derivz_generic(Engine& e, const double* F, int w_nodes, double* out) {
+  k_derivz_generic<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nz, w_nodes, e.idz);
+}
+
+__global__ void k_div_finish(double* div, const double* __restrict__ f, size_t n, int nz, int w,
+                             double idz) {
+  GRID_STRIDE(i, n) { div[i] = div[i] + dz_generic(f, i, (int)(i % nz), nz, w, idz); }
+}
+
+void divergence_finish(Engine& e, double* div, const double* fz, int w_nodes) {
+  k_div_finish<<<nblocks(e.N()), TPB, 0, e.stream>>>(div, fz, e.N(), e.nz, w_nodes, e.idz);
+}
+
+// ---------------------------------------------------------------------------
+// buoyancy: NSE_BuoyancyTerms.py:49-150 (dry, H = 0)
+// ---------------------------------------------------------------------------
+__global__ void k_buoy(const double* __restrict__ TH, const double* __restrict__ bar, double* out,
+                       size_t n, int nz, double T0, int by_mean, double hg) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    if (z == 0) {
+      out[i] = 0.0;
+    } else {
+      const double b1 = bar[z], b0 = bar[z - 1];
+      const double t1 = (TH[i] + T0) * 1.0, t0 = (TH[i - 1] + T0) * 1.0;
+      const double n1 = (t1 - b1) / (by_mean ? b1 : T0);
+      const double n0 = (t0 - b0) / (by_mean ? b0 : T0);
+      out[i] = hg * (n1 + n0);
+    }
+  }
+}
+
+__global__ void k_add_const(const double* __restrict__ a, double c, double* out, size_t n) {
+  GRID_STRIDE(i, n) { out[i] = (a[i] + c) * 1.0; }
+}
+
+void buoyancy(Engine& e, const double* TH, int opt, double* out) {
+  // THv = (TH + T_0)(1 + 0.61 H), H = 0; its plane mean
+  double* thv = e.W;  // first workspace field
+  k_add_const<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.T0_nondim, thv, e.N());
+  const double* f[1] = {thv};
+  plane_means(e, f, 1, e.scal);
+  k_buoy<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.scal, out, e.N(), e.nz, e.T0_nondim, opt,
+                                                0.5 * e.g_nondim);
+}
+
+// ---------------------------------------------------------------------------
+// strain rates: StrainRates.py:56-141 (uvp), 219-299 (w)
+// ---------------------------------------------------------------------------
+struct G9 {
+  const double* g[9];
+};
+
+__device__ __forceinline__ double smag_of(double s11, double s22, double s33, double s12,
+                                          double s13, double s23) {
+  return sqrt(2.0 * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12) +
+                     2.0 * (s13 * s13) + 2.0 * (s23 * s23)));
+}
+
+__global__ void k_strains_uvp(G9 G, double* S12, double* S13, double* S23, double* S, size_t n,
+                              int nz) {
+  // g: dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const double* const* g = G.g;
+    double uz, vz, wx, wy;
+    if (z == 0) {
+      uz = g[6][i];
+      vz = g[7][i];
+      wx = 0.5 * g[2][i + 1];
+      wy = 0.5 * g[5][i + 1];
+    } else if (z == nz - 1) {
+      uz = g[6][i];
+      vz = g[7][i];
+      wx = g[2][i];
+      wy = g[5][i];
+    } else {
+      uz = 0.5 * (g[6][i] + g[6][i + 1]);
+      vz = 0.5 * (g[7][i] + g[7][i + 1]);
+      wx = 0.5 * (g[2][i] + g[2][i + 1]);
+      wy = 0.5 * (g[5][i] + g[5][i + 1]);
+    }
+    const double s11 = g[0][i], s22 = g[4][i], s33 = g[8][i];
+    const double s12 = 0.5 * (g[3][i] + g[1][i]);
+    const double s13 = 0.5 * (uz + wx);
+    const double s23 = 0.5 * (vz + wy);
+    S12[i] = s12;
+    S13[i] = s13;
+    S23[i] = s23;
+    S[i] = smag_of(s11, s22, s33, s12, s13, s23);
+  }
+}
+
+void strains_uvp(Engine& e, const double* const g[9], double* S12, double* S13, double* S23,
+                 double* S) {
+  G9 G;
+  for (int i = 0; i < 9; i++) G.g[i] = g[i];
+  k_strains_uvp<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, S12, S13, S23, S, e.N(), e.nz);
+}
+
+__global__ void k_smag_w(G9 G, double* Sw, size_t n, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const double* const* g = G.g;
+    auto stag = [&](const double* d) -> double {
+      if (z == 0) return d[i];
+      if (z == nz - 1) return 0.0;
+      return 0.5 * (d[i - 1] + d[i]);
+    };
+    const double s11 = stag(g[0]), s22 = stag(g[4]), s33 = stag(g[8]);
+    const double s12 = 0.5 * (stag(g[3]) + stag(g[1]));
+    const double wx = (z == 0) ? 0.5 * (g[2][i] + g[2][i + 1]) : g[2][i];
+    const double wy = (z == 0) ? 0.5 * (g[5][i] + g[5][i + 1]) : g[5][i];
+    const double s13 = 0.5 * (g[6][i] + wx);
+    const double s23 = 0.5 * (g[7][i] + wy);
+    Sw[i] = smag_of(s11, s22, s33, s12, s13, s23);
+  }
+}
+
+void smag_w(Engine& e, const double* const g[9], double* Sw) {
+  G9 G;
+  for (int i = 0; i < 9; i++) G.g[i] = g[i];
+  k_smag_w<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, Sw, e.N(), e.nz);
+}
+
+struct P6 {
+  const double* s[6];
+};
+
+__global__ void k_smag6(P6 P, double* out, size_t n) {
+  GRID_STRIDE(i, n) {
+    out[i] = smag_of(P.s[0][i], P.s[1][i], P.s[2][i], P.s[3][i], P.s[4][i], P.s[5][i]);
+  }
+}
+
+void smag6(Engine& e, const double* const s[6], size_t n, double* out) {
+  P6 P;
+  for (int i = 0; i < 6; i++) P.s[i] = s[i];
+  k_smag6<<<nblocks(n), TPB, 0, e.stream>>>(P, out, n);
+}
+
+void smag6_n(Engine& e, const double* const s[6], double* out) { smag6(e, s, e.N(), out); }
+
+// w_ of DynamicSGS_LASDD_SM.py:180-183
+__global__ void k_wstar(const double* __restrict__ w, double* out, size_t n, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    if (z == 0) out[i] = 0.5 * w[i + 1];
+    else if (z == nz - 1) out[i] = w[i - 1];
+    else out[i] = 0.5 * (w[i] + w[i + 1]);
+  }
+}
+
+void wstar(Engine& e, const double* w, double* w_) {
+  k_wstar<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, w_, e.N(), e.nz);
+}
+
+// ---------------------------------------------------------------------------
+// LASDD (DynamicSGS_LASDD_SM.py:250-352): Germano contractions
+// ---------------------------------------------------------------------------
+struct LasddConst {
+  double cA, cB1, cB2, cC, cD1, cD2, cE1, cE2, T1, T2;
+};
+
+__device__ __forceinline__ double contract6(const double* A, const double* B) {
+  return A[0] * B[0] + A[1] * B[1] + A[2] * B[2] + 2.0 * (A[3] * B[3] + A[4] * B[4] + A[5] * B[5]);
+}
+__device__ __forceinline__ double sq6(const double* A) {
+  return A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + 2.0 * (A[3] * A[3] + A[4] * A[4] + A[5] * A[5]);
+}
+
+__device__ __forceinline__ void leonard(const double* const* ph, const double* const* hat, size_t i,
+                                        double* Lo) {
+  const double u = hat[0][i], v = hat[1][i], w = hat[2][i];
+  Lo[0] = ph[0][i] - u * u;
+  Lo[1] = ph[1][i] - v * v;
+  Lo[2] = ph[2][i] - w * w;
+  Lo[3] = ph[3][i] - u * v;
+  Lo[4] = ph[4][i] - u * w;
+  Lo[5] = ph[5][i] - v * w;
+}
+
+__global__ void k_lasdd_partial(LasddFields f, LasddConst c, size_t H, int nz,
+                                double* __restrict__ part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t r = r0; r < r1; r++) {
+      const size_t i = r * nz + z;
+      double Lm[6], Qm[6], S1[6], S2[6], SS1[6], SS2[6];
+      leonard(f.ph, f.hat, i, Lm);
+      leonard(f.pd, f.hatd, i, Qm);
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        S1[q] = f.Sh[q][i];
+        S2[q] = f.Sd[q][i];
+        SS1[q] = f.SSh[q][i];
+        SS2[q] = f.SSd[q][i];
+      }
+      const double Sh = f.S_hat[i], Sd = f.S_hatd[i];
+      s[0] += c.cA * contract6(Lm, SS1);
+      s[1] += c.cA * contract6(Qm, SS2);
+      s[2] += c.cB1 * Sh * contract6(Lm, S1);
+      s[3] += c.cB2 * Sd * contract6(Qm, S2);
+      s[4] += c.cC * sq6(SS1);
+      s[5] += c.cC * sq6(SS2);
+      s[6] += c.cD1 * (Sh * Sh) * sq6(S1);
+      s[7] += c.cD2 * (Sd * Sd) * sq6(S2);
+      s[8] += c.cE1 * Sh * contract6(S1, SS1);
+      s[9] += c.cE2 * Sd * contract6(S2, SS2);
+    }
+#pragma unroll
+    for (int q = 0; q < 10; q++) part[((size_t)blockIdx.x * 10 + q) * nz + z] = s[q];
+  }
+}
+
+static LasddConst lasdd_const(const Engine& e) {
+  const double L = e.L, T = e.TFR;
+  LasddConst c;
+  c.cA = 2 * std::pow(L, 2.0);
+  c.cB1 = 2 * std::pow(L, 2.0) * std::pow(T, 2.0);
+  c.cB2 = 2 * std::pow(L, 2.0) * std::pow(T, 4.0);
+  c.cC = std::pow(2 * std::pow(L, 2.0), 2.0);
+  c.cD1 = (4 * std::pow(L, 4.0)) * std::pow(T, 4.0);
+  c.cD2 = (4 * std::pow(L, 4.0)) * std::pow(T, 8.0);
+  c.cE1 = (8 * std::pow(L, 4.0)) * std::pow(T, 2.0);
+  c.cE2 = (8 * std::pow(L, 4.0)) * std::pow(T, 4.0);
+  c.T1 = 2 * std::pow(L, 2.0);
+  c.T2 = 2 * std::pow(T * L, 2.0);
+  return c;
+}
+
+void lasdd_sums(Engine& e, const LasddFields& f, double* sums10) {
+  const int nb = red_blocks(e);
+  k_lasdd_partial<<<nb, 128, 0, e.stream>>>(f, lasdd_const(e), e.H(), e.nz, e.red);
+  k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
+                                                                       1.0 / (double)e.H(), sums10);
+}
+
+// polynomial coefficients per level (ff, ee, dd, cc, bb, aa) from plane means
+__global__ void k_poly(const double* __restrict__ m, int nz, int scalar, double* co) {
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    double a1 = m[0 * nz + z], a2 = m[1 * nz + z], b1 = m[2 * nz + z], b2 = m[3 * nz + z];
+    double c1 = m[4 * nz + z], c2 = m[5 * nz + z], d1 = m[6 * nz + z], d2 = m[7 * nz + z];
+    double e1 = m[8 * nz + z], e2 = m[9 * nz + z];
+    double aa, bb, cc, dd, ee, ff;
+    if (!scalar) {  // DynamicSGS_LASDD_SM.py:314-319
+      aa = a1 * c2 - a2 * c1;
+      bb = a2 * e1 - b1 * c2;
+      cc = b2 * c1 - a1 * e2 - a2 * d1;
+      dd = b1 * e2 - b2 * e1;
+      ee = a1 * d2 + b2 * d1;
+      ff = -b1 * d2;
+    } else {  // DynamicSGS_ScalarLASDD_SM.py:285-290 (slots: a2 b2 c2 d2 e2 a4 b4 c4 d4 e4)
+      const double A2 = a1, B2 = a2, C2 = b1, D2 = b2, E2 = c1;
+      const double A4 = c2, B4 = d1, C4 = d2, D4 = e1, E4 = e2;
+      aa = A2 * C4 - A4 * C2;
+      bb = -A4 * D2 + B2 * C4;
+      cc = -C2 * B4 + A2 * D4 - A4 * E2;
+      dd = B2 * D4 - B4 * D2;
+      ee = A2 * E4 - B4 * E2;
+      ff = B2 * E4;
+    }
+    co[0 * nz + z] = ff;
+    co[1 * nz + z] = ee;
+    co[2 * nz + z] = dd;
+    co[3 * nz + z] = cc;
+    co[4 * nz + z] = bb;
+    co[5 * nz + z] = aa;
+  }
+}
+
+void lasdd_poly(Engine& e, const double* sums10, int scalar, double* coeffs6) {
+  k_poly<<<1, 256, 0, e.stream>>>(sums10, e.nz, scalar, coeffs6);
+}
+
+// ---------------------------------------------------------------------------
+// Laguerre iteration (Utilities.py:123-241) from 8 guesses per level and the
+// beta selection of ComputeBeta1/2: one thread per (level, guess)
+// ---------------------------------------------------------------------------
+struct cx {
+  double r, i;
+};
+__device__ __forceinline__ cx cxadd(cx a, cx b) { return {a.r + b.r, a.i + b.i}; }
+__device__ __forceinline__ cx cxsub(cx a, cx b) { return {a.r - b.r, a.i - b.i}; }
+__device__ __forceinline__ cx cxmul(cx a, cx b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+__device__ __forceinline__ double cxabs(cx a) { return hypot(a.r, a.i); }
+// Smith's algorithm for a / b
+__device__ cx cxdiv(cx a, cx b) {
+  if (fabs(b.r) >= fabs(b.i)) {
+    if (b.r == 0.0 && b.i == 0.0) return {a.r / fabs(b.r), a.i / fabs(b.i)};
+    const double rat = b.i / b.r;
+    const double den = b.r + b.i * rat;
+    return {(a.r + a.i * rat) / den, (a.i - a.r * rat) / den};
+  }
+  const double rat = b.r / b.i;
+  const double den = b.i + b.r * rat;
+  return {(a.r * rat + a.i) / den, (a.i * rat - a.r) / den};
+}
+// principal square root
+__device__ cx cxsqrt(cx a) {
+  if (a.r == 0.0 && a.i == 0.0) return {0.0, a.i};
+  const double t = sqrt((fabs(a.r) + hypot(a.r, a.i)) * 0.5);
+  if (a.r >= 0.0) return {t, a.i / (2.0 * t)};
+  return {fabs(a.i) / (2.0 * t), copysign(t, a.i)};
+}
+
+__global__ void k_beta(const double* __restrict__ co, int nlev, double* beta) {
+  const double guesses[8] = {0.5, 0.75, 1.0, 1.25, 1.5, 2.0, 3.0, 4.5};
+  __shared__ double best[32][8];
+  const int lvl_local = threadIdx.x / 8;
+  const int g = threadIdx.x % 8;
+  const int lvl = blockIdx.x * 32 + lvl_local;
+  double val = -INFINITY;
+  if (lvl < nlev) {
+    double p[6];
+#pragma unroll
+    for (int j = 0; j < 6; j++) p[j] = co[j * nlev + lvl];
+    const int n = 5;
+    cx dp[5], d2p[4];
+#pragma unroll
+    for (int j = 0; j < 5; j++) dp[j] = {p[j] * (double)(n - j), 0.0};
+#pragma unroll
+    for (int j = 0; j < 4; j++) d2p[j] = {dp[j].r * (double)(n - 1 - j), 0.0};
+    cx x = {guesses[g], 0.0};
+    bool conv = false;
+    const double tol = 1e-6;
+    const cx eps = {1e-16, 0.0};
+    for (int it = 0; it < 20 && !conv; it++) {
+      cx f = {0.0, 0.0}, df = {0.0, 0.0}, d2f = {0.0, 0.0};
+      for (int j = 0; j < 6; j++) f = cxadd(cxmul(f, x), cx{p[j], 0.0});
+      for (int j = 0; j < 5; j++) df = cxadd(cxmul(df, x), dp[j]);
+      for (int j = 0; j < 4; j++) d2f = cxadd(cxmul(d2f, x), d2p[j]);
+      const cx fs = (cxabs(f) < 1e-16) ? eps : f;
+      const cx G = cxdiv(df, fs);
+      const cx G2 = cxmul(G, G);
+      const cx Hh = cxsub(G2, cxdiv(d2f, fs));
+      const cx inner = cxsub(cx{n * Hh.r, n * Hh.i}, G2);
+      const cx disc = {(n - 1) * inner.r, (n - 1) * inner.i};
+      const cx sq = cxsqrt(disc);
+      const cx d1 = cxadd(G, sq), dd2 = cxsub(G, sq);
+      cx den = (cxabs(d1) > cxabs(dd2)) ? d1 : dd2;
+      if (cxabs(den) < 1e-16) den = eps;
+      const cx xn = cxsub(x, cxdiv(cx{(double)n, 0.0}, den));
+      conv = (cxabs(cxsub(xn, x)) < tol * (1.0 + cxabs(x))) || (cxabs(f) < tol);
+      x = xn;
+    }
+    if (conv && fabs(x.i) < 1e-6 && x.r > 0.0 && x.r < 5.0) val = x.r;
+  }
+  best[lvl_local][g] = val;
+  __syncthreads();
+  if (g == 0 && lvl < nlev) {
+    double m = -INFINITY;
+    for (int j = 0; j < 8; j++) m = fmax(m, best[lvl_local][j]);
+    beta[lvl] = isinf(m) ? 1.0 : m;
+  }
+}
+
+void compute_beta(Engine& e, const double* coeffs6, int nlev, double* beta) {
+  k_beta<<<(nlev + 31) / 32, 256, 0, e.stream>>>(coeffs6, nlev, beta);
+}
+
+__global__ void k_ones(double* p, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 1.0;
+}
+
+__global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ beta, double* LM,
+                        double* MM, size_t n, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    double Lm[6], Mm[6];
+    leonard(f.ph, f.hat, i, Lm);
+    const double b = beta[z];
+    const double Sh = f.S_hat[i];
+#pragma unroll
+    for (int q = 0; q < 6; q++) Mm[q] = c.T1 * f.SSh[q][i] - c.T2 * b * Sh * f.Sh[q][i];
+    LM[i] = (Lm[0] * Mm[0] + Lm[1] * Mm[1] + Lm[2] * Mm[2]) +
+            2.0 * (Lm[3] * Mm[3] + Lm[4] * Mm[4] + Lm[5] * Mm[5]);
+    MM[i] = sq6(Mm);
+  }
+}
+
+void lasdd_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM) {
+  k_LM_MM<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, lasdd_const(e), beta, LM, MM, e.N(), e.nz);
+}
+
+// 3x3 periodic box mean (Utilities.py:87-115) at (x, y, z)
+__device__ __forceinline__ double box9(const double* F, int x, int y, int z, int nx, int ny,
+                                       int nz) {
+  double s = 0.0;
+  const double w = 1.0 / 9.0;
+  for (int a = 0; a < 3; a++) {
+    const int xx = (x + a - 1 + nx) % nx;
+    for (int b = 0; b < 3; b++) {
+      const int yy = (y + b - 1 + ny) % ny;
+      s = s + F[((size_t)xx * ny + yy) * nz + z] * w;
+    }
+  }
+  return s;
+}
+
+__global__ void k_clip_ratio(const double* __restrict__ num, const double* __restrict__ den,
+                             double* out, size_t n, int nx, int ny, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const size_t r = i / nz;
+    const int y = (int)(r % ny), x = (int)(r / ny);
+    const double nf = box9(num, x, y, z, nx, ny, nz);
+    const double df = box9(den, x, y, z, nx, ny, nz);
+    const double q = nf / df;
+    const bool bad = (fabs(df) < 1e-10) || (q < 0.0) || (q > 1.0);
+    out[i] = bad ? 0.0 : q;
+  }
+}
+
+void clip_ratio(Engine& e, const double* num, const double* den, double* out) {
+  k_clip_ratio<<<nblocks(e.N()), TPB, 0, e.stream>>>(num, den, out, e.N(), e.nx, e.ny, e.nz);
+}
+
+__global__ void k_imfilter(const double* __restrict__ F, double* out, size_t n, int nx, int ny,
+                           int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const size_t r = i / nz;
+    out[i] = box9(F, (int)(r / ny), (int)(r % ny), z, nx, ny, nz);
+  }
+}
+
+void imfilter(Engine& e, const double* F, double* out) {
+  k_imfilter<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nx, e.ny, e.nz);
+}
+
+__global__ void k_cs2_partial(const double* __restrict__ C, size_t H, int nz, double* part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double s0 = 0.0, s1 = 0.0;
+    for (size_t r = r0; r < r1; r++) {
+      const double c = C[r * nz + z];
+      s0 += sqrt(c);
+      s1 += c;
+    }
+    part[((size_t)blockIdx.x * 2 + 0) * nz + z] = s0;
+    part[((size_t)blockIdx.x * 2 + 1) * nz + z] = s1;
+  }
+}
+
+__global__ void k_cs2_finish(const double* __restrict__ m, int nz, double* avg1, double* avg2) {
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    const double a = m[z];
+    if (avg1) avg1[z] = a * a;
+    if (avg2) avg2[z] = m[nz + z];
+  }
+}
+
+void cs2_profiles(Engine& e, const double* Cs2, double* avg1, double* avg2) {
+  const int nb = red_blocks(e);
+  k_cs2_partial<<<nb, 128, 0, e.stream>>>(Cs2, e.H(), e.nz, e.red);
+  double* m = e.scal + 64;
+  k_partial_finish<<<nblocks((size_t)2 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 2, e.nz,
+                                                                      1.0 / (double)e.H(), m);
+  k_cs2_finish<<<1, 256, 0, e.stream>>>(m, e.nz, avg1, avg2);
+}
+
+// ---------------------------------------------------------------------------
+// Scalar LASDD (DynamicSGS_ScalarLASDD_SM.py:224-307)
+// ---------------------------------------------------------------------------
+struct SLConst {
+  double cL2, cb2, cL4, cd2, ce2, cb4, cd4, ce4;
+};
+
+static SLConst sl_const(const Engine& e) {
+  const double L = e.L, T = e.TFR;
+  SLConst c;
+  c.cL2 = std::pow(L, 2.0);
+  c.cb2 = -std::pow(L, 2.0) * std::pow(T, 2.0);
+  c.cL4 = std::pow(L, 4.0);
+  c.cd2 = -2 * std::pow(L, 4.0) * std::pow(T, 2.0);
+  c.ce2 = std::pow(L, 4.0) * std::pow(T, 4.0);
+  c.cb4 = -std::pow(L, 2.0) * std::pow(T, 4.0);
+  c.cd4 = -2 * std::pow(L, 4.0) * std::pow(T, 4.0);
+  c.ce4 = std::pow(L, 4.0) * std::pow(T, 8.0);
+  return c;
+}
+
+struct SLTerms {
+  double a, b, c, d, e;
+};
+
+__device__ __forceinline__ SLTerms sl_terms(const double* const* uT, const double* const* hat,
+                                            const double* Tf, const double* const* SG,
+                                            const double* const* G, const double* S, size_t i) {
+  const double T = Tf[i], s = S[i];
+  double LT[3], sg[3], g[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    LT[q] = uT[q][i] - hat[q][i] * T;
+    sg[q] = SG[q][i];
+    g[q] = G[q][i];
+  }
+  SLTerms t;
+  t.a = LT[0] * sg[0] + LT[1] * sg[1] + LT[2] * sg[2];
+  t.b = LT[0] * s * g[0] + LT[1] * s * g[1] + LT[2] * s * g[2];
+  t.c = sg[0] * sg[0] + sg[1] * sg[1] + sg[2] * sg[2];
+  t.d = sg[0] * s * g[0] + sg[1] * s * g[1] + sg[2] * s * g[2];
+  const double p0 = s * g[0], p1 = s * g[1], p2 = s * g[2];
+  t.e = p0 * p0 + p1 * p1 + p2 * p2;
+  return t;
+}
+
+__global__ void k_sl_partial(ScalarLasddFields f, SLConst c, size_t H, int nz, double* part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t r = r0; r < r1; r++) {
+      const size_t i = r * nz + z;
+      const SLTerms t1 = sl_terms(f.uTh, f.hat, f.Th, f.SGh, f.Gh, f.S_hat, i);
+      const SLTerms t2 = sl_terms(f.uTd, f.hatd, f.Td, f.SGd, f.Gd, f.S_hatd, i);
+      s[0] += c.cL2 * t1.a;
+      s[1] += c.cb2 * t1.b;
+      s[2] += c.cL4 * t1.c;
+      s[3] += c.cd2 * t1.d;
+      s[4] += c.ce2 * t1.e;
+      s[5] += c.cL2 * t2.a;
+      s[6] += c.cb4 * t2.b;
+      s[7] += c.cL4 * t2.c;
+      s[8] += c.cd4 * t2.d;
+      s[9] += c.ce4 * t2.e;
+    }
+#pragma unroll
+    for (int q = 0; q < 10; q++) part[((size_t)blockIdx.x * 10 + q) * nz + z] = s[q];
+  }
+}
+
+void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10) {
+  const int nb = red_blocks(e);
+  k_sl_partial<<<nb, 128, 0, e.stream>>>(f, sl_const(e), e.H(), e.nz, e.red);
+  k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
+                                                                       1.0 / (double)e.H(), sums10);
+}
+
+__global__ void k_sl_TupTdn(ScalarLasddFields f, SLConst c, const double* __restrict__ beta,
+                            double* Tup, double* Tdn, size_t n, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const SLTerms t = sl_terms(f.uTh, f.hat, f.Th, f.SGh, f.Gh, f.S_hat, i);
+    const double b = beta[z];
+    Tup[i] = c.cL2 * t.a + c.cb2 * t.b * b;
+    Tdn[i] = c.cL4 * t.c + c.cd2 * t.d * b + c.ce2 * t.e * (b * b);
+  }
+}
+
+void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
+                    double* Tdn) {
+  k_sl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, sl_const(e), beta, Tup, Tdn, e.N(), e.nz);
+}
+
+// ---------------------------------------------------------------------------
+// wall stresses (SGSStresses_SM.py:63-90, 238-241) and plane-0 overrides
+// ---------------------------------------------------------------------------
+__global__ void k_wall(const double* __restrict__ u, const double* __restrict__ v,
+                       const double* __restrict__ M, const double* __restrict__ pm,
+                       const double* __restrict__ pm0, double* txz, double* tyz, size_t H, int nz,
+                       double log_m, double Ugal) {
+  GRID_STRIDE(r, H) {
+    const double denom = log_m + pm[r] - pm0[r];
+    const double us = 0.4 * M[r] / denom;
+    const size_t i = r * nz;
+    txz[i] = -(us * us) * (u[i] + Ugal) / M[r];
+    tyz[i] = -(us * us) * v[i] / M[r];
+  }
+}
+
+void wall_override(Engine& e, const double* u, const double* v, const double* M,
+                   const double* psi_m, const double* psi_m0, double* txz, double* tyz) {
+  const double log_m = std::log(0.5 * e.dz * e.z_scale / e.cfg.z0m);
+  k_wall<<<nblocks(e.H()), TPB, 0, e.stream>>>(u, v, M, psi_m, psi_m0, txz, tyz, e.H(), e.nz,
+                                                log_m, e.cfg.Ugal);
+}
+
+__global__ void k_set_plane0(const double* __restrict__ p, double* f, size_t H, int nz) {
+  GRID_STRIDE(r, H) { f[r * nz] = p[r]; }
+}
+
+void set_plane0(Engine& e, const double* plane, double* field) {
+  k_set_plane0<<<nblocks(e.H()), TPB, 0, e.stream>>>(plane, field, e.H(), e.nz);
+}
+
+// ---------------------------------------------------------------------------
+// RHS assembly: NSE_AllTerms.py:82-102, SCL_AllTerms.py:68-80
+// ---------------------------------------------------------------------------
+struct RhsM {
+  const double *u, *v, *w, *Ug, *Vg, *Cx, *Cy, *Cz, *b, *dx, *dy, *dz, *Uadv, *Vadv, *ubar, *vbar,
+      *rd, *rds;
+  double *Ru, *Rv, *Rw;
+  double f, Ugal;
+  int adv, damp;
+};
+
+__global__ void k_rhs_m(RhsM a, size_t n, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    double ru = -a.Cx[i] - a.dx[i] - a.f * (a.Vg[z] - a.v[i]);
+    double rv = -a.Cy[i] - a.dy[i] + a.f * (a.Ug[z] - a.Ugal - a.u[i]);
+    double rw = -a.Cz[i] - a.dz[i] + a.b[i];
+    if (a.adv) {
+      ru = ru + a.Uadv[z];
+      rv = rv + a.Vadv[z];
+    }
+    if (a.damp) {
+      ru = ru - a.rds[z] * (a.u[i] - a.ubar[z]);
+      rv = rv - a.rds[z] * (a.v[i] - a.vbar[z]);
+      rw = rw - a.rd[z] * a.w[i];
+    }
+    a.Ru[i] = ru;
+    a.Rv[i] = rv;
+    a.Rw[i] = rw;
+  }
+}
+
+void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
+                  const double* Ug, const double* Vg, const double* Cx, const double* Cy,
+                  const double* Cz, const double* b, const double* dx, const double* dy,
+                  const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
+                  const double* vbar, double* Ru, double* Rv, double* Rw) {
+  RhsM a{u, v, w, Ug, Vg, Cx, Cy, Cz, b, dx, dy, dz, Uadv, Vadv, ubar, vbar, e.d_rd, e.d_rd_stag,
+         Ru, Rv, Rw, e.f_nondim, e.cfg.Ugal, e.cfg.optAdvection >= 1, e.cfg.optDamping == 1};
+  k_rhs_m<<<nblocks(e.N()), TPB, 0, e.stream>>>(a, e.N(), e.nz);
+}
+
+__global__ void k_rhs_s(const double* __restrict__ TH, const double* __restrict__ adv,
+                        const double* __restrict__ dq, const double* __restrict__ THadv,
+                        const double* __restrict__ bar, const double* __restrict__ rds, double* R,
+                        size_t n, int nz, int doadv, int damp) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    double r = -adv[i] - dq[i];
+    if (doadv) r = r + THadv[z];
+    if (damp) r = r - rds[z] * (TH[i] - bar[z]);
+    R[i] = r;
+  }
+}
+
+void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
+                const double* THadv, const double* THbar, double* R) {
+  k_rhs_s<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, adv, divq, THadv, THbar, e.d_rd_stag, R,
+                                                 e.N(), e.nz, e.cfg.optAdvection >= 1,
+                                                 e.cfg.optDamping == 1);
+}
+
+// ---------------------------------------------------------------------------
+// pressure: NSE_PressureTerms.py:150-182 (RC assembly) and
+// NSE_PressureTerms_Thomas.py:246-275 (masked solve + zero mode)
+// ---------------------------------------------------------------------------
+__global__ void k_rc(const cd* __restrict__ fRx, const cd* __restrict__ fRy,
+                     const cd* __restrict__ fRz, const cd* __restrict__ fb2,
+                     const double* __restrict__ kr, double* RCr, double* RCi, double* fRzr,
+                     int nx, int nyh, int nz, double dz) {
+  const size_t n = (size_t)nx * nyh * (nz + 1);
+  GRID_STRIDE(t, n) {
+    const int k = (int)(t % (nz + 1));
+    const size_t m = t / (nz + 1);  // mode (i, j)
+    const int j = (int)(m % nyh), i = (int)(m / nyh);
+    if (k == 0) {
+      const cd f = fb2[m * 2 + 0];
+      RCr[t] = -dz * f.x;
+      RCi[t] = -dz * f.y;
+    } else if (k == nz) {
+      const cd f = fb2[m * 2 + 1];
+      RCr[t] = -dz * f.x;
+      RCi[t] = -dz * f.y;
+    } else {
+      const size_t a = m * nz + (k - 1);
+      const double q = kr[i], c = (double)j;
+      double hr = -q * fRx[a].y;
+      hr = hr - c * fRy[a].y;
+      double hi = q * fRx[a].x;
+      hi = hi + c * fRy[a].x;
+      RCr[t] = hr + (fRz[a + 1].x - fRz[a].x) / dz;
+      RCi[t] = hi + (fRz[a + 1].y - fRz[a].y) / dz;
+    }
+    if (k < nz) fRzr[m * nz + k] = fRz[m * nz + k].x;
+  }
+}
+
+void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const cd* fb2,
+                 const cd* /*unused*/, double* RCr, double* RCi, double* fRz_real) {
+  k_rc<<<nblocks((size_t)e.nx * e.nyh * (e.nz + 1)), TPB, 0, e.stream>>>(
+      fRx, fRy, fRz, fb2, e.d_kr, RCr, RCi, fRz_real, e.nx, e.nyh, e.nz, e.dz);
+}
+
+__global__ void k_thomas(const double* __restrict__ RCr, const double* __restrict__ RCi,
+                         const double* __restrict__ fRzr, const double* __restrict__ bt,
+                         const double* __restrict__ mt, const double* __restrict__ cp, cd* fp,
+                         int nx, int nyh, int nz, double dz) {
+  const size_t nm = (size_t)nx * nyh;
+  GRID_STRIDE(m, nm) {
+    const int j = (int)(m % nyh), i = (int)(m / nyh);
+    const size_t base = m * (nz + 1);
+    cd* out = fp + m * nz;
+    if (i == 0 && j == 0) {
+      // zero mode by direct integration (Thomas.py:271-275)
+      const double z0 = RCr[0];
+      out[0] = make_double2(z0, 0.0);
+      double s = 0.0;
+      for (int k = 1; k < nz; k++) {
+        s = s + fRzr[k] * dz;
+        out[k] = make_double2(z0 + s, 0.0);
+      }
+      continue;
+    }
+    if (i == nx / 2 || j == nyh - 1) {  // x- and y-Nyquist rows masked
+      for (int k = 0; k < nz; k++) out[k] = make_double2(0.0, 0.0);
+      continue;
+    }
+    // forward sweep (d_mod stored in out[k-1] for k >= 1)
+    double dr = RCr[base], di = RCi[base];
+    const double d0r = dr, d0i = di;
+    for (int k = 1; k <= nz; k++) {
+      const double mk = mt[(size_t)(k - 1) * nm + m];
+      dr = RCr[base + k] - mk * dr;
+      di = RCi[base + k] - mk * di;
+      out[k - 1] = make_double2(dr, di);
+    }
+    (void)d0r;
+    (void)d0i;
+    // back substitution, x[k] for k = nz .. 1 (x[0] is not used)
+    double xr = dr / bt[base + nz], xi = di / bt[base + nz];
+    out[nz - 1] = make_double2(xr, xi);
+    for (int k = nz - 1; k >= 1; k--) {
+      const cd dm = out[k - 1];
+      const double b = bt[base + k], c = cp[k];
+      xr = (dm.x - c * xr) / b;
+      xi = (dm.y - c * xi) / b;
+      out[k - 1] = make_double2(xr, xi);
+    }
+  }
+}
+
+void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double* fRz_real, cd* fp) {
+  const size_t nm = (size_t)e.nx * e.nyh;
+  k_thomas<<<(int)((nm + 127) / 128), 128, 0, e.stream>>>(RCr, RCi, fRz_real, e.d_b_thomas,
+                                                          e.d_m_thomas, e.d_c_p, fp, e.nx, e.nyh,
+                                                          e.nz, e.dz);
+}
+
+__global__ void k_sub3(double* a, double* b, double* c, const double* __restrict__ x,
+                       const double* __restrict__ y, const double* __restrict__ z, size_t n) {
+  GRID_STRIDE(i, n) {
+    a[i] = a[i] - x[i];
+    b[i] = b[i] - y[i];
+    c[i] = c[i] - z[i];
+  }
+}
+
+void subtract3(Engine& e, double* Ru, double* Rv, double* Rw, const double* a, const double* b,
+               const double* c) {
+  k_sub3<<<nblocks(e.N()), TPB, 0, e.stream>>>(Ru, Rv, Rw, a, b, c, e.N());
+}
+
+// ---------------------------------------------------------------------------
+// AB2: NSE_TimeAdvancement.py:66-74, SCL_TimeAdvancement.py:64-69.  The
+// thread of level nz-2 also writes level nz-1, so in-place update is safe.
+// ---------------------------------------------------------------------------
+__global__ void k_ab2(const double* u, const double* __restrict__ R, const double* __restrict__ Rp,
+                      double* un, size_t n, int nz, double dt, int mode, double top_add) {
+  // mode 0: u/v (top copies nz-2), 1: w (top and bottom 0), 2: TH (top = nz-2 + c)
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    if (z == nz - 1) continue;
+    const double val = u[i] + dt * (1.5 * R[i] - 0.5 * Rp[i]);
+    if (mode == 1) {
+      un[i] = (z == 0) ? 0.0 : val;
+      if (z == nz - 2) un[i + 1] = 0.0;
+    } else {
+      un[i] = val;
+      if (z == nz - 2) un[i + 1] = (mode == 2) ? val + top_add : val;
+    }
+  }
+}
+
+void ab2_uvw(Engine& e, const double* u, const double* v, const double* w, const double* Ru,
+             const double* Rup, const double* Rv, const double* Rvp, const double* Rw,
+             const double* Rwp, double* un, double* vn, double* wn) {
+  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, Ru, Rup, un, e.N(), e.nz, e.dt_nondim, 0, 0.0);
+  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(v, Rv, Rvp, vn, e.N(), e.nz, e.dt_nondim, 0, 0.0);
+  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, Rw, Rwp, wn, e.N(), e.nz, e.dt_nondim, 1, 0.0);
+}
+
+void ab2_th(Engine& e, const double* TH, const double* R, const double* Rp, double* out) {
+  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
+                                               e.inversion_nondim * e.dz);
+}
+
+// max |u|, |v|, |w| (Main.py:534-537)
+__global__ void k_absmax_partial(const double* __restrict__ a, const double* __restrict__ b,
+                                 const double* __restrict__ c, size_t n, double* part) {
+  __shared__ double sh[3][256];
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  GRID_STRIDE(i, n) {
+    m0 = fmax(m0, fabs(a[i]));
+    m1 = fmax(m1, fabs(b[i]));
+    m2 = fmax(m2, fabs(c[i]));
+  }
+  sh[0][threadIdx.x] = m0;
+  sh[1][threadIdx.x] = m1;
+  sh[2][threadIdx.x] = m2;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int q = 0; q < 3; q++) sh[q][threadIdx.x] = fmax(sh[q][threadIdx.x], sh[q][threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; q++) part[blockIdx.x * 3 + q] = sh[q][0];
+}
+
+__global__ void k_absmax_finish(const double* part, int nb, double* out) {
+  if (threadIdx.x < 3) {
+    double m = 0.0;
+    for (int b = 0; b < nb; b++) m = fmax(m, part[b * 3 + threadIdx.x]);
+    out[threadIdx.x] = m;
+  }
+}
+
+void cfl_max(Engine& e, const double* u, const double* v, const double* w, double* out3) {
+  const int nb = 256;
+  k_absmax_partial<<<nb, 256, 0, e.stream>>>(u, v, w, e.N(), e.red);
+  k_absmax_finish<<<1, 32, 0, e.stream>>>(e.red, nb, out3);
+}
+
+// copy z-planes k0 and k1 of F into a (nx, ny, 2) field
+__global__ void k_planes(const double* __restrict__ F, int k0, int k1, double* out, size_t H,
+                         int nz) {
+  GRID_STRIDE(r, H) {
+    out[r * 2 + 0] = F[r * nz + k0];
+    out[r * 2 + 1] = F[r * nz + k1];
+  }
+}
+
+void copy_planes_z(Engine& e, const double* F, int k0, int k1, double* out2) {
+  k_planes<<<nblocks(e.H()), TPB, 0, e.stream>>>(F, k0, k1, out2, e.H(), e.nz);
+}
+
+}  // namespace alfa

@@ -1,0 +1,111 @@
+// Physical-space kernels of the LES step (declarations; alfa_physics.cu).
+#pragma once
+#include "alfa_internal.cuh"
+
+namespace alfa {
+
+// ---- reductions over (x, y) planes: deterministic two-level sums -------
+// sums[q][z] = sum over the plane of field q (nq fields)
+void plane_sums(Engine& e, const double* const* fields, int nq, double* sums);
+void plane_means(Engine& e, const double* const* fields, int nq, double* means);
+
+// ---- surface (SurfaceFlux.py) --------------------------------------------
+struct SurfaceIO {
+  const double* u;
+  const double* v;
+  const double* TH;
+  const double* most_in[6];
+  double* M;
+  double* ustar;
+  double* q2;        // qz_sfc_2D (may be null for constant-flux variants)
+  double* qavg;      // device scalar
+  double* invOB;
+  double* most_out[6];
+};
+// variant: 0 HomConst, 1 HetConst, 2 HomVary, 3 HetVary, 4 HomPresT, 5 HetPresT
+int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io);
+
+// ---- z derivatives (Derivatives.py) --------------------------------------
+void derivz_M(Engine& e, const double* u, const double* v, const double* w, const double* ustar,
+              const double* M, const double* fi_m, double* dudz, double* dvdz, double* dwdz);
+void derivz_TH(Engine& e, const double* TH, const double* ustar, const double* qz,
+               const double* fi_h, double* dTHdz);
+void derivz_generic(Engine& e, const double* F, int w_nodes, double* out);
+
+// ---- buoyancy ------------------------------------------------------------
+void buoyancy(Engine& e, const double* TH, int opt, double* out);
+
+// ---- strains -------------------------------------------------------------
+// uvp nodes: S12, S13, S23, |S| (S11, S22, S33 are dudx, dvdy, dwdz)
+void strains_uvp(Engine& e, const double* const g[9], double* S12, double* S13, double* S23,
+                 double* S);
+// |S| at w nodes from the gradients (non-padded)
+void smag_w(Engine& e, const double* const g[9], double* Sw);
+// |S| of six padded components
+void smag6(Engine& e, const double* const s[6], size_t n, double* out);
+
+// ---- LASDD ---------------------------------------------------------------
+void wstar(Engine& e, const double* w, double* w_);
+void smag6_n(Engine& e, const double* const s[6], double* out);
+// Germano terms: 10 plane sums (a1, a2, b1, b2, c1, c2, d1, d2, e1, e2)
+struct LasddFields {
+  const double* hat[3];    // u_hat v_hat w_hat
+  const double* hatd[3];
+  const double* ph[6];     // uu_hat .. vw_hat
+  const double* pd[6];
+  const double* Sh[6];
+  const double* Sd[6];
+  const double* SSh[6];
+  const double* SSd[6];
+  const double* S_hat;
+  const double* S_hatd;
+};
+void lasdd_sums(Engine& e, const LasddFields& f, double* sums10);
+void lasdd_poly(Engine& e, const double* sums10, int scalar, double* coeffs6);
+void compute_beta(Engine& e, const double* coeffs6, int nlev, double* beta);
+void lasdd_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM);
+void clip_ratio(Engine& e, const double* num, const double* den, double* out);
+void cs2_profiles(Engine& e, const double* Cs2, double* avg1, double* avg2);
+
+struct ScalarLasddFields {
+  const double* hat[3];
+  const double* hatd[3];
+  const double* Th, *Td;
+  const double* uTh[3], *uTd[3];
+  const double* Gh[3], *Gd[3];
+  const double* SGh[3], *SGd[3];
+  const double* S_hat, *S_hatd;
+};
+void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10);
+void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
+                    double* Tdn);
+
+// ---- stresses / fluxes / divergence -------------------------------------
+void wall_override(Engine& e, const double* u, const double* v, const double* M,
+                   const double* psi_m, const double* psi_m0, double* txz, double* tyz);
+void set_plane0(Engine& e, const double* plane, double* field);
+void divergence_finish(Engine& e, double* div, const double* fz, int w_nodes);
+
+// ---- RHS, pressure, time advance ---------------------------------------
+void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
+                  const double* Ug, const double* Vg, const double* Cx, const double* Cy,
+                  const double* Cz, const double* b, const double* dx, const double* dy,
+                  const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
+                  const double* vbar, double* Ru, double* Rv, double* Rw);
+void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
+                const double* THadv, const double* THbar, double* R);
+void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const cd* fbot,
+                 const cd* ftop, double* RCr, double* RCi, double* fRz_real);
+void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double* fRz_real,
+                  cd* fp);
+void subtract3(Engine& e, double* Ru, double* Rv, double* Rw, const double* a, const double* b,
+               const double* c);
+void ab2_uvw(Engine& e, const double* u, const double* v, const double* w, const double* Ru,
+             const double* Rup, const double* Rv, const double* Rvp, const double* Rw,
+             const double* Rwp, double* un, double* vn, double* wn);
+void ab2_th(Engine& e, const double* TH, const double* R, const double* Rp, double* out);
+void cfl_max(Engine& e, const double* u, const double* v, const double* w, double* out3);
+void copy_planes_z(Engine& e, const double* F, int k0, int k1, double* out2);
+void imfilter(Engine& e, const double* F, double* out);
+
+}  // namespace alfa

