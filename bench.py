@@ -1,0 +1,343 @@
+"""Throughput of the LES step on B200: grid-point-steps per second.
+
+Workload (default): the neutral ABL case at 256^3 (LASDD-SM dynamic SGS,
+3/2-rule dealiasing, Thomas pressure solve), FP64 -- the 256^3 LASDD-SM
+FP64 configuration of the reference's A100 benchmark table.  Synthetic
+seeded initial fields (log-law u with 0.5 % noise below 500 m); every field
+(134 MB) is larger than L2 (126 MB), so no L2 flush is needed between steps.
+
+  value  : device-timed whole steps (alfa_step, state resident in HBM),
+           CUDA events on the launching stream, max over ranks.
+  e2e    : the same steps through the reference-facing per-function API
+           (jax_alfa_b200.driver.MainLoop, the Main.py loop on the C-ABI),
+           with the initial state copied in from pinned host memory, the
+           forcing row going in and the CFL check coming out every step, and
+           the final state copied back, all inside the timed region.
+  --impl reference : the reference's CPU implementation of the same step
+           (the NumPy FP64 port of it, scipy.fft with every host thread) on a
+           bounded sample: one step of the same physics on a 128^3 grid.
+
+Multi-GPU: ``replicas only`` -- each rank advances its own independent
+simulation (no data-path collective); scaling is weak.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+A100_BASELINE = 93.4e6   # gp-steps/s, 256^3 LASDD-SM FP64 on A100 (reference notebook)
+METRIC = "LES grid-point-steps/s at 256^3"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="alfa", choices=["alfa", "reference"])
+    ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(grid, nsteps):
+    from jax_alfa_b200 import cases
+    cfg = cases.neutral(*grid, nsteps=nsteps)
+    cfg["case"] = "neutral"
+    return cfg
+
+
+def config_block(grid, world):
+    return {"workload": f"neutral ABL {grid[0]}x{grid[1]}x{grid[2]}, LASDD-SM dynamic SGS, "
+                        "3/2-rule dealiasing, Thomas pressure, AB2, FP64",
+            "grid": list(grid), "sgs": "LASDD-SM (optSgs=1, dynamic every step)",
+            "precision": "FP64 plain drop-in", "l2": "every field (8 B x N) exceeds L2; no flush",
+            "parallelism": f"replicas x{world} (no sharding)",
+            "baseline": "A100 JAX 256^3 LASDD-SM FP64, 93.4 M gp-steps/s"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.idx)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "dominant_kernel_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for ln in f:
+            if ln.startswith("{"):
+                return json.loads(ln)
+    return None
+
+
+def cpu_baseline(threads, grid=(128, 128, 128)):
+    """One step of the NumPy FP64 port of the reference on the host."""
+    from jax_alfa_b200 import cases
+    from oracle import alfa_oracle
+    from oracle.alfa_oracle import AlfaOracle, OracleRun
+    alfa_oracle.set_fft_workers(threads)
+    cfg = workload_config(grid, 2)
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    o = AlfaOracle(cfg)
+    r = OracleRun(cfg, u, v, w, th, adv=o.adv_series(*cases.adv_forcing_series(cfg)))
+    t = time.perf_counter()
+    with np.errstate(all="ignore"):
+        r.step()
+    dt = time.perf_counter() - t
+    n = grid[0] * grid[1] * grid[2]
+    return n / dt, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from jax_alfa_b200 import cases
+    from oracle import alfa_oracle
+    from oracle.alfa_oracle import AlfaOracle, OracleRun
+    alfa_oracle.set_fft_workers(threads)
+    grid = (128, 128, 128)
+    total = args.warmup + args.steps
+    cfg = workload_config(grid, total + 1)
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    o = AlfaOracle(cfg)
+    r = OracleRun(cfg, u, v, w, th, adv=o.adv_series(*cases.adv_forcing_series(cfg)))
+    with np.errstate(all="ignore"):
+        for _ in range(args.warmup):
+            r.step()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            r.step()
+        dt = time.perf_counter() - t
+    n = grid[0] * grid[1] * grid[2]
+    value = n * args.steps / dt
+    sample = (f"{args.steps} steps of the same physics on a 128^3 grid (1/8 of the 256^3 "
+              f"points), {dt / args.steps:.2f} s/step, NumPy FP64 port of the reference with "
+              f"scipy.fft on {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "gp-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / A100_BASELINE, "dtype": "f64", "data": "synthetic",
+        "config": config_block(args.grid, world),
+        "cpu_baseline": {"value": value, "unit": "gp-steps/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "gp-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_alfa(args, rank, world, dist):
+    import torch
+    from jax_alfa_b200 import _lib, cases
+    from jax_alfa_b200.api import Simulation
+    from jax_alfa_b200.driver import MainLoop
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    grid = tuple(args.grid)
+    n_gp = grid[0] * grid[1] * grid[2]
+    total = args.warmup + args.steps + 2
+    cfg = workload_config(grid, total)
+    u, v, w, th = cases.initial_fields(cfg, rank)
+    adv = cases.adv_forcing_series(cfg)
+    lib = _lib.load()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident whole step -----------------------------------
+    sim = Simulation(cfg, u, v, w, th, adv_series=adv)
+    sim.step(args.warmup)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    n0 = lib.alfa_launch_count()
+    e0.record(stream)
+    sim.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    n1 = lib.alfa_launch_count()
+    barrier()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    d = sim.diag()
+    if not np.isfinite(d["CFL"]):
+        raise RuntimeError("non-finite state in the timed run")
+    value = n_gp * args.steps * world / (ms / 1e3)
+
+    # ---- dominant kernel, live --------------------------------------------
+    import ctypes
+    roof = None
+    peak, peak_kind = measured_peaks()
+    t_ms, t_bytes = ctypes.c_double(), ctypes.c_double()
+    a = sim.alfa
+    a.lib.alfa_set_stream(a.ctx, ctypes.c_void_p(stream.cuda_stream))
+    if a.lib.alfa_time_kernel(a.ctx, 3, 20, ctypes.byref(t_ms), ctypes.byref(t_bytes)) == 0:
+        gbs = t_bytes.value / (t_ms.value * 1e-3) / 1e9
+        tr = ncu_traffic()
+        roof = {"kernel": "k_y_inv (half spectrum -> 3/2-padded real field, y pass)",
+                "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                "frac": gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                "alg_bytes_per_launch": t_bytes.value, "avg_launch_ms": t_ms.value,
+                "traffic": None if tr is None else tr.get("dram_bytes_per_launch")}
+    del sim
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the reference-facing API ------------------
+    e2e = None
+    if not args.no_e2e:
+        host = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in (u, v, w, th)]
+        ml_warm = MainLoop(cfg, u, v, w, th, adv_series=adv)
+        for _ in range(args.warmup):
+            ml_warm.step()
+        api = ml_warm.a
+        del ml_warm
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        ml = MainLoop(cfg, *[h.numpy() for h in host], adv_series=adv, api=api)
+        for _ in range(args.steps):
+            ml.step()
+        outs = [x.to("cpu", non_blocking=True) for x in (ml.u, ml.v, ml.w, ml.TH)]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        state_bytes = 4 * 8 * n_gp
+        e2e = {"value": n_gp * args.steps * world / (e2e_ms / 1e3), "unit": "gp-steps/s",
+               "h2d_bytes_per_step": (state_bytes + ml.h2d_bytes) / args.steps,
+               "d2h_bytes_per_step": (state_bytes + ml.d2h_bytes) / args.steps,
+               "path": "MainLoop: Main.py loop body on the per-function C-ABI, state in/out "
+                       "from pinned host memory inside the timed region",
+               "host_wall_ms": 1e3 * (time.perf_counter() - t0)}
+        del outs
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v1, dt1 = cpu_baseline(1)
+        cpu = {"value": v1, "unit": "gp-steps/s", "cores": 1, "kind": "port",
+               "sample": f"1 step of the same physics on 128^3 (1/8 of the points), "
+                         f"{dt1:.1f} s, NumPy FP64 port of the reference, 1 thread"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "gp-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": value / A100_BASELINE,
+            "dtype": "f64", "data": "synthetic", "config": config_block(grid, world),
+            "clocks": clk, "gpu_launches": int(n1 - n0), "roofline": roof,
+            "cpu_baseline": cpu, "e2e": e2e,
+        }), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl" if args.impl == "alfa" else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_alfa(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

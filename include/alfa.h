@@ -216,6 +216,12 @@ int alfa_AB2_uvw(alfa_ctx*, const double* u, const double* v, const double* w,
 int alfa_AB2_TH(alfa_ctx*, const double* TH, const double* RHS_TH,
                 const double* RHS_TH_previous, double* TH_new); /* SCL_TimeAdvancement.py:46 */
 
+/* Main.py:498-500 — RHS_i -= dp/dx_i, in place. */
+int alfa_AddPressureGradient(alfa_ctx*, double* RHS_u, double* RHS_v, double* RHS_w,
+                             const double* dpdx, const double* dpdy, const double* dpdz);
+/* Main.py:534-536 — cfl3 (device) = max|u| dt/dx, max|v| dt/dy, max|w| dt/dz. */
+int alfa_CFL(alfa_ctx*, const double* u, const double* v, const double* w, double* cfl3);
+
 /* ---- whole step: the loop body of src/Main.py:156-541 -------------------
  * State is held in the context.  init_state takes non-dimensional fields as
  * Main.py holds them after Initialize_uvw/TH (u without Ugal, TH - T_0).
@@ -229,6 +235,19 @@ int alfa_set_series(alfa_ctx*, const double* Uadv, const double* Vadv, const dou
 int alfa_step(alfa_ctx*, int nsteps);
 int alfa_get_state(alfa_ctx*, double* u, double* v, double* w, double* TH, double* p);
 int alfa_get_diag(alfa_ctx*, alfa_diag* out /* host; synchronises the stream */);
+
+/* Diagnostics with no reference counterpart: the number of kernels this
+ * library has launched in this process (all contexts, all streams). */
+unsigned long long alfa_launch_count(void);
+/* Times `reps` back-to-back launches of one building-block kernel on the
+ * context's stream with CUDA events (inputs: the context's state/workspace):
+ *   0 y-forward real->half spectrum, regular grid   (reads N, writes S)
+ *   1 x-column: forward FFT + two i*k outputs       (reads S, writes 2 S)
+ *   2 y-inverse half spectrum->real, regular grid   (reads S, writes N)
+ *   3 y-inverse onto the 3/2-padded grid            (reads mx*nyh*nz, writes P)
+ * ms = average duration of one launch; bytes = its algorithmic HBM bytes. */
+int alfa_time_kernel(alfa_ctx*, int which, int reps, double* ms /* host */,
+                     double* bytes /* host */);
 
 #ifdef __cplusplus
 }

@@ -101,6 +101,8 @@ SIGNATURES = {
     "alfa_ThomasPressureSolve": [P] * 7,
     "alfa_AB2_uvw": [P] * 12,
     "alfa_AB2_TH": [P] * 4,
+    "alfa_AddPressureGradient": [P] * 6,
+    "alfa_CFL": [P] * 4,
     "alfa_init_state": [P] * 4,
     "alfa_set_series": [c_double_p, c_double_p, c_double_p, c_double_p, I],
     "alfa_step": [I],
@@ -137,6 +139,10 @@ def load():
     lib.alfa_workspace_bytes.restype = ctypes.c_size_t
     lib.alfa_get_diag.argtypes = [CTX, ctypes.POINTER(AlfaDiag)]
     lib.alfa_get_diag.restype = I
+    lib.alfa_launch_count.argtypes = []
+    lib.alfa_launch_count.restype = ctypes.c_ulonglong
+    lib.alfa_time_kernel.argtypes = [CTX, I, I, c_double_p, c_double_p]
+    lib.alfa_time_kernel.restype = I
     for name, args in SIGNATURES.items():
         f = getattr(lib, name)
         f.argtypes = [CTX] + args

@@ -392,6 +392,19 @@ class Alfa:
                    self._p(fRz_real, self.S), *[self._p(x) for x in out])
         return tuple(out)
 
+    def AddPressureGradient(self, RHS_u, RHS_v, RHS_w, dpdx, dpdy, dpdz):
+        """Main.py:498-500 (RHS_i - dp/dx_i), returning new tensors."""
+        out = [x.clone() for x in (RHS_u, RHS_v, RHS_w)]
+        self._call("alfa_AddPressureGradient", *[self._p(x) for x in out], self._f(dpdx),
+                   self._f(dpdy), self._f(dpdz))
+        return tuple(out)
+
+    def CFL(self, u, v, w):
+        """Main.py:534-537: (CFLx, CFLy, CFLz) on the device."""
+        out = self._new((3,))
+        self._call("alfa_CFL", self._f(u), self._f(v), self._f(w), self._p(out))
+        return out
+
     def AB2_uvw(self, u, v, w, RHS_u, RHS_u_previous, RHS_v, RHS_v_previous, RHS_w,
                 RHS_w_previous):
         out = [self._new(self.N) for _ in range(3)]

@@ -12,7 +12,12 @@
 
 using namespace alfa;
 
+#include <atomic>
+
 namespace alfa {
+
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------------------
 // Workspace: named field slots carved from one allocation
@@ -545,7 +550,7 @@ static int dynamic_sgs(alfa_ctx* c, const double* const g[9], const double* u, c
     lasdd_poly(e, sums, 0, co);
     compute_beta(e, co, e.nz, beta1);
   } else {
-    k_ones_ext<<<1, 256, 0, e.stream>>>(beta1, e.nz);  // LAD: beta = 1 (:321-325)
+    ::alfa::note_launch(); k_ones_ext<<<1, 256, 0, e.stream>>>(beta1, e.nz);  // LAD: beta = 1 (:321-325)
   }
   lasdd_LM_MM(e, f, beta1, W.LM, W.MM);
   clip_ratio(e, W.LM, W.MM, Cs2);
@@ -632,7 +637,7 @@ static int dynamic_sgs_scalar(alfa_ctx* c, const double* const m15[15], const do
     lasdd_poly(e, sums, 1, co);
     compute_beta(e, co, e.nz, beta2);
   } else {
-    k_ones_ext<<<1, 256, 0, e.stream>>>(beta2, e.nz);
+    ::alfa::note_launch(); k_ones_ext<<<1, 256, 0, e.stream>>>(beta2, e.nz);
   }
   scalar_Tup_Tdn(e, f, beta2, W.LM, W.MM);
   clip_ratio(e, W.LM, W.MM, r3);
@@ -1254,6 +1259,94 @@ int alfa_AB2_uvw(alfa_ctx* c, const double* u, const double* v, const double* w,
   return check_launch(c->e, "AB2_uvw");
 }
 
+int alfa_AddPressureGradient(alfa_ctx* c, double* Ru, double* Rv, double* Rw, const double* dpdx,
+                             const double* dpdy, const double* dpdz) {
+  CTX_CHECK(c);
+  NN(Ru); NN(Rv); NN(Rw); NN(dpdx); NN(dpdy); NN(dpdz);
+  subtract3(c->e, Ru, Rv, Rw, dpdx, dpdy, dpdz);
+  return check_launch(c->e, "AddPressureGradient");
+}
+
+__global__ void k_cfl3(const double* __restrict__ m, double* out, double dt, double dx, double dy,
+                       double dz) {
+  if (threadIdx.x == 0) {
+    out[0] = m[0] * dt / dx;
+    out[1] = m[1] * dt / dy;
+    out[2] = m[2] * dt / dz;
+  }
+}
+
+int alfa_CFL(alfa_ctx* c, const double* u, const double* v, const double* w, double* cfl3) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(cfl3);
+  Engine& e = c->e;
+  cfl_max(e, u, v, w, c->w.d_cfl);
+  // Main.py:534-536: max|.| * dt_nondim / dx
+  ::alfa::note_launch();
+  k_cfl3<<<1, 32, 0, e.stream>>>(c->w.d_cfl, cfl3, e.dt_nondim, e.dx, e.dy, e.dz);
+  return check_launch(e, "CFL");
+}
+
+unsigned long long alfa_launch_count(void) { return g_launches.load(); }
+
+int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes) {
+  CTX_CHECK(c);
+  if (!ms || !bytes || reps < 1 || which < 0 || which > 3)
+    return c->e.fail("time_kernel: bad arguments", ALFA_E_SHAPE);
+  Engine& e = c->e;
+  Work& W = c->w;
+  const double S16 = 16.0 * e.nx * e.nyh * e.nz, N8 = 8.0 * e.N();
+  // inputs for the inverse kernels: one forward + x pass
+  launch_y_fwd(e, ld_field(e, W.u), e.nx, e.pny, e.nyh, e.T[0]);
+  XOut o[2];
+  for (int i = 0; i < 2; i++) {
+    o[i] = XOut{};
+    o[i].kind = XO_INV;
+    o[i].map = i == 0 ? MAP_DX : MAP_DY;
+    o[i].K = e.nyh;
+    o[i].rows = e.nx;
+    o[i].dst = e.T[1 + i];
+    o[i].inv = e.pnx;
+  }
+  launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh);
+  XOut op = XOut{};
+  op.kind = XO_INV;
+  op.map = MAP_PAD;
+  op.K = e.nyh;
+  op.rows = e.mx;
+  op.dst = e.T[3];
+  op.inv = e.pmx;
+  launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 1, &op, e.nyh);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  auto run = [&]() {
+    switch (which) {
+      case 0: launch_y_fwd(e, ld_field(e, W.u), e.nx, e.pny, e.nyh, e.T[0]); break;
+      case 1: launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh); break;
+      case 2: launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, 1.0, e.W, 0); break;
+      default: launch_y_inv(e, e.T[3], e.mx, e.nyh, e.pmy, 1.0, W.Pb[0], 0); break;
+    }
+  };
+  run();  // warm
+  cudaEventRecord(a, e.stream);
+  for (int r = 0; r < reps; r++) run();
+  cudaEventRecord(b, e.stream);
+  cudaEventSynchronize(b);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = (double)t / reps;
+  switch (which) {
+    case 0: *bytes = N8 + S16; break;
+    case 1: *bytes = S16 + 2 * S16; break;
+    case 2: *bytes = S16 + N8; break;
+    default: *bytes = 16.0 * e.mx * e.nyh * e.nz + 8.0 * e.P(); break;
+  }
+  return check_launch(e, "time_kernel");
+}
+
 int alfa_AB2_TH(alfa_ctx* c, const double* TH, const double* R, const double* Rp, double* out) {
   CTX_CHECK(c);
   NN(TH); NN(R); NN(Rp); NN(out);
@@ -1285,13 +1378,16 @@ int alfa_init_state(alfa_ctx* c, const double* u, const double* v, const double*
     cudaMemsetAsync(W.RHS[i], 0, N * 8, e.stream);
     cudaMemsetAsync(W.RHSp[i], 0, N * 8, e.stream);
   }
-  for (int i = 0; i < 6; i++) k_fill_n<<<64, 256, 0, e.stream>>>(W.most[i], i >= 4 ? 1.0 : 0.0, H);
-  k_fill_n<<<64, 256, 0, e.stream>>>(W.qz_plane, e.qz_sfc_const, H);
-  k_fill_n<<<256, 256, 0, e.stream>>>(W.Cs2, e.Cs2_init, N);
-  k_fill_n<<<256, 256, 0, e.stream>>>(W.Cs2Pr, e.Cs2PrRatio_init, N);
-  k_fill<<<1, 256, 0, e.stream>>>(W.Ug, e.cfg.Ug2 / 1.0, e.nz);
-  k_fill<<<1, 256, 0, e.stream>>>(W.Vg, e.cfg.Vg2 / 1.0, e.nz);
-  k_fill<<<1, 256, 0, e.stream>>>(W.zero_prof, 0.0, e.nz);
+  for (int i = 0; i < 6; i++) {
+    ::alfa::note_launch();
+    k_fill_n<<<64, 256, 0, e.stream>>>(W.most[i], i >= 4 ? 1.0 : 0.0, H);
+  }
+  ::alfa::note_launch(); k_fill_n<<<64, 256, 0, e.stream>>>(W.qz_plane, e.qz_sfc_const, H);
+  ::alfa::note_launch(); k_fill_n<<<256, 256, 0, e.stream>>>(W.Cs2, e.Cs2_init, N);
+  ::alfa::note_launch(); k_fill_n<<<256, 256, 0, e.stream>>>(W.Cs2Pr, e.Cs2PrRatio_init, N);
+  ::alfa::note_launch(); k_fill<<<1, 256, 0, e.stream>>>(W.Ug, e.cfg.Ug2 / 1.0, e.nz);
+  ::alfa::note_launch(); k_fill<<<1, 256, 0, e.stream>>>(W.Vg, e.cfg.Vg2 / 1.0, e.nz);
+  ::alfa::note_launch(); k_fill<<<1, 256, 0, e.stream>>>(W.zero_prof, 0.0, e.nz);
   W.iteration = e.cfg.istep;
   W.have_state = 1;
   W.CFLmax = 0;

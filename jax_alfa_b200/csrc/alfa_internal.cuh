@@ -10,6 +10,10 @@
 
 namespace alfa {
 
+// Process-wide count of kernel launches made by this library (every launch
+// site calls note_launch(); read through alfa_launch_count()).
+void note_launch();
+
 // ---------------------------------------------------------------------------
 // Physical-space value producers for the y-forward FFT stage.  Instead of
 // materialising a product or a staggered combination as a full field and

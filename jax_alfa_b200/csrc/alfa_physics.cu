@@ -61,8 +61,8 @@ void plane_sums(Engine& e, const double* const* fields, int nq, double* sums) {
   a.nq = nq;
   for (int q = 0; q < nq; q++) a.f[q] = fields[q];
   const int nb = red_blocks(e);
-  k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
-  k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(e.red, nb, nq, e.nz, 1.0,
+  ::alfa::note_launch(); k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(e.red, nb, nq, e.nz, 1.0,
                                                                        sums);
 }
 
@@ -71,8 +71,8 @@ void plane_means(Engine& e, const double* const* fields, int nq, double* means) 
   a.nq = nq;
   for (int q = 0; q < nq; q++) a.f[q] = fields[q];
   const int nb = red_blocks(e);
-  k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
-  k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(
+  ::alfa::note_launch(); k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(
       e.red, nb, nq, e.nz, 1.0 / (double)e.H(), means);
 }
 
@@ -241,7 +241,7 @@ int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io) {
   p.q2 = io.q2;
   p.qavg = io.qavg;
   p.invOB = io.invOB;
-  k_surface<<<1, 1024, 0, e.stream>>>(c, p);
+  ::alfa::note_launch(); k_surface<<<1, 1024, 0, e.stream>>>(c, p);
   return 0;
 }
 
@@ -273,7 +273,7 @@ __global__ void k_derivz_M(const double* __restrict__ u, const double* __restric
 
 void derivz_M(Engine& e, const double* u, const double* v, const double* w, const double* ustar,
               const double* M, const double* fi_m, double* dudz, double* dvdz, double* dwdz) {
-  k_derivz_M<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, v, w, ustar, M, fi_m, dudz, dvdz, dwdz,
+  ::alfa::note_launch(); k_derivz_M<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, v, w, ustar, M, fi_m, dudz, dvdz, dwdz,
                                                     e.N(), e.nz, e.idz, e.cfg.Ugal, e.dz);
 }
 
@@ -293,7 +293,7 @@ __global__ void k_derivz_TH(const double* __restrict__ T, const double* __restri
 
 void derivz_TH(Engine& e, const double* TH, const double* ustar, const double* qz,
                const double* fi_h, double* dTHdz) {
-  k_derivz_TH<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, ustar, qz, fi_h, dTHdz, e.N(), e.nz,
+  ::alfa::note_launch(); k_derivz_TH<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, ustar, qz, fi_h, dTHdz, e.N(), e.nz,
                                                      e.idz, 0.4 * 0.5 * e.dz);
 }
 
@@ -309,7 +309,7 @@ __global__ void k_derivz_generic(const double* __restrict__ F, double* out, size
 }
 
 void derivz_generic(Engine& e, const double* F, int w_nodes, double* out) {
-  k_derivz_generic<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nz, w_nodes, e.idz);
+  ::alfa::note_launch(); k_derivz_generic<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nz, w_nodes, e.idz);
 }
 
 __global__ void k_div_finish(double* div, const double* __restrict__ f, size_t n, int nz, int w,
@@ -318,7 +318,7 @@ __global__ void k_div_finish(double* div, const double* __restrict__ f, size_t n
 }
 
 void divergence_finish(Engine& e, double* div, const double* fz, int w_nodes) {
-  k_div_finish<<<nblocks(e.N()), TPB, 0, e.stream>>>(div, fz, e.N(), e.nz, w_nodes, e.idz);
+  ::alfa::note_launch(); k_div_finish<<<nblocks(e.N()), TPB, 0, e.stream>>>(div, fz, e.N(), e.nz, w_nodes, e.idz);
 }
 
 // ---------------------------------------------------------------------------
@@ -347,10 +347,10 @@ __global__ void k_add_const(const double* __restrict__ a, double c, double* out,
 void buoyancy(Engine& e, const double* TH, int opt, double* out) {
   // THv = (TH + T_0)(1 + 0.61 H), H = 0; its plane mean
   double* thv = e.W;  // first workspace field
-  k_add_const<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.T0_nondim, thv, e.N());
+  ::alfa::note_launch(); k_add_const<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.T0_nondim, thv, e.N());
   const double* f[1] = {thv};
   plane_means(e, f, 1, e.scal);
-  k_buoy<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.scal, out, e.N(), e.nz, e.T0_nondim, opt,
+  ::alfa::note_launch(); k_buoy<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.scal, out, e.N(), e.nz, e.T0_nondim, opt,
                                                 0.5 * e.g_nondim);
 }
 
@@ -405,7 +405,7 @@ void strains_uvp(Engine& e, const double* const g[9], double* S12, double* S13, 
                  double* S) {
   G9 G;
   for (int i = 0; i < 9; i++) G.g[i] = g[i];
-  k_strains_uvp<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, S12, S13, S23, S, e.N(), e.nz);
+  ::alfa::note_launch(); k_strains_uvp<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, S12, S13, S23, S, e.N(), e.nz);
 }
 
 __global__ void k_smag_w(G9 G, double* Sw, size_t n, int nz) {
@@ -430,7 +430,7 @@ __global__ void k_smag_w(G9 G, double* Sw, size_t n, int nz) {
 void smag_w(Engine& e, const double* const g[9], double* Sw) {
   G9 G;
   for (int i = 0; i < 9; i++) G.g[i] = g[i];
-  k_smag_w<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, Sw, e.N(), e.nz);
+  ::alfa::note_launch(); k_smag_w<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, Sw, e.N(), e.nz);
 }
 
 struct P6 {
@@ -446,7 +446,7 @@ __global__ void k_smag6(P6 P, double* out, size_t n) {
 void smag6(Engine& e, const double* const s[6], size_t n, double* out) {
   P6 P;
   for (int i = 0; i < 6; i++) P.s[i] = s[i];
-  k_smag6<<<nblocks(n), TPB, 0, e.stream>>>(P, out, n);
+  ::alfa::note_launch(); k_smag6<<<nblocks(n), TPB, 0, e.stream>>>(P, out, n);
 }
 
 void smag6_n(Engine& e, const double* const s[6], double* out) { smag6(e, s, e.N(), out); }
@@ -462,7 +462,7 @@ __global__ void k_wstar(const double* __restrict__ w, double* out, size_t n, int
 }
 
 void wstar(Engine& e, const double* w, double* w_) {
-  k_wstar<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, w_, e.N(), e.nz);
+  ::alfa::note_launch(); k_wstar<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, w_, e.N(), e.nz);
 }
 
 // ---------------------------------------------------------------------------
@@ -544,8 +544,8 @@ static LasddConst lasdd_const(const Engine& e) {
 
 void lasdd_sums(Engine& e, const LasddFields& f, double* sums10) {
   const int nb = red_blocks(e);
-  k_lasdd_partial<<<nb, 128, 0, e.stream>>>(f, lasdd_const(e), e.H(), e.nz, e.red);
-  k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
+  ::alfa::note_launch(); k_lasdd_partial<<<nb, 128, 0, e.stream>>>(f, lasdd_const(e), e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
                                                                        1.0 / (double)e.H(), sums10);
 }
 
@@ -583,7 +583,7 @@ __global__ void k_poly(const double* __restrict__ m, int nz, int scalar, double*
 }
 
 void lasdd_poly(Engine& e, const double* sums10, int scalar, double* coeffs6) {
-  k_poly<<<1, 256, 0, e.stream>>>(sums10, e.nz, scalar, coeffs6);
+  ::alfa::note_launch(); k_poly<<<1, 256, 0, e.stream>>>(sums10, e.nz, scalar, coeffs6);
 }
 
 // ---------------------------------------------------------------------------
@@ -669,7 +669,7 @@ __global__ void k_beta(const double* __restrict__ co, int nlev, double* beta) {
 }
 
 void compute_beta(Engine& e, const double* coeffs6, int nlev, double* beta) {
-  k_beta<<<(nlev + 31) / 32, 256, 0, e.stream>>>(coeffs6, nlev, beta);
+  ::alfa::note_launch(); k_beta<<<(nlev + 31) / 32, 256, 0, e.stream>>>(coeffs6, nlev, beta);
 }
 
 __global__ void k_ones(double* p, int n) {
@@ -693,7 +693,7 @@ __global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ 
 }
 
 void lasdd_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM) {
-  k_LM_MM<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, lasdd_const(e), beta, LM, MM, e.N(), e.nz);
+  ::alfa::note_launch(); k_LM_MM<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, lasdd_const(e), beta, LM, MM, e.N(), e.nz);
 }
 
 // 3x3 periodic box mean (Utilities.py:87-115) at (x, y, z)
@@ -726,7 +726,7 @@ __global__ void k_clip_ratio(const double* __restrict__ num, const double* __res
 }
 
 void clip_ratio(Engine& e, const double* num, const double* den, double* out) {
-  k_clip_ratio<<<nblocks(e.N()), TPB, 0, e.stream>>>(num, den, out, e.N(), e.nx, e.ny, e.nz);
+  ::alfa::note_launch(); k_clip_ratio<<<nblocks(e.N()), TPB, 0, e.stream>>>(num, den, out, e.N(), e.nx, e.ny, e.nz);
 }
 
 __global__ void k_imfilter(const double* __restrict__ F, double* out, size_t n, int nx, int ny,
@@ -739,7 +739,7 @@ __global__ void k_imfilter(const double* __restrict__ F, double* out, size_t n, 
 }
 
 void imfilter(Engine& e, const double* F, double* out) {
-  k_imfilter<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nx, e.ny, e.nz);
+  ::alfa::note_launch(); k_imfilter<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nx, e.ny, e.nz);
 }
 
 __global__ void k_cs2_partial(const double* __restrict__ C, size_t H, int nz, double* part) {
@@ -768,11 +768,11 @@ __global__ void k_cs2_finish(const double* __restrict__ m, int nz, double* avg1,
 
 void cs2_profiles(Engine& e, const double* Cs2, double* avg1, double* avg2) {
   const int nb = red_blocks(e);
-  k_cs2_partial<<<nb, 128, 0, e.stream>>>(Cs2, e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_cs2_partial<<<nb, 128, 0, e.stream>>>(Cs2, e.H(), e.nz, e.red);
   double* m = e.scal + 64;
-  k_partial_finish<<<nblocks((size_t)2 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 2, e.nz,
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)2 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 2, e.nz,
                                                                       1.0 / (double)e.H(), m);
-  k_cs2_finish<<<1, 256, 0, e.stream>>>(m, e.nz, avg1, avg2);
+  ::alfa::note_launch(); k_cs2_finish<<<1, 256, 0, e.stream>>>(m, e.nz, avg1, avg2);
 }
 
 // ---------------------------------------------------------------------------
@@ -849,8 +849,8 @@ __global__ void k_sl_partial(ScalarLasddFields f, SLConst c, size_t H, int nz, d
 
 void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10) {
   const int nb = red_blocks(e);
-  k_sl_partial<<<nb, 128, 0, e.stream>>>(f, sl_const(e), e.H(), e.nz, e.red);
-  k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
+  ::alfa::note_launch(); k_sl_partial<<<nb, 128, 0, e.stream>>>(f, sl_const(e), e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
                                                                        1.0 / (double)e.H(), sums10);
 }
 
@@ -867,7 +867,7 @@ __global__ void k_sl_TupTdn(ScalarLasddFields f, SLConst c, const double* __rest
 
 void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
                     double* Tdn) {
-  k_sl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, sl_const(e), beta, Tup, Tdn, e.N(), e.nz);
+  ::alfa::note_launch(); k_sl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, sl_const(e), beta, Tup, Tdn, e.N(), e.nz);
 }
 
 // ---------------------------------------------------------------------------
@@ -889,7 +889,7 @@ __global__ void k_wall(const double* __restrict__ u, const double* __restrict__ 
 void wall_override(Engine& e, const double* u, const double* v, const double* M,
                    const double* psi_m, const double* psi_m0, double* txz, double* tyz) {
   const double log_m = std::log(0.5 * e.dz * e.z_scale / e.cfg.z0m);
-  k_wall<<<nblocks(e.H()), TPB, 0, e.stream>>>(u, v, M, psi_m, psi_m0, txz, tyz, e.H(), e.nz,
+  ::alfa::note_launch(); k_wall<<<nblocks(e.H()), TPB, 0, e.stream>>>(u, v, M, psi_m, psi_m0, txz, tyz, e.H(), e.nz,
                                                 log_m, e.cfg.Ugal);
 }
 
@@ -898,7 +898,7 @@ __global__ void k_set_plane0(const double* __restrict__ p, double* f, size_t H, 
 }
 
 void set_plane0(Engine& e, const double* plane, double* field) {
-  k_set_plane0<<<nblocks(e.H()), TPB, 0, e.stream>>>(plane, field, e.H(), e.nz);
+  ::alfa::note_launch(); k_set_plane0<<<nblocks(e.H()), TPB, 0, e.stream>>>(plane, field, e.H(), e.nz);
 }
 
 // ---------------------------------------------------------------------------
@@ -940,7 +940,7 @@ void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
                   const double* vbar, double* Ru, double* Rv, double* Rw) {
   RhsM a{u, v, w, Ug, Vg, Cx, Cy, Cz, b, dx, dy, dz, Uadv, Vadv, ubar, vbar, e.d_rd, e.d_rd_stag,
          Ru, Rv, Rw, e.f_nondim, e.cfg.Ugal, e.cfg.optAdvection >= 1, e.cfg.optDamping == 1};
-  k_rhs_m<<<nblocks(e.N()), TPB, 0, e.stream>>>(a, e.N(), e.nz);
+  ::alfa::note_launch(); k_rhs_m<<<nblocks(e.N()), TPB, 0, e.stream>>>(a, e.N(), e.nz);
 }
 
 __global__ void k_rhs_s(const double* __restrict__ TH, const double* __restrict__ adv,
@@ -958,7 +958,7 @@ __global__ void k_rhs_s(const double* __restrict__ TH, const double* __restrict_
 
 void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
                 const double* THadv, const double* THbar, double* R) {
-  k_rhs_s<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, adv, divq, THadv, THbar, e.d_rd_stag, R,
+  ::alfa::note_launch(); k_rhs_s<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, adv, divq, THadv, THbar, e.d_rd_stag, R,
                                                  e.N(), e.nz, e.cfg.optAdvection >= 1,
                                                  e.cfg.optDamping == 1);
 }
@@ -1000,7 +1000,7 @@ __global__ void k_rc(const cd* __restrict__ fRx, const cd* __restrict__ fRy,
 
 void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const cd* fb2,
                  const cd* /*unused*/, double* RCr, double* RCi, double* fRz_real) {
-  k_rc<<<nblocks((size_t)e.nx * e.nyh * (e.nz + 1)), TPB, 0, e.stream>>>(
+  ::alfa::note_launch(); k_rc<<<nblocks((size_t)e.nx * e.nyh * (e.nz + 1)), TPB, 0, e.stream>>>(
       fRx, fRy, fRz, fb2, e.d_kr, RCr, RCi, fRz_real, e.nx, e.nyh, e.nz, e.dz);
 }
 
@@ -1054,7 +1054,7 @@ __global__ void k_thomas(const double* __restrict__ RCr, const double* __restric
 
 void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double* fRz_real, cd* fp) {
   const size_t nm = (size_t)e.nx * e.nyh;
-  k_thomas<<<(int)((nm + 127) / 128), 128, 0, e.stream>>>(RCr, RCi, fRz_real, e.d_b_thomas,
+  ::alfa::note_launch(); k_thomas<<<(int)((nm + 127) / 128), 128, 0, e.stream>>>(RCr, RCi, fRz_real, e.d_b_thomas,
                                                           e.d_m_thomas, e.d_c_p, fp, e.nx, e.nyh,
                                                           e.nz, e.dz);
 }
@@ -1070,7 +1070,7 @@ __global__ void k_sub3(double* a, double* b, double* c, const double* __restrict
 
 void subtract3(Engine& e, double* Ru, double* Rv, double* Rw, const double* a, const double* b,
                const double* c) {
-  k_sub3<<<nblocks(e.N()), TPB, 0, e.stream>>>(Ru, Rv, Rw, a, b, c, e.N());
+  ::alfa::note_launch(); k_sub3<<<nblocks(e.N()), TPB, 0, e.stream>>>(Ru, Rv, Rw, a, b, c, e.N());
 }
 
 // ---------------------------------------------------------------------------
@@ -1097,13 +1097,13 @@ __global__ void k_ab2(const double* u, const double* __restrict__ R, const doubl
 void ab2_uvw(Engine& e, const double* u, const double* v, const double* w, const double* Ru,
              const double* Rup, const double* Rv, const double* Rvp, const double* Rw,
              const double* Rwp, double* un, double* vn, double* wn) {
-  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, Ru, Rup, un, e.N(), e.nz, e.dt_nondim, 0, 0.0);
-  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(v, Rv, Rvp, vn, e.N(), e.nz, e.dt_nondim, 0, 0.0);
-  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, Rw, Rwp, wn, e.N(), e.nz, e.dt_nondim, 1, 0.0);
+  ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, Ru, Rup, un, e.N(), e.nz, e.dt_nondim, 0, 0.0);
+  ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(v, Rv, Rvp, vn, e.N(), e.nz, e.dt_nondim, 0, 0.0);
+  ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, Rw, Rwp, wn, e.N(), e.nz, e.dt_nondim, 1, 0.0);
 }
 
 void ab2_th(Engine& e, const double* TH, const double* R, const double* Rp, double* out) {
-  k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
+  ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
                                                e.inversion_nondim * e.dz);
 }
 
@@ -1140,8 +1140,8 @@ __global__ void k_absmax_finish(const double* part, int nb, double* out) {
 
 void cfl_max(Engine& e, const double* u, const double* v, const double* w, double* out3) {
   const int nb = 256;
-  k_absmax_partial<<<nb, 256, 0, e.stream>>>(u, v, w, e.N(), e.red);
-  k_absmax_finish<<<1, 32, 0, e.stream>>>(e.red, nb, out3);
+  ::alfa::note_launch(); k_absmax_partial<<<nb, 256, 0, e.stream>>>(u, v, w, e.N(), e.red);
+  ::alfa::note_launch(); k_absmax_finish<<<1, 32, 0, e.stream>>>(e.red, nb, out3);
 }
 
 // copy z-planes k0 and k1 of F into a (nx, ny, 2) field
@@ -1154,7 +1154,7 @@ __global__ void k_planes(const double* __restrict__ F, int k0, int k1, double* o
 }
 
 void copy_planes_z(Engine& e, const double* F, int k0, int k1, double* out2) {
-  k_planes<<<nblocks(e.H()), TPB, 0, e.stream>>>(F, k0, k1, out2, e.H(), e.nz);
+  ::alfa::note_launch(); k_planes<<<nblocks(e.H()), TPB, 0, e.stream>>>(F, k0, k1, out2, e.H(), e.nz);
 }
 
 }  // namespace alfa

@@ -301,7 +301,7 @@ void launch_y_fwd(Engine& e, const Loader& L, int rows, const FftPlan& p, int K,
   const size_t smem = 2 * (size_t)p.n * YC * sizeof(cd);
   set_smem((const void*)k_y_fwd, smem);
   dim3 g((L.nz + 2 * YC - 1) / (2 * YC), rows);
-  k_y_fwd<<<g, YTHREADS, smem, e.stream>>>(L, p, K, T);
+  ::alfa::note_launch(); k_y_fwd<<<g, YTHREADS, smem, e.stream>>>(L, p, K, T);
 }
 
 void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
@@ -309,7 +309,7 @@ void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, dou
   const size_t smem = 2 * (size_t)p.n * YC * sizeof(cd);
   set_smem((const void*)k_y_inv, smem);
   dim3 g((e.nz + 2 * YC - 1) / (2 * YC), rows);
-  k_y_inv<<<g, YTHREADS, smem, e.stream>>>(T, K, p, e.nz, scale, out, accumulate);
+  ::alfa::note_launch(); k_y_inv<<<g, YTHREADS, smem, e.stream>>>(T, K, p, e.nz, scale, out, accumulate);
 }
 
 void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const FftPlan& fwd,
@@ -336,7 +336,7 @@ void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const
   const size_t smem = 3 * (size_t)maxrows * a.C * sizeof(cd);
   set_smem((const void*)k_x, smem);
   dim3 g((e.nz + a.C - 1) / a.C, Kgrid);
-  k_x<<<g, XTHREADS, smem, e.stream>>>(a);
+  ::alfa::note_launch(); k_x<<<g, XTHREADS, smem, e.stream>>>(a);
 }
 
 // ---------------------------------------------------------------------------

@@ -26,6 +26,30 @@ import math
 import numpy as np
 
 PI = math.pi          # src/config/DerivedVars.py:39
+
+_FFT_WORKERS = None
+
+
+def set_fft_workers(n):
+    """Route the transforms through scipy.fft with ``n`` threads (used only to
+    time the CPU baseline; None restores NumPy's single-threaded pocketfft,
+    with which the golden vectors were recorded)."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = n
+
+
+def _rfft2(F):
+    if _FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.rfft2(F, axes=(0, 1), workers=_FFT_WORKERS)
+    return np.fft.rfft2(F, axes=(0, 1))
+
+
+def _irfft2(F, shape):
+    if _FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.irfft2(F, axes=(0, 1), s=shape, workers=_FFT_WORKERS)
+    return np.fft.irfft2(F, axes=(0, 1), s=shape)
 G = 9.81              # src/config/DerivedVars.py:40
 VONK = 0.4            # src/config/DerivedVars.py:41
 
@@ -101,12 +125,12 @@ class AlfaOracle:
     # ------------------------------------------------------------------
     @staticmethod
     def FFT(F):
-        return np.fft.rfft2(F, axes=(0, 1))
+        return _rfft2(F)
 
     FFT_pad = FFT
 
     def _irfft2(self, F, shape):
-        return np.fft.irfft2(F, axes=(0, 1), s=shape)
+        return _irfft2(F, shape)
 
     # ------------------------------------------------------------------
     # src/operations/Dealiasing.py:51-114.  Dealias1 copies the x-Nyquist
@@ -1026,8 +1050,8 @@ class AlfaOracle:
         fRx, fRy, fRz = self.FFT(Rx), self.FFT(Ry), self.FFT(Rz)
         RCr = np.zeros((nx, nyr, nz + 1))
         RCi = np.zeros((nx, nyr, nz + 1))
-        fb = np.fft.rfft2(divtz[:, :, 0], axes=(0, 1))
-        ft = np.fft.rfft2(divtz[:, :, -1], axes=(0, 1))
+        fb = _rfft2(divtz[:, :, 0])
+        ft = _rfft2(divtz[:, :, -1])
         RCr[:, :, 0] = -dz * fb.real
         RCi[:, :, 0] = -dz * fb.imag
         RCr[:, :, nz] = -dz * ft.real

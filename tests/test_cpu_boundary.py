@@ -20,7 +20,8 @@ def test_signature_table_covers_header():
     declared = set(_lib.exported_symbols())
     bound = set(_lib.SIGNATURES) | {"alfa_create", "alfa_destroy", "alfa_last_error",
                                     "alfa_set_stream", "alfa_get_derived",
-                                    "alfa_workspace_bytes", "alfa_get_diag"}
+                                    "alfa_workspace_bytes", "alfa_get_diag",
+                                    "alfa_launch_count", "alfa_time_kernel"}
     assert declared <= bound, declared - bound
 
 
