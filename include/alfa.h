@@ -36,6 +36,7 @@ extern "C" {
 #define ALFA_E_NUMERIC (-4)  /* non-finite state detected                  */
 #define ALFA_E_TIMEOUT (-5)  /* a bounded device wait gave up              */
 #define ALFA_E_STATE (-6)    /* call order (e.g. step before init_state)   */
+#define ALFA_E_NOALLOC_LIMIT (-7) /* size above a no-allocation entry's limit */
 
 typedef struct alfa_ctx alfa_ctx;
 
@@ -235,6 +236,23 @@ int alfa_set_series(alfa_ctx*, const double* Uadv, const double* Vadv, const dou
 int alfa_step(alfa_ctx*, int nsteps);
 int alfa_get_state(alfa_ctx*, double* u, double* v, double* w, double* TH, double* p);
 int alfa_get_diag(alfa_ctx*, alfa_diag* out /* host; synchronises the stream */);
+
+/* No counterpart in the reference.  alfa_PlanarMean without a context and
+ * without any device allocation, for callers that may not allocate: code
+ * running inside another runtime's memory management, such as a JAX/XLA
+ * custom call (XLA reserves most of the GPU for its own allocator and gives
+ * the call only its buffers) or an application with a fixed device-memory
+ * budget.  F is (nx, ny, nz) z-fastest, mean_nz receives the nz plane means;
+ * both are the caller's device buffers; the work runs on cuda_stream.
+ * Limit: nz <= 2048 (larger returns ALFA_E_NOALLOC_LIMIT before any launch).
+ * The partial sums live in a fixed 4 MiB array inside the library, one per
+ * device that loads it, kept until the process exits.  The first call on each
+ * device looks that array's address up (with the device current); make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls that overlap on the GPU (different streams, no ordering)
+ * race and must be serialised by the caller. */
+int alfa_PlanarMean_noalloc(const double* F, int nx, int ny, int nz, double* mean_nz,
+                            void* cuda_stream);
 
 /* Diagnostics with no reference counterpart: the number of kernels this
  * library has launched in this process (all contexts, all streams). */

@@ -143,6 +143,8 @@ def load():
     lib.alfa_launch_count.restype = ctypes.c_ulonglong
     lib.alfa_time_kernel.argtypes = [CTX, I, I, c_double_p, c_double_p]
     lib.alfa_time_kernel.restype = I
+    lib.alfa_PlanarMean_noalloc.argtypes = [P, I, I, I, P, c_void_p]
+    lib.alfa_PlanarMean_noalloc.restype = I
     for name, args in SIGNATURES.items():
         f = getattr(lib, name)
         f.argtypes = [CTX] + args

@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalfa.so")
-SOURCES = ["alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu"]
+SOURCES = ["alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu", "alfa_noalloc.cu"]
 HEADERS = ["alfa_fft.cuh", "alfa_internal.cuh", "alfa_physics.cuh"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,72 @@
+// alfa_PlanarMean_noalloc: the plane mean of alfa_PlanarMean for callers
+// that may not allocate device memory.
+//
+// Who needs it: code that runs inside another runtime's memory management.
+// A JAX/XLA custom call is the case closest to this project: XLA reserves
+// most of the GPU's memory for its own allocator when it starts and hands a
+// custom call only the buffers it owns, so a cudaMalloc inside the call can
+// fail, or take memory XLA has already promised to other buffers.  The same
+// holds for applications that fix their device-memory budget at start-up.
+// Such callers cannot create an alfa_ctx (its set-up allocates the
+// workspace), so this entry point needs no context.
+//
+// The two-level reduction keeps one partial sum per (block, level); here
+// those partials live in a fixed array in the library's device image, so
+// nothing is allocated at call time.  Every device that loads the library
+// holds its own copy of the array until the process exits.
+#include <mutex>
+
+#include "alfa.h"
+#include "alfa_internal.cuh"
+
+namespace alfa {
+// alfa_physics.cu: the reduction kernels of plane_means, fed explicit scratch
+void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials, double* mean,
+                             cudaStream_t s);
+}  // namespace alfa
+
+namespace {
+
+constexpr int kBlocks = 256;       // partial sums per level (as plane_means)
+constexpr int kMaxLevels = 2048;   // largest nz accepted
+// 256 x 2048 doubles = 4 MiB per device
+static __device__ __align__(256) double g_partials[kBlocks * kMaxLevels];
+
+std::mutex g_mu;
+constexpr int kMaxDevices = 256;
+double* g_addr[kMaxDevices] = {};
+
+// Device address of g_partials on the current device, looked up once per
+// device with that device current.  (In host code the name g_partials is a
+// host-side stand-in, not a device address, so it is never passed as is.)
+int partials_on_current_device(double** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ALFA_E_CUDA;
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (g_addr[dev] == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_partials) != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return ALFA_E_CUDA;
+    }
+    g_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_addr[dev];
+  return ALFA_OK;
+}
+
+}  // namespace
+
+extern "C" int alfa_PlanarMean_noalloc(const double* F, int nx, int ny, int nz, double* mean_nz,
+                                       void* cuda_stream) {
+  if (!F || !mean_nz || nx < 1 || ny < 1 || nz < 1) return ALFA_E_SHAPE;
+  if (nz > kMaxLevels) return ALFA_E_NOALLOC_LIMIT;
+  double* partials = nullptr;
+  const int st = partials_on_current_device(&partials);
+  if (st != ALFA_OK) return st;
+  // Every partial read by the final sum is written by this call's first
+  // kernel, so the array needs no clearing; it keeps the last call's values.
+  alfa::plane_mean_with_scratch(F, (size_t)nx * (size_t)ny, nz, partials, mean_nz,
+                                static_cast<cudaStream_t>(cuda_stream));
+  return cudaGetLastError() == cudaSuccess ? ALFA_OK : ALFA_E_CUDA;
+}

@@ -66,6 +66,19 @@ void plane_sums(Engine& e, const double* const* fields, int nq, double* sums) {
                                                                        sums);
 }
 
+// The plane mean of one field with caller-provided partial-sum storage
+// (RED_BLOCKS x nz doubles); same kernels and block count as plane_means.
+void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials, double* mean,
+                             cudaStream_t s) {
+  RedArgs a{};
+  a.nq = 1;
+  a.f[0] = F;
+  const int nb = (int)(H < (size_t)RED_BLOCKS ? H : RED_BLOCKS);
+  ::alfa::note_launch(); k_plane_partial<<<nb, 128, 0, s>>>(a, H, nz, partials);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)nz), TPB, 0, s>>>(
+      partials, nb, 1, nz, 1.0 / (double)H, mean);
+}
+
 void plane_means(Engine& e, const double* const* fields, int nq, double* means) {
   RedArgs a{};
   a.nq = nq;
