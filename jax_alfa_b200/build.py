@@ -9,7 +9,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalfa.so")
 SOURCES = ["alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu", "alfa_noalloc.cu"]
-HEADERS = ["alfa_fft.cuh", "alfa_internal.cuh", "alfa_physics.cuh"]
+HEADERS = ["alfa_fft.cuh", "alfa_fft_ct.cuh", "alfa_internal.cuh", "alfa_physics.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -137,6 +137,8 @@ int engine_init(Engine& e, const alfa_config& c) {
   if (c.dynamicSGS_call_time < 1) return e.fail("dynamicSGS_call_time must be >= 1", ALFA_E_CONFIG);
   e.mx = (int)(1.5 * c.nx);
   e.my = (int)(1.5 * c.ny);
+  if (c.ny > 512 || c.nx > 1024)
+    return e.fail("grid too large for the FFT tiles (ny <= 512, nx <= 1024)", ALFA_E_CONFIG);
   e.nxh = c.nx / 2 + 1;
   e.nyh = c.ny / 2 + 1;
   e.mxh = e.mx / 2 + 1;

@@ -147,14 +147,14 @@ struct FftPlan {
 // One Stockham pass of radix R over C columns (Govindaraju et al., "High
 // performance discrete Fourier transforms on graphics processors", SC 2008,
 // Stockham formulation).  src/dst are n x C shared-memory tiles.
-template <int R, int S>
+template <int R, int S, int C>
 __device__ __forceinline__ void stockham_pass(const cd* __restrict__ src, cd* __restrict__ dst, int n,
-                                              int Ns, int C, const cd* __restrict__ tw) {
+                                              int Ns, const cd* __restrict__ tw) {
   const int nR = n / R;
   const int B = nR * C;
   const int stride = n / (Ns * R);
   for (int b = threadIdx.x; b < B; b += blockDim.x) {
-    const int c = b % C;
+    const int c = b % C;  // C is a power of two: shifts and masks
     const int j = b / C;
     cd v[R];
 #pragma unroll
@@ -178,19 +178,19 @@ __device__ __forceinline__ void stockham_pass(const cd* __restrict__ src, cd* __
 // Full unnormalised transform of the n x C tile in buf[0]; buf[1] is
 // scratch of the same size.  Returns the index (0/1) of the buffer holding
 // the result.  S = -1 forward, +1 inverse.  Leaves a __syncthreads() behind.
-template <int S>
-__device__ int fft_tile(cd* buf0, cd* buf1, const FftPlan& p, int C) {
+template <int S, int C>
+__device__ int fft_tile(cd* buf0, cd* buf1, const FftPlan& p) {
   cd* src = buf0;
   cd* dst = buf1;
   int Ns = 1;
   for (int i = 0; i < p.npass; i++) {
     __syncthreads();
     switch (p.rad[i]) {
-      case 16: stockham_pass<16, S>(src, dst, p.n, Ns, C, p.tw); break;
-      case 8: stockham_pass<8, S>(src, dst, p.n, Ns, C, p.tw); break;
-      case 4: stockham_pass<4, S>(src, dst, p.n, Ns, C, p.tw); break;
-      case 3: stockham_pass<3, S>(src, dst, p.n, Ns, C, p.tw); break;
-      default: stockham_pass<2, S>(src, dst, p.n, Ns, C, p.tw); break;
+      case 16: stockham_pass<16, S, C>(src, dst, p.n, Ns, p.tw); break;
+      case 8: stockham_pass<8, S, C>(src, dst, p.n, Ns, p.tw); break;
+      case 4: stockham_pass<4, S, C>(src, dst, p.n, Ns, p.tw); break;
+      case 3: stockham_pass<3, S, C>(src, dst, p.n, Ns, p.tw); break;
+      default: stockham_pass<2, S, C>(src, dst, p.n, Ns, p.tw); break;
     }
     Ns *= p.rad[i];
     cd* t = src;
@@ -199,6 +199,105 @@ __device__ int fft_tile(cd* buf0, cd* buf1, const FftPlan& p, int C) {
   }
   __syncthreads();
   return src == buf0 ? 0 : 1;
+}
+
+// In-place variant: one n x C tile, no second buffer.  In each pass every
+// thread first reads all of its butterflies (at most MB of them, R inputs
+// each) into registers, the block synchronises, and only then are the
+// results written back over the tile.  With blockDim.x >= C*n/16 a thread
+// holds at most 18 complex values in any pass (radix 16: 1 butterfly,
+// 8: 2, 4: 4, 3: 6, 2: 8).
+// (not inlined: one all-radix body inlined into the pass loop makes the
+// register allocator keep every variant's arrays live and spill)
+template <int R, int S, int C, int MB>
+__device__ __noinline__ void stockham_inplace(cd* __restrict__ buf, int n, int Ns,
+                                                 const cd* __restrict__ tw) {
+  const int nR = n / R;
+  const int B = nR * C;
+  const int stride = n / (Ns * R);
+  cd v[MB * R];
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * blockDim.x;
+    if (b < B) {
+      const int c = b % C;
+      const int j = b / C;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[q * R + r] = buf[(j + r * nR) * C + c];
+      const int k = j % Ns;
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+          cd w = __ldg(&tw[k * r * stride]);
+          if (S > 0) w.y = -w.y;
+          v[q * R + r] = cmul(v[q * R + r], w);
+        }
+      }
+      dftR<R, S>(v + q * R);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * blockDim.x;
+    if (b < B) {
+      const int c = b % C;
+      const int j = b / C;
+      const int k = j % Ns;
+      const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; r++) buf[(idxD + r * Ns) * C + c] = v[q * R + r];
+    }
+  }
+}
+
+template <int R, int S, int C>
+__device__ __forceinline__ void inplace_pass(cd* buf, int n, int Ns, const cd* tw) {
+  const int B = (n / R) * C;
+  const int mb = (B + blockDim.x - 1) / blockDim.x;
+  if (R == 16) {
+    stockham_inplace<R, S, C, 1>(buf, n, Ns, tw);
+  } else if (R == 8) {
+    if (mb <= 1) stockham_inplace<R, S, C, 1>(buf, n, Ns, tw);
+    else stockham_inplace<R, S, C, 2>(buf, n, Ns, tw);
+  } else if (R == 4) {
+    if (mb <= 2) stockham_inplace<R, S, C, 2>(buf, n, Ns, tw);
+    else stockham_inplace<R, S, C, 4>(buf, n, Ns, tw);
+  } else if (R == 3) {
+    if (mb <= 2) stockham_inplace<R, S, C, 2>(buf, n, Ns, tw);
+    else if (mb <= 4) stockham_inplace<R, S, C, 4>(buf, n, Ns, tw);
+    else stockham_inplace<R, S, C, 6>(buf, n, Ns, tw);
+  } else {
+    if (mb <= 2) stockham_inplace<R, S, C, 2>(buf, n, Ns, tw);
+    else if (mb <= 4) stockham_inplace<R, S, C, 4>(buf, n, Ns, tw);
+    else stockham_inplace<R, S, C, 8>(buf, n, Ns, tw);
+  }
+}
+
+// Full unnormalised in-place transform of the n x C tile `buf`; requires
+// blockDim.x >= ceil(C*n/16).  Leaves a __syncthreads() behind.
+template <int S, int C>
+__device__ void fft_inplace(cd* buf, const FftPlan& p) {
+  int Ns = 1;
+  for (int i = 0; i < p.npass; i++) {
+    __syncthreads();
+    switch (p.rad[i]) {
+      case 16: inplace_pass<16, S, C>(buf, p.n, Ns, p.tw); break;
+      case 8: inplace_pass<8, S, C>(buf, p.n, Ns, p.tw); break;
+      case 4: inplace_pass<4, S, C>(buf, p.n, Ns, p.tw); break;
+      case 3: inplace_pass<3, S, C>(buf, p.n, Ns, p.tw); break;
+      default: inplace_pass<2, S, C>(buf, p.n, Ns, p.tw); break;
+    }
+    Ns *= p.rad[i];
+  }
+  __syncthreads();
+}
+
+// threads needed by fft_inplace for lengths up to n_max over C columns
+inline int inplace_threads(int C, int n_max) {
+  int t = (C * n_max + 15) / 16;
+  t = (t + 31) / 32 * 32;
+  return t < 64 ? 64 : t;
 }
 
 }  // namespace alfa

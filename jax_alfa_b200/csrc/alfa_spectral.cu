@@ -15,120 +15,174 @@
 //             parts of the ky=0 and ky=ny/2 bins ignored, as irfft does).
 // Only the ky columns a consumer needs are computed and stored (a level-1
 // test filter keeps ky < ny/4, so its tiles hold a quarter of the columns).
+//
+// Every tile kernel first issues all of a thread's global loads for a batch
+// of U elements into registers and only then writes them to shared memory,
+// so a thread keeps U loads in flight instead of waiting on each one.
 #include <cmath>
 
+#include "alfa_fft_ct.cuh"
 #include "alfa_internal.cuh"
 
 namespace alfa {
 
 static constexpr int YC = 8;    // complex columns (= 16 real z levels) per y tile
-static constexpr int YTHREADS = 128;
-static constexpr int XTHREADS = 128;
+static constexpr int MAXTHREADS = 384;  // in-place sweeps need C*n/16 threads
+static constexpr int U = 8;     // loads in flight per thread
 
 // ---------------------------------------------------------------------------
-// Loader evaluation (value of the real input at linear index i, level z)
+// Loader evaluation (value of the real input at linear index i, level z);
+// the kind is a compile-time constant in the tile kernels.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double ld_eval(const Loader& L, size_t i, int z) {
+template <int KIND>
+__device__ __forceinline__ double ldv(const Loader& L, size_t i, int z) {
   const int nz = L.nz;
-  switch (L.kind) {
-    case LD_FIELD:
-      return L.a[0][i];
-    case LD_MUL:
-      return L.a[0][i] * L.a[1][i];
-    case LD_MUL3:
-      return L.a[0][i] * L.a[1][i] * L.a[2][i];
-    case LD_PRESSURE_R:  // NSE_PressureTerms.py:140-142
-      return L.a[0][i] - L.c[0] * L.a[1][i] + L.c[1] * L.a[2][i];
-    case LD_ADV_XY: {  // NSE_AdvectionTerms.py:105-116 (Cx) and :122-132 (Cy)
-      const double arg1 = L.a[0][i] * (L.a[1][i] - L.a[2][i]);
-      if (z == 0) {
-        const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
-        return arg1 + 0.5 * a2n;
-      }
-      const double a2 = L.a[3][i] * (L.a[4][i] - L.a[5][i]);
-      if (z == nz - 1) return arg1 + a2;
+  if constexpr (KIND == LD_FIELD) {
+    return L.a[0][i];
+  } else if constexpr (KIND == LD_MUL) {
+    return L.a[0][i] * L.a[1][i];
+  } else if constexpr (KIND == LD_MUL3) {
+    return L.a[0][i] * L.a[1][i] * L.a[2][i];
+  } else if constexpr (KIND == LD_PRESSURE_R) {  // NSE_PressureTerms.py:140-142
+    return L.a[0][i] - L.c[0] * L.a[1][i] + L.c[1] * L.a[2][i];
+  } else if constexpr (KIND == LD_ADV_XY) {  // NSE_AdvectionTerms.py:105-116, :122-132
+    const double arg1 = L.a[0][i] * (L.a[1][i] - L.a[2][i]);
+    if (z == 0) {
       const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
-      return arg1 + 0.5 * (a2 + a2n);
+      return arg1 + 0.5 * a2n;
     }
-    case LD_ADV_Z: {  // NSE_AdvectionTerms.py:137-151
-      if (z == 0 || z == nz - 1) return 0.0;
-      const double ug = 0.5 * (L.a[0][i - 1] + L.a[0][i]);
-      const double vg = 0.5 * (L.a[1][i - 1] + L.a[1][i]);
-      const double a1 = ug * (L.a[2][i] - L.a[3][i]);
-      const double a2 = vg * (L.a[4][i] - L.a[5][i]);
-      return a1 + a2;
-    }
-    case LD_SCALAR_ADV: {  // SCL_AdvectionTerms.py:89-101
-      const double c1 = L.a[0][i] * L.a[3][i] + L.a[1][i] * L.a[4][i];
-      const double c2 = L.a[2][i] * L.a[5][i];
-      if (z == nz - 1) return c1 + c2;
-      const double c2n = L.a[2][i + 1] * L.a[5][i + 1];
-      return c1 + 0.5 * (c2 + c2n);
-    }
-    case LD_STRESS_UVP:  // SGSStresses_SM.py:122-132, ScalarSGSFluxes_SM.py:78-84
+    const double a2 = L.a[3][i] * (L.a[4][i] - L.a[5][i]);
+    if (z == nz - 1) return arg1 + a2;
+    const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
+    return arg1 + 0.5 * (a2 + a2n);
+  } else if constexpr (KIND == LD_ADV_Z) {  // NSE_AdvectionTerms.py:137-151
+    if (z == 0 || z == nz - 1) return 0.0;
+    const double ug = 0.5 * (L.a[0][i - 1] + L.a[0][i]);
+    const double vg = 0.5 * (L.a[1][i - 1] + L.a[1][i]);
+    const double a1 = ug * (L.a[2][i] - L.a[3][i]);
+    const double a2 = vg * (L.a[4][i] - L.a[5][i]);
+    return a1 + a2;
+  } else if constexpr (KIND == LD_SCALAR_ADV) {  // SCL_AdvectionTerms.py:89-101
+    const double c1 = L.a[0][i] * L.a[3][i] + L.a[1][i] * L.a[4][i];
+    const double c2 = L.a[2][i] * L.a[5][i];
+    if (z == nz - 1) return c1 + c2;
+    const double c2n = L.a[2][i + 1] * L.a[5][i + 1];
+    return c1 + 0.5 * (c2 + c2n);
+  } else if constexpr (KIND == LD_STRESS_UVP) {  // SGSStresses_SM.py:122-132
+    if (z == nz - 1) return 0.0;
+    return L.c[0] * L.a[0][i] * L.a[1][i] * L.a[2][i];
+  } else if constexpr (KIND == LD_STRESS_W) {  // SGSStresses_SM.py:223-232
+    if (z == 0 || z == nz - 1) return 0.0;
+    return L.c[0] * (0.5 * (L.a[0][i - 1] + L.a[0][i])) * L.a[1][i] * L.a[2][i];
+  } else if constexpr (KIND == LD_W_SXX) {  // StrainRates.py:250-276, component L.sub
+    const double* const* g = L.a;  // dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
+    auto stag = [&](const double* d) -> double {
+      if (z == 0) return d[i];
       if (z == nz - 1) return 0.0;
-      return L.c[0] * L.a[0][i] * L.a[1][i] * L.a[2][i];
-    case LD_STRESS_W:  // SGSStresses_SM.py:223-232, ScalarSGSFluxes_SM.py:163-169
-      if (z == 0 || z == nz - 1) return 0.0;
-      return L.c[0] * (0.5 * (L.a[0][i - 1] + L.a[0][i])) * L.a[1][i] * L.a[2][i];
-    case LD_W_SXX: {  // StrainRates.py:250-276: component L.sub of the w-node strain
-      const double* const* g = L.a;  // dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
-      auto stag = [&](const double* d) -> double {
-        if (z == 0) return d[i];
-        if (z == nz - 1) return 0.0;
-        return 0.5 * (d[i - 1] + d[i]);
-      };
-      switch (L.sub) {
-        case 0: return stag(g[0]);                                  // S11 = ux
-        case 1: return stag(g[4]);                                  // S22 = vy
-        case 2: return stag(g[8]);                                  // S33 = wz
-        case 3: return 0.5 * (stag(g[3]) + stag(g[1]));             // S12
-        case 4: {                                                   // S13
-          const double wx = (z == 0) ? 0.5 * (g[2][i] + g[2][i + 1]) : g[2][i];
-          return 0.5 * (g[6][i] + wx);
-        }
-        default: {                                                  // S23
-          const double wy = (z == 0) ? 0.5 * (g[5][i] + g[5][i + 1]) : g[5][i];
-          return 0.5 * (g[7][i] + wy);
+      return 0.5 * (d[i - 1] + d[i]);
+    };
+    switch (L.sub) {
+      case 0: return stag(g[0]);                       // S11 = ux
+      case 1: return stag(g[4]);                       // S22 = vy
+      case 2: return stag(g[8]);                       // S33 = wz
+      case 3: return 0.5 * (stag(g[3]) + stag(g[1]));  // S12
+      case 4: {                                        // S13
+        const double wx = (z == 0) ? 0.5 * (g[2][i] + g[2][i + 1]) : g[2][i];
+        return 0.5 * (g[6][i] + wx);
+      }
+      default: {                                       // S23
+        const double wy = (z == 0) ? 0.5 * (g[5][i] + g[5][i + 1]) : g[5][i];
+        return 0.5 * (g[7][i] + wy);
+      }
+    }
+  } else if constexpr (KIND == LD_THZ) {  // DynamicSGS_ScalarLASDD_SM.py:182-185
+    const double* d = L.a[0];
+    if (z == 0 || z == nz - 1) return d[i];
+    return 0.5 * (d[i] + d[i + 1]);
+  } else {  // LD_MUL_THZ: S * THz
+    const double* d = L.a[1];
+    const double t = (z == 0 || z == nz - 1) ? d[i] : 0.5 * (d[i] + d[i + 1]);
+    return L.a[0][i] * t;
+  }
+}
+
+// Load the (n x 16 z) real tile of row `row` into b0 as n x 8 complex
+// (z pairs), U elements per thread in flight.
+template <int KIND>
+__device__ __forceinline__ void y_fwd_load(const Loader& L, int row, int n, int z0, cd* b0) {
+  const int nz = L.nz;
+  const int total = n * YC;
+  const bool vec = (KIND == LD_FIELD) && ((nz & 1) == 0);
+  for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
+    cd v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      v[u] = make_double2(0.0, 0.0);
+      if (t < total) {
+        const int y = t / YC, c = t % YC;
+        const int z = z0 + 2 * c;
+        const size_t i = ((size_t)row * n + y) * nz + z;
+        if (vec && z + 1 < nz) {
+          v[u] = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+        } else {
+          if (z < nz) v[u].x = ldv<KIND>(L, i, z);
+          if (z + 1 < nz) v[u].y = ldv<KIND>(L, i + 1, z + 1);
         }
       }
     }
-    case LD_THZ: {  // DynamicSGS_ScalarLASDD_SM.py:182-185
-      const double* d = L.a[0];
-      if (z == 0 || z == nz - 1) return d[i];
-      return 0.5 * (d[i] + d[i + 1]);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t < total) b0[t] = v[u];
     }
-    case LD_MUL_THZ: {  // S * THz
-      const double* d = L.a[1];
-      const double t = (z == 0 || z == nz - 1) ? d[i] : 0.5 * (d[i] + d[i + 1]);
-      return L.a[0][i] * t;
-    }
-    default:
-      return 0.0;
   }
+}
+
+// Transform of an n x C tile: compile-time specialised for the lengths in
+// the dispatch tables below (N > 0), the runtime plan otherwise (N == 0).
+template <int S, int C, int N, int NT>
+__device__ __forceinline__ void tile_fft(cd* buf, const FftPlan& p) {
+  if constexpr (N == 0) {
+    fft_inplace<S, C>(buf, p);
+  } else {
+    fft_ct<S, C, N, NT>(buf, p.tw);
+  }
+}
+
+template <int C, int N>
+__host__ __device__ constexpr int tile_threads() {
+  return N == 0 ? MAXTHREADS : ct_threads(C, N);
 }
 
 // ---------------------------------------------------------------------------
 // k_y_fwd: rows x n(y) x nz real -> T (rows, K, nz) complex, ky < K
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(YTHREADS) k_y_fwd(Loader L, FftPlan p, int K, cd* __restrict__ T) {
+template <int N>
+__global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
+    k_y_fwd(Loader L, FftPlan p, int K, cd* __restrict__ T) {
   extern __shared__ cd sm[];
-  const int n = p.n;
+  const int n = (N > 0) ? N : p.n;
   const int nz = L.nz;
   const int z0 = blockIdx.x * (2 * YC);
   const int row = blockIdx.y;
   cd* b0 = sm;
-  cd* b1 = sm + n * YC;
-  for (int t = threadIdx.x; t < n * YC; t += blockDim.x) {
-    const int y = t / YC, c = t % YC;
-    const int z = z0 + 2 * c;
-    const size_t base = ((size_t)row * n + y) * nz;
-    const double re = (z < nz) ? ld_eval(L, base + z, z) : 0.0;
-    const double im = (z + 1 < nz) ? ld_eval(L, base + z + 1, z + 1) : 0.0;
-    b0[t] = make_double2(re, im);
+  switch (L.kind) {
+    case LD_FIELD: y_fwd_load<LD_FIELD>(L, row, n, z0, b0); break;
+    case LD_MUL: y_fwd_load<LD_MUL>(L, row, n, z0, b0); break;
+    case LD_MUL3: y_fwd_load<LD_MUL3>(L, row, n, z0, b0); break;
+    case LD_PRESSURE_R: y_fwd_load<LD_PRESSURE_R>(L, row, n, z0, b0); break;
+    case LD_ADV_XY: y_fwd_load<LD_ADV_XY>(L, row, n, z0, b0); break;
+    case LD_ADV_Z: y_fwd_load<LD_ADV_Z>(L, row, n, z0, b0); break;
+    case LD_SCALAR_ADV: y_fwd_load<LD_SCALAR_ADV>(L, row, n, z0, b0); break;
+    case LD_STRESS_UVP: y_fwd_load<LD_STRESS_UVP>(L, row, n, z0, b0); break;
+    case LD_STRESS_W: y_fwd_load<LD_STRESS_W>(L, row, n, z0, b0); break;
+    case LD_W_SXX: y_fwd_load<LD_W_SXX>(L, row, n, z0, b0); break;
+    case LD_THZ: y_fwd_load<LD_THZ>(L, row, n, z0, b0); break;
+    default: y_fwd_load<LD_MUL_THZ>(L, row, n, z0, b0); break;
   }
-  const int r = fft_tile<-1>(b0, b1, p, YC);
-  const cd* Z = r ? b1 : b0;
+  tile_fft<-1, YC, N, tile_threads<YC, N>()>(b0, p);
+  const cd* Z = b0;
   for (int t = threadIdx.x; t < K * YC; t += blockDim.x) {
     const int k = t / YC, c = t % YC;
     const int z = z0 + 2 * c;
@@ -145,45 +199,102 @@ __global__ void __launch_bounds__(YTHREADS) k_y_fwd(Loader L, FftPlan p, int K, 
 // ---------------------------------------------------------------------------
 // k_y_inv: T (rows, K, nz), ky < K nonzero -> rows x n(y) x nz real
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(YTHREADS) k_y_inv(const cd* __restrict__ T, int K, FftPlan p,
-                                                    int nz, double scale, double* __restrict__ out,
-                                                    int accumulate) {
+template <int N>
+__global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
+    k_y_inv(const cd* __restrict__ T, int K, FftPlan p, int nz, double scale,
+            double* __restrict__ out, int accumulate) {
   extern __shared__ cd sm[];
-  const int n = p.n;
+  const int n = (N > 0) ? N : p.n;
   const int h = n / 2;
   const int z0 = blockIdx.x * (2 * YC);
   const int row = blockIdx.y;
   cd* b0 = sm;
-  cd* b1 = sm + n * YC;
-  for (int t = threadIdx.x; t < (h + 1) * YC; t += blockDim.x) {
-    const int k = t / YC, c = t % YC;
-    const int z = z0 + 2 * c;
-    cd A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-    if (k < K) {
-      const size_t o = ((size_t)row * K + k) * nz + z;
-      if (z < nz) A = T[o];
-      if (z + 1 < nz) B = T[o + 1];
+  const int total = (h + 1) * YC;
+  const bool pair = (nz & 1) == 0;  // z, z+1 both present whenever z is
+  for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
+    cd A[U], B[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      A[u] = make_double2(0.0, 0.0);
+      B[u] = make_double2(0.0, 0.0);
+      const int k = t / YC, c = t % YC;
+      const int z = z0 + 2 * c;
+      if (t < total && k < K) {
+        const size_t o = ((size_t)row * K + k) * nz + z;
+        if (pair && z < nz) {
+          A[u] = __ldg(T + o);
+          B[u] = __ldg(T + o + 1);
+        } else {
+          if (z < nz) A[u] = T[o];
+          if (z + 1 < nz) B[u] = T[o + 1];
+        }
+      }
     }
-    if (k == 0 || k == h) {
-      A.y = 0.0;
-      B.y = 0.0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= total) continue;
+      const int k = t / YC, c = t % YC;
+      cd a = A[u], b = B[u];
+      if (k == 0 || k == h) {
+        a.y = 0.0;
+        b.y = 0.0;
+      }
+      b0[k * YC + c] = make_double2(a.x - b.y, a.y + b.x);
+      if (k > 0 && k < h) b0[(n - k) * YC + c] = make_double2(a.x + b.y, b.x - a.y);
     }
-    b0[k * YC + c] = make_double2(A.x - B.y, A.y + B.x);
-    if (k > 0 && k < h) b0[(n - k) * YC + c] = make_double2(A.x + B.y, B.x - A.y);
   }
-  const int r = fft_tile<+1>(b0, b1, p, YC);
-  const cd* Z = r ? b1 : b0;
-  for (int t = threadIdx.x; t < n * YC; t += blockDim.x) {
-    const int y = t / YC, c = t % YC;
-    const int z = z0 + 2 * c;
-    const size_t o = ((size_t)row * n + y) * nz + z;
-    const cd v = Z[t];
-    if (accumulate) {
-      if (z < nz) out[o] = out[o] + scale * v.x;
-      if (z + 1 < nz) out[o + 1] = out[o + 1] + scale * v.y;
-    } else {
-      if (z < nz) out[o] = scale * v.x;
-      if (z + 1 < nz) out[o + 1] = scale * v.y;
+  tile_fft<+1, YC, N, tile_threads<YC, N>()>(b0, p);
+  const cd* Z = b0;
+  if (accumulate) {
+    for (int t0 = threadIdx.x; t0 < n * YC; t0 += U * blockDim.x) {
+      double2 prev[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int t = t0 + u * blockDim.x;
+        const int y = t / YC, c = t % YC;
+        const int z = z0 + 2 * c;
+        const size_t o = ((size_t)row * n + y) * nz + z;
+        prev[u] = make_double2(0.0, 0.0);
+        if (t < n * YC) {
+          if (pair && z < nz) {
+            prev[u] = *reinterpret_cast<const double2*>(out + o);
+          } else {
+            if (z < nz) prev[u].x = out[o];
+            if (z + 1 < nz) prev[u].y = out[o + 1];
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int t = t0 + u * blockDim.x;
+        if (t >= n * YC) continue;
+        const int y = t / YC, c = t % YC;
+        const int z = z0 + 2 * c;
+        const size_t o = ((size_t)row * n + y) * nz + z;
+        const cd v = Z[t];
+        const double2 w = make_double2(prev[u].x + scale * v.x, prev[u].y + scale * v.y);
+        if (pair && z < nz) {
+          *reinterpret_cast<double2*>(out + o) = w;
+        } else {
+          if (z < nz) out[o] = w.x;
+          if (z + 1 < nz) out[o + 1] = w.y;
+        }
+      }
+    }
+  } else {
+    for (int t = threadIdx.x; t < n * YC; t += blockDim.x) {
+      const int y = t / YC, c = t % YC;
+      const int z = z0 + 2 * c;
+      const size_t o = ((size_t)row * n + y) * nz + z;
+      const cd v = Z[t];
+      if (pair && z < nz) {
+        *reinterpret_cast<double2*>(out + o) = make_double2(scale * v.x, scale * v.y);
+      } else {
+        if (z < nz) out[o] = scale * v.x;
+        if (z + 1 < nz) out[o + 1] = scale * v.y;
+      }
     }
   }
 }
@@ -194,7 +305,7 @@ __global__ void __launch_bounds__(YTHREADS) k_y_inv(const cd* __restrict__ T, in
 struct XArgs {
   const cd* src;
   int in_spec;   // 1: src is already a spectrum column set (no forward FFT)
-  int rows_in, Kin, nz, C;
+  int rows_in, Kin, nz;
   FftPlan fwd;
   int nout;
   XOut out[3];
@@ -203,8 +314,9 @@ struct XArgs {
   int nx, mx, maxrows;
 };
 
-__device__ __forceinline__ cd map_value(const XArgs& a, const XOut& o, const cd* S, int k,
-                                        int ky, int c, int C) {
+template <int C>
+__device__ __forceinline__ cd map_value(const XArgs& a, const XOut& o, const cd* S, int k, int ky,
+                                        int c) {
   switch (o.map) {
     case MAP_IDENT:
       return S[k * C + c];
@@ -237,32 +349,43 @@ __device__ __forceinline__ cd map_value(const XArgs& a, const XOut& o, const cd*
   }
 }
 
-__global__ void __launch_bounds__(XTHREADS) k_x(XArgs a) {
+// NI / NO: compile-time forward / inverse lengths (0: runtime plans)
+template <int C, int NI, int NO>
+__global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x(XArgs a) {
+  constexpr int NT = tile_threads<C, (NI > NO ? NI : NO)>();
   extern __shared__ cd sm[];
-  const int C = a.C;
   const int nz = a.nz;
   const int z0 = blockIdx.x * C;
   const int ky = blockIdx.y;
   const int M = a.maxrows * C;
-  cd* buf[3] = {sm, sm + M, sm + 2 * M};
+  cd* buf[2] = {sm, sm + M};
 
-  // load the input column set
-  for (int t = threadIdx.x; t < a.rows_in * C; t += blockDim.x) {
-    const int r = t / C, c = t % C;
-    const int z = z0 + c;
-    cd v = make_double2(0.0, 0.0);
-    if (ky < a.Kin && z < nz) v = a.src[((size_t)r * a.Kin + ky) * nz + z];
-    buf[0][t] = v;
+  // load the input column set, U loads in flight per thread
+  const int total = a.rows_in * C;
+  const bool have = ky < a.Kin;
+  for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
+    cd v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int r = t / C, c = t % C;
+      const int z = z0 + c;
+      v[u] = make_double2(0.0, 0.0);
+      if (have && t < total && z < nz) v[u] = __ldg(&a.src[((size_t)r * a.Kin + ky) * nz + z]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t < total) buf[0][t] = v[u];
+    }
   }
-  int s = 0;
   if (!a.in_spec) {
-    s = fft_tile<-1>(buf[0], buf[1], a.fwd, C);
+    tile_fft<-1, C, NI, NT>(buf[0], a.fwd);
   } else {
     __syncthreads();
   }
-  const cd* S = buf[s];
-  cd* f0 = buf[s == 0 ? 1 : 0];
-  cd* f1 = buf[2];
+  const cd* S = buf[0];
+  cd* f0 = buf[1];
 
   for (int oi = 0; oi < a.nout; oi++) {
     const XOut& o = a.out[oi];
@@ -270,17 +393,17 @@ __global__ void __launch_bounds__(XTHREADS) k_x(XArgs a) {
       for (int t = threadIdx.x; t < o.rows * C; t += blockDim.x) {
         const int k = t / C, c = t % C;
         const int z = z0 + c;
-        if (z < nz) o.dst[((size_t)k * o.K + ky) * nz + z] = map_value(a, o, S, k, ky, c, C);
+        if (z < nz) o.dst[((size_t)k * o.K + ky) * nz + z] = map_value<C>(a, o, S, k, ky, c);
       }
       continue;
     }
     if (ky >= o.K) continue;  // column not stored: zero by convention
     for (int t = threadIdx.x; t < o.rows * C; t += blockDim.x) {
       const int k = t / C, c = t % C;
-      f0[t] = map_value(a, o, S, k, ky, c, C);
+      f0[t] = map_value<C>(a, o, S, k, ky, c);
     }
-    const int r = fft_tile<+1>(f0, f1, o.inv, C);
-    const cd* R = r ? f1 : f0;
+    tile_fft<+1, C, NO, NT>(f0, o.inv);
+    const cd* R = f0;
     for (int t = threadIdx.x; t < o.rows * C; t += blockDim.x) {
       const int k = t / C, c = t % C;
       const int z = z0 + c;
@@ -291,26 +414,70 @@ __global__ void __launch_bounds__(XTHREADS) k_x(XArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// launchers
+// launchers (dispatch to the specialised lengths)
 // ---------------------------------------------------------------------------
 static void set_smem(const void* f, size_t bytes) {
   cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-void launch_y_fwd(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T) {
-  const size_t smem = 2 * (size_t)p.n * YC * sizeof(cd);
-  set_smem((const void*)k_y_fwd, smem);
+#define ALFA_Y_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \
+  X(512) X(768)
+
+template <int N>
+static void y_fwd_n(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T) {
+  const size_t smem = (size_t)p.n * YC * sizeof(cd);
+  set_smem((const void*)k_y_fwd<N>, smem);
   dim3 g((L.nz + 2 * YC - 1) / (2 * YC), rows);
-  ::alfa::note_launch(); k_y_fwd<<<g, YTHREADS, smem, e.stream>>>(L, p, K, T);
+  const int nt = N > 0 ? tile_threads<YC, N>() : inplace_threads(YC, p.n);
+  k_y_fwd<N><<<g, nt, smem, e.stream>>>(L, p, K, T);
+}
+
+template <int N>
+static void y_inv_n(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
+                    double* out, int accumulate) {
+  const size_t smem = (size_t)p.n * YC * sizeof(cd);
+  set_smem((const void*)k_y_inv<N>, smem);
+  dim3 g((e.nz + 2 * YC - 1) / (2 * YC), rows);
+  const int nt = N > 0 ? tile_threads<YC, N>() : inplace_threads(YC, p.n);
+  k_y_inv<N><<<g, nt, smem, e.stream>>>(T, K, p, e.nz, scale, out, accumulate);
+}
+
+void launch_y_fwd(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T) {
+  ::alfa::note_launch();
+  switch (p.n) {
+#define ALFA_CASE(n) \
+  case n: y_fwd_n<n>(e, L, rows, p, K, T); return;
+    ALFA_Y_LENGTHS(ALFA_CASE)
+#undef ALFA_CASE
+    default: y_fwd_n<0>(e, L, rows, p, K, T);
+  }
 }
 
 void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
                   double* out, int accumulate) {
-  const size_t smem = 2 * (size_t)p.n * YC * sizeof(cd);
-  set_smem((const void*)k_y_inv, smem);
-  dim3 g((e.nz + 2 * YC - 1) / (2 * YC), rows);
-  ::alfa::note_launch(); k_y_inv<<<g, YTHREADS, smem, e.stream>>>(T, K, p, e.nz, scale, out, accumulate);
+  ::alfa::note_launch();
+  switch (p.n) {
+#define ALFA_CASE(n) \
+  case n: y_inv_n<n>(e, T, rows, K, p, scale, out, accumulate); return;
+    ALFA_Y_LENGTHS(ALFA_CASE)
+#undef ALFA_CASE
+    default: y_inv_n<0>(e, T, rows, K, p, scale, out, accumulate);
+  }
 }
+
+template <int C, int NI, int NO>
+static void x_n(Engine& e, const XArgs& a, int Kgrid) {
+  const size_t smem = 2 * (size_t)a.maxrows * C * sizeof(cd);
+  set_smem((const void*)k_x<C, NI, NO>, smem);
+  dim3 g((e.nz + C - 1) / C, Kgrid);
+  const int nt = (NI > 0) ? tile_threads<C, (NI > NO ? NI : NO)>() : inplace_threads(C, a.maxrows);
+  k_x<C, NI, NO><<<g, nt, smem, e.stream>>>(a);
+}
+
+// (forward length, inverse length) pairs with a specialised k_x
+#define ALFA_X_PAIRS(X) X(16, 16) X(16, 24) X(24, 16) X(24, 24) X(32, 32) X(32, 48) X(48, 32) \
+  X(48, 48) X(64, 64) X(64, 96) X(96, 64) X(96, 96) X(128, 128) X(128, 192) X(192, 128)         \
+  X(192, 192) X(256, 256) X(256, 384) X(384, 256) X(384, 384)
 
 void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const FftPlan& fwd,
               int nout, const XOut* outs, int Kgrid) {
@@ -323,20 +490,36 @@ void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const
   a.fwd = fwd;
   a.nout = nout;
   int maxrows = rows_in;
+  int ninv = 0;
+  bool same_inv = true;
   for (int i = 0; i < nout; i++) {
     a.out[i] = outs[i];
     if (outs[i].rows > maxrows) maxrows = outs[i].rows;
+    if (outs[i].kind == XO_INV) {
+      if (ninv != 0 && outs[i].inv.n != ninv) same_inv = false;
+      ninv = outs[i].inv.n;
+    }
   }
+  if (ninv == 0) ninv = rows_in;
   a.kx = e.d_kx;
   a.ky = e.d_ky;
   a.nx = e.nx;
   a.mx = e.mx;
   a.maxrows = maxrows;
-  a.C = (3 * (size_t)maxrows * 8 * sizeof(cd) <= 100 * 1024) ? 8 : 4;
-  const size_t smem = 3 * (size_t)maxrows * a.C * sizeof(cd);
-  set_smem((const void*)k_x, smem);
-  dim3 g((e.nz + a.C - 1) / a.C, Kgrid);
-  ::alfa::note_launch(); k_x<<<g, XTHREADS, smem, e.stream>>>(a);
+  ::alfa::note_launch();
+  const int ni = in_spec ? ninv : rows_in;  // no forward transform: only the inverse length matters
+  if (same_inv) {
+#define ALFA_CASE(p, q)                                        \
+  if (ni == p && ninv == q) {                                  \
+    if ((p > q ? p : q) <= 256) x_n<8, p, q>(e, a, Kgrid);     \
+    else x_n<4, p, q>(e, a, Kgrid);                            \
+    return;                                                    \
+  }
+    ALFA_X_PAIRS(ALFA_CASE)
+#undef ALFA_CASE
+  }
+  if (maxrows <= 256) x_n<8, 0, 0>(e, a, Kgrid);
+  else x_n<4, 0, 0>(e, a, Kgrid);
 }
 
 // ---------------------------------------------------------------------------
