@@ -49,6 +49,8 @@ struct Work {
   double *Th, *Td, *uTh[3], *uTd[3], *Gh[3], *Gd[3], *SGh[3], *SGd[3];
   double *qx, *qy;
   double* Pb[10];  // padded fields
+  double* Lpad;    // (nx, my, nz): between the two passes of a pad / unpad
+  double* L2;      // two N fields: between the passes of filter + derivatives
   // pressure
   double *RCr, *RCi, *fRzr;
   cd *fRx, *fRy, *fRz, *fp, *fb2;
@@ -339,6 +341,8 @@ static void carve(alfa_ctx* c, Carver& k) {
   w.qx = k.take<double>(N);
   w.qy = k.take<double>(N);
   for (int i = 0; i < 10; i++) w.Pb[i] = k.take<double>(P);
+  w.Lpad = k.take<double>((size_t)e.nx * e.my * nz);
+  w.L2 = k.take<double>(2 * N);
   w.RCr = k.take<double>(R);
   w.RCi = k.take<double>(R);
   w.fRzr = k.take<double>(S);
@@ -381,25 +385,7 @@ static Loader ld(const Engine& e, int kind, std::initializer_list<const double*>
 // Derivxy(FFT(field)) with per-output accumulate flags
 static void deriv_field_acc(Engine& e, const Loader& L, double* dx, int accx, double* dy,
                             int accy) {
-  launch_y_fwd(e, L, e.nx, e.pny, e.nyh, e.T[0]);
-  XOut o[2];
-  int n = 0;
-  auto mk = [&](int map, cd* T) {
-    XOut x{};
-    x.kind = XO_INV;
-    x.map = map;
-    x.K = e.nyh;
-    x.rows = e.nx;
-    x.dst = T;
-    x.inv = e.pnx;
-    return x;
-  };
-  if (dx) o[n++] = mk(MAP_DX, e.T[1]);
-  if (dy) o[n++] = mk(MAP_DY, e.T[2]);
-  launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, n, o, e.nyh);
-  const double s = 1.0 / ((double)e.nx * e.ny);
-  if (dx) launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, s, dx, accx);
-  if (dy) launch_y_inv(e, e.T[2], e.nx, e.nyh, e.pny, s, dy, accy);
+  op2_deriv(e, L, dx, accx, dy, accy);
 }
 
 // NSE_SGSTerms.py:55-105
@@ -432,11 +418,11 @@ static void advection(alfa_ctx* c, const double* u, const double* v, const doubl
   Engine& e = c->e;
   double* const* Pb = c->w.Pb;
   const double* src[9] = {u, v, w, uy, uz, vx, vz, wx, wy};
-  for (int i = 0; i < 9; i++) op_pad(e, ld_field(e, src[i]), Pb[i]);
+  for (int i = 0; i < 9; i++) op2_pad(e, ld_field(e, src[i]), Pb[i], c->w.Lpad);
   // Pb: 0 up 1 vp 2 wp 3 uy 4 uz 5 vx 6 vz 7 wx 8 wy
-  op_unpad(e, ld(e, LD_ADV_XY, {Pb[1], Pb[3], Pb[5], Pb[2], Pb[4], Pb[7]}), Cx);
-  op_unpad(e, ld(e, LD_ADV_XY, {Pb[0], Pb[5], Pb[3], Pb[2], Pb[6], Pb[8]}), Cy);
-  op_unpad(e, ld(e, LD_ADV_Z, {Pb[0], Pb[1], Pb[7], Pb[4], Pb[8], Pb[6]}), Cz);
+  op2_unpad(e, ld(e, LD_ADV_XY, {Pb[1], Pb[3], Pb[5], Pb[2], Pb[4], Pb[7]}), Cx, c->w.Lpad);
+  op2_unpad(e, ld(e, LD_ADV_XY, {Pb[0], Pb[5], Pb[3], Pb[2], Pb[6], Pb[8]}), Cy, c->w.Lpad);
+  op2_unpad(e, ld(e, LD_ADV_Z, {Pb[0], Pb[1], Pb[7], Pb[4], Pb[8], Pb[6]}), Cz, c->w.Lpad);
 }
 
 // SCL_AdvectionTerms.py:57-106; reuse_uvw: Pb[0..2] already hold the padded
@@ -447,14 +433,14 @@ static void scalar_advection(alfa_ctx* c, const double* u, const double* v, cons
   Engine& e = c->e;
   double* const* Pb = c->w.Pb;
   if (!reuse_uvw) {
-    op_pad(e, ld_field(e, u), Pb[0]);
-    op_pad(e, ld_field(e, v), Pb[1]);
-    op_pad(e, ld_field(e, w), Pb[2]);
+    op2_pad(e, ld_field(e, u), Pb[0], c->w.Lpad);
+    op2_pad(e, ld_field(e, v), Pb[1], c->w.Lpad);
+    op2_pad(e, ld_field(e, w), Pb[2], c->w.Lpad);
   }
-  op_pad(e, ld_field(e, sx), Pb[3]);
-  op_pad(e, ld_field(e, sy), Pb[4]);
-  op_pad(e, ld_field(e, sz), Pb[5]);
-  op_unpad(e, ld(e, LD_SCALAR_ADV, {Pb[0], Pb[1], Pb[2], Pb[3], Pb[4], Pb[5]}), out);
+  op2_pad(e, ld_field(e, sx), Pb[3], c->w.Lpad);
+  op2_pad(e, ld_field(e, sy), Pb[4], c->w.Lpad);
+  op2_pad(e, ld_field(e, sz), Pb[5], c->w.Lpad);
+  op2_unpad(e, ld(e, LD_SCALAR_ADV, {Pb[0], Pb[1], Pb[2], Pb[3], Pb[4], Pb[5]}), out, c->w.Lpad);
 }
 
 // Stresses of StressesUVPnodes_Dealias / StressesWnodes_Dealias from the
@@ -467,17 +453,17 @@ static void sgs_stresses(alfa_ctx* c, const double* const g[9], const double* S_
   double* const* Pb = c->w.Pb;
   const double cst = -2 * std::pow(e.L, 2.0);
   for (int i = 0; i < 4; i++)
-    op_unpad(e, ld(e, LD_STRESS_UVP, {Pb[9], S_uvp_pad, Pb[i]}, cst), t6[i]);
+    op2_unpad(e, ld(e, LD_STRESS_UVP, {Pb[9], S_uvp_pad, Pb[i]}, cst), t6[i], c->w.Lpad);
   Loader Lw = ld(e, LD_W_SXX, {g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8]});
   for (int s = 0; s < 6; s++) {
     Lw.sub = s;
-    op_pad(e, Lw, Pb[s]);
+    op2_pad(e, Lw, Pb[s], c->w.Lpad);
   }
   smag_w(e, g, S_w);
   const double* q6[6] = {Pb[0], Pb[1], Pb[2], Pb[3], Pb[4], Pb[5]};
   smag6(e, q6, e.P(), S_w_pad);
-  op_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[4]}, cst), t6[4]);
-  op_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[5]}, cst), t6[5]);
+  op2_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[4]}, cst), t6[4], c->w.Lpad);
+  op2_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[5]}, cst), t6[5], c->w.Lpad);
   wall_override(e, u, v, M, pm, pm0, t6[4], t6[5]);
 }
 
@@ -493,7 +479,7 @@ static void uvp_strains_padded(alfa_ctx* c, const double* const g[9], const doub
   Sij[3] = w.S12;
   Sij[4] = w.S13;
   Sij[5] = w.S23;
-  for (int i = 0; i < 6; i++) op_pad(e, ld_field(e, Sij[i]), w.Pb[i]);
+  for (int i = 0; i < 6; i++) op2_pad(e, ld_field(e, Sij[i]), w.Pb[i], c->w.Lpad);
   const double* p6[6] = {w.Pb[0], w.Pb[1], w.Pb[2], w.Pb[3], w.Pb[4], w.Pb[5]};
   smag6(e, p6, e.P(), S_uvp_pad);
 }
@@ -558,7 +544,7 @@ static int dynamic_sgs(alfa_ctx* c, const double* const g[9], const double* u, c
   clip_ratio(e, W.LM, W.MM, Cs2);
   cs2_profiles(e, Cs2, avg1, avg2);
   // stresses (SGSStresses_SM.py) with Cs2_3D_pad = Dealias1(FFT(Cs2_3D))
-  op_pad(e, ld_field(e, Cs2), W.Pb[9]);
+  op2_pad(e, ld_field(e, Cs2), W.Pb[9], c->w.Lpad);
   double* t6[6] = {mom[0], mom[1], mom[2], mom[3], mom[4], mom[5]};
   sgs_stresses(c, g, mom[20], u, v, M, pm, pm0, t6, mom[21], mom[22]);
   div_stress(c, mom[0], mom[1], mom[2], mom[3], mom[4], mom[5], divt[0], divt[1], divt[2]);
@@ -573,7 +559,7 @@ static int static_sgs(alfa_ctx* c, const double* const g[9], const double* Cs2, 
   Work& W = c->w;
   const double* Sij[6];
   uvp_strains_padded(c, g, Sij, mom10[6], mom10[7]);
-  op_pad(e, ld_field(e, Cs2), W.Pb[9]);
+  op2_pad(e, ld_field(e, Cs2), W.Pb[9], c->w.Lpad);
   double* t6[6] = {mom10[0], mom10[1], mom10[2], mom10[3], mom10[4], mom10[5]};
   sgs_stresses(c, g, mom10[7], u, v, M, pm, pm0, t6, mom10[8], mom10[9]);
   div_stress(c, mom10[0], mom10[1], mom10[2], mom10[3], mom10[4], mom10[5], divt[0], divt[1],
@@ -587,14 +573,14 @@ static void scalar_fluxes(alfa_ctx* c, const double* S_uvp_pad, const double* S_
                           const double* qz_sfc, double* qz, double* divq) {
   Engine& e = c->e;
   Work& W = c->w;
-  op_pad(e, ld_field(e, gx), W.Pb[0]);
-  op_pad(e, ld_field(e, gy), W.Pb[1]);
-  op_pad(e, ld_field(e, gz), W.Pb[2]);
-  op_pad(e, ld_field(e, r3), W.Pb[3]);
+  op2_pad(e, ld_field(e, gx), W.Pb[0], c->w.Lpad);
+  op2_pad(e, ld_field(e, gy), W.Pb[1], c->w.Lpad);
+  op2_pad(e, ld_field(e, gz), W.Pb[2], c->w.Lpad);
+  op2_pad(e, ld_field(e, r3), W.Pb[3], c->w.Lpad);
   const double cst = -2 * std::pow(e.L, 2.0);
-  op_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[0]}, cst), W.qx);
-  op_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[1]}, cst), W.qy);
-  op_unpad(e, ld(e, LD_STRESS_W, {W.Pb[3], S_w_pad, W.Pb[2]}, cst), qz);
+  op2_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[0]}, cst), W.qx, c->w.Lpad);
+  op2_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[1]}, cst), W.qy, c->w.Lpad);
+  op2_unpad(e, ld(e, LD_STRESS_W, {W.Pb[3], S_w_pad, W.Pb[2]}, cst), qz, c->w.Lpad);
   set_plane0(e, qz_sfc, qz);
   div_flux(c, W.qx, W.qy, qz, divq);
 }
@@ -712,14 +698,18 @@ static int one_step(alfa_ctx* c) {
   // filtering (Main.py:193-197): the filtered field replaces the state, so
   // filter into the (not yet used) gradient slot and swap the two N-sized
   // buffers; the TH spectrum is discarded as in the reference.
-  op_filter_explicit(e, ld_field(e, W.u), W.g[0], W.ufft);
-  std::swap(W.u, W.g[0]);
-  op_filter_explicit(e, ld_field(e, W.v), W.g[0], W.vfft);
-  std::swap(W.v, W.g[0]);
-  op_filter_explicit(e, ld_field(e, W.w), W.g[0], W.wfft);
-  std::swap(W.w, W.g[0]);
-  op_filter_explicit(e, ld_field(e, W.TH), W.g[0], W.fp);
-  std::swap(W.TH, W.g[0]);
+  // The x and y derivatives of the filtered fields (velocityGradients,
+  // potentialTemperatureGradients: Derivxy of the filtered spectrum) come
+  // out of the same separable passes.  Filtered fields land in buffers
+  // that are free until advection, then swap with the state.
+  op2_filter_deriv(e, ld_field(e, W.u), W.Cx, W.g[0], W.g[3], W.L2);
+  std::swap(W.u, W.Cx);
+  op2_filter_deriv(e, ld_field(e, W.v), W.Cy, W.g[1], W.g[4], W.L2);
+  std::swap(W.v, W.Cy);
+  op2_filter_deriv(e, ld_field(e, W.w), W.Cz, W.g[2], W.g[5], W.L2);
+  std::swap(W.w, W.Cz);
+  op2_filter_deriv(e, ld_field(e, W.TH), W.THadv, W.gT[0], W.gT[1], W.L2);
+  std::swap(W.TH, W.THadv);
   // surface fluxes (Main.py:213-243)
   const int var = surface_variant(cf);
   double sfc = 0.0;
@@ -744,11 +734,7 @@ static int one_step(alfa_ctx* c) {
   for (int i = 0; i < 6; i++) std::swap(W.most[i], W.most_new[i]);
   const double* qz_step = (var <= 1) ? W.qz_plane : W.q2;
   // gradients (Main.py:275-290)
-  op_deriv_spec(e, W.ufft, W.g[0], W.g[3]);
-  op_deriv_spec(e, W.vfft, W.g[1], W.g[4]);
-  op_deriv_spec(e, W.wfft, W.g[2], W.g[5]);
   derivz_M(e, W.u, W.v, W.w, W.ustar, W.M, W.most[4], W.g[6], W.g[7], W.g[8]);
-  deriv_field_acc(e, ld_field(e, W.TH), W.gT[0], 0, W.gT[1], 0);
   derivz_TH(e, W.TH, W.ustar, qz_step, W.most[5], W.gT[2]);
   // advection (Main.py:301-311)
   advection(c, W.u, W.v, W.w, W.g[3], W.g[6], W.g[1], W.g[7], W.g[2], W.g[5], W.Cx, W.Cy, W.Cz);

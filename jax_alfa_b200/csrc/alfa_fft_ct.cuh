@@ -82,4 +82,82 @@ __device__ __forceinline__ void fft_ct(cd* buf, const cd* tw) {
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident ends of the same transform.  The first pass (NS = 1)
+// reads x[j + r*N/R] of column c for butterfly b = threadIdx.x + q*NT
+// (c = b % C, j = b / C) and the last pass writes X[j + r*NS_last] of the
+// same butterfly, so a kernel can load the first pass's inputs straight
+// from global memory into registers and store the last pass's outputs
+// straight from registers, skipping two trips through shared memory.
+// ---------------------------------------------------------------------------
+
+// the remaining-length product NS at which the last pass of length N starts
+__host__ __device__ constexpr int ct_last_ns(int N, int NS = 1) {
+  return NS * ct_radix(N / NS) >= N ? NS : ct_last_ns(N, NS * ct_radix(N / NS));
+}
+
+// butterflies per thread of the pass that starts at NS
+__host__ __device__ constexpr int ct_mb(int C, int N, int NS, int NT) {
+  return ((N / ct_radix(N / NS)) * C + NT - 1) / NT;
+}
+
+// First pass from registers v[q*R + r]; outputs go to buf.  The caller makes
+// sure no thread still reads buf.  Requires more than one pass.
+template <int S, int C, int N, int NT>
+__device__ __forceinline__ void ct_first_reg(cd* v, cd* __restrict__ buf) {
+  constexpr int R = ct_radix(N);
+  constexpr int B = (N / R) * C;
+  constexpr int MB = (B + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    if (B % NT == 0 || b < B) {
+      const int c = b % C;
+      const int j = b / C;
+      dftR<R, S>(v + q * R);
+#pragma unroll
+      for (int r = 0; r < R; r++) buf[(j * R + r) * C + c] = v[q * R + r];
+    }
+  }
+}
+
+// Passes that start at NS, up to but excluding the last one, in buf.
+template <int S, int C, int N, int NS, int NT>
+__device__ __forceinline__ void ct_mid_passes(cd* buf, const cd* tw) {
+  if constexpr (NS < ct_last_ns(N)) {
+    constexpr int R = ct_radix(N / NS);
+    __syncthreads();
+    ct_pass<R, S, C, N, NS, NT>(buf, tw);
+    ct_mid_passes<S, C, N, NS * R, NT>(buf, tw);
+  }
+}
+
+// Last pass from buf into registers v[q*R + r] = X[j + r*NS] (the caller
+// synchronises before).  Requires more than one pass.
+template <int S, int C, int N, int NT>
+__device__ __forceinline__ void ct_last_reg(const cd* __restrict__ buf, const cd* __restrict__ tw,
+                                            cd* v) {
+  constexpr int NS = ct_last_ns(N);
+  constexpr int R = N / NS;
+  constexpr int B = NS * C;
+  constexpr int MB = (B + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    if (B % NT == 0 || b < B) {
+      const int c = b % C;
+      const int j = b / C;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[q * R + r] = buf[(j + r * NS) * C + c];
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        cd w = __ldg(&tw[j * r]);
+        if (S > 0) w.y = -w.y;
+        v[q * R + r] = cmul(v[q * R + r], w);
+      }
+      dftR<R, S>(v + q * R);
+    }
+  }
+}
+
 }  // namespace alfa

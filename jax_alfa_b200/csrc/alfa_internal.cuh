@@ -61,6 +61,19 @@ struct XOut {
   FftPlan inv;
 };
 
+// 1-D line operators (k_line): a transform along x or y of real fields,
+// two real z columns packed per complex line.  Maps act on the full packed
+// spectrum of length n_in and produce n_out entries.
+enum LineMap { LM_IDENT = 0, LM_TRUNC, LM_DERIV, LM_TRUNC_DERIV, LM_PAD, LM_UNPAD };
+
+struct LineOut {
+  int map;
+  int cut;          // LM_TRUNC / LM_TRUNC_DERIV: keep k < cut or k >= n - cut + 1
+  double scale;     // applied to the inverse transform (1/n_out, times any extra factor)
+  int accumulate;   // 1: dst += result
+  double* dst;
+};
+
 struct Engine;
 
 // ---------------------------------------------------------------------------
@@ -123,6 +136,18 @@ void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const
               int nout, const XOut* outs, int Kgrid);
 void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
                   double* out, int accumulate);
+
+// 1-D line passes (alfa_spectral.cu).  axis 0: lines along x of a field
+// (X, Y, nz); axis 1: lines along y.  X/Y of the input field; the output
+// field has n_out in place of the transformed extent.
+void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
+                 int nout, const LineOut* outs);
+// separable spectral operators on real fields
+void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
+                      double* scratch2);  // explicit filter and its x/y derivatives
+void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int accy);
+void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch);
+void op2_unpad(Engine& e, const Loader& L_pad, double* out, double* scratch);
 
 // composite transforms on regular/padded grids
 Loader ld_field(const Engine& e, const double* a);
