@@ -8,8 +8,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalfa.so")
-SOURCES = ["alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu", "alfa_noalloc.cu"]
-HEADERS = ["alfa_fft.cuh", "alfa_fft_ct.cuh", "alfa_internal.cuh", "alfa_physics.cuh"]
+SOURCES = ["alfa_line.cu", "alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu",
+           "alfa_noalloc.cu"]
+HEADERS = ["alfa_fft.cuh", "alfa_fft_ct.cuh", "alfa_internal.cuh", "alfa_physics.cuh",
+           "alfa_tile.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -39,19 +41,25 @@ def build(force=False, verbose=False):
     """Compile every CUDA source into jax_alfa_b200/libalfa.so."""
     if not force and not _stale():
         return LIB
-    objs = []
-    for src in SOURCES:
+    objs, procs = [], []
+    for src in SOURCES:  # translation units compile concurrently
         obj = os.path.join(CSRC, src.replace(".cu", ".o"))
         cmd = [nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
-        if verbose:
-            sys.stderr.write(r.stderr)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                            stderr=subprocess.PIPE, text=True)))
         objs.append(obj)
+    failed = []
+    for src, pr in procs:
+        _, err = pr.communicate()
+        if pr.returncode != 0:
+            failed.append(f"nvcc failed on {src}:\n{err}")
+        elif verbose:
+            sys.stderr.write(err)
+    if failed:
+        raise RuntimeError("\n".join(failed))
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs,
            "-o", LIB, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,0 +1,798 @@
+// 1-D line passes along x or y of z-fastest real fields: the separable
+// forms of the reference's spectral operators (explicit filter with its
+// derivatives, derivatives, 3/2-rule pad and unpad), each a forward
+// transform of 16-level z runs, a map, and an inverse transform.
+#include <cmath>
+
+#include "alfa_tile.cuh"
+
+namespace alfa {
+
+// ---------------------------------------------------------------------------
+// k_line: 1-D spectral operator along x or y on real fields.  A CTA takes one
+// line index f (an x row for y lines, a y column for x lines) and 16
+// consecutive z levels packed as 8 complex lines, transforms them forward,
+// and for each output applies a map to the full packed spectrum, transforms
+// back and stores the real pair.  Packing two real lines in one complex
+// transform is exact for these maps because each is a real operator
+// (Hermitian-symmetric: truncation, i*k with the Nyquist zeroed, the 3/2-rule
+// pad with the Nyquist repeated, unpad).
+// ---------------------------------------------------------------------------
+struct LineArgs {
+  Loader L;
+  int n_in, n_out;
+  long long fs_in, rs_in, fs_out, rs_out;  // line and row strides (elements)
+  int nz;
+  int nouts;
+  LineOut out[3];
+  FftPlan pin, pout;
+};
+
+template <int KIND>
+__device__ __forceinline__ void line_load(const LineArgs& a, long long f, int z0, int n, cd* S) {
+  const Loader& L = a.L;
+  const int nz = a.nz;
+  const int total = n * YC;
+  const bool vec = (KIND == LD_FIELD) && ((nz & 1) == 0);
+  for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
+    cd v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      v[u] = make_double2(0.0, 0.0);
+      if (t < total) {
+        const int r = t / YC, c = t % YC;
+        const int z = z0 + 2 * c;
+        const size_t i = (size_t)(f * a.fs_in + r * a.rs_in) + z;
+        if (vec && z + 1 < nz) {
+          v[u] = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+        } else {
+          if (z < nz) v[u].x = ldv<KIND>(L, i, z);
+          if (z + 1 < nz) v[u].y = ldv<KIND>(L, i + 1, z + 1);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t < total) S[t] = v[u];
+    }
+  }
+}
+
+__device__ __forceinline__ cd line_map(const LineOut& o, const cd* S, int k, int c, int n, int m) {
+  auto deriv = [&](cd v) -> cd {
+    const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
+    const double q = (double)kk;
+    return make_double2(-(q * v.y), q * v.x);
+  };
+  switch (o.map) {
+    case LM_IDENT:
+      return S[k * YC + c];
+    case LM_TRUNC:
+      return (k < o.cut || k >= n - o.cut + 1) ? S[k * YC + c] : make_double2(0.0, 0.0);
+    case LM_DERIV:
+      return deriv(S[k * YC + c]);
+    case LM_TRUNC_DERIV:
+      return (k < o.cut || k >= n - o.cut + 1) ? deriv(S[k * YC + c]) : make_double2(0.0, 0.0);
+    case LM_PAD: {  // n -> m = 3n/2, Nyquist row repeated (Dealiasing.py:67-73)
+      const int h = n / 2;
+      if (k <= h) return S[k * YC + c];
+      if (k >= m - h) return S[(k - m + n) * YC + c];
+      return make_double2(0.0, 0.0);
+    }
+    default: {  // LM_UNPAD: n = 3m/2 -> m, Nyquist dropped (Dealiasing.py:102-109)
+      const int h = m / 2;
+      if (k < h) return S[k * YC + c];
+      if (k == h) return make_double2(0.0, 0.0);
+      return S[(k - m + n) * YC + c];
+    }
+  }
+}
+
+template <int NIN, int NOUT>
+__global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(), 1)
+    k_line(LineArgs a) {
+  constexpr int NT = tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>();
+  extern __shared__ cd sm[];
+  const int n = NIN > 0 ? NIN : a.n_in;
+  const int m = NOUT > 0 ? NOUT : a.n_out;
+  const int nz = a.nz;
+  const int z0 = blockIdx.x * (2 * YC);
+  const long long f = blockIdx.y;
+  cd* S = sm;
+  cd* W = sm + n * YC;
+  switch (a.L.kind) {
+    case LD_FIELD: line_load<LD_FIELD>(a, f, z0, n, S); break;
+    case LD_MUL: line_load<LD_MUL>(a, f, z0, n, S); break;
+    case LD_MUL3: line_load<LD_MUL3>(a, f, z0, n, S); break;
+    case LD_PRESSURE_R: line_load<LD_PRESSURE_R>(a, f, z0, n, S); break;
+    case LD_ADV_XY: line_load<LD_ADV_XY>(a, f, z0, n, S); break;
+    case LD_ADV_Z: line_load<LD_ADV_Z>(a, f, z0, n, S); break;
+    case LD_SCALAR_ADV: line_load<LD_SCALAR_ADV>(a, f, z0, n, S); break;
+    case LD_STRESS_UVP: line_load<LD_STRESS_UVP>(a, f, z0, n, S); break;
+    case LD_STRESS_W: line_load<LD_STRESS_W>(a, f, z0, n, S); break;
+    case LD_W_SXX: line_load<LD_W_SXX>(a, f, z0, n, S); break;
+    case LD_THZ: line_load<LD_THZ>(a, f, z0, n, S); break;
+    default: line_load<LD_MUL_THZ>(a, f, z0, n, S); break;
+  }
+  tile_fft<-1, YC, NIN, NT>(S, a.pin);
+  const bool pair = (nz & 1) == 0;
+  for (int oi = 0; oi < a.nouts; oi++) {
+    const LineOut& o = a.out[oi];
+    for (int t = threadIdx.x; t < m * YC; t += blockDim.x) {
+      const int k = t / YC, c = t % YC;
+      W[t] = line_map(o, S, k, c, n, m);
+    }
+    tile_fft<+1, YC, NOUT, NT>(W, a.pout);
+    const double sc = o.scale;
+    if (o.accumulate) {
+      for (int t0 = threadIdx.x; t0 < m * YC; t0 += U * blockDim.x) {
+        double2 prev[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int t = t0 + u * blockDim.x;
+          const int r = t / YC, c = t % YC;
+          const int z = z0 + 2 * c;
+          const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
+          prev[u] = make_double2(0.0, 0.0);
+          if (t < m * YC) {
+            if (pair && z < nz) {
+              prev[u] = *reinterpret_cast<const double2*>(o.dst + i);
+            } else {
+              if (z < nz) prev[u].x = o.dst[i];
+              if (z + 1 < nz) prev[u].y = o.dst[i + 1];
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int t = t0 + u * blockDim.x;
+          if (t >= m * YC) continue;
+          const int r = t / YC, c = t % YC;
+          const int z = z0 + 2 * c;
+          const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
+          const cd v = W[t];
+          const double2 w = make_double2(prev[u].x + sc * v.x, prev[u].y + sc * v.y);
+          if (pair && z < nz) {
+            *reinterpret_cast<double2*>(o.dst + i) = w;
+          } else {
+            if (z < nz) o.dst[i] = w.x;
+            if (z + 1 < nz) o.dst[i + 1] = w.y;
+          }
+        }
+      }
+    } else {
+      for (int t = threadIdx.x; t < m * YC; t += blockDim.x) {
+        const int r = t / YC, c = t % YC;
+        const int z = z0 + 2 * c;
+        const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
+        const cd v = W[t];
+        if (pair && z < nz) {
+          *reinterpret_cast<double2*>(o.dst + i) = make_double2(sc * v.x, sc * v.y);
+        } else {
+          if (z < nz) o.dst[i] = sc * v.x;
+          if (z + 1 < nz) o.dst[i + 1] = sc * v.y;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_line_rr: k_line for compile-time lengths with register-resident ends.
+// The forward transform's first pass takes its inputs straight from global
+// memory (every thread issues all of its loads before the first butterfly)
+// and each inverse transform's last pass stores straight from registers.
+// When input and output lengths match and the first and last radix of the
+// transform agree (n = 256 = 16 x 16), the forward spectrum also stays in
+// registers: the thread that ends the forward transform with bins
+// j + NS*r holds exactly the inputs of the inverse's first butterfly, so the
+// map is applied in registers and shared memory carries one exchange per
+// transform.  Otherwise each inverse reads its first-pass inputs from the
+// forward spectrum in shared memory through the map.  GEN: the input is any
+// Loader kind (else a plain field, with a leaner register budget).
+// ---------------------------------------------------------------------------
+template <int C, int NIN, int NOUT>
+__host__ __device__ constexpr int line_threads() {
+  return ct_threads(C, NIN) > ct_threads(C, NOUT) ? ct_threads(C, NIN) : ct_threads(C, NOUT);
+}
+
+// value pair (z, z+1) of the loader at linear index i
+template <int KIND>
+__device__ __forceinline__ cd load_pair(const Loader& L, size_t i, int z, int nz) {
+  cd t = make_double2(0.0, 0.0);
+  if (KIND == LD_FIELD && (nz & 1) == 0) {
+    if (z < nz) t = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+  } else {
+    if (z < nz) t.x = ldv<KIND>(L, i, z);
+    if (z + 1 < nz) t.y = ldv<KIND>(L, i + 1, z + 1);
+  }
+  return t;
+}
+
+// store (or accumulate) a scaled value pair at linear index i
+__device__ __forceinline__ void store_pair(const LineOut& o, size_t i, int z, int nz, cd v) {
+  if (z >= nz) return;
+  double* __restrict__ dst = o.dst;
+  double2 w = make_double2(o.scale * v.x, o.scale * v.y);
+  if ((nz & 1) == 0) {
+    double2* p = reinterpret_cast<double2*>(dst + i);
+    if (o.accumulate) {
+      const double2 pv = *p;
+      w.x += pv.x;
+      w.y += pv.y;
+    }
+    *p = w;
+  } else {
+    if (o.accumulate) {
+      w.x += dst[i];
+      if (z + 1 < nz) w.y += dst[i + 1];
+    }
+    dst[i] = w.x;
+    if (z + 1 < nz) dst[i + 1] = w.y;
+  }
+}
+
+// first-pass gather: v[q*R + r] = (x, x') at row j + r*NR of line c
+template <int KIND, int C, int N, int NT>
+__device__ __forceinline__ void line_gather(const LineArgs& a, long long f, int z0, cd* v) {
+  constexpr int R = ct_radix(N);
+  constexpr int NR = N / R;
+  constexpr int B = NR * C;
+  constexpr int MB = (B + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 2 * c;
+    const bool ok = (B % NT == 0 || b < B);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const size_t i = (size_t)(f * a.fs_in + (long long)(j + r * NR) * a.rs_in) + z;
+      v[q * R + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
+    }
+  }
+}
+
+template <int C, int N, int NT>
+__device__ __forceinline__ void line_gather_any(const LineArgs& a, long long f, int z0, cd* v) {
+  switch (a.L.kind) {
+    case LD_FIELD: line_gather<LD_FIELD, C, N, NT>(a, f, z0, v); break;
+    case LD_MUL: line_gather<LD_MUL, C, N, NT>(a, f, z0, v); break;
+    case LD_MUL3: line_gather<LD_MUL3, C, N, NT>(a, f, z0, v); break;
+    case LD_PRESSURE_R: line_gather<LD_PRESSURE_R, C, N, NT>(a, f, z0, v); break;
+    case LD_ADV_XY: line_gather<LD_ADV_XY, C, N, NT>(a, f, z0, v); break;
+    case LD_ADV_Z: line_gather<LD_ADV_Z, C, N, NT>(a, f, z0, v); break;
+    case LD_SCALAR_ADV: line_gather<LD_SCALAR_ADV, C, N, NT>(a, f, z0, v); break;
+    case LD_STRESS_UVP: line_gather<LD_STRESS_UVP, C, N, NT>(a, f, z0, v); break;
+    case LD_STRESS_W: line_gather<LD_STRESS_W, C, N, NT>(a, f, z0, v); break;
+    case LD_W_SXX: line_gather<LD_W_SXX, C, N, NT>(a, f, z0, v); break;
+    case LD_THZ: line_gather<LD_THZ, C, N, NT>(a, f, z0, v); break;
+    default: line_gather<LD_MUL_THZ, C, N, NT>(a, f, z0, v); break;
+  }
+}
+
+// store (or accumulate) v[q*R + r] = value at row j + r*STEP of line c
+template <int C, int R, int STEP, int B, int NT>
+__device__ __forceinline__ void line_scatter(const LineArgs& a, const LineOut& o, long long f,
+                                             int z0, const cd* v) {
+  constexpr int MB = (B + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    if (!(B % NT == 0 || b < B)) continue;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 2 * c;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const size_t i = (size_t)(f * a.fs_out + (long long)(j + r * STEP) * a.rs_out) + z;
+      store_pair(o, i, z, a.nz, v[q * R + r]);
+    }
+  }
+}
+
+// same-length maps applied to bin k of a length-n spectrum (as line_map)
+__device__ __forceinline__ cd map_reg(const LineOut& o, cd v, int k, int n) {
+  if ((o.map == LM_TRUNC || o.map == LM_TRUNC_DERIV) && !(k < o.cut || k >= n - o.cut + 1))
+    return make_double2(0.0, 0.0);
+  if (o.map == LM_DERIV || o.map == LM_TRUNC_DERIV) {
+    const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
+    const double q = (double)kk;
+    return make_double2(-(q * v.y), q * v.x);
+  }
+  return v;
+}
+
+template <int N, int NT>
+__host__ __device__ constexpr bool line_reg_path() {
+  return N > 16 && ct_radix(N) == N / ct_last_ns(N) &&
+         ct_mb(YC, N, 1, NT) == ct_mb(YC, N, ct_last_ns(N), NT);
+}
+
+template <int NIN, int NOUT, bool GEN>
+__global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
+    k_line_rr(LineArgs a) {
+  constexpr int C = YC;
+  constexpr int NT = line_threads<C, NIN, NOUT>();
+  constexpr int NMAX = NIN > NOUT ? NIN : NOUT;
+  constexpr bool REG = (NIN == NOUT) && line_reg_path<NIN, NT>();
+  extern __shared__ cd sm[];
+  cd* S = sm;
+  const int z0 = blockIdx.x * (2 * C);
+  const long long f = blockIdx.y;
+  if constexpr (REG) {
+    constexpr int R = ct_radix(NIN);
+    constexpr int NSL = ct_last_ns(NIN);
+    constexpr int MB = ct_mb(C, NIN, 1, NT);
+    cd X[MB * R];
+    {
+      cd v[MB * R];
+      if constexpr (GEN) line_gather_any<C, NIN, NT>(a, f, z0, v);
+      else line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v);
+      ct_first_reg<-1, C, NIN, NT>(v, S);
+      ct_mid_passes<-1, C, NIN, R, NT>(S, a.pin.tw);
+      __syncthreads();
+      ct_last_reg<-1, C, NIN, NT>(S, a.pin.tw, X);
+    }
+    for (int oi = 0; oi < a.nouts; oi++) {
+      const LineOut& o = a.out[oi];
+      cd v[MB * R];
+#pragma unroll
+      for (int q = 0; q < MB; q++) {
+        const int j = (threadIdx.x + q * NT) / C;
+#pragma unroll
+        for (int r = 0; r < R; r++) v[q * R + r] = map_reg(o, X[q * R + r], j + NSL * r, NIN);
+      }
+      __syncthreads();  // every read of S by the previous pass is done
+      ct_first_reg<+1, C, NOUT, NT>(v, S);
+      ct_mid_passes<+1, C, NOUT, R, NT>(S, a.pout.tw);
+      __syncthreads();
+      cd u[MB * R];
+      ct_last_reg<+1, C, NOUT, NT>(S, a.pout.tw, u);
+      line_scatter<C, R, NSL, NSL * C, NT>(a, o, f, z0, u);
+    }
+  } else {
+    cd* Wb = a.nouts > 1 ? sm + NMAX * C : sm;
+    // forward transform of the NIN-line tile into S
+    {
+      constexpr int R = ct_radix(NIN);
+      constexpr int MB = ct_mb(C, NIN, 1, NT);
+      cd v[MB * R];
+      if constexpr (GEN) line_gather_any<C, NIN, NT>(a, f, z0, v);
+      else line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v);
+      if constexpr (R == NIN) {
+        if (threadIdx.x < C) {
+          dftR<R, -1>(v);
+#pragma unroll
+          for (int r = 0; r < R; r++) S[r * C + threadIdx.x] = v[r];
+        }
+      } else {
+        ct_first_reg<-1, C, NIN, NT>(v, S);
+        ct_passes<-1, C, NIN, R, NT>(S, a.pin.tw);
+      }
+      __syncthreads();
+    }
+    // outputs: map, inverse transform, store
+    for (int oi = 0; oi < a.nouts; oi++) {
+      const LineOut& o = a.out[oi];
+      constexpr int R = ct_radix(NOUT);
+      constexpr int NR = NOUT / R;
+      constexpr int B = NR * C;
+      constexpr int MB = ct_mb(C, NOUT, 1, NT);
+      cd v[MB * R];
+#pragma unroll
+      for (int q = 0; q < MB; q++) {
+        const int b = threadIdx.x + q * NT;
+        const int c = b % C;
+        const int j = b / C;
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          v[q * R + r] = (B % NT == 0 || b < B) ? line_map(o, S, j + r * NR, c, NIN, NOUT)
+                                                : make_double2(0.0, 0.0);
+      }
+      if constexpr (R == NOUT) {
+#pragma unroll
+        for (int q = 0; q < MB; q++) dftR<R, +1>(v + q * R);
+        line_scatter<C, R, 1, C, NT>(a, o, f, z0, v);
+      } else {
+        __syncthreads();  // Wb may alias S
+        ct_first_reg<+1, C, NOUT, NT>(v, Wb);
+        ct_mid_passes<+1, C, NOUT, R, NT>(Wb, a.pout.tw);
+        __syncthreads();
+        constexpr int NSL = ct_last_ns(NOUT);
+        constexpr int RL = NOUT / NSL;
+        constexpr int ML = ct_mb(C, NOUT, NSL, NT);
+        cd u[ML * RL];
+        ct_last_reg<+1, C, NOUT, NT>(Wb, a.pout.tw, u);
+        line_scatter<C, RL, NSL, NSL * C, NT>(a, o, f, z0, u);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3/2-rule pad and unpad by phases.  With n = 2L and m = 3L, output sample
+// t = 3s + p (p = 0, 1, 2) of the length-m inverse transform of a padded
+// spectrum Y is the length-L inverse transform of the folded spectrum
+//   Z_p[q] = sum_{k = q mod L} Y[k] w_m^{kp}.
+// The pad spectrum (Y[k] = X[k] for k <= L and k >= 2L, the Nyquist bin X[L]
+// repeated at both ends, zero between) folds to
+//   Z_p[0] = X[0] + X[L] (w_3^p + w_3^{2p}),
+//   Z_p[q] = w_m^{qp} (X[q] + w_3^{2p} X[q + L]),  0 < q < L,
+// and the forward transform of a length-m line (decimated the same way into
+// F_p = DFT_L of x[3s + p]) truncated to n bins (Nyquist bin zeroed) is
+//   X[q] = sum_p w_m^{-qp} F_p[q],
+//   X[L + q] = sum_p w_m^{-qp} w_3^{-2p} F_p[q]  (q > 0),  X[L] = 0.
+// For n = 256 (= 16 x 16) a thread that ends the length-n forward transform
+// holds bins j + 16r (r < 16), i.e. X[q] and X[q + L] for q = j + 16r',
+// r' < 8: the folds are thread-local and each length-128 phase transform
+// is one radix-8 pass in registers, one shared-memory exchange and one
+// radix-16 pass.  The length-m transform and its radix-3 pass disappear.
+// ---------------------------------------------------------------------------
+template <int N>
+__host__ __device__ constexpr bool pad3_ok() {
+  return ct_last_ns(N) == ct_radix(N) && ct_radix(N) * ct_radix(N) == N && ct_radix(N) >= 4 &&
+         ct_mb(YC, N, 1, ct_threads(YC, N)) == 1;
+}
+
+__device__ __forceinline__ cd cconj(cd a) { return make_double2(a.x, -a.y); }
+
+template <int N, bool GEN>
+__global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
+  constexpr int C = YC;
+  constexpr int NT = ct_threads(C, N);
+  constexpr int R = ct_radix(N);   // both passes of the length-N transform
+  constexpr int L = N / 2;
+  constexpr int RA = R / 2;        // first radix of the length-L phase transforms
+  constexpr int RB = L / RA;       // their second radix (= R)
+  static_assert(pad3_ok<N>() && RB == R, "pad3 layout");
+  extern __shared__ cd sm[];
+  cd* S = sm;  // forward exchange, then three phase tiles of L x C
+  const int z0 = blockIdx.x * (2 * C);
+  const long long f = blockIdx.y;
+  const LineOut& o = a.out[0];
+  const cd* twN = a.pin.tw;   // exp(-2 pi i q / N)
+  const cd* twM = a.pout.tw;  // exp(-2 pi i q / 3L)
+  const int c = threadIdx.x % C;
+  const int j = threadIdx.x / C;  // 0 .. R-1
+  cd X[R];
+  {
+    cd v[R];
+    if constexpr (GEN) line_gather_any<C, N, NT>(a, f, z0, v);
+    else line_gather<LD_FIELD, C, N, NT>(a, f, z0, v);
+    ct_first_reg<-1, C, N, NT>(v, S);
+    __syncthreads();
+    ct_last_reg<-1, C, N, NT>(S, twN, X);  // X[r] = bin j + R r
+  }
+  __syncthreads();
+  const cd w3a = cconj(__ldg(&twM[2 * L]));  // w_3^{2} (inverse sign)
+  const cd w3b = cconj(__ldg(&twM[L]));      // w_3^{4} = w_3
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    cd z[RA];
+#pragma unroll
+    for (int r = 0; r < RA; r++) {
+      const int k = j + R * r;
+      const cd lo = X[r], hi = X[r + RA];
+      cd t;
+      if (p == 0) {
+        t = (k == 0) ? make_double2(lo.x + 2.0 * hi.x, lo.y + 2.0 * hi.y) : cadd(lo, hi);
+      } else if (k == 0) {
+        t = csub(lo, hi);
+      } else {
+        t = cmul(cadd(lo, cmul(p == 1 ? w3a : w3b, hi)), cconj(__ldg(&twM[k * p])));
+      }
+      z[r] = t;
+    }
+    dftR<RA, +1>(z);
+    cd* P = S + p * L * C;
+#pragma unroll
+    for (int r = 0; r < RA; r++) P[(j * RA + r) * C + c] = z[r];
+  }
+  __syncthreads();
+  constexpr int BB = 3 * RA * C;
+  constexpr int MBB = (BB + NT - 1) / NT;
+  const int nz = a.nz;
+#pragma unroll
+  for (int q = 0; q < MBB; q++) {
+    const int b = threadIdx.x + q * NT;
+    if (!(BB % NT == 0 || b < BB)) continue;
+    const int p = b / (RA * C);
+    const int bb = b % (RA * C);
+    const int cc = bb % C;
+    const int jj = bb / C;  // 0 .. RA-1
+    const cd* P = S + p * L * C;
+    cd v[RB];
+#pragma unroll
+    for (int r = 0; r < RB; r++) v[r] = P[(jj + r * RA) * C + cc];
+#pragma unroll
+    for (int r = 1; r < RB; r++) v[r] = cmul(v[r], cconj(__ldg(&twM[3 * jj * r])));
+    dftR<RB, +1>(v);
+    const int z = z0 + 2 * cc;
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      const int row = 3 * (jj + RA * r) + p;
+      const size_t i = (size_t)(f * a.fs_out + (long long)row * a.rs_out) + z;
+      store_pair(o, i, z, nz, v[r]);
+    }
+  }
+}
+
+// gather of the unpad phase transforms' first pass: butterfly (p, jj, c),
+// v[q*RB + r] = x[3 (jj + RA r) + p] of line c
+template <int KIND, int C, int RA, int RB, int NT>
+__device__ __forceinline__ void phase_gather(const LineArgs& a, long long f, int z0, cd* v) {
+  constexpr int BB = 3 * RA * C;
+  constexpr int MBB = (BB + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MBB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const bool ok = (BB % NT == 0 || b < BB);
+    const int p = b / (RA * C);
+    const int bb = b % (RA * C);
+    const int c = bb % C;
+    const int jj = bb / C;
+    const int z = z0 + 2 * c;
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      const long long row = 3 * (jj + RA * r) + p;
+      const size_t i = (size_t)(f * a.fs_in + row * a.rs_in) + z;
+      v[q * RB + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
+    }
+  }
+}
+
+template <int C, int RA, int RB, int NT>
+__device__ __forceinline__ void phase_gather_any(const LineArgs& a, long long f, int z0, cd* v) {
+  switch (a.L.kind) {
+    case LD_FIELD: phase_gather<LD_FIELD, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_MUL: phase_gather<LD_MUL, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_MUL3: phase_gather<LD_MUL3, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_PRESSURE_R: phase_gather<LD_PRESSURE_R, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_ADV_XY: phase_gather<LD_ADV_XY, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_ADV_Z: phase_gather<LD_ADV_Z, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_SCALAR_ADV: phase_gather<LD_SCALAR_ADV, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_STRESS_UVP: phase_gather<LD_STRESS_UVP, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_STRESS_W: phase_gather<LD_STRESS_W, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_W_SXX: phase_gather<LD_W_SXX, C, RA, RB, NT>(a, f, z0, v); break;
+    case LD_THZ: phase_gather<LD_THZ, C, RA, RB, NT>(a, f, z0, v); break;
+    default: phase_gather<LD_MUL_THZ, C, RA, RB, NT>(a, f, z0, v); break;
+  }
+}
+
+template <int N, bool GEN>
+__global__ void __launch_bounds__(ct_threads(YC, N)) k_unpad3(LineArgs a) {
+  constexpr int C = YC;
+  constexpr int NT = ct_threads(C, N);
+  constexpr int R = ct_radix(N);   // both passes of the length-N inverse
+  constexpr int L = N / 2;
+  constexpr int RA = R / 2;        // last radix of the length-L phase transforms
+  constexpr int RB = L / RA;       // their first radix (= R)
+  static_assert(pad3_ok<N>() && RB == R, "unpad3 layout");
+  constexpr int BB = 3 * RA * C;
+  constexpr int MBB = (BB + NT - 1) / NT;
+  extern __shared__ cd sm[];
+  cd* S = sm;  // three phase tiles of L x C, then the inverse exchange
+  const int z0 = blockIdx.x * (2 * C);
+  const long long f = blockIdx.y;
+  const LineOut& o = a.out[0];
+  const cd* twM = a.pin.tw;   // exp(-2 pi i q / 3L)
+  const cd* twN = a.pout.tw;  // exp(-2 pi i q / N)
+  {
+    cd v[MBB * RB];
+    if constexpr (GEN) phase_gather_any<C, RA, RB, NT>(a, f, z0, v);
+    else phase_gather<LD_FIELD, C, RA, RB, NT>(a, f, z0, v);
+#pragma unroll
+    for (int q = 0; q < MBB; q++) {
+      const int b = threadIdx.x + q * NT;
+      if (!(BB % NT == 0 || b < BB)) continue;
+      const int p = b / (RA * C);
+      const int bb = b % (RA * C);
+      const int cc = bb % C;
+      const int jj = bb / C;
+      dftR<RB, -1>(v + q * RB);
+      cd* P = S + p * L * C;
+#pragma unroll
+      for (int r = 0; r < RB; r++) P[(jj * RB + r) * C + cc] = v[q * RB + r];
+    }
+  }
+  __syncthreads();
+  const int c = threadIdx.x % C;
+  const int j = threadIdx.x / C;  // 0 .. R-1
+  cd out[R];
+  {
+    cd F[3][RA];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const cd* P = S + p * L * C;
+#pragma unroll
+      for (int r = 0; r < RA; r++) F[p][r] = P[(j + r * RB) * C + c];
+#pragma unroll
+      for (int r = 1; r < RA; r++) F[p][r] = cmul(F[p][r], __ldg(&twM[3 * j * r]));
+      dftR<RA, -1>(F[p]);  // F[p][r] = F_p[j + R r]
+    }
+    const cd w3a = __ldg(&twM[2 * L]);  // w_3^{-2}
+    const cd w3b = __ldg(&twM[L]);      // w_3^{-4} = w_3^{-1}
+#pragma unroll
+    for (int r = 0; r < RA; r++) {
+      const int k = j + R * r;
+      const cd g0 = F[0][r];
+      const cd g1 = cmul(F[1][r], __ldg(&twM[k]));
+      const cd g2 = cmul(F[2][r], __ldg(&twM[2 * k]));
+      out[r] = cadd(cadd(g0, g1), g2);
+      out[r + RA] = (k == 0) ? make_double2(0.0, 0.0)
+                             : cadd(cadd(g0, cmul(w3a, g1)), cmul(w3b, g2));
+    }
+  }
+  __syncthreads();  // phase tiles fully read
+  ct_first_reg<+1, C, N, NT>(out, S);
+  __syncthreads();
+  cd u[R];
+  ct_last_reg<+1, C, N, NT>(S, twN, u);
+  line_scatter<C, R, R, R * C, NT>(a, o, f, z0, u);
+}
+
+template <int NIN, int NOUT>
+static void line_n(Engine& e, const LineArgs& a, int F) {
+  dim3 g((a.nz + 2 * YC - 1) / (2 * YC), F);
+  if constexpr (NIN > 0) {
+    const int nmax = NIN > NOUT ? NIN : NOUT;
+    constexpr int nt = line_threads<YC, NIN, NOUT>();
+    constexpr bool reg = (NIN == NOUT) && line_reg_path<NIN, nt>();
+    const size_t smem = (size_t)(nmax + (!reg && a.nouts > 1 ? NOUT : 0)) * YC * sizeof(cd);
+    if (a.L.kind == LD_FIELD) {
+      set_smem((const void*)k_line_rr<NIN, NOUT, false>, smem);
+      k_line_rr<NIN, NOUT, false><<<g, nt, smem, e.stream>>>(a);
+    } else {
+      set_smem((const void*)k_line_rr<NIN, NOUT, true>, smem);
+      k_line_rr<NIN, NOUT, true><<<g, nt, smem, e.stream>>>(a);
+    }
+  } else {
+    const size_t smem = (size_t)(a.n_in + a.n_out) * YC * sizeof(cd);
+    set_smem((const void*)k_line<0, 0>, smem);
+    const int nt = inplace_threads(YC, a.n_in > a.n_out ? a.n_in : a.n_out);
+    k_line<0, 0><<<g, nt, smem, e.stream>>>(a);
+  }
+}
+
+// 3/2-rule pad (PAD) or unpad by phases, n = N
+template <int N, bool PAD>
+static void phase_n(Engine& e, const LineArgs& a, int F) {
+  dim3 g((a.nz + 2 * YC - 1) / (2 * YC), F);
+  constexpr int nt = ct_threads(YC, N);
+  const size_t smem = (size_t)(3 * N / 2) * YC * sizeof(cd);
+  const bool gen = a.L.kind != LD_FIELD;
+  if (PAD) {
+    if (gen) {
+      set_smem((const void*)k_pad3<N, true>, smem);
+      k_pad3<N, true><<<g, nt, smem, e.stream>>>(a);
+    } else {
+      set_smem((const void*)k_pad3<N, false>, smem);
+      k_pad3<N, false><<<g, nt, smem, e.stream>>>(a);
+    }
+  } else {
+    if (gen) {
+      set_smem((const void*)k_unpad3<N, true>, smem);
+      k_unpad3<N, true><<<g, nt, smem, e.stream>>>(a);
+    } else {
+      set_smem((const void*)k_unpad3<N, false>, smem);
+      k_unpad3<N, false><<<g, nt, smem, e.stream>>>(a);
+    }
+  }
+}
+
+static const FftPlan& plan_for(const Engine& e, int n) {
+  if (n == e.nx) return e.pnx;
+  if (n == e.ny) return e.pny;
+  if (n == e.mx) return e.pmx;
+  return e.pmy;
+}
+
+void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
+                 int nout, const LineOut* outs) {
+  LineArgs a;
+  a.L = L;
+  a.n_in = n_in;
+  a.n_out = n_out;
+  a.nz = L.nz;
+  const long long nz = L.nz;
+  int F;
+  if (axis == 0) {  // x lines of (X=n_in, Y, nz) -> (n_out, Y, nz)
+    a.fs_in = nz;
+    a.rs_in = (long long)Y * nz;
+    a.fs_out = nz;
+    a.rs_out = (long long)Y * nz;
+    F = Y;
+  } else {  // y lines of (X, Y=n_in, nz) -> (X, n_out, nz)
+    a.fs_in = (long long)n_in * nz;
+    a.rs_in = nz;
+    a.fs_out = (long long)n_out * nz;
+    a.rs_out = nz;
+    F = X;
+  }
+  a.nouts = nout;
+  for (int i = 0; i < nout; i++) a.out[i] = outs[i];
+  a.pin = plan_for(e, n_in);
+  a.pout = plan_for(e, n_out);
+  ::alfa::note_launch();
+  if (nout == 1 && outs[0].map == LM_PAD && n_in == 256 && n_out == 384) {
+    phase_n<256, true>(e, a, F);
+    return;
+  }
+  if (nout == 1 && outs[0].map == LM_UNPAD && n_in == 384 && n_out == 256) {
+    phase_n<256, false>(e, a, F);
+    return;
+  }
+#define ALFA_CASE(p, q)               \
+  if (n_in == p && n_out == q) {      \
+    line_n<p, q>(e, a, F);            \
+    return;                           \
+  }
+  ALFA_X_PAIRS(ALFA_CASE)
+#undef ALFA_CASE
+  line_n<0, 0>(e, a, F);
+}
+
+static LineOut lo(int map, double* dst, double scale, int cut = 0, int acc = 0) {
+  LineOut o;
+  o.map = map;
+  o.cut = cut;
+  o.scale = scale;
+  o.accumulate = acc;
+  o.dst = dst;
+  return o;
+}
+
+// Filtering_Explicit followed by Derivxy in x and y (Filtering.py:50-89,
+// Derivatives.py:161-182), as separable passes: x pass (filter, and filter +
+// d/dx), then y passes.  scratch2: two N-sized fields.
+void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
+                      double* scratch2) {
+  double* sx = scratch2;
+  double* sdx = scratch2 + e.N();
+  const double ix = 1.0 / e.nx, iy = 1.0 / e.ny;
+  LineOut ox[2] = {lo(LM_TRUNC, sx, ix, e.cut_e[0]), lo(LM_TRUNC_DERIV, sdx, ix, e.cut_e[0])};
+  launch_line(e, 0, L, e.nx, e.ny, e.nx, e.nx, dx ? 2 : 1, ox);
+  LineOut oy[2] = {lo(LM_TRUNC, f, iy, e.cut_e[1]), lo(LM_TRUNC_DERIV, dy, iy, e.cut_e[1])};
+  launch_line(e, 1, ld_field(e, sx), e.nx, e.ny, e.ny, e.ny, dy ? 2 : 1, oy);
+  if (dx) {
+    LineOut od = lo(LM_TRUNC, dx, iy, e.cut_e[1]);
+    launch_line(e, 1, ld_field(e, sdx), e.nx, e.ny, e.ny, e.ny, 1, &od);
+  }
+}
+
+// Derivxy(FFT(field), kx2) and (.., ky2) as one x pass and one y pass
+void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int accy) {
+  if (dx) {
+    LineOut o = lo(LM_DERIV, dx, 1.0 / e.nx, 0, accx);
+    launch_line(e, 0, L, e.nx, e.ny, e.nx, e.nx, 1, &o);
+  }
+  if (dy) {
+    LineOut o = lo(LM_DERIV, dy, 1.0 / e.ny, 0, accy);
+    launch_line(e, 1, L, e.nx, e.ny, e.ny, e.ny, 1, &o);
+  }
+}
+
+// Dealias1(FFT(field)): y pad (ny -> my) into scratch (nx, my, nz), then x pad
+void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch) {
+  LineOut oy = lo(LM_PAD, scratch, 1.0 / e.my);
+  launch_line(e, 1, L, e.nx, e.ny, e.ny, e.my, 1, &oy);
+  LineOut ox = lo(LM_PAD, out_pad, 1.0 / e.mx);
+  launch_line(e, 0, ld_field(e, scratch), e.nx, e.my, e.nx, e.mx, 1, &ox);
+}
+
+// Dealias2(FFT_pad(padded field)): x unpad (mx -> nx) into scratch
+// (nx, my, nz), then y unpad with the 9/4 factor
+void op2_unpad(Engine& e, const Loader& L_pad, double* out, double* scratch) {
+  LineOut ox = lo(LM_UNPAD, scratch, 1.0 / e.nx);
+  launch_line(e, 0, L_pad, e.mx, e.my, e.mx, e.nx, 1, &ox);
+  LineOut oy = lo(LM_UNPAD, out, (9.0 / 4.0) * (1.0 / e.ny));
+  launch_line(e, 1, ld_field(e, scratch), e.nx, e.my, e.my, e.ny, 1, &oy);
+}
+
+}  // namespace alfa

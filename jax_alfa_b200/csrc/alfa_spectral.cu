@@ -21,90 +21,9 @@
 // so a thread keeps U loads in flight instead of waiting on each one.
 #include <cmath>
 
-#include "alfa_fft_ct.cuh"
-#include "alfa_internal.cuh"
+#include "alfa_tile.cuh"
 
 namespace alfa {
-
-static constexpr int YC = 8;    // complex columns (= 16 real z levels) per y tile
-static constexpr int MAXTHREADS = 384;  // in-place sweeps need C*n/16 threads
-static constexpr int U = 8;     // loads in flight per thread
-
-// ---------------------------------------------------------------------------
-// Loader evaluation (value of the real input at linear index i, level z);
-// the kind is a compile-time constant in the tile kernels.
-// ---------------------------------------------------------------------------
-template <int KIND>
-__device__ __forceinline__ double ldv(const Loader& L, size_t i, int z) {
-  const int nz = L.nz;
-  if constexpr (KIND == LD_FIELD) {
-    return L.a[0][i];
-  } else if constexpr (KIND == LD_MUL) {
-    return L.a[0][i] * L.a[1][i];
-  } else if constexpr (KIND == LD_MUL3) {
-    return L.a[0][i] * L.a[1][i] * L.a[2][i];
-  } else if constexpr (KIND == LD_PRESSURE_R) {  // NSE_PressureTerms.py:140-142
-    return L.a[0][i] - L.c[0] * L.a[1][i] + L.c[1] * L.a[2][i];
-  } else if constexpr (KIND == LD_ADV_XY) {  // NSE_AdvectionTerms.py:105-116, :122-132
-    const double arg1 = L.a[0][i] * (L.a[1][i] - L.a[2][i]);
-    if (z == 0) {
-      const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
-      return arg1 + 0.5 * a2n;
-    }
-    const double a2 = L.a[3][i] * (L.a[4][i] - L.a[5][i]);
-    if (z == nz - 1) return arg1 + a2;
-    const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
-    return arg1 + 0.5 * (a2 + a2n);
-  } else if constexpr (KIND == LD_ADV_Z) {  // NSE_AdvectionTerms.py:137-151
-    if (z == 0 || z == nz - 1) return 0.0;
-    const double ug = 0.5 * (L.a[0][i - 1] + L.a[0][i]);
-    const double vg = 0.5 * (L.a[1][i - 1] + L.a[1][i]);
-    const double a1 = ug * (L.a[2][i] - L.a[3][i]);
-    const double a2 = vg * (L.a[4][i] - L.a[5][i]);
-    return a1 + a2;
-  } else if constexpr (KIND == LD_SCALAR_ADV) {  // SCL_AdvectionTerms.py:89-101
-    const double c1 = L.a[0][i] * L.a[3][i] + L.a[1][i] * L.a[4][i];
-    const double c2 = L.a[2][i] * L.a[5][i];
-    if (z == nz - 1) return c1 + c2;
-    const double c2n = L.a[2][i + 1] * L.a[5][i + 1];
-    return c1 + 0.5 * (c2 + c2n);
-  } else if constexpr (KIND == LD_STRESS_UVP) {  // SGSStresses_SM.py:122-132
-    if (z == nz - 1) return 0.0;
-    return L.c[0] * L.a[0][i] * L.a[1][i] * L.a[2][i];
-  } else if constexpr (KIND == LD_STRESS_W) {  // SGSStresses_SM.py:223-232
-    if (z == 0 || z == nz - 1) return 0.0;
-    return L.c[0] * (0.5 * (L.a[0][i - 1] + L.a[0][i])) * L.a[1][i] * L.a[2][i];
-  } else if constexpr (KIND == LD_W_SXX) {  // StrainRates.py:250-276, component L.sub
-    const double* const* g = L.a;  // dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
-    auto stag = [&](const double* d) -> double {
-      if (z == 0) return d[i];
-      if (z == nz - 1) return 0.0;
-      return 0.5 * (d[i - 1] + d[i]);
-    };
-    switch (L.sub) {
-      case 0: return stag(g[0]);                       // S11 = ux
-      case 1: return stag(g[4]);                       // S22 = vy
-      case 2: return stag(g[8]);                       // S33 = wz
-      case 3: return 0.5 * (stag(g[3]) + stag(g[1]));  // S12
-      case 4: {                                        // S13
-        const double wx = (z == 0) ? 0.5 * (g[2][i] + g[2][i + 1]) : g[2][i];
-        return 0.5 * (g[6][i] + wx);
-      }
-      default: {                                       // S23
-        const double wy = (z == 0) ? 0.5 * (g[5][i] + g[5][i + 1]) : g[5][i];
-        return 0.5 * (g[7][i] + wy);
-      }
-    }
-  } else if constexpr (KIND == LD_THZ) {  // DynamicSGS_ScalarLASDD_SM.py:182-185
-    const double* d = L.a[0];
-    if (z == 0 || z == nz - 1) return d[i];
-    return 0.5 * (d[i] + d[i + 1]);
-  } else {  // LD_MUL_THZ: S * THz
-    const double* d = L.a[1];
-    const double t = (z == 0 || z == nz - 1) ? d[i] : 0.5 * (d[i] + d[i + 1]);
-    return L.a[0][i] * t;
-  }
-}
 
 // Load the (n x 16 z) real tile of row `row` into b0 as n x 8 complex
 // (z pairs), U elements per thread in flight.
@@ -137,22 +56,6 @@ __device__ __forceinline__ void y_fwd_load(const Loader& L, int row, int n, int 
       if (t < total) b0[t] = v[u];
     }
   }
-}
-
-// Transform of an n x C tile: compile-time specialised for the lengths in
-// the dispatch tables below (N > 0), the runtime plan otherwise (N == 0).
-template <int S, int C, int N, int NT>
-__device__ __forceinline__ void tile_fft(cd* buf, const FftPlan& p) {
-  if constexpr (N == 0) {
-    fft_inplace<S, C>(buf, p);
-  } else {
-    fft_ct<S, C, N, NT>(buf, p.tw);
-  }
-}
-
-template <int C, int N>
-__host__ __device__ constexpr int tile_threads() {
-  return N == 0 ? MAXTHREADS : ct_threads(C, N);
 }
 
 // ---------------------------------------------------------------------------
@@ -416,13 +319,6 @@ __global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x
 // ---------------------------------------------------------------------------
 // launchers (dispatch to the specialised lengths)
 // ---------------------------------------------------------------------------
-static void set_smem(const void* f, size_t bytes) {
-  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
-#define ALFA_Y_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \
-  X(512) X(768)
-
 template <int N>
 static void y_fwd_n(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T) {
   const size_t smem = (size_t)p.n * YC * sizeof(cd);
@@ -474,11 +370,6 @@ static void x_n(Engine& e, const XArgs& a, int Kgrid) {
   k_x<C, NI, NO><<<g, nt, smem, e.stream>>>(a);
 }
 
-// (forward length, inverse length) pairs with a specialised k_x
-#define ALFA_X_PAIRS(X) X(16, 16) X(16, 24) X(24, 16) X(24, 24) X(32, 32) X(32, 48) X(48, 32) \
-  X(48, 48) X(64, 64) X(64, 96) X(96, 64) X(96, 96) X(128, 128) X(128, 192) X(192, 128)         \
-  X(192, 192) X(256, 256) X(256, 384) X(384, 256) X(384, 384)
-
 void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const FftPlan& fwd,
               int nout, const XOut* outs, int Kgrid) {
   XArgs a;
@@ -520,475 +411,6 @@ void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const
   }
   if (maxrows <= 256) x_n<8, 0, 0>(e, a, Kgrid);
   else x_n<4, 0, 0>(e, a, Kgrid);
-}
-
-// ---------------------------------------------------------------------------
-// k_line: 1-D spectral operator along x or y on real fields.  A CTA takes one
-// line index f (an x row for y lines, a y column for x lines) and 16
-// consecutive z levels packed as 8 complex lines, transforms them forward,
-// and for each output applies a map to the full packed spectrum, transforms
-// back and stores the real pair.  Packing two real lines in one complex
-// transform is exact for these maps because each is a real operator
-// (Hermitian-symmetric: truncation, i*k with the Nyquist zeroed, the 3/2-rule
-// pad with the Nyquist repeated, unpad).
-// ---------------------------------------------------------------------------
-struct LineArgs {
-  Loader L;
-  int n_in, n_out;
-  long long fs_in, rs_in, fs_out, rs_out;  // line and row strides (elements)
-  int nz;
-  int nouts;
-  LineOut out[3];
-  FftPlan pin, pout;
-};
-
-template <int KIND>
-__device__ __forceinline__ void line_load(const LineArgs& a, long long f, int z0, int n, cd* S) {
-  const Loader& L = a.L;
-  const int nz = a.nz;
-  const int total = n * YC;
-  const bool vec = (KIND == LD_FIELD) && ((nz & 1) == 0);
-  for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
-    cd v[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int t = t0 + u * blockDim.x;
-      v[u] = make_double2(0.0, 0.0);
-      if (t < total) {
-        const int r = t / YC, c = t % YC;
-        const int z = z0 + 2 * c;
-        const size_t i = (size_t)(f * a.fs_in + r * a.rs_in) + z;
-        if (vec && z + 1 < nz) {
-          v[u] = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
-        } else {
-          if (z < nz) v[u].x = ldv<KIND>(L, i, z);
-          if (z + 1 < nz) v[u].y = ldv<KIND>(L, i + 1, z + 1);
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int t = t0 + u * blockDim.x;
-      if (t < total) S[t] = v[u];
-    }
-  }
-}
-
-__device__ __forceinline__ cd line_map(const LineOut& o, const cd* S, int k, int c, int n, int m) {
-  auto deriv = [&](cd v) -> cd {
-    const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
-    const double q = (double)kk;
-    return make_double2(-(q * v.y), q * v.x);
-  };
-  switch (o.map) {
-    case LM_IDENT:
-      return S[k * YC + c];
-    case LM_TRUNC:
-      return (k < o.cut || k >= n - o.cut + 1) ? S[k * YC + c] : make_double2(0.0, 0.0);
-    case LM_DERIV:
-      return deriv(S[k * YC + c]);
-    case LM_TRUNC_DERIV:
-      return (k < o.cut || k >= n - o.cut + 1) ? deriv(S[k * YC + c]) : make_double2(0.0, 0.0);
-    case LM_PAD: {  // n -> m = 3n/2, Nyquist row repeated (Dealiasing.py:67-73)
-      const int h = n / 2;
-      if (k <= h) return S[k * YC + c];
-      if (k >= m - h) return S[(k - m + n) * YC + c];
-      return make_double2(0.0, 0.0);
-    }
-    default: {  // LM_UNPAD: n = 3m/2 -> m, Nyquist dropped (Dealiasing.py:102-109)
-      const int h = m / 2;
-      if (k < h) return S[k * YC + c];
-      if (k == h) return make_double2(0.0, 0.0);
-      return S[(k - m + n) * YC + c];
-    }
-  }
-}
-
-template <int NIN, int NOUT>
-__global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(), 1)
-    k_line(LineArgs a) {
-  constexpr int NT = tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>();
-  extern __shared__ cd sm[];
-  const int n = NIN > 0 ? NIN : a.n_in;
-  const int m = NOUT > 0 ? NOUT : a.n_out;
-  const int nz = a.nz;
-  const int z0 = blockIdx.x * (2 * YC);
-  const long long f = blockIdx.y;
-  cd* S = sm;
-  cd* W = sm + n * YC;
-  switch (a.L.kind) {
-    case LD_FIELD: line_load<LD_FIELD>(a, f, z0, n, S); break;
-    case LD_MUL: line_load<LD_MUL>(a, f, z0, n, S); break;
-    case LD_MUL3: line_load<LD_MUL3>(a, f, z0, n, S); break;
-    case LD_PRESSURE_R: line_load<LD_PRESSURE_R>(a, f, z0, n, S); break;
-    case LD_ADV_XY: line_load<LD_ADV_XY>(a, f, z0, n, S); break;
-    case LD_ADV_Z: line_load<LD_ADV_Z>(a, f, z0, n, S); break;
-    case LD_SCALAR_ADV: line_load<LD_SCALAR_ADV>(a, f, z0, n, S); break;
-    case LD_STRESS_UVP: line_load<LD_STRESS_UVP>(a, f, z0, n, S); break;
-    case LD_STRESS_W: line_load<LD_STRESS_W>(a, f, z0, n, S); break;
-    case LD_W_SXX: line_load<LD_W_SXX>(a, f, z0, n, S); break;
-    case LD_THZ: line_load<LD_THZ>(a, f, z0, n, S); break;
-    default: line_load<LD_MUL_THZ>(a, f, z0, n, S); break;
-  }
-  tile_fft<-1, YC, NIN, NT>(S, a.pin);
-  const bool pair = (nz & 1) == 0;
-  for (int oi = 0; oi < a.nouts; oi++) {
-    const LineOut& o = a.out[oi];
-    for (int t = threadIdx.x; t < m * YC; t += blockDim.x) {
-      const int k = t / YC, c = t % YC;
-      W[t] = line_map(o, S, k, c, n, m);
-    }
-    tile_fft<+1, YC, NOUT, NT>(W, a.pout);
-    const double sc = o.scale;
-    if (o.accumulate) {
-      for (int t0 = threadIdx.x; t0 < m * YC; t0 += U * blockDim.x) {
-        double2 prev[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          const int t = t0 + u * blockDim.x;
-          const int r = t / YC, c = t % YC;
-          const int z = z0 + 2 * c;
-          const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
-          prev[u] = make_double2(0.0, 0.0);
-          if (t < m * YC) {
-            if (pair && z < nz) {
-              prev[u] = *reinterpret_cast<const double2*>(o.dst + i);
-            } else {
-              if (z < nz) prev[u].x = o.dst[i];
-              if (z + 1 < nz) prev[u].y = o.dst[i + 1];
-            }
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          const int t = t0 + u * blockDim.x;
-          if (t >= m * YC) continue;
-          const int r = t / YC, c = t % YC;
-          const int z = z0 + 2 * c;
-          const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
-          const cd v = W[t];
-          const double2 w = make_double2(prev[u].x + sc * v.x, prev[u].y + sc * v.y);
-          if (pair && z < nz) {
-            *reinterpret_cast<double2*>(o.dst + i) = w;
-          } else {
-            if (z < nz) o.dst[i] = w.x;
-            if (z + 1 < nz) o.dst[i + 1] = w.y;
-          }
-        }
-      }
-    } else {
-      for (int t = threadIdx.x; t < m * YC; t += blockDim.x) {
-        const int r = t / YC, c = t % YC;
-        const int z = z0 + 2 * c;
-        const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
-        const cd v = W[t];
-        if (pair && z < nz) {
-          *reinterpret_cast<double2*>(o.dst + i) = make_double2(sc * v.x, sc * v.y);
-        } else {
-          if (z < nz) o.dst[i] = sc * v.x;
-          if (z + 1 < nz) o.dst[i + 1] = sc * v.y;
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// k_line_rr: k_line for compile-time lengths with register-resident ends.
-// The forward transform's first pass takes its inputs straight from global
-// memory (every thread issues all of its loads before the first butterfly);
-// each output's inverse transform reads its first-pass inputs from the
-// forward spectrum through the map, and its last pass stores straight from
-// registers.  Shared memory holds the forward spectrum and the inverse's
-// intermediate passes only.  GEN: the input is any Loader kind (else a
-// plain field, with a leaner register budget).
-// ---------------------------------------------------------------------------
-template <int C, int NIN, int NOUT>
-__host__ __device__ constexpr int line_threads() {
-  return ct_threads(C, NIN) > ct_threads(C, NOUT) ? ct_threads(C, NIN) : ct_threads(C, NOUT);
-}
-
-// first-pass gather: v[q*R + r] = (x, x') at row j + r*NR of line c
-template <int KIND, int C, int N, int NT>
-__device__ __forceinline__ void line_gather(const LineArgs& a, long long f, int z0, cd* v) {
-  constexpr int R = ct_radix(N);
-  constexpr int NR = N / R;
-  constexpr int B = NR * C;
-  constexpr int MB = (B + NT - 1) / NT;
-  const Loader& L = a.L;
-  const int nz = a.nz;
-  const bool vec = (KIND == LD_FIELD) && ((nz & 1) == 0);
-#pragma unroll
-  for (int q = 0; q < MB; q++) {
-    const int b = threadIdx.x + q * NT;
-    const int c = b % C;
-    const int j = b / C;
-    const int z = z0 + 2 * c;
-    const bool ok = (B % NT == 0 || b < B);
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      const size_t i = (size_t)(f * a.fs_in + (long long)(j + r * NR) * a.rs_in) + z;
-      cd t = make_double2(0.0, 0.0);
-      if (ok) {
-        if (vec && z + 1 < nz) {
-          t = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
-        } else {
-          if (z < nz) t.x = ldv<KIND>(L, i, z);
-          if (z + 1 < nz) t.y = ldv<KIND>(L, i + 1, z + 1);
-        }
-      }
-      v[q * R + r] = t;
-    }
-  }
-}
-
-// store (or accumulate) v[q*R + r] = value at row j + r*STEP of line c
-template <int C, int R, int STEP, int B, int NT>
-__device__ __forceinline__ void line_scatter(const LineArgs& a, const LineOut& o, long long f,
-                                             int z0, const cd* v) {
-  constexpr int MB = (B + NT - 1) / NT;
-  const int nz = a.nz;
-  const bool pair = (nz & 1) == 0;
-  const double sc = o.scale;
-  double* __restrict__ dst = o.dst;
-#pragma unroll
-  for (int q = 0; q < MB; q++) {
-    const int b = threadIdx.x + q * NT;
-    if (!(B % NT == 0 || b < B)) continue;
-    const int c = b % C;
-    const int j = b / C;
-    const int z = z0 + 2 * c;
-    if (z >= nz) continue;
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      const size_t i = (size_t)(f * a.fs_out + (long long)(j + r * STEP) * a.rs_out) + z;
-      double2 w = make_double2(sc * v[q * R + r].x, sc * v[q * R + r].y);
-      if (pair) {
-        double2* p = reinterpret_cast<double2*>(dst + i);
-        if (o.accumulate) {
-          const double2 pv = *p;
-          w.x += pv.x;
-          w.y += pv.y;
-        }
-        *p = w;
-      } else {
-        if (o.accumulate) {
-          w.x += dst[i];
-          if (z + 1 < nz) w.y += dst[i + 1];
-        }
-        dst[i] = w.x;
-        if (z + 1 < nz) dst[i + 1] = w.y;
-      }
-    }
-  }
-}
-
-template <int NIN, int NOUT, bool GEN>
-__global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
-    k_line_rr(LineArgs a) {
-  constexpr int C = YC;
-  constexpr int NT = line_threads<C, NIN, NOUT>();
-  constexpr int NMAX = NIN > NOUT ? NIN : NOUT;
-  extern __shared__ cd sm[];
-  cd* S = sm;
-  cd* Wb = a.nouts > 1 ? sm + NMAX * C : sm;
-  const int z0 = blockIdx.x * (2 * C);
-  const long long f = blockIdx.y;
-  // forward transform of the NIN-line tile into S
-  {
-    constexpr int R = ct_radix(NIN);
-    constexpr int MB = ct_mb(C, NIN, 1, NT);
-    cd v[MB * R];
-    if constexpr (GEN) {
-      switch (a.L.kind) {
-        case LD_FIELD: line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v); break;
-        case LD_MUL: line_gather<LD_MUL, C, NIN, NT>(a, f, z0, v); break;
-        case LD_MUL3: line_gather<LD_MUL3, C, NIN, NT>(a, f, z0, v); break;
-        case LD_PRESSURE_R: line_gather<LD_PRESSURE_R, C, NIN, NT>(a, f, z0, v); break;
-        case LD_ADV_XY: line_gather<LD_ADV_XY, C, NIN, NT>(a, f, z0, v); break;
-        case LD_ADV_Z: line_gather<LD_ADV_Z, C, NIN, NT>(a, f, z0, v); break;
-        case LD_SCALAR_ADV: line_gather<LD_SCALAR_ADV, C, NIN, NT>(a, f, z0, v); break;
-        case LD_STRESS_UVP: line_gather<LD_STRESS_UVP, C, NIN, NT>(a, f, z0, v); break;
-        case LD_STRESS_W: line_gather<LD_STRESS_W, C, NIN, NT>(a, f, z0, v); break;
-        case LD_W_SXX: line_gather<LD_W_SXX, C, NIN, NT>(a, f, z0, v); break;
-        case LD_THZ: line_gather<LD_THZ, C, NIN, NT>(a, f, z0, v); break;
-        default: line_gather<LD_MUL_THZ, C, NIN, NT>(a, f, z0, v); break;
-      }
-    } else {
-      line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v);
-    }
-    if constexpr (R == NIN) {
-      if (threadIdx.x < C) {
-        dftR<R, -1>(v);
-#pragma unroll
-        for (int r = 0; r < R; r++) S[r * C + threadIdx.x] = v[r];
-      }
-    } else {
-      ct_first_reg<-1, C, NIN, NT>(v, S);
-      ct_passes<-1, C, NIN, R, NT>(S, a.pin.tw);
-    }
-    __syncthreads();
-  }
-  // outputs: map, inverse transform, store
-  for (int oi = 0; oi < a.nouts; oi++) {
-    const LineOut& o = a.out[oi];
-    constexpr int R = ct_radix(NOUT);
-    constexpr int NR = NOUT / R;
-    constexpr int B = NR * C;
-    constexpr int MB = ct_mb(C, NOUT, 1, NT);
-    cd v[MB * R];
-#pragma unroll
-    for (int q = 0; q < MB; q++) {
-      const int b = threadIdx.x + q * NT;
-      const int c = b % C;
-      const int j = b / C;
-#pragma unroll
-      for (int r = 0; r < R; r++)
-        v[q * R + r] = (B % NT == 0 || b < B) ? line_map(o, S, j + r * NR, c, NIN, NOUT)
-                                              : make_double2(0.0, 0.0);
-    }
-    if constexpr (R == NOUT) {
-#pragma unroll
-      for (int q = 0; q < MB; q++) dftR<R, +1>(v + q * R);
-      line_scatter<C, R, 1, C, NT>(a, o, f, z0, v);
-    } else {
-      __syncthreads();  // Wb may alias S
-      ct_first_reg<+1, C, NOUT, NT>(v, Wb);
-      ct_mid_passes<+1, C, NOUT, R, NT>(Wb, a.pout.tw);
-      __syncthreads();
-      constexpr int NSL = ct_last_ns(NOUT);
-      constexpr int RL = NOUT / NSL;
-      constexpr int ML = ct_mb(C, NOUT, NSL, NT);
-      cd u[ML * RL];
-      ct_last_reg<+1, C, NOUT, NT>(Wb, a.pout.tw, u);
-      line_scatter<C, RL, NSL, NSL * C, NT>(a, o, f, z0, u);
-    }
-    __syncthreads();
-  }
-}
-
-template <int NIN, int NOUT>
-static void line_n(Engine& e, const LineArgs& a, int F) {
-  dim3 g((a.nz + 2 * YC - 1) / (2 * YC), F);
-  if constexpr (NIN > 0) {
-    const int nmax = NIN > NOUT ? NIN : NOUT;
-    const size_t smem = (size_t)(nmax + (a.nouts > 1 ? NOUT : 0)) * YC * sizeof(cd);
-    constexpr int nt = line_threads<YC, NIN, NOUT>();
-    if (a.L.kind == LD_FIELD) {
-      set_smem((const void*)k_line_rr<NIN, NOUT, false>, smem);
-      k_line_rr<NIN, NOUT, false><<<g, nt, smem, e.stream>>>(a);
-    } else {
-      set_smem((const void*)k_line_rr<NIN, NOUT, true>, smem);
-      k_line_rr<NIN, NOUT, true><<<g, nt, smem, e.stream>>>(a);
-    }
-  } else {
-    const size_t smem = (size_t)(a.n_in + a.n_out) * YC * sizeof(cd);
-    set_smem((const void*)k_line<0, 0>, smem);
-    const int nt = inplace_threads(YC, a.n_in > a.n_out ? a.n_in : a.n_out);
-    k_line<0, 0><<<g, nt, smem, e.stream>>>(a);
-  }
-}
-
-static const FftPlan& plan_for(const Engine& e, int n) {
-  if (n == e.nx) return e.pnx;
-  if (n == e.ny) return e.pny;
-  if (n == e.mx) return e.pmx;
-  return e.pmy;
-}
-
-void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
-                 int nout, const LineOut* outs) {
-  LineArgs a;
-  a.L = L;
-  a.n_in = n_in;
-  a.n_out = n_out;
-  a.nz = L.nz;
-  const long long nz = L.nz;
-  int F;
-  if (axis == 0) {  // x lines of (X=n_in, Y, nz) -> (n_out, Y, nz)
-    a.fs_in = nz;
-    a.rs_in = (long long)Y * nz;
-    a.fs_out = nz;
-    a.rs_out = (long long)Y * nz;
-    F = Y;
-  } else {  // y lines of (X, Y=n_in, nz) -> (X, n_out, nz)
-    a.fs_in = (long long)n_in * nz;
-    a.rs_in = nz;
-    a.fs_out = (long long)n_out * nz;
-    a.rs_out = nz;
-    F = X;
-  }
-  a.nouts = nout;
-  for (int i = 0; i < nout; i++) a.out[i] = outs[i];
-  a.pin = plan_for(e, n_in);
-  a.pout = plan_for(e, n_out);
-  ::alfa::note_launch();
-#define ALFA_CASE(p, q)               \
-  if (n_in == p && n_out == q) {      \
-    line_n<p, q>(e, a, F);            \
-    return;                           \
-  }
-  ALFA_X_PAIRS(ALFA_CASE)
-#undef ALFA_CASE
-  line_n<0, 0>(e, a, F);
-}
-
-static LineOut lo(int map, double* dst, double scale, int cut = 0, int acc = 0) {
-  LineOut o;
-  o.map = map;
-  o.cut = cut;
-  o.scale = scale;
-  o.accumulate = acc;
-  o.dst = dst;
-  return o;
-}
-
-// Filtering_Explicit followed by Derivxy in x and y (Filtering.py:50-89,
-// Derivatives.py:161-182), as separable passes: x pass (filter, and filter +
-// d/dx), then y passes.  scratch2: two N-sized fields.
-void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
-                      double* scratch2) {
-  double* sx = scratch2;
-  double* sdx = scratch2 + e.N();
-  const double ix = 1.0 / e.nx, iy = 1.0 / e.ny;
-  LineOut ox[2] = {lo(LM_TRUNC, sx, ix, e.cut_e[0]), lo(LM_TRUNC_DERIV, sdx, ix, e.cut_e[0])};
-  launch_line(e, 0, L, e.nx, e.ny, e.nx, e.nx, dx ? 2 : 1, ox);
-  LineOut oy[2] = {lo(LM_TRUNC, f, iy, e.cut_e[1]), lo(LM_TRUNC_DERIV, dy, iy, e.cut_e[1])};
-  launch_line(e, 1, ld_field(e, sx), e.nx, e.ny, e.ny, e.ny, dy ? 2 : 1, oy);
-  if (dx) {
-    LineOut od = lo(LM_TRUNC, dx, iy, e.cut_e[1]);
-    launch_line(e, 1, ld_field(e, sdx), e.nx, e.ny, e.ny, e.ny, 1, &od);
-  }
-}
-
-// Derivxy(FFT(field), kx2) and (.., ky2) as one x pass and one y pass
-void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int accy) {
-  if (dx) {
-    LineOut o = lo(LM_DERIV, dx, 1.0 / e.nx, 0, accx);
-    launch_line(e, 0, L, e.nx, e.ny, e.nx, e.nx, 1, &o);
-  }
-  if (dy) {
-    LineOut o = lo(LM_DERIV, dy, 1.0 / e.ny, 0, accy);
-    launch_line(e, 1, L, e.nx, e.ny, e.ny, e.ny, 1, &o);
-  }
-}
-
-// Dealias1(FFT(field)): y pad (ny -> my) into scratch (nx, my, nz), then x pad
-void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch) {
-  LineOut oy = lo(LM_PAD, scratch, 1.0 / e.my);
-  launch_line(e, 1, L, e.nx, e.ny, e.ny, e.my, 1, &oy);
-  LineOut ox = lo(LM_PAD, out_pad, 1.0 / e.mx);
-  launch_line(e, 0, ld_field(e, scratch), e.nx, e.my, e.nx, e.mx, 1, &ox);
-}
-
-// Dealias2(FFT_pad(padded field)): x unpad (mx -> nx) into scratch
-// (nx, my, nz), then y unpad with the 9/4 factor
-void op2_unpad(Engine& e, const Loader& L_pad, double* out, double* scratch) {
-  LineOut ox = lo(LM_UNPAD, scratch, 1.0 / e.nx);
-  launch_line(e, 0, L_pad, e.mx, e.my, e.mx, e.nx, 1, &ox);
-  LineOut oy = lo(LM_UNPAD, out, (9.0 / 4.0) * (1.0 / e.ny));
-  launch_line(e, 1, ld_field(e, scratch), e.nx, e.my, e.my, e.ny, 1, &oy);
 }
 
 // ---------------------------------------------------------------------------
