@@ -364,6 +364,7 @@ static void carve(alfa_ctx* c, Carver& k) {
   e.scal = k.take<double>(64 * nz + 256);
   e.W_elems = N;
   e.W = k.take<double>(N);
+  e.mat = k.take<double>(e.P());
 }
 
 // ---------------------------------------------------------------------------

@@ -114,6 +114,7 @@ struct Engine {
   double* scal = nullptr;         // small device scalars / profiles
   double* W = nullptr;            // field workspace arena
   size_t W_elems = 0;
+  double* mat = nullptr;          // a loader's expression, materialised (P elements)
 
   size_t N() const { return (size_t)nx * ny * nz; }
   size_t P() const { return (size_t)mx * my * nz; }
@@ -148,6 +149,8 @@ void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double*
 void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int accy);
 void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch);
 void op2_unpad(Engine& e, const Loader& L_pad, double* out, double* scratch);
+// value of a loader at every point of its n-element domain, written to out
+void materialize(Engine& e, const Loader& L, size_t n, double* out);
 
 // composite transforms on regular/padded grids
 Loader ld_field(const Engine& e, const double* a);

@@ -185,14 +185,11 @@ __global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(),
 // The forward transform's first pass takes its inputs straight from global
 // memory (every thread issues all of its loads before the first butterfly)
 // and each inverse transform's last pass stores straight from registers.
-// When input and output lengths match and the first and last radix of the
-// transform agree (n = 256 = 16 x 16), the forward spectrum also stays in
-// registers: the thread that ends the forward transform with bins
-// j + NS*r holds exactly the inputs of the inverse's first butterfly, so the
-// map is applied in registers and shared memory carries one exchange per
-// transform.  Otherwise each inverse reads its first-pass inputs from the
-// forward spectrum in shared memory through the map.  GEN: the input is any
-// Loader kind (else a plain field, with a leaner register budget).
+// Each inverse reads its first-pass inputs from the forward spectrum in
+// shared memory through the map.  GEN: the input is any Loader kind (else a
+// plain field, with a leaner register budget).  (Keeping the forward
+// spectrum in registers for same-length maps, which the n = 16 x 16 layout
+// allows, measured slower: the register budget halved the resident CTAs.)
 // ---------------------------------------------------------------------------
 template <int C, int NIN, int NOUT>
 __host__ __device__ constexpr int line_threads() {
@@ -252,7 +249,10 @@ __device__ __forceinline__ void line_gather(const LineArgs& a, long long f, int 
 #pragma unroll
     for (int r = 0; r < R; r++) {
       const size_t i = (size_t)(f * a.fs_in + (long long)(j + r * NR) * a.rs_in) + z;
-      v[q * R + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
+      if (KIND != LD_FIELD && (a.nz & 1) == 0)
+        v[q * R + r] = eval_pair<KIND, C>(a.L, i, z, a.nz, c, ok);
+      else
+        v[q * R + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
     }
   }
 }
@@ -295,67 +295,17 @@ __device__ __forceinline__ void line_scatter(const LineArgs& a, const LineOut& o
   }
 }
 
-// same-length maps applied to bin k of a length-n spectrum (as line_map)
-__device__ __forceinline__ cd map_reg(const LineOut& o, cd v, int k, int n) {
-  if ((o.map == LM_TRUNC || o.map == LM_TRUNC_DERIV) && !(k < o.cut || k >= n - o.cut + 1))
-    return make_double2(0.0, 0.0);
-  if (o.map == LM_DERIV || o.map == LM_TRUNC_DERIV) {
-    const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
-    const double q = (double)kk;
-    return make_double2(-(q * v.y), q * v.x);
-  }
-  return v;
-}
-
-template <int N, int NT>
-__host__ __device__ constexpr bool line_reg_path() {
-  return N > 16 && ct_radix(N) == N / ct_last_ns(N) &&
-         ct_mb(YC, N, 1, NT) == ct_mb(YC, N, ct_last_ns(N), NT);
-}
-
 template <int NIN, int NOUT, bool GEN>
 __global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
     k_line_rr(LineArgs a) {
   constexpr int C = YC;
   constexpr int NT = line_threads<C, NIN, NOUT>();
   constexpr int NMAX = NIN > NOUT ? NIN : NOUT;
-  constexpr bool REG = (NIN == NOUT) && line_reg_path<NIN, NT>();
   extern __shared__ cd sm[];
   cd* S = sm;
   const int z0 = blockIdx.x * (2 * C);
   const long long f = blockIdx.y;
-  if constexpr (REG) {
-    constexpr int R = ct_radix(NIN);
-    constexpr int NSL = ct_last_ns(NIN);
-    constexpr int MB = ct_mb(C, NIN, 1, NT);
-    cd X[MB * R];
-    {
-      cd v[MB * R];
-      if constexpr (GEN) line_gather_any<C, NIN, NT>(a, f, z0, v);
-      else line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v);
-      ct_first_reg<-1, C, NIN, NT>(v, S);
-      ct_mid_passes<-1, C, NIN, R, NT>(S, a.pin.tw);
-      __syncthreads();
-      ct_last_reg<-1, C, NIN, NT>(S, a.pin.tw, X);
-    }
-    for (int oi = 0; oi < a.nouts; oi++) {
-      const LineOut& o = a.out[oi];
-      cd v[MB * R];
-#pragma unroll
-      for (int q = 0; q < MB; q++) {
-        const int j = (threadIdx.x + q * NT) / C;
-#pragma unroll
-        for (int r = 0; r < R; r++) v[q * R + r] = map_reg(o, X[q * R + r], j + NSL * r, NIN);
-      }
-      __syncthreads();  // every read of S by the previous pass is done
-      ct_first_reg<+1, C, NOUT, NT>(v, S);
-      ct_mid_passes<+1, C, NOUT, R, NT>(S, a.pout.tw);
-      __syncthreads();
-      cd u[MB * R];
-      ct_last_reg<+1, C, NOUT, NT>(S, a.pout.tw, u);
-      line_scatter<C, R, NSL, NSL * C, NT>(a, o, f, z0, u);
-    }
-  } else {
+  {
     cd* Wb = a.nouts > 1 ? sm + NMAX * C : sm;
     // forward transform of the NIN-line tile into S
     {
@@ -442,7 +392,14 @@ __host__ __device__ constexpr bool pad3_ok() {
 
 __device__ __forceinline__ cd cconj(cd a) { return make_double2(a.x, -a.y); }
 
-template <int N, bool GEN>
+template <int KIND, int C, int N, int NT>
+__device__ __forceinline__ void line_gather_sel(const LineArgs& a, long long f, int z0, cd* v) {
+  if constexpr (KIND >= 0) line_gather<KIND, C, N, NT>(a, f, z0, v);
+  else line_gather_any<C, N, NT>(a, f, z0, v);
+}
+
+// KIND: the loader kind, or -1 for any kind (chosen at run time)
+template <int N, int KIND>
 __global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
   constexpr int C = YC;
   constexpr int NT = ct_threads(C, N);
@@ -463,8 +420,7 @@ __global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
   cd X[R];
   {
     cd v[R];
-    if constexpr (GEN) line_gather_any<C, N, NT>(a, f, z0, v);
-    else line_gather<LD_FIELD, C, N, NT>(a, f, z0, v);
+    line_gather_sel<KIND, C, N, NT>(a, f, z0, v);
     ct_first_reg<-1, C, N, NT>(v, S);
     __syncthreads();
     ct_last_reg<-1, C, N, NT>(S, twN, X);  // X[r] = bin j + R r
@@ -542,7 +498,10 @@ __device__ __forceinline__ void phase_gather(const LineArgs& a, long long f, int
     for (int r = 0; r < RB; r++) {
       const long long row = 3 * (jj + RA * r) + p;
       const size_t i = (size_t)(f * a.fs_in + row * a.rs_in) + z;
-      v[q * RB + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
+      if (KIND != LD_FIELD && (a.nz & 1) == 0)
+        v[q * RB + r] = eval_pair<KIND, C>(a.L, i, z, a.nz, c, ok);
+      else
+        v[q * RB + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
     }
   }
 }
@@ -565,8 +524,9 @@ __device__ __forceinline__ void phase_gather_any(const LineArgs& a, long long f,
   }
 }
 
-template <int N, bool GEN>
-__global__ void __launch_bounds__(ct_threads(YC, N)) k_unpad3(LineArgs a) {
+// three CTAs per SM measured faster than the unconstrained register budget
+template <int N, int KIND>
+__global__ void __launch_bounds__(ct_threads(YC, N), 3) k_unpad3(LineArgs a) {
   constexpr int C = YC;
   constexpr int NT = ct_threads(C, N);
   constexpr int R = ct_radix(N);   // both passes of the length-N inverse
@@ -585,8 +545,8 @@ __global__ void __launch_bounds__(ct_threads(YC, N)) k_unpad3(LineArgs a) {
   const cd* twN = a.pout.tw;  // exp(-2 pi i q / N)
   {
     cd v[MBB * RB];
-    if constexpr (GEN) phase_gather_any<C, RA, RB, NT>(a, f, z0, v);
-    else phase_gather<LD_FIELD, C, RA, RB, NT>(a, f, z0, v);
+    if constexpr (KIND >= 0) phase_gather<KIND, C, RA, RB, NT>(a, f, z0, v);
+    else phase_gather_any<C, RA, RB, NT>(a, f, z0, v);
 #pragma unroll
     for (int q = 0; q < MBB; q++) {
       const int b = threadIdx.x + q * NT;
@@ -643,8 +603,7 @@ static void line_n(Engine& e, const LineArgs& a, int F) {
   if constexpr (NIN > 0) {
     const int nmax = NIN > NOUT ? NIN : NOUT;
     constexpr int nt = line_threads<YC, NIN, NOUT>();
-    constexpr bool reg = (NIN == NOUT) && line_reg_path<NIN, nt>();
-    const size_t smem = (size_t)(nmax + (!reg && a.nouts > 1 ? NOUT : 0)) * YC * sizeof(cd);
+    const size_t smem = (size_t)(nmax + (a.nouts > 1 ? NOUT : 0)) * YC * sizeof(cd);
     if (a.L.kind == LD_FIELD) {
       set_smem((const void*)k_line_rr<NIN, NOUT, false>, smem);
       k_line_rr<NIN, NOUT, false><<<g, nt, smem, e.stream>>>(a);
@@ -660,29 +619,31 @@ static void line_n(Engine& e, const LineArgs& a, int F) {
   }
 }
 
-// 3/2-rule pad (PAD) or unpad by phases, n = N
+// 3/2-rule pad or unpad by phases, n = N: a plain field (the form op2_pad /
+// op2_unpad hand over), or any loader kind through the run-time switch
+template <int N, int KIND>
+static void pad3_k(Engine& e, const LineArgs& a, dim3 g, size_t smem) {
+  set_smem((const void*)k_pad3<N, KIND>, smem);
+  k_pad3<N, KIND><<<g, ct_threads(YC, N), smem, e.stream>>>(a);
+}
+
+template <int N, int KIND>
+static void unpad3_k(Engine& e, const LineArgs& a, dim3 g, size_t smem) {
+  set_smem((const void*)k_unpad3<N, KIND>, smem);
+  k_unpad3<N, KIND><<<g, ct_threads(YC, N), smem, e.stream>>>(a);
+}
+
 template <int N, bool PAD>
 static void phase_n(Engine& e, const LineArgs& a, int F) {
   dim3 g((a.nz + 2 * YC - 1) / (2 * YC), F);
-  constexpr int nt = ct_threads(YC, N);
   const size_t smem = (size_t)(3 * N / 2) * YC * sizeof(cd);
-  const bool gen = a.L.kind != LD_FIELD;
+  const bool field = a.L.kind == LD_FIELD;
   if (PAD) {
-    if (gen) {
-      set_smem((const void*)k_pad3<N, true>, smem);
-      k_pad3<N, true><<<g, nt, smem, e.stream>>>(a);
-    } else {
-      set_smem((const void*)k_pad3<N, false>, smem);
-      k_pad3<N, false><<<g, nt, smem, e.stream>>>(a);
-    }
+    if (field) pad3_k<N, LD_FIELD>(e, a, g, smem);
+    else pad3_k<N, -1>(e, a, g, smem);
   } else {
-    if (gen) {
-      set_smem((const void*)k_unpad3<N, true>, smem);
-      k_unpad3<N, true><<<g, nt, smem, e.stream>>>(a);
-    } else {
-      set_smem((const void*)k_unpad3<N, false>, smem);
-      k_unpad3<N, false><<<g, nt, smem, e.stream>>>(a);
-    }
+    if (field) unpad3_k<N, LD_FIELD>(e, a, g, smem);
+    else unpad3_k<N, -1>(e, a, g, smem);
   }
 }
 
@@ -778,8 +739,45 @@ void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int
   }
 }
 
-// Dealias1(FFT(field)): y pad (ny -> my) into scratch (nx, my, nz), then x pad
-void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch) {
+// Elementwise evaluation of a loader (its kind a template constant): one
+// level per thread, stencil neighbours through the cache.  A separate pass
+// costs one extra write and read of the domain but keeps the transform
+// kernels' gathers to a single 16-byte load per element: gathering several
+// inputs per element inside the transform kernel limits the loads a thread
+// keeps in flight and measured slower than the two passes.
+template <int KIND>
+__global__ void __launch_bounds__(256) k_materialize(Loader L, size_t n, double* __restrict__ out) {
+  const int nz = L.nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = ldv<KIND>(L, i, (int)(i % nz));
+}
+
+void materialize(Engine& e, const Loader& L, size_t n, double* out) {
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e.device);
+  const size_t want = (n + 255) / 256;
+  const unsigned blocks = (unsigned)(want < (size_t)dev_sms * 16 ? want : (size_t)dev_sms * 16);
+  ::alfa::note_launch();
+  switch (L.kind) {
+#define ALFA_MAT(K) \
+  case K: k_materialize<K><<<blocks, 256, 0, e.stream>>>(L, n, out); break;
+    ALFA_MAT(LD_FIELD) ALFA_MAT(LD_MUL) ALFA_MAT(LD_MUL3) ALFA_MAT(LD_PRESSURE_R)
+    ALFA_MAT(LD_ADV_XY) ALFA_MAT(LD_ADV_Z) ALFA_MAT(LD_SCALAR_ADV) ALFA_MAT(LD_STRESS_UVP)
+    ALFA_MAT(LD_STRESS_W) ALFA_MAT(LD_W_SXX) ALFA_MAT(LD_THZ)
+    default: k_materialize<LD_MUL_THZ><<<blocks, 256, 0, e.stream>>>(L, n, out); break;
+#undef ALFA_MAT
+  }
+}
+
+// Dealias1(FFT(field)): y pad (ny -> my) into scratch (nx, my, nz), then x
+// pad; a non-field loader is first materialised
+void op2_pad(Engine& e, const Loader& L0, double* out_pad, double* scratch) {
+  Loader L = L0;
+  if (L.kind != LD_FIELD) {
+    materialize(e, L, e.N(), e.mat);
+    L = ld_field(e, e.mat);
+  }
   LineOut oy = lo(LM_PAD, scratch, 1.0 / e.my);
   launch_line(e, 1, L, e.nx, e.ny, e.ny, e.my, 1, &oy);
   LineOut ox = lo(LM_PAD, out_pad, 1.0 / e.mx);
@@ -787,10 +785,16 @@ void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch) {
 }
 
 // Dealias2(FFT_pad(padded field)): x unpad (mx -> nx) into scratch
-// (nx, my, nz), then y unpad with the 9/4 factor
-void op2_unpad(Engine& e, const Loader& L_pad, double* out, double* scratch) {
+// (nx, my, nz), then y unpad with the 9/4 factor; a non-field loader is
+// first materialised
+void op2_unpad(Engine& e, const Loader& L0, double* out, double* scratch) {
+  Loader L = L0;
+  if (L.kind != LD_FIELD) {
+    materialize(e, L, e.P(), e.mat);
+    L = ld_field(e, e.mat);
+  }
   LineOut ox = lo(LM_UNPAD, scratch, 1.0 / e.nx);
-  launch_line(e, 0, L_pad, e.mx, e.my, e.mx, e.nx, 1, &ox);
+  launch_line(e, 0, L, e.mx, e.my, e.mx, e.nx, 1, &ox);
   LineOut oy = lo(LM_UNPAD, out, (9.0 / 4.0) * (1.0 / e.ny));
   launch_line(e, 1, ld_field(e, scratch), e.nx, e.my, e.my, e.ny, 1, &oy);
 }

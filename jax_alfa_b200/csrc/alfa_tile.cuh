@@ -11,79 +11,164 @@ static constexpr int MAXTHREADS = 384;  // in-place sweeps need C*n/16 threads
 static constexpr int U = 8;     // loads in flight per thread
 
 // ---------------------------------------------------------------------------
-// Loader evaluation (value of the real input at linear index i, level z);
-// the kind is a compile-time constant in the tile kernels.
+// Loader evaluation.  ev_kind states each expression once in terms of an
+// accessor at(k, d) = input k at level z + d (d = -1, 0, +1); ldv evaluates
+// it at one linear index i, eval_pair at the two levels (z, z+1) of a packed
+// complex column.  The kind is a compile-time constant in the tile kernels.
 // ---------------------------------------------------------------------------
-template <int KIND>
-__device__ __forceinline__ double ldv(const Loader& L, size_t i, int z) {
-  const int nz = L.nz;
+template <int KIND, class At>
+__device__ __forceinline__ double ev_kind(const Loader& L, const At& at, int z, int nz) {
   if constexpr (KIND == LD_FIELD) {
-    return L.a[0][i];
+    return at(0, 0);
   } else if constexpr (KIND == LD_MUL) {
-    return L.a[0][i] * L.a[1][i];
+    return at(0, 0) * at(1, 0);
   } else if constexpr (KIND == LD_MUL3) {
-    return L.a[0][i] * L.a[1][i] * L.a[2][i];
+    return at(0, 0) * at(1, 0) * at(2, 0);
   } else if constexpr (KIND == LD_PRESSURE_R) {  // NSE_PressureTerms.py:140-142
-    return L.a[0][i] - L.c[0] * L.a[1][i] + L.c[1] * L.a[2][i];
+    return at(0, 0) - L.c[0] * at(1, 0) + L.c[1] * at(2, 0);
   } else if constexpr (KIND == LD_ADV_XY) {  // NSE_AdvectionTerms.py:105-116, :122-132
-    const double arg1 = L.a[0][i] * (L.a[1][i] - L.a[2][i]);
+    const double arg1 = at(0, 0) * (at(1, 0) - at(2, 0));
     if (z == 0) {
-      const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
+      const double a2n = at(3, 1) * (at(4, 1) - at(5, 1));
       return arg1 + 0.5 * a2n;
     }
-    const double a2 = L.a[3][i] * (L.a[4][i] - L.a[5][i]);
+    const double a2 = at(3, 0) * (at(4, 0) - at(5, 0));
     if (z == nz - 1) return arg1 + a2;
-    const double a2n = L.a[3][i + 1] * (L.a[4][i + 1] - L.a[5][i + 1]);
+    const double a2n = at(3, 1) * (at(4, 1) - at(5, 1));
     return arg1 + 0.5 * (a2 + a2n);
   } else if constexpr (KIND == LD_ADV_Z) {  // NSE_AdvectionTerms.py:137-151
     if (z == 0 || z == nz - 1) return 0.0;
-    const double ug = 0.5 * (L.a[0][i - 1] + L.a[0][i]);
-    const double vg = 0.5 * (L.a[1][i - 1] + L.a[1][i]);
-    const double a1 = ug * (L.a[2][i] - L.a[3][i]);
-    const double a2 = vg * (L.a[4][i] - L.a[5][i]);
+    const double ug = 0.5 * (at(0, -1) + at(0, 0));
+    const double vg = 0.5 * (at(1, -1) + at(1, 0));
+    const double a1 = ug * (at(2, 0) - at(3, 0));
+    const double a2 = vg * (at(4, 0) - at(5, 0));
     return a1 + a2;
   } else if constexpr (KIND == LD_SCALAR_ADV) {  // SCL_AdvectionTerms.py:89-101
-    const double c1 = L.a[0][i] * L.a[3][i] + L.a[1][i] * L.a[4][i];
-    const double c2 = L.a[2][i] * L.a[5][i];
+    const double c1 = at(0, 0) * at(3, 0) + at(1, 0) * at(4, 0);
+    const double c2 = at(2, 0) * at(5, 0);
     if (z == nz - 1) return c1 + c2;
-    const double c2n = L.a[2][i + 1] * L.a[5][i + 1];
+    const double c2n = at(2, 1) * at(5, 1);
     return c1 + 0.5 * (c2 + c2n);
   } else if constexpr (KIND == LD_STRESS_UVP) {  // SGSStresses_SM.py:122-132
     if (z == nz - 1) return 0.0;
-    return L.c[0] * L.a[0][i] * L.a[1][i] * L.a[2][i];
+    return L.c[0] * at(0, 0) * at(1, 0) * at(2, 0);
   } else if constexpr (KIND == LD_STRESS_W) {  // SGSStresses_SM.py:223-232
     if (z == 0 || z == nz - 1) return 0.0;
-    return L.c[0] * (0.5 * (L.a[0][i - 1] + L.a[0][i])) * L.a[1][i] * L.a[2][i];
+    return L.c[0] * (0.5 * (at(0, -1) + at(0, 0))) * at(1, 0) * at(2, 0);
   } else if constexpr (KIND == LD_W_SXX) {  // StrainRates.py:250-276, component L.sub
-    const double* const* g = L.a;  // dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
-    auto stag = [&](const double* d) -> double {
-      if (z == 0) return d[i];
+    // inputs: dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
+    auto stag = [&](int k) -> double {
+      if (z == 0) return at(k, 0);
       if (z == nz - 1) return 0.0;
-      return 0.5 * (d[i - 1] + d[i]);
+      return 0.5 * (at(k, -1) + at(k, 0));
     };
     switch (L.sub) {
-      case 0: return stag(g[0]);                       // S11 = ux
-      case 1: return stag(g[4]);                       // S22 = vy
-      case 2: return stag(g[8]);                       // S33 = wz
-      case 3: return 0.5 * (stag(g[3]) + stag(g[1]));  // S12
-      case 4: {                                        // S13
-        const double wx = (z == 0) ? 0.5 * (g[2][i] + g[2][i + 1]) : g[2][i];
-        return 0.5 * (g[6][i] + wx);
+      case 0: return stag(0);                    // S11 = ux
+      case 1: return stag(4);                    // S22 = vy
+      case 2: return stag(8);                    // S33 = wz
+      case 3: return 0.5 * (stag(3) + stag(1));  // S12
+      case 4: {                                  // S13
+        const double wx = (z == 0) ? 0.5 * (at(2, 0) + at(2, 1)) : at(2, 0);
+        return 0.5 * (at(6, 0) + wx);
       }
-      default: {                                       // S23
-        const double wy = (z == 0) ? 0.5 * (g[5][i] + g[5][i + 1]) : g[5][i];
-        return 0.5 * (g[7][i] + wy);
+      default: {                                 // S23
+        const double wy = (z == 0) ? 0.5 * (at(5, 0) + at(5, 1)) : at(5, 0);
+        return 0.5 * (at(7, 0) + wy);
       }
     }
   } else if constexpr (KIND == LD_THZ) {  // DynamicSGS_ScalarLASDD_SM.py:182-185
-    const double* d = L.a[0];
-    if (z == 0 || z == nz - 1) return d[i];
-    return 0.5 * (d[i] + d[i + 1]);
+    if (z == 0 || z == nz - 1) return at(0, 0);
+    return 0.5 * (at(0, 0) + at(0, 1));
   } else {  // LD_MUL_THZ: S * THz
-    const double* d = L.a[1];
-    const double t = (z == 0 || z == nz - 1) ? d[i] : 0.5 * (d[i] + d[i + 1]);
-    return L.a[0][i] * t;
+    const double t = (z == 0 || z == nz - 1) ? at(1, 0) : 0.5 * (at(1, 0) + at(1, 1));
+    return at(0, 0) * t;
   }
+}
+
+template <int KIND>
+__device__ __forceinline__ double ldv(const Loader& L, size_t i, int z) {
+  return ev_kind<KIND>(L, [&](int k, int d) { return L.a[k][i + d]; }, z, L.nz);
+}
+
+// Input k around a packed column: levels z-1, z, z+1, z+2.
+struct Q4 {
+  double m, x, y, p;
+};
+
+// One 16-byte load per input for the pair (z, z+1); the z-1 and z+2
+// neighbours (NM, NP) come from the adjacent columns of the same row, which
+// sit in adjacent lanes (lane % C == column), by warp shuffles, and from a
+// scalar load at the tile's edge columns.  Every lane of the warp must call
+// it; lanes with ok == false contribute zeros.
+template <int C, bool NM, bool NP>
+__device__ __forceinline__ Q4 fetch_q4(const double* a, size_t i, int z, int nz, int c, bool ok) {
+  Q4 q{0.0, 0.0, 0.0, 0.0};
+  const bool in = ok && z < nz;
+  if (in) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(a + i));
+    q.x = v.x;
+    q.y = v.y;
+  }
+  if constexpr (NM) {
+    const double t = __shfl_up_sync(0xffffffffu, q.y, 1);
+    q.m = (c == 0) ? ((in && z > 0) ? __ldg(a + i - 1) : 0.0) : t;
+  }
+  if constexpr (NP) {
+    const double t = __shfl_down_sync(0xffffffffu, q.x, 1);
+    q.p = (c == C - 1) ? ((in && z + 2 < nz) ? __ldg(a + i + 2) : 0.0) : t;
+  }
+  return q;
+}
+
+// Value pair (z, z+1) of the loader at linear index i of level z (z even,
+// nz even).  Warp-collective (see fetch_q4).
+template <int KIND, int C>
+__device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz, int c,
+                                        bool ok) {
+  constexpr int NIN = (KIND == LD_FIELD || KIND == LD_THZ) ? 1
+                      : (KIND == LD_MUL || KIND == LD_MUL_THZ) ? 2
+                      : (KIND == LD_MUL3 || KIND == LD_PRESSURE_R || KIND == LD_STRESS_UVP ||
+                         KIND == LD_STRESS_W) ? 3
+                      : (KIND == LD_W_SXX) ? 9 : 6;
+  Q4 q[NIN];
+  if constexpr (KIND == LD_W_SXX) {
+#pragma unroll
+    for (int k = 0; k < NIN; k++) q[k] = Q4{0.0, 0.0, 0.0, 0.0};
+    switch (L.sub) {  // uniform over the launch
+      case 0: q[0] = fetch_q4<C, true, false>(L.a[0], i, z, nz, c, ok); break;
+      case 1: q[4] = fetch_q4<C, true, false>(L.a[4], i, z, nz, c, ok); break;
+      case 2: q[8] = fetch_q4<C, true, false>(L.a[8], i, z, nz, c, ok); break;
+      case 3:
+        q[3] = fetch_q4<C, true, false>(L.a[3], i, z, nz, c, ok);
+        q[1] = fetch_q4<C, true, false>(L.a[1], i, z, nz, c, ok);
+        break;
+      case 4:
+        q[6] = fetch_q4<C, false, false>(L.a[6], i, z, nz, c, ok);
+        q[2] = fetch_q4<C, false, false>(L.a[2], i, z, nz, c, ok);
+        break;
+      default:
+        q[7] = fetch_q4<C, false, false>(L.a[7], i, z, nz, c, ok);
+        q[5] = fetch_q4<C, false, false>(L.a[5], i, z, nz, c, ok);
+        break;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NIN; k++) {
+      constexpr bool any_m = (KIND == LD_ADV_Z || KIND == LD_STRESS_W);
+      constexpr bool any_p = (KIND == LD_ADV_XY || KIND == LD_SCALAR_ADV || KIND == LD_THZ ||
+                              KIND == LD_MUL_THZ);
+      const bool nm = (KIND == LD_ADV_Z && k < 2) || (KIND == LD_STRESS_W && k == 0);
+      const bool np = (KIND == LD_ADV_XY && k >= 3) ||
+                      (KIND == LD_SCALAR_ADV && (k == 2 || k == 5)) || (KIND == LD_THZ) ||
+                      (KIND == LD_MUL_THZ && k == 1);
+      if (any_m && nm) q[k] = fetch_q4<C, true, false>(L.a[k], i, z, nz, c, ok);
+      else if (any_p && np) q[k] = fetch_q4<C, false, true>(L.a[k], i, z, nz, c, ok);
+      else q[k] = fetch_q4<C, false, false>(L.a[k], i, z, nz, c, ok);
+    }
+  }
+  auto at0 = [&](int k, int d) -> double { return d < 0 ? q[k].m : (d == 0 ? q[k].x : q[k].y); };
+  auto at1 = [&](int k, int d) -> double { return d < 0 ? q[k].x : (d == 0 ? q[k].y : q[k].p); };
+  return make_double2(ev_kind<KIND>(L, at0, z, nz), ev_kind<KIND>(L, at1, z + 1, nz));
 }
 
 // Transform of an n x C tile: compile-time specialised for the lengths in
