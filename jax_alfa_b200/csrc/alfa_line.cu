@@ -196,65 +196,10 @@ __host__ __device__ constexpr int line_threads() {
   return ct_threads(C, NIN) > ct_threads(C, NOUT) ? ct_threads(C, NIN) : ct_threads(C, NOUT);
 }
 
-// value pair (z, z+1) of the loader at linear index i
-template <int KIND>
-__device__ __forceinline__ cd load_pair(const Loader& L, size_t i, int z, int nz) {
-  cd t = make_double2(0.0, 0.0);
-  if (KIND == LD_FIELD && (nz & 1) == 0) {
-    if (z < nz) t = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
-  } else {
-    if (z < nz) t.x = ldv<KIND>(L, i, z);
-    if (z + 1 < nz) t.y = ldv<KIND>(L, i + 1, z + 1);
-  }
-  return t;
-}
-
-// store (or accumulate) a scaled value pair at linear index i
-__device__ __forceinline__ void store_pair(const LineOut& o, size_t i, int z, int nz, cd v) {
-  if (z >= nz) return;
-  double* __restrict__ dst = o.dst;
-  double2 w = make_double2(o.scale * v.x, o.scale * v.y);
-  if ((nz & 1) == 0) {
-    double2* p = reinterpret_cast<double2*>(dst + i);
-    if (o.accumulate) {
-      const double2 pv = *p;
-      w.x += pv.x;
-      w.y += pv.y;
-    }
-    *p = w;
-  } else {
-    if (o.accumulate) {
-      w.x += dst[i];
-      if (z + 1 < nz) w.y += dst[i + 1];
-    }
-    dst[i] = w.x;
-    if (z + 1 < nz) dst[i + 1] = w.y;
-  }
-}
-
 // first-pass gather: v[q*R + r] = (x, x') at row j + r*NR of line c
 template <int KIND, int C, int N, int NT>
 __device__ __forceinline__ void line_gather(const LineArgs& a, long long f, int z0, cd* v) {
-  constexpr int R = ct_radix(N);
-  constexpr int NR = N / R;
-  constexpr int B = NR * C;
-  constexpr int MB = (B + NT - 1) / NT;
-#pragma unroll
-  for (int q = 0; q < MB; q++) {
-    const int b = threadIdx.x + q * NT;
-    const int c = b % C;
-    const int j = b / C;
-    const int z = z0 + 2 * c;
-    const bool ok = (B % NT == 0 || b < B);
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      const size_t i = (size_t)(f * a.fs_in + (long long)(j + r * NR) * a.rs_in) + z;
-      if (KIND != LD_FIELD && (a.nz & 1) == 0)
-        v[q * R + r] = eval_pair<KIND, C>(a.L, i, z, a.nz, c, ok);
-      else
-        v[q * R + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
-    }
-  }
+  gather_rows<KIND, C, N, NT>(a.L, a.nz, (size_t)(f * a.fs_in), (size_t)a.rs_in, z0, v);
 }
 
 template <int C, int N, int NT>

@@ -70,6 +70,33 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
   const int z0 = blockIdx.x * (2 * YC);
   const int row = blockIdx.y;
   cd* b0 = sm;
+  if constexpr (N > 0) {
+    // first pass straight from global memory (register-resident start)
+    constexpr int NT = tile_threads<YC, N>();
+    constexpr int R = ct_radix(N);
+    cd v[ct_mb(YC, N, 1, NT) * R];
+    const size_t base = (size_t)row * N * nz;
+    switch (L.kind) {
+#define ALFA_G(K) \
+  case K: gather_rows<K, YC, N, NT>(L, nz, base, (size_t)nz, z0, v); break;
+      ALFA_G(LD_FIELD) ALFA_G(LD_MUL) ALFA_G(LD_MUL3) ALFA_G(LD_PRESSURE_R) ALFA_G(LD_ADV_XY)
+      ALFA_G(LD_ADV_Z) ALFA_G(LD_SCALAR_ADV) ALFA_G(LD_STRESS_UVP) ALFA_G(LD_STRESS_W)
+      ALFA_G(LD_W_SXX) ALFA_G(LD_THZ)
+#undef ALFA_G
+      default: gather_rows<LD_MUL_THZ, YC, N, NT>(L, nz, base, (size_t)nz, z0, v); break;
+    }
+    if constexpr (R == N) {
+      if (threadIdx.x < YC) {
+        dftR<R, -1>(v);
+#pragma unroll
+        for (int r = 0; r < R; r++) b0[r * YC + threadIdx.x] = v[r];
+      }
+    } else {
+      ct_first_reg<-1, YC, N, NT>(v, b0);
+      ct_passes<-1, YC, N, R, NT>(b0, p.tw);
+    }
+    __syncthreads();
+  } else {
   switch (L.kind) {
     case LD_FIELD: y_fwd_load<LD_FIELD>(L, row, n, z0, b0); break;
     case LD_MUL: y_fwd_load<LD_MUL>(L, row, n, z0, b0); break;
@@ -85,6 +112,7 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
     default: y_fwd_load<LD_MUL_THZ>(L, row, n, z0, b0); break;
   }
   tile_fft<-1, YC, N, tile_threads<YC, N>()>(b0, p);
+  }
   const cd* Z = b0;
   for (int t = threadIdx.x; t < K * YC; t += blockDim.x) {
     const int k = t / YC, c = t % YC;
@@ -112,8 +140,76 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
   const int z0 = blockIdx.x * (2 * YC);
   const int row = blockIdx.y;
   cd* b0 = sm;
-  const int total = (h + 1) * YC;
   const bool pair = (nz & 1) == 0;  // z, z+1 both present whenever z is
+  if constexpr (N > 0) {
+    // Hermitian expansion of the two packed columns straight into the first
+    // pass's registers; the last pass stores straight from registers
+    constexpr int NT = tile_threads<YC, N>();
+    constexpr int R = ct_radix(N);
+    constexpr int NR = N / R;
+    constexpr int B = NR * YC;
+    constexpr int MB = ct_mb(YC, N, 1, NT);
+    cd v[MB * R];
+#pragma unroll
+    for (int q = 0; q < MB; q++) {
+      const int b = threadIdx.x + q * NT;
+      const int c = b % YC;
+      const int j = b / YC;
+      const int z = z0 + 2 * c;
+      const bool ok = (B % NT == 0 || b < B) && z < nz;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int k = j + r * NR;
+        const int src = k <= h ? k : N - k;
+        cd a = make_double2(0.0, 0.0), bb = make_double2(0.0, 0.0);
+        if (ok && src < K) {
+          const size_t o = ((size_t)row * K + src) * nz + z;
+          a = __ldg(T + o);
+          if (pair || z + 1 < nz) bb = __ldg(T + o + 1);
+        }
+        if (k == 0 || k == h) {
+          a.y = 0.0;
+          bb.y = 0.0;
+        }
+        v[q * R + r] = k <= h ? make_double2(a.x - bb.y, a.y + bb.x)
+                              : make_double2(a.x + bb.y, bb.x - a.y);
+      }
+    }
+    const size_t base = (size_t)row * N * nz;
+    if constexpr (R == N) {
+      if (threadIdx.x < YC) {
+        dftR<R, +1>(v);
+        const int z = z0 + 2 * threadIdx.x;
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          store_pair2(out, scale, accumulate, base + (size_t)r * nz + z, z, nz, v[r]);
+      }
+    } else {
+      ct_first_reg<+1, YC, N, NT>(v, b0);
+      ct_mid_passes<+1, YC, N, R, NT>(b0, p.tw);
+      __syncthreads();
+      constexpr int NSL = ct_last_ns(N);
+      constexpr int RL = N / NSL;
+      constexpr int BL = NSL * YC;
+      constexpr int ML = ct_mb(YC, N, NSL, NT);
+      cd u[ML * RL];
+      ct_last_reg<+1, YC, N, NT>(b0, p.tw, u);
+#pragma unroll
+      for (int q = 0; q < ML; q++) {
+        const int b = threadIdx.x + q * NT;
+        if (!(BL % NT == 0 || b < BL)) continue;
+        const int c = b % YC;
+        const int j = b / YC;
+        const int z = z0 + 2 * c;
+#pragma unroll
+        for (int r = 0; r < RL; r++)
+          store_pair2(out, scale, accumulate, base + (size_t)(j + r * NSL) * nz + z, z, nz,
+                      u[q * RL + r]);
+      }
+    }
+    return;
+  }
+  const int total = (h + 1) * YC;
   for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
     cd A[U], B[U];
 #pragma unroll

@@ -171,6 +171,75 @@ __device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz
   return make_double2(ev_kind<KIND>(L, at0, z, nz), ev_kind<KIND>(L, at1, z + 1, nz));
 }
 
+// value pair (z, z+1) of the loader at linear index i
+template <int KIND>
+__device__ __forceinline__ cd load_pair(const Loader& L, size_t i, int z, int nz) {
+  cd t = make_double2(0.0, 0.0);
+  if (KIND == LD_FIELD && (nz & 1) == 0) {
+    if (z < nz) t = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+  } else {
+    if (z < nz) t.x = ldv<KIND>(L, i, z);
+    if (z + 1 < nz) t.y = ldv<KIND>(L, i + 1, z + 1);
+  }
+  return t;
+}
+
+// store (or accumulate) a scaled value pair at linear index i of dst
+__device__ __forceinline__ void store_pair2(double* __restrict__ dst, double scale, int accumulate,
+                                            size_t i, int z, int nz, cd v) {
+  if (z >= nz) return;
+  double2 w = make_double2(scale * v.x, scale * v.y);
+  if ((nz & 1) == 0) {
+    double2* p = reinterpret_cast<double2*>(dst + i);
+    if (accumulate) {
+      const double2 pv = *p;
+      w.x += pv.x;
+      w.y += pv.y;
+    }
+    *p = w;
+  } else {
+    if (accumulate) {
+      w.x += dst[i];
+      if (z + 1 < nz) w.y += dst[i + 1];
+    }
+    dst[i] = w.x;
+    if (z + 1 < nz) dst[i + 1] = w.y;
+  }
+}
+
+__device__ __forceinline__ void store_pair(const LineOut& o, size_t i, int z, int nz, cd v) {
+  store_pair2(o.dst, o.scale, o.accumulate, i, z, nz, v);
+}
+
+// First-pass gather of a length-N transform over C packed columns:
+// v[q*R + r] = loader pair at row j + r*(N/R) of column c, for butterfly
+// b = threadIdx.x + q*NT (c = b % C, j = b / C); element index
+// base + row*rs + z.  Warp-collective for non-field kinds (eval_pair).
+template <int KIND, int C, int N, int NT>
+__device__ __forceinline__ void gather_rows(const Loader& L, int nz, size_t base, size_t rs,
+                                            int z0, cd* v) {
+  constexpr int R = ct_radix(N);
+  constexpr int NR = N / R;
+  constexpr int B = NR * C;
+  constexpr int MB = (B + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 2 * c;
+    const bool ok = (B % NT == 0 || b < B);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const size_t i = base + (size_t)(j + r * NR) * rs + z;
+      if (KIND != LD_FIELD && (nz & 1) == 0)
+        v[q * R + r] = eval_pair<KIND, C>(L, i, z, nz, c, ok);
+      else
+        v[q * R + r] = ok ? load_pair<KIND>(L, i, z, nz) : make_double2(0.0, 0.0);
+    }
+  }
+}
+
 // Transform of an n x C tile: compile-time specialised for the lengths in
 // the dispatch tables below (N > 0), the runtime plan otherwise (N == 0).
 template <int S, int C, int N, int NT>
