@@ -259,10 +259,15 @@ int alfa_PlanarMean_noalloc(const double* F, int nx, int ny, int nz, double* mea
 unsigned long long alfa_launch_count(void);
 /* Times `reps` back-to-back launches of one building-block kernel on the
  * context's stream with CUDA events (inputs: the context's state/workspace):
- *   0 y-forward real->half spectrum, regular grid   (reads N, writes S)
- *   1 x-column: forward FFT + two i*k outputs       (reads S, writes 2 S)
- *   2 y-inverse half spectrum->real, regular grid   (reads S, writes N)
- *   3 y-inverse onto the 3/2-padded grid            (reads mx*nyh*nz, writes P)
+ *   0 y pad pass   (nx,ny,nz) -> (nx,my,nz)        (reads N, writes nx*my*nz)
+ *   1 x pad pass   (nx,my,nz) -> (mx,my,nz)        (reads nx*my*nz, writes P)
+ *   2 x unpad pass (mx,my,nz) -> (nx,my,nz)        (reads P, writes nx*my*nz)
+ *   3 y unpad pass (nx,my,nz) -> (nx,ny,nz)        (reads nx*my*nz, writes N)
+ *   4 x derivative line pass                       (reads N, writes N)
+ *   5 y-forward real -> half spectrum (2-D path)   (reads N, writes S)
+ *   6 x-column: forward FFT + two i*k outputs      (reads S, writes 2 S)
+ *   7 y-inverse half spectrum -> real (2-D path)   (reads S, writes N)
+ * (N, P, S: real, padded real and half-spectrum complex field sizes.)
  * ms = average duration of one launch; bytes = its algorithmic HBM bytes. */
 int alfa_time_kernel(alfa_ctx*, int which, int reps, double* ms /* host */,
                      double* bytes /* host */);

@@ -13,11 +13,26 @@
 using namespace alfa;
 
 #include <atomic>
+#include <map>
+#include <mutex>
 
 namespace alfa {
 
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> g(mu);
+  size_t& have = done[{dev, kernel}];
+  if (have >= bytes) return;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+      cudaSuccess)
+    have = bytes;
+}
 
 // ---------------------------------------------------------------------------
 // Workspace: named field slots carved from one allocation
@@ -816,6 +831,7 @@ int alfa_create(const alfa_config* cfg, alfa_ctx** out) {
   alfa_ctx* c = new alfa_ctx();
   cudaGetDevice(&c->e.device);
   int st = engine_init(c->e, *cfg);
+  if (!st) cudaDeviceGetAttribute(&c->e.sms, cudaDevAttrMultiProcessorCount, c->e.device);
   if (st) {
     g_create_error = c->e.err;
     engine_free(c->e);
@@ -1280,13 +1296,19 @@ unsigned long long alfa_launch_count(void) { return g_launches.load(); }
 
 int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes) {
   CTX_CHECK(c);
-  if (!ms || !bytes || reps < 1 || which < 0 || which > 3)
+  if (!ms || !bytes || reps < 1 || which < 0 || which > 7)
     return c->e.fail("time_kernel: bad arguments", ALFA_E_SHAPE);
   Engine& e = c->e;
   Work& W = c->w;
-  const double S16 = 16.0 * e.nx * e.nyh * e.nz, N8 = 8.0 * e.N();
-  // inputs for the inverse kernels: one forward + x pass
-  launch_y_fwd(e, ld_field(e, W.u), e.nx, e.pny, e.nyh, e.T[0]);
+  const double N8 = 8.0 * e.N(), Y8 = 8.0 * e.nx * e.my * e.nz, P8 = 8.0 * e.P();
+  const double S16 = 16.0 * e.nx * e.nyh * e.nz;
+  auto lo1 = [](int map, double* dst, double scale) {
+    LineOut o{};
+    o.map = map;
+    o.scale = scale;
+    o.dst = dst;
+    return o;
+  };
   XOut o[2];
   for (int i = 0; i < 2; i++) {
     o[i] = XOut{};
@@ -1297,29 +1319,50 @@ int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes
     o[i].dst = e.T[1 + i];
     o[i].inv = e.pnx;
   }
-  launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh);
-  XOut op = XOut{};
-  op.kind = XO_INV;
-  op.map = MAP_PAD;
-  op.K = e.nyh;
-  op.rows = e.mx;
-  op.dst = e.T[3];
-  op.inv = e.pmx;
-  launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 1, &op, e.nyh);
+  // inputs of the later stages: one pass of each earlier stage
+  auto run = [&](int w) {
+    switch (w) {
+      case 0: {  // y pad pass: (nx, ny, nz) -> (nx, my, nz)
+        LineOut q = lo1(LM_PAD, W.Lpad, 1.0 / e.my);
+        launch_line(e, 1, ld_field(e, W.u), e.nx, e.ny, e.ny, e.my, 1, &q);
+        break;
+      }
+      case 1: {  // x pad pass: (nx, my, nz) -> (mx, my, nz)
+        LineOut q = lo1(LM_PAD, W.Pb[0], 1.0 / e.mx);
+        launch_line(e, 0, ld_field(e, W.Lpad), e.nx, e.my, e.nx, e.mx, 1, &q);
+        break;
+      }
+      case 2: {  // x unpad pass: (mx, my, nz) -> (nx, my, nz)
+        LineOut q = lo1(LM_UNPAD, W.Lpad, 1.0 / e.nx);
+        launch_line(e, 0, ld_field(e, W.Pb[0]), e.mx, e.my, e.mx, e.nx, 1, &q);
+        break;
+      }
+      case 3: {  // y unpad pass: (nx, my, nz) -> (nx, ny, nz)
+        LineOut q = lo1(LM_UNPAD, e.W, (9.0 / 4.0) / e.ny);
+        launch_line(e, 1, ld_field(e, W.Lpad), e.nx, e.my, e.my, e.ny, 1, &q);
+        break;
+      }
+      case 4: {  // x derivative pass
+        LineOut q = lo1(LM_DERIV, e.W, 1.0 / e.nx);
+        launch_line(e, 0, ld_field(e, W.u), e.nx, e.ny, e.nx, e.nx, 1, &q);
+        break;
+      }
+      case 5: launch_y_fwd(e, ld_field(e, W.u), e.nx, e.pny, e.nyh, e.T[0]); break;
+      case 6: launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh); break;
+      default: launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, 1.0, e.W, 0); break;
+    }
+  };
+  if (which == 1 || which == 2 || which == 3) run(0);
+  if (which == 2 || which == 3) run(1);
+  if (which == 3) run(2);
+  if (which == 6 || which == 7) run(5);
+  if (which == 7) run(6);
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
-  auto run = [&]() {
-    switch (which) {
-      case 0: launch_y_fwd(e, ld_field(e, W.u), e.nx, e.pny, e.nyh, e.T[0]); break;
-      case 1: launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh); break;
-      case 2: launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, 1.0, e.W, 0); break;
-      default: launch_y_inv(e, e.T[3], e.mx, e.nyh, e.pmy, 1.0, W.Pb[0], 0); break;
-    }
-  };
-  run();  // warm
+  run(which);  // warm
   cudaEventRecord(a, e.stream);
-  for (int r = 0; r < reps; r++) run();
+  for (int r = 0; r < reps; r++) run(which);
   cudaEventRecord(b, e.stream);
   cudaEventSynchronize(b);
   float t = 0.f;
@@ -1328,10 +1371,14 @@ int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes
   cudaEventDestroy(b);
   *ms = (double)t / reps;
   switch (which) {
-    case 0: *bytes = N8 + S16; break;
-    case 1: *bytes = S16 + 2 * S16; break;
-    case 2: *bytes = S16 + N8; break;
-    default: *bytes = 16.0 * e.mx * e.nyh * e.nz + 8.0 * e.P(); break;
+    case 0: *bytes = N8 + Y8; break;
+    case 1: *bytes = Y8 + P8; break;
+    case 2: *bytes = P8 + Y8; break;
+    case 3: *bytes = Y8 + N8; break;
+    case 4: *bytes = 2 * N8; break;
+    case 5: *bytes = N8 + S16; break;
+    case 6: *bytes = 3 * S16; break;
+    default: *bytes = S16 + N8; break;
   }
   return check_launch(e, "time_kernel");
 }

@@ -14,6 +14,11 @@ namespace alfa {
 // site calls note_launch(); read through alfa_launch_count()).
 void note_launch();
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device (the attribute call is made once per kernel, device and
+// size increase, not on every launch).
+void raise_smem_limit(const void* kernel, size_t bytes);
+
 // ---------------------------------------------------------------------------
 // Physical-space value producers for the y-forward FFT stage.  Instead of
 // materialising a product or a staggered combination as a full field and
@@ -84,6 +89,7 @@ struct Engine {
   cudaStream_t stream = 0;
   std::string err;
   int device = 0;
+  int sms = 148;  // multiprocessors of the device
 
   // grid
   int nx, ny, nz, mx, my, nxh, nyh, mxh, myh;

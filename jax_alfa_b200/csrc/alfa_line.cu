@@ -699,10 +699,8 @@ __global__ void __launch_bounds__(256) k_materialize(Loader L, size_t n, double*
 }
 
 void materialize(Engine& e, const Loader& L, size_t n, double* out) {
-  int dev_sms = 148;
-  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e.device);
   const size_t want = (n + 255) / 256;
-  const unsigned blocks = (unsigned)(want < (size_t)dev_sms * 16 ? want : (size_t)dev_sms * 16);
+  const unsigned blocks = (unsigned)(want < (size_t)e.sms * 16 ? want : (size_t)e.sms * 16);
   ::alfa::note_launch();
   switch (L.kind) {
 #define ALFA_MAT(K) \

@@ -359,9 +359,107 @@ __global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x
   const int M = a.maxrows * C;
   cd* buf[2] = {sm, sm + M};
 
+  const bool have = ky < a.Kin;
+  if constexpr (NI > 0 && NO > 0) {
+    if (!a.in_spec) {
+      // forward transform with its first pass straight from global memory
+      constexpr int R = ct_radix(NI);
+      constexpr int NR = NI / R;
+      constexpr int B = NR * C;
+      constexpr int MB = ct_mb(C, NI, 1, NT);
+      cd v[MB * R];
+#pragma unroll
+      for (int q = 0; q < MB; q++) {
+        const int b = threadIdx.x + q * NT;
+        const int c = b % C;
+        const int j = b / C;
+        const int z = z0 + c;
+        const bool ok = have && (B % NT == 0 || b < B) && z < nz;
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          v[q * R + r] = ok ? __ldg(&a.src[((size_t)(j + r * NR) * a.Kin + ky) * nz + z])
+                            : make_double2(0.0, 0.0);
+      }
+      if constexpr (R == NI) {
+        if (threadIdx.x < C) {
+          dftR<R, -1>(v);
+#pragma unroll
+          for (int r = 0; r < R; r++) buf[0][r * C + threadIdx.x] = v[r];
+        }
+      } else {
+        ct_first_reg<-1, C, NI, NT>(v, buf[0]);
+        ct_passes<-1, C, NI, R, NT>(buf[0], a.fwd.tw);
+      }
+      __syncthreads();
+      const cd* S = buf[0];
+      cd* f0 = buf[1];
+      for (int oi = 0; oi < a.nout; oi++) {
+        const XOut& o = a.out[oi];
+        if (o.kind == XO_SPEC) {
+          for (int t = threadIdx.x; t < o.rows * C; t += blockDim.x) {
+            const int k = t / C, c = t % C;
+            const int z = z0 + c;
+            if (z < nz) o.dst[((size_t)k * o.K + ky) * nz + z] = map_value<C>(a, o, S, k, ky, c);
+          }
+          continue;
+        }
+        if (ky >= o.K) continue;  // column not stored: zero by convention
+        // inverse transform: first pass fed through the map, last pass
+        // stored straight from registers
+        constexpr int RO = ct_radix(NO);
+        constexpr int NRO = NO / RO;
+        constexpr int BO = NRO * C;
+        constexpr int MBO = ct_mb(C, NO, 1, NT);
+        cd w[MBO * RO];
+#pragma unroll
+        for (int q = 0; q < MBO; q++) {
+          const int b = threadIdx.x + q * NT;
+          const int c = b % C;
+          const int j = b / C;
+#pragma unroll
+          for (int r = 0; r < RO; r++)
+            w[q * RO + r] = (BO % NT == 0 || b < BO) ? map_value<C>(a, o, S, j + r * NRO, ky, c)
+                                                      : make_double2(0.0, 0.0);
+        }
+        if constexpr (RO == NO) {
+          if (threadIdx.x < C) {
+            dftR<RO, +1>(w);
+            const int z = z0 + threadIdx.x;
+            if (z < nz) {
+#pragma unroll
+              for (int r = 0; r < RO; r++) o.dst[((size_t)r * o.K + ky) * nz + z] = w[r];
+            }
+          }
+        } else {
+          ct_first_reg<+1, C, NO, NT>(w, f0);
+          ct_mid_passes<+1, C, NO, RO, NT>(f0, o.inv.tw);
+          __syncthreads();
+          constexpr int NSL = ct_last_ns(NO);
+          constexpr int RL = NO / NSL;
+          constexpr int BL = NSL * C;
+          constexpr int ML = ct_mb(C, NO, NSL, NT);
+          cd u[ML * RL];
+          ct_last_reg<+1, C, NO, NT>(f0, o.inv.tw, u);
+#pragma unroll
+          for (int q = 0; q < ML; q++) {
+            const int b = threadIdx.x + q * NT;
+            if (!(BL % NT == 0 || b < BL)) continue;
+            const int c = b % C;
+            const int j = b / C;
+            const int z = z0 + c;
+            if (z >= nz) continue;
+#pragma unroll
+            for (int r = 0; r < RL; r++)
+              o.dst[((size_t)(j + r * NSL) * o.K + ky) * nz + z] = u[q * RL + r];
+          }
+        }
+        __syncthreads();
+      }
+      return;
+    }
+  }
   // load the input column set, U loads in flight per thread
   const int total = a.rows_in * C;
-  const bool have = ky < a.Kin;
   for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
     cd v[U];
 #pragma unroll

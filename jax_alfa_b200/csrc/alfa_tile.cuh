@@ -256,9 +256,7 @@ __host__ __device__ constexpr int tile_threads() {
   return N == 0 ? MAXTHREADS : ct_threads(C, N);
 }
 
-static inline void set_smem(const void* f, size_t bytes) {
-  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
+static inline void set_smem(const void* f, size_t bytes) { raise_smem_limit(f, bytes); }
 
 #define ALFA_Y_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \
   X(512) X(768)
