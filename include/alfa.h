@@ -59,7 +59,7 @@ typedef struct alfa_config {
   double T_0;                    /* K */
   int optSgs;                    /* 0 static, 1 LASDD-SM, 3 LAD-SM */
   int dynamicSGS_call_time;
-  int FGR;                       /* 1 (3/2-rule dealiasing) */
+  int FGR;                       /* 1: 3/2-rule dealiasing, TFR 2; >= 2: no dealiasing, TFR sqrt(2) */
   double Cs2, Cs2PrRatio;        /* initial coefficients */
   int optDamping;
   double z_damping, RelaxTime;   /* m, s */
@@ -165,7 +165,8 @@ int alfa_BuoyancyOpt2(alfa_ctx*, const double* TH, double* buoyancy); /* NSE_Buo
 /* grads[9] as velocityGradients' out.  mom[25] receives DynamicSGS's tuple
  * (DynamicSGS_Main.py:323-331): txx, tyy, tzz, txy, txz, tyz, Cs2_1D_avg1,
  * Cs2_1D_avg2, beta1_1D, Cs2_3D, u_, v_, w_, u_hat, v_hat, w_hat, u_hatd,
- * v_hatd, w_hatd, S_uvp, S_uvp_pad (mx,my,nz), S_w, S_w_pad (mx,my,nz),
+ * v_hatd, w_hatd, S_uvp, S_uvp_pad (mx,my,nz; (nx,ny,nz) when FGR > 1), S_w,
+ * S_w_pad (as S_uvp_pad),
  * S_uvp_hat, S_uvp_hatd.  Entries 6..9 may be NULL (they duplicate the
  * dedicated outputs).                                  NSE_SGSTerms.py:113 */
 int alfa_DivStressDynamicSGS(alfa_ctx*, const double* const grads[9], const double* u,

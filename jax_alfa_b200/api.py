@@ -109,6 +109,13 @@ class Alfa:
     def H(self):
         return (self.nx, self.ny)
 
+    @property
+    def Q(self):
+        """Shape of the reference's ``*_pad`` SGS slots: padded with FGR = 1,
+        the unpadded field itself otherwise (``DynamicSGS_Main.py`` passes
+        ``S_uvp_pad = S_uvp`` on the no-dealias branch)."""
+        return self.P if int(self.cfg.get("FGR", 1)) == 1 else self.N
+
     def _f(self, t):
         return self._p(t, self.N)
 
@@ -305,7 +312,7 @@ class Alfa:
         return out
 
     def _mom25(self):
-        return [None if 6 <= i <= 9 else self._new(self.P if i in (20, 22) else self.N)
+        return [None if 6 <= i <= 9 else self._new(self.Q if i in (20, 22) else self.N)
                 for i in range(25)]
 
     def DivStressDynamicSGS(self, dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz,
@@ -326,7 +333,7 @@ class Alfa:
     def DivFluxDynamicSGS(self, dynamicSGSmomentum, TH, dTHdx, dTHdy, dTHdz, SHFX, ZeRo3D=None,
                           ZeRo3D_fft=None, ZeRo3D_pad_fft=None, kx2=None, ky2=None):
         m = list(dynamicSGSmomentum)
-        shapes = [self.P if i in (10, 12) else self.N for i in range(15)]
+        shapes = [self.Q if i in (10, 12) else self.N for i in range(15)]
         qz, divq, r3 = self._new(self.N), self._new(self.N), self._new(self.N)
         r1, b2 = self._new((self.nz,)), self._new((self.nz,))
         self._call("alfa_DivFluxDynamicSGS", self._pp(m, shapes), self._f(TH), self._f(dTHdx),
@@ -339,7 +346,7 @@ class Alfa:
                            ZeRo3D_pad_fft=None, kx2=None, ky2=None):
         g = self._pp([dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz], [self.N] * 9)
         divt = [self._new(self.N) for _ in range(3)]
-        mom = [self._new(self.P if i in (7, 9) else self.N) for i in range(10)]
+        mom = [self._new(self.Q if i in (7, 9) else self.N) for i in range(10)]
         self._call("alfa_DivStressStaticSGS", g, self._f(Cs2_3D), self._f(u), self._f(v),
                    self._p(M_sfc_loc, self.H), self._p(MOSTfunctions[0], self.H),
                    self._p(MOSTfunctions[1], self.H), *[self._p(x) for x in divt], self._pp(mom))
@@ -349,7 +356,7 @@ class Alfa:
                          ZeRo3D=None, ZeRo3D_fft=None, ZeRo3D_pad_fft=None, kx2=None, ky2=None):
         m = list(staticSGSmomentum)
         qz, divq = self._new(self.N), self._new(self.N)
-        self._call("alfa_DivFluxStaticSGS", self._pp(m, [self.N, self.P, self.N, self.P]),
+        self._call("alfa_DivFluxStaticSGS", self._pp(m, [self.N, self.Q, self.N, self.Q]),
                    self._f(Cs2PrRatio_3D), self._f(dTHdx), self._f(dTHdy), self._f(dTHdz),
                    self._p(SHFX.contiguous(), self.H), self._p(qz), self._p(divq))
         return qz, divq

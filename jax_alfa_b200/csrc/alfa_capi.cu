@@ -148,7 +148,7 @@ int engine_init(Engine& e, const alfa_config& c) {
   e.nz = c.nz;
   if (c.nx < 4 || c.ny < 4 || c.nz < 3 || (c.nx % 2) || (c.ny % 2))
     return e.fail("grid must have even nx, ny >= 4 and nz >= 3", ALFA_E_CONFIG);
-  if (c.FGR != 1) return e.fail("only FGR = 1 (3/2-rule dealiasing) is implemented", ALFA_E_CONFIG);
+  if (c.FGR < 1) return e.fail("FGR must be >= 1", ALFA_E_CONFIG);
   if (!(c.optSgs == 0 || c.optSgs == 1 || c.optSgs == 3))
     return e.fail("optSgs must be 0 (static), 1 (LASDD-SM) or 3 (LAD-SM)", ALFA_E_CONFIG);
   if (c.dynamicSGS_call_time < 1) return e.fail("dynamicSGS_call_time must be >= 1", ALFA_E_CONFIG);
@@ -173,8 +173,11 @@ int engine_init(Engine& e, const alfa_config& c) {
   e.idz = 1.0 / e.dz;
   e.L = c.FGR * std::pow(e.dx * e.dy * e.dz, 1.0 / 3.0);
   e.dt_nondim = c.dt * 1.0 / e.z_scale;
-  e.TFR = 2;
-  e.optDealias = 1;
+  // DerivedVars.py: FGR = 1 -> 3/2-rule dealiasing with TFR = 2; FGR > 1 -> the
+  // grid filter removes the aliased band, products are formed in physical
+  // space (the *_NoDealias functions) and TFR = sqrt(2)
+  e.TFR = (c.FGR == 1) ? 2.0 : std::sqrt(2.0);
+  e.optDealias = (c.FGR == 1) ? 1 : 0;
   e.Cs2_init = c.Cs2;
   e.Cs2PrRatio_init = c.Cs2PrRatio;
   e.z_damping_nondim = c.z_damping / e.z_scale;
@@ -433,6 +436,12 @@ static void advection(alfa_ctx* c, const double* u, const double* v, const doubl
                       const double* wx, const double* wy, double* Cx, double* Cy, double* Cz) {
   Engine& e = c->e;
   double* const* Pb = c->w.Pb;
+  if (!e.optDealias) {  // Advection_NoDealias, NSE_AdvectionTerms.py:163-238
+    materialize(e, ld(e, LD_ADV_XY, {v, uy, vx, w, uz, wx}), e.N(), Cx);
+    materialize(e, ld(e, LD_ADV_XY, {u, vx, uy, w, vz, wy}), e.N(), Cy);
+    materialize(e, ld(e, LD_ADV_Z, {u, v, wx, uz, wy, vz}), e.N(), Cz);
+    return;
+  }
   const double* src[9] = {u, v, w, uy, uz, vx, vz, wx, wy};
   for (int i = 0; i < 9; i++) op2_pad(e, ld_field(e, src[i]), Pb[i], c->w.Lpad);
   // Pb: 0 up 1 vp 2 wp 3 uy 4 uz 5 vx 6 vz 7 wx 8 wy
@@ -448,6 +457,10 @@ static void scalar_advection(alfa_ctx* c, const double* u, const double* v, cons
                              bool reuse_uvw) {
   Engine& e = c->e;
   double* const* Pb = c->w.Pb;
+  if (!e.optDealias) {  // SCL_AdvectionTerms.py:114-150
+    materialize(e, ld(e, LD_SCALAR_ADV, {u, v, w, sx, sy, sz}), e.N(), out);
+    return;
+  }
   if (!reuse_uvw) {
     op2_pad(e, ld_field(e, u), Pb[0], c->w.Lpad);
     op2_pad(e, ld_field(e, v), Pb[1], c->w.Lpad);
@@ -483,6 +496,31 @@ static void sgs_stresses(alfa_ctx* c, const double* const g[9], const double* S_
   wall_override(e, u, v, M, pm, pm0, t6[4], t6[5]);
 }
 
+// StressesUVPnodes_NoDealias / StrainsWnodes_NoDealias / StressesWnodes_NoDealias
+// (SGSStresses_SM.py:149-178, :251-290; StrainRates.py:307-368): the same
+// products in physical space; S_w_pad receives S_w.
+static void sgs_stresses_nodealias(alfa_ctx* c, const double* const g[9], const double* Sij[6],
+                                   const double* S_uvp, const double* Cs2, const double* u,
+                                   const double* v, const double* M, const double* pm,
+                                   const double* pm0, double* const t6[6], double* S_w,
+                                   double* S_w_pad) {
+  Engine& e = c->e;
+  double* const* Pb = c->w.Pb;
+  const double cst = -2 * std::pow(e.L, 2.0);
+  for (int i = 0; i < 4; i++)
+    materialize(e, ld(e, LD_STRESS_UVP, {Cs2, S_uvp, Sij[i]}, cst), e.N(), t6[i]);
+  Loader Lw = ld(e, LD_W_SXX, {g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8]});
+  Lw.sub = 4;
+  materialize(e, Lw, e.N(), Pb[0]);  // S13 on w nodes
+  Lw.sub = 5;
+  materialize(e, Lw, e.N(), Pb[1]);  // S23 on w nodes
+  smag_w(e, g, S_w);
+  cudaMemcpyAsync(S_w_pad, S_w, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  materialize(e, ld(e, LD_STRESS_W, {Cs2, S_w, Pb[0]}, cst), e.N(), t6[4]);
+  materialize(e, ld(e, LD_STRESS_W, {Cs2, S_w, Pb[1]}, cst), e.N(), t6[5]);
+  wall_override(e, u, v, M, pm, pm0, t6[4], t6[5]);
+}
+
 // uvp strains + their padded copies: S11..S33 alias dudx, dvdy, dwdz.
 static void uvp_strains_padded(alfa_ctx* c, const double* const g[9], const double* Sij[6],
                                double* S_uvp, double* S_uvp_pad) {
@@ -495,6 +533,10 @@ static void uvp_strains_padded(alfa_ctx* c, const double* const g[9], const doub
   Sij[3] = w.S12;
   Sij[4] = w.S13;
   Sij[5] = w.S23;
+  if (!e.optDealias) {  // StrainsUVPnodes_NoDealias: S_uvp_pad is S_uvp
+    cudaMemcpyAsync(S_uvp_pad, S_uvp, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+    return;
+  }
   for (int i = 0; i < 6; i++) op2_pad(e, ld_field(e, Sij[i]), w.Pb[i], c->w.Lpad);
   const double* p6[6] = {w.Pb[0], w.Pb[1], w.Pb[2], w.Pb[3], w.Pb[4], w.Pb[5]};
   smag6(e, p6, e.P(), S_uvp_pad);
@@ -560,9 +602,13 @@ static int dynamic_sgs(alfa_ctx* c, const double* const g[9], const double* u, c
   clip_ratio(e, W.LM, W.MM, Cs2);
   cs2_profiles(e, Cs2, avg1, avg2);
   // stresses (SGSStresses_SM.py) with Cs2_3D_pad = Dealias1(FFT(Cs2_3D))
-  op2_pad(e, ld_field(e, Cs2), W.Pb[9], c->w.Lpad);
   double* t6[6] = {mom[0], mom[1], mom[2], mom[3], mom[4], mom[5]};
-  sgs_stresses(c, g, mom[20], u, v, M, pm, pm0, t6, mom[21], mom[22]);
+  if (e.optDealias) {
+    op2_pad(e, ld_field(e, Cs2), W.Pb[9], c->w.Lpad);
+    sgs_stresses(c, g, mom[20], u, v, M, pm, pm0, t6, mom[21], mom[22]);
+  } else {
+    sgs_stresses_nodealias(c, g, Sij, S_uvp, Cs2, u, v, M, pm, pm0, t6, mom[21], mom[22]);
+  }
   div_stress(c, mom[0], mom[1], mom[2], mom[3], mom[4], mom[5], divt[0], divt[1], divt[2]);
   return check_launch(e, "DivStressDynamicSGS");
 }
@@ -575,9 +621,13 @@ static int static_sgs(alfa_ctx* c, const double* const g[9], const double* Cs2, 
   Work& W = c->w;
   const double* Sij[6];
   uvp_strains_padded(c, g, Sij, mom10[6], mom10[7]);
-  op2_pad(e, ld_field(e, Cs2), W.Pb[9], c->w.Lpad);
   double* t6[6] = {mom10[0], mom10[1], mom10[2], mom10[3], mom10[4], mom10[5]};
-  sgs_stresses(c, g, mom10[7], u, v, M, pm, pm0, t6, mom10[8], mom10[9]);
+  if (e.optDealias) {
+    op2_pad(e, ld_field(e, Cs2), W.Pb[9], c->w.Lpad);
+    sgs_stresses(c, g, mom10[7], u, v, M, pm, pm0, t6, mom10[8], mom10[9]);
+  } else {
+    sgs_stresses_nodealias(c, g, Sij, mom10[6], Cs2, u, v, M, pm, pm0, t6, mom10[8], mom10[9]);
+  }
   div_stress(c, mom10[0], mom10[1], mom10[2], mom10[3], mom10[4], mom10[5], divt[0], divt[1],
              divt[2]);
   return check_launch(e, "DivStressStaticSGS");
@@ -589,11 +639,19 @@ static void scalar_fluxes(alfa_ctx* c, const double* S_uvp_pad, const double* S_
                           const double* qz_sfc, double* qz, double* divq) {
   Engine& e = c->e;
   Work& W = c->w;
+  const double cst = -2 * std::pow(e.L, 2.0);
+  if (!e.optDealias) {  // ScalarFluxes*_NoDealias (ScalarSGSFluxes_SM.py:98-126, :185-222)
+    materialize(e, ld(e, LD_STRESS_UVP, {r3, S_uvp_pad, gx}, cst), e.N(), W.qx);
+    materialize(e, ld(e, LD_STRESS_UVP, {r3, S_uvp_pad, gy}, cst), e.N(), W.qy);
+    materialize(e, ld(e, LD_STRESS_W, {r3, S_w_pad, gz}, cst), e.N(), qz);
+    set_plane0(e, qz_sfc, qz);
+    div_flux(c, W.qx, W.qy, qz, divq);
+    return;
+  }
   op2_pad(e, ld_field(e, gx), W.Pb[0], c->w.Lpad);
   op2_pad(e, ld_field(e, gy), W.Pb[1], c->w.Lpad);
   op2_pad(e, ld_field(e, gz), W.Pb[2], c->w.Lpad);
   op2_pad(e, ld_field(e, r3), W.Pb[3], c->w.Lpad);
-  const double cst = -2 * std::pow(e.L, 2.0);
   op2_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[0]}, cst), W.qx, c->w.Lpad);
   op2_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[1]}, cst), W.qy, c->w.Lpad);
   op2_unpad(e, ld(e, LD_STRESS_W, {W.Pb[3], S_w_pad, W.Pb[2]}, cst), qz, c->w.Lpad);

@@ -18,6 +18,8 @@ CALL_FIXTURES = [
     ("ref_convective_fluxhet_12x12x8.npz", "convective"),
     ("ref_stable_lu_12x12x8.npz", "stable"),
     ("ref_stable_het_12x12x8.npz", "stable"),
+    ("ref_convective_fgr2_12x12x8.npz", "convective"),  # FGR = 2: no dealiasing
+    ("ref_stable_fgr2_12x12x8.npz", "stable"),
 ]
 # The oracle restates the reference operation for operation; on the same
 # NumPy FFT it reproduces the recorded results to the last bit.  The bound
