@@ -736,6 +736,117 @@ class AlfaOracle:
         return r3, self.PlanarMean(r3), beta2
 
     # ------------------------------------------------------------------
+    # Wong-Lilly base model (optSgs = 2, 4)
+    # ------------------------------------------------------------------
+    def _wl_coeffs(self, a1, a3, a6, a8):
+        """Quintic coefficients (ff, ee, dd, cc, bb, aa) of the WL procedure
+        from the four independent plane means
+        (``DynamicSGS_LASDD_WL.py:262-277``, ``DynamicSGS_ScalarLASDD_WL.py:230-245``)."""
+        TFR = self.TFR
+        a2 = -(TFR ** (8 / 3)) * a1
+        a4 = -2 * TFR ** (4 / 3) * a3
+        a5 = TFR ** (8 / 3) * a3
+        a7 = -TFR ** (4 / 3) * a6
+        a9 = -2 * TFR ** (8 / 3) * a8
+        a10 = TFR ** (16 / 3) * a8
+        aa = a1 * a3 - a6 * a8
+        bb = a1 * a4 - a7 * a8
+        cc = a2 * a3 + a1 * a5 - a6 * a9
+        dd = a2 * a4 - a7 * a9
+        ee = a2 * a5 - a6 * a10
+        ff = -a7 * a10
+        return ff, ee, dd, cc, bb, aa
+
+    def LASDD_WL(self, u, v, w, S11, S22, S33, S12, S13, S23, ZeRo3D=None):
+        """``src/subgridscale/DynamicSGS_LASDD_WL.py:127-313``."""
+        nz, L, TFR = self.nz, self.L, self.TFR
+        u_, v_ = u.copy(), v.copy()
+        w_ = np.zeros_like(w)
+        w_[:, :, 1:nz - 1] = self.StagGridAvg(w[:, :, 1:nz])
+        w_[:, :, 0] = 0.5 * w[:, :, 1]
+        w_[:, :, nz - 1] = w[:, :, nz - 2]
+        (u_h, u_d), (v_h, v_d), (w_h, w_d) = (self._level1_level2(x) for x in (u_, v_, w_))
+        prods = (u_ ** 2, v_ ** 2, w_ ** 2, u_ * v_, u_ * w_, v_ * w_)
+        ph = [self._level1_level2(x) for x in prods]
+        Sh = [self._level1_level2(x) for x in (S11, S22, S33, S12, S13, S23)]
+        S1 = [x[0] for x in Sh]
+        S2 = [x[1] for x in Sh]
+        S_hat = self._smag(*S1)
+        S_hatd = self._smag(*S2)
+        hat1 = (u_h, v_h, w_h)
+        hat2 = (u_d, v_d, w_d)
+        pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+        Lij = [ph[i][0] - (hat1[a] ** 2 if a == b else hat1[a] * hat1[b])
+               for i, (a, b) in enumerate(pairs)]
+        Qij = [ph[i][1] - (hat2[a] ** 2 if a == b else hat2[a] * hat2[b])
+               for i, (a, b) in enumerate(pairs)]
+
+        def contract(A, B):
+            return (A[0] * B[0] + A[1] * B[1] + A[2] * B[2]
+                    + 2 * (A[3] * B[3] + A[4] * B[4] + A[5] * B[5]))
+
+        def sq(A):
+            return (A[0] ** 2 + A[1] ** 2 + A[2] ** 2 + 2 * (A[3] ** 2 + A[4] ** 2 + A[5] ** 2))
+
+        PM = self.PlanarMean
+        a1 = PM(contract(Qij, S1))
+        a3 = PM(sq(S1))
+        a6 = PM(contract(Lij, S1))
+        a8 = PM(sq(S2))
+        if self.optSgs in (1, 2):
+            beta1 = self.ComputeBeta1(*self._wl_coeffs(a1, a3, a6, a8))
+        else:
+            beta1 = np.ones(nz)
+        b3 = beta1.reshape(1, 1, nz)
+        T1 = 2 * L ** (4 / 3)
+        T2 = 2 * (TFR * L) ** (4 / 3)
+        Mij = [T1 * S1[i] - T2 * b3 * S2[i] for i in range(6)]
+        LM = ((Lij[0] * Mij[0] + Lij[1] * Mij[1] + Lij[2] * Mij[2])
+              + 2 * (Lij[3] * Mij[3] + Lij[4] * Mij[4] + Lij[5] * Mij[5]))
+        MM = sq(Mij)
+        Cwl_3D = self._clip_ratio(LM, MM)
+        avg1 = self.PlanarMean(np.sqrt(Cwl_3D)) ** 2
+        avg2 = self.PlanarMean(Cwl_3D)
+        return (u_, v_, w_, u_h, v_h, w_h, u_d, v_d, w_d, S_hat, S_hatd,
+                Cwl_3D, avg1, avg2, beta1)
+
+    def ScalarLASDD_WL(self, u_, v_, w_, u_hat, v_hat, w_hat, u_hatd, v_hatd, w_hatd,
+                       TH, dTHdx, dTHdy, dTHdz, ZeRo3D=None):
+        """``src/subgridscale/DynamicSGS_ScalarLASDD_WL.py:130-275``."""
+        nz, L, TFR = self.nz, self.L, self.TFR
+        THz = np.zeros_like(TH)
+        THz[:, :, 1:nz - 1] = self.StagGridAvg(dTHdz[:, :, 1:nz])
+        THz[:, :, 0] = dTHdz[:, :, 0]
+        THz[:, :, nz - 1] = dTHdz[:, :, nz - 1]
+        T_h, T_d = self._level1_level2(TH)
+        uT = [self._level1_level2(x * TH) for x in (u_, v_, w_)]
+        Gf = [self._level1_level2(x) for x in (dTHdx, dTHdy, THz)]
+        G1 = [x[0] for x in Gf]
+        G2 = [x[1] for x in Gf]
+        LT = [uT[0][0] - u_hat * T_h, uT[1][0] - v_hat * T_h, uT[2][0] - w_hat * T_h]
+        QT = [uT[0][1] - u_hatd * T_d, uT[1][1] - v_hatd * T_d, uT[2][1] - w_hatd * T_d]
+        PM = self.PlanarMean
+        a1 = PM(QT[0] * G1[0] + QT[1] * G1[1] + QT[2] * G1[2])
+        a3_t = G1[0] ** 2 + G1[1] ** 2 + G1[2] ** 2
+        a3 = PM(a3_t)
+        a6_t = LT[0] * G1[0] + LT[1] * G1[1] + LT[2] * G1[2]
+        a6 = PM(a6_t)
+        a8_t = G2[0] ** 2 + G2[1] ** 2 + G2[2] ** 2
+        a8 = PM(a8_t)
+        if self.optSgs in (1, 2):
+            beta2 = self.ComputeBeta2(*self._wl_coeffs(a1, a3, a6, a8))
+        else:
+            beta2 = np.ones(nz)
+        b3 = beta2.reshape(1, 1, nz)
+        b6_t = LT[0] * G2[0] + LT[1] * G2[1] + LT[2] * G2[2]
+        c36_t = G1[0] * G2[0] + G1[1] * G2[1] + G1[2] * G2[2]
+        T_up = L ** (4 / 3) * (a6_t - TFR ** (4 / 3) * b3 * b6_t)
+        T_dn = L ** (8 / 3) * (a3_t - 2 * TFR ** (4 / 3) * b3 * c36_t
+                               + TFR ** (8 / 3) * b3 ** 2 * a8_t)
+        r3 = self._clip_ratio(T_up, T_dn)
+        return r3, self.PlanarMean(r3), beta2
+
+    # ------------------------------------------------------------------
     # src/subgridscale/SGSStresses_SM.py:63-297
     # ------------------------------------------------------------------
     def Wall(self, u, v, M_sfc_loc, psi2D_m, psi2D_m0):
@@ -830,39 +941,123 @@ class AlfaOracle:
         qz[:, :, 0] = qz_sfc
         return qz
 
+    # src/subgridscale/SGSStresses_WL.py:70-240 (tau = -2 L^(4/3) C_WL S_ij)
+    def StressesUVPnodes_Dealias_WL(self, S11_pad, S22_pad, S33_pad, S12_pad, Cwl_3D_pad,
+                                    ZeRo3D_fft=None):
+        return tuple(self._unpad(t) for t in self._wl_uvp((S11_pad, S22_pad, S33_pad, S12_pad),
+                                                           Cwl_3D_pad, -2 * (self.L ** (4 / 3))))
+
+    def StressesUVPnodes_NoDealias_WL(self, S11, S22, S33, S12, Cwl_3D):
+        return self._wl_uvp((S11, S22, S33, S12), Cwl_3D, -2 * (self.L ** (4 / 3)))
+
+    def _wl_uvp(self, comps, C, c0):
+        pre = c0 * C
+        out = []
+        for s in comps:
+            t = pre * s
+            t[:, :, self.nz - 1] = 0
+            out.append(t)
+        return tuple(out)
+
+    def _wl_w(self, comps, C, c0):
+        nz = self.nz
+        pre = c0 * self.StagGridAvg(C[:, :, :nz - 1])
+        out = []
+        for s in comps:
+            t = np.zeros_like(s)
+            t[:, :, 1:nz - 1] = pre * s[:, :, 1:nz - 1]
+            t[:, :, nz - 1] = 0
+            out.append(t)
+        return tuple(out)
+
+    def StressesWnodes_Dealias_WL(self, S13_pad, S23_pad, Cwl_3D_pad, u, v, M_sfc_loc,
+                                  psi2D_m, psi2D_m0, ZeRo3D_fft=None):
+        txz_p, tyz_p = self._wl_w((S13_pad, S23_pad), Cwl_3D_pad, -2 * (self.L ** (4 / 3)))
+        txz, tyz = self._unpad(txz_p), self._unpad(tyz_p)
+        wx, wy = self.Wall(u, v, M_sfc_loc, psi2D_m, psi2D_m0)
+        txz[:, :, 0] = wx
+        tyz[:, :, 0] = wy
+        return txz, tyz
+
+    def StressesWnodes_NoDealias_WL(self, S13, S23, Cwl_3D, u, v, M_sfc_loc, psi2D_m, psi2D_m0):
+        txz, tyz = self._wl_w((S13, S23), Cwl_3D, -2 * (self.L ** (4 / 3)))
+        wx, wy = self.Wall(u, v, M_sfc_loc, psi2D_m, psi2D_m0)
+        txz[:, :, 0] = wx
+        tyz[:, :, 0] = wy
+        return txz, tyz
+
+    # src/subgridscale/ScalarSGSFluxes_WL.py:56-201 (q = -L^(4/3) (C_WL/Pr) grad)
+    def ScalarFluxesUVPnodes_Dealias_WL(self, dTHdx_pad, dTHdy_pad, r_pad, ZeRo3D_fft=None):
+        return tuple(self._unpad(q) for q in self._wl_uvp((dTHdx_pad, dTHdy_pad), r_pad,
+                                                          -(self.L ** (4 / 3))))
+
+    def ScalarFluxesUVPnodes_NoDealias_WL(self, dTHdx, dTHdy, r):
+        return self._wl_uvp((dTHdx, dTHdy), r, -(self.L ** (4 / 3)))
+
+    def ScalarFluxesWnodes_Dealias_WL(self, dTHdz_pad, r_pad, qz_sfc, ZeRo3D_fft=None):
+        qz = self._unpad(self._wl_w((dTHdz_pad,), r_pad, -(self.L ** (4 / 3)))[0])
+        qz[:, :, 0] = qz_sfc
+        return qz
+
+    def ScalarFluxesWnodes_NoDealias_WL(self, dTHdz, r, qz_sfc):
+        qz = self._wl_w((dTHdz,), r, -(self.L ** (4 / 3)))[0]
+        qz[:, :, 0] = qz_sfc
+        return qz
+
     # ------------------------------------------------------------------
     # src/subgridscale/DynamicSGS_Main.py:85-478 and StaticSGS_Main.py:76-360
-    # (SM variants, optSgs in {0, 1, 3})
+    # (SM variants optSgs 0, 1, 3; Wong-Lilly variants optSgs 2, 4)
     # ------------------------------------------------------------------
-    def _require_sm(self):
-        if self.optSgs in (2, 4):
-            raise NotImplementedError("Wong-Lilly variants (optSgs=2,4) are not restated")
+    @property
+    def _wl(self):
+        return self.optSgs in (2, 4)
 
     def DynamicSGS(self, dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz,
                    u, v, w, M_sfc_loc, psi2D_m, psi2D_m0,
                    ZeRo3D=None, ZeRo3D_fft=None, ZeRo3D_pad_fft=None):
-        self._require_sm()
         g = (dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz)
+        wl = self._wl
         if self.optDealias == 1:
             (S11, S22, S33, S12, S13, S23, S_uvp,
              P11, P22, P33, P12, P13, P23, S_uvp_pad) = self.StrainsUVPnodes_Dealias(*g)
-            las = self.LASDD(u, v, w, S11, S22, S33, S12, S13, S23, S_uvp)
+            if wl:
+                las = self.LASDD_WL(u, v, w, S11, S22, S33, S12, S13, S23)
+            else:
+                las = self.LASDD(u, v, w, S11, S22, S33, S12, S13, S23, S_uvp)
             Cs2_3D = las[11]
             Cs2_pad = self._pad(Cs2_3D)
-            txx, tyy, tzz, txy = self.StressesUVPnodes_Dealias(P11, P22, P33, P12, S_uvp_pad, Cs2_pad)
+            if wl:
+                txx, tyy, tzz, txy = self.StressesUVPnodes_Dealias_WL(P11, P22, P33, P12, Cs2_pad)
+            else:
+                txx, tyy, tzz, txy = self.StressesUVPnodes_Dealias(P11, P22, P33, P12, S_uvp_pad,
+                                                                   Cs2_pad)
             W13, W23, S_w, S_w_pad = self.StrainsWnodes_Dealias(*g)
-            txz, tyz = self.StressesWnodes_Dealias(W13, W23, S_w_pad, Cs2_pad, u, v, M_sfc_loc,
-                                                   psi2D_m, psi2D_m0)
+            if wl:
+                txz, tyz = self.StressesWnodes_Dealias_WL(W13, W23, Cs2_pad, u, v, M_sfc_loc,
+                                                          psi2D_m, psi2D_m0)
+            else:
+                txz, tyz = self.StressesWnodes_Dealias(W13, W23, S_w_pad, Cs2_pad, u, v, M_sfc_loc,
+                                                       psi2D_m, psi2D_m0)
         else:
             S11, S22, S33, S12, S13, S23, S_uvp = self.StrainsUVPnodes_NoDealias(*g)
             S_uvp_pad = S_uvp
-            las = self.LASDD(u, v, w, S11, S22, S33, S12, S13, S23, S_uvp)
-            Cs2_3D = las[11]
-            txx, tyy, tzz, txy = self.StressesUVPnodes_NoDealias(S11, S22, S33, S12, S_uvp, Cs2_3D)
+            if wl:
+                las = self.LASDD_WL(u, v, w, S11, S22, S33, S12, S13, S23)
+                Cs2_3D = las[11]
+                txx, tyy, tzz, txy = self.StressesUVPnodes_NoDealias_WL(S11, S22, S33, S12, Cs2_3D)
+            else:
+                las = self.LASDD(u, v, w, S11, S22, S33, S12, S13, S23, S_uvp)
+                Cs2_3D = las[11]
+                txx, tyy, tzz, txy = self.StressesUVPnodes_NoDealias(S11, S22, S33, S12, S_uvp,
+                                                                     Cs2_3D)
             W13, W23, S_w = self.StrainsWnodes_NoDealias(*g)
             S_w_pad = S_w
-            txz, tyz = self.StressesWnodes_NoDealias(W13, W23, S_w, Cs2_3D, u, v, M_sfc_loc,
-                                                     psi2D_m, psi2D_m0)
+            if wl:
+                txz, tyz = self.StressesWnodes_NoDealias_WL(W13, W23, Cs2_3D, u, v, M_sfc_loc,
+                                                            psi2D_m, psi2D_m0)
+            else:
+                txz, tyz = self.StressesWnodes_NoDealias(W13, W23, S_w, Cs2_3D, u, v, M_sfc_loc,
+                                                         psi2D_m, psi2D_m0)
         (u_, v_, w_, u_h, v_h, w_h, u_d, v_d, w_d, S_hat, S_hatd, _, avg1, avg2, beta1) = las
         return (txx, tyy, tzz, txy, txz, tyz, avg1, avg2, beta1, Cs2_3D,
                 u_, v_, w_, u_h, v_h, w_h, u_d, v_d, w_d,
@@ -872,9 +1067,13 @@ class AlfaOracle:
                          S_uvp, S_uvp_pad, S_w, S_w_pad, S_uvp_hat, S_uvp_hatd,
                          TH, dTHdx, dTHdy, dTHdz, qz_sfc,
                          ZeRo3D=None, ZeRo3D_fft=None, ZeRo3D_pad_fft=None):
-        self._require_sm()
-        r3, r1, beta2 = self.ScalarLASDD(u_, v_, w_, u_hat, v_hat, w_hat, u_hatd, v_hatd, w_hatd,
-                                         TH, dTHdx, dTHdy, dTHdz, S_uvp, S_uvp_hat, S_uvp_hatd)
+        if self._wl:
+            r3, r1, beta2 = self.ScalarLASDD_WL(u_, v_, w_, u_hat, v_hat, w_hat, u_hatd, v_hatd,
+                                                w_hatd, TH, dTHdx, dTHdy, dTHdz)
+        else:
+            r3, r1, beta2 = self.ScalarLASDD(u_, v_, w_, u_hat, v_hat, w_hat, u_hatd, v_hatd,
+                                             w_hatd, TH, dTHdx, dTHdy, dTHdz, S_uvp, S_uvp_hat,
+                                             S_uvp_hatd)
         qx, qy, qz = self.StaticSGSscalar(S_uvp, S_uvp_pad, S_w, S_w_pad, r3,
                                           dTHdx, dTHdy, dTHdz, qz_sfc)
         return qx, qy, qz, r3, r1, beta2
@@ -882,37 +1081,60 @@ class AlfaOracle:
     def StaticSGS(self, dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz, Cs2_3D,
                   u, v, M_sfc_loc, psi2D_m, psi2D_m0,
                   ZeRo3D=None, ZeRo3D_fft=None, ZeRo3D_pad_fft=None):
-        self._require_sm()
         g = (dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz)
+        wl = self._wl
         if self.optDealias == 1:
             (S11, S22, S33, S12, S13, S23, S_uvp,
              P11, P22, P33, P12, P13, P23, S_uvp_pad) = self.StrainsUVPnodes_Dealias(*g)
             Cs2_pad = self._pad(Cs2_3D)
-            txx, tyy, tzz, txy = self.StressesUVPnodes_Dealias(P11, P22, P33, P12, S_uvp_pad, Cs2_pad)
+            if wl:
+                txx, tyy, tzz, txy = self.StressesUVPnodes_Dealias_WL(P11, P22, P33, P12, Cs2_pad)
+            else:
+                txx, tyy, tzz, txy = self.StressesUVPnodes_Dealias(P11, P22, P33, P12, S_uvp_pad,
+                                                                   Cs2_pad)
             W13, W23, S_w, S_w_pad = self.StrainsWnodes_Dealias(*g)
-            txz, tyz = self.StressesWnodes_Dealias(W13, W23, S_w_pad, Cs2_pad, u, v, M_sfc_loc,
-                                                   psi2D_m, psi2D_m0)
+            if wl:
+                txz, tyz = self.StressesWnodes_Dealias_WL(W13, W23, Cs2_pad, u, v, M_sfc_loc,
+                                                          psi2D_m, psi2D_m0)
+            else:
+                txz, tyz = self.StressesWnodes_Dealias(W13, W23, S_w_pad, Cs2_pad, u, v, M_sfc_loc,
+                                                       psi2D_m, psi2D_m0)
         else:
             S11, S22, S33, S12, S13, S23, S_uvp = self.StrainsUVPnodes_NoDealias(*g)
             S_uvp_pad = S_uvp
-            txx, tyy, tzz, txy = self.StressesUVPnodes_NoDealias(S11, S22, S33, S12, S_uvp, Cs2_3D)
+            if wl:
+                txx, tyy, tzz, txy = self.StressesUVPnodes_NoDealias_WL(S11, S22, S33, S12, Cs2_3D)
+            else:
+                txx, tyy, tzz, txy = self.StressesUVPnodes_NoDealias(S11, S22, S33, S12, S_uvp,
+                                                                     Cs2_3D)
             W13, W23, S_w = self.StrainsWnodes_NoDealias(*g)
             S_w_pad = S_w
-            txz, tyz = self.StressesWnodes_NoDealias(W13, W23, S_w, Cs2_3D, u, v, M_sfc_loc,
-                                                     psi2D_m, psi2D_m0)
+            if wl:
+                txz, tyz = self.StressesWnodes_NoDealias_WL(W13, W23, Cs2_3D, u, v, M_sfc_loc,
+                                                            psi2D_m, psi2D_m0)
+            else:
+                txz, tyz = self.StressesWnodes_NoDealias(W13, W23, S_w, Cs2_3D, u, v, M_sfc_loc,
+                                                         psi2D_m, psi2D_m0)
         return txx, tyy, tzz, txy, txz, tyz, S_uvp, S_uvp_pad, S_w, S_w_pad
 
     def StaticSGSscalar(self, S_uvp, S_uvp_pad, S_w, S_w_pad, Cs2PrRatio_3D,
                         dTHdx, dTHdy, dTHdz, qz_sfc, ZeRo3D_fft=None, ZeRo3D_pad_fft=None):
-        self._require_sm()
         if self.optDealias == 1:
             gx, gy, gz = self._pad(dTHdx), self._pad(dTHdy), self._pad(dTHdz)
             rp = self._pad(Cs2PrRatio_3D)
-            qx, qy = self.ScalarFluxesUVPnodes_Dealias(gx, gy, S_uvp_pad, rp)
-            qz = self.ScalarFluxesWnodes_Dealias(gz, S_w_pad, rp, qz_sfc)
+            if self._wl:
+                qx, qy = self.ScalarFluxesUVPnodes_Dealias_WL(gx, gy, rp)
+                qz = self.ScalarFluxesWnodes_Dealias_WL(gz, rp, qz_sfc)
+            else:
+                qx, qy = self.ScalarFluxesUVPnodes_Dealias(gx, gy, S_uvp_pad, rp)
+                qz = self.ScalarFluxesWnodes_Dealias(gz, S_w_pad, rp, qz_sfc)
         else:
-            qx, qy = self.ScalarFluxesUVPnodes_NoDealias(dTHdx, dTHdy, S_uvp, Cs2PrRatio_3D)
-            qz = self.ScalarFluxesWnodes_NoDealias(dTHdz, S_w, Cs2PrRatio_3D, qz_sfc)
+            if self._wl:
+                qx, qy = self.ScalarFluxesUVPnodes_NoDealias_WL(dTHdx, dTHdy, Cs2PrRatio_3D)
+                qz = self.ScalarFluxesWnodes_NoDealias_WL(dTHdz, Cs2PrRatio_3D, qz_sfc)
+            else:
+                qx, qy = self.ScalarFluxesUVPnodes_NoDealias(dTHdx, dTHdy, S_uvp, Cs2PrRatio_3D)
+                qz = self.ScalarFluxesWnodes_NoDealias(dTHdz, S_w, Cs2PrRatio_3D, qz_sfc)
         return qx, qy, qz
 
     # ------------------------------------------------------------------
@@ -1165,8 +1387,8 @@ class AlfaOracle:
 
 
 class OracleRun:
-    """The time loop of ``src/Main.py:46-541`` on the oracle (dry, optSgs in
-    {0,1,3}, constant geostrophic wind).  ``step()`` advances one iteration
+    """The time loop of ``src/Main.py:46-541`` on the oracle (dry, optSgs 0-4,
+    constant geostrophic wind).  ``step()`` advances one iteration
     and keeps the same state variables Main.py keeps between iterations."""
 
     def __init__(self, cfg, u, v, w, th, surface_series=None, adv=None):

@@ -20,6 +20,9 @@ CALL_FIXTURES = [
     ("ref_stable_het_12x12x8.npz", "stable"),
     ("ref_convective_fgr2_12x12x8.npz", "convective"),  # FGR = 2: no dealiasing
     ("ref_stable_fgr2_12x12x8.npz", "stable"),
+    ("ref_convective_wl_12x12x8.npz", "convective"),  # LASDD-WL (optSgs = 2)
+    ("ref_stable_wl4_12x12x8.npz", "stable"),  # LAD-WL (optSgs = 4)
+    ("ref_convective_wl_fgr2_12x12x8.npz", "convective"),  # LASDD-WL, FGR = 2
 ]
 # The oracle restates the reference operation for operation; on the same
 # NumPy FFT it reproduces the recorded results to the last bit.  The bound
