@@ -57,10 +57,10 @@ typedef struct alfa_config {
   double inversion;              /* K/m */
   int optBuoyancy;               /* 0: /T_0, 1: /<THv> */
   double T_0;                    /* K */
-  int optSgs;                    /* 0 static, 1 LASDD-SM, 3 LAD-SM */
+  int optSgs;                    /* 0 static, 1 LASDD-SM, 2 LASDD-WL, 3 LAD-SM, 4 LAD-WL */
   int dynamicSGS_call_time;
   int FGR;                       /* 1: 3/2-rule dealiasing, TFR 2; >= 2: no dealiasing, TFR sqrt(2) */
-  double Cs2, Cs2PrRatio;        /* initial coefficients */
+  double Cs2, Cs2PrRatio;        /* initial coefficients (Cwl, CwlPrRatio for optSgs 2, 4) */
   int optDamping;
   double z_damping, RelaxTime;   /* m, s */
   int optAdvection;

@@ -28,10 +28,15 @@ CONFIG_KEYS = [f for f, _ in _lib.AlfaConfig._fields_]
 
 
 def make_config(cfg):
+    """alfa_config from a reference-style config dict.  The Wong-Lilly models
+    (optSgs 2, 4) start from Cwl / CwlPrRatio, as DerivedVars.py:101-103 does."""
     c = _lib.AlfaConfig()
     for k in CONFIG_KEYS:
         v = cfg[k]
         setattr(c, k, int(v) if isinstance(getattr(c, k), int) else float(v))
+    if int(cfg["optSgs"]) in (2, 4):
+        c.Cs2 = float(cfg.get("Cwl", cfg["Cs2"]))
+        c.Cs2PrRatio = float(cfg.get("CwlPrRatio", cfg["Cs2PrRatio"]))
     return c
 
 

@@ -149,8 +149,9 @@ int engine_init(Engine& e, const alfa_config& c) {
   if (c.nx < 4 || c.ny < 4 || c.nz < 3 || (c.nx % 2) || (c.ny % 2))
     return e.fail("grid must have even nx, ny >= 4 and nz >= 3", ALFA_E_CONFIG);
   if (c.FGR < 1) return e.fail("FGR must be >= 1", ALFA_E_CONFIG);
-  if (!(c.optSgs == 0 || c.optSgs == 1 || c.optSgs == 3))
-    return e.fail("optSgs must be 0 (static), 1 (LASDD-SM) or 3 (LAD-SM)", ALFA_E_CONFIG);
+  if (c.optSgs < 0 || c.optSgs > 4)
+    return e.fail("optSgs must be 0 (static), 1 (LASDD-SM), 2 (LASDD-WL), 3 (LAD-SM) or 4 (LAD-WL)",
+                  ALFA_E_CONFIG);
   if (c.dynamicSGS_call_time < 1) return e.fail("dynamicSGS_call_time must be >= 1", ALFA_E_CONFIG);
   e.mx = (int)(1.5 * c.nx);
   e.my = (int)(1.5 * c.ny);
@@ -401,6 +402,11 @@ static Loader ld(const Engine& e, int kind, std::initializer_list<const double*>
   return L;
 }
 
+// Wong-Lilly base model (optSgs 2, 4) instead of Smagorinsky (0, 1, 3)
+static bool wong_lilly(const Engine& e) { return e.cfg.optSgs == 2 || e.cfg.optSgs == 4; }
+// scale-dependent procedures compute beta; the LAD variants (3, 4) set it to 1
+static bool compute_beta_flag(const Engine& e) { return e.cfg.optSgs == 1 || e.cfg.optSgs == 2; }
+
 // Derivxy(FFT(field)) with per-output accumulate flags
 static void deriv_field_acc(Engine& e, const Loader& L, double* dx, int accx, double* dy,
                             int accy) {
@@ -480,9 +486,13 @@ static void sgs_stresses(alfa_ctx* c, const double* const g[9], const double* S_
                          const double* pm0, double* const t6[6], double* S_w, double* S_w_pad) {
   Engine& e = c->e;
   double* const* Pb = c->w.Pb;
+  const bool wl = wong_lilly(e);
   const double cst = -2 * std::pow(e.L, 2.0);
+  const double cwl = -2 * std::pow(e.L, 4.0 / 3.0);  // SGSStresses_WL.py:90
   for (int i = 0; i < 4; i++)
-    op2_unpad(e, ld(e, LD_STRESS_UVP, {Pb[9], S_uvp_pad, Pb[i]}, cst), t6[i], c->w.Lpad);
+    op2_unpad(e, wl ? ld(e, LD_WL_UVP, {Pb[9], Pb[i]}, cwl)
+                    : ld(e, LD_STRESS_UVP, {Pb[9], S_uvp_pad, Pb[i]}, cst),
+              t6[i], c->w.Lpad);
   Loader Lw = ld(e, LD_W_SXX, {g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8]});
   for (int s = 0; s < 6; s++) {
     Lw.sub = s;
@@ -491,8 +501,10 @@ static void sgs_stresses(alfa_ctx* c, const double* const g[9], const double* S_
   smag_w(e, g, S_w);
   const double* q6[6] = {Pb[0], Pb[1], Pb[2], Pb[3], Pb[4], Pb[5]};
   smag6(e, q6, e.P(), S_w_pad);
-  op2_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[4]}, cst), t6[4], c->w.Lpad);
-  op2_unpad(e, ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[5]}, cst), t6[5], c->w.Lpad);
+  for (int i = 4; i < 6; i++)
+    op2_unpad(e, wl ? ld(e, LD_WL_W, {Pb[9], Pb[i]}, cwl)
+                    : ld(e, LD_STRESS_W, {Pb[9], S_w_pad, Pb[i]}, cst),
+              t6[i], c->w.Lpad);
   wall_override(e, u, v, M, pm, pm0, t6[4], t6[5]);
 }
 
@@ -506,9 +518,13 @@ static void sgs_stresses_nodealias(alfa_ctx* c, const double* const g[9], const 
                                    double* S_w_pad) {
   Engine& e = c->e;
   double* const* Pb = c->w.Pb;
+  const bool wl = wong_lilly(e);
   const double cst = -2 * std::pow(e.L, 2.0);
+  const double cwl = -2 * std::pow(e.L, 4.0 / 3.0);
   for (int i = 0; i < 4; i++)
-    materialize(e, ld(e, LD_STRESS_UVP, {Cs2, S_uvp, Sij[i]}, cst), e.N(), t6[i]);
+    materialize(e, wl ? ld(e, LD_WL_UVP, {Cs2, Sij[i]}, cwl)
+                      : ld(e, LD_STRESS_UVP, {Cs2, S_uvp, Sij[i]}, cst),
+                e.N(), t6[i]);
   Loader Lw = ld(e, LD_W_SXX, {g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8]});
   Lw.sub = 4;
   materialize(e, Lw, e.N(), Pb[0]);  // S13 on w nodes
@@ -516,8 +532,10 @@ static void sgs_stresses_nodealias(alfa_ctx* c, const double* const g[9], const 
   materialize(e, Lw, e.N(), Pb[1]);  // S23 on w nodes
   smag_w(e, g, S_w);
   cudaMemcpyAsync(S_w_pad, S_w, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
-  materialize(e, ld(e, LD_STRESS_W, {Cs2, S_w, Pb[0]}, cst), e.N(), t6[4]);
-  materialize(e, ld(e, LD_STRESS_W, {Cs2, S_w, Pb[1]}, cst), e.N(), t6[5]);
+  for (int i = 0; i < 2; i++)
+    materialize(e, wl ? ld(e, LD_WL_W, {Cs2, Pb[i]}, cwl)
+                      : ld(e, LD_STRESS_W, {Cs2, S_w, Pb[i]}, cst),
+                e.N(), t6[4 + i]);
   wall_override(e, u, v, M, pm, pm0, t6[4], t6[5]);
 }
 
@@ -569,7 +587,10 @@ static int dynamic_sgs(alfa_ctx* c, const double* const g[9], const double* u, c
   const double* pb[6] = {u_, v_, w_, v_, w_, w_};
   for (int i = 0; i < 6; i++) op_filter12(e, ld(e, LD_MUL, {pa[i], pb[i]}), W.ph[i], W.pd[i]);
   for (int i = 0; i < 6; i++) op_filter12(e, ld_field(e, Sij[i]), W.Sh[i], W.Sd[i]);
-  for (int i = 0; i < 6; i++) op_filter12(e, ld(e, LD_MUL, {S_uvp, Sij[i]}), W.SSh[i], W.SSd[i]);
+  const bool wl = wong_lilly(e);
+  if (!wl)  // the Wong-Lilly procedure has no S|S_ij| products
+    for (int i = 0; i < 6; i++)
+      op_filter12(e, ld(e, LD_MUL, {S_uvp, Sij[i]}), W.SSh[i], W.SSd[i]);
   const double* sh6[6] = {W.Sh[0], W.Sh[1], W.Sh[2], W.Sh[3], W.Sh[4], W.Sh[5]};
   const double* sd6[6] = {W.Sd[0], W.Sd[1], W.Sd[2], W.Sd[3], W.Sd[4], W.Sd[5]};
   smag6_n(e, sh6, mom[23]);
@@ -591,14 +612,22 @@ static int dynamic_sgs(alfa_ctx* c, const double* const g[9], const double* u, c
   f.S_hatd = mom[24];
   double* sums = W.prof;
   double* co = W.prof + 10 * e.nz;
-  if (e.cfg.optSgs == 1) {
-    lasdd_sums(e, f, sums);
-    lasdd_poly(e, sums, 0, co);
+  if (compute_beta_flag(e)) {
+    if (wl) {  // DynamicSGS_LASDD_WL.py:245-284
+      lasdd_wl_sums(e, f, sums);
+      wl_poly(e, sums, co);
+    } else {
+      lasdd_sums(e, f, sums);
+      lasdd_poly(e, sums, 0, co);
+    }
     compute_beta(e, co, e.nz, beta1);
   } else {
     ::alfa::note_launch(); k_ones_ext<<<1, 256, 0, e.stream>>>(beta1, e.nz);  // LAD: beta = 1 (:321-325)
   }
-  lasdd_LM_MM(e, f, beta1, W.LM, W.MM);
+  if (wl)
+    lasdd_wl_LM_MM(e, f, beta1, W.LM, W.MM);
+  else
+    lasdd_LM_MM(e, f, beta1, W.LM, W.MM);
   clip_ratio(e, W.LM, W.MM, Cs2);
   cs2_profiles(e, Cs2, avg1, avg2);
   // stresses (SGSStresses_SM.py) with Cs2_3D_pad = Dealias1(FFT(Cs2_3D))
@@ -640,10 +669,15 @@ static void scalar_fluxes(alfa_ctx* c, const double* S_uvp_pad, const double* S_
   Engine& e = c->e;
   Work& W = c->w;
   const double cst = -2 * std::pow(e.L, 2.0);
+  const bool wl = wong_lilly(e);
+  const double cwl = -std::pow(e.L, 4.0 / 3.0);  // ScalarSGSFluxes_WL.py:76
   if (!e.optDealias) {  // ScalarFluxes*_NoDealias (ScalarSGSFluxes_SM.py:98-126, :185-222)
-    materialize(e, ld(e, LD_STRESS_UVP, {r3, S_uvp_pad, gx}, cst), e.N(), W.qx);
-    materialize(e, ld(e, LD_STRESS_UVP, {r3, S_uvp_pad, gy}, cst), e.N(), W.qy);
-    materialize(e, ld(e, LD_STRESS_W, {r3, S_w_pad, gz}, cst), e.N(), qz);
+    materialize(e, wl ? ld(e, LD_WL_UVP, {r3, gx}, cwl) : ld(e, LD_STRESS_UVP, {r3, S_uvp_pad, gx}, cst),
+                e.N(), W.qx);
+    materialize(e, wl ? ld(e, LD_WL_UVP, {r3, gy}, cwl) : ld(e, LD_STRESS_UVP, {r3, S_uvp_pad, gy}, cst),
+                e.N(), W.qy);
+    materialize(e, wl ? ld(e, LD_WL_W, {r3, gz}, cwl) : ld(e, LD_STRESS_W, {r3, S_w_pad, gz}, cst),
+                e.N(), qz);
     set_plane0(e, qz_sfc, qz);
     div_flux(c, W.qx, W.qy, qz, divq);
     return;
@@ -652,9 +686,15 @@ static void scalar_fluxes(alfa_ctx* c, const double* S_uvp_pad, const double* S_
   op2_pad(e, ld_field(e, gy), W.Pb[1], c->w.Lpad);
   op2_pad(e, ld_field(e, gz), W.Pb[2], c->w.Lpad);
   op2_pad(e, ld_field(e, r3), W.Pb[3], c->w.Lpad);
-  op2_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[0]}, cst), W.qx, c->w.Lpad);
-  op2_unpad(e, ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[1]}, cst), W.qy, c->w.Lpad);
-  op2_unpad(e, ld(e, LD_STRESS_W, {W.Pb[3], S_w_pad, W.Pb[2]}, cst), qz, c->w.Lpad);
+  op2_unpad(e, wl ? ld(e, LD_WL_UVP, {W.Pb[3], W.Pb[0]}, cwl)
+                  : ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[0]}, cst),
+            W.qx, c->w.Lpad);
+  op2_unpad(e, wl ? ld(e, LD_WL_UVP, {W.Pb[3], W.Pb[1]}, cwl)
+                  : ld(e, LD_STRESS_UVP, {W.Pb[3], S_uvp_pad, W.Pb[1]}, cst),
+            W.qy, c->w.Lpad);
+  op2_unpad(e, wl ? ld(e, LD_WL_W, {W.Pb[3], W.Pb[2]}, cwl)
+                  : ld(e, LD_STRESS_W, {W.Pb[3], S_w_pad, W.Pb[2]}, cst),
+            qz, c->w.Lpad);
   set_plane0(e, qz_sfc, qz);
   div_flux(c, W.qx, W.qy, qz, divq);
 }
@@ -674,9 +714,12 @@ static int dynamic_sgs_scalar(alfa_ctx* c, const double* const m15[15], const do
   op_filter12(e, ld_field(e, gx), W.Gh[0], W.Gd[0]);
   op_filter12(e, ld_field(e, gy), W.Gh[1], W.Gd[1]);
   op_filter12(e, ld(e, LD_THZ, {gz}), W.Gh[2], W.Gd[2]);
-  op_filter12(e, ld(e, LD_MUL, {S, gx}), W.SGh[0], W.SGd[0]);
-  op_filter12(e, ld(e, LD_MUL, {S, gy}), W.SGh[1], W.SGd[1]);
-  op_filter12(e, ld(e, LD_MUL_THZ, {S, gz}), W.SGh[2], W.SGd[2]);
+  const bool wl = wong_lilly(e);
+  if (!wl) {  // the Wong-Lilly procedure has no |S| grad(theta) products
+    op_filter12(e, ld(e, LD_MUL, {S, gx}), W.SGh[0], W.SGd[0]);
+    op_filter12(e, ld(e, LD_MUL, {S, gy}), W.SGh[1], W.SGd[1]);
+    op_filter12(e, ld(e, LD_MUL_THZ, {S, gz}), W.SGh[2], W.SGd[2]);
+  }
   ScalarLasddFields f;
   for (int i = 0; i < 3; i++) {
     f.hat[i] = m15[3 + i];
@@ -694,14 +737,22 @@ static int dynamic_sgs_scalar(alfa_ctx* c, const double* const m15[15], const do
   f.S_hatd = m15[14];
   double* sums = W.prof;
   double* co = W.prof + 10 * e.nz;
-  if (e.cfg.optSgs == 1) {
-    scalar_lasdd_sums(e, f, sums);
-    lasdd_poly(e, sums, 1, co);
+  if (compute_beta_flag(e)) {
+    if (wl) {  // DynamicSGS_ScalarLASDD_WL.py:214-252
+      scalar_lasdd_wl_sums(e, f, sums);
+      wl_poly(e, sums, co);
+    } else {
+      scalar_lasdd_sums(e, f, sums);
+      lasdd_poly(e, sums, 1, co);
+    }
     compute_beta(e, co, e.nz, beta2);
   } else {
     ::alfa::note_launch(); k_ones_ext<<<1, 256, 0, e.stream>>>(beta2, e.nz);
   }
-  scalar_Tup_Tdn(e, f, beta2, W.LM, W.MM);
+  if (wl)
+    scalar_wl_Tup_Tdn(e, f, beta2, W.LM, W.MM);
+  else
+    scalar_Tup_Tdn(e, f, beta2, W.LM, W.MM);
   clip_ratio(e, W.LM, W.MM, r3);
   const double* fr[1] = {r3};
   plane_means(e, fr, 1, r1);
@@ -1212,8 +1263,8 @@ int alfa_DivStressDynamicSGS(alfa_ctx* c, const double* const g[9], const double
   for (int i = 0; i < 9; i++) NN(g[i]);
   for (int i = 0; i < 25; i++)
     if (!(i >= 6 && i <= 9)) NN(mom[i]);
-  if (c->e.cfg.optSgs != 1 && c->e.cfg.optSgs != 3)
-    return c->e.fail("DivStressDynamicSGS needs optSgs 1 or 3", ALFA_E_CONFIG);
+  if (c->e.cfg.optSgs < 1 || c->e.cfg.optSgs > 4)
+    return c->e.fail("DivStressDynamicSGS needs optSgs 1-4", ALFA_E_CONFIG);
   double* divt[3] = {dtx, dty, dtz};
   double* m[25];
   for (int i = 0; i < 25; i++) m[i] = mom[i];
@@ -1235,8 +1286,8 @@ int alfa_DivFluxDynamicSGS(alfa_ctx* c, const double* const m15[15], const doubl
   NN(m15); NN(TH); NN(gx); NN(gy); NN(gz); NN(qz_sfc); NN(qz); NN(divq); NN(r3); NN(r1);
   NN(beta2);
   for (int i = 0; i < 15; i++) NN(m15[i]);
-  if (c->e.cfg.optSgs != 1 && c->e.cfg.optSgs != 3)
-    return c->e.fail("DivFluxDynamicSGS needs optSgs 1 or 3", ALFA_E_CONFIG);
+  if (c->e.cfg.optSgs < 1 || c->e.cfg.optSgs > 4)
+    return c->e.fail("DivFluxDynamicSGS needs optSgs 1-4", ALFA_E_CONFIG);
   return dynamic_sgs_scalar(c, m15, TH, gx, gy, gz, qz_sfc, qz, divq, r3, r1, beta2);
 }
 

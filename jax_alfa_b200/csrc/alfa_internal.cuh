@@ -41,7 +41,16 @@ enum LoadKind {
   LD_W_SXX,          // w-node strain components from gradients
   LD_THZ,            // THz of ScalarLASDD
   LD_MUL_THZ,        // a0 * THz(a1)
+  LD_WL_UVP,         // c0 * a0 * a1, top row 0 (Wong-Lilly stresses / fluxes, uvp nodes)
+  LD_WL_W,           // interior c0 * stag(a0) * a1, rows 0 and top 0 (w nodes)
 };
+
+// Every kind a tile kernel evaluates (switches expand this list, so a kind
+// added above and here is handled everywhere).
+#define ALFA_LOADER_KINDS(X)                                                          \
+  X(LD_FIELD) X(LD_MUL) X(LD_MUL3) X(LD_PRESSURE_R) X(LD_ADV_XY) X(LD_ADV_Z)           \
+  X(LD_SCALAR_ADV) X(LD_STRESS_UVP) X(LD_STRESS_W) X(LD_W_SXX) X(LD_THZ) X(LD_MUL_THZ) \
+  X(LD_WL_UVP) X(LD_WL_W)
 
 struct Loader {
   int kind;

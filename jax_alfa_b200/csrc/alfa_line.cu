@@ -103,18 +103,11 @@ __global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(),
   cd* S = sm;
   cd* W = sm + n * YC;
   switch (a.L.kind) {
-    case LD_FIELD: line_load<LD_FIELD>(a, f, z0, n, S); break;
-    case LD_MUL: line_load<LD_MUL>(a, f, z0, n, S); break;
-    case LD_MUL3: line_load<LD_MUL3>(a, f, z0, n, S); break;
-    case LD_PRESSURE_R: line_load<LD_PRESSURE_R>(a, f, z0, n, S); break;
-    case LD_ADV_XY: line_load<LD_ADV_XY>(a, f, z0, n, S); break;
-    case LD_ADV_Z: line_load<LD_ADV_Z>(a, f, z0, n, S); break;
-    case LD_SCALAR_ADV: line_load<LD_SCALAR_ADV>(a, f, z0, n, S); break;
-    case LD_STRESS_UVP: line_load<LD_STRESS_UVP>(a, f, z0, n, S); break;
-    case LD_STRESS_W: line_load<LD_STRESS_W>(a, f, z0, n, S); break;
-    case LD_W_SXX: line_load<LD_W_SXX>(a, f, z0, n, S); break;
-    case LD_THZ: line_load<LD_THZ>(a, f, z0, n, S); break;
-    default: line_load<LD_MUL_THZ>(a, f, z0, n, S); break;
+#define ALFA_K(K) \
+  case K: line_load<K>(a, f, z0, n, S); break;
+    ALFA_LOADER_KINDS(ALFA_K)
+#undef ALFA_K
+    default: break;
   }
   tile_fft<-1, YC, NIN, NT>(S, a.pin);
   const bool pair = (nz & 1) == 0;
@@ -205,18 +198,11 @@ __device__ __forceinline__ void line_gather(const LineArgs& a, long long f, int 
 template <int C, int N, int NT>
 __device__ __forceinline__ void line_gather_any(const LineArgs& a, long long f, int z0, cd* v) {
   switch (a.L.kind) {
-    case LD_FIELD: line_gather<LD_FIELD, C, N, NT>(a, f, z0, v); break;
-    case LD_MUL: line_gather<LD_MUL, C, N, NT>(a, f, z0, v); break;
-    case LD_MUL3: line_gather<LD_MUL3, C, N, NT>(a, f, z0, v); break;
-    case LD_PRESSURE_R: line_gather<LD_PRESSURE_R, C, N, NT>(a, f, z0, v); break;
-    case LD_ADV_XY: line_gather<LD_ADV_XY, C, N, NT>(a, f, z0, v); break;
-    case LD_ADV_Z: line_gather<LD_ADV_Z, C, N, NT>(a, f, z0, v); break;
-    case LD_SCALAR_ADV: line_gather<LD_SCALAR_ADV, C, N, NT>(a, f, z0, v); break;
-    case LD_STRESS_UVP: line_gather<LD_STRESS_UVP, C, N, NT>(a, f, z0, v); break;
-    case LD_STRESS_W: line_gather<LD_STRESS_W, C, N, NT>(a, f, z0, v); break;
-    case LD_W_SXX: line_gather<LD_W_SXX, C, N, NT>(a, f, z0, v); break;
-    case LD_THZ: line_gather<LD_THZ, C, N, NT>(a, f, z0, v); break;
-    default: line_gather<LD_MUL_THZ, C, N, NT>(a, f, z0, v); break;
+#define ALFA_K(K) \
+  case K: line_gather<K, C, N, NT>(a, f, z0, v); break;
+    ALFA_LOADER_KINDS(ALFA_K)
+#undef ALFA_K
+    default: break;
   }
 }
 
@@ -454,18 +440,11 @@ __device__ __forceinline__ void phase_gather(const LineArgs& a, long long f, int
 template <int C, int RA, int RB, int NT>
 __device__ __forceinline__ void phase_gather_any(const LineArgs& a, long long f, int z0, cd* v) {
   switch (a.L.kind) {
-    case LD_FIELD: phase_gather<LD_FIELD, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_MUL: phase_gather<LD_MUL, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_MUL3: phase_gather<LD_MUL3, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_PRESSURE_R: phase_gather<LD_PRESSURE_R, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_ADV_XY: phase_gather<LD_ADV_XY, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_ADV_Z: phase_gather<LD_ADV_Z, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_SCALAR_ADV: phase_gather<LD_SCALAR_ADV, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_STRESS_UVP: phase_gather<LD_STRESS_UVP, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_STRESS_W: phase_gather<LD_STRESS_W, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_W_SXX: phase_gather<LD_W_SXX, C, RA, RB, NT>(a, f, z0, v); break;
-    case LD_THZ: phase_gather<LD_THZ, C, RA, RB, NT>(a, f, z0, v); break;
-    default: phase_gather<LD_MUL_THZ, C, RA, RB, NT>(a, f, z0, v); break;
+#define ALFA_K(K) \
+  case K: phase_gather<K, C, RA, RB, NT>(a, f, z0, v); break;
+    ALFA_LOADER_KINDS(ALFA_K)
+#undef ALFA_K
+    default: break;
   }
 }
 
@@ -705,11 +684,9 @@ void materialize(Engine& e, const Loader& L, size_t n, double* out) {
   switch (L.kind) {
 #define ALFA_MAT(K) \
   case K: k_materialize<K><<<blocks, 256, 0, e.stream>>>(L, n, out); break;
-    ALFA_MAT(LD_FIELD) ALFA_MAT(LD_MUL) ALFA_MAT(LD_MUL3) ALFA_MAT(LD_PRESSURE_R)
-    ALFA_MAT(LD_ADV_XY) ALFA_MAT(LD_ADV_Z) ALFA_MAT(LD_SCALAR_ADV) ALFA_MAT(LD_STRESS_UVP)
-    ALFA_MAT(LD_STRESS_W) ALFA_MAT(LD_W_SXX) ALFA_MAT(LD_THZ)
-    default: k_materialize<LD_MUL_THZ><<<blocks, 256, 0, e.stream>>>(L, n, out); break;
+    ALFA_LOADER_KINDS(ALFA_MAT)
 #undef ALFA_MAT
+    default: break;
   }
 }
 

@@ -709,6 +709,165 @@ void lasdd_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM
   ::alfa::note_launch(); k_LM_MM<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, lasdd_const(e), beta, LM, MM, e.N(), e.nz);
 }
 
+// ---------------------------------------------------------------------------
+// Wong-Lilly procedure (DynamicSGS_LASDD_WL.py:127-313,
+// DynamicSGS_ScalarLASDD_WL.py:130-275): four plane means a1, a3, a6, a8,
+// the quintic mapped from them, then M_ij / T_up, T_dn with the Delta^(4/3)
+// scaling.
+// ---------------------------------------------------------------------------
+__global__ void k_wl_partial(LasddFields f, size_t H, int nz, double* __restrict__ part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double s[4] = {0, 0, 0, 0};
+    for (size_t r = r0; r < r1; r++) {
+      const size_t i = r * nz + z;
+      double Lm[6], Qm[6], S1[6], S2[6];
+      leonard(f.ph, f.hat, i, Lm);
+      leonard(f.pd, f.hatd, i, Qm);
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        S1[q] = f.Sh[q][i];
+        S2[q] = f.Sd[q][i];
+      }
+      s[0] += contract6(Qm, S1);  // a1
+      s[1] += sq6(S1);            // a3
+      s[2] += contract6(Lm, S1);  // a6
+      s[3] += sq6(S2);            // a8
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) part[((size_t)blockIdx.x * 4 + q) * nz + z] = s[q];
+  }
+}
+
+void lasdd_wl_sums(Engine& e, const LasddFields& f, double* sums4) {
+  const int nb = red_blocks(e);
+  ::alfa::note_launch(); k_wl_partial<<<nb, 128, 0, e.stream>>>(f, e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)4 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 4, e.nz,
+                                                                       1.0 / (double)e.H(), sums4);
+}
+
+struct WLPow {
+  double p43, p83, p163;  // TFR^(4/3), TFR^(8/3), TFR^(16/3)
+};
+
+static WLPow wl_pow(const Engine& e) {
+  return WLPow{std::pow(e.TFR, 4.0 / 3.0), std::pow(e.TFR, 8.0 / 3.0),
+               std::pow(e.TFR, 16.0 / 3.0)};
+}
+
+// (ff, ee, dd, cc, bb, aa) per level from (a1, a3, a6, a8)
+__global__ void k_poly_wl(const double* __restrict__ m, int nz, WLPow P, double* co) {
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    const double a1 = m[0 * nz + z], a3 = m[1 * nz + z], a6 = m[2 * nz + z], a8 = m[3 * nz + z];
+    const double a2 = -(P.p83) * a1;
+    const double a4 = -2 * P.p43 * a3;
+    const double a5 = P.p83 * a3;
+    const double a7 = -P.p43 * a6;
+    const double a9 = -2 * P.p83 * a8;
+    const double a10 = P.p163 * a8;
+    co[0 * nz + z] = -a7 * a10;                     // ff
+    co[1 * nz + z] = a2 * a5 - a6 * a10;            // ee
+    co[2 * nz + z] = a2 * a4 - a7 * a9;             // dd
+    co[3 * nz + z] = a2 * a3 + a1 * a5 - a6 * a9;   // cc
+    co[4 * nz + z] = a1 * a4 - a7 * a8;             // bb
+    co[5 * nz + z] = a1 * a3 - a6 * a8;             // aa
+  }
+}
+
+void wl_poly(Engine& e, const double* sums4, double* coeffs6) {
+  ::alfa::note_launch(); k_poly_wl<<<1, 256, 0, e.stream>>>(sums4, e.nz, wl_pow(e), coeffs6);
+}
+
+__global__ void k_LM_MM_wl(LasddFields f, double T1, double T2, const double* __restrict__ beta,
+                           double* LM, double* MM, size_t n, int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    double Lm[6], Mm[6];
+    leonard(f.ph, f.hat, i, Lm);
+    const double b = beta[z];
+#pragma unroll
+    for (int q = 0; q < 6; q++) Mm[q] = T1 * f.Sh[q][i] - T2 * b * f.Sd[q][i];
+    LM[i] = (Lm[0] * Mm[0] + Lm[1] * Mm[1] + Lm[2] * Mm[2]) +
+            2.0 * (Lm[3] * Mm[3] + Lm[4] * Mm[4] + Lm[5] * Mm[5]);
+    MM[i] = sq6(Mm);
+  }
+}
+
+void lasdd_wl_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM) {
+  const double T1 = 2 * std::pow(e.L, 4.0 / 3.0);
+  const double T2 = 2 * std::pow(e.TFR * e.L, 4.0 / 3.0);
+  ::alfa::note_launch(); k_LM_MM_wl<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, T1, T2, beta, LM, MM, e.N(), e.nz);
+}
+
+struct WLScalarTerms {
+  double a1, a3, a6, a8, b6, c36;
+};
+
+__device__ __forceinline__ WLScalarTerms wl_scalar_terms(const ScalarLasddFields& f, size_t i) {
+  const double T1 = f.Th[i], T2 = f.Td[i];
+  double LT[3], QT[3], G1[3], G2[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    LT[q] = f.uTh[q][i] - f.hat[q][i] * T1;
+    QT[q] = f.uTd[q][i] - f.hatd[q][i] * T2;
+    G1[q] = f.Gh[q][i];
+    G2[q] = f.Gd[q][i];
+  }
+  WLScalarTerms t;
+  t.a1 = QT[0] * G1[0] + QT[1] * G1[1] + QT[2] * G1[2];
+  t.a3 = G1[0] * G1[0] + G1[1] * G1[1] + G1[2] * G1[2];
+  t.a6 = LT[0] * G1[0] + LT[1] * G1[1] + LT[2] * G1[2];
+  t.a8 = G2[0] * G2[0] + G2[1] * G2[1] + G2[2] * G2[2];
+  t.b6 = LT[0] * G2[0] + LT[1] * G2[1] + LT[2] * G2[2];
+  t.c36 = G1[0] * G2[0] + G1[1] * G2[1] + G1[2] * G2[2];
+  return t;
+}
+
+__global__ void k_slwl_partial(ScalarLasddFields f, size_t H, int nz, double* part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double s[4] = {0, 0, 0, 0};
+    for (size_t r = r0; r < r1; r++) {
+      const WLScalarTerms t = wl_scalar_terms(f, r * nz + z);
+      s[0] += t.a1;
+      s[1] += t.a3;
+      s[2] += t.a6;
+      s[3] += t.a8;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) part[((size_t)blockIdx.x * 4 + q) * nz + z] = s[q];
+  }
+}
+
+void scalar_lasdd_wl_sums(Engine& e, const ScalarLasddFields& f, double* sums4) {
+  const int nb = red_blocks(e);
+  ::alfa::note_launch(); k_slwl_partial<<<nb, 128, 0, e.stream>>>(f, e.H(), e.nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)4 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 4, e.nz,
+                                                                       1.0 / (double)e.H(), sums4);
+}
+
+__global__ void k_slwl_TupTdn(ScalarLasddFields f, double L43, double L83, WLPow P,
+                              const double* __restrict__ beta, double* Tup, double* Tdn, size_t n,
+                              int nz) {
+  GRID_STRIDE(i, n) {
+    const int z = (int)(i % nz);
+    const WLScalarTerms t = wl_scalar_terms(f, i);
+    const double b = beta[z];
+    Tup[i] = L43 * (t.a6 - P.p43 * b * t.b6);
+    Tdn[i] = L83 * (t.a3 - 2 * P.p43 * b * t.c36 + P.p83 * (b * b) * t.a8);
+  }
+}
+
+void scalar_wl_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
+                       double* Tdn) {
+  const double L43 = std::pow(e.L, 4.0 / 3.0), L83 = std::pow(e.L, 8.0 / 3.0);
+  ::alfa::note_launch(); k_slwl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, L43, L83, wl_pow(e), beta, Tup, Tdn, e.N(), e.nz);
+}
+
 // 3x3 periodic box mean (Utilities.py:87-115) at (x, y, z)
 __device__ __forceinline__ double box9(const double* F, int x, int y, int z, int nx, int ny,
                                        int nz) {

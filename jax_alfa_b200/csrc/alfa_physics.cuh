@@ -80,6 +80,14 @@ void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10);
 void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
                     double* Tdn);
 
+// Wong-Lilly procedure (optSgs 2, 4)
+void lasdd_wl_sums(Engine& e, const LasddFields& f, double* sums4);
+void wl_poly(Engine& e, const double* sums4, double* coeffs6);
+void lasdd_wl_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM);
+void scalar_lasdd_wl_sums(Engine& e, const ScalarLasddFields& f, double* sums4);
+void scalar_wl_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
+                       double* Tdn);
+
 // ---- stresses / fluxes / divergence -------------------------------------
 void wall_override(Engine& e, const double* u, const double* v, const double* M,
                    const double* psi_m, const double* psi_m0, double* txz, double* tyz);

@@ -79,11 +79,9 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
     switch (L.kind) {
 #define ALFA_G(K) \
   case K: gather_rows<K, YC, N, NT>(L, nz, base, (size_t)nz, z0, v); break;
-      ALFA_G(LD_FIELD) ALFA_G(LD_MUL) ALFA_G(LD_MUL3) ALFA_G(LD_PRESSURE_R) ALFA_G(LD_ADV_XY)
-      ALFA_G(LD_ADV_Z) ALFA_G(LD_SCALAR_ADV) ALFA_G(LD_STRESS_UVP) ALFA_G(LD_STRESS_W)
-      ALFA_G(LD_W_SXX) ALFA_G(LD_THZ)
+      ALFA_LOADER_KINDS(ALFA_G)
 #undef ALFA_G
-      default: gather_rows<LD_MUL_THZ, YC, N, NT>(L, nz, base, (size_t)nz, z0, v); break;
+      default: break;
     }
     if constexpr (R == N) {
       if (threadIdx.x < YC) {
@@ -98,18 +96,11 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
     __syncthreads();
   } else {
   switch (L.kind) {
-    case LD_FIELD: y_fwd_load<LD_FIELD>(L, row, n, z0, b0); break;
-    case LD_MUL: y_fwd_load<LD_MUL>(L, row, n, z0, b0); break;
-    case LD_MUL3: y_fwd_load<LD_MUL3>(L, row, n, z0, b0); break;
-    case LD_PRESSURE_R: y_fwd_load<LD_PRESSURE_R>(L, row, n, z0, b0); break;
-    case LD_ADV_XY: y_fwd_load<LD_ADV_XY>(L, row, n, z0, b0); break;
-    case LD_ADV_Z: y_fwd_load<LD_ADV_Z>(L, row, n, z0, b0); break;
-    case LD_SCALAR_ADV: y_fwd_load<LD_SCALAR_ADV>(L, row, n, z0, b0); break;
-    case LD_STRESS_UVP: y_fwd_load<LD_STRESS_UVP>(L, row, n, z0, b0); break;
-    case LD_STRESS_W: y_fwd_load<LD_STRESS_W>(L, row, n, z0, b0); break;
-    case LD_W_SXX: y_fwd_load<LD_W_SXX>(L, row, n, z0, b0); break;
-    case LD_THZ: y_fwd_load<LD_THZ>(L, row, n, z0, b0); break;
-    default: y_fwd_load<LD_MUL_THZ>(L, row, n, z0, b0); break;
+#define ALFA_K(K) \
+  case K: y_fwd_load<K>(L, row, n, z0, b0); break;
+    ALFA_LOADER_KINDS(ALFA_K)
+#undef ALFA_K
+    default: break;
   }
   tile_fft<-1, YC, N, tile_threads<YC, N>()>(b0, p);
   }

@@ -79,9 +79,15 @@ __device__ __forceinline__ double ev_kind(const Loader& L, const At& at, int z, 
   } else if constexpr (KIND == LD_THZ) {  // DynamicSGS_ScalarLASDD_SM.py:182-185
     if (z == 0 || z == nz - 1) return at(0, 0);
     return 0.5 * (at(0, 0) + at(0, 1));
-  } else {  // LD_MUL_THZ: S * THz
+  } else if constexpr (KIND == LD_MUL_THZ) {  // S * THz
     const double t = (z == 0 || z == nz - 1) ? at(1, 0) : 0.5 * (at(1, 0) + at(1, 1));
     return at(0, 0) * t;
+  } else if constexpr (KIND == LD_WL_UVP) {  // SGSStresses_WL.py:90-99, ScalarSGSFluxes_WL.py:76-81
+    if (z == nz - 1) return 0.0;
+    return L.c[0] * at(0, 0) * at(1, 0);
+  } else {  // LD_WL_W: SGSStresses_WL.py:175-187, ScalarSGSFluxes_WL.py:149-157
+    if (z == 0 || z == nz - 1) return 0.0;
+    return L.c[0] * (0.5 * (at(0, -1) + at(0, 0))) * at(1, 0);
   }
 }
 
@@ -126,7 +132,8 @@ template <int KIND, int C>
 __device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz, int c,
                                         bool ok) {
   constexpr int NIN = (KIND == LD_FIELD || KIND == LD_THZ) ? 1
-                      : (KIND == LD_MUL || KIND == LD_MUL_THZ) ? 2
+                      : (KIND == LD_MUL || KIND == LD_MUL_THZ || KIND == LD_WL_UVP ||
+                         KIND == LD_WL_W) ? 2
                       : (KIND == LD_MUL3 || KIND == LD_PRESSURE_R || KIND == LD_STRESS_UVP ||
                          KIND == LD_STRESS_W) ? 3
                       : (KIND == LD_W_SXX) ? 9 : 6;
@@ -154,10 +161,11 @@ __device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz
   } else {
 #pragma unroll
     for (int k = 0; k < NIN; k++) {
-      constexpr bool any_m = (KIND == LD_ADV_Z || KIND == LD_STRESS_W);
+      constexpr bool any_m = (KIND == LD_ADV_Z || KIND == LD_STRESS_W || KIND == LD_WL_W);
       constexpr bool any_p = (KIND == LD_ADV_XY || KIND == LD_SCALAR_ADV || KIND == LD_THZ ||
                               KIND == LD_MUL_THZ);
-      const bool nm = (KIND == LD_ADV_Z && k < 2) || (KIND == LD_STRESS_W && k == 0);
+      const bool nm = (KIND == LD_ADV_Z && k < 2) || (KIND == LD_STRESS_W && k == 0) ||
+                      (KIND == LD_WL_W && k == 0);
       const bool np = (KIND == LD_ADV_XY && k >= 3) ||
                       (KIND == LD_SCALAR_ADV && (k == 2 || k == 5)) || (KIND == LD_THZ) ||
                       (KIND == LD_MUL_THZ && k == 1);

@@ -37,8 +37,9 @@ class MainLoop:
         self.RHS_prev = [zeros(N) for _ in range(4)]
         H = a.H
         self.MOST = (zeros(H), zeros(H), zeros(H), zeros(H), zeros(H) + 1.0, zeros(H) + 1.0)
-        self.Cs2_3D = zeros(N) + cfg["Cs2"]
-        self.Cs2PrRatio_3D = zeros(N) + cfg["Cs2PrRatio"]
+        wl = int(cfg["optSgs"]) in (2, 4)  # DerivedVars.py:101-106
+        self.Cs2_3D = zeros(N) + cfg["Cwl" if wl else "Cs2"]
+        self.Cs2PrRatio_3D = zeros(N) + cfg["CwlPrRatio" if wl else "Cs2PrRatio"]
         self.qz_sfc = zeros(H) + cfg["SensibleHeatFlux"]
         self.zero_prof = zeros(a.nz)
         # series stay on the host (pinned); one row goes to the device per step

@@ -42,6 +42,9 @@ FIXTURES = [
     ("ref_stable_het_12x12x8.npz", "stable"),
     ("ref_convective_fgr2_12x12x8.npz", "convective"),  # FGR = 2: no dealiasing
     ("ref_stable_fgr2_12x12x8.npz", "stable"),
+    ("ref_convective_wl_12x12x8.npz", "convective"),  # LASDD-WL (optSgs = 2)
+    ("ref_stable_wl4_12x12x8.npz", "stable"),  # LAD-WL (optSgs = 4)
+    ("ref_convective_wl_fgr2_12x12x8.npz", "convective"),  # LASDD-WL, FGR = 2
 ]
 # name of the libalfa entry for a recorded reference function
 ALIASES = {"PressureSolve": "ThomasPressureSolve"}
@@ -192,6 +195,8 @@ def test_whole_step_matches_reference_main():
     ("stable", (24, 24, 16), 10, {}),
     ("convective", (24, 24, 16), 10, {"FGR": 2}),  # no dealiasing, TFR = sqrt(2)
     ("stable", (24, 24, 16), 10, {"FGR": 2}),
+    ("convective", (24, 24, 16), 10, {"optSgs": 2}),  # Wong-Lilly
+    ("stable", (24, 24, 16), 10, {"optSgs": 4, "FGR": 2}),
 ])
 def test_whole_step_matches_oracle(case, grid, steps, over):
     from jax_alfa_b200.api import Simulation
