@@ -238,6 +238,40 @@ int alfa_step(alfa_ctx*, int nsteps);
 int alfa_get_state(alfa_ctx*, double* u, double* v, double* w, double* TH, double* p);
 int alfa_get_diag(alfa_ctx*, alfa_diag* out /* host; synchronises the stream */);
 
+/* ---- statistics: src/utilities/Statistics.py:47-328 (ComputeStats) -------
+ * Adds one sample to acc (device, ALFA_STATS_LEN(nz) doubles): 31 profiles
+ * of nz, in the reference's key order U V W TH dUdz dVdz dTHdz u2 v2 w2 TH2
+ * uv uw vw uTH vTH wTH txy txz tyz qz Cs2_1 Cs2_2 Cs2PrRatio Beta1 Beta2 Q
+ * dQdz Q2 wQ qHz, then the scalars M_sfc ustar qz_sfc qm_sfc.  Dimensional
+ * (u_scale = TH_scale = 1, z from z_scale), Ugal added to U and u, T_0 to TH;
+ * dry runs accumulate zeros in the moisture entries.  Zeroing acc is the
+ * reference's ResetFlag = 1; the averages are acc / samples.  M_sfc_loc,
+ * ustar: (nx, ny); qz_sfc_avg: one device double; profiles: (nz). */
+#define ALFA_STATS_NPROF 31
+#define ALFA_STATS_LEN(nz) (ALFA_STATS_NPROF * (nz) + 4)
+int alfa_ComputeStats(alfa_ctx*, const double* u, const double* v, const double* w,
+                      const double* TH, const double* dudz, const double* dvdz,
+                      const double* dTHdz, const double* M_sfc_loc, const double* ustar,
+                      const double* qz_sfc_avg, const double* txy, const double* txz,
+                      const double* tyz, const double* qz, const double* Cs2_1D_avg1,
+                      const double* Cs2_1D_avg2, const double* Cs2PrRatio_1D,
+                      const double* beta1_1D, const double* beta2_1D, double* acc);
+/* The same sample from the context's state after alfa_step (the arguments
+ * Main.py:550-558 passes: the new u, v, w, TH, this step's gradients, surface
+ * fields, SGS stresses and flux, and the latest coefficient profiles). */
+int alfa_stats_sample(alfa_ctx*, double* acc);
+
+/* ---- checkpoint / restart (no counterpart in the reference) --------------
+ * Everything alfa_step carries from one iteration to the next: u v w TH p,
+ * the previous right-hand sides, the 3-D SGS coefficients, the MOST planes,
+ * the coefficient profiles, the iteration counter and CFLmax.  dst / src are
+ * device buffers of alfa_checkpoint_doubles(ctx) doubles; a context of the
+ * same configuration that loads a checkpoint continues bit for bit as the
+ * one that saved it (series set with alfa_set_series are not included). */
+size_t alfa_checkpoint_doubles(const alfa_ctx*);
+int alfa_save_checkpoint(alfa_ctx*, double* dst);
+int alfa_load_checkpoint(alfa_ctx*, const double* src);
+
 /* No counterpart in the reference.  alfa_PlanarMean without a context and
  * without any device allocation, for callers that may not allocate: code
  * running inside another runtime's memory management, such as a JAX/XLA

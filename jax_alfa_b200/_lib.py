@@ -107,6 +107,10 @@ SIGNATURES = {
     "alfa_set_series": [c_double_p, c_double_p, c_double_p, c_double_p, I],
     "alfa_step": [I],
     "alfa_get_state": [P] * 5,
+    "alfa_ComputeStats": [P] * 20,
+    "alfa_stats_sample": [P],
+    "alfa_save_checkpoint": [P],
+    "alfa_load_checkpoint": [P],
 }
 
 _lib = None
@@ -145,6 +149,8 @@ def load():
     lib.alfa_time_kernel.restype = I
     lib.alfa_PlanarMean_noalloc.argtypes = [P, I, I, I, P, c_void_p]
     lib.alfa_PlanarMean_noalloc.restype = I
+    lib.alfa_checkpoint_doubles.argtypes = [CTX]
+    lib.alfa_checkpoint_doubles.restype = ctypes.c_size_t
     for name, args in SIGNATURES.items():
         f = getattr(lib, name)
         f.argtypes = [CTX] + args

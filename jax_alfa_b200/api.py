@@ -15,6 +15,7 @@ in libalfa's kernels.
 on the device.
 """
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -316,6 +317,37 @@ class Alfa:
         self._call("alfa_BuoyancyOpt2", self._f(TH), self._p(out))
         return out
 
+    def InitializeStats(self, ZeRo1D=None):
+        """``Statistics.py:335-380``."""
+        nz = self.nz
+        return stats_to_dict(np.zeros(len(STATS_PROFILE_KEYS) * nz + len(STATS_SCALAR_KEYS)),
+                             nz, float(self.cfg["Ugal"]))
+
+    def ComputeStats(self, u, v, w, TH, Q, dudz, dvdz, dTHdz, dQdz, M_sfc_loc, ustar,
+                     qz_sfc_avg, qm_sfc_avg, txy, txz, tyz, qz, qHz_q, Cs2_1D_avg1,
+                     Cs2_1D_avg2, Cs2PrRatio_1D, beta1_1D, beta2_1D, StatsDict, ResetFlag,
+                     ZeRo3D=None):
+        """``Statistics.py:47-328`` (dry: Q, dQdz, qHz_q must be zero or None)."""
+        if ResetFlag == 1:
+            d = self.InitializeStats()
+            d["Ugal"] = StatsDict["Ugal"]
+            return d
+        for x in (Q, dQdz, qHz_q):
+            if x is not None and bool(torch.any(torch.as_tensor(x) != 0)):
+                raise _lib.AlfaError("moisture statistics are not implemented (dry runs only)")
+        if qm_sfc_avg not in (None, 0, 0.0):
+            raise _lib.AlfaError("moisture statistics are not implemented (dry runs only)")
+        nz = self.nz
+        acc = dict_to_stats(StatsDict, nz, self.device)
+        q = torch.as_tensor(qz_sfc_avg, dtype=F64, device=self.device).reshape(1).contiguous()
+        profs = [self._prof(x) for x in (Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D, beta1_1D,
+                                         beta2_1D)]
+        self._call("alfa_ComputeStats", self._f(u), self._f(v), self._f(w), self._f(TH),
+                   self._f(dudz), self._f(dvdz), self._f(dTHdz), self._p(M_sfc_loc, self.H),
+                   self._p(ustar, self.H), self._p(q), self._f(txy), self._f(txz),
+                   self._f(tyz), self._f(qz), *[self._p(x) for x in profs], self._p(acc))
+        return stats_to_dict(acc, nz, StatsDict["Ugal"])
+
     def _mom25(self):
         return [None if 6 <= i <= 9 else self._new(self.Q if i in (20, 22) else self.N)
                 for i in range(25)]
@@ -432,6 +464,59 @@ class Alfa:
         return out
 
 
+# ----------------------------------------------------------------------
+# Statistics (src/utilities/Statistics.py:47-380) and output writers
+# (src/Main.py:588-635), on the GPU accumulator of alfa_ComputeStats
+# ----------------------------------------------------------------------
+STATS_PROFILE_KEYS = ("U", "V", "W", "TH", "dUdz", "dVdz", "dTHdz",
+                      "u2", "v2", "w2", "TH2", "uv", "uw", "vw", "uTH", "vTH", "wTH",
+                      "txy", "txz", "tyz", "qz", "Cs2_1", "Cs2_2", "Cs2PrRatio",
+                      "Beta1", "Beta2", "Q", "dQdz", "Q2", "wQ", "qHz")
+STATS_SCALAR_KEYS = ("M_sfc", "ustar", "qz_sfc", "qm_sfc")
+
+
+def stats_to_dict(acc, nz, Ugal):
+    """Accumulator (ALFA_STATS_LEN(nz) doubles) -> the reference's StatsDict."""
+    a = acc.detach().cpu().numpy() if isinstance(acc, torch.Tensor) else np.asarray(acc)
+    d = {k: a[i * nz:(i + 1) * nz].copy() for i, k in enumerate(STATS_PROFILE_KEYS)}
+    base = len(STATS_PROFILE_KEYS) * nz
+    d.update({k: float(a[base + j]) for j, k in enumerate(STATS_SCALAR_KEYS)})
+    d["Ugal"] = Ugal
+    d["ZeRo1D"] = np.zeros(nz)
+    return d
+
+
+def dict_to_stats(d, nz, device):
+    """The reference's StatsDict -> accumulator tensor on ``device``."""
+    acc = np.zeros(len(STATS_PROFILE_KEYS) * nz + len(STATS_SCALAR_KEYS))
+    for i, k in enumerate(STATS_PROFILE_KEYS):
+        acc[i * nz:(i + 1) * nz] = np.asarray(d[k], dtype=np.float64)
+    base = len(STATS_PROFILE_KEYS) * nz
+    for j, k in enumerate(STATS_SCALAR_KEYS):
+        acc[base + j] = float(d[k])
+    return torch.as_tensor(acc, dtype=F64, device=device)
+
+
+def write_statistics(out_dir, iteration, StatsDict, SampleCounter):
+    """``Main.py:588-603``: the averages over SampleCounter samples saved as
+    ALFA_Statistics_Iteration_<iteration>.npz (Ugal and ZeRo1D as they are)."""
+    out = {}
+    for k, v in StatsDict.items():
+        out[k] = v if k in ("Ugal", "ZeRo1D") else np.asarray(v) / SampleCounter
+    path = os.path.join(out_dir, f"ALFA_Statistics_Iteration_{iteration}.npz")
+    np.savez(path, **out)
+    return path
+
+
+def write_3d_fields(out_dir, iteration, u, v, w, TH, Ugal, T_0_nondim):
+    """``Main.py:620-635``: u with Ugal added back, TH absolute, saved as
+    ALFA_3DFields_Iteration_<iteration>.npz."""
+    h = lambda t: t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+    path = os.path.join(out_dir, f"ALFA_3DFields_Iteration_{iteration}.npz")
+    np.savez(path, u=h(u) + Ugal, v=h(v), w=h(w), TH=h(TH) + T_0_nondim)
+    return path
+
+
 class Simulation:
     """The reference's time loop (``src/Main.py:156-541``) run by libalfa
     with the state on the device.  Fields in: dimensional (u total incl.
@@ -475,6 +560,45 @@ class Simulation:
         out = [a._new(a.N) for _ in range(5)]
         self._call("alfa_get_state", *[a._p(x) for x in out])
         return dict(zip(("u", "v", "w", "TH", "p"), out))
+
+    def stats_sample(self, acc=None):
+        """Add this iteration's statistics sample (Main.py:547-558) to the
+        accumulator ``acc`` (a new zeroed one if None) and return it."""
+        a = self.alfa
+        if acc is None:
+            acc = torch.zeros(len(STATS_PROFILE_KEYS) * a.nz + len(STATS_SCALAR_KEYS),
+                              dtype=F64, device=a.device)
+        self._call("alfa_stats_sample", a._p(acc))
+        return acc
+
+    def checkpoint(self):
+        """Everything the time loop carries between iterations, as one device
+        tensor (alfa_save_checkpoint)."""
+        a = self.alfa
+        buf = torch.empty(int(a.lib.alfa_checkpoint_doubles(a.ctx)), dtype=F64, device=a.device)
+        self._call("alfa_save_checkpoint", a._p(buf))
+        return buf
+
+    def restore(self, buf):
+        """Continue from a checkpoint() of a run with the same configuration."""
+        a = self.alfa
+        n = int(a.lib.alfa_checkpoint_doubles(a.ctx))
+        buf = torch.as_tensor(buf, dtype=F64).to(a.device).contiguous()
+        if buf.numel() != n:
+            raise ValueError(f"checkpoint holds {buf.numel()} values, this configuration {n}")
+        self._call("alfa_load_checkpoint", a._p(buf))
+        return self
+
+    def save(self, path):
+        """checkpoint() written to an .npz file (key "checkpoint", plus the grid)."""
+        a = self.alfa
+        np.savez(path, checkpoint=self.checkpoint().cpu().numpy(),
+                 grid=np.array([a.nx, a.ny, a.nz]))
+        return path
+
+    def load(self, path):
+        z = np.load(path)
+        return self.restore(torch.as_tensor(z["checkpoint"]))
 
     def diag(self):
         d = _lib.AlfaDiag()

@@ -378,12 +378,13 @@ static void carve(alfa_ctx* c, Carver& k) {
   // engine scratch
   e.T_elems = (size_t)e.mx * e.myh * nz;
   for (int i = 0; i < 4; i++) e.T[i] = k.take<cd>(e.T_elems);
-  e.red_elems = (size_t)256 * 12 * nz + 1024;
+  e.red_elems = (size_t)256 * 16 * nz + 1024;
   e.red = k.take<double>(e.red_elems);
   e.scal = k.take<double>(64 * nz + 256);
   e.W_elems = N;
   e.W = k.take<double>(N);
   e.mat = k.take<double>(e.P());
+  e.stat = k.take<double>((size_t)24 * nz + 64);
 }
 
 // ---------------------------------------------------------------------------
@@ -1615,6 +1616,93 @@ int alfa_get_diag(alfa_ctx* c, alfa_diag* o) {
   o->qz_sfc_avg = q;
   if (!std::isfinite(cfl)) return e.fail("non-finite velocity", ALFA_E_NUMERIC);
   return ALFA_OK;
+}
+
+int alfa_ComputeStats(alfa_ctx* c, const double* u, const double* v, const double* w,
+                      const double* TH, const double* dudz, const double* dvdz,
+                      const double* dTHdz, const double* M_sfc_loc, const double* ustar,
+                      const double* qz_sfc_avg, const double* txy, const double* txz,
+                      const double* tyz, const double* qz, const double* Cs2_1D_avg1,
+                      const double* Cs2_1D_avg2, const double* Cs2PrRatio_1D,
+                      const double* beta1_1D, const double* beta2_1D, double* acc) {
+  CTX_CHECK(c);
+  NN(u); NN(v); NN(w); NN(TH); NN(dudz); NN(dvdz); NN(dTHdz); NN(M_sfc_loc); NN(ustar);
+  NN(qz_sfc_avg); NN(txy); NN(txz); NN(tyz); NN(qz); NN(Cs2_1D_avg1); NN(Cs2_1D_avg2);
+  NN(Cs2PrRatio_1D); NN(beta1_1D); NN(beta2_1D); NN(acc);
+  Engine& e = c->e;
+  StatsIn a{u, v, w, TH, dudz, dvdz, dTHdz, txy, txz, tyz, qz, M_sfc_loc, ustar, qz_sfc_avg,
+            Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D, beta1_1D, beta2_1D, e.cfg.Ugal,
+            e.T0_nondim};
+  compute_stats(e, a, acc);
+  return check_launch(e, "ComputeStats");
+}
+
+int alfa_stats_sample(alfa_ctx* c, double* acc) {
+  CTX_CHECK(c);
+  NN(acc);
+  Work& W = c->w;
+  if (!W.have_state) return c->e.fail("alfa_stats_sample before alfa_init_state", ALFA_E_STATE);
+  const int nz = c->e.nz;
+  return alfa_ComputeStats(c, W.u, W.v, W.w, W.TH, W.g[6], W.g[7], W.gT[2], W.M, W.ustar,
+                           W.d_qavg, W.mom[3], W.mom[4], W.mom[5], W.qz, W.prof + 21 * nz,
+                           W.prof + 22 * nz, W.prof + 23 * nz, W.prof + 20 * nz,
+                           W.prof + 24 * nz, acc);
+}
+
+// checkpoint layout: u v w TH p RHS[4] Cs2 Cs2Pr (N each), most[6] (H each),
+// profiles (PROF doubles), then iteration and CFLmax
+static size_t ckpt_prof(const Engine& e) { return (size_t)64 * e.nz + 64; }
+
+size_t alfa_checkpoint_doubles(const alfa_ctx* c) {
+  if (!c) return 0;
+  const Engine& e = c->e;
+  return 11 * e.N() + 6 * e.H() + ckpt_prof(e) + 2;
+}
+
+static int checkpoint_copy(alfa_ctx* c, double* buf, bool save) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const size_t N = e.N(), H = e.H();
+  double* f[11] = {W.u, W.v, W.w, W.TH, W.p, W.RHS[0], W.RHS[1], W.RHS[2], W.RHS[3], W.Cs2,
+                   W.Cs2Pr};
+  size_t off = 0;
+  auto mv = [&](double* dev, size_t n) {
+    if (save)
+      cudaMemcpyAsync(buf + off, dev, n * 8, cudaMemcpyDeviceToDevice, e.stream);
+    else
+      cudaMemcpyAsync(dev, buf + off, n * 8, cudaMemcpyDeviceToDevice, e.stream);
+    off += n;
+  };
+  for (double* p : f) mv(p, N);
+  for (int i = 0; i < 6; i++) mv(W.most[i], H);
+  mv(W.prof, ckpt_prof(e));
+  double tail[2] = {(double)W.iteration, W.CFLmax};
+  if (save) {
+    cudaMemcpyAsync(buf + off, tail, 2 * 8, cudaMemcpyHostToDevice, e.stream);
+  } else {
+    cudaMemcpyAsync(tail, buf + off, 2 * 8, cudaMemcpyDeviceToHost, e.stream);
+  }
+  if (cudaStreamSynchronize(e.stream) != cudaSuccess)
+    return e.fail("checkpoint copy failed", ALFA_E_CUDA);
+  if (!save) {
+    W.iteration = (int)tail[0];
+    W.CFLmax = tail[1];
+    W.have_state = 1;
+  }
+  return ALFA_OK;
+}
+
+int alfa_save_checkpoint(alfa_ctx* c, double* dst) {
+  CTX_CHECK(c);
+  NN(dst);
+  if (!c->w.have_state) return c->e.fail("alfa_save_checkpoint before alfa_init_state", ALFA_E_STATE);
+  return checkpoint_copy(c, dst, true);
+}
+
+int alfa_load_checkpoint(alfa_ctx* c, const double* src) {
+  CTX_CHECK(c);
+  NN(src);
+  return checkpoint_copy(c, const_cast<double*>(src), false);
 }
 
 }  // extern "C"

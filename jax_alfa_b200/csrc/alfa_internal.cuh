@@ -130,6 +130,7 @@ struct Engine {
   double* W = nullptr;            // field workspace arena
   size_t W_elems = 0;
   double* mat = nullptr;          // a loader's expression, materialised (P elements)
+  double* stat = nullptr;         // statistics scratch (24 nz)
 
   size_t N() const { return (size_t)nx * ny * nz; }
   size_t P() const { return (size_t)mx * my * nz; }

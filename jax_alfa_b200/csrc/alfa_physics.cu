@@ -23,7 +23,7 @@ static inline int nblocks(size_t n, int tpb = TPB) {
 // order sum of the partials (deterministic, independent of timing)
 // ---------------------------------------------------------------------------
 static constexpr int RED_BLOCKS = 256;
-static constexpr int RED_MAXQ = 12;
+static constexpr int RED_MAXQ = 16;  // e.red holds RED_BLOCKS x RED_MAXQ x nz partials
 
 struct RedArgs {
   const double* f[RED_MAXQ];
@@ -866,6 +866,171 @@ void scalar_wl_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta
                        double* Tdn) {
   const double L43 = std::pow(e.L, 4.0 / 3.0), L83 = std::pow(e.L, 8.0 / 3.0);
   ::alfa::note_launch(); k_slwl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, L43, L83, wl_pow(e), beta, Tup, Tdn, e.N(), e.nz);
+}
+
+// ---------------------------------------------------------------------------
+// Plane-averaged statistics (Statistics.py:47-328), one sample added to the
+// accumulator acc[key * nz + z] (profile keys in STATS order) and
+// acc[31 * nz + j] (M_sfc, ustar, qz_sfc, qm_sfc).  Dry: the moisture
+// entries (Q, dQdz, Q2, wQ, qHz, qm_sfc) accumulate zeros.
+// ---------------------------------------------------------------------------
+enum StatKey {
+  ST_U = 0, ST_V, ST_W, ST_TH, ST_dUdz, ST_dVdz, ST_dTHdz, ST_u2, ST_v2, ST_w2, ST_TH2, ST_uv,
+  ST_uw, ST_vw, ST_uTH, ST_vTH, ST_wTH, ST_txy, ST_txz, ST_tyz, ST_qz, ST_Cs2_1, ST_Cs2_2,
+  ST_Cs2PrRatio, ST_Beta1, ST_Beta2, ST_NPROF = 31
+};
+
+// pass 1 sums per level: u v w TH dudz dvdz dTHdz txy txz tyz qz u_st v_st TH_st
+__global__ void k_stats_mean_partial(StatsIn a, size_t H, int nz, double* __restrict__ part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double s[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t r = r0; r < r1; r++) {
+      const size_t i = r * nz + z;
+      const double u = a.u[i], v = a.v[i], T = a.TH[i];
+      s[0] += u;
+      s[1] += v;
+      s[2] += a.w[i];
+      s[3] += T;
+      s[4] += a.dudz[i];
+      s[5] += a.dvdz[i];
+      s[6] += a.dTHdz[i];
+      s[7] += a.txy[i];
+      s[8] += a.txz[i];
+      s[9] += a.tyz[i];
+      s[10] += a.qz[i];
+      if (z == 0) {
+        s[11] += u + a.Ugal;
+        s[12] += v;
+        s[13] += T;
+      } else {
+        s[11] += 0.5 * (a.u[i - 1] + u);
+        s[12] += 0.5 * (a.v[i - 1] + v);
+        s[13] += 0.5 * (a.TH[i - 1] + T);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 14; q++) part[((size_t)blockIdx.x * 14 + q) * nz + z] = s[q];
+  }
+}
+
+// pass 2 sums of fluctuation products, with m = the pass-1 plane means
+__global__ void k_stats_var_partial(StatsIn a, const double* __restrict__ m, size_t H, int nz,
+                                    double* __restrict__ part) {
+  const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
+  const size_t r0 = blockIdx.x * rpb;
+  const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
+  const double Ug = a.Ugal;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    const double mU = m[0 * nz + z] + Ug, mV = m[1 * nz + z], mW = m[2 * nz + z];
+    const double mT = m[3 * nz + z];
+    const double muS = m[11 * nz + z] + Ug, mvS = m[12 * nz + z], mTS = m[13 * nz + z];
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t r = r0; r < r1; r++) {
+      const size_t i = r * nz + z;
+      const double u = a.u[i], v = a.v[i], T = a.TH[i];
+      const double uf = u + Ug - mU, vf = v - mV, wf = a.w[i] - mW, Tf = T - mT;
+      s[0] += uf * uf;
+      s[1] += vf * vf;
+      s[2] += wf * wf;
+      s[3] += Tf * Tf;
+      s[4] += uf * vf;
+      s[5] += uf * Tf;
+      s[6] += vf * Tf;
+      double uS, vS, TS;
+      if (z == 0) {
+        uS = u + Ug;
+        vS = v;
+        TS = T;
+      } else {
+        uS = 0.5 * (a.u[i - 1] + u);
+        vS = 0.5 * (a.v[i - 1] + v);
+        TS = 0.5 * (a.TH[i - 1] + T);
+      }
+      const double usf = uS + Ug - muS, vsf = vS - mvS, wsf = wf, Tsf = TS - mTS;
+      s[7] += usf * wsf;
+      s[8] += vsf * wsf;
+      s[9] += wsf * Tsf;
+    }
+#pragma unroll
+    for (int q = 0; q < 10; q++) part[((size_t)blockIdx.x * 10 + q) * nz + z] = s[q];
+  }
+}
+
+// surface means (one block) and the accumulation of every entry
+__global__ void k_stats_accumulate(StatsIn a, const double* __restrict__ m,
+                                   const double* __restrict__ var, size_t H, int nz,
+                                   double us_zs, double* acc) {
+  __shared__ double red[2][1024];
+  double sM = 0.0, sU = 0.0;
+  for (size_t r = threadIdx.x; r < H; r += blockDim.x) {
+    sM += a.M[r];
+    sU += a.ustar[r] * a.ustar[r];
+  }
+  red[0][threadIdx.x] = sM;
+  red[1][threadIdx.x] = sU;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + w];
+      red[1][threadIdx.x] += red[1][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  const double Ug = a.Ugal;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double* A = acc;
+    A[ST_U * nz + z] += m[0 * nz + z] + Ug;
+    A[ST_V * nz + z] += m[1 * nz + z];
+    A[ST_W * nz + z] += m[2 * nz + z];
+    A[ST_TH * nz + z] += m[3 * nz + z] + a.T0;
+    A[ST_dUdz * nz + z] += m[4 * nz + z] * us_zs;
+    A[ST_dVdz * nz + z] += m[5 * nz + z] * us_zs;
+    A[ST_dTHdz * nz + z] += m[6 * nz + z] * us_zs;
+    A[ST_u2 * nz + z] += var[0 * nz + z];
+    A[ST_v2 * nz + z] += var[1 * nz + z];
+    A[ST_w2 * nz + z] += var[2 * nz + z];
+    A[ST_TH2 * nz + z] += var[3 * nz + z];
+    A[ST_uv * nz + z] += var[4 * nz + z];
+    A[ST_uTH * nz + z] += var[5 * nz + z];
+    A[ST_vTH * nz + z] += var[6 * nz + z];
+    A[ST_uw * nz + z] += var[7 * nz + z];
+    A[ST_vw * nz + z] += var[8 * nz + z];
+    A[ST_wTH * nz + z] += var[9 * nz + z];
+    A[ST_txy * nz + z] += m[7 * nz + z];
+    A[ST_txz * nz + z] += m[8 * nz + z];
+    A[ST_tyz * nz + z] += m[9 * nz + z];
+    A[ST_qz * nz + z] += m[10 * nz + z];
+    A[ST_Cs2_1 * nz + z] += a.cs2_1[z];
+    A[ST_Cs2_2 * nz + z] += a.cs2_2[z];
+    A[ST_Cs2PrRatio * nz + z] += a.cs2pr[z];
+    A[ST_Beta1 * nz + z] += a.beta1[z];
+    A[ST_Beta2 * nz + z] += a.beta2[z];
+  }
+  if (threadIdx.x == 0) {
+    double* S = acc + (size_t)ST_NPROF * nz;
+    S[0] += red[0][0] / (double)H;
+    S[1] += sqrt(red[1][0] / (double)H);
+    S[2] += *a.qz_sfc_avg;
+  }
+}
+
+void compute_stats(Engine& e, const StatsIn& a, double* acc) {
+  const int nb = red_blocks(e);
+  const int nz = e.nz;
+  double* m = e.stat;             // 14 nz plane means
+  double* var = e.stat + 14 * nz;  // 10 nz
+  ::alfa::note_launch(); k_stats_mean_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)14 * nz), TPB, 0, e.stream>>>(
+      e.red, nb, 14, nz, 1.0 / (double)e.H(), m);
+  ::alfa::note_launch(); k_stats_var_partial<<<nb, 128, 0, e.stream>>>(a, m, e.H(), nz, e.red);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)10 * nz), TPB, 0, e.stream>>>(
+      e.red, nb, 10, nz, 1.0 / (double)e.H(), var);
+  // u_scale = TH_scale = 1: dUdz, dVdz, dTHdz scale by 1 / z_scale
+  ::alfa::note_launch(); k_stats_accumulate<<<1, 1024, 0, e.stream>>>(a, m, var, e.H(), nz,
+                                                                     1.0 / e.z_scale, acc);
 }
 
 // 3x3 periodic box mean (Utilities.py:87-115) at (x, y, z)

@@ -80,6 +80,15 @@ void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10);
 void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
                     double* Tdn);
 
+// plane-averaged statistics (Statistics.py:47-328): one sample added to acc
+struct StatsIn {
+  const double *u, *v, *w, *TH, *dudz, *dvdz, *dTHdz, *txy, *txz, *tyz, *qz;
+  const double *M, *ustar, *qz_sfc_avg;  // planes (nx, ny) and one scalar
+  const double *cs2_1, *cs2_2, *cs2pr, *beta1, *beta2;  // profiles (nz)
+  double Ugal, T0;
+};
+void compute_stats(Engine& e, const StatsIn& a, double* acc);
+
 // Wong-Lilly procedure (optSgs 2, 4)
 void lasdd_wl_sums(Engine& e, const LasddFields& f, double* sums4);
 void wl_poly(Engine& e, const double* sums4, double* coeffs6);

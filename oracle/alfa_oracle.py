@@ -1386,6 +1386,95 @@ class AlfaOracle:
                 T * self.z_scale / (self.u_scale * self.TH_scale))
 
 
+# ----------------------------------------------------------------------
+# src/utilities/Statistics.py:47-380: plane-averaged statistics (dry:
+# the moisture entries accumulate zeros)
+# ----------------------------------------------------------------------
+STATS_PROFILE_KEYS = ("U", "V", "W", "TH", "dUdz", "dVdz", "dTHdz",
+                      "u2", "v2", "w2", "TH2", "uv", "uw", "vw", "uTH", "vTH", "wTH",
+                      "txy", "txz", "tyz", "qz", "Cs2_1", "Cs2_2", "Cs2PrRatio",
+                      "Beta1", "Beta2", "Q", "dQdz", "Q2", "wQ", "qHz")
+STATS_SCALAR_KEYS = ("M_sfc", "ustar", "qz_sfc", "qm_sfc")
+
+
+def InitializeStats(o, nz):
+    """``Statistics.py:335-380``."""
+    d = {k: np.zeros(nz) for k in STATS_PROFILE_KEYS}
+    d.update({k: 0.0 for k in STATS_SCALAR_KEYS})
+    d["Ugal"] = o.Ugal
+    d["ZeRo1D"] = np.zeros(nz)
+    return d
+
+
+def ComputeStats(o, u, v, w, TH, dudz, dvdz, dTHdz, M_sfc_loc, ustar, qz_sfc_avg,
+                 txy, txz, tyz, qz, Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D,
+                 beta1_1D, beta2_1D, StatsDict, ResetFlag):
+    """``Statistics.py:47-328`` for a dry run (Q = dQdz = qHz = 0)."""
+    nz = o.nz
+    if ResetFlag == 1:
+        return InitializeStats(o, nz) | {"Ugal": StatsDict["Ugal"]}
+    us, ts, zs = o.u_scale, o.TH_scale, o.z_scale
+    Ugal = StatsDict["Ugal"]
+    m = lambda f: np.mean(f, axis=(0, 1))
+    mU = (m(u) + Ugal) * us
+    mV = m(v) * us
+    mW = m(w) * us
+    mTH_anom = m(TH)
+    mTH = (mTH_anom + o.T_0_nondim) * ts
+    new = {}
+    new["U"], new["V"], new["W"], new["TH"] = mU, mV, mW, mTH
+    new["dUdz"] = m(dudz) * (us / zs)
+    new["dVdz"] = m(dvdz) * (us / zs)
+    new["dTHdz"] = m(dTHdz) * (ts / zs)
+    uf = u + Ugal - mU
+    vf = v - mV
+    wf = w - mW
+    Tf = TH - mTH_anom
+    new["u2"] = m(uf ** 2) * us ** 2
+    new["v2"] = m(vf ** 2) * us ** 2
+    new["w2"] = m(wf ** 2) * us ** 2
+    new["TH2"] = m(Tf ** 2) * ts ** 2
+    new["uv"] = m(uf * vf) * us ** 2
+    new["uTH"] = m(uf * Tf) * (us * ts)
+    new["vTH"] = m(vf * Tf) * (us * ts)
+    u_st = np.zeros_like(u)
+    v_st = np.zeros_like(v)
+    T_st = np.zeros_like(TH)
+    u_st[:, :, 1:nz] = o.StagGridAvg(u)
+    v_st[:, :, 1:nz] = o.StagGridAvg(v)
+    T_st[:, :, 1:nz] = o.StagGridAvg(TH)
+    u_st[:, :, 0] = u[:, :, 0] + Ugal
+    v_st[:, :, 0] = v[:, :, 0]
+    T_st[:, :, 0] = TH[:, :, 0]
+    mu_st = (m(u_st) + Ugal) * us
+    mv_st = m(v_st) * us
+    mw_st = m(w) * us
+    mT_st = m(T_st) * ts
+    usf = u_st + Ugal - mu_st
+    vsf = v_st - mv_st
+    wsf = w - mw_st
+    Tsf = T_st - mT_st
+    new["uw"] = m(usf * wsf) * us ** 2
+    new["vw"] = m(vsf * wsf) * us ** 2
+    new["wTH"] = m(wsf * Tsf) * (us * ts)
+    new["txy"] = m(txy) * us ** 2
+    new["txz"] = m(txz) * us ** 2
+    new["tyz"] = m(tyz) * us ** 2
+    new["qz"] = m(qz) * (us * ts)
+    new["Cs2_1"], new["Cs2_2"], new["Cs2PrRatio"] = Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D
+    new["Beta1"], new["Beta2"] = beta1_1D, beta2_1D
+    for k in ("Q", "dQdz", "Q2", "wQ", "qHz"):
+        new[k] = np.zeros(nz)
+    new["M_sfc"] = np.mean(M_sfc_loc)
+    new["ustar"] = np.sqrt(np.mean(ustar ** 2)) * us
+    new["qz_sfc"] = qz_sfc_avg * us * ts
+    new["qm_sfc"] = 0.0
+    out = {k: StatsDict[k] + new[k] for k in STATS_PROFILE_KEYS + STATS_SCALAR_KEYS}
+    out["Ugal"] = Ugal
+    out["ZeRo1D"] = StatsDict["ZeRo1D"]
+    return out
+
+
 class OracleRun:
     """The time loop of ``src/Main.py:46-541`` on the oracle (dry, optSgs 0-4,
     constant geostrophic wind).  ``step()`` advances one iteration
@@ -1416,6 +1505,9 @@ class OracleRun:
         self.istep = int(cfg["istep"])
         self.CFLmax = 0.0
         self.last = {}
+        nz = o.nz  # coefficient profiles start at zero (Main.py:141-145)
+        self.Cs2_1D_avg1, self.Cs2_1D_avg2, self.Cs2PrRatio_1D = (np.zeros(nz) for _ in range(3))
+        self.beta1_1D, self.beta2_1D = np.zeros(nz), np.zeros(nz)
 
     def step(self):
         o, it, c = self.o, self.iteration, self.cfg
@@ -1494,5 +1586,17 @@ class OracleRun:
         self.CFL = cfl
         self.CFLmax = max(self.CFLmax, cfl)
         self.ustar, self.M_sfc_loc, self.qz_sfc_avg = ustar, M, qavg
+        self.last.update(dudz=grads[6], dvdz=grads[7], dTHdz=dTHdz, txy=mom[3], txz=mom[4],
+                         tyz=mom[5], qz=qz)
         self.iteration += 1
         return self
+
+    def stats_sample(self, StatsDict):
+        """ComputeStats with the arguments Main.py:550-558 passes after this
+        iteration."""
+        L = self.last
+        return ComputeStats(self.o, self.u, self.v, self.w, self.TH, L["dudz"], L["dvdz"],
+                            L["dTHdz"], self.M_sfc_loc, self.ustar, float(self.qz_sfc_avg),
+                            L["txy"], L["txz"], L["tyz"], L["qz"], self.Cs2_1D_avg1,
+                            self.Cs2_1D_avg2, self.Cs2PrRatio_1D, self.beta1_1D, self.beta2_1D,
+                            StatsDict, 0)
