@@ -261,6 +261,25 @@ int alfa_ComputeStats(alfa_ctx*, const double* u, const double* v, const double*
  * fields, SGS stresses and flux, and the latest coefficient profiles). */
 int alfa_stats_sample(alfa_ctx*, double* acc);
 
+/* ---- CUDA-graph step and ensembles (no counterpart in the reference) -----
+ * alfa_step_graph: as alfa_step, each step replayed from a captured CUDA
+ * graph (one per iteration parity and dynamic/static SGS step, captured on
+ * first use; the bootstrap step runs directly).  Needs a non-default stream
+ * (alfa_set_stream).  Results equal alfa_step's bit for bit.
+ * Ensemble: independent contexts of any grid sizes advanced together; each
+ * step of all members is one CUDA graph launch in which every member runs on
+ * its own stream.  Members must have state; create gives each member its own
+ * stream (restored to the default at destroy).  Members at different
+ * iterations or with different dynamic intervals step one by one instead.
+ * alfa_ensemble_sync waits for the work issued so far. */
+int alfa_step_graph(alfa_ctx*, int nsteps);
+typedef struct alfa_ensemble alfa_ensemble;
+int alfa_ensemble_create(alfa_ctx* const* members, int n, alfa_ensemble** out);
+int alfa_ensemble_step(alfa_ensemble*, int nsteps);
+int alfa_ensemble_sync(alfa_ensemble*);
+const char* alfa_ensemble_error(const alfa_ensemble*);
+void alfa_ensemble_destroy(alfa_ensemble*);
+
 /* ---- checkpoint / restart (no counterpart in the reference) --------------
  * Everything alfa_step carries from one iteration to the next: u v w TH p,
  * the previous right-hand sides, the 3-D SGS coefficients, the MOST planes,

@@ -111,6 +111,7 @@ SIGNATURES = {
     "alfa_stats_sample": [P],
     "alfa_save_checkpoint": [P],
     "alfa_load_checkpoint": [P],
+    "alfa_step_graph": [I],
 }
 
 _lib = None
@@ -151,6 +152,16 @@ def load():
     lib.alfa_PlanarMean_noalloc.restype = I
     lib.alfa_checkpoint_doubles.argtypes = [CTX]
     lib.alfa_checkpoint_doubles.restype = ctypes.c_size_t
+    lib.alfa_ensemble_create.argtypes = [ctypes.POINTER(c_void_p), I, ctypes.POINTER(c_void_p)]
+    lib.alfa_ensemble_create.restype = I
+    lib.alfa_ensemble_step.argtypes = [c_void_p, I]
+    lib.alfa_ensemble_step.restype = I
+    lib.alfa_ensemble_sync.argtypes = [c_void_p]
+    lib.alfa_ensemble_sync.restype = I
+    lib.alfa_ensemble_error.argtypes = [c_void_p]
+    lib.alfa_ensemble_error.restype = ctypes.c_char_p
+    lib.alfa_ensemble_destroy.argtypes = [c_void_p]
+    lib.alfa_ensemble_destroy.restype = None
     for name, args in SIGNATURES.items():
         f = getattr(lib, name)
         f.argtypes = [CTX] + args

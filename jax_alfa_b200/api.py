@@ -464,6 +464,50 @@ class Alfa:
         return out
 
 
+class Ensemble:
+    """Independent simulations (any grid sizes) advanced together: every step
+    of all members is one CUDA graph launch (alfa_ensemble_*)."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        self.lib = _lib.load()
+        for s in self.sims:  # their setup work must be done first
+            torch.cuda.current_stream(s.alfa.device).synchronize()
+        arr = (ctypes.c_void_p * len(self.sims))(*[s.alfa.ctx.value for s in self.sims])
+        h = ctypes.c_void_p()
+        rc = self.lib.alfa_ensemble_create(arr, len(self.sims), ctypes.byref(h))
+        if rc != 0:
+            raise _lib.AlfaError(f"alfa_ensemble_create failed ({rc})")
+        self.h = h
+
+    def step(self, n=1):
+        rc = self.lib.alfa_ensemble_step(self.h, int(n))
+        if rc != 0:
+            raise _lib.AlfaError(f"alfa_ensemble_step failed ({rc}): "
+                                 f"{self.lib.alfa_ensemble_error(self.h).decode()}")
+        return self
+
+    def sync(self):
+        if self.lib.alfa_ensemble_sync(self.h) != 0:
+            raise _lib.AlfaError("ensemble synchronisation failed")
+        return self
+
+    def states(self):
+        self.sync()
+        return [s.state() for s in self.sims]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.alfa_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ----------------------------------------------------------------------
 # Statistics (src/utilities/Statistics.py:47-380) and output writers
 # (src/Main.py:588-635), on the GPU accumulator of alfa_ComputeStats
@@ -551,8 +595,19 @@ class Simulation:
             raise ValueError("series lengths differ")
         self._call("alfa_set_series", ptr(U), ptr(V), ptr(T), ptr(S), nrows)
 
-    def step(self, n=1):
-        self._call("alfa_step", int(n))
+    def step(self, n=1, graph=False):
+        """n steps; graph=True replays captured CUDA graphs (alfa_step_graph),
+        on a stream of this simulation's own."""
+        if not graph:
+            self._call("alfa_step", int(n))
+            return self
+        if getattr(self, "_gstream", None) is None:
+            self._gstream = torch.cuda.Stream(self.alfa.device)
+        cur = torch.cuda.current_stream(self.alfa.device)
+        self._gstream.wait_stream(cur)
+        with torch.cuda.stream(self._gstream):
+            self._call("alfa_step_graph", int(n))
+        cur.wait_stream(self._gstream)
         return self
 
     def state(self):

@@ -51,6 +51,8 @@ struct Work {
   double* series_adv = nullptr;  // (nrows, 3, nz) non-dimensional Uadv, Vadv, THadv
   int series_rows = 0;
   std::vector<double> sfc_series;  // host
+  double* d_sfc = nullptr;         // device copy of sfc_series
+  int* d_it;                       // the iteration counter, on the device
   // step temporaries
   double* g[9];
   double* gT[3];
@@ -79,6 +81,35 @@ struct Work {
   double* d_qavg;
 };
 
+// The swappable buffer pointers of Work: a step exchanges the filtered state
+// with its scratch, the MOST planes with their successors and the right-hand
+// sides with the previous ones, so the pointer set alternates with the
+// iteration's parity.  A captured step graph is valid for one pointer set.
+struct StepPtrs {
+  double *u, *v, *w, *TH, *Cx, *Cy, *Cz, *THadv;
+  double *most[6], *most_new[6], *RHS[4], *RHSp[4];
+  static StepPtrs of(const Work& W) {
+    StepPtrs p;
+    p.u = W.u; p.v = W.v; p.w = W.w; p.TH = W.TH;
+    p.Cx = W.Cx; p.Cy = W.Cy; p.Cz = W.Cz; p.THadv = W.THadv;
+    for (int i = 0; i < 6; i++) { p.most[i] = W.most[i]; p.most_new[i] = W.most_new[i]; }
+    for (int i = 0; i < 4; i++) { p.RHS[i] = W.RHS[i]; p.RHSp[i] = W.RHSp[i]; }
+    return p;
+  }
+  void apply(Work& W) const {
+    W.u = u; W.v = v; W.w = w; W.TH = TH;
+    W.Cx = Cx; W.Cy = Cy; W.Cz = Cz; W.THadv = THadv;
+    for (int i = 0; i < 6; i++) { W.most[i] = most[i]; W.most_new[i] = most_new[i]; }
+    for (int i = 0; i < 4; i++) { W.RHS[i] = RHS[i]; W.RHSp[i] = RHSp[i]; }
+  }
+  bool operator==(const StepPtrs& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
+struct StepGraph {
+  cudaGraphExec_t exec = nullptr;
+  StepPtrs before, after;
+};
+
 }  // namespace alfa
 
 struct alfa_ctx {
@@ -86,6 +117,7 @@ struct alfa_ctx {
   Work w;
   void* base = nullptr;
   size_t bytes = 0;
+  StepGraph graphs[4];  // captured steps by (iteration parity, dynamic SGS step)
 };
 
 // ---------------------------------------------------------------------------
@@ -375,6 +407,7 @@ static void carve(alfa_ctx* c, Carver& k) {
   w.prof = k.take<double>(64 * nz + 64);
   w.d_cfl = k.take<double>(4);
   w.d_qavg = k.take<double>(4);
+  w.d_it = k.take<int>(64);
   // engine scratch
   e.T_elems = (size_t)e.mx * e.myh * nz;
   for (int i = 0; i < 4; i++) e.T[i] = k.take<cd>(e.T_elems);
@@ -805,6 +838,9 @@ static int surface_variant(const alfa_config& c) {
 // ---------------------------------------------------------------------------
 // whole step: src/Main.py:156-541 (dry, constant geostrophic wind)
 // ---------------------------------------------------------------------------
+__global__ void k_add_int(int* p, int d) { *p += d; }
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
 static int one_step(alfa_ctx* c) {
   Engine& e = c->e;
   Work& W = c->w;
@@ -813,13 +849,16 @@ static int one_step(alfa_ctx* c) {
   const int nz = e.nz;
   if (it > cf.istep)
     for (int i = 0; i < 4; i++) std::swap(W.RHSp[i], W.RHS[i]);
+  // forcing rows (Main.py:179-188) are selected on the device from the
+  // device iteration counter, so a captured step replays with the current row
   const double *Uadv = W.zero_prof, *Vadv = W.zero_prof, *THadv = W.zero_prof;
+  const int* itp = nullptr;
   if (cf.optAdvection >= 1) {
     if (it - 1 >= W.series_rows) return e.fail("advection series exhausted", ALFA_E_STATE);
-    const double* row = W.series_adv + (size_t)(it - 1) * 3 * nz;
-    Uadv = row;
-    Vadv = row + nz;
-    THadv = row + 2 * nz;
+    Uadv = W.series_adv;
+    Vadv = W.series_adv + nz;
+    THadv = W.series_adv + 2 * nz;
+    itp = W.d_it;
   }
   // filtering (Main.py:193-197): the filtered field replaces the state, so
   // filter into the (not yet used) gradient slot and swap the two N-sized
@@ -843,6 +882,7 @@ static int one_step(alfa_ctx* c) {
     if (it - 1 >= (int)W.sfc_series.size()) return e.fail("surface series exhausted", ALFA_E_STATE);
     sfc = W.sfc_series[it - 1];
   }
+  const double* sfc_dev = (cf.optSurfBC >= 1) ? W.d_sfc : nullptr;
   SurfaceIO io;
   io.u = W.u;
   io.v = W.v;
@@ -856,7 +896,7 @@ static int one_step(alfa_ctx* c) {
   io.q2 = W.q2;
   io.qavg = W.d_qavg;
   io.invOB = W.invOB;
-  surface_flux(e, var, sfc, io);
+  surface_flux(e, var, sfc, io, sfc_dev, W.d_it);
   for (int i = 0; i < 6; i++) std::swap(W.most[i], W.most_new[i]);
   const double* qz_step = (var <= 1) ? W.qz_plane : W.q2;
   // gradients (Main.py:275-290)
@@ -900,8 +940,9 @@ static int one_step(alfa_ctx* c) {
     plane_means(e, f3, 3, bars);
   }
   rhs_momentum(e, W.u, W.v, W.w, W.Ug, W.Vg, W.Cx, W.Cy, W.Cz, W.buoy, W.divt[0], W.divt[1],
-               W.divt[2], Uadv, Vadv, bars, bars + nz, W.RHS[0], W.RHS[1], W.RHS[2]);
-  rhs_scalar(e, W.TH, W.THadv, W.divq, THadv, bars + 2 * nz, W.RHS[3]);
+               W.divt[2], Uadv, Vadv, bars, bars + nz, W.RHS[0], W.RHS[1], W.RHS[2], itp,
+               3LL * nz);
+  rhs_scalar(e, W.TH, W.THadv, W.divq, THadv, bars + 2 * nz, W.RHS[3], itp, 3LL * nz);
   // pressure (Main.py:481-500)
   st = pressure_rc_fn(c, W.u, W.v, W.w, W.RHS[0], W.RHS[1], W.RHS[2], W.RHSp[0], W.RHSp[1],
                       W.RHSp[2], W.divt[2], W.RCr, W.RCi, W.fRzr);
@@ -919,6 +960,7 @@ static int one_step(alfa_ctx* c) {
       cudaMemcpyAsync(W.RHSp[i], W.RHS[i], e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
   // CFL (Main.py:534-540): maxima stay on the device, read by alfa_get_diag
   cfl_max(e, W.u, W.v, W.w, W.d_cfl);
+  ::alfa::note_launch(); k_add_int<<<1, 1, 0, e.stream>>>(W.d_it, 1);
   W.iteration++;
   return check_launch(e, "step");
 }
@@ -932,6 +974,66 @@ static int one_step(alfa_ctx* c) {
   } while (0)
 
 static thread_local std::string g_create_error;
+
+static void release_graphs(alfa_ctx* c) {
+  for (StepGraph& g : c->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+  }
+}
+
+// One step as a CUDA graph.  The step's launches depend on the host only
+// through (a) the buffer pointers, which alternate with the iteration's
+// parity, and (b) whether the dynamic SGS procedure runs; the forcing rows
+// and the surface value are read on the device from the device iteration
+// counter.  So one graph per (parity, dynamic) pair, captured the first time
+// it is needed, replays every later step of that kind.  The bootstrap step
+// (iteration == istep) runs directly.
+static int graph_step(alfa_ctx* c) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  const alfa_config& cf = e.cfg;
+  const int it = W.iteration;
+  if (it == cf.istep) return one_step(c);
+  if (cf.optAdvection >= 1 && it - 1 >= W.series_rows)
+    return e.fail("advection series exhausted", ALFA_E_STATE);
+  if (cf.optSurfBC >= 1 && it - 1 >= (int)W.sfc_series.size())
+    return e.fail("surface series exhausted", ALFA_E_STATE);
+  const bool dyn = (cf.optSgs >= 1 && cf.optSgs <= 4) && (it % cf.dynamicSGS_call_time == 0);
+  StepGraph& g = c->graphs[(it & 1) * 2 + (dyn ? 1 : 0)];
+  const StepPtrs now = StepPtrs::of(W);
+  if (!g.exec || !(g.before == now)) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    if (e.stream == 0) return e.fail("graph capture needs a non-default stream", ALFA_E_STATE);
+    if (cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return e.fail("cudaStreamBeginCapture failed", ALFA_E_CUDA);
+    const int st = one_step(c);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e.stream, &graph);
+    const StepPtrs after = StepPtrs::of(W);
+    now.apply(W);  // nothing ran yet: undo the host side of the captured step
+    W.iteration = it;
+    if (st || ce != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return st ? st : e.fail("step capture failed", ALFA_E_CUDA);
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      g.exec = nullptr;
+      return e.fail("step graph instantiation failed", ALFA_E_CUDA);
+    }
+    g.before = now;
+    g.after = after;
+  }
+  if (cudaGraphLaunch(g.exec, e.stream) != cudaSuccess)
+    return e.fail("step graph launch failed", ALFA_E_CUDA);
+  g.after.apply(W);
+  W.iteration = it + 1;
+  return ALFA_OK;
+}
 
 extern "C" {
 
@@ -967,6 +1069,8 @@ int alfa_create(const alfa_config* cfg, alfa_ctx** out) {
 void alfa_destroy(alfa_ctx* c) {
   if (!c) return;
   if (c->w.series_adv) cudaFree(c->w.series_adv);
+  if (c->w.d_sfc) cudaFree(c->w.d_sfc);
+  release_graphs(c);
   cudaFree(c->base);
   engine_free(c->e);
   delete c;
@@ -1535,6 +1639,7 @@ int alfa_init_state(alfa_ctx* c, const double* u, const double* v, const double*
   ::alfa::note_launch(); k_fill<<<1, 256, 0, e.stream>>>(W.Vg, e.cfg.Vg2 / 1.0, e.nz);
   ::alfa::note_launch(); k_fill<<<1, 256, 0, e.stream>>>(W.zero_prof, 0.0, e.nz);
   W.iteration = e.cfg.istep;
+  ::alfa::note_launch(); k_set_int<<<1, 1, 0, e.stream>>>(W.d_it, W.iteration);
   W.have_state = 1;
   W.CFLmax = 0;
   return check_launch(e, "init_state");
@@ -1566,6 +1671,16 @@ int alfa_set_series(alfa_ctx* c, const double* Uadv, const double* Vadv, const d
     W.series_rows = nrows;
   }
   W.sfc_series.assign(sfc ? sfc : (const double*)nullptr, sfc ? sfc + nrows : (const double*)nullptr);
+  if (W.d_sfc) {
+    cudaFree(W.d_sfc);
+    W.d_sfc = nullptr;
+  }
+  if (sfc && nrows > 0) {
+    if (cudaMalloc(&W.d_sfc, (size_t)nrows * 8) != cudaSuccess)
+      return e.fail("series allocation failed", ALFA_E_CUDA);
+    cudaMemcpy(W.d_sfc, sfc, (size_t)nrows * 8, cudaMemcpyHostToDevice);
+  }
+  release_graphs(c);  // captured steps point at the old series
   return ALFA_OK;
 }
 
@@ -1577,6 +1692,16 @@ int alfa_step(alfa_ctx* c, int nsteps) {
     if (st) return st;
   }
   return ALFA_OK;
+}
+
+int alfa_step_graph(alfa_ctx* c, int nsteps) {
+  CTX_CHECK(c);
+  if (!c->w.have_state) return c->e.fail("alfa_step_graph before alfa_init_state", ALFA_E_STATE);
+  for (int s = 0; s < nsteps; s++) {
+    int st = graph_step(c);
+    if (st) return st;
+  }
+  return check_launch(c->e, "step_graph");
 }
 
 int alfa_get_state(alfa_ctx* c, double* u, double* v, double* w, double* TH, double* p) {
@@ -1688,6 +1813,7 @@ static int checkpoint_copy(alfa_ctx* c, double* buf, bool save) {
     W.iteration = (int)tail[0];
     W.CFLmax = tail[1];
     W.have_state = 1;
+    ::alfa::note_launch(); k_set_int<<<1, 1, 0, e.stream>>>(W.d_it, W.iteration);
   }
   return ALFA_OK;
 }
@@ -1703,6 +1829,186 @@ int alfa_load_checkpoint(alfa_ctx* c, const double* src) {
   CTX_CHECK(c);
   NN(src);
   return checkpoint_copy(c, const_cast<double*>(src), false);
+}
+
+// ---------------------------------------------------------------------------
+// ensemble: independent contexts stepped together, one graph per step
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct alfa_ensemble {
+  std::vector<alfa_ctx*> m;
+  std::vector<cudaStream_t> own;  // one stream per member
+  std::vector<cudaEvent_t> done;  // member i finished its part of the graph
+  cudaStream_t master = nullptr;
+  cudaEvent_t start = nullptr;
+  struct G {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<StepPtrs> before, after;
+  } graphs[4];
+  std::string err;
+};
+
+static void ens_release(alfa_ensemble* E) {
+  for (auto& g : E->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+  }
+}
+
+// one step of every member inside one captured graph (members at the same
+// iteration, same istep and dynamic interval); returns nonzero to ask the
+// caller for the member-by-member path
+static int ens_graph_step(alfa_ensemble* E) {
+  for (size_t i = 0; i < E->m.size(); i++) E->m[i]->e.stream = E->own[i];
+  alfa_ctx* c0 = E->m[0];
+  const int it = c0->w.iteration;
+  const alfa_config& cf0 = c0->e.cfg;
+  for (alfa_ctx* c : E->m) {
+    const alfa_config& cf = c->e.cfg;
+    if (c->w.iteration != it || cf.istep != cf0.istep ||
+        cf.dynamicSGS_call_time != cf0.dynamicSGS_call_time ||
+        ((cf.optSgs >= 1 && cf.optSgs <= 4) != (cf0.optSgs >= 1 && cf0.optSgs <= 4)))
+      return 1;
+    if (cf.optAdvection >= 1 && it - 1 >= c->w.series_rows) return 1;
+    if (cf.optSurfBC >= 1 && it - 1 >= (int)c->w.sfc_series.size()) return 1;
+  }
+  if (it == cf0.istep) return 1;
+  const bool dyn = (cf0.optSgs >= 1 && cf0.optSgs <= 4) && (it % cf0.dynamicSGS_call_time == 0);
+  auto& g = E->graphs[(it & 1) * 2 + (dyn ? 1 : 0)];
+  const size_t n = E->m.size();
+  std::vector<StepPtrs> now(n);
+  for (size_t i = 0; i < n; i++) now[i] = StepPtrs::of(E->m[i]->w);
+  bool same = g.exec && g.before.size() == n;
+  for (size_t i = 0; same && i < n; i++) same = g.before[i] == now[i];
+  if (!same) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    if (cudaStreamBeginCapture(E->master, cudaStreamCaptureModeRelaxed) != cudaSuccess) return 1;
+    cudaEventRecord(E->start, E->master);
+    int st = 0;
+    std::vector<StepPtrs> after(n);
+    for (size_t i = 0; i < n; i++) {
+      alfa_ctx* c = E->m[i];
+      cudaStreamWaitEvent(E->own[i], E->start, 0);
+      if (!st) st = one_step(c);
+      after[i] = StepPtrs::of(c->w);
+      cudaEventRecord(E->done[i], E->own[i]);
+      cudaStreamWaitEvent(E->master, E->done[i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(E->master, &graph);
+    for (size_t i = 0; i < n; i++) {  // nothing ran yet: undo the host side
+      now[i].apply(E->m[i]->w);
+      E->m[i]->w.iteration = it;
+    }
+    if (st || ce != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      E->err = st ? E->m[0]->e.err : "ensemble capture failed";
+      return st ? st : ALFA_E_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      g.exec = nullptr;
+      E->err = "ensemble graph instantiation failed";
+      return ALFA_E_CUDA;
+    }
+    g.before = now;
+    g.after = after;
+  }
+  if (cudaGraphLaunch(g.exec, E->master) != cudaSuccess) {
+    E->err = "ensemble graph launch failed";
+    return ALFA_E_CUDA;
+  }
+  for (size_t i = 0; i < n; i++) {
+    g.after[i].apply(E->m[i]->w);
+    E->m[i]->w.iteration = it + 1;
+  }
+  return ALFA_OK;
+}
+
+extern "C" {
+
+int alfa_ensemble_create(alfa_ctx* const* members, int n, alfa_ensemble** out) {
+  if (!members || n < 1 || !out) return ALFA_E_SHAPE;
+  alfa_ensemble* E = new alfa_ensemble();
+  for (int i = 0; i < n; i++) {
+    if (!members[i] || !members[i]->w.have_state) {
+      delete E;
+      return ALFA_E_STATE;
+    }
+    E->m.push_back(members[i]);
+  }
+  bool ok = cudaStreamCreateWithFlags(&E->master, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&E->start, cudaEventDisableTiming) == cudaSuccess;
+  E->own.resize(n, nullptr);
+  E->done.resize(n, nullptr);
+  for (int i = 0; ok && i < n; i++) {
+    ok = cudaStreamCreateWithFlags(&E->own[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&E->done[i], cudaEventDisableTiming) == cudaSuccess;
+    if (ok) {
+      release_graphs(members[i]);
+      members[i]->e.stream = E->own[i];
+    }
+  }
+  if (!ok) {
+    alfa_ensemble_destroy(E);
+    return ALFA_E_CUDA;
+  }
+  *out = E;
+  return ALFA_OK;
+}
+
+int alfa_ensemble_step(alfa_ensemble* E, int nsteps) {
+  if (!E) return ALFA_E_STATE;
+  for (int s = 0; s < nsteps; s++) {
+    int st = ens_graph_step(E);
+    if (st == ALFA_OK) continue;
+    if (st < 0) return st;
+    // member by member (bootstrap step, or members not in lockstep); the
+    // master waits for every member so the next graph starts after them
+    cudaEventRecord(E->start, E->master);
+    for (size_t i = 0; i < E->m.size(); i++) {
+      cudaStreamWaitEvent(E->own[i], E->start, 0);
+      const int r = graph_step(E->m[i]);
+      if (r) {
+        E->err = E->m[i]->e.err;
+        return r;
+      }
+      cudaEventRecord(E->done[i], E->own[i]);
+      cudaStreamWaitEvent(E->master, E->done[i], 0);
+    }
+  }
+  return ALFA_OK;
+}
+
+int alfa_ensemble_sync(alfa_ensemble* E) {
+  if (!E) return ALFA_E_STATE;
+  return cudaStreamSynchronize(E->master) == cudaSuccess ? ALFA_OK : ALFA_E_CUDA;
+}
+
+const char* alfa_ensemble_error(const alfa_ensemble* E) { return E ? E->err.c_str() : ""; }
+
+void alfa_ensemble_destroy(alfa_ensemble* E) {
+  if (!E) return;
+  if (E->master) cudaStreamSynchronize(E->master);
+  ens_release(E);
+  for (size_t i = 0; i < E->own.size(); i++) {
+    if (E->own[i]) {
+      cudaStreamSynchronize(E->own[i]);
+      if (i < E->m.size() && E->m[i]->e.stream == E->own[i]) {
+        release_graphs(E->m[i]);
+        E->m[i]->e.stream = 0;
+      }
+      cudaStreamDestroy(E->own[i]);
+    }
+    if (E->done[i]) cudaEventDestroy(E->done[i]);
+  }
+  if (E->start) cudaEventDestroy(E->start);
+  if (E->master) cudaStreamDestroy(E->master);
+  delete E;
 }
 
 }  // extern "C"

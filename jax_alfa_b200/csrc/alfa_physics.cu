@@ -97,6 +97,8 @@ struct SurfConst {
   double Ugal, T0, vonk_g, log_m, log_h, half_dz, z0m_s, zT_s;
   int variant;
   double sfc_val, qz_const;
+  const double* sfc_series;  // non-null: sfc_val is sfc_series[*itp - 1]
+  const int* itp;
   size_t H;
   int nz;
 };
@@ -148,6 +150,7 @@ struct SurfPtr {
 
 __global__ void k_surface(SurfConst c, SurfPtr p) {
   __shared__ double sh[1024];
+  if (c.sfc_series) c.sfc_val = c.sfc_series[*c.itp - 1];
   const size_t H = c.H;
   const int nz = c.nz;
   const bool hom = (c.variant == 0 || c.variant == 2 || c.variant == 4);
@@ -225,7 +228,8 @@ __global__ void k_surface(SurfConst c, SurfPtr p) {
   }
 }
 
-int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io) {
+int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io,
+                 const double* sfc_series, const int* itp) {
   SurfConst c;
   c.Ugal = e.cfg.Ugal;
   c.T0 = e.T0_nondim;
@@ -238,6 +242,8 @@ int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io) {
   c.zT_s = zref / e.z_scale;
   c.variant = variant;
   c.sfc_val = sfc_val;
+  c.sfc_series = sfc_series;
+  c.itp = itp;
   c.qz_const = e.qz_sfc_const;
   c.H = e.H();
   c.nz = e.nz;
@@ -1247,6 +1253,8 @@ struct RhsM {
   double *Ru, *Rv, *Rw;
   double f, Ugal;
   int adv, damp;
+  const int* itp;   // non-null: the forcing profiles are row (*itp - 1) of a series
+  long long rs;     // row stride of that series
 };
 
 __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
@@ -1256,8 +1264,9 @@ __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
     double rv = -a.Cy[i] - a.dy[i] + a.f * (a.Ug[z] - a.Ugal - a.u[i]);
     double rw = -a.Cz[i] - a.dz[i] + a.b[i];
     if (a.adv) {
-      ru = ru + a.Uadv[z];
-      rv = rv + a.Vadv[z];
+      const size_t row = a.itp ? (size_t)(*a.itp - 1) * a.rs : 0;
+      ru = ru + a.Uadv[row + z];
+      rv = rv + a.Vadv[row + z];
     }
     if (a.damp) {
       ru = ru - a.rds[z] * (a.u[i] - a.ubar[z]);
@@ -1274,30 +1283,34 @@ void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
                   const double* Ug, const double* Vg, const double* Cx, const double* Cy,
                   const double* Cz, const double* b, const double* dx, const double* dy,
                   const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
-                  const double* vbar, double* Ru, double* Rv, double* Rw) {
+                  const double* vbar, double* Ru, double* Rv, double* Rw, const int* itp,
+                  long long rs) {
   RhsM a{u, v, w, Ug, Vg, Cx, Cy, Cz, b, dx, dy, dz, Uadv, Vadv, ubar, vbar, e.d_rd, e.d_rd_stag,
-         Ru, Rv, Rw, e.f_nondim, e.cfg.Ugal, e.cfg.optAdvection >= 1, e.cfg.optDamping == 1};
+         Ru, Rv, Rw, e.f_nondim, e.cfg.Ugal, e.cfg.optAdvection >= 1, e.cfg.optDamping == 1, itp,
+         rs};
   ::alfa::note_launch(); k_rhs_m<<<nblocks(e.N()), TPB, 0, e.stream>>>(a, e.N(), e.nz);
 }
 
 __global__ void k_rhs_s(const double* __restrict__ TH, const double* __restrict__ adv,
                         const double* __restrict__ dq, const double* __restrict__ THadv,
                         const double* __restrict__ bar, const double* __restrict__ rds, double* R,
-                        size_t n, int nz, int doadv, int damp) {
+                        size_t n, int nz, int doadv, int damp, const int* itp, long long rs) {
+  const size_t row = (doadv && itp) ? (size_t)(*itp - 1) * rs : 0;
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     double r = -adv[i] - dq[i];
-    if (doadv) r = r + THadv[z];
+    if (doadv) r = r + THadv[row + z];
     if (damp) r = r - rds[z] * (TH[i] - bar[z]);
     R[i] = r;
   }
 }
 
 void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
-                const double* THadv, const double* THbar, double* R) {
+                const double* THadv, const double* THbar, double* R, const int* itp,
+                long long rs) {
   ::alfa::note_launch(); k_rhs_s<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, adv, divq, THadv, THbar, e.d_rd_stag, R,
                                                  e.N(), e.nz, e.cfg.optAdvection >= 1,
-                                                 e.cfg.optDamping == 1);
+                                                 e.cfg.optDamping == 1, itp, rs);
 }
 
 // ---------------------------------------------------------------------------

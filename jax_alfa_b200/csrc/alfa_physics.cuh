@@ -23,7 +23,10 @@ struct SurfaceIO {
   double* most_out[6];
 };
 // variant: 0 HomConst, 1 HetConst, 2 HomVary, 3 HetVary, 4 HomPresT, 5 HetPresT
-int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io);
+// sfc_series / itp: when given, the surface value is sfc_series[*itp - 1]
+// (read on the device, so a captured step replays with the current row)
+int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io,
+                 const double* sfc_series = nullptr, const int* itp = nullptr);
 
 // ---- z derivatives (Derivatives.py) --------------------------------------
 void derivz_M(Engine& e, const double* u, const double* v, const double* w, const double* ustar,
@@ -108,9 +111,13 @@ void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
                   const double* Ug, const double* Vg, const double* Cx, const double* Cy,
                   const double* Cz, const double* b, const double* dx, const double* dy,
                   const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
-                  const double* vbar, double* Ru, double* Rv, double* Rw);
+                  const double* vbar, double* Ru, double* Rv, double* Rw,
+                  const int* itp = nullptr, long long rs = 0);
+// itp / rs: when given, the forcing profiles are row (*itp - 1) of a series
+// with row stride rs (read on the device)
 void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
-                const double* THadv, const double* THbar, double* R);
+                const double* THadv, const double* THbar, double* R, const int* itp = nullptr,
+                long long rs = 0);
 void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const cd* fbot,
                  const cd* ftop, double* RCr, double* RCi, double* fRz_real);
 void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double* fRz_real,
