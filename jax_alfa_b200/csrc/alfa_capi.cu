@@ -108,6 +108,7 @@ struct StepPtrs {
 struct StepGraph {
   cudaGraphExec_t exec = nullptr;
   StepPtrs before, after;
+  unsigned long long kernels = 0;  // kernel launches the graph replays
 };
 
 }  // namespace alfa
@@ -1008,7 +1009,10 @@ static int graph_step(alfa_ctx* c) {
     if (e.stream == 0) return e.fail("graph capture needs a non-default stream", ALFA_E_STATE);
     if (cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return e.fail("cudaStreamBeginCapture failed", ALFA_E_CUDA);
+    const unsigned long long l0 = g_launches.load();
     const int st = one_step(c);
+    // capturing counted the step's kernels once; the launch below runs them
+    g.kernels = g_launches.load() - l0;
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(e.stream, &graph);
     const StepPtrs after = StepPtrs::of(W);
@@ -1027,6 +1031,8 @@ static int graph_step(alfa_ctx* c) {
     }
     g.before = now;
     g.after = after;
+  } else {
+    g_launches.fetch_add(g.kernels, std::memory_order_relaxed);  // replayed kernels
   }
   if (cudaGraphLaunch(g.exec, e.stream) != cudaSuccess)
     return e.fail("step graph launch failed", ALFA_E_CUDA);
@@ -1845,6 +1851,7 @@ struct alfa_ensemble {
   struct G {
     cudaGraphExec_t exec = nullptr;
     std::vector<StepPtrs> before, after;
+    unsigned long long kernels = 0;
   } graphs[4];
   std::string err;
 };
@@ -1887,6 +1894,7 @@ static int ens_graph_step(alfa_ensemble* E) {
     if (cudaStreamBeginCapture(E->master, cudaStreamCaptureModeRelaxed) != cudaSuccess) return 1;
     cudaEventRecord(E->start, E->master);
     int st = 0;
+    const unsigned long long l0 = g_launches.load();
     std::vector<StepPtrs> after(n);
     for (size_t i = 0; i < n; i++) {
       alfa_ctx* c = E->m[i];
@@ -1917,6 +1925,9 @@ static int ens_graph_step(alfa_ensemble* E) {
     }
     g.before = now;
     g.after = after;
+    g.kernels = g_launches.load() - l0;
+  } else {
+    g_launches.fetch_add(g.kernels, std::memory_order_relaxed);
   }
   if (cudaGraphLaunch(g.exec, E->master) != cudaSuccess) {
     E->err = "ensemble graph launch failed";
