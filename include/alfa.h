@@ -280,6 +280,48 @@ int alfa_ensemble_sync(alfa_ensemble*);
 const char* alfa_ensemble_error(const alfa_ensemble*);
 void alfa_ensemble_destroy(alfa_ensemble*);
 
+/* ---- learned SGS coefficient (no counterpart in the reference) ----------
+ * A 10 -> 64 -> 64 -> 2 network (tanh) attached to a context predicts Cs^2
+ * (and beta) from local strain-rate and scalar-gradient features: log of
+ * Delta^2 |S|, the six S_ij / |S|, dtheta/dz, z / Delta and the gradient
+ * Richardson number Ri as Ri / (1 + |Ri|).  Hand-written kernels train it (FP32 master weights,
+ * Adam) on samples of the dynamic procedure's Cs^2 and beta, and infer it
+ * with BF16 weights and FP32 accumulation.
+ * collect: npoints random samples of the context's last step, which must
+ *   have run the dynamic procedure, into a ring of `capacity` samples.
+ * train: epochs over the collected samples (shuffled), batch, learning rate;
+ *   loss_out = last epoch's mean squared error in normalised units.
+ * loss_grad: gradient of that loss for n given samples (device X: n x 10,
+ *   T: n x 2, norm: 24 floats = means of the 10 features and 2 targets, then
+ *   their standard deviations) with the FP32 weights, into grad
+ *   (ALFA_MLP_NPARAM floats) and loss (one float).
+ * params: W1 (64 x 10), b1, W2 (64 x 64), b2, W3 (2 x 64), b3, FP32.
+ * step_learned: steps whose Cs^2 comes from the network (static stresses and
+ *   fluxes with it); every judge_every-th step runs the dynamic procedure
+ *   instead and compares the network's plane-averaged Cs^2 on that state
+ *   with the procedure's (relative L2 difference of the two profiles):
+ *   a drift above tol reverts to the dynamic procedure for good; otherwise
+ *   refresh_points samples of that step are collected and the network trains
+ *   refresh_epochs more epochs (0, 0: no refresh). */
+#define ALFA_MLP_NPARAM 4994
+typedef struct alfa_mlp alfa_mlp;
+typedef struct {
+  int steps, learned_steps, judged, reverted, reverted_at;
+  double last_drift, max_drift;
+} alfa_mlp_report;
+int alfa_mlp_create(alfa_ctx*, int capacity, unsigned long long seed, alfa_mlp** out);
+void alfa_mlp_destroy(alfa_mlp*);
+int alfa_mlp_collect(alfa_mlp*, int npoints);
+int alfa_mlp_train(alfa_mlp*, int epochs, int batch, double lr, double* loss_out /* host */);
+int alfa_mlp_loss_grad(alfa_mlp*, const float* X, const float* T, const float* norm, int n,
+                       float* grad, float* loss);
+int alfa_mlp_get_params(alfa_mlp*, float* params, float* norm);
+int alfa_mlp_set_params(alfa_mlp*, const float* params, const float* norm);
+int alfa_mlp_features(alfa_mlp*, float* X /* N x 10, from the context's last step */);
+int alfa_mlp_infer(alfa_mlp*, double* Cs2, double* beta /* may be NULL */);
+int alfa_step_learned(alfa_mlp*, int nsteps, int judge_every, double tol, int refresh_points,
+                      int refresh_epochs, alfa_mlp_report* report /* host, accumulated */);
+
 /* ---- checkpoint / restart (no counterpart in the reference) --------------
  * Everything alfa_step carries from one iteration to the next: u v w TH p,
  * the previous right-hand sides, the 3-D SGS coefficients, the MOST planes,

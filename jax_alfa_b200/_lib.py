@@ -114,6 +114,11 @@ SIGNATURES = {
     "alfa_step_graph": [I],
 }
 
+class AlfaMlpReport(ctypes.Structure):
+    _fields_ = [("steps", I), ("learned_steps", I), ("judged", I), ("reverted", I),
+                ("reverted_at", I), ("last_drift", D), ("max_drift", D)]
+
+
 _lib = None
 
 
@@ -162,6 +167,22 @@ def load():
     lib.alfa_ensemble_error.restype = ctypes.c_char_p
     lib.alfa_ensemble_destroy.argtypes = [c_void_p]
     lib.alfa_ensemble_destroy.restype = None
+    M = c_void_p
+    for name, args in {
+            "alfa_mlp_create": [CTX, I, ctypes.c_ulonglong, ctypes.POINTER(c_void_p)],
+            "alfa_mlp_collect": [M, I],
+            "alfa_mlp_train": [M, I, I, D, c_double_p],
+            "alfa_mlp_loss_grad": [M, P, P, P, I, P, P],
+            "alfa_mlp_get_params": [M, P, P],
+            "alfa_mlp_set_params": [M, P, P],
+            "alfa_mlp_features": [M, P],
+            "alfa_mlp_infer": [M, P, P],
+            "alfa_step_learned": [M, I, I, D, I, I, ctypes.POINTER(AlfaMlpReport)]}.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = I
+    lib.alfa_mlp_destroy.argtypes = [M]
+    lib.alfa_mlp_destroy.restype = None
     for name, args in SIGNATURES.items():
         f = getattr(lib, name)
         f.argtypes = [CTX] + args

@@ -464,6 +464,113 @@ class Alfa:
         return out
 
 
+MLP_NPARAM = 4994
+
+
+class Learned:
+    """The learned SGS coefficient network attached to a Simulation
+    (alfa_mlp_*): collect samples of the dynamic procedure, train, infer,
+    and step with the network judged by the procedure."""
+
+    def __init__(self, sim, capacity=200_000, seed=0):
+        self.sim = sim
+        a = sim.alfa
+        self.lib = a.lib
+        self._sync()
+        h = ctypes.c_void_p()
+        rc = self.lib.alfa_mlp_create(a.ctx, int(capacity), int(seed), ctypes.byref(h))
+        if rc != 0:
+            raise _lib.AlfaError(f"alfa_mlp_create failed ({rc}): "
+                                 f"{self.lib.alfa_last_error(a.ctx).decode()}")
+        self.h = h
+        self.report = _lib.AlfaMlpReport()
+
+    def _sync(self):
+        a = self.sim.alfa
+        a.lib.alfa_set_stream(a.ctx, ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream))
+
+    def _chk(self, rc, what):
+        if rc != 0:
+            a = self.sim.alfa
+            raise _lib.AlfaError(f"{what} failed ({rc}): {self.lib.alfa_last_error(a.ctx).decode()}")
+
+    def collect(self, npoints):
+        self._sync()
+        self._chk(self.lib.alfa_mlp_collect(self.h, int(npoints)), "alfa_mlp_collect")
+
+    def train(self, epochs, batch=1024, lr=1e-3):
+        self._sync()
+        loss = ctypes.c_double()
+        self._chk(self.lib.alfa_mlp_train(self.h, int(epochs), int(batch), float(lr),
+                                          ctypes.byref(loss)), "alfa_mlp_train")
+        return loss.value
+
+    def loss_grad(self, X, T, norm):
+        a = self.sim.alfa
+        X, T, norm = (torch.as_tensor(v, dtype=torch.float32, device=a.device).contiguous()
+                      for v in (X, T, norm))
+        g = torch.empty(MLP_NPARAM, dtype=torch.float32, device=a.device)
+        l = torch.empty(1, dtype=torch.float32, device=a.device)
+        self._sync()
+        self._chk(self.lib.alfa_mlp_loss_grad(self.h, X.data_ptr(), T.data_ptr(), norm.data_ptr(),
+                                              int(X.shape[0]), g.data_ptr(), l.data_ptr()),
+                  "alfa_mlp_loss_grad")
+        return float(l.item()), g.cpu().numpy()
+
+    def params(self):
+        a = self.sim.alfa
+        P = torch.empty(MLP_NPARAM, dtype=torch.float32, device=a.device)
+        nm = torch.empty(24, dtype=torch.float32, device=a.device)
+        self._sync()
+        self._chk(self.lib.alfa_mlp_get_params(self.h, P.data_ptr(), nm.data_ptr()),
+                  "alfa_mlp_get_params")
+        return P.cpu().numpy(), nm.cpu().numpy()
+
+    def set_params(self, P, norm=None):
+        a = self.sim.alfa
+        P = torch.as_tensor(P, dtype=torch.float32, device=a.device).contiguous()
+        nm = None if norm is None else torch.as_tensor(norm, dtype=torch.float32,
+                                                       device=a.device).contiguous()
+        self._sync()
+        self._chk(self.lib.alfa_mlp_set_params(self.h, P.data_ptr(),
+                                               None if nm is None else nm.data_ptr()),
+                  "alfa_mlp_set_params")
+        torch.cuda.current_stream(a.device).synchronize()
+
+    def features(self):
+        a = self.sim.alfa
+        X = torch.empty((a.nx, a.ny, a.nz, 10), dtype=torch.float32, device=a.device)
+        self._sync()
+        self._chk(self.lib.alfa_mlp_features(self.h, X.data_ptr()), "alfa_mlp_features")
+        return X
+
+    def infer(self):
+        a = self.sim.alfa
+        c = a._new(a.N)
+        b = a._new(a.N)
+        self._sync()
+        self._chk(self.lib.alfa_mlp_infer(self.h, c.data_ptr(), b.data_ptr()), "alfa_mlp_infer")
+        return c, b
+
+    def step(self, n, judge_every=20, tol=0.05, refresh_points=0, refresh_epochs=0):
+        self._sync()
+        self._chk(self.lib.alfa_step_learned(self.h, int(n), int(judge_every), float(tol),
+                                             int(refresh_points), int(refresh_epochs),
+                                             ctypes.byref(self.report)), "alfa_step_learned")
+        return {k: getattr(self.report, k) for k, _ in self.report._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.alfa_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Ensemble:
     """Independent simulations (any grid sizes) advanced together: every step
     of all members is one CUDA graph launch (alfa_ensemble_*)."""

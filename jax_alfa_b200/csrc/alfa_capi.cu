@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "alfa_internal.cuh"
+#include "alfa_mlp.cuh"
 #include "alfa_physics.cuh"
 
 using namespace alfa;
@@ -76,6 +77,7 @@ struct Work {
   double* prof;  // small profiles scratch
   int iteration = 1;
   int have_state = 0;
+  int last_dyn = 0;  // the last step ran the dynamic procedure
   double CFL = 0, CFLmax = 0;
   double* d_cfl;  // 3 maxima
   double* d_qavg;
@@ -119,6 +121,20 @@ struct alfa_ctx {
   void* base = nullptr;
   size_t bytes = 0;
   StepGraph graphs[4];  // captured steps by (iteration parity, dynamic SGS step)
+  struct alfa_mlp* mlp = nullptr;  // attached learned-coefficient network
+};
+
+struct alfa_mlp {
+  alfa_ctx* c = nullptr;
+  int cap = 0, count = 0, offset = 0, adam_t = 0;
+  unsigned long long seed = 0, draws = 0;
+  float *X = nullptr, *T = nullptr, *norm = nullptr, *P = nullptr, *G = nullptr, *M = nullptr,
+        *V = nullptr, *loss = nullptr;
+  int* perm = nullptr;
+  __nv_bfloat16* Pb = nullptr;
+  double* scratch = nullptr;  // N: the network's Cs^2 on a judge step
+  double* means = nullptr;    // 2 nz plane means
+  int trained = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -842,7 +858,13 @@ static int surface_variant(const alfa_config& c) {
 __global__ void k_add_int(int* p, int d) { *p += d; }
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
-static int one_step(alfa_ctx* c) {
+// sgs_mode: 0 the reference's rule (dynamic on the call interval), 1 learned
+// (the attached network's Cs^2 with the static stresses), 2 dynamic
+static int one_step(alfa_ctx* c, int sgs_mode = 0);
+
+static void learned_cs2(alfa_ctx* c, double* Cs2_out);
+
+static int one_step(alfa_ctx* c, int sgs_mode) {
   Engine& e = c->e;
   Work& W = c->w;
   const alfa_config& cf = e.cfg;
@@ -910,8 +932,12 @@ static int one_step(alfa_ctx* c) {
   buoyancy(e, W.TH, cf.optBuoyancy == 0 ? 0 : 1, W.buoy);
   // SGS (Main.py:333-455)
   const double* g9[9] = {W.g[0], W.g[1], W.g[2], W.g[3], W.g[4], W.g[5], W.g[6], W.g[7], W.g[8]};
-  const bool dyn = (cf.optSgs >= 1 && cf.optSgs <= 4) &&
-                   (it == cf.istep || it % cf.dynamicSGS_call_time == 0);
+  bool dyn = (cf.optSgs >= 1 && cf.optSgs <= 4) &&
+             (it == cf.istep || it % cf.dynamicSGS_call_time == 0);
+  if (sgs_mode == 1) dyn = false;
+  if (sgs_mode == 2) dyn = true;
+  W.last_dyn = dyn ? 1 : 0;
+  if (sgs_mode == 1) learned_cs2(c, W.Cs2);  // the network replaces the procedure
   int st;
   if (dyn) {
     double* mom[25];
@@ -1074,6 +1100,7 @@ int alfa_create(const alfa_config* cfg, alfa_ctx** out) {
 
 void alfa_destroy(alfa_ctx* c) {
   if (!c) return;
+  if (c->mlp) c->mlp->c = nullptr;  // the network outlives its context only as memory
   if (c->w.series_adv) cudaFree(c->w.series_adv);
   if (c->w.d_sfc) cudaFree(c->w.d_sfc);
   release_graphs(c);
@@ -2020,6 +2047,248 @@ void alfa_ensemble_destroy(alfa_ensemble* E) {
   if (E->start) cudaEventDestroy(E->start);
   if (E->master) cudaStreamDestroy(E->master);
   delete E;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// learned SGS coefficient (alfa_mlp.cu): data collection, training, the
+// learned step with the dynamic procedure as periodic judge
+// ---------------------------------------------------------------------------
+
+static MlpFeatIn feat_in(alfa_ctx* c) {
+  Engine& e = c->e;
+  Work& W = c->w;
+  MlpFeatIn a;
+  for (int i = 0; i < 9; i++) a.g[i] = W.g[i];
+  a.dTHdz = W.gT[2];
+  a.L = e.L;
+  a.dz = e.dz;
+  a.g_over_T0 = e.g_nondim / e.T0_nondim;
+  a.nz = e.nz;
+  return a;
+}
+
+static void learned_cs2(alfa_ctx* c, double* Cs2_out) {
+  alfa_mlp* m = c->mlp;
+  mlp_infer(c->e.stream, c->e.sms, feat_in(c), m->Pb, m->norm, c->e.N(), Cs2_out, nullptr);
+}
+
+extern "C" {
+
+void alfa_mlp_destroy(alfa_mlp* m) {
+  if (!m) return;
+  if (m->c && m->c->mlp == m) m->c->mlp = nullptr;
+  for (void* p : {(void*)m->X, (void*)m->T, (void*)m->norm, (void*)m->P, (void*)m->G,
+                  (void*)m->M, (void*)m->V, (void*)m->loss, (void*)m->perm, (void*)m->Pb,
+                  (void*)m->scratch, (void*)m->means})
+    if (p) cudaFree(p);
+  delete m;
+}
+
+int alfa_mlp_create(alfa_ctx* c, int capacity, unsigned long long seed, alfa_mlp** out) {
+  CTX_CHECK(c);
+  if (!out || capacity < 64) return c->e.fail("mlp_create: bad arguments", ALFA_E_SHAPE);
+  alfa_mlp* m = new alfa_mlp();
+  m->c = c;
+  m->cap = capacity;
+  m->seed = seed;
+  const size_t N = c->e.N();
+  bool ok = true;
+  auto al = [&](void** p, size_t bytes) {
+    if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
+  };
+  al((void**)&m->X, (size_t)capacity * MLP_IN * 4);
+  al((void**)&m->T, (size_t)capacity * 2 * 4);
+  al((void**)&m->norm, 2 * (MLP_IN + 2) * 4);
+  al((void**)&m->P, MLP_NPARAM * 4);
+  al((void**)&m->G, MLP_NPARAM * 4);
+  al((void**)&m->M, MLP_NPARAM * 4);
+  al((void**)&m->V, MLP_NPARAM * 4);
+  al((void**)&m->loss, 16);
+  al((void**)&m->perm, (size_t)capacity * 4);
+  al((void**)&m->Pb, MLP_NPARAM * 2);
+  al((void**)&m->scratch, N * 8);
+  al((void**)&m->means, (size_t)2 * c->e.nz * 8);
+  if (!ok) {
+    alfa_mlp_destroy(m);
+    return c->e.fail("mlp_create: device allocation failed", ALFA_E_CUDA);
+  }
+  // Glorot-uniform weights, zero biases (host RNG from the seed)
+  std::vector<float> p(MLP_NPARAM, 0.0f);
+  unsigned long long x = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto uni = [&]() {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+  };
+  auto fill = [&](int off, int rows, int cols) {
+    const double a = std::sqrt(6.0 / (rows + cols));
+    for (int q = 0; q < rows * cols; q++) p[off + q] = (float)((2.0 * uni() - 1.0) * a);
+  };
+  const int OW1 = 0, OB1 = MLP_H * MLP_IN, OW2 = OB1 + MLP_H, OB2 = OW2 + MLP_H * MLP_H,
+            OW3 = OB2 + MLP_H;
+  fill(OW1, MLP_H, MLP_IN);
+  fill(OW2, MLP_H, MLP_H);
+  fill(OW3, 2, MLP_H);
+  std::vector<float> nm(2 * (MLP_IN + 2), 0.0f);
+  for (int q = MLP_IN + 2; q < 2 * (MLP_IN + 2); q++) nm[q] = 1.0f;
+  cudaMemcpy(m->P, p.data(), MLP_NPARAM * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(m->norm, nm.data(), nm.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemset(m->G, 0, MLP_NPARAM * 4);
+  cudaMemset(m->M, 0, MLP_NPARAM * 4);
+  cudaMemset(m->V, 0, MLP_NPARAM * 4);
+  mlp_to_bf16(c->e.stream, m->P, m->Pb);
+  c->mlp = m;
+  *out = m;
+  return check_launch(c->e, "mlp_create");
+}
+
+int alfa_mlp_collect(alfa_mlp* m, int npoints) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  alfa_ctx* c = m->c;
+  if (!c->w.last_dyn)
+    return c->e.fail("mlp_collect: the last step did not run the dynamic procedure", ALFA_E_STATE);
+  if (npoints < 1 || npoints > m->cap) return c->e.fail("mlp_collect: bad count", ALFA_E_SHAPE);
+  const int nz = c->e.nz;
+  mlp_sample(c->e.stream, feat_in(c), c->w.Cs2, c->w.prof + 20 * nz, c->e.N(),
+             m->seed + (++m->draws), npoints, m->X, m->T, m->offset, m->cap);
+  m->offset = (m->offset + npoints) % m->cap;
+  m->count = std::min(m->cap, m->count + npoints);
+  return check_launch(c->e, "mlp_collect");
+}
+
+int alfa_mlp_train(alfa_mlp* m, int epochs, int batch, double lr, double* loss_out) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  alfa_ctx* c = m->c;
+  Engine& e = c->e;
+  if (m->count < batch || batch < 1 || epochs < 1)
+    return e.fail("mlp_train: too few samples for one batch", ALFA_E_SHAPE);
+  if (!m->trained) mlp_norm(e.stream, m->X, m->T, m->count, m->norm);
+  m->trained = 1;
+  std::vector<int> perm(m->count);
+  unsigned long long x = m->seed ^ 0x5DEECE66Dull;
+  double last = 0.0;
+  for (int ep = 0; ep < epochs; ep++) {
+    for (int q = 0; q < m->count; q++) perm[q] = q;
+    for (int q = m->count - 1; q > 0; q--) {  // Fisher-Yates
+      x = x * 6364136223846793005ull + 1442695040888963407ull;
+      const int r = (int)((x >> 33) % (unsigned long long)(q + 1));
+      std::swap(perm[q], perm[r]);
+    }
+    cudaMemcpyAsync(m->perm, perm.data(), (size_t)m->count * 4, cudaMemcpyHostToDevice, e.stream);
+    cudaMemsetAsync(m->loss, 0, 4, e.stream);
+    int nb = 0;
+    for (int s0 = 0; s0 + batch <= m->count; s0 += batch, nb++) {
+      mlp_grad(e.stream, m->P, m->X, m->T, m->perm, s0, batch, m->count, m->norm, m->G, m->loss);
+      mlp_adam(e.stream, m->P, m->G, m->M, m->V, m->Pb, (float)lr, ++m->adam_t);
+    }
+    float l = 0.0f;
+    cudaMemcpyAsync(&l, m->loss, 4, cudaMemcpyDeviceToHost, e.stream);
+    if (cudaStreamSynchronize(e.stream) != cudaSuccess) return e.fail("mlp_train failed", ALFA_E_CUDA);
+    last = nb ? l / nb : 0.0;
+  }
+  if (loss_out) *loss_out = last;
+  return check_launch(e, "mlp_train");
+}
+
+int alfa_mlp_loss_grad(alfa_mlp* m, const float* X, const float* T, const float* norm, int n,
+                       float* grad, float* loss) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  alfa_ctx* c = m->c;
+  NN(X); NN(T); NN(norm); NN(grad); NN(loss);
+  if (n < 1) return ALFA_E_SHAPE;
+  Engine& e = m->c->e;
+  cudaMemsetAsync(grad, 0, MLP_NPARAM * 4, e.stream);
+  cudaMemsetAsync(loss, 0, 4, e.stream);
+  mlp_grad(e.stream, m->P, X, T, nullptr, 0, n, n, norm, grad, loss);
+  return check_launch(e, "mlp_loss_grad");
+}
+
+int alfa_mlp_get_params(alfa_mlp* m, float* P, float* norm) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  Engine& e = m->c->e;
+  if (P) cudaMemcpyAsync(P, m->P, MLP_NPARAM * 4, cudaMemcpyDeviceToDevice, e.stream);
+  if (norm) cudaMemcpyAsync(norm, m->norm, 2 * (MLP_IN + 2) * 4, cudaMemcpyDeviceToDevice, e.stream);
+  return check_launch(e, "mlp_get_params");
+}
+
+int alfa_mlp_set_params(alfa_mlp* m, const float* P, const float* norm) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  Engine& e = m->c->e;
+  if (P) cudaMemcpyAsync(m->P, P, MLP_NPARAM * 4, cudaMemcpyDeviceToDevice, e.stream);
+  if (norm) {
+    cudaMemcpyAsync(m->norm, norm, 2 * (MLP_IN + 2) * 4, cudaMemcpyDeviceToDevice, e.stream);
+    m->trained = 1;
+  }
+  mlp_to_bf16(e.stream, m->P, m->Pb);
+  return check_launch(e, "mlp_set_params");
+}
+
+int alfa_mlp_features(alfa_mlp* m, float* X) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  alfa_ctx* c = m->c;
+  NN(X);
+  mlp_features_all(m->c->e.stream, feat_in(m->c), m->c->e.N(), X);
+  return check_launch(m->c->e, "mlp_features");
+}
+
+int alfa_mlp_infer(alfa_mlp* m, double* Cs2, double* beta) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  alfa_ctx* c = m->c;
+  NN(Cs2);
+  mlp_infer(m->c->e.stream, m->c->e.sms, feat_in(m->c), m->Pb, m->norm, m->c->e.N(), Cs2, beta);
+  return check_launch(m->c->e, "mlp_infer");
+}
+
+int alfa_step_learned(alfa_mlp* m, int nsteps, int judge_every, double tol, int refresh_points,
+                      int refresh_epochs, alfa_mlp_report* rep) {
+  if (!m || !m->c) return ALFA_E_STATE;
+  alfa_ctx* c = m->c;
+  Engine& e = c->e;
+  Work& W = c->w;
+  if (e.cfg.optSgs < 1 || e.cfg.optSgs > 4)
+    return e.fail("step_learned needs a dynamic SGS model (optSgs 1-4)", ALFA_E_CONFIG);
+  if (!m->trained) return e.fail("step_learned before mlp_train", ALFA_E_STATE);
+  if (judge_every < 1 || !rep) return e.fail("step_learned: bad arguments", ALFA_E_SHAPE);
+  const int nz = e.nz;
+  for (int s = 0; s < nsteps; s++) {
+    const int it = W.iteration;
+    const bool judge = rep->reverted || it == e.cfg.istep || it % judge_every == 0;
+    int st = one_step(c, judge ? 2 : 1);
+    if (st) return st;
+    rep->steps++;
+    if (!judge) {
+      rep->learned_steps++;
+      continue;
+    }
+    if (rep->reverted) continue;
+    // judge: the network on the same state against the procedure's Cs^2
+    learned_cs2(c, m->scratch);
+    const double* f2[2] = {m->scratch, W.Cs2};
+    plane_means(e, f2, 2, m->means);
+    std::vector<double> h(2 * nz);
+    cudaMemcpyAsync(h.data(), m->means, 2 * nz * 8, cudaMemcpyDeviceToHost, e.stream);
+    if (cudaStreamSynchronize(e.stream) != cudaSuccess) return e.fail("judge failed", ALFA_E_CUDA);
+    double num = 0.0, den = 0.0;  // relative L2 difference of the two profiles
+    for (int z = 0; z < nz; z++) {
+      num += (h[z] - h[nz + z]) * (h[z] - h[nz + z]);
+      den += h[nz + z] * h[nz + z];
+    }
+    const double drift = den > 0 ? std::sqrt(num / den) : 0.0;
+    rep->judged++;
+    rep->last_drift = drift;
+    rep->max_drift = std::max(rep->max_drift, drift);
+    if (drift > tol) {
+      rep->reverted = 1;
+      rep->reverted_at = it;
+    } else if (refresh_points > 0 && refresh_epochs > 0) {
+      // keep learning from the procedure's own fields of this judge step
+      st = alfa_mlp_collect(m, std::min(refresh_points, m->cap));
+      if (!st && m->count >= 1024) st = alfa_mlp_train(m, refresh_epochs, 1024, 1e-3, nullptr);
+      if (st) return st;
+    }
+  }
+  return check_launch(e, "step_learned");
 }
 
 }  // extern "C"

@@ -1587,7 +1587,7 @@ class OracleRun:
         self.CFLmax = max(self.CFLmax, cfl)
         self.ustar, self.M_sfc_loc, self.qz_sfc_avg = ustar, M, qavg
         self.last.update(dudz=grads[6], dvdz=grads[7], dTHdz=dTHdz, txy=mom[3], txz=mom[4],
-                         tyz=mom[5], qz=qz)
+                         tyz=mom[5], qz=qz, grads=grads)
         self.iteration += 1
         return self
 

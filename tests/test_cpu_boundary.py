@@ -25,7 +25,11 @@ def test_signature_table_covers_header():
                                     "alfa_PlanarMean_noalloc", "alfa_checkpoint_doubles",
                                     "alfa_ensemble_create", "alfa_ensemble_step",
                                     "alfa_ensemble_sync", "alfa_ensemble_error",
-                                    "alfa_ensemble_destroy"}
+                                    "alfa_ensemble_destroy", "alfa_mlp_create",
+                                    "alfa_mlp_destroy", "alfa_mlp_collect", "alfa_mlp_train",
+                                    "alfa_mlp_loss_grad", "alfa_mlp_get_params",
+                                    "alfa_mlp_set_params", "alfa_mlp_features",
+                                    "alfa_mlp_infer", "alfa_step_learned"}
     assert declared <= bound, declared - bound
 
 
