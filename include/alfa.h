@@ -368,6 +368,31 @@ unsigned long long alfa_launch_count(void);
 int alfa_time_kernel(alfa_ctx*, int which, int reps, double* ms /* host */,
                      double* bytes /* host */);
 
+/* One candidate of the autotuner: a line-pass shape (axis 0 = x, 1 = y;
+ * n_in -> n_out points along it; `outputs` outputs, the first with map
+ * `map`: 1 truncate, 2 derivative, 3 truncate+derivative, 4 pad, 5 unpad)
+ * run with `variant` (0 the default dispatch, 1 the compile-time transform
+ * in place of a phase-split pad/unpad, 2/3/4 the runtime-plan transform
+ * with radix schedule "largest radix 8" / "largest radix 4" / "default
+ * factors in ascending order"), its average launch time, whether its
+ * outputs equal the default's to 1e-12 of their maximum, and whether it was
+ * chosen. */
+typedef struct alfa_tune_entry {
+  int axis, n_in, n_out, outputs, map, variant, chosen, equal;
+  double ms;
+} alfa_tune_entry;
+
+/* Times every variant of the eight line-pass shapes of a step (y pad, x pad,
+ * x unpad, y unpad, x/y derivative, x/y filter + derivative) on a synthetic
+ * field, `reps` launches each with CUDA events, and makes the fastest
+ * variant whose outputs equal the default's the one later steps use.  Call
+ * between steps; model state is not touched (only step scratch), captured
+ * step graphs are released.  Writes up to max_out entries to `out` and the
+ * number of candidates to *n_out.  Replaces nothing in the reference (JAX
+ * picks its FFT plans inside XLA); the choice is the engine's own. */
+int alfa_autotune(alfa_ctx*, int reps, alfa_tune_entry* out /* host */, int max_out,
+                  int* n_out /* host */);
+
 #ifdef __cplusplus
 }
 #endif

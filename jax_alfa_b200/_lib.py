@@ -114,6 +114,13 @@ SIGNATURES = {
     "alfa_step_graph": [I],
 }
 
+class AlfaTuneEntry(ctypes.Structure):
+    """``alfa_tune_entry`` (include/alfa.h)."""
+    _fields_ = [("axis", ctypes.c_int), ("n_in", ctypes.c_int), ("n_out", ctypes.c_int),
+                ("outputs", ctypes.c_int), ("map", ctypes.c_int), ("variant", ctypes.c_int),
+                ("chosen", ctypes.c_int), ("equal", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
 class AlfaMlpReport(ctypes.Structure):
     _fields_ = [("steps", I), ("learned_steps", I), ("judged", I), ("reverted", I),
                 ("reverted_at", I), ("last_drift", D), ("max_drift", D)]
@@ -153,6 +160,9 @@ def load():
     lib.alfa_launch_count.restype = ctypes.c_ulonglong
     lib.alfa_time_kernel.argtypes = [CTX, I, I, c_double_p, c_double_p]
     lib.alfa_time_kernel.restype = I
+    lib.alfa_autotune.argtypes = [CTX, I, ctypes.POINTER(AlfaTuneEntry), I,
+                                  ctypes.POINTER(ctypes.c_int)]
+    lib.alfa_autotune.restype = I
     lib.alfa_PlanarMean_noalloc.argtypes = [P, I, I, I, P, c_void_p]
     lib.alfa_PlanarMean_noalloc.restype = I
     lib.alfa_checkpoint_doubles.argtypes = [CTX]

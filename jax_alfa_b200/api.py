@@ -73,6 +73,30 @@ class Alfa:
         except Exception:
             pass
 
+    TUNE_SHAPES = ("y pad", "x pad", "x unpad", "y unpad", "x derivative", "y derivative",
+                   "x filter+derivative", "y filter+derivative")
+    TUNE_VARIANTS = ("default", "compile-time", "radix-8", "radix-4", "ascending")
+
+    def autotune(self, reps=5):
+        """Time every line-pass variant of the step's pass shapes and keep the
+        fastest one whose outputs equal the default's (alfa_autotune).
+        Returns a list of dicts, one per candidate."""
+        cap = 64
+        buf = (_lib.AlfaTuneEntry * cap)()
+        n = ctypes.c_int(0)
+        self._call("alfa_autotune", int(reps), buf, cap, ctypes.byref(n))
+        torch.cuda.synchronize(self.device)
+        out, shape, last = [], -1, None
+        for e in buf[:min(n.value, cap)]:
+            key = (e.axis, e.n_in, e.n_out, e.outputs, e.map)
+            if key != last:
+                shape, last = shape + 1, key
+            out.append({"shape": self.TUNE_SHAPES[shape], "axis": e.axis, "n_in": e.n_in,
+                        "n_out": e.n_out, "outputs": e.outputs, "map": e.map,
+                        "variant": self.TUNE_VARIANTS[e.variant], "ms": e.ms,
+                        "equal": bool(e.equal), "chosen": bool(e.chosen)})
+        return out
+
     # ---------------------------------------------------------------- plumbing
     def _call(self, name, *args):
         self.lib.alfa_set_stream(self.ctx, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
@@ -716,6 +740,10 @@ class Simulation:
             self._call("alfa_step_graph", int(n))
         cur.wait_stream(self._gstream)
         return self
+
+    def autotune(self, reps=5):
+        """Alfa.autotune on this simulation's context (between steps)."""
+        return self.alfa.autotune(reps)
 
     def state(self):
         a = self.alfa

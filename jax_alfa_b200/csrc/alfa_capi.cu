@@ -154,9 +154,33 @@ static bool factor_23(int n, int* rad, int* np) {
   return m == 1 && n >= 2;
 }
 
-static int make_plan(Engine& e, int n, FftPlan* p) {
+// radix schedule r of the autotuner: 0 largest radix 8, 1 largest radix 4,
+// 2 the default factors in ascending order
+static bool factor_sched(int n, int r, int* rad, int* np) {
+  if (r == 2) {
+    if (!factor_23(n, rad, np)) return false;
+    std::reverse(rad, rad + *np);
+    return true;
+  }
+  const int rs8[4] = {8, 4, 3, 2}, rs4[3] = {4, 3, 2};
+  const int* rs = r == 0 ? rs8 : rs4;
+  const int nr = r == 0 ? 4 : 3;
+  int m = n, k = 0;
+  for (int t = 0; t < nr; t++) {
+    while (m % rs[t] == 0 && m > 1) {
+      if (k >= 8) return false;
+      rad[k++] = rs[t];
+      m /= rs[t];
+    }
+  }
+  *np = k;
+  return m == 1 && n >= 2;
+}
+
+static int make_plan(Engine& e, int n, FftPlan* p, int sched = -1) {
   p->n = n;
-  if (!factor_23(n, p->rad, &p->npass)) return -1;
+  if (sched < 0 ? !factor_23(n, p->rad, &p->npass) : !factor_sched(n, sched, p->rad, &p->npass))
+    return -1;
   std::vector<cd> tw(n);
   for (int q = 0; q < n; q++) {
     const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)q / n;
@@ -246,6 +270,14 @@ int engine_init(Engine& e, const alfa_config& c) {
       make_plan(e, e.my, &e.pmy))
     return e.fail("nx and ny must be of the form 2^a 3^b (FFT radices 2, 3, 4, 8, 16)",
                   ALFA_E_CONFIG);
+  {  // alternative radix schedules for the autotuner (a schedule with more
+     // than 8 passes falls back to the default factors)
+    const int lens[4] = {e.nx, e.ny, e.mx, e.my};
+    const FftPlan* def[4] = {&e.pnx, &e.pny, &e.pmx, &e.pmy};
+    for (int L = 0; L < 4; L++)
+      for (int r = 0; r < Engine::N_SCHED; r++)
+        if (make_plan(e, lens[L], &e.alt_plans[L][r], r)) e.alt_plans[L][r] = *def[L];
+  }
 
   // wavenumbers (Preprocess.py:89-94): fftfreq / rfftfreq with Nyquist 0
   std::vector<double> kx(c.nx), ky(e.nyh), kr(c.nx);
@@ -1628,6 +1660,155 @@ int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes
     default: *bytes = S16 + N8; break;
   }
   return check_launch(e, "time_kernel");
+}
+
+// Deterministic test field for the autotuner: a hash of the index mapped to
+// [-1, 1) (no model state is touched).
+__global__ void k_fill_hash(double* __restrict__ x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long h = (i + 1) * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    x[i] = (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  }
+}
+
+// out[0] = max |a - b|, out[1] = max |b| (non-negative doubles order like
+// their bit patterns, so an integer atomicMax reduces them)
+__global__ void k_maxdiff(const double* __restrict__ a, const double* __restrict__ b, size_t n,
+                          unsigned long long* out) {
+  double d = 0.0, m = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    d = fmax(d, fabs(a[i] - b[i]));
+    m = fmax(m, fabs(b[i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, (unsigned long long)__double_as_longlong(d));
+    atomicMax(out + 1, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+int alfa_autotune(alfa_ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
+  CTX_CHECK(c);
+  Engine& e = c->e;
+  if (reps < 1 || (max_out > 0 && !out)) return e.fail("autotune: bad arguments", ALFA_E_SHAPE);
+  Work& W = c->w;
+  const size_t N = e.N(), Y = (size_t)e.nx * e.my * e.nz, P = e.P();
+  double* src = W.Pb[4];
+  double* ref[2] = {W.Pb[2], W.Pb[3]};
+  unsigned long long* dmax = reinterpret_cast<unsigned long long*>(W.Pb[5]);
+  k_fill_hash<<<4 * 148, 256, 0, e.stream>>>(src, N);
+  // the pass shapes of a step: (X, Y) are the input's x and y extents
+  struct Shape {
+    int axis, X, Y, n_in, n_out, nout, map[2];
+    const double* in;
+    double* dst[2];
+    size_t len;
+    double scale;
+    int cut;
+  };
+  const double* Lp = W.Lpad;
+  const int nx = e.nx, ny = e.ny, mx = e.mx, my = e.my;
+  const Shape shapes[8] = {
+      {1, nx, ny, ny, my, 1, {LM_PAD, 0}, src, {W.Lpad, nullptr}, Y, 1.0 / my, 0},
+      {0, nx, my, nx, mx, 1, {LM_PAD, 0}, Lp, {W.Pb[0], nullptr}, P, 1.0 / mx, 0},
+      {0, mx, my, mx, nx, 1, {LM_UNPAD, 0}, W.Pb[0], {W.Lpad, nullptr}, Y, 1.0 / nx, 0},
+      {1, nx, my, my, ny, 1, {LM_UNPAD, 0}, Lp, {e.W, nullptr}, N, (9.0 / 4.0) / ny, 0},
+      {0, nx, ny, nx, nx, 1, {LM_DERIV, 0}, src, {e.W, nullptr}, N, 1.0 / nx, 0},
+      {1, nx, ny, ny, ny, 1, {LM_DERIV, 0}, src, {e.W, nullptr}, N, 1.0 / ny, 0},
+      {0, nx, ny, nx, nx, 2, {LM_TRUNC, LM_TRUNC_DERIV}, src, {W.L2, W.L2 + N}, N, 1.0 / nx,
+       e.cut_e[0]},
+      {1, nx, ny, ny, ny, 2, {LM_TRUNC, LM_TRUNC_DERIV}, src, {W.L2, W.L2 + N}, N, 1.0 / ny,
+       e.cut_e[1]},
+  };
+  cudaEvent_t ea, eb;
+  cudaEventCreate(&ea);
+  cudaEventCreate(&eb);
+  int n = 0;
+  int rc = ALFA_OK;
+  for (const Shape& sh : shapes) {
+    LineOut o[2];
+    for (int q = 0; q < sh.nout; q++) {
+      o[q] = LineOut{};
+      o[q].map = sh.map[q];
+      o[q].scale = sh.scale;
+      o[q].cut = sh.cut;
+      o[q].dst = sh.dst[q];
+    }
+    const long long key = line_key(sh.axis, sh.n_in, sh.n_out, sh.map[0], sh.nout);
+    const bool phase = sh.nout == 1 &&
+                       ((sh.map[0] == LM_PAD && sh.n_in == 256 && sh.n_out == 384) ||
+                        (sh.map[0] == LM_UNPAD && sh.n_in == 384 && sh.n_out == 256));
+    auto run = [&] {
+      launch_line(e, sh.axis, ld_field(e, sh.in), sh.X, sh.Y, sh.n_in, sh.n_out, sh.nout, o);
+    };
+    e.line_variant[key] = 0;
+    run();
+    for (int q = 0; q < sh.nout; q++)
+      cudaMemcpyAsync(ref[q], sh.dst[q], sh.len * sizeof(double), cudaMemcpyDeviceToDevice,
+                      e.stream);
+    int best = -1;
+    double best_ms = 0.0;
+    const int first = n;
+    for (int v = 0; v < 2 + Engine::N_SCHED; v++) {
+      if (v == 1 && !phase) continue;
+      e.line_variant[key] = v;
+      run();
+      bool same = true;
+      for (int q = 0; q < sh.nout; q++) {
+        cudaMemsetAsync(dmax, 0, 2 * sizeof(unsigned long long), e.stream);
+        k_maxdiff<<<4 * 148, 256, 0, e.stream>>>(sh.dst[q], ref[q], sh.len, dmax);
+        unsigned long long h[2] = {0, 0};
+        cudaMemcpyAsync(h, dmax, sizeof h, cudaMemcpyDeviceToHost, e.stream);
+        cudaStreamSynchronize(e.stream);
+        double dd, mm;
+        std::memcpy(&dd, &h[0], 8);
+        std::memcpy(&mm, &h[1], 8);
+        if (!(dd <= 1e-12 * mm)) same = false;
+      }
+      run();  // warm
+      cudaEventRecord(ea, e.stream);
+      for (int r = 0; r < reps; r++) run();
+      cudaEventRecord(eb, e.stream);
+      cudaEventSynchronize(eb);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ea, eb);
+      const double ms = (double)t / reps;
+      if (same && (best < 0 || ms < best_ms)) {
+        best = v;
+        best_ms = ms;
+      }
+      if (n < max_out) {
+        alfa_tune_entry& te = out[n];
+        te.axis = sh.axis;
+        te.n_in = sh.n_in;
+        te.n_out = sh.n_out;
+        te.outputs = sh.nout;
+        te.map = sh.map[0];
+        te.variant = v;
+        te.chosen = 0;
+        te.equal = same ? 1 : 0;
+        te.ms = ms;
+      }
+      n++;
+    }
+    if (best < 0) best = 0;
+    e.line_variant[key] = best;
+    for (int i = first; i < n && i < max_out; i++) out[i].chosen = out[i].variant == best;
+    if ((rc = check_launch(e, "autotune")) != ALFA_OK) break;
+  }
+  cudaEventDestroy(ea);
+  cudaEventDestroy(eb);
+  release_graphs(c);  // captured steps hold the old choices
+  if (n_out) *n_out = n;
+  return rc;
 }
 
 int alfa_AB2_TH(alfa_ctx* c, const double* TH, const double* R, const double* Rp, double* out) {

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -132,6 +133,15 @@ struct Engine {
   double* mat = nullptr;          // a loader's expression, materialised (P elements)
   double* stat = nullptr;         // statistics scratch (24 nz)
 
+  // Line-pass variants chosen by the autotuner (alfa_autotune), by pass
+  // shape (line_key): 0 the default dispatch, 1 the compile-time transform
+  // even where a phase-split pad/unpad exists, 2 + r the runtime-plan
+  // transform with radix schedule r of alt_plans (largest radix 8, largest
+  // radix 4, ascending order).
+  std::map<long long, int> line_variant;
+  static constexpr int N_SCHED = 3;
+  FftPlan alt_plans[4][N_SCHED];  // for nx, ny, mx, my
+
   size_t N() const { return (size_t)nx * ny * nz; }
   size_t P() const { return (size_t)mx * my * nz; }
   size_t S() const { return (size_t)nx * nyh * nz; }
@@ -159,6 +169,8 @@ void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, dou
 // field has n_out in place of the transformed extent.
 void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
                  int nout, const LineOut* outs);
+// the autotuner's key of a line pass
+long long line_key(int axis, int n_in, int n_out, int map, int nout);
 // separable spectral operators on real fields
 void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
                       double* scratch2);  // explicit filter and its x/y derivatives

@@ -571,6 +571,13 @@ static void phase_n(Engine& e, const LineArgs& a, int F) {
   }
 }
 
+static const FftPlan& alt_plan_for(const Engine& e, int n, int r) {
+  if (n == e.nx) return e.alt_plans[0][r];
+  if (n == e.ny) return e.alt_plans[1][r];
+  if (n == e.mx) return e.alt_plans[2][r];
+  return e.alt_plans[3][r];
+}
+
 static const FftPlan& plan_for(const Engine& e, int n) {
   if (n == e.nx) return e.pnx;
   if (n == e.ny) return e.pny;
@@ -605,6 +612,19 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
   a.pin = plan_for(e, n_in);
   a.pout = plan_for(e, n_out);
   ::alfa::note_launch();
+  int variant = 0;
+  if (!e.line_variant.empty()) {
+    auto it = e.line_variant.find(line_key(axis, n_in, n_out, outs[0].map, nout));
+    if (it != e.line_variant.end()) variant = it->second;
+  }
+  if (variant >= 2) {  // runtime plans with an alternative radix schedule
+    const int r = variant - 2;
+    a.pin = alt_plan_for(e, n_in, r);
+    a.pout = alt_plan_for(e, n_out, r);
+    line_n<0, 0>(e, a, F);
+    return;
+  }
+  if (variant == 1) goto compile_time;
   if (nout == 1 && outs[0].map == LM_PAD && n_in == 256 && n_out == 384) {
     phase_n<256, true>(e, a, F);
     return;
@@ -613,6 +633,7 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
     phase_n<256, false>(e, a, F);
     return;
   }
+compile_time:
 #define ALFA_CASE(p, q)               \
   if (n_in == p && n_out == q) {      \
     line_n<p, q>(e, a, F);            \
@@ -621,6 +642,11 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
   ALFA_X_PAIRS(ALFA_CASE)
 #undef ALFA_CASE
   line_n<0, 0>(e, a, F);
+}
+
+long long line_key(int axis, int n_in, int n_out, int map, int nout) {
+  const int cls = (map == LM_PAD) ? 1 : (map == LM_UNPAD ? 2 : 0);
+  return ((((long long)axis * 8192 + n_in) * 8192 + n_out) * 4 + cls) * 4 + nout;
 }
 
 static LineOut lo(int map, double* dst, double scale, int cut = 0, int acc = 0) {

@@ -47,3 +47,35 @@ def test_ensemble_equals_members_run_alone():
         for k in got:
             assert np.array_equal(got[k], alone[i][k]), (i, k)
     ens.close()
+
+
+@pytest.mark.parametrize("grid", [(48, 48, 32), (256, 256, 16)])
+def test_autotune_picks_the_fastest_equivalent_variant(grid):
+    cfg = cases.neutral(*grid, nsteps=4)
+    base = _state(_sim(cfg).step(4))
+    sim = _sim(cfg)
+    cands = sim.autotune(reps=3)
+    shapes = {}
+    for c in cands:
+        shapes.setdefault(c["shape"], []).append(c)
+    assert len(shapes) == 8
+    for name, cs in shapes.items():
+        assert [c["variant"] for c in cs][0] == "default"
+        chosen = [c for c in cs if c["chosen"]]
+        assert len(chosen) == 1, name
+        assert chosen[0]["equal"], name
+        assert chosen[0]["ms"] == min(c["ms"] for c in cs if c["equal"]), name
+        # the compile-time candidate exists only where a phase-split pass does
+        phase = name.endswith("pad") and grid[0] == 256
+        assert any(c["variant"] == "compile-time" for c in cs) == phase, name
+    tuned = _state(sim.step(4))
+    for k in base:
+        scale = max(np.abs(base[k]).max(), 1e-300)
+        assert np.abs(tuned[k] - base[k]).max() <= 1e-12 * scale, k
+    # graphs captured after tuning replay the tuned passes
+    g = _sim(cfg)
+    g.autotune(reps=1)
+    graphed = _state(g.step(4, graph=True))
+    for k in base:
+        scale = max(np.abs(base[k]).max(), 1e-300)
+        assert np.abs(graphed[k] - base[k]).max() <= 1e-12 * scale, k
