@@ -65,6 +65,14 @@ typedef struct alfa_config {
   double z_damping, RelaxTime;   /* m, s */
   int optAdvection;
   int optPressureSolver;         /* 1 Thomas, 0 dense (same tridiagonal system) */
+  int optGeoWind;                /* 0 constant Ug2, Vg2; 1 time/height-varying series
+                                    (alfa_set_geowind_series), ConfigLoader.py:77-82 */
+  /* moisture (ConfigLoader.py:100-124, DerivedVars.py:69-75) */
+  int optMoisture;               /* 0 dry, 1 specific humidity Q transported */
+  int optMoistureSurfBC;         /* 0 constant MoistureFlux, 1 flux series, 2 surface Q series */
+  double MoistureFlux;           /* kg/kg m/s */
+  double zMoisture;              /* m; reference height of the prescribed-Q flux (0: z0T) */
+  double q_inversion;            /* kg/kg/m, Q lapse rate above the domain top */
 } alfa_config;
 
 /* Derived constants (src/config/DerivedVars.py:48-112, Preprocess.py:44-62). */
@@ -113,6 +121,10 @@ int alfa_velocityGradients(alfa_ctx*, const double* u, const double* v, const do
 int alfa_potentialTemperatureGradients(alfa_ctx*, const double* TH, const double* ustar,
                                        const double* qz_sfc, const double* fi2D_h,
                                        double* const out[3]);            /* Derivatives.py:107 */
+/* out[3] = dQdx, dQdy, dQdz: the theta form with the moisture flux qm_sfc */
+int alfa_moistureGradients(alfa_ctx*, const double* Q, const double* ustar,
+                           const double* qm_sfc, const double* fi2D_h,
+                           double* const out[3]);                    /* Derivatives.py:281 */
 int alfa_Derivz_Generic_uvp(alfa_ctx*, const double* F, double* dFdz);  /* Derivatives.py:310 */
 int alfa_Derivz_Generic_w(alfa_ctx*, const double* F, double* dFdz);    /* Derivatives.py:340 */
 
@@ -150,6 +162,15 @@ int alfa_SurfaceFlux_HeterogeneousPrescribedTemperature(alfa_ctx*, const double*
     const double* v, const double* TH, double sfc_val, const double* const most_in[6],
     double* M_sfc_loc, double* ustar, double* qz_sfc_2D, double* qz_sfc_avg, double* invOB,
     double* const most_out[6]);                                              /* :393 */
+/* optMoistureSurfBC = 2: the surface moisture flux qm_sfc_2D (nx, ny) from
+ * the prescribed surface humidity Q_sfc_t (kg/kg) and psi2D_h, psi2D_h0 of
+ * MOSTfunctions (most[2], most[3]; the other four are not read). */
+int alfa_SurfaceMoistureFlux_HomogeneousPrescribedQ(alfa_ctx*, const double* Q,
+    const double* ustar, double Q_sfc_t, const double* const most[6],
+    double* qm_sfc_2D);                                                      /* :452 */
+int alfa_SurfaceMoistureFlux_HeterogeneousPrescribedQ(alfa_ctx*, const double* Q,
+    const double* ustar, double Q_sfc_t, const double* const most[6],
+    double* qm_sfc_2D);                                                      /* :483 */
 
 /* ---- src/pde ------------------------------------------------------------ */
 int alfa_Advection(alfa_ctx*, const double* u, const double* v, const double* w,
@@ -159,8 +180,10 @@ int alfa_Advection(alfa_ctx*, const double* u, const double* v, const double* w,
 int alfa_ScalarAdvection(alfa_ctx*, const double* u, const double* v, const double* w,
                          const double* dsdx, const double* dsdy, const double* dsdz,
                          double* out);                        /* SCL_AdvectionTerms.py:158 */
-int alfa_BuoyancyOpt1(alfa_ctx*, const double* TH, double* buoyancy); /* NSE_BuoyancyTerms.py:49 */
-int alfa_BuoyancyOpt2(alfa_ctx*, const double* TH, double* buoyancy); /* NSE_BuoyancyTerms.py:104 */
+int alfa_BuoyancyOpt1(alfa_ctx*, const double* TH, const double* H /* Q or NULL */,
+                      double* buoyancy); /* NSE_BuoyancyTerms.py:49 */
+int alfa_BuoyancyOpt2(alfa_ctx*, const double* TH, const double* H /* Q or NULL */,
+                      double* buoyancy); /* NSE_BuoyancyTerms.py:104 */
 
 /* grads[9] as velocityGradients' out.  mom[25] receives DynamicSGS's tuple
  * (DynamicSGS_Main.py:323-331): txx, tyy, tzz, txy, txz, tyz, Cs2_1D_avg1,
@@ -201,6 +224,9 @@ int alfa_RHS_Momentum(alfa_ctx*, const double* u, const double* v, const double*
                       double* RHS_w);                          /* NSE_AllTerms.py:48 */
 int alfa_RHS_Scalar(alfa_ctx*, const double* TH, const double* THAdvectionSum,
                     const double* divq, const double* THadv, double* RHS_TH); /* SCL_AllTerms.py:48 */
+/* Qadv: (nz) profile, always added */
+int alfa_RHS_Moisture(alfa_ctx*, const double* Q, const double* QAdvectionSum,
+                      const double* divqm, const double* Qadv, double* RHS_Q); /* SCL_AllTerms.py:86 */
 int alfa_PressureRC(alfa_ctx*, const double* u, const double* v, const double* w,
                     const double* RHS_u, const double* RHS_v, const double* RHS_w,
                     const double* RHS_u_previous, const double* RHS_v_previous,
@@ -217,6 +243,8 @@ int alfa_AB2_uvw(alfa_ctx*, const double* u, const double* v, const double* w,
                  double* w_new);                          /* NSE_TimeAdvancement.py:45 */
 int alfa_AB2_TH(alfa_ctx*, const double* TH, const double* RHS_TH,
                 const double* RHS_TH_previous, double* TH_new); /* SCL_TimeAdvancement.py:46 */
+int alfa_AB2_Q(alfa_ctx*, const double* Q, const double* RHS_Q, const double* RHS_Q_previous,
+               double* Q_new);                              /* SCL_TimeAdvancement.py:79 */
 
 /* Main.py:498-500 — RHS_i -= dp/dx_i, in place. */
 int alfa_AddPressureGradient(alfa_ctx*, double* RHS_u, double* RHS_v, double* RHS_w,
@@ -234,6 +262,21 @@ int alfa_init_state(alfa_ctx*, const double* u, const double* v, const double* w
                     const double* TH);
 int alfa_set_series(alfa_ctx*, const double* Uadv, const double* Vadv, const double* THadv,
                     const double* sfc, int nrows);
+/* optGeoWind = 1: the geostrophic wind series (host, copied), Ug and Vg
+ * (nrows, nz) non-dimensional as Initialize_GeoWind_Varying returns them
+ * (Initialization.py:163-246); row iteration-1 is the profile of each
+ * iteration (Main.py:84-86, 170-174). */
+int alfa_set_geowind_series(alfa_ctx*, const double* Ug, const double* Vg, int nrows);
+/* optMoisture = 1 (Main.py:71-76): the initial specific humidity Q (device,
+ * kg/kg as Initialize_Q loads it; required before the first step), and the
+ * moisture series (host, copied): Qadv (nrows, nz) non-dimensional
+ * (Initialize_AdvForcing's AdvForcing_Q, or NULL) and msfc (nrows) as
+ * Initialize_MoistureSurfaceBC returns it (or NULL); row iteration-1 is used
+ * at each iteration (Main.py:186-188, 253-267).  get_moisture copies the
+ * current Q out. */
+int alfa_init_moisture(alfa_ctx*, const double* Q);
+int alfa_set_moisture_series(alfa_ctx*, const double* Qadv, const double* msfc, int nrows);
+int alfa_get_moisture(alfa_ctx*, double* Q);
 int alfa_step(alfa_ctx*, int nsteps);
 int alfa_get_state(alfa_ctx*, double* u, double* v, double* w, double* TH, double* p);
 int alfa_get_diag(alfa_ctx*, alfa_diag* out /* host; synchronises the stream */);

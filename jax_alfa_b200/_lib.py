@@ -36,6 +36,10 @@ class AlfaConfig(ctypes.Structure):
         ("z_damping", ctypes.c_double), ("RelaxTime", ctypes.c_double),
         ("optAdvection", ctypes.c_int),
         ("optPressureSolver", ctypes.c_int),
+        ("optGeoWind", ctypes.c_int),
+        ("optMoisture", ctypes.c_int), ("optMoistureSurfBC", ctypes.c_int),
+        ("MoistureFlux", ctypes.c_double), ("zMoisture", ctypes.c_double),
+        ("q_inversion", ctypes.c_double),
     ]
 
 
@@ -76,6 +80,9 @@ SIGNATURES = {
     "alfa_Derivxy": [P, I, P],
     "alfa_velocityGradients": [P, P, P, P, P, P, P, P, P, PP],
     "alfa_potentialTemperatureGradients": [P, P, P, P, PP],
+    "alfa_moistureGradients": [P, P, P, P, PP],
+    "alfa_SurfaceMoistureFlux_HomogeneousPrescribedQ": [P, P, D, PP, P],
+    "alfa_SurfaceMoistureFlux_HeterogeneousPrescribedQ": [P, P, D, PP, P],
     "alfa_Derivz_Generic_uvp": [P, P],
     "alfa_Derivz_Generic_w": [P, P],
     "alfa_PlanarMean": [P, P],
@@ -89,22 +96,28 @@ SIGNATURES = {
     "alfa_SurfaceFlux_HeterogeneousPrescribedTemperature": [P, P, P, D, PP, P, P, P, P, P, PP],
     "alfa_Advection": [P] * 12,
     "alfa_ScalarAdvection": [P] * 7,
-    "alfa_BuoyancyOpt1": [P, P],
-    "alfa_BuoyancyOpt2": [P, P],
+    "alfa_BuoyancyOpt1": [P, P, P],
+    "alfa_BuoyancyOpt2": [P, P, P],
     "alfa_DivStressDynamicSGS": [PP, P, P, P, P, P, P, P, P, P, P, P, P, P, PP],
     "alfa_DivFluxDynamicSGS": [PP, P, P, P, P, P, P, P, P, P, P],
     "alfa_DivStressStaticSGS": [PP, P, P, P, P, P, P, P, P, P, PP],
     "alfa_DivFluxStaticSGS": [PP, P, P, P, P, P, P, P],
     "alfa_RHS_Momentum": [P] * 17,
     "alfa_RHS_Scalar": [P] * 5,
+    "alfa_RHS_Moisture": [P] * 5,
     "alfa_PressureRC": [P] * 13,
     "alfa_ThomasPressureSolve": [P] * 7,
     "alfa_AB2_uvw": [P] * 12,
     "alfa_AB2_TH": [P] * 4,
+    "alfa_AB2_Q": [P] * 4,
     "alfa_AddPressureGradient": [P] * 6,
     "alfa_CFL": [P] * 4,
     "alfa_init_state": [P] * 4,
     "alfa_set_series": [c_double_p, c_double_p, c_double_p, c_double_p, I],
+    "alfa_set_geowind_series": [c_double_p, c_double_p, I],
+    "alfa_init_moisture": [P],
+    "alfa_set_moisture_series": [c_double_p, c_double_p, I],
+    "alfa_get_moisture": [P],
     "alfa_step": [I],
     "alfa_get_state": [P] * 5,
     "alfa_ComputeStats": [P] * 20,

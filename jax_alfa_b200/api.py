@@ -26,6 +26,8 @@ F64 = torch.float64
 C128 = torch.complex128
 
 CONFIG_KEYS = [f for f, _ in _lib.AlfaConfig._fields_]
+OPTIONAL_KEYS = ("optGeoWind", "optMoisture", "optMoistureSurfBC", "MoistureFlux", "zMoisture",
+                 "q_inversion")
 
 
 def make_config(cfg):
@@ -33,7 +35,9 @@ def make_config(cfg):
     (optSgs 2, 4) start from Cwl / CwlPrRatio, as DerivedVars.py:101-103 does."""
     c = _lib.AlfaConfig()
     for k in CONFIG_KEYS:
-        v = cfg[k]
+        # options newer than the original Config.py default to off / zero
+        # (ConfigLoader.py:77-124)
+        v = cfg.get(k, 0) if k in OPTIONAL_KEYS else cfg[k]
         setattr(c, k, int(v) if isinstance(getattr(c, k), int) else float(v))
     if int(cfg["optSgs"]) in (2, 4):
         c.Cs2 = float(cfg.get("Cwl", cfg["Cs2"]))
@@ -242,6 +246,12 @@ class Alfa:
                    self._p(qz_sfc, self.H), self._p(MOSTfunctions[5], self.H), self._pp(out))
         return tuple(out)
 
+    def moistureGradients(self, Q, kx2, ky2, ustar, qm_sfc, MOSTfunctions, ZeRo3D=None):
+        out = [self._new(self.N) for _ in range(3)]
+        self._call("alfa_moistureGradients", self._f(Q), self._p(ustar, self.H),
+                   self._p(qm_sfc, self.H), self._p(MOSTfunctions[5], self.H), self._pp(out))
+        return tuple(out)
+
     def Derivz_Generic_uvp(self, F, ZeRo3D=None):
         out = self._new(self.N)
         self._call("alfa_Derivz_Generic_uvp", self._f(F), self._p(out))
@@ -325,20 +335,44 @@ class Alfa:
                    self._p(out))
         return out
 
-    def _check_dry(self, H):
-        if H is not None and bool(torch.as_tensor(H).abs().max() != 0):
-            raise NotImplementedError("moisture (H != 0) is not part of this build")
-
     def BuoyancyOpt1(self, TH, H=None, ZeRo3D=None):
-        self._check_dry(H)
+        """H: the specific humidity (THv = (TH + T_0)(1 + 0.61 H)) or None."""
         out = self._new(self.N)
-        self._call("alfa_BuoyancyOpt1", self._f(TH), self._p(out))
+        self._call("alfa_BuoyancyOpt1", self._f(TH), None if H is None else self._f(H),
+                   self._p(out))
         return out
 
     def BuoyancyOpt2(self, TH, H=None, ZeRo3D=None):
-        self._check_dry(H)
         out = self._new(self.N)
-        self._call("alfa_BuoyancyOpt2", self._f(TH), self._p(out))
+        self._call("alfa_BuoyancyOpt2", self._f(TH), None if H is None else self._f(H),
+                   self._p(out))
+        return out
+
+    def SurfaceMoistureFlux_HomogeneousPrescribedQ(self, Q, ustar, Q_sfc_t, MOSTfunctions):
+        return self._moisture_surface("alfa_SurfaceMoistureFlux_HomogeneousPrescribedQ", Q,
+                                      ustar, Q_sfc_t, MOSTfunctions)
+
+    def SurfaceMoistureFlux_HeterogeneousPrescribedQ(self, Q, ustar, Q_sfc_t, MOSTfunctions):
+        return self._moisture_surface("alfa_SurfaceMoistureFlux_HeterogeneousPrescribedQ", Q,
+                                      ustar, Q_sfc_t, MOSTfunctions)
+
+    def _moisture_surface(self, name, Q, ustar, Q_sfc_t, MOST):
+        out = self._new(self.H)
+        self._call(name, self._f(Q), self._p(ustar, self.H), ctypes.c_double(float(Q_sfc_t)),
+                   self._pp(list(MOST), [self.H] * 6), self._p(out))
+        return out
+
+    def RHS_Moisture(self, Q, QAdvectionSum, divqm, RayleighDampCoeff_stag=None, Qadv=None):
+        out = self._new(self.N)
+        Qa = torch.zeros(self.nz, dtype=F64, device=self.device) if Qadv is None else self._prof(Qadv)
+        self._call("alfa_RHS_Moisture", self._f(Q), self._f(QAdvectionSum), self._f(divqm),
+                   self._p(Qa), self._p(out))
+        return out
+
+    def AB2_Q(self, Q, RHS_Q, RHS_Q_previous):
+        out = self._new(self.N)
+        self._call("alfa_AB2_Q", self._f(Q), self._f(RHS_Q), self._f(RHS_Q_previous),
+                   self._p(out))
         return out
 
     def InitializeStats(self, ZeRo1D=None):
@@ -692,12 +726,49 @@ def write_3d_fields(out_dir, iteration, u, v, w, TH, Ugal, T_0_nondim):
     return path
 
 
+def load_geowind(path, cfg):
+    """The geostrophic wind series of a GeoWind ``.npz`` file, (Ug, Vg) of
+    shape (nsteps+1, nz) in m/s, with the checks and the per-level linear
+    interpolation of compact profiles of ``Initialize_GeoWind_Varying``
+    (``Initialization.py:163-246``).  Raises ValueError as the reference
+    does on a mismatched dt, option, length or nz."""
+    d = np.load(path)
+    dt, nz = float(cfg["dt"]), int(cfg["nz"])
+    nsteps = int(np.ceil(cfg["SimTime"] / dt))  # DerivedVars.py:90
+    if abs(float(d["dt_geo"]) - dt) > 1e-6:
+        raise ValueError(f"GeoWind file dt_geo={float(d['dt_geo']):.6f} s does not match "
+                         f"Config dt={dt:.6f} s")
+    if int(d["optGeoWind"]) != int(cfg["optGeoWind"]):
+        raise ValueError("GeoWind file optGeoWind does not match Config optGeoWind")
+    if "Ug_series" in d and "Vg_series" in d:
+        Ug, Vg = np.asarray(d["Ug_series"]), np.asarray(d["Vg_series"])
+        if Ug.shape[0] != nsteps + 1:
+            raise ValueError(f"GeoWind series length {Ug.shape[0]} != nsteps+1={nsteps + 1}")
+        if Ug.shape[1] != nz:
+            raise ValueError(f"GeoWind nz={Ug.shape[1]} != Config nz={nz}")
+        return Ug, Vg
+    t, Up, Vp = np.asarray(d["t_profile"]), np.asarray(d["Ug_profile"]), np.asarray(d["Vg_profile"])
+    if Up.shape[1] != nz:
+        raise ValueError(f"GeoWind nz={Up.shape[1]} != Config nz={nz}")
+    tt = np.arange(nsteps + 1) * dt
+    if tt[0] < t[0] - 1e-6 or tt[-1] > t[-1] + 1e-6:
+        raise ValueError("GeoWind compact profiles do not cover the configured simulation interval")
+    Ug = np.stack([np.interp(tt, t, Up[:, k]) for k in range(nz)], axis=1)
+    Vg = np.stack([np.interp(tt, t, Vp[:, k]) for k in range(nz)], axis=1)
+    return Ug, Vg
+
+
 class Simulation:
     """The reference's time loop (``src/Main.py:156-541``) run by libalfa
     with the state on the device.  Fields in: dimensional (u total incl.
     Ugal, theta absolute) as the reference's input files hold them."""
 
-    def __init__(self, cfg, u, v, w, th, surface_series=None, adv_series=None, device=None):
+    def __init__(self, cfg, u, v, w, th, surface_series=None, adv_series=None, device=None,
+                 geowind_series=None, Q=None, moisture_series=None):
+        """optMoisture = 1 takes Q (kg/kg, as Initialize_Q loads it),
+        moisture_series (the MoistureSurfaceBC data series when
+        optMoistureSurfBC >= 1) and, with optAdvection, an optional fourth
+        adv_series entry Qadv (kg/kg s^-1)."""
         self.alfa = Alfa(cfg, device)
         a = self.alfa
         z = a.derived.z_scale
@@ -714,7 +785,7 @@ class Simulation:
         keep = []
         U = V = T = S = None
         if adv_series is not None:
-            U, V, T = [np.ascontiguousarray(x * z, dtype=np.float64) for x in adv_series]
+            U, V, T = [np.ascontiguousarray(x * z, dtype=np.float64) for x in adv_series[:3]]
             nrows = U.shape[0]
             keep += [U, V, T]
         if surface_series is not None:
@@ -725,6 +796,33 @@ class Simulation:
         if U is not None and S is not None and S.shape[0] != U.shape[0]:
             raise ValueError("series lengths differ")
         self._call("alfa_set_series", ptr(U), ptr(V), ptr(T), ptr(S), nrows)
+        if int(cfg.get("optGeoWind", 0)) >= 1:
+            if geowind_series is None:
+                raise ValueError("optGeoWind >= 1 needs geowind_series (Ug, Vg)")
+            # non-dimensional = m/s / u_scale, u_scale = 1 (Initialization.py:241-244)
+            Ug, Vg = [np.ascontiguousarray(x, dtype=np.float64) for x in geowind_series]
+            if Ug.shape != Vg.shape or Ug.ndim != 2 or Ug.shape[1] != a.nz:
+                raise ValueError("geowind_series: Ug, Vg must both be (nrows, nz)")
+            self._call("alfa_set_geowind_series", ptr(Ug), ptr(Vg), Ug.shape[0])
+        self.moist = int(cfg.get("optMoisture", 0)) >= 1
+        if self.moist:
+            if Q is None:
+                raise ValueError("optMoisture >= 1 needs the initial humidity Q")
+            q = tt(Q)
+            self._call("alfa_init_moisture", a._f(q))
+            torch.cuda.current_stream(dev).synchronize()
+            # Initialize_AdvForcing / Initialize_MoistureSurfaceBC (u_scale = Q_scale = 1)
+            Qa = (np.ascontiguousarray(adv_series[3] * z, dtype=np.float64)
+                  if adv_series is not None and len(adv_series) > 3 else None)
+            Ms = None
+            if int(cfg.get("optMoistureSurfBC", 0)) >= 1:
+                if moisture_series is None:
+                    raise ValueError("optMoistureSurfBC >= 1 needs moisture_series")
+                Ms = np.ascontiguousarray(moisture_series, dtype=np.float64)
+            rows = [x.shape[0] for x in (Qa, Ms) if x is not None]
+            if len(set(rows)) > 1:
+                raise ValueError("moisture series lengths differ")
+            self._call("alfa_set_moisture_series", ptr(Qa), ptr(Ms), rows[0] if rows else 0)
 
     def step(self, n=1, graph=False):
         """n steps; graph=True replays captured CUDA graphs (alfa_step_graph),
@@ -749,7 +847,11 @@ class Simulation:
         a = self.alfa
         out = [a._new(a.N) for _ in range(5)]
         self._call("alfa_get_state", *[a._p(x) for x in out])
-        return dict(zip(("u", "v", "w", "TH", "p"), out))
+        st = dict(zip(("u", "v", "w", "TH", "p"), out))
+        if self.moist:
+            st["Q"] = a._new(a.N)
+            self._call("alfa_get_moisture", a._p(st["Q"]))
+        return st
 
     def stats_sample(self, acc=None):
         """Add this iteration's statistics sample (Main.py:547-558) to the

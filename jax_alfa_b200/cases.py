@@ -148,6 +148,40 @@ def initial_fields(cfg, seed=0):
     return u, v, w, th
 
 
+def initial_moisture(cfg, seed=0):
+    """Initial specific humidity (kg/kg, absolute; ``Initialize_Q``), (nx,
+    ny, nz) C-order: 8 g/kg at the surface drying by 2 g/kg over the domain
+    depth, with 0.1 g/kg seeded noise in the lower third."""
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    z = z_uvp(cfg)
+    rng = np.random.default_rng(1000 + seed)
+    q = np.empty((nx, ny, nz))
+    q[:] = (8.0e-3 - 2.0e-3 * z / cfg["l_z"])[None, None, :]
+    for k in range(nz):
+        if z[k] < cfg["l_z"] / 3:
+            q[:, :, k] += 1.0e-4 * rng.uniform(-1.0, 1.0, (nx, ny))
+    return q
+
+
+def moisture_surface_series(cfg):
+    """The moisture surface series at every step (``Initialization.py:
+    344-388`` format): for ``optMoistureSurfBC=1`` a flux (kg/kg m/s)
+    oscillating about MoistureFlux, for ``=2`` the surface humidity (kg/kg)
+    near 10 g/kg."""
+    n = nsteps_of(cfg) + 1
+    ph = 2 * np.pi * np.arange(n) / 5.0
+    if cfg["optMoistureSurfBC"] == 1:
+        return cfg["MoistureFlux"] + 2.0e-5 * np.sin(ph)
+    return 1.0e-2 + 5.0e-4 * np.sin(ph)
+
+
+def adv_moisture_series(cfg):
+    """Qadv (kg/kg s^-1) at every step and level for the AdvForcing file."""
+    n = nsteps_of(cfg) + 1
+    zh = (np.arange(cfg["nz"]) + 0.5) / cfg["nz"]
+    return np.broadcast_to(-2.0e-8 * (1.0 - zh)[None, :], (n, cfg["nz"])).copy()
+
+
 def surface_bc_series(cfg):
     """Surface boundary series at every step, t=0..SimTime, in the
     ``Initialization.py:107-160`` format: for ``optSurfBC=2`` the surface
@@ -168,6 +202,20 @@ def adv_forcing_series(cfg):
     nz = cfg["nz"]
     U = np.full((n, nz), cfg.get("Uadv_const", 0.0))
     return U, np.zeros((n, nz)), np.zeros((n, nz))
+
+
+def geowind_series(cfg):
+    """Time- and height-varying geostrophic wind (Ug, Vg) in m/s at every
+    step and level, (nsteps+1, nz) each (``Initialization.py:173-246``
+    per-step format): a height shear about (Ug2, Vg2) plus an oscillation
+    with a period of seven steps, so every step's row differs."""
+    n = nsteps_of(cfg) + 1
+    nz = cfg["nz"]
+    zh = (np.arange(nz) + 0.5) / nz
+    ph = 2 * np.pi * np.arange(n)[:, None] / 7.0
+    Ug = cfg["Ug2"] + 1.5 * zh[None, :] + 0.8 * np.sin(ph) * (1.0 - zh[None, :])
+    Vg = cfg["Vg2"] - 0.6 * zh[None, :] + 0.5 * np.cos(ph) * zh[None, :]
+    return Ug, Vg
 
 
 def to_reference_files(cfg, u, v, w, th):
@@ -201,11 +249,24 @@ def write_run_dir(cfg, path, seed=0):
     if cfg["optSurfBC"] >= 1:
         np.savez(os.path.join(path, cfg["SurfaceBCFile"]), dt_surf=cfg["dt"],
                  optSurfBC=np.int32(cfg["optSurfBC"]), data_series=surface_bc_series(cfg))
+    moist = cfg.get("optMoisture", 0) >= 1
+    if moist:
+        q = initial_moisture(cfg, seed)
+        np.save(os.path.join(path, "input", "Q.npy"), q.reshape(-1, order="F"))
+        if cfg["optMoistureSurfBC"] >= 1:
+            np.savez(os.path.join(path, cfg["MoistureSurfaceBCFile"]), dt_moist=cfg["dt"],
+                     optMoistureSurfBC=np.int32(cfg["optMoistureSurfBC"]),
+                     data_series=moisture_surface_series(cfg))
+    if cfg.get("optGeoWind", 0) >= 1:
+        Ug, Vg = geowind_series(cfg)
+        np.savez(os.path.join(path, cfg["GeoWindFile"]), dt_geo=cfg["dt"],
+                 optGeoWind=np.int32(cfg["optGeoWind"]), Ug_series=Ug, Vg_series=Vg)
     if cfg["optAdvection"] >= 1:
         U, V, T = adv_forcing_series(cfg)
+        extra = {"Qadv_series": adv_moisture_series(cfg)} if moist else {}
         np.savez(os.path.join(path, cfg["AdvectionFile"]), dt_adv=cfg["dt"],
                  optAdvection=np.int32(cfg["optAdvection"]),
-                 Uadv_series=U, Vadv_series=V, THadv_series=T)
+                 Uadv_series=U, Vadv_series=V, THadv_series=T, **extra)
 
 
 def gp_per_step(cfg):
@@ -214,4 +275,5 @@ def gp_per_step(cfg):
 
 __all__ = ["CASES", "neutral", "neutral256", "convective", "stable",
            "initial_fields", "write_run_dir", "nsteps_of", "surface_bc_series",
-           "adv_forcing_series", "gp_per_step"]
+           "adv_forcing_series", "geowind_series", "initial_moisture",
+           "moisture_surface_series", "adv_moisture_series", "gp_per_step"]

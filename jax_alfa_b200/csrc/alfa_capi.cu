@@ -51,6 +51,18 @@ struct Work {
   double* zero_prof;
   double* series_adv = nullptr;  // (nrows, 3, nz) non-dimensional Uadv, Vadv, THadv
   int series_rows = 0;
+  double* series_geo = nullptr;  // (nrows, 2, nz) non-dimensional Ug, Vg (optGeoWind >= 1)
+  int geo_rows = 0;
+  // moisture (optMoisture >= 1; carved only then)
+  double *Q = nullptr, *RHSQ = nullptr, *RHSQp = nullptr;
+  double* gQ[3] = {nullptr, nullptr, nullptr};  // dQdx dQdy dQdz
+  double *Qadvs = nullptr, *divqm = nullptr, *qzq = nullptr;  // QAdvectionSum, divqm, qHz_q
+  double* qm_plane = nullptr;                                 // qm_sfc_step (nx, ny)
+  double* series_q = nullptr;  // (nrows, nz) non-dimensional Qadv
+  int q_rows = 0;
+  double* d_msfc = nullptr;  // (nrows) moisture surface series
+  int msfc_rows = 0;
+  int have_q = 0;
   std::vector<double> sfc_series;  // host
   double* d_sfc = nullptr;         // device copy of sfc_series
   int* d_it;                       // the iteration counter, on the device
@@ -241,10 +253,17 @@ int engine_init(Engine& e, const alfa_config& c) {
   e.T0_nondim = c.T_0 / 1.0;
   e.inversion_nondim = c.inversion * (e.z_scale / 1.0);
   e.qz_sfc_const = c.SensibleHeatFlux * 1.0 / (1.0 * 1.0);
+  // moisture: DerivedVars.py:69-75 (Q_scale = 1), SurfaceFlux.py:475-476
+  if (c.optMoisture < 0 || c.optMoisture > 1 || c.optMoistureSurfBC < 0 ||
+      c.optMoistureSurfBC > 2)
+    return e.fail("optMoisture must be 0 or 1 and optMoistureSurfBC 0, 1 or 2", ALFA_E_CONFIG);
+  e.q_inversion_nondim = c.q_inversion * (e.z_scale / 1.0);
+  e.qm_sfc_const = c.MoistureFlux / (1.0 * 1.0);
   e.dx = 2 * PI / c.nx;
   e.dy = 2 * PI / c.ny;
   e.dz = (c.l_z / e.z_scale) / (c.nz - 1);
   e.idz = 1.0 / e.dz;
+  e.log_zq = std::log(0.5 * e.dz * e.z_scale / (c.zMoisture > 0.0 ? c.zMoisture : c.z0T));
   e.L = c.FGR * std::pow(e.dx * e.dy * e.dz, 1.0 / 3.0);
   e.dt_nondim = c.dt * 1.0 / e.z_scale;
   // DerivedVars.py: FGR = 1 -> 3/2-rule dealiasing with TFR = 2; FGR > 1 -> the
@@ -440,6 +459,16 @@ static void carve(alfa_ctx* c, Carver& k) {
   }
   w.qx = k.take<double>(N);
   w.qy = k.take<double>(N);
+  if (e.cfg.optMoisture >= 1) {
+    w.Q = k.take<double>(N);
+    w.RHSQ = k.take<double>(N);
+    w.RHSQp = k.take<double>(N);
+    for (int i = 0; i < 3; i++) w.gQ[i] = k.take<double>(N);
+    w.Qadvs = k.take<double>(N);
+    w.divqm = k.take<double>(N);
+    w.qzq = k.take<double>(N);
+    w.qm_plane = k.take<double>(H);
+  }
   for (int i = 0; i < 10; i++) w.Pb[i] = k.take<double>(P);
   w.Lpad = k.take<double>((size_t)e.nx * e.my * nz);
   w.L2 = k.take<double>(2 * N);
@@ -902,12 +931,36 @@ static int one_step(alfa_ctx* c, int sgs_mode) {
   const alfa_config& cf = e.cfg;
   const int it = W.iteration;
   const int nz = e.nz;
-  if (it > cf.istep)
+  const bool moist = cf.optMoisture >= 1;
+  if (moist && !W.have_q)
+    return e.fail("optMoisture = 1 needs alfa_init_moisture before stepping", ALFA_E_STATE);
+  if (moist && cf.optMoistureSurfBC >= 1 && it - 1 >= W.msfc_rows)
+    return e.fail("moisture surface series exhausted", ALFA_E_STATE);
+  if (it > cf.istep) {
     for (int i = 0; i < 4; i++) std::swap(W.RHSp[i], W.RHS[i]);
+    if (moist) std::swap(W.RHSQp, W.RHSQ);
+  }
+  // Qadv rows (Main.py:186-188): zero unless a Qadv series was given
+  const double* Qadvp = W.zero_prof;
+  const int* qtp = nullptr;
+  if (moist && cf.optAdvection >= 1 && W.series_q) {
+    if (it - 1 >= W.q_rows) return e.fail("moisture advection series exhausted", ALFA_E_STATE);
+    Qadvp = W.series_q;
+    qtp = W.d_it;
+  }
   // forcing rows (Main.py:179-188) are selected on the device from the
   // device iteration counter, so a captured step replays with the current row
   const double *Uadv = W.zero_prof, *Vadv = W.zero_prof, *THadv = W.zero_prof;
   const int* itp = nullptr;
+  // geostrophic wind rows (Main.py:170-174), selected the same way
+  const double *Ugp = W.Ug, *Vgp = W.Vg;
+  const int* gtp = nullptr;
+  if (cf.optGeoWind >= 1) {
+    if (it - 1 >= W.geo_rows) return e.fail("geostrophic wind series exhausted", ALFA_E_STATE);
+    Ugp = W.series_geo;
+    Vgp = W.series_geo + nz;
+    gtp = W.d_it;
+  }
   if (cf.optAdvection >= 1) {
     if (it - 1 >= W.series_rows) return e.fail("advection series exhausted", ALFA_E_STATE);
     Uadv = W.series_adv;
@@ -930,6 +983,10 @@ static int one_step(alfa_ctx* c, int sgs_mode) {
   std::swap(W.w, W.Cz);
   op2_filter_deriv(e, ld_field(e, W.TH), W.THadv, W.gT[0], W.gT[1], W.L2);
   std::swap(W.TH, W.THadv);
+  if (moist) {  // Main.py:198-199; moistureGradients' Derivxy from the same passes
+    op2_filter_deriv(e, ld_field(e, W.Q), W.Qadvs, W.gQ[0], W.gQ[1], W.L2);
+    std::swap(W.Q, W.Qadvs);
+  }
   // surface fluxes (Main.py:213-243)
   const int var = surface_variant(cf);
   double sfc = 0.0;
@@ -954,14 +1011,29 @@ static int one_step(alfa_ctx* c, int sgs_mode) {
   surface_flux(e, var, sfc, io, sfc_dev, W.d_it);
   for (int i = 0; i < 6; i++) std::swap(W.most[i], W.most_new[i]);
   const double* qz_step = (var <= 1) ? W.qz_plane : W.q2;
+  // surface moisture flux (Main.py:253-267): a constant plane (filled by
+  // alfa_init_moisture), the series value, or from the prescribed humidity
+  // with this step's ustar and psi functions
+  if (moist && cf.optMoistureSurfBC >= 1) {
+    const double* qbar0 = nullptr;
+    if (cf.optMoistureSurfBC == 2 && cf.optSurfFlux == 0) {
+      const double* f1[1] = {W.Q};
+      plane_means(e, f1, 1, W.prof + 36 * nz);
+      qbar0 = W.prof + 36 * nz;
+    }
+    moisture_surface(e, cf.optMoistureSurfBC, cf.optSurfFlux != 0, W.Q, W.ustar, W.most[2],
+                     W.most[3], W.d_msfc, W.d_it, 0.0, qbar0, W.qm_plane);
+  }
   // gradients (Main.py:275-290)
   derivz_M(e, W.u, W.v, W.w, W.ustar, W.M, W.most[4], W.g[6], W.g[7], W.g[8]);
   derivz_TH(e, W.TH, W.ustar, qz_step, W.most[5], W.gT[2]);
+  if (moist) derivz_TH(e, W.Q, W.ustar, W.qm_plane, W.most[5], W.gQ[2]);  // Derivatives.py:304
   // advection (Main.py:301-311)
   advection(c, W.u, W.v, W.w, W.g[3], W.g[6], W.g[1], W.g[7], W.g[2], W.g[5], W.Cx, W.Cy, W.Cz);
   scalar_advection(c, W.u, W.v, W.w, W.gT[0], W.gT[1], W.gT[2], W.THadv, true);
-  // buoyancy (Main.py:323-327)
-  buoyancy(e, W.TH, cf.optBuoyancy == 0 ? 0 : 1, W.buoy);
+  if (moist) scalar_advection(c, W.u, W.v, W.w, W.gQ[0], W.gQ[1], W.gQ[2], W.Qadvs, true);
+  // buoyancy (Main.py:323-327), H = Q when moist
+  buoyancy(e, W.TH, moist ? W.Q : nullptr, cf.optBuoyancy == 0 ? 0 : 1, W.buoy);
   // SGS (Main.py:333-455)
   const double* g9[9] = {W.g[0], W.g[1], W.g[2], W.g[3], W.g[4], W.g[5], W.g[6], W.g[7], W.g[8]};
   bool dyn = (cf.optSgs >= 1 && cf.optSgs <= 4) &&
@@ -985,23 +1057,33 @@ static int one_step(alfa_ctx* c, int sgs_mode) {
     st = dynamic_sgs_scalar(c, m15, W.TH, W.gT[0], W.gT[1], W.gT[2], qz_step, W.qz, W.divq,
                             W.Cs2Pr, W.prof + 23 * nz, W.prof + 24 * nz);
     if (st) return st;
+    // moisture: the static scalar flux with heat's new Cs2PrRatio and the
+    // strains dynamicSGSmomentum[19:23] (Main.py:358-369)
+    if (moist)
+      scalar_fluxes(c, mom[20], mom[22], W.Cs2Pr, W.gQ[0], W.gQ[1], W.gQ[2], W.qm_plane, W.qzq,
+                    W.divqm);
   } else {
     double* m10[10] = {W.mom[0], W.mom[1], W.mom[2], W.mom[3], W.mom[4],
                        W.mom[5], W.mom[19], W.mom[20], W.mom[21], W.mom[22]};
     st = static_sgs(c, g9, W.Cs2, W.u, W.v, W.M, W.most[0], W.most[1], W.divt, m10);
     if (st) return st;
     scalar_fluxes(c, m10[7], m10[9], W.Cs2Pr, W.gT[0], W.gT[1], W.gT[2], qz_step, W.qz, W.divq);
+    if (moist)  // Main.py:444-453
+      scalar_fluxes(c, m10[7], m10[9], W.Cs2Pr, W.gQ[0], W.gQ[1], W.gQ[2], W.qm_plane, W.qzq,
+                    W.divqm);
   }
   // RHS (Main.py:464-473)
   double* bars = W.prof + 30 * nz;
   if (cf.optDamping == 1) {
-    const double* f3[3] = {W.u, W.v, W.TH};
-    plane_means(e, f3, 3, bars);
+    const double* f4[4] = {W.u, W.v, W.TH, W.Q};
+    plane_means(e, f4, moist ? 4 : 3, bars);
   }
-  rhs_momentum(e, W.u, W.v, W.w, W.Ug, W.Vg, W.Cx, W.Cy, W.Cz, W.buoy, W.divt[0], W.divt[1],
+  rhs_momentum(e, W.u, W.v, W.w, Ugp, Vgp, W.Cx, W.Cy, W.Cz, W.buoy, W.divt[0], W.divt[1],
                W.divt[2], Uadv, Vadv, bars, bars + nz, W.RHS[0], W.RHS[1], W.RHS[2], itp,
-               3LL * nz);
+               3LL * nz, gtp, 2LL * nz);
   rhs_scalar(e, W.TH, W.THadv, W.divq, THadv, bars + 2 * nz, W.RHS[3], itp, 3LL * nz);
+  if (moist)  // RHS_Moisture (SCL_AllTerms.py:86-110)
+    rhs_scalar(e, W.Q, W.Qadvs, W.divqm, Qadvp, bars + 3 * nz, W.RHSQ, qtp, nz, 1);
   // pressure (Main.py:481-500)
   st = pressure_rc_fn(c, W.u, W.v, W.w, W.RHS[0], W.RHS[1], W.RHS[2], W.RHSp[0], W.RHSp[1],
                       W.RHSp[2], W.divt[2], W.RCr, W.RCi, W.fRzr);
@@ -1014,9 +1096,13 @@ static int one_step(alfa_ctx* c, int sgs_mode) {
   for (int i = 0; i < 4; i++) Rp[i] = (it == cf.istep) ? W.RHS[i] : W.RHSp[i];
   ab2_uvw(e, W.u, W.v, W.w, W.RHS[0], Rp[0], W.RHS[1], Rp[1], W.RHS[2], Rp[2], W.u, W.v, W.w);
   ab2_th(e, W.TH, W.RHS[3], Rp[3], W.TH);
-  if (it == cf.istep)
+  if (moist) ab2_q(e, W.Q, W.RHSQ, (it == cf.istep) ? W.RHSQ : W.RHSQp, W.Q);
+  if (it == cf.istep) {
     for (int i = 0; i < 4; i++)
       cudaMemcpyAsync(W.RHSp[i], W.RHS[i], e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+    if (moist)
+      cudaMemcpyAsync(W.RHSQp, W.RHSQ, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  }
   // CFL (Main.py:534-540): maxima stay on the device, read by alfa_get_diag
   cfl_max(e, W.u, W.v, W.w, W.d_cfl);
   ::alfa::note_launch(); k_add_int<<<1, 1, 0, e.stream>>>(W.d_it, 1);
@@ -1056,6 +1142,14 @@ static int graph_step(alfa_ctx* c) {
   if (it == cf.istep) return one_step(c);
   if (cf.optAdvection >= 1 && it - 1 >= W.series_rows)
     return e.fail("advection series exhausted", ALFA_E_STATE);
+  if (cf.optGeoWind >= 1 && it - 1 >= W.geo_rows)
+    return e.fail("geostrophic wind series exhausted", ALFA_E_STATE);
+  if (cf.optMoisture >= 1 && !W.have_q)
+    return e.fail("optMoisture = 1 needs alfa_init_moisture before stepping", ALFA_E_STATE);
+  if (cf.optMoisture >= 1 && cf.optMoistureSurfBC >= 1 && it - 1 >= W.msfc_rows)
+    return e.fail("moisture surface series exhausted", ALFA_E_STATE);
+  if (cf.optMoisture >= 1 && cf.optAdvection >= 1 && W.series_q && it - 1 >= W.q_rows)
+    return e.fail("moisture advection series exhausted", ALFA_E_STATE);
   if (cf.optSurfBC >= 1 && it - 1 >= (int)W.sfc_series.size())
     return e.fail("surface series exhausted", ALFA_E_STATE);
   const bool dyn = (cf.optSgs >= 1 && cf.optSgs <= 4) && (it % cf.dynamicSGS_call_time == 0);
@@ -1134,6 +1228,9 @@ void alfa_destroy(alfa_ctx* c) {
   if (!c) return;
   if (c->mlp) c->mlp->c = nullptr;  // the network outlives its context only as memory
   if (c->w.series_adv) cudaFree(c->w.series_adv);
+  if (c->w.series_geo) cudaFree(c->w.series_geo);
+  if (c->w.series_q) cudaFree(c->w.series_q);
+  if (c->w.d_msfc) cudaFree(c->w.d_msfc);
   if (c->w.d_sfc) cudaFree(c->w.d_sfc);
   release_graphs(c);
   cudaFree(c->base);
@@ -1296,6 +1393,16 @@ int alfa_potentialTemperatureGradients(alfa_ctx* c, const double* TH, const doub
   return check_launch(e, "potentialTemperatureGradients");
 }
 
+int alfa_moistureGradients(alfa_ctx* c, const double* Q, const double* ustar, const double* qm,
+                           const double* fi_h, double* const out[3]) {
+  CTX_CHECK(c);
+  NN(Q); NN(ustar); NN(qm); NN(fi_h); NN(out); NN(out[0]); NN(out[1]); NN(out[2]);
+  Engine& e = c->e;
+  deriv_field_acc(e, ld_field(e, Q), out[0], 0, out[1], 0);
+  derivz_TH(e, Q, ustar, qm, fi_h, out[2]);
+  return check_launch(e, "moistureGradients");
+}
+
 int alfa_Derivz_Generic_uvp(alfa_ctx* c, const double* F, double* d) {
   CTX_CHECK(c);
   NN(F); NN(d);
@@ -1390,6 +1497,32 @@ int alfa_SurfaceFlux_HeterogeneousPrescribedTemperature(alfa_ctx* c, const doubl
   return surf(c, 5, s, u, v, TH, mi, M, ustar, q2, qavg, invOB, mo);
 }
 
+static int moisture_prescribed(alfa_ctx* c, int het, const double* Q, const double* ustar,
+                               double Qs, const double* const most[6], double* qm,
+                               const char* name) {
+  CTX_CHECK(c);
+  NN(Q); NN(ustar); NN(most); NN(most[2]); NN(most[3]); NN(qm);
+  Engine& e = c->e;
+  const double* qbar0 = nullptr;
+  if (!het) {
+    const double* f1[1] = {Q};
+    plane_means(e, f1, 1, c->w.prof + 44 * e.nz);
+    qbar0 = c->w.prof + 44 * e.nz;
+  }
+  moisture_surface(e, 2, het, Q, ustar, most[2], most[3], nullptr, nullptr, Qs, qbar0, qm);
+  return check_launch(e, name);
+}
+int alfa_SurfaceMoistureFlux_HomogeneousPrescribedQ(alfa_ctx* c, const double* Q,
+    const double* ustar, double Qs, const double* const most[6], double* qm) {
+  return moisture_prescribed(c, 0, Q, ustar, Qs, most, qm,
+                             "SurfaceMoistureFlux_HomogeneousPrescribedQ");
+}
+int alfa_SurfaceMoistureFlux_HeterogeneousPrescribedQ(alfa_ctx* c, const double* Q,
+    const double* ustar, double Qs, const double* const most[6], double* qm) {
+  return moisture_prescribed(c, 1, Q, ustar, Qs, most, qm,
+                             "SurfaceMoistureFlux_HeterogeneousPrescribedQ");
+}
+
 int alfa_Advection(alfa_ctx* c, const double* u, const double* v, const double* w,
                    const double* dudy, const double* dudz, const double* dvdx, const double* dvdz,
                    const double* dwdx, const double* dwdy, double* Cx, double* Cy, double* Cz) {
@@ -1408,17 +1541,17 @@ int alfa_ScalarAdvection(alfa_ctx* c, const double* u, const double* v, const do
   return check_launch(c->e, "ScalarAdvection");
 }
 
-int alfa_BuoyancyOpt1(alfa_ctx* c, const double* TH, double* b) {
+int alfa_BuoyancyOpt1(alfa_ctx* c, const double* TH, const double* H, double* b) {
   CTX_CHECK(c);
   NN(TH); NN(b);
-  buoyancy(c->e, TH, 0, b);
+  buoyancy(c->e, TH, H, 0, b);
   return check_launch(c->e, "BuoyancyOpt1");
 }
 
-int alfa_BuoyancyOpt2(alfa_ctx* c, const double* TH, double* b) {
+int alfa_BuoyancyOpt2(alfa_ctx* c, const double* TH, const double* H, double* b) {
   CTX_CHECK(c);
   NN(TH); NN(b);
-  buoyancy(c->e, TH, 1, b);
+  buoyancy(c->e, TH, H, 1, b);
   return check_launch(c->e, "BuoyancyOpt2");
 }
 
@@ -1514,6 +1647,20 @@ int alfa_RHS_Scalar(alfa_ctx* c, const double* TH, const double* adv, const doub
   }
   rhs_scalar(e, TH, adv, divq, THadv, bar, R);
   return check_launch(e, "RHS_Scalar");
+}
+
+int alfa_RHS_Moisture(alfa_ctx* c, const double* Q, const double* adv, const double* divqm,
+                      const double* Qadv, double* R) {
+  CTX_CHECK(c);
+  NN(Q); NN(adv); NN(divqm); NN(Qadv); NN(R);
+  Engine& e = c->e;
+  double* bar = c->w.prof + 42 * e.nz;
+  if (e.cfg.optDamping == 1) {
+    const double* f1[1] = {Q};
+    plane_means(e, f1, 1, bar);
+  }
+  rhs_scalar(e, Q, adv, divqm, Qadv, bar, R, nullptr, 0, 1);
+  return check_launch(e, "RHS_Moisture");
 }
 
 int alfa_PressureRC(alfa_ctx* c, const double* u, const double* v, const double* w,
@@ -1818,6 +1965,13 @@ int alfa_AB2_TH(alfa_ctx* c, const double* TH, const double* R, const double* Rp
   return check_launch(c->e, "AB2_TH");
 }
 
+int alfa_AB2_Q(alfa_ctx* c, const double* Q, const double* R, const double* Rp, double* out) {
+  CTX_CHECK(c);
+  NN(Q); NN(R); NN(Rp); NN(out);
+  ab2_q(c->e, Q, R, Rp, out);
+  return check_launch(c->e, "AB2_Q");
+}
+
 __global__ void k_fill(double* p, double v, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
 }
@@ -1898,6 +2052,34 @@ int alfa_set_series(alfa_ctx* c, const double* Uadv, const double* Vadv, const d
   return ALFA_OK;
 }
 
+int alfa_set_geowind_series(alfa_ctx* c, const double* Ug, const double* Vg, int nrows) {
+  CTX_CHECK(c);
+  Engine& e = c->e;
+  Work& W = c->w;
+  if (nrows < 0 || (nrows > 0 && (!Ug || !Vg)))
+    return e.fail("set_geowind_series: bad arguments", ALFA_E_SHAPE);
+  const int nz = e.nz;
+  if (W.series_geo) {
+    cudaFree(W.series_geo);
+    W.series_geo = nullptr;
+  }
+  W.geo_rows = 0;
+  if (nrows > 0) {
+    std::vector<double> h((size_t)nrows * 2 * nz);
+    for (int r = 0; r < nrows; r++)
+      for (int k = 0; k < nz; k++) {
+        h[((size_t)r * 2 + 0) * nz + k] = Ug[(size_t)r * nz + k];
+        h[((size_t)r * 2 + 1) * nz + k] = Vg[(size_t)r * nz + k];
+      }
+    if (cudaMalloc(&W.series_geo, h.size() * 8) != cudaSuccess)
+      return e.fail("series allocation failed", ALFA_E_CUDA);
+    cudaMemcpy(W.series_geo, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+    W.geo_rows = nrows;
+  }
+  release_graphs(c);  // captured steps point at the old series
+  return ALFA_OK;
+}
+
 int alfa_step(alfa_ctx* c, int nsteps) {
   CTX_CHECK(c);
   if (!c->w.have_state) return c->e.fail("alfa_step before alfa_init_state", ALFA_E_STATE);
@@ -1916,6 +2098,57 @@ int alfa_step_graph(alfa_ctx* c, int nsteps) {
     if (st) return st;
   }
   return check_launch(c->e, "step_graph");
+}
+
+int alfa_init_moisture(alfa_ctx* c, const double* Q) {
+  CTX_CHECK(c);
+  NN(Q);
+  Engine& e = c->e;
+  Work& W = c->w;
+  if (e.cfg.optMoisture < 1) return e.fail("alfa_init_moisture with optMoisture = 0", ALFA_E_STATE);
+  const size_t N = e.N();
+  cudaMemcpyAsync(W.Q, Q, N * 8, cudaMemcpyDeviceToDevice, e.stream);
+  cudaMemsetAsync(W.RHSQ, 0, N * 8, e.stream);
+  cudaMemsetAsync(W.RHSQp, 0, N * 8, e.stream);
+  // DerivedVars.py:72, the plane every optMoistureSurfBC = 0 step uses
+  ::alfa::note_launch(); k_fill_n<<<64, 256, 0, e.stream>>>(W.qm_plane, e.qm_sfc_const, e.H());
+  W.have_q = 1;
+  return check_launch(e, "init_moisture");
+}
+
+int alfa_set_moisture_series(alfa_ctx* c, const double* Qadv, const double* msfc, int nrows) {
+  CTX_CHECK(c);
+  Engine& e = c->e;
+  Work& W = c->w;
+  if (nrows < 0) return e.fail("set_moisture_series: bad arguments", ALFA_E_SHAPE);
+  if (W.series_q) cudaFree(W.series_q);
+  if (W.d_msfc) cudaFree(W.d_msfc);
+  W.series_q = nullptr;
+  W.d_msfc = nullptr;
+  W.q_rows = W.msfc_rows = 0;
+  if (Qadv && nrows > 0) {
+    if (cudaMalloc(&W.series_q, (size_t)nrows * e.nz * 8) != cudaSuccess)
+      return e.fail("series allocation failed", ALFA_E_CUDA);
+    cudaMemcpy(W.series_q, Qadv, (size_t)nrows * e.nz * 8, cudaMemcpyHostToDevice);
+    W.q_rows = nrows;
+  }
+  if (msfc && nrows > 0) {
+    if (cudaMalloc(&W.d_msfc, (size_t)nrows * 8) != cudaSuccess)
+      return e.fail("series allocation failed", ALFA_E_CUDA);
+    cudaMemcpy(W.d_msfc, msfc, (size_t)nrows * 8, cudaMemcpyHostToDevice);
+    W.msfc_rows = nrows;
+  }
+  release_graphs(c);  // captured steps point at the old series
+  return ALFA_OK;
+}
+
+int alfa_get_moisture(alfa_ctx* c, double* Q) {
+  CTX_CHECK(c);
+  NN(Q);
+  Engine& e = c->e;
+  if (e.cfg.optMoisture < 1) return e.fail("alfa_get_moisture with optMoisture = 0", ALFA_E_STATE);
+  cudaMemcpyAsync(Q, c->w.Q, e.N() * 8, cudaMemcpyDeviceToDevice, e.stream);
+  return check_launch(e, "get_moisture");
 }
 
 int alfa_get_state(alfa_ctx* c, double* u, double* v, double* w, double* TH, double* p) {
@@ -1988,14 +2221,16 @@ int alfa_stats_sample(alfa_ctx* c, double* acc) {
                            W.prof + 24 * nz, acc);
 }
 
-// checkpoint layout: u v w TH p RHS[4] Cs2 Cs2Pr (N each), most[6] (H each),
+// checkpoint layout: u v w TH p RHS[4] Cs2 Cs2Pr (N each), Q RHS_Q (N each, when
+// optMoisture = 1), most[6] (H each),
 // profiles (PROF doubles), then iteration and CFLmax
 static size_t ckpt_prof(const Engine& e) { return (size_t)64 * e.nz + 64; }
 
 size_t alfa_checkpoint_doubles(const alfa_ctx* c) {
   if (!c) return 0;
   const Engine& e = c->e;
-  return 11 * e.N() + 6 * e.H() + ckpt_prof(e) + 2;
+  const size_t nf = e.cfg.optMoisture >= 1 ? 13 : 11;  // + Q, RHS_Q when moist
+  return nf * e.N() + 6 * e.H() + ckpt_prof(e) + 2;
 }
 
 static int checkpoint_copy(alfa_ctx* c, double* buf, bool save) {
@@ -2013,6 +2248,10 @@ static int checkpoint_copy(alfa_ctx* c, double* buf, bool save) {
     off += n;
   };
   for (double* p : f) mv(p, N);
+  if (e.cfg.optMoisture >= 1) {
+    mv(W.Q, N);
+    mv(W.RHSQ, N);
+  }
   for (int i = 0; i < 6; i++) mv(W.most[i], H);
   mv(W.prof, ckpt_prof(e));
   double tail[2] = {(double)W.iteration, W.CFLmax};
@@ -2027,6 +2266,10 @@ static int checkpoint_copy(alfa_ctx* c, double* buf, bool save) {
     W.iteration = (int)tail[0];
     W.CFLmax = tail[1];
     W.have_state = 1;
+    if (e.cfg.optMoisture >= 1) {
+      W.have_q = 1;
+      ::alfa::note_launch(); k_fill_n<<<64, 256, 0, e.stream>>>(W.qm_plane, e.qm_sfc_const, H);
+    }
     ::alfa::note_launch(); k_set_int<<<1, 1, 0, e.stream>>>(W.d_it, W.iteration);
   }
   return ALFA_OK;
@@ -2086,6 +2329,11 @@ static int ens_graph_step(alfa_ensemble* E) {
         ((cf.optSgs >= 1 && cf.optSgs <= 4) != (cf0.optSgs >= 1 && cf0.optSgs <= 4)))
       return 1;
     if (cf.optAdvection >= 1 && it - 1 >= c->w.series_rows) return 1;
+    if (cf.optGeoWind >= 1 && it - 1 >= c->w.geo_rows) return 1;
+    if (cf.optMoisture >= 1 &&
+        (!c->w.have_q || (cf.optMoistureSurfBC >= 1 && it - 1 >= c->w.msfc_rows) ||
+         (cf.optAdvection >= 1 && c->w.series_q && it - 1 >= c->w.q_rows)))
+      return 1;
     if (cf.optSurfBC >= 1 && it - 1 >= (int)c->w.sfc_series.size()) return 1;
   }
   if (it == cf0.istep) return 1;

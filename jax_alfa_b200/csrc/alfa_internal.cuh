@@ -105,6 +105,10 @@ struct Engine {
   int nx, ny, nz, mx, my, nxh, nyh, mxh, myh;
   // DerivedVars (src/config/DerivedVars.py:48-112), in the reference's order
   double z_scale, g_nondim, f_nondim, T0_nondim, inversion_nondim, qz_sfc_const;
+  // moisture (DerivedVars.py:69-75; SurfaceFlux.py:475-476): q_inversion
+  // non-dimensional, the constant surface moisture flux, and
+  // log(0.5 dz z_scale / z_ref) of the prescribed-Q flux
+  double q_inversion_nondim = 0, qm_sfc_const = 0, log_zq = 0;
   double dx, dy, dz, idz, L, dt_nondim, TFR;
   int optDealias;
   double Cs2_init, Cs2PrRatio_init, z_damping_nondim, RelaxTime_nondim;

@@ -343,15 +343,21 @@ void divergence_finish(Engine& e, double* div, const double* fz, int w_nodes) {
 // ---------------------------------------------------------------------------
 // buoyancy: NSE_BuoyancyTerms.py:49-150 (dry, H = 0)
 // ---------------------------------------------------------------------------
-__global__ void k_buoy(const double* __restrict__ TH, const double* __restrict__ bar, double* out,
-                       size_t n, int nz, double T0, int by_mean, double hg) {
+__device__ __forceinline__ double thv_of(const double* __restrict__ TH,
+                                        const double* __restrict__ H, size_t i, double T0) {
+  return (TH[i] + T0) * (H ? __dadd_rn(1.0, __dmul_rn(0.61, H[i])) : 1.0);
+}
+
+__global__ void k_buoy(const double* __restrict__ TH, const double* __restrict__ H,
+                       const double* __restrict__ bar, double* out, size_t n, int nz, double T0,
+                       int by_mean, double hg) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     if (z == 0) {
       out[i] = 0.0;
     } else {
       const double b1 = bar[z], b0 = bar[z - 1];
-      const double t1 = (TH[i] + T0) * 1.0, t0 = (TH[i - 1] + T0) * 1.0;
+      const double t1 = thv_of(TH, H, i, T0), t0 = thv_of(TH, H, i - 1, T0);
       const double n1 = (t1 - b1) / (by_mean ? b1 : T0);
       const double n0 = (t0 - b0) / (by_mean ? b0 : T0);
       out[i] = hg * (n1 + n0);
@@ -359,18 +365,49 @@ __global__ void k_buoy(const double* __restrict__ TH, const double* __restrict__
   }
 }
 
-__global__ void k_add_const(const double* __restrict__ a, double c, double* out, size_t n) {
-  GRID_STRIDE(i, n) { out[i] = (a[i] + c) * 1.0; }
+__global__ void k_thv(const double* __restrict__ TH, const double* __restrict__ H, double T0,
+                      double* out, size_t n) {
+  GRID_STRIDE(i, n) { out[i] = thv_of(TH, H, i, T0); }
 }
 
-void buoyancy(Engine& e, const double* TH, int opt, double* out) {
-  // THv = (TH + T_0)(1 + 0.61 H), H = 0; its plane mean
+void buoyancy(Engine& e, const double* TH, const double* H, int opt, double* out) {
+  // THv = (TH + T_0)(1 + 0.61 H) and its plane mean
   double* thv = e.W;  // first workspace field
-  ::alfa::note_launch(); k_add_const<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.T0_nondim, thv, e.N());
+  ::alfa::note_launch(); k_thv<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, H, e.T0_nondim, thv, e.N());
   const double* f[1] = {thv};
   plane_means(e, f, 1, e.scal);
-  ::alfa::note_launch(); k_buoy<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, e.scal, out, e.N(), e.nz, e.T0_nondim, opt,
-                                                0.5 * e.g_nondim);
+  ::alfa::note_launch(); k_buoy<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, H, e.scal, out, e.N(), e.nz,
+                                                                      e.T0_nondim, opt,
+                                                                      0.5 * e.g_nondim);
+}
+
+// surface moisture flux (Main.py:253-267; SurfaceFlux.py:447-504):
+// qm = ustar vonk (Q_s - Q_air) / (log(0.5 dz z_scale / z_ref) + psi_h - psi_h0)
+__global__ void k_moisture_surface(int mode, int het, const double* __restrict__ Q,
+                                   const double* __restrict__ ustar,
+                                   const double* __restrict__ psi_h,
+                                   const double* __restrict__ psi_h0,
+                                   const double* __restrict__ series, const int* itp,
+                                   double q_host, const double* __restrict__ qbar0, double log_zq,
+                                   double* qm, size_t H, int nz) {
+  const double s = series ? series[*itp - 1] : q_host;
+  GRID_STRIDE(r, H) {
+    if (mode == 1) {
+      qm[r] = s;
+    } else {
+      const double qa = het ? Q[r * nz] : qbar0[0];
+      qm[r] = ustar[r] * 0.4 * (s - qa) / (log_zq + psi_h[r] - psi_h0[r]);
+    }
+  }
+}
+
+void moisture_surface(Engine& e, int mode, int het, const double* Q, const double* ustar,
+                      const double* psi_h, const double* psi_h0, const double* series,
+                      const int* itp, double q_host, const double* qbar0, double* qm) {
+  ::alfa::note_launch();
+  k_moisture_surface<<<nblocks(e.H()), TPB, 0, e.stream>>>(mode, het, Q, ustar, psi_h, psi_h0,
+                                                           series, itp, q_host, qbar0, e.log_zq,
+                                                           qm, e.H(), e.nz);
 }
 
 // ---------------------------------------------------------------------------
@@ -1255,13 +1292,16 @@ struct RhsM {
   int adv, damp;
   const int* itp;   // non-null: the forcing profiles are row (*itp - 1) of a series
   long long rs;     // row stride of that series
+  const int* gtp;   // non-null: Ug, Vg are row (*gtp - 1) of the geostrophic series
+  long long grs;    // row stride of that series
 };
 
 __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
+  const size_t grow = a.gtp ? (size_t)(*a.gtp - 1) * a.grs : 0;
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
-    double ru = -a.Cx[i] - a.dx[i] - a.f * (a.Vg[z] - a.v[i]);
-    double rv = -a.Cy[i] - a.dy[i] + a.f * (a.Ug[z] - a.Ugal - a.u[i]);
+    double ru = -a.Cx[i] - a.dx[i] - a.f * (a.Vg[grow + z] - a.v[i]);
+    double rv = -a.Cy[i] - a.dy[i] + a.f * (a.Ug[grow + z] - a.Ugal - a.u[i]);
     double rw = -a.Cz[i] - a.dz[i] + a.b[i];
     if (a.adv) {
       const size_t row = a.itp ? (size_t)(*a.itp - 1) * a.rs : 0;
@@ -1284,10 +1324,10 @@ void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
                   const double* Cz, const double* b, const double* dx, const double* dy,
                   const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
                   const double* vbar, double* Ru, double* Rv, double* Rw, const int* itp,
-                  long long rs) {
+                  long long rs, const int* gtp, long long grs) {
   RhsM a{u, v, w, Ug, Vg, Cx, Cy, Cz, b, dx, dy, dz, Uadv, Vadv, ubar, vbar, e.d_rd, e.d_rd_stag,
          Ru, Rv, Rw, e.f_nondim, e.cfg.Ugal, e.cfg.optAdvection >= 1, e.cfg.optDamping == 1, itp,
-         rs};
+         rs, gtp, grs};
   ::alfa::note_launch(); k_rhs_m<<<nblocks(e.N()), TPB, 0, e.stream>>>(a, e.N(), e.nz);
 }
 
@@ -1307,9 +1347,10 @@ __global__ void k_rhs_s(const double* __restrict__ TH, const double* __restrict_
 
 void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
                 const double* THadv, const double* THbar, double* R, const int* itp,
-                long long rs) {
+                long long rs, int always_adv) {
   ::alfa::note_launch(); k_rhs_s<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, adv, divq, THadv, THbar, e.d_rd_stag, R,
-                                                 e.N(), e.nz, e.cfg.optAdvection >= 1,
+                                                 e.N(), e.nz,
+                                                 always_adv || e.cfg.optAdvection >= 1,
                                                  e.cfg.optDamping == 1, itp, rs);
 }
 
@@ -1455,6 +1496,11 @@ void ab2_uvw(Engine& e, const double* u, const double* v, const double* w, const
 void ab2_th(Engine& e, const double* TH, const double* R, const double* Rp, double* out) {
   ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
                                                e.inversion_nondim * e.dz);
+}
+
+void ab2_q(Engine& e, const double* Q, const double* R, const double* Rp, double* out) {
+  ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(Q, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
+                                               e.q_inversion_nondim * e.dz);
 }
 
 // max |u|, |v|, |w| (Main.py:534-537)

@@ -36,7 +36,17 @@ void derivz_TH(Engine& e, const double* TH, const double* ustar, const double* q
 void derivz_generic(Engine& e, const double* F, int w_nodes, double* out);
 
 // ---- buoyancy ------------------------------------------------------------
-void buoyancy(Engine& e, const double* TH, int opt, double* out);
+// H: the specific humidity (THv = (TH + T_0)(1 + 0.61 H)), or null (dry)
+void buoyancy(Engine& e, const double* TH, const double* H, int opt, double* out);
+
+// ---- surface moisture flux (Main.py:253-267, SurfaceFlux.py:447-504) -----
+// mode 1: the flux series value; mode 2: from the prescribed surface
+// humidity (het: per column, else against the plane mean qbar0 of Q's first
+// level).  The series value is series[*itp - 1] when series is given, else
+// q_host.
+void moisture_surface(Engine& e, int mode, int het, const double* Q, const double* ustar,
+                      const double* psi_h, const double* psi_h0, const double* series,
+                      const int* itp, double q_host, const double* qbar0, double* qm);
 
 // ---- strains -------------------------------------------------------------
 // uvp nodes: S12, S13, S23, |S| (S11, S22, S33 are dudx, dvdy, dwdz)
@@ -112,12 +122,15 @@ void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
                   const double* Cz, const double* b, const double* dx, const double* dy,
                   const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
                   const double* vbar, double* Ru, double* Rv, double* Rw,
-                  const int* itp = nullptr, long long rs = 0);
+                  const int* itp = nullptr, long long rs = 0, const int* gtp = nullptr,
+                  long long grs = 0);
 // itp / rs: when given, the forcing profiles are row (*itp - 1) of a series
 // with row stride rs (read on the device)
 void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
                 const double* THadv, const double* THbar, double* R, const int* itp = nullptr,
-                long long rs = 0);
+                long long rs = 0, int always_adv = 0);
+// always_adv: add the forcing profile whatever optAdvection is (RHS_Moisture,
+// SCL_AllTerms.py:103, adds Qadv unconditionally)
 void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const cd* fbot,
                  const cd* ftop, double* RCr, double* RCi, double* fRz_real);
 void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double* fRz_real,
@@ -128,6 +141,8 @@ void ab2_uvw(Engine& e, const double* u, const double* v, const double* w, const
              const double* Rup, const double* Rv, const double* Rvp, const double* Rw,
              const double* Rwp, double* un, double* vn, double* wn);
 void ab2_th(Engine& e, const double* TH, const double* R, const double* Rp, double* out);
+// AB2_Q (SCL_TimeAdvancement.py:79-99): the q_inversion top condition
+void ab2_q(Engine& e, const double* Q, const double* R, const double* Rp, double* out);
 void cfl_max(Engine& e, const double* u, const double* v, const double* w, double* out3);
 void copy_planes_z(Engine& e, const double* F, int k0, int k1, double* out2);
 void imfilter(Engine& e, const double* F, double* out);

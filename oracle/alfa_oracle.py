@@ -78,6 +78,10 @@ class AlfaOracle:
         self.T_0_nondim = c["T_0"] / self.TH_scale
         self.inversion_nondim = c["inversion"] * (self.z_scale / self.TH_scale)
         self.qz_sfc = c["SensibleHeatFlux"] * np.ones((nx, ny)) / (self.u_scale * self.TH_scale)
+        # moisture (DerivedVars.py:69-75)
+        self.Q_scale = 1
+        self.qm_sfc = c.get("MoistureFlux", 0.0) * np.ones((nx, ny)) / (self.u_scale * self.Q_scale)
+        self.q_inversion_nondim = c.get("q_inversion", 0.0) * (self.z_scale / self.Q_scale)
         self.dx = 2 * PI / nx
         self.dy = 2 * PI / ny
         self.dz = (c["l_z"] / self.z_scale) / (nz - 1)
@@ -239,6 +243,10 @@ class AlfaOracle:
         dTHdy = self.Derivxy(T, ky2)
         dTHdz = self.Derivz_TH(TH, ustar, qz_sfc, MOSTfunctions[5])
         return dTHdx, dTHdy, dTHdz
+
+    def moistureGradients(self, Q, kx2, ky2, ustar, qm_sfc, MOSTfunctions, ZeRo3D=None):
+        """``Derivatives.py:281-306``: the theta form with the moisture flux."""
+        return self.potentialTemperatureGradients(Q, kx2, ky2, ustar, qm_sfc, MOSTfunctions)
 
     # ------------------------------------------------------------------
     # src/utilities/Utilities.py:41-241
@@ -428,6 +436,22 @@ class AlfaOracle:
         TH_ref = (np.mean(th_air) + self.T_0_nondim) * np.ones((self.nx, self.ny))
         MOST, invOB = self._update_MOSTfunctions(ustar, qavg, TH_ref, psi_m, psi_m0, psi_h, psi_h0)
         return M, ustar, q2, qavg, invOB, MOST
+
+    # src/surface/SurfaceFlux.py:447-504 (optMoistureSurfBC = 2)
+    def _denom_q(self, psi_h, psi_h0):
+        z = self.cfg.get("zMoisture", 0.0)
+        zref = z if z > 0.0 else self.cfg["z0T"]
+        return np.log(0.5 * self.dz * self.z_scale / zref) + psi_h - psi_h0
+
+    def SurfaceMoistureFlux_HomogeneousPrescribedQ(self, Q, ustar, Q_sfc_t, MOST):
+        one = np.ones((self.nx, self.ny))
+        psi_h, psi_h0 = MOST[2], MOST[3]
+        q_air = np.mean(Q[:, :, 0])
+        return ustar * VONK * (Q_sfc_t - q_air) * one / self._denom_q(psi_h, psi_h0)
+
+    def SurfaceMoistureFlux_HeterogeneousPrescribedQ(self, Q, ustar, Q_sfc_t, MOST):
+        psi_h, psi_h0 = MOST[2], MOST[3]
+        return ustar * VONK * (Q_sfc_t - Q[:, :, 0]) / self._denom_q(psi_h, psi_h0)
 
     # ------------------------------------------------------------------
     # src/pde/NSE_AdvectionTerms.py:65-155 (3/2-rule dealiased form)
@@ -1212,6 +1236,14 @@ class AlfaOracle:
             r = r - RayleighDampCoeff_stag * (TH - self.PlanarMean(TH).reshape(1, 1, -1))
         return r
 
+    def RHS_Moisture(self, Q, QAdvectionSum, divqm, RayleighDampCoeff_stag, Qadv):
+        """``SCL_AllTerms.py:86-110``: Qadv is always added (zero when no
+        forcing is prescribed)."""
+        r = -QAdvectionSum - divqm + Qadv
+        if self.cfg["optDamping"] == 1:
+            r = r - RayleighDampCoeff_stag * (Q - self.PlanarMean(Q).reshape(1, 1, -1))
+        return r
+
     # ------------------------------------------------------------------
     # src/pde/NSE_PressureTerms.py:55-335, NSE_PressureTerms_Thomas.py:74-292
     # ------------------------------------------------------------------
@@ -1349,6 +1381,13 @@ class AlfaOracle:
         t[:, :, nz - 1] = t[:, :, nz - 2] + self.inversion_nondim * self.dz
         return t
 
+    def AB2_Q(self, Q, R, Rp):
+        """``SCL_TimeAdvancement.py:79-99``."""
+        dt, nz = self.dt_nondim, self.nz
+        q = Q + dt * (1.5 * R - 0.5 * Rp)
+        q[:, :, nz - 1] = q[:, :, nz - 2] + self.q_inversion_nondim * self.dz
+        return q
+
     # ------------------------------------------------------------------
     # src/initialization/Initialization.py:58-460
     # ------------------------------------------------------------------
@@ -1379,6 +1418,11 @@ class AlfaOracle:
         if self.cfg["optSurfBC"] == 1:
             return series_dim / (self.u_scale * self.TH_scale)
         return (series_dim - self.cfg["T_0"]) / self.TH_scale
+
+    def geowind_series(self, Ug, Vg):
+        """``Initialize_GeoWind_Varying`` non-dimensionalisation
+        (``Initialization.py:241-244``): (nsteps+1, nz) rows / u_scale."""
+        return np.asarray(Ug) / self.u_scale, np.asarray(Vg) / self.u_scale
 
     def adv_series(self, U, V, T):
         """``Initialize_AdvForcing`` non-dimensionalisation (``:305-314``)."""
@@ -1477,10 +1521,15 @@ def ComputeStats(o, u, v, w, TH, dudz, dvdz, dTHdz, M_sfc_loc, ustar, qz_sfc_avg
 
 class OracleRun:
     """The time loop of ``src/Main.py:46-541`` on the oracle (dry, optSgs 0-4,
-    constant geostrophic wind).  ``step()`` advances one iteration
+    constant or time/height-varying geostrophic wind).  ``step()`` advances one iteration
     and keeps the same state variables Main.py keeps between iterations."""
 
-    def __init__(self, cfg, u, v, w, th, surface_series=None, adv=None):
+    def __init__(self, cfg, u, v, w, th, surface_series=None, adv=None, geowind=None,
+                 Q=None, moisture_series=None):
+        """Q: the initial specific humidity (kg/kg, as Initialize_Q loads it)
+        when optMoisture >= 1; moisture_series: the non-dimensional
+        Initialize_MoistureSurfaceBC series (optMoistureSurfBC >= 1); adv may
+        carry a fourth, Qadv, series."""
         o = self.o = AlfaOracle(cfg)
         self.cfg = o.cfg
         self.kx2, self.ky2 = o.Wavenumber()
@@ -1499,6 +1548,12 @@ class OracleRun:
         self.MOST = (z2.copy(), z2.copy(), z2.copy(), z2.copy(), 1.0 + z2, 1.0 + z2)
         self.surface = surface_series
         self.adv = adv
+        self.geowind = geowind  # non-dimensional (Ug, Vg) rows when optGeoWind >= 1
+        self.moist = int(cfg.get("optMoisture", 0)) >= 1
+        if self.moist:  # Main.py:71-76
+            self.Q = np.array(Q, dtype=np.float64)
+            self.RHS_prev.append(np.zeros(shp))
+            self.moisture_series = moisture_series
         self.Cs2_3D = o.Cs2_init * np.ones(shp)
         self.Cs2PrRatio_3D = o.Cs2PrRatio_init * np.ones(shp)
         self.iteration = int(cfg["istep"])
@@ -1515,17 +1570,26 @@ class OracleRun:
         zero3 = None
         if it > self.istep:
             self.RHS_prev = list(self.RHS)
+        if c.get("optGeoWind", 0) >= 1:  # Main.py:170-174
+            GU, GV = self.geowind
+            self.Ug = np.broadcast_to(GU[it - 1].reshape(1, 1, nz), self.u.shape)
+            self.Vg = np.broadcast_to(GV[it - 1].reshape(1, 1, nz), self.u.shape)
+        Qadv = np.zeros(self.u.shape)
         if c["optAdvection"] >= 1:
-            U, V, T = self.adv
+            U, V, T = self.adv[:3]
             Uadv = np.broadcast_to(U[it - 1].reshape(1, 1, nz), self.u.shape)
             Vadv = np.broadcast_to(V[it - 1].reshape(1, 1, nz), self.u.shape)
             THadv = np.broadcast_to(T[it - 1].reshape(1, 1, nz), self.u.shape)
+            if self.moist and len(self.adv) > 3:
+                Qadv = np.broadcast_to(self.adv[3][it - 1].reshape(1, 1, nz), self.u.shape)
         else:
             Uadv = Vadv = THadv = np.zeros(self.u.shape)
         u, u_fft = o.Filtering_Explicit(o.FFT(self.u))
         v, v_fft = o.Filtering_Explicit(o.FFT(self.v))
         w, w_fft = o.Filtering_Explicit(o.FFT(self.w))
         TH, _ = o.Filtering_Explicit(o.FFT(self.TH))
+        if self.moist:
+            Q, _ = o.Filtering_Explicit(o.FFT(self.Q))
         if c["optSurfBC"] == 0:
             f = (o.SurfaceFlux_HomogeneousConstantFlux if c["optSurfFlux"] == 0
                  else o.SurfaceFlux_HeterogeneousConstantFlux)
@@ -1540,6 +1604,16 @@ class OracleRun:
                 f = (o.SurfaceFlux_HomogeneousPrescribedTemperature if c["optSurfFlux"] == 0
                      else o.SurfaceFlux_HeterogeneousPrescribedTemperature)
             M, ustar, qz_step, qavg, invOB, self.MOST = f(u, v, TH, val, self.MOST)
+        if self.moist:  # Main.py:253-267
+            mb = c.get("optMoistureSurfBC", 0)
+            if mb == 0:
+                qm_step = o.qm_sfc
+            elif mb == 1:
+                qm_step = self.moisture_series[it - 1] * np.ones((o.nx, o.ny))
+            else:
+                fq = (o.SurfaceMoistureFlux_HomogeneousPrescribedQ if c["optSurfFlux"] == 0
+                      else o.SurfaceMoistureFlux_HeterogeneousPrescribedQ)
+                qm_step = fq(Q, ustar, self.moisture_series[it - 1], self.MOST)
         grads = o.velocityGradients(u, v, w, u_fft, v_fft, w_fft, self.kx2, self.ky2,
                                     ustar, M, self.MOST)
         dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz = grads
@@ -1547,7 +1621,11 @@ class OracleRun:
                                                               qz_step, self.MOST)
         Cx, Cy, Cz = o.Advection(u, v, w, dudy, dudz, dvdx, dvdz, dwdx, dwdy)
         THadvsum = o.ScalarAdvection(u, v, w, dTHdx, dTHdy, dTHdz)
-        H = np.zeros(u.shape)
+        if self.moist:
+            dQdx, dQdy, dQdz = o.moistureGradients(Q, self.kx2, self.ky2, ustar, qm_step,
+                                                   self.MOST)
+            Qadvsum = o.ScalarAdvection(u, v, w, dQdx, dQdy, dQdz)
+        H = Q if self.moist else np.zeros(u.shape)
         buoy = o.BuoyancyOpt1(TH, H) if c["optBuoyancy"] == 0 else o.BuoyancyOpt2(TH, H)
         dyn = 1 <= o.optSgs <= 4 and (it == self.istep or it % c["dynamicSGS_call_time"] == 0)
         if dyn:
@@ -1557,14 +1635,21 @@ class OracleRun:
             qz, divq, self.Cs2PrRatio_3D, self.Cs2PrRatio_1D, self.beta2_1D = \
                 o.DivFluxDynamicSGS(mom[10:], TH, dTHdx, dTHdy, dTHdz, qz_step,
                                     zero3, zero3, zero3, self.kx2, self.ky2)
+            strains = mom[19:23]
         else:
             divtx, divty, divtz, mom = o.DivStressStaticSGS(
                 *grads, self.Cs2_3D, u, v, M, self.MOST, zero3, zero3, zero3, self.kx2, self.ky2)
             qz, divq = o.DivFluxStaticSGS(mom[6:], self.Cs2PrRatio_3D, dTHdx, dTHdy, dTHdz,
                                           qz_step, zero3, zero3, zero3, self.kx2, self.ky2)
+            strains = mom[6:]
+        if self.moist:  # Main.py:358-369, 444-453: heat's Cs2PrRatio and strains
+            qHz_q, divqm = o.DivFluxStaticSGS(strains, self.Cs2PrRatio_3D, dQdx, dQdy, dQdz,
+                                              qm_step, zero3, zero3, zero3, self.kx2, self.ky2)
         Ru, Rv, Rw = o.RHS_Momentum(u, v, w, self.Ug, self.Vg, Cx, Cy, Cz, buoy,
                                     divtx, divty, divtz, self.Rd, self.Rd_stag, Uadv, Vadv)
         RT = o.RHS_Scalar(TH, THadvsum, divq, self.Rd_stag, THadv)
+        if self.moist:
+            RQ = o.RHS_Moisture(Q, Qadvsum, divqm, self.Rd_stag, Qadv)
         RCr, RCi, fRz = o.PressureRC(u, v, w, Ru, Rv, Rw, *self.RHS_prev[:3], divtz,
                                      self.kr2, self.kc2)
         if c["optPressureSolver"] == 1:
@@ -1573,12 +1658,15 @@ class OracleRun:
         else:
             p, dpdx, dpdy, dpdz = o.PressureSolve(RCr, RCi, fRz, self.a_p, self.b_p, self.c_p)
         Ru, Rv, Rw = Ru - dpdx, Rv - dpdy, Rw - dpdz
-        self.RHS = [Ru, Rv, Rw, RT]
+        self.RHS = [Ru, Rv, Rw, RT] + ([RQ] if self.moist else [])
         if it == self.istep:
             self.RHS_prev = list(self.RHS)
         self.u, self.v, self.w = o.AB2_uvw(u, v, w, Ru, self.RHS_prev[0], Rv, self.RHS_prev[1],
                                            Rw, self.RHS_prev[2])
         self.TH = o.AB2_TH(TH, RT, self.RHS_prev[3])
+        if self.moist:
+            self.Q = o.AB2_Q(Q, RQ, self.RHS_prev[4])
+            self.last.update(Q_filtered=Q, dQdz=dQdz, qHz_q=qHz_q, qm_sfc_step=qm_step)
         self.p = p
         cfl = max(np.max(np.abs(self.u)) * o.dt_nondim / o.dx,
                   np.max(np.abs(self.v)) * o.dt_nondim / o.dy,

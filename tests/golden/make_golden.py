@@ -43,22 +43,25 @@ TAPPED = {
         "SurfaceFlux_HomogeneousConstantFlux", "SurfaceFlux_HeterogeneousConstantFlux",
         "SurfaceFlux_HomogeneousVaryingFlux", "SurfaceFlux_HeterogeneousVaryingFlux",
         "SurfaceFlux_HomogeneousPrescribedTemperature",
-        "SurfaceFlux_HeterogeneousPrescribedTemperature"],
-    "src.operations.Derivatives": ["velocityGradients", "potentialTemperatureGradients"],
+        "SurfaceFlux_HeterogeneousPrescribedTemperature",
+        "SurfaceMoistureFlux_HomogeneousPrescribedQ",
+        "SurfaceMoistureFlux_HeterogeneousPrescribedQ"],
+    "src.operations.Derivatives": ["velocityGradients", "potentialTemperatureGradients",
+                                   "moistureGradients"],
     "src.pde.NSE_AdvectionTerms": ["Advection"],
     "src.pde.SCL_AdvectionTerms": ["ScalarAdvection"],
     "src.pde.NSE_BuoyancyTerms": ["BuoyancyOpt1", "BuoyancyOpt2"],
     "src.pde.NSE_SGSTerms": ["DivStressDynamicSGS", "DivStressStaticSGS"],
     "src.pde.SCL_SGSTerms": ["DivFluxDynamicSGS", "DivFluxStaticSGS"],
     "src.pde.NSE_AllTerms": ["RHS_Momentum"],
-    "src.pde.SCL_AllTerms": ["RHS_Scalar"],
+    "src.pde.SCL_AllTerms": ["RHS_Scalar", "RHS_Moisture"],
     "src.pde.NSE_PressureTerms": ["PressureRC", "PressureSolve"],
     "src.pde.NSE_PressureTerms_Thomas": ["ThomasPressureSolve"],
     "src.pde.NSE_TimeAdvancement": ["AB2_uvw"],
-    "src.pde.SCL_TimeAdvancement": ["AB2_TH"],
+    "src.pde.SCL_TimeAdvancement": ["AB2_TH", "AB2_Q"],
 }
 
-FINAL_NAMES = ["u", "v", "w", "TH", "p", "dpdx", "dpdy", "dpdz",
+FINAL_NAMES = ["u", "v", "w", "TH", "Q", "p", "dpdx", "dpdy", "dpdz",
                "RHS_u", "RHS_v", "RHS_w", "RHS_TH", "Cs2_3D", "Cs2PrRatio_3D",
                "beta1_1D", "beta2_1D", "Cs2_1D_avg1", "Cs2_1D_avg2", "Cs2PrRatio_1D",
                "ustar", "M_sfc_loc", "qz_sfc_avg", "psi2D_m", "psi2D_m0",
@@ -100,6 +103,8 @@ def run(case, grid, steps, record, out_path, seed, overrides, final_names=FINAL_
 
     import importlib
     state = {"iteration": 1}
+    # the last state update of an iteration (Main.py:522-528)
+    last_update = "AB2_Q" if int(cfg.get("optMoisture", 0)) >= 1 else "AB2_TH"
     calls = {}
     rec = {}
 
@@ -115,7 +120,7 @@ def run(case, grid, steps, record, out_path, seed, overrides, final_names=FINAL_
                 _flatten(f"{fname}.{c}.out", res if isinstance(res, tuple) else (res,), d)
                 rec.update({k.replace(".out.", ".out"): v for k, v in d.items()})
                 rec[f"{fname}.{c}.iteration"] = np.array(state["iteration"])
-            if fname == "AB2_TH":
+            if fname == last_update:
                 state["iteration"] += 1
             return res
         return wrapped

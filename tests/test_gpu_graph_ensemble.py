@@ -13,7 +13,16 @@ def _sim(cfg, seed=0):
     u, v, w, th = cases.initial_fields(cfg, seed)
     adv = cases.adv_forcing_series(cfg) if cfg["optAdvection"] else None
     sfc = cases.surface_bc_series(cfg) if cfg["optSurfBC"] else None
-    return Simulation(cfg, u, v, w, th, surface_series=sfc, adv_series=adv)
+    geo = cases.geowind_series(cfg) if cfg["optGeoWind"] else None
+    moist = {}
+    if cfg["optMoisture"]:
+        moist["Q"] = cases.initial_moisture(cfg, seed)
+        if cfg["optMoistureSurfBC"]:
+            moist["moisture_series"] = cases.moisture_surface_series(cfg)
+        if adv is not None:
+            adv = adv + (cases.adv_moisture_series(cfg),)
+    return Simulation(cfg, u, v, w, th, surface_series=sfc, adv_series=adv, geowind_series=geo,
+                      **moist)
 
 
 def _state(sim):
@@ -24,6 +33,9 @@ def _state(sim):
     ("neutral", (32, 32, 32), {}),                                # advection forcing series
     ("stable", (24, 24, 16), {}),                                 # surface temperature series
     ("convective", (24, 24, 16), {"dynamicSGS_call_time": 3}),    # dynamic and static steps
+    ("stable", (24, 24, 16), {"optGeoWind": 1}),                  # geostrophic wind series
+    ("neutral", (24, 24, 16), {"optMoisture": 1, "optMoistureSurfBC": 1,
+                               "MoistureFlux": 5e-5}),            # moisture with Qadv
 ])
 def test_graph_step_equals_direct_step(case, grid, over):
     cfg = cases.CASES[case](*grid, nsteps=7, **over)

@@ -45,7 +45,13 @@ FIXTURES = [
     ("ref_convective_wl_12x12x8.npz", "convective"),  # LASDD-WL (optSgs = 2)
     ("ref_stable_wl4_12x12x8.npz", "stable"),  # LAD-WL (optSgs = 4)
     ("ref_convective_wl_fgr2_12x12x8.npz", "convective"),  # LASDD-WL, FGR = 2
+    ("ref_stable_geo_12x12x8.npz", "stable"),  # time/height-varying geostrophic wind
+    ("ref_convective_moist_12x12x8.npz", "convective"),  # moisture, constant flux, Qadv
+    ("ref_stable_moistq_12x12x8.npz", "stable"),  # moisture, prescribed surface Q
+    ("ref_convective_moistq_12x12x8.npz", "convective"),  # heterogeneous surface Q
+    ("ref_convective_moistwl_12x12x8.npz", "convective"),  # flux series, LAD-WL, FGR 2
 ]
+MOIST = [f for f in FIXTURES if "moist" in f[0]]
 # name of the libalfa entry for a recorded reference function
 ALIASES = {"PressureSolve": "ThomasPressureSolve"}
 ULP = 2.0 ** -52
@@ -189,6 +195,73 @@ def test_whole_step_matches_reference_main():
         assert err <= TOL, (k, err)
 
 
+def test_varying_geowind_matches_reference_main():
+    """optGeoWind = 1 over four steps: the whole-step engine and the
+    per-function MainLoop both against the reference's Main.py state."""
+    from jax_alfa_b200.api import Simulation
+    from jax_alfa_b200.driver import MainLoop
+    g = replay.load(os.path.join(GOLDEN, "ref_stable_geo_12x12x8.npz"))
+    grid = tuple(int(x) for x in g["meta.grid"])
+    cfg = cases.stable(*grid, nsteps=int(g["meta.steps"]), optGeoWind=1)
+    steps = cases.nsteps_of(cfg)  # Main.py runs ceil(SimTime / dt) steps
+    u, v, w, th, adv, sfc, o = _initial(cfg)
+    geo = cases.geowind_series(cfg)
+    sim = Simulation(cfg, u, v, w, th, surface_series=sfc, geowind_series=geo)
+    st = {k: t.cpu().numpy() for k, t in sim.step(steps).state().items()}
+    ml = MainLoop(cfg, u, v, w, th, surface_series=sfc, geowind_series=geo)
+    for _ in range(steps):
+        ml.step()
+    mst = {k: getattr(ml, k).cpu().numpy() for k in ("u", "v", "w", "TH")}
+    # four steps of the dynamic procedure (condition ~1e5-1e6 per step, see
+    # the module docstring): the multi-step bar of 1e-10
+    for k in ("u", "v", "w", "TH", "p"):
+        err = replay.rel_err(st[k], g["final." + k])
+        print(f"geowind {k}: {err:.2e}")
+        assert err <= 1e-10, (k, err)
+        if k in mst:
+            assert replay.rel_err(mst[k], g["final." + k]) <= 1e-10, k
+
+
+def moist_inputs(cfg, seed=0):
+    """Simulation / MainLoop keyword arguments of a moist case: the inputs
+    ``cases.write_run_dir`` gave the reference (dimensional)."""
+    kw = {"Q": cases.initial_moisture(cfg, seed)}
+    if cfg["optMoistureSurfBC"] >= 1:
+        kw["moisture_series"] = cases.moisture_surface_series(cfg)
+    if cfg["optSurfBC"] >= 1:
+        kw["surface_series"] = cases.surface_bc_series(cfg)
+    if cfg["optAdvection"] >= 1:
+        kw["adv_series"] = cases.adv_forcing_series(cfg) + (cases.adv_moisture_series(cfg),)
+    return kw
+
+
+@pytest.mark.parametrize("fname,case", MOIST)
+def test_moisture_whole_step_matches_reference_main(fname, case):
+    """optMoisture = 1: the whole-step engine and the per-function MainLoop
+    against the reference's Main.py state (humidity included) after
+    ceil(SimTime / dt) steps."""
+    from jax_alfa_b200.api import Simulation
+    from jax_alfa_b200.driver import MainLoop
+    g = replay.load(os.path.join(GOLDEN, fname))
+    cfg = _cfg(g, case)
+    steps = cases.nsteps_of(cfg)
+    seed = int(g["meta.seed"])
+    u, v, w, th = cases.initial_fields(cfg, seed)
+    kw = moist_inputs(cfg, seed)
+    sim = Simulation(cfg, u, v, w, th, **kw)
+    st = {k: t.cpu().numpy() for k, t in sim.step(steps).state().items()}
+    ml = MainLoop(cfg, u, v, w, th, **kw)
+    for _ in range(steps):
+        ml.step()
+    for k in ("u", "v", "w", "TH", "Q", "p"):
+        err = replay.rel_err(st[k], g["final." + k])
+        print(f"{fname} {k}: whole step {err:.2e}")
+        assert err <= 1e-10, (k, err)
+        if k != "p":
+            err = replay.rel_err(getattr(ml, k).cpu().numpy(), g["final." + k])
+            assert err <= 1e-10, ("MainLoop", k, err)
+
+
 @pytest.mark.parametrize("case,grid,steps,over", [
     ("neutral", (32, 32, 32), 20, {}),
     ("convective", (24, 24, 16), 10, {}),
@@ -197,18 +270,21 @@ def test_whole_step_matches_reference_main():
     ("stable", (24, 24, 16), 10, {"FGR": 2}),
     ("convective", (24, 24, 16), 10, {"optSgs": 2}),  # Wong-Lilly
     ("stable", (24, 24, 16), 10, {"optSgs": 4, "FGR": 2}),
+    ("stable", (24, 24, 16), 10, {"optGeoWind": 1}),  # varying geostrophic wind
 ])
 def test_whole_step_matches_oracle(case, grid, steps, over):
     from jax_alfa_b200.api import Simulation
     from oracle.alfa_oracle import OracleRun
     cfg = cases.CASES[case](*grid, nsteps=steps, **over)
     u, v, w, th, adv, sfc, o = _initial(cfg)
-    sim = Simulation(cfg, u, v, w, th, surface_series=sfc, adv_series=adv)
+    geo = cases.geowind_series(cfg) if cfg["optGeoWind"] else None
+    sim = Simulation(cfg, u, v, w, th, surface_series=sfc, adv_series=adv, geowind_series=geo)
     sim.step(steps)
     st = {k: t.cpu().numpy() for k, t in sim.state().items()}
     advn = o.adv_series(*adv) if adv is not None else None
     sfcn = o.surface_series(sfc) if sfc is not None else None
-    r = OracleRun(cfg, u, v, w, th, surface_series=sfcn, adv=advn)
+    r = OracleRun(cfg, u, v, w, th, surface_series=sfcn, adv=advn,
+                  geowind=o.geowind_series(*geo) if geo is not None else None)
     with np.errstate(all="ignore"):
         for _ in range(steps):
             r.step()

@@ -111,3 +111,27 @@ def test_checkpoint_restart_is_bitwise(tmp_path):
     for k in ref:
         assert np.array_equal(ref[k], got[k]), k
     assert c.diag()["iteration"] == a.diag()["iteration"]
+
+
+def test_moist_checkpoint_restart_is_bitwise(tmp_path):
+    """The same with optMoisture = 1 (Q and its RHS cross the restart) and a
+    prescribed surface humidity series."""
+    from jax_alfa_b200.api import Simulation
+    cfg = cases.convective(24, 24, 16, nsteps=4, dynamicSGS_call_time=2, optMoisture=1,
+                           optMoistureSurfBC=2)
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    kw = dict(Q=cases.initial_moisture(cfg, 0),
+              moisture_series=cases.moisture_surface_series(cfg))
+
+    def sim():
+        return Simulation(cfg, u, v, w, th, **kw)
+    a = sim().step(4)
+    ref = {k: t.cpu().numpy() for k, t in a.state().items()}
+    assert "Q" in ref
+    b = sim().step(2)
+    path = b.save(os.path.join(tmp_path, "ckpt.npz"))
+    del b
+    c = sim().load(path).step(2)
+    got = {k: t.cpu().numpy() for k, t in c.state().items()}
+    for k in ref:
+        assert np.array_equal(ref[k], got[k]), k

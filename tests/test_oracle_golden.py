@@ -23,7 +23,13 @@ CALL_FIXTURES = [
     ("ref_convective_wl_12x12x8.npz", "convective"),  # LASDD-WL (optSgs = 2)
     ("ref_stable_wl4_12x12x8.npz", "stable"),  # LAD-WL (optSgs = 4)
     ("ref_convective_wl_fgr2_12x12x8.npz", "convective"),  # LASDD-WL, FGR = 2
+    ("ref_stable_geo_12x12x8.npz", "stable"),  # time/height-varying geostrophic wind
+    ("ref_convective_moist_12x12x8.npz", "convective"),  # moisture, constant flux, Qadv
+    ("ref_stable_moistq_12x12x8.npz", "stable"),  # moisture, prescribed surface Q
+    ("ref_convective_moistq_12x12x8.npz", "convective"),  # heterogeneous surface Q
+    ("ref_convective_moistwl_12x12x8.npz", "convective"),  # flux series, LAD-WL, FGR 2
 ]
+MOIST_FIXTURES = [f for f in CALL_FIXTURES if "moist" in f[0]]
 # The oracle restates the reference operation for operation; on the same
 # NumPy FFT it reproduces the recorded results to the last bit.  The bound
 # leaves room for a different NumPy build's pairwise-sum order.
@@ -85,6 +91,55 @@ def test_time_loop_one_step_matches_reference_main():
     g = replay.load(os.path.join(GOLDEN, "ref_neutral_32_step1.npz"))
     r = _run(1)
     for name in ("u", "v", "w", "TH", "p", "beta1_1D", "beta2_1D", "Cs2_1D_avg2"):
+        assert replay.rel_err(getattr(r, name), g["final." + name]) <= TOL, name
+
+
+def test_time_loop_varying_geowind_matches_reference_main():
+    """optGeoWind = 1: the geostrophic wind row of each iteration
+    (``Main.py:170-174``) reaches the momentum RHS."""
+    g = replay.load(os.path.join(GOLDEN, "ref_stable_geo_12x12x8.npz"))
+    cfg = _cfg_of(g, "stable")
+    steps = cases.nsteps_of(cfg)  # Main.py runs ceil(SimTime / dt) steps
+    o = AlfaOracle(cfg)
+    u, v, w, th = cases.initial_fields(cfg, int(g["meta.seed"]))
+    r = OracleRun(cfg, u, v, w, th,
+                  surface_series=o.surface_series(cases.surface_bc_series(cfg)),
+                  geowind=o.geowind_series(*cases.geowind_series(cfg)))
+    with np.errstate(all="ignore"):
+        for _ in range(steps):
+            r.step()
+    for name in ("u", "v", "w", "TH", "p"):
+        assert replay.rel_err(getattr(r, name), g["final." + name]) <= TOL, name
+
+
+def moist_run_inputs(cfg, o, seed):
+    """OracleRun keyword arguments for a moist case (the reference's input
+    files as ``cases.write_run_dir`` writes them, non-dimensionalised)."""
+    kw = {"Q": cases.initial_moisture(cfg, seed)}
+    if cfg["optMoistureSurfBC"] >= 1:
+        kw["moisture_series"] = cases.moisture_surface_series(cfg)  # u_scale = Q_scale = 1
+    if cfg["optSurfBC"] >= 1:
+        kw["surface_series"] = o.surface_series(cases.surface_bc_series(cfg))
+    if cfg["optAdvection"] >= 1:
+        kw["adv"] = o.adv_series(*cases.adv_forcing_series(cfg)) + (
+            cases.adv_moisture_series(cfg) * o.z_scale,)
+    return kw
+
+
+@pytest.mark.parametrize("fname,case", MOIST_FIXTURES)
+def test_time_loop_with_moisture_matches_reference_main(fname, case):
+    """optMoisture = 1 (Main.py:71-76, 164-198, 246-369, 474-528): the
+    humidity and every other state variable after the recorded steps."""
+    g = replay.load(os.path.join(GOLDEN, fname))
+    cfg = _cfg_of(g, case)
+    o = AlfaOracle(cfg)
+    seed = int(g["meta.seed"])
+    u, v, w, th = cases.initial_fields(cfg, seed)
+    r = OracleRun(cfg, u, v, w, th, **moist_run_inputs(cfg, o, seed))
+    with np.errstate(all="ignore"):
+        for _ in range(cases.nsteps_of(cfg)):  # Main.py runs ceil(SimTime / dt) steps
+            r.step()
+    for name in ("u", "v", "w", "TH", "Q", "p"):
         assert replay.rel_err(getattr(r, name), g["final." + name]) <= TOL, name
 
 
