@@ -286,17 +286,21 @@ int alfa_get_diag(alfa_ctx*, alfa_diag* out /* host; synchronises the stream */)
  * of nz, in the reference's key order U V W TH dUdz dVdz dTHdz u2 v2 w2 TH2
  * uv uw vw uTH vTH wTH txy txz tyz qz Cs2_1 Cs2_2 Cs2PrRatio Beta1 Beta2 Q
  * dQdz Q2 wQ qHz, then the scalars M_sfc ustar qz_sfc qm_sfc.  Dimensional
- * (u_scale = TH_scale = 1, z from z_scale), Ugal added to U and u, T_0 to TH;
- * dry runs accumulate zeros in the moisture entries.  Zeroing acc is the
- * reference's ResetFlag = 1; the averages are acc / samples.  M_sfc_loc,
- * ustar: (nx, ny); qz_sfc_avg: one device double; profiles: (nz). */
+ * (u_scale = TH_scale = Q_scale = 1, z from z_scale), Ugal added to U and u,
+ * T_0 to TH.  Arguments in the reference's order; a dry sample passes NULL
+ * for Q, dQdz, qm_sfc_avg and qHz_q and accumulates zeros in the moisture
+ * entries.  Zeroing acc is the reference's ResetFlag = 1; the averages are
+ * acc / samples.  M_sfc_loc, ustar: (nx, ny); qz_sfc_avg, qm_sfc_avg: one
+ * device double each; profiles: (nz). */
 #define ALFA_STATS_NPROF 31
 #define ALFA_STATS_LEN(nz) (ALFA_STATS_NPROF * (nz) + 4)
 int alfa_ComputeStats(alfa_ctx*, const double* u, const double* v, const double* w,
-                      const double* TH, const double* dudz, const double* dvdz,
-                      const double* dTHdz, const double* M_sfc_loc, const double* ustar,
-                      const double* qz_sfc_avg, const double* txy, const double* txz,
-                      const double* tyz, const double* qz, const double* Cs2_1D_avg1,
+                      const double* TH, const double* Q, const double* dudz,
+                      const double* dvdz, const double* dTHdz, const double* dQdz,
+                      const double* M_sfc_loc, const double* ustar,
+                      const double* qz_sfc_avg, const double* qm_sfc_avg, const double* txy,
+                      const double* txz, const double* tyz, const double* qz,
+                      const double* qHz_q, const double* Cs2_1D_avg1,
                       const double* Cs2_1D_avg2, const double* Cs2PrRatio_1D,
                       const double* beta1_1D, const double* beta2_1D, double* acc);
 /* The same sample from the context's state after alfa_step (the arguments

@@ -120,7 +120,7 @@ SIGNATURES = {
     "alfa_get_moisture": [P],
     "alfa_step": [I],
     "alfa_get_state": [P] * 5,
-    "alfa_ComputeStats": [P] * 20,
+    "alfa_ComputeStats": [P] * 24,
     "alfa_stats_sample": [P],
     "alfa_save_checkpoint": [P],
     "alfa_load_checkpoint": [P],

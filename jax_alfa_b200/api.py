@@ -385,25 +385,27 @@ class Alfa:
                      qz_sfc_avg, qm_sfc_avg, txy, txz, tyz, qz, qHz_q, Cs2_1D_avg1,
                      Cs2_1D_avg2, Cs2PrRatio_1D, beta1_1D, beta2_1D, StatsDict, ResetFlag,
                      ZeRo3D=None):
-        """``Statistics.py:47-328`` (dry: Q, dQdz, qHz_q must be zero or None)."""
+        """``Statistics.py:47-328``.  A dry sample passes None for Q, dQdz,
+        qm_sfc_avg and qHz_q (the reference passes zeros)."""
         if ResetFlag == 1:
             d = self.InitializeStats()
             d["Ugal"] = StatsDict["Ugal"]
             return d
-        for x in (Q, dQdz, qHz_q):
-            if x is not None and bool(torch.any(torch.as_tensor(x) != 0)):
-                raise _lib.AlfaError("moisture statistics are not implemented (dry runs only)")
-        if qm_sfc_avg not in (None, 0, 0.0):
-            raise _lib.AlfaError("moisture statistics are not implemented (dry runs only)")
         nz = self.nz
         acc = dict_to_stats(StatsDict, nz, self.device)
-        q = torch.as_tensor(qz_sfc_avg, dtype=F64, device=self.device).reshape(1).contiguous()
+        scal = lambda x: torch.as_tensor(x, dtype=F64, device=self.device).reshape(1).contiguous()
+        q = scal(qz_sfc_avg)
+        moist = Q is not None
+        qm = scal(0.0 if qm_sfc_avg is None else qm_sfc_avg) if moist else None
         profs = [self._prof(x) for x in (Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D, beta1_1D,
                                          beta2_1D)]
+        opt = lambda x: self._f(x) if moist else None
         self._call("alfa_ComputeStats", self._f(u), self._f(v), self._f(w), self._f(TH),
-                   self._f(dudz), self._f(dvdz), self._f(dTHdz), self._p(M_sfc_loc, self.H),
-                   self._p(ustar, self.H), self._p(q), self._f(txy), self._f(txz),
-                   self._f(tyz), self._f(qz), *[self._p(x) for x in profs], self._p(acc))
+                   opt(Q), self._f(dudz), self._f(dvdz), self._f(dTHdz), opt(dQdz),
+                   self._p(M_sfc_loc, self.H), self._p(ustar, self.H), self._p(q),
+                   None if qm is None else self._p(qm), self._f(txy), self._f(txz),
+                   self._f(tyz), self._f(qz), opt(qHz_q), *[self._p(x) for x in profs],
+                   self._p(acc))
         return stats_to_dict(acc, nz, StatsDict["Ugal"])
 
     def _mom25(self):

@@ -489,13 +489,13 @@ static void carve(alfa_ctx* c, Carver& k) {
   // engine scratch
   e.T_elems = (size_t)e.mx * e.myh * nz;
   for (int i = 0; i < 4; i++) e.T[i] = k.take<cd>(e.T_elems);
-  e.red_elems = (size_t)256 * 16 * nz + 1024;
+  e.red_elems = (size_t)256 * 18 * nz + 1024;  // 18: the statistics' first pass
   e.red = k.take<double>(e.red_elems);
   e.scal = k.take<double>(64 * nz + 256);
   e.W_elems = N;
   e.W = k.take<double>(N);
   e.mat = k.take<double>(e.P());
-  e.stat = k.take<double>((size_t)24 * nz + 64);
+  e.stat = k.take<double>((size_t)30 * nz + 64);
 }
 
 // ---------------------------------------------------------------------------
@@ -2190,35 +2190,53 @@ int alfa_get_diag(alfa_ctx* c, alfa_diag* o) {
   return ALFA_OK;
 }
 
+static int compute_stats_checked(alfa_ctx* c, StatsIn& a, double* acc) {
+  CTX_CHECK(c);
+  NN(a.u); NN(a.v); NN(a.w); NN(a.TH); NN(a.dudz); NN(a.dvdz); NN(a.dTHdz); NN(a.M);
+  NN(a.ustar); NN(a.qz_sfc_avg); NN(a.txy); NN(a.txz); NN(a.tyz); NN(a.qz); NN(a.cs2_1);
+  NN(a.cs2_2); NN(a.cs2pr); NN(a.beta1); NN(a.beta2); NN(acc);
+  if (a.Q && (!a.dQdz || !a.qHz))
+    return c->e.fail("ComputeStats: Q needs dQdz and qHz_q", ALFA_E_SHAPE);
+  compute_stats(c->e, a, acc);
+  return check_launch(c->e, "ComputeStats");
+}
+
 int alfa_ComputeStats(alfa_ctx* c, const double* u, const double* v, const double* w,
-                      const double* TH, const double* dudz, const double* dvdz,
-                      const double* dTHdz, const double* M_sfc_loc, const double* ustar,
-                      const double* qz_sfc_avg, const double* txy, const double* txz,
-                      const double* tyz, const double* qz, const double* Cs2_1D_avg1,
+                      const double* TH, const double* Q, const double* dudz, const double* dvdz,
+                      const double* dTHdz, const double* dQdz, const double* M_sfc_loc,
+                      const double* ustar, const double* qz_sfc_avg, const double* qm_sfc_avg,
+                      const double* txy, const double* txz, const double* tyz, const double* qz,
+                      const double* qHz_q, const double* Cs2_1D_avg1,
                       const double* Cs2_1D_avg2, const double* Cs2PrRatio_1D,
                       const double* beta1_1D, const double* beta2_1D, double* acc) {
   CTX_CHECK(c);
-  NN(u); NN(v); NN(w); NN(TH); NN(dudz); NN(dvdz); NN(dTHdz); NN(M_sfc_loc); NN(ustar);
-  NN(qz_sfc_avg); NN(txy); NN(txz); NN(tyz); NN(qz); NN(Cs2_1D_avg1); NN(Cs2_1D_avg2);
-  NN(Cs2PrRatio_1D); NN(beta1_1D); NN(beta2_1D); NN(acc);
   Engine& e = c->e;
   StatsIn a{u, v, w, TH, dudz, dvdz, dTHdz, txy, txz, tyz, qz, M_sfc_loc, ustar, qz_sfc_avg,
             Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D, beta1_1D, beta2_1D, e.cfg.Ugal,
             e.T0_nondim};
-  compute_stats(e, a, acc);
-  return check_launch(e, "ComputeStats");
+  a.Q = Q;
+  a.dQdz = dQdz;
+  a.qHz = qHz_q;
+  a.qm_sfc_avg = qm_sfc_avg;
+  return compute_stats_checked(c, a, acc);
 }
 
 int alfa_stats_sample(alfa_ctx* c, double* acc) {
   CTX_CHECK(c);
-  NN(acc);
+  Engine& e = c->e;
   Work& W = c->w;
-  if (!W.have_state) return c->e.fail("alfa_stats_sample before alfa_init_state", ALFA_E_STATE);
-  const int nz = c->e.nz;
-  return alfa_ComputeStats(c, W.u, W.v, W.w, W.TH, W.g[6], W.g[7], W.gT[2], W.M, W.ustar,
-                           W.d_qavg, W.mom[3], W.mom[4], W.mom[5], W.qz, W.prof + 21 * nz,
-                           W.prof + 22 * nz, W.prof + 23 * nz, W.prof + 20 * nz,
-                           W.prof + 24 * nz, acc);
+  if (!W.have_state) return e.fail("alfa_stats_sample before alfa_init_state", ALFA_E_STATE);
+  const int nz = e.nz;
+  StatsIn a{W.u, W.v, W.w, W.TH, W.g[6], W.g[7], W.gT[2], W.mom[3], W.mom[4], W.mom[5], W.qz,
+            W.M, W.ustar, W.d_qavg, W.prof + 21 * nz, W.prof + 22 * nz, W.prof + 23 * nz,
+            W.prof + 20 * nz, W.prof + 24 * nz, e.cfg.Ugal, e.T0_nondim};
+  if (e.cfg.optMoisture >= 1) {  // Main.py:549-553: Q, dQdz, qm_sfc_avg, qHz_q
+    a.Q = W.Q;
+    a.dQdz = W.gQ[2];
+    a.qHz = W.qzq;
+    a.qm_plane = W.qm_plane;
+  }
+  return compute_stats_checked(c, a, acc);
 }
 
 // checkpoint layout: u v w TH p RHS[4] Cs2 Cs2Pr (N each), Q RHS_Q (N each, when

@@ -914,22 +914,26 @@ void scalar_wl_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta
 // ---------------------------------------------------------------------------
 // Plane-averaged statistics (Statistics.py:47-328), one sample added to the
 // accumulator acc[key * nz + z] (profile keys in STATS order) and
-// acc[31 * nz + j] (M_sfc, ustar, qz_sfc, qm_sfc).  Dry: the moisture
-// entries (Q, dQdz, Q2, wQ, qHz, qm_sfc) accumulate zeros.
+// acc[31 * nz + j] (M_sfc, ustar, qz_sfc, qm_sfc).  A dry sample (no Q)
+// accumulates zeros in the moisture entries (Q, dQdz, Q2, wQ, qHz, qm_sfc).
+// Q_scale = 1 (Statistics.py:166-168, 199-201, 231-256, 275, 289).
 // ---------------------------------------------------------------------------
 enum StatKey {
   ST_U = 0, ST_V, ST_W, ST_TH, ST_dUdz, ST_dVdz, ST_dTHdz, ST_u2, ST_v2, ST_w2, ST_TH2, ST_uv,
   ST_uw, ST_vw, ST_uTH, ST_vTH, ST_wTH, ST_txy, ST_txz, ST_tyz, ST_qz, ST_Cs2_1, ST_Cs2_2,
-  ST_Cs2PrRatio, ST_Beta1, ST_Beta2, ST_NPROF = 31
+  ST_Cs2PrRatio, ST_Beta1, ST_Beta2, ST_Q, ST_dQdz, ST_Q2, ST_wQ, ST_qHz, ST_NPROF = 31
 };
+static constexpr int ST_NM = 18;  // pass-1 sums
+static constexpr int ST_NV = 12;  // pass-2 sums
 
-// pass 1 sums per level: u v w TH dudz dvdz dTHdz txy txz tyz qz u_st v_st TH_st
+// pass 1 sums per level: u v w TH dudz dvdz dTHdz txy txz tyz qz u_st v_st TH_st,
+// then Q dQdz qHz Q_st
 __global__ void k_stats_mean_partial(StatsIn a, size_t H, int nz, double* __restrict__ part) {
   const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
   const size_t r0 = blockIdx.x * rpb;
   const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
   for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-    double s[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double s[ST_NM] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (size_t r = r0; r < r1; r++) {
       const size_t i = r * nz + z;
       const double u = a.u[i], v = a.v[i], T = a.TH[i];
@@ -953,9 +957,16 @@ __global__ void k_stats_mean_partial(StatsIn a, size_t H, int nz, double* __rest
         s[12] += 0.5 * (a.v[i - 1] + v);
         s[13] += 0.5 * (a.TH[i - 1] + T);
       }
+      if (a.Q) {
+        const double q = a.Q[i];
+        s[14] += q;
+        s[15] += a.dQdz[i];
+        s[16] += a.qHz[i];
+        s[17] += (z == 0) ? q : 0.5 * (a.Q[i - 1] + q);
+      }
     }
 #pragma unroll
-    for (int q = 0; q < 14; q++) part[((size_t)blockIdx.x * 14 + q) * nz + z] = s[q];
+    for (int q = 0; q < ST_NM; q++) part[((size_t)blockIdx.x * ST_NM + q) * nz + z] = s[q];
   }
 }
 
@@ -970,7 +981,8 @@ __global__ void k_stats_var_partial(StatsIn a, const double* __restrict__ m, siz
     const double mU = m[0 * nz + z] + Ug, mV = m[1 * nz + z], mW = m[2 * nz + z];
     const double mT = m[3 * nz + z];
     const double muS = m[11 * nz + z] + Ug, mvS = m[12 * nz + z], mTS = m[13 * nz + z];
-    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double mQ = m[14 * nz + z], mQS = m[17 * nz + z];
+    double s[ST_NV] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (size_t r = r0; r < r1; r++) {
       const size_t i = r * nz + z;
       const double u = a.u[i], v = a.v[i], T = a.TH[i];
@@ -996,9 +1008,16 @@ __global__ void k_stats_var_partial(StatsIn a, const double* __restrict__ m, siz
       s[7] += usf * wsf;
       s[8] += vsf * wsf;
       s[9] += wsf * Tsf;
+      if (a.Q) {
+        const double q = a.Q[i];
+        const double Qf = q - mQ;
+        const double QS = (z == 0) ? q : 0.5 * (a.Q[i - 1] + q);
+        s[10] += Qf * Qf;
+        s[11] += wsf * (QS - mQS);
+      }
     }
 #pragma unroll
-    for (int q = 0; q < 10; q++) part[((size_t)blockIdx.x * 10 + q) * nz + z] = s[q];
+    for (int q = 0; q < ST_NV; q++) part[((size_t)blockIdx.x * ST_NV + q) * nz + z] = s[q];
   }
 }
 
@@ -1006,19 +1025,22 @@ __global__ void k_stats_var_partial(StatsIn a, const double* __restrict__ m, siz
 __global__ void k_stats_accumulate(StatsIn a, const double* __restrict__ m,
                                    const double* __restrict__ var, size_t H, int nz,
                                    double us_zs, double* acc) {
-  __shared__ double red[2][1024];
-  double sM = 0.0, sU = 0.0;
+  __shared__ double red[3][1024];
+  double sM = 0.0, sU = 0.0, sQ = 0.0;
   for (size_t r = threadIdx.x; r < H; r += blockDim.x) {
     sM += a.M[r];
     sU += a.ustar[r] * a.ustar[r];
+    if (a.qm_plane) sQ += a.qm_plane[r];
   }
   red[0][threadIdx.x] = sM;
   red[1][threadIdx.x] = sU;
+  red[2][threadIdx.x] = sQ;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w) {
       red[0][threadIdx.x] += red[0][threadIdx.x + w];
       red[1][threadIdx.x] += red[1][threadIdx.x + w];
+      red[2][threadIdx.x] += red[2][threadIdx.x + w];
     }
     __syncthreads();
   }
@@ -1051,26 +1073,37 @@ __global__ void k_stats_accumulate(StatsIn a, const double* __restrict__ m,
     A[ST_Cs2PrRatio * nz + z] += a.cs2pr[z];
     A[ST_Beta1 * nz + z] += a.beta1[z];
     A[ST_Beta2 * nz + z] += a.beta2[z];
+    if (a.Q) {
+      A[ST_Q * nz + z] += m[14 * nz + z];
+      A[ST_dQdz * nz + z] += m[15 * nz + z] * us_zs;
+      A[ST_Q2 * nz + z] += var[10 * nz + z];
+      A[ST_wQ * nz + z] += var[11 * nz + z];
+      A[ST_qHz * nz + z] += m[16 * nz + z];
+    }
   }
   if (threadIdx.x == 0) {
     double* S = acc + (size_t)ST_NPROF * nz;
     S[0] += red[0][0] / (double)H;
     S[1] += sqrt(red[1][0] / (double)H);
     S[2] += *a.qz_sfc_avg;
+    if (a.qm_plane)
+      S[3] += red[2][0] / (double)H;
+    else if (a.qm_sfc_avg)
+      S[3] += *a.qm_sfc_avg;
   }
 }
 
 void compute_stats(Engine& e, const StatsIn& a, double* acc) {
   const int nb = red_blocks(e);
   const int nz = e.nz;
-  double* m = e.stat;             // 14 nz plane means
-  double* var = e.stat + 14 * nz;  // 10 nz
+  double* m = e.stat;                // ST_NM nz plane means
+  double* var = e.stat + ST_NM * nz;  // ST_NV nz
   ::alfa::note_launch(); k_stats_mean_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)14 * nz), TPB, 0, e.stream>>>(
-      e.red, nb, 14, nz, 1.0 / (double)e.H(), m);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)ST_NM * nz), TPB, 0, e.stream>>>(
+      e.red, nb, ST_NM, nz, 1.0 / (double)e.H(), m);
   ::alfa::note_launch(); k_stats_var_partial<<<nb, 128, 0, e.stream>>>(a, m, e.H(), nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)10 * nz), TPB, 0, e.stream>>>(
-      e.red, nb, 10, nz, 1.0 / (double)e.H(), var);
+  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)ST_NV * nz), TPB, 0, e.stream>>>(
+      e.red, nb, ST_NV, nz, 1.0 / (double)e.H(), var);
   // u_scale = TH_scale = 1: dUdz, dVdz, dTHdz scale by 1 / z_scale
   ::alfa::note_launch(); k_stats_accumulate<<<1, 1024, 0, e.stream>>>(a, m, var, e.H(), nz,
                                                                      1.0 / e.z_scale, acc);

@@ -99,6 +99,11 @@ struct StatsIn {
   const double *M, *ustar, *qz_sfc_avg;  // planes (nx, ny) and one scalar
   const double *cs2_1, *cs2_2, *cs2pr, *beta1, *beta2;  // profiles (nz)
   double Ugal, T0;
+  // moisture (null: a dry sample, zeros accumulated): Q, dQdz, qHz_q fields;
+  // the surface flux as a device scalar (qm_sfc_avg) or as the plane whose
+  // mean it is (qm_plane, used when given)
+  const double *Q = nullptr, *dQdz = nullptr, *qHz = nullptr;
+  const double *qm_sfc_avg = nullptr, *qm_plane = nullptr;
 };
 void compute_stats(Engine& e, const StatsIn& a, double* acc);
 

@@ -1450,10 +1450,11 @@ def InitializeStats(o, nz):
     return d
 
 
-def ComputeStats(o, u, v, w, TH, dudz, dvdz, dTHdz, M_sfc_loc, ustar, qz_sfc_avg,
-                 txy, txz, tyz, qz, Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D,
+def ComputeStats(o, u, v, w, TH, Q, dudz, dvdz, dTHdz, dQdz, M_sfc_loc, ustar, qz_sfc_avg,
+                 qm_sfc_avg, txy, txz, tyz, qz, qHz_q, Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D,
                  beta1_1D, beta2_1D, StatsDict, ResetFlag):
-    """``Statistics.py:47-328`` for a dry run (Q = dQdz = qHz = 0)."""
+    """``Statistics.py:47-328`` with the reference's argument order; a dry run
+    passes None (zeros) for Q, dQdz, qHz_q and qm_sfc_avg."""
     nz = o.nz
     if ResetFlag == 1:
         return InitializeStats(o, nz) | {"Ugal": StatsDict["Ugal"]}
@@ -1507,12 +1508,25 @@ def ComputeStats(o, u, v, w, TH, dudz, dvdz, dTHdz, M_sfc_loc, ustar, qz_sfc_avg
     new["qz"] = m(qz) * (us * ts)
     new["Cs2_1"], new["Cs2_2"], new["Cs2PrRatio"] = Cs2_1D_avg1, Cs2_1D_avg2, Cs2PrRatio_1D
     new["Beta1"], new["Beta2"] = beta1_1D, beta2_1D
-    for k in ("Q", "dQdz", "Q2", "wQ", "qHz"):
-        new[k] = np.zeros(nz)
+    if Q is None:
+        for k in ("Q", "dQdz", "Q2", "wQ", "qHz"):
+            new[k] = np.zeros(nz)
+    else:  # Statistics.py:166-168, 199-201, 231-256, 275 (Q_scale = 1)
+        qs = o.Q_scale
+        mQ = m(Q) * qs
+        new["Q"] = mQ
+        new["dQdz"] = m(dQdz) * (qs / zs)
+        new["Q2"] = m((Q - mQ / qs) ** 2) * qs ** 2
+        Q_st = np.zeros_like(Q)
+        Q_st[:, :, 1:nz] = o.StagGridAvg(Q)
+        Q_st[:, :, 0] = Q[:, :, 0]
+        mQ_st = m(Q_st) * qs
+        new["wQ"] = m(wsf * (Q_st - mQ_st / qs)) * (us * qs)
+        new["qHz"] = m(qHz_q) * (us * qs)
     new["M_sfc"] = np.mean(M_sfc_loc)
     new["ustar"] = np.sqrt(np.mean(ustar ** 2)) * us
     new["qz_sfc"] = qz_sfc_avg * us * ts
-    new["qm_sfc"] = 0.0
+    new["qm_sfc"] = 0.0 if qm_sfc_avg is None else qm_sfc_avg * us * o.Q_scale
     out = {k: StatsDict[k] + new[k] for k in STATS_PROFILE_KEYS + STATS_SCALAR_KEYS}
     out["Ugal"] = Ugal
     out["ZeRo1D"] = StatsDict["ZeRo1D"]
@@ -1683,8 +1697,13 @@ class OracleRun:
         """ComputeStats with the arguments Main.py:550-558 passes after this
         iteration."""
         L = self.last
-        return ComputeStats(self.o, self.u, self.v, self.w, self.TH, L["dudz"], L["dvdz"],
-                            L["dTHdz"], self.M_sfc_loc, self.ustar, float(self.qz_sfc_avg),
-                            L["txy"], L["txz"], L["tyz"], L["qz"], self.Cs2_1D_avg1,
+        moist = self.moist
+        return ComputeStats(self.o, self.u, self.v, self.w, self.TH,
+                            self.Q if moist else None, L["dudz"], L["dvdz"], L["dTHdz"],
+                            L["dQdz"] if moist else None, self.M_sfc_loc, self.ustar,
+                            float(self.qz_sfc_avg),
+                            float(np.mean(L["qm_sfc_step"])) if moist else None,
+                            L["txy"], L["txz"], L["tyz"], L["qz"],
+                            L["qHz_q"] if moist else None, self.Cs2_1D_avg1,
                             self.Cs2_1D_avg2, self.Cs2PrRatio_1D, self.beta1_1D, self.beta2_1D,
                             StatsDict, 0)

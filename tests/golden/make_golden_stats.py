@@ -2,7 +2,7 @@
 reference's own ``ComputeStats`` / ``InitializeStats``
 (``src/utilities/Statistics.py:47-380``) on the NumPy stand-in for ``jax``
 (see ``make_golden.py``), for seeded synthetic inputs of the stable case's
-configuration (Galilean velocity Ugal = 5 m/s):
+configuration (Galilean velocity Ugal = 5 m/s), moisture entries included:
 
   ``in<s>.<name>``  inputs of sample s = 1, 2 (fields, planes, profiles);
   ``acc<s>.<key>``  the statistics dictionary after accumulating samples
@@ -23,7 +23,8 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 REFERENCE = os.environ.get("ALFA_REFERENCE_DIR", "/root/reference")
 
 GRID = (12, 16, 8)
-FIELDS = ("u", "v", "w", "TH", "dudz", "dvdz", "dTHdz", "txy", "txz", "tyz", "qz")
+FIELDS = ("u", "v", "w", "TH", "dudz", "dvdz", "dTHdz", "txy", "txz", "tyz", "qz",
+          "Q", "dQdz", "qHz_q")
 PLANES = ("M_sfc_loc", "ustar")
 PROFILES = ("Cs2_1D_avg1", "Cs2_1D_avg2", "Cs2PrRatio_1D", "beta1_1D", "beta2_1D")
 
@@ -32,11 +33,15 @@ def sample_inputs(rng, nx, ny, nz):
     d = {k: rng.standard_normal((nx, ny, nz)) for k in FIELDS}
     d["TH"] = 0.5 * d["TH"] + np.linspace(0.0, 3.0, nz)   # anomaly with a mean profile
     d["u"] = d["u"] + 2.0
+    d["Q"] = 8.0e-3 + 1.0e-4 * d["Q"] - 1.0e-4 * np.linspace(0.0, 1.0, nz)  # specific humidity
+    d["dQdz"] = 1.0e-5 * d["dQdz"]
+    d["qHz_q"] = 1.0e-5 * d["qHz_q"]
     for k in PLANES:
         d[k] = 0.2 + rng.random((nx, ny))
     for k in PROFILES:
         d[k] = rng.random(nz)
     d["qz_sfc_avg"] = np.array(rng.standard_normal() * 1e-3)
+    d["qm_sfc_avg"] = np.array(rng.standard_normal() * 1e-5)
     return d
 
 
@@ -61,10 +66,11 @@ def main():
     out = {}
 
     def call(d, stats, reset):
-        return ComputeStats(d["u"], d["v"], d["w"], d["TH"], zero3,
-                            d["dudz"], d["dvdz"], d["dTHdz"], zero3,
-                            d["M_sfc_loc"], d["ustar"], float(d["qz_sfc_avg"]), 0.0,
-                            d["txy"], d["txz"], d["tyz"], d["qz"], zero3,
+        return ComputeStats(d["u"], d["v"], d["w"], d["TH"], d["Q"],
+                            d["dudz"], d["dvdz"], d["dTHdz"], d["dQdz"],
+                            d["M_sfc_loc"], d["ustar"], float(d["qz_sfc_avg"]),
+                            float(d["qm_sfc_avg"]),
+                            d["txy"], d["txz"], d["tyz"], d["qz"], d["qHz_q"],
                             d["Cs2_1D_avg1"], d["Cs2_1D_avg2"], d["Cs2PrRatio_1D"],
                             d["beta1_1D"], d["beta2_1D"], stats, reset, zero3)
 

@@ -19,7 +19,8 @@ TOL = 1e-12
 # the largest statistic of its group
 GROUPS = (("U", "V", "W"), ("dUdz", "dVdz"),
           ("u2", "v2", "w2", "uv", "uw", "vw", "txy", "txz", "tyz"),
-          ("uTH", "vTH", "wTH", "qz"), ("Cs2_1", "Cs2_2", "Cs2PrRatio", "Beta1", "Beta2"))
+          ("uTH", "vTH", "wTH", "qz"), ("Cs2_1", "Cs2_2", "Cs2PrRatio", "Beta1", "Beta2"),
+          ("wQ", "qHz"))
 
 
 def stats_err(got, exp, key):
@@ -32,8 +33,8 @@ def stats_err(got, exp, key):
 
 
 def test_compute_stats_matches_reference():
-    """Two accumulated samples and a reset through alfa_ComputeStats against
-    the reference's own ComputeStats outputs."""
+    """Two accumulated samples (moisture entries included) and a reset through
+    alfa_ComputeStats against the reference's own ComputeStats outputs."""
     from jax_alfa_b200.api import Alfa, STATS_PROFILE_KEYS, STATS_SCALAR_KEYS
     z = np.load(os.path.join(GOLDEN, "ref_stats.npz"))
     a = Alfa(cases.stable(12, 16, 8, nsteps=1))
@@ -42,10 +43,11 @@ def test_compute_stats_matches_reference():
     st = a.InitializeStats()
     for s in (1, 2):
         d = {k[len(f"in{s}."):]: z[k] for k in z.files if k.startswith(f"in{s}.")}
-        st = a.ComputeStats(t(d["u"]), t(d["v"]), t(d["w"]), t(d["TH"]), None, t(d["dudz"]),
-                            t(d["dvdz"]), t(d["dTHdz"]), None, t(d["M_sfc_loc"]),
-                            t(d["ustar"]), float(d["qz_sfc_avg"]), 0.0, t(d["txy"]),
-                            t(d["txz"]), t(d["tyz"]), t(d["qz"]), None, t(d["Cs2_1D_avg1"]),
+        st = a.ComputeStats(t(d["u"]), t(d["v"]), t(d["w"]), t(d["TH"]), t(d["Q"]),
+                            t(d["dudz"]), t(d["dvdz"]), t(d["dTHdz"]), t(d["dQdz"]),
+                            t(d["M_sfc_loc"]), t(d["ustar"]), float(d["qz_sfc_avg"]),
+                            float(d["qm_sfc_avg"]), t(d["txy"]), t(d["txz"]), t(d["tyz"]),
+                            t(d["qz"]), t(d["qHz_q"]), t(d["Cs2_1D_avg1"]),
                             t(d["Cs2_1D_avg2"]), t(d["Cs2PrRatio_1D"]), t(d["beta1_1D"]),
                             t(d["beta2_1D"]), st, 0)
         exp = {k: z[f"acc{s}.{k}"] for k in STATS_PROFILE_KEYS + STATS_SCALAR_KEYS}
@@ -87,6 +89,36 @@ def test_stats_sample_matches_oracle_run():
             r.step()
             st = r.stats_sample(st)
     got = stats_to_dict(acc, 16, cfg["Ugal"])
+    for k in STATS_PROFILE_KEYS + STATS_SCALAR_KEYS:
+        if not np.any(st[k]):
+            assert not np.any(got[k]), k
+            continue
+        err = stats_err(got, st, k)
+        print(f"{k}: {err:.2e}")
+        assert err <= 1e-10, (k, err)
+
+
+def test_moist_stats_sample_matches_oracle_run():
+    """The same with optMoisture = 1: Q, dQdz, Q2, wQ, qHz and qm_sfc from the
+    engine's state (heterogeneous prescribed surface humidity)."""
+    from oracle.alfa_oracle import OracleRun, InitializeStats
+    from jax_alfa_b200.api import Simulation, STATS_PROFILE_KEYS, STATS_SCALAR_KEYS, stats_to_dict
+    cfg = cases.convective(24, 24, 16, nsteps=4, optMoisture=1, optMoistureSurfBC=2)
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    Q, ms = cases.initial_moisture(cfg, 0), cases.moisture_surface_series(cfg)
+    sim = Simulation(cfg, u, v, w, th, Q=Q, moisture_series=ms)
+    r = OracleRun(cfg, u, v, w, th, Q=Q, moisture_series=ms)
+    acc = None
+    st = InitializeStats(r.o, 16)
+    with np.errstate(all="ignore"):
+        for _ in range(3):
+            sim.step(1)
+            acc = sim.stats_sample(acc)
+            r.step()
+            st = r.stats_sample(st)
+    got = stats_to_dict(acc, 16, cfg["Ugal"])
+    for k in ("Q", "dQdz", "Q2", "wQ", "qHz", "qm_sfc"):
+        assert np.any(st[k]), k
     for k in STATS_PROFILE_KEYS + STATS_SCALAR_KEYS:
         if not np.any(st[k]):
             assert not np.any(got[k]), k

@@ -207,7 +207,8 @@ def test_dealias_triple_product_quirk():
 
 def test_statistics_match_reference():
     """ComputeStats / InitializeStats (Statistics.py:47-380): two accumulated
-    samples and a reset, against the reference's own outputs."""
+    samples (moisture entries included) and a reset, against the reference's
+    own outputs."""
     from oracle import alfa_oracle
     z = np.load(os.path.join(GOLDEN, "ref_stats.npz"))
     o = alfa_oracle.AlfaOracle(cases.stable(12, 16, 8, nsteps=1))
@@ -216,13 +217,14 @@ def test_statistics_match_reference():
     for s in (1, 2):
         d = {k[len(f"in{s}."):]: z[k] for k in z.files if k.startswith(f"in{s}.")}
         st = alfa_oracle.ComputeStats(
-            o, d["u"], d["v"], d["w"], d["TH"], d["dudz"], d["dvdz"], d["dTHdz"],
-            d["M_sfc_loc"], d["ustar"], float(d["qz_sfc_avg"]), d["txy"], d["txz"], d["tyz"],
-            d["qz"], d["Cs2_1D_avg1"], d["Cs2_1D_avg2"], d["Cs2PrRatio_1D"], d["beta1_1D"],
+            o, d["u"], d["v"], d["w"], d["TH"], d["Q"], d["dudz"], d["dvdz"], d["dTHdz"],
+            d["dQdz"], d["M_sfc_loc"], d["ustar"], float(d["qz_sfc_avg"]),
+            float(d["qm_sfc_avg"]), d["txy"], d["txz"], d["tyz"], d["qz"], d["qHz_q"],
+            d["Cs2_1D_avg1"], d["Cs2_1D_avg2"], d["Cs2PrRatio_1D"], d["beta1_1D"],
             d["beta2_1D"], st, 0)
         for k in keys:
             np.testing.assert_allclose(st[k], z[f"acc{s}.{k}"], rtol=1e-13, atol=1e-15,
                                        err_msg=f"sample {s} {k}")
-    st = alfa_oracle.ComputeStats(o, *([None] * 19), st, 1)
+    st = alfa_oracle.ComputeStats(o, *([None] * 23), st, 1)
     for k in keys:
         np.testing.assert_array_equal(st[k], z[f"reset.{k}"])
