@@ -489,7 +489,7 @@ static void carve(alfa_ctx* c, Carver& k) {
   // engine scratch
   e.T_elems = (size_t)e.mx * e.myh * nz;
   for (int i = 0; i < 4; i++) e.T[i] = k.take<cd>(e.T_elems);
-  e.red_elems = (size_t)256 * 18 * nz + 1024;  // 18: the statistics' first pass
+  e.red_elems = (size_t)1024 * 18 * nz + 1024;  // 1024 blocks x 18 sums (statistics' pass 1)
   e.red = k.take<double>(e.red_elems);
   e.scal = k.take<double>(64 * nz + 256);
   e.W_elems = N;

@@ -22,8 +22,13 @@ static inline int nblocks(size_t n, int tpb = TPB) {
 // plane reductions: partial sums over blocks of (x, y) rows, then a fixed
 // order sum of the partials (deterministic, independent of timing)
 // ---------------------------------------------------------------------------
-static constexpr int RED_BLOCKS = 256;
-static constexpr int RED_MAXQ = 16;  // e.red holds RED_BLOCKS x RED_MAXQ x nz partials
+// 1024 blocks of 128 threads: ~28 resident warps per SM for the wide
+// LASDD / statistics sums (256 blocks left ~7 per SM and these kernels
+// latency-bound); e.red holds RED_BLOCKS x 18 x nz partials
+static constexpr int RED_BLOCKS = 1024;
+static constexpr int RED_MAXQ = 16;
+// the no-allocation entry's fixed partial array holds 256 x nz
+static constexpr int NOALLOC_RED_BLOCKS = 256;
 
 struct RedArgs {
   const double* f[RED_MAXQ];
@@ -43,14 +48,28 @@ __global__ void k_plane_partial(RedArgs a, size_t H, int nz, double* __restrict_
   }
 }
 
+// Sum of the per-block partials in a fixed order (deterministic): thread
+// (x, y) of a 32 x 32 block adds partials b = y, y + 32, ... of entry
+// t = 32 blockIdx.x + x, then the 32 column sums are added in order of y.
+// Launch with finish_grid(nq * nz) blocks of dim3(32, 32).
 __global__ void k_partial_finish(const double* __restrict__ part, int nblk, int nq, int nz,
                                  double scale, double* __restrict__ out) {
-  GRID_STRIDE(t, (size_t)nq * nz) {
-    double s = 0.0;
-    for (int b = 0; b < nblk; b++) s += part[(size_t)b * nq * nz + t];
-    out[t] = s * scale;
+  __shared__ double sh[32][33];
+  const size_t n = (size_t)nq * nz;
+  const size_t t = (size_t)blockIdx.x * 32 + threadIdx.x;
+  double s = 0.0;
+  if (t < n)
+    for (int b = threadIdx.y; b < nblk; b += 32) s += part[(size_t)b * n + t];
+  sh[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && t < n) {
+    double r = 0.0;
+    for (int y = 0; y < 32; y++) r += sh[y][threadIdx.x];
+    out[t] = r * scale;
   }
 }
+
+static inline unsigned finish_grid(size_t n) { return (unsigned)((n + 31) / 32); }
 
 static int red_blocks(const Engine& e) {
   return (int)(e.H() < (size_t)RED_BLOCKS ? e.H() : RED_BLOCKS);
@@ -62,20 +81,20 @@ void plane_sums(Engine& e, const double* const* fields, int nq, double* sums) {
   for (int q = 0; q < nq; q++) a.f[q] = fields[q];
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(e.red, nb, nq, e.nz, 1.0,
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)nq * e.nz), dim3(32, 32), 0, e.stream>>>(e.red, nb, nq, e.nz, 1.0,
                                                                        sums);
 }
 
 // The plane mean of one field with caller-provided partial-sum storage
-// (RED_BLOCKS x nz doubles); same kernels and block count as plane_means.
+// (NOALLOC_RED_BLOCKS x nz doubles); the same kernels as plane_means.
 void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials, double* mean,
                              cudaStream_t s) {
   RedArgs a{};
   a.nq = 1;
   a.f[0] = F;
-  const int nb = (int)(H < (size_t)RED_BLOCKS ? H : RED_BLOCKS);
+  const int nb = (int)(H < (size_t)NOALLOC_RED_BLOCKS ? H : NOALLOC_RED_BLOCKS);
   ::alfa::note_launch(); k_plane_partial<<<nb, 128, 0, s>>>(a, H, nz, partials);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)nz), TPB, 0, s>>>(
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)nz), dim3(32, 32), 0, s>>>(
       partials, nb, 1, nz, 1.0 / (double)H, mean);
 }
 
@@ -85,7 +104,7 @@ void plane_means(Engine& e, const double* const* fields, int nq, double* means) 
   for (int q = 0; q < nq; q++) a.f[q] = fields[q];
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_plane_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), e.nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)nq * e.nz), TPB, 0, e.stream>>>(
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)nq * e.nz), dim3(32, 32), 0, e.stream>>>(
       e.red, nb, nq, e.nz, 1.0 / (double)e.H(), means);
 }
 
@@ -601,7 +620,7 @@ static LasddConst lasdd_const(const Engine& e) {
 void lasdd_sums(Engine& e, const LasddFields& f, double* sums10) {
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_lasdd_partial<<<nb, 128, 0, e.stream>>>(f, lasdd_const(e), e.H(), e.nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)10 * e.nz), dim3(32, 32), 0, e.stream>>>(e.red, nb, 10, e.nz,
                                                                        1.0 / (double)e.H(), sums10);
 }
 
@@ -787,7 +806,7 @@ __global__ void k_wl_partial(LasddFields f, size_t H, int nz, double* __restrict
 void lasdd_wl_sums(Engine& e, const LasddFields& f, double* sums4) {
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_wl_partial<<<nb, 128, 0, e.stream>>>(f, e.H(), e.nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)4 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 4, e.nz,
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)4 * e.nz), dim3(32, 32), 0, e.stream>>>(e.red, nb, 4, e.nz,
                                                                        1.0 / (double)e.H(), sums4);
 }
 
@@ -889,7 +908,7 @@ __global__ void k_slwl_partial(ScalarLasddFields f, size_t H, int nz, double* pa
 void scalar_lasdd_wl_sums(Engine& e, const ScalarLasddFields& f, double* sums4) {
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_slwl_partial<<<nb, 128, 0, e.stream>>>(f, e.H(), e.nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)4 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 4, e.nz,
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)4 * e.nz), dim3(32, 32), 0, e.stream>>>(e.red, nb, 4, e.nz,
                                                                        1.0 / (double)e.H(), sums4);
 }
 
@@ -1099,10 +1118,10 @@ void compute_stats(Engine& e, const StatsIn& a, double* acc) {
   double* m = e.stat;                // ST_NM nz plane means
   double* var = e.stat + ST_NM * nz;  // ST_NV nz
   ::alfa::note_launch(); k_stats_mean_partial<<<nb, 128, 0, e.stream>>>(a, e.H(), nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)ST_NM * nz), TPB, 0, e.stream>>>(
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)ST_NM * nz), dim3(32, 32), 0, e.stream>>>(
       e.red, nb, ST_NM, nz, 1.0 / (double)e.H(), m);
   ::alfa::note_launch(); k_stats_var_partial<<<nb, 128, 0, e.stream>>>(a, m, e.H(), nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)ST_NV * nz), TPB, 0, e.stream>>>(
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)ST_NV * nz), dim3(32, 32), 0, e.stream>>>(
       e.red, nb, ST_NV, nz, 1.0 / (double)e.H(), var);
   // u_scale = TH_scale = 1: dUdz, dVdz, dTHdz scale by 1 / z_scale
   ::alfa::note_launch(); k_stats_accumulate<<<1, 1024, 0, e.stream>>>(a, m, var, e.H(), nz,
@@ -1183,7 +1202,7 @@ void cs2_profiles(Engine& e, const double* Cs2, double* avg1, double* avg2) {
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_cs2_partial<<<nb, 128, 0, e.stream>>>(Cs2, e.H(), e.nz, e.red);
   double* m = e.scal + 64;
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)2 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 2, e.nz,
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)2 * e.nz), dim3(32, 32), 0, e.stream>>>(e.red, nb, 2, e.nz,
                                                                       1.0 / (double)e.H(), m);
   ::alfa::note_launch(); k_cs2_finish<<<1, 256, 0, e.stream>>>(m, e.nz, avg1, avg2);
 }
@@ -1263,7 +1282,7 @@ __global__ void k_sl_partial(ScalarLasddFields f, SLConst c, size_t H, int nz, d
 void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10) {
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_sl_partial<<<nb, 128, 0, e.stream>>>(f, sl_const(e), e.H(), e.nz, e.red);
-  ::alfa::note_launch(); k_partial_finish<<<nblocks((size_t)10 * e.nz), TPB, 0, e.stream>>>(e.red, nb, 10, e.nz,
+  ::alfa::note_launch(); k_partial_finish<<<finish_grid((size_t)10 * e.nz), dim3(32, 32), 0, e.stream>>>(e.red, nb, 10, e.nz,
                                                                        1.0 / (double)e.H(), sums10);
 }
 
