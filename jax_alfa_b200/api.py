@@ -845,6 +845,29 @@ class Simulation:
         """Alfa.autotune on this simulation's context (between steps)."""
         return self.alfa.autotune(reps)
 
+    def reset(self, u, v, w, th, Q=None):
+        """Start again from new initial fields (dimensional, as the
+        constructor takes them; torch CPU tensors, pinned for asynchronous
+        copies, or arrays): Main.py's state at iteration istep.  Series and
+        captured step graphs are kept."""
+        a = self.alfa
+        cfg = a.cfg
+        dev = a.device
+
+        def dev_copy(x):
+            t = x if isinstance(x, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(x))
+            return t.to(dev, dtype=F64, non_blocking=True)
+        fields = (dev_copy(u) - cfg["Ugal"], dev_copy(v), dev_copy(w), dev_copy(th) - cfg["T_0"])
+        self._call("alfa_init_state", *[a._f(x) for x in fields])
+        if self.moist:
+            if Q is None:
+                raise ValueError("optMoisture >= 1 needs the initial humidity Q")
+            q = dev_copy(Q)
+            self._call("alfa_init_moisture", a._f(q))
+        # the copies stay referenced until the stream has consumed them
+        self._reset_keep = fields + ((q,) if self.moist else ())
+        return self
+
     def state(self):
         a = self.alfa
         out = [a._new(a.N) for _ in range(5)]

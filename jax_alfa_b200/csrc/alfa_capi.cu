@@ -102,12 +102,14 @@ struct Work {
 struct StepPtrs {
   double *u, *v, *w, *TH, *Cx, *Cy, *Cz, *THadv;
   double *most[6], *most_new[6], *RHS[4], *RHSp[4];
+  double *Q, *Qadvs, *RHSQ, *RHSQp;  // moisture (null when dry)
   static StepPtrs of(const Work& W) {
     StepPtrs p;
     p.u = W.u; p.v = W.v; p.w = W.w; p.TH = W.TH;
     p.Cx = W.Cx; p.Cy = W.Cy; p.Cz = W.Cz; p.THadv = W.THadv;
     for (int i = 0; i < 6; i++) { p.most[i] = W.most[i]; p.most_new[i] = W.most_new[i]; }
     for (int i = 0; i < 4; i++) { p.RHS[i] = W.RHS[i]; p.RHSp[i] = W.RHSp[i]; }
+    p.Q = W.Q; p.Qadvs = W.Qadvs; p.RHSQ = W.RHSQ; p.RHSQp = W.RHSQp;
     return p;
   }
   void apply(Work& W) const {
@@ -115,6 +117,7 @@ struct StepPtrs {
     W.Cx = Cx; W.Cy = Cy; W.Cz = Cz; W.THadv = THadv;
     for (int i = 0; i < 6; i++) { W.most[i] = most[i]; W.most_new[i] = most_new[i]; }
     for (int i = 0; i < 4; i++) { W.RHS[i] = RHS[i]; W.RHSp[i] = RHSp[i]; }
+    W.Q = Q; W.Qadvs = Qadvs; W.RHSQ = RHSQ; W.RHSQp = RHSQp;
   }
   bool operator==(const StepPtrs& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -133,6 +136,7 @@ struct alfa_ctx {
   void* base = nullptr;
   size_t bytes = 0;
   StepGraph graphs[4];  // captured steps by (iteration parity, dynamic SGS step)
+  StepPtrs canon{};     // the buffer arrangement as carved; init_state returns to it
   struct alfa_mlp* mlp = nullptr;  // attached learned-coefficient network
 };
 
@@ -1220,6 +1224,7 @@ int alfa_create(const alfa_config* cfg, alfa_ctx** out) {
   cudaMemset(c->base, 0, c->bytes);
   Carver k2{(char*)c->base, 0, false};
   carve(c, k2);
+  c->canon = StepPtrs::of(c->w);
   *out = c;
   return ALFA_OK;
 }
@@ -1988,6 +1993,16 @@ int alfa_init_state(alfa_ctx* c, const double* u, const double* v, const double*
   Engine& e = c->e;
   Work& W = c->w;
   const size_t N = e.N(), H = e.H();
+  // back to the arrangement the buffers were carved in, so that every run
+  // from init_state swaps through the same sequence (and replays the same
+  // captured step graphs); a humidity field already set moves along
+  if (W.Q && W.Q != c->canon.Q)
+    cudaMemcpyAsync(c->canon.Q, W.Q, N * 8, cudaMemcpyDeviceToDevice, e.stream);
+  c->canon.apply(W);
+  if (W.RHSQ) {
+    cudaMemsetAsync(W.RHSQ, 0, N * 8, e.stream);
+    cudaMemsetAsync(W.RHSQp, 0, N * 8, e.stream);
+  }
   cudaMemcpyAsync(W.u, u, N * 8, cudaMemcpyDeviceToDevice, e.stream);
   cudaMemcpyAsync(W.v, v, N * 8, cudaMemcpyDeviceToDevice, e.stream);
   cudaMemcpyAsync(W.w, w, N * 8, cudaMemcpyDeviceToDevice, e.stream);

@@ -91,3 +91,18 @@ def test_autotune_picks_the_fastest_equivalent_variant(grid):
     for k in base:
         scale = max(np.abs(base[k]).max(), 1e-300)
         assert np.abs(graphed[k] - base[k]).max() <= 1e-12 * scale, k
+
+
+def test_reset_restarts_the_run_bitwise():
+    """Simulation.reset (alfa_init_state on a used context) starts the same
+    run again: the buffers return to their carved arrangement, so the steps
+    (and the step graphs captured before the reset) repeat bit for bit."""
+    cfg = cases.neutral(24, 24, 16, nsteps=6, optMoisture=1, MoistureFlux=5e-5)
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    q = cases.initial_moisture(cfg, 0)
+    fresh = _state(_sim(cfg).step(5, graph=True))
+    s = _sim(cfg).step(3, graph=True)
+    s.reset(u, v, w, th, Q=q)
+    again = _state(s.step(5, graph=True))
+    for k in fresh:
+        assert np.array_equal(fresh[k], again[k]), k
