@@ -62,7 +62,7 @@ __device__ __forceinline__ void y_fwd_load(const Loader& L, int row, int n, int 
 // k_y_fwd: rows x n(y) x nz real -> T (rows, K, nz) complex, ky < K
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
+__global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() == 128 ? 4 : 1))
     k_y_fwd(Loader L, FftPlan p, int K, cd* __restrict__ T) {
   extern __shared__ cd sm[];
   const int n = (N > 0) ? N : p.n;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
 // k_y_inv: T (rows, K, nz), ky < K nonzero -> rows x n(y) x nz real
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(tile_threads<YC, N>(), 1)
+__global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() == 128 ? 4 : 1))
     k_y_inv(const cd* __restrict__ T, int K, FftPlan p, int nz, double scale,
             double* __restrict__ out, int accumulate) {
   extern __shared__ cd sm[];
