@@ -440,6 +440,19 @@ typedef struct alfa_tune_entry {
 int alfa_autotune(alfa_ctx*, int reps, alfa_tune_entry* out /* host */, int max_out,
                   int* n_out /* host */);
 
+/* ---- split-BF16 tensor-core line pass (FP32; no counterpart in the
+ * reference, whose FFT passes run in the run's precision) -----------------
+ * Y (n_out, ncols) = scale * M X for X (n_in, ncols) FP32 row-major (the x
+ * lines of an (nx, ny, nz) FP32 field: n_in = nx, ncols = ny * nz), M the
+ * real operator of line map `map` (1 truncate at `cut`, 2 derivative with the
+ * Nyquist mode zeroed, 3 both, 4 the 3/2 pad n -> 3n/2, 5 the unpad 3n/2 ->
+ * n; 0 identity) exactly as the FP64 line passes apply it.  Runs as a GEMM
+ * on tcgen05 with BF16 hi/lo operand pairs (three products, FP32
+ * accumulation in tensor memory): about 1e-5 relative accuracy.  n_out and
+ * ncols multiples of 128, n_in of 64.  Synchronises the stream. */
+int alfa_tc_line_apply(alfa_ctx*, int map, int cut, int n_in, int n_out, double scale,
+                       long long ncols, const float* X, float* Y);
+
 #ifdef __cplusplus
 }
 #endif

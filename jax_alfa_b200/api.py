@@ -101,6 +101,27 @@ class Alfa:
                         "equal": bool(e.equal), "chosen": bool(e.chosen)})
         return out
 
+    TC_MAPS = {"identity": 0, "truncate": 1, "derivative": 2, "truncate+derivative": 3,
+               "pad": 4, "unpad": 5}
+
+    def tc_line_apply(self, X, map="derivative", n_out=None, scale=None, cut=0):
+        """scale * M X on the tensor cores in split BF16 (alfa_tc_line_apply):
+        X an (n_in, ncols) float32 CUDA tensor of lines stored as rows; M the
+        line map's operator; scale defaults to 1 / n_out, the FP64 passes'
+        normalisation of the unnormalised inverse transform."""
+        m = self.TC_MAPS[map]
+        n_in = X.shape[0]
+        ncols = X[0].numel()
+        if n_out is None:
+            n_out = {4: 3 * n_in // 2, 5: 2 * n_in // 3}.get(m, n_in)
+        if scale is None:
+            scale = 1.0 / n_out
+        Y = torch.empty((n_out,) + tuple(X.shape[1:]), dtype=torch.float32, device=self.device)
+        self._call("alfa_tc_line_apply", m, int(cut), int(n_in), int(n_out), float(scale),
+                   int(ncols), self._p(X, tuple(X.shape), torch.float32),
+                   self._p(Y, tuple(Y.shape), torch.float32))
+        return Y
+
     # ---------------------------------------------------------------- plumbing
     def _call(self, name, *args):
         self.lib.alfa_set_stream(self.ctx, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))

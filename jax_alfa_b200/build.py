@@ -9,7 +9,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalfa.so")
 SOURCES = ["alfa_line.cu", "alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu",
-           "alfa_noalloc.cu", "alfa_mlp.cu"]
+           "alfa_noalloc.cu", "alfa_mlp.cu", "alfa_tc.cu"]
 HEADERS = ["alfa_fft.cuh", "alfa_fft_ct.cuh", "alfa_internal.cuh", "alfa_physics.cuh",
            "alfa_tile.cuh", "alfa_mlp.cuh"]
 

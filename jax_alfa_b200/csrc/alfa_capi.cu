@@ -1963,6 +1963,14 @@ int alfa_autotune(alfa_ctx* c, int reps, alfa_tune_entry* out, int max_out, int*
   return rc;
 }
 
+int alfa_tc_line_apply(alfa_ctx* c, int map, int cut, int n_in, int n_out, double scale,
+                       long long ncols, const float* X, float* Y) {
+  CTX_CHECK(c);
+  NN(X); NN(Y);
+  if (map < LM_IDENT || map > LM_UNPAD) return c->e.fail("tc_line_apply: unknown map", ALFA_E_SHAPE);
+  return tc_line_apply(c->e, map, cut, n_in, n_out, scale, ncols, X, Y);
+}
+
 int alfa_AB2_TH(alfa_ctx* c, const double* TH, const double* R, const double* Rp, double* out) {
   CTX_CHECK(c);
   NN(TH); NN(R); NN(Rp); NN(out);

@@ -143,6 +143,15 @@ struct Engine {
   // transform with radix schedule r of alt_plans (largest radix 8, largest
   // radix 4, ascending order).
   std::map<long long, int> line_variant;
+  // split-BF16 tensor-core line operators built so far (alfa_tc.cu), and
+  // that kernel's error flag
+  struct TcOp {
+    int map, cut, n_in, n_out;
+    double scale;
+    void *hi, *lo;
+  };
+  std::vector<TcOp> tc_ops;
+  int* tc_err = nullptr;
   static constexpr int N_SCHED = 3;
   FftPlan alt_plans[4][N_SCHED];  // for nx, ny, mx, my
 
@@ -175,6 +184,11 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
                  int nout, const LineOut* outs);
 // the autotuner's key of a line pass
 long long line_key(int axis, int n_in, int n_out, int map, int nout);
+// Y (n_out, ncols) = M X (X: (n_in, ncols) FP32) for the line map's
+// operator M times scale, on the tensor cores in split BF16 (alfa_tc.cu);
+// synchronises the stream
+int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale,
+                  long long ncols, const float* X, float* Y);
 // separable spectral operators on real fields
 void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
                       double* scratch2);  // explicit filter and its x/y derivatives

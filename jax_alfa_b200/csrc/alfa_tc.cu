@@ -1,0 +1,369 @@
+// Split-BF16 line passes on the 5th-generation tensor cores (tcgen05).
+//
+// Every separable spectral line pass of the step (truncation, i*k, the 3/2
+// pad and unpad) is a real linear operator along one axis: for a slab of
+// lines stored as rows of an (n_in, ncols) matrix X (x lines of an (nx, ny,
+// nz) field: ncols = ny * nz, contiguous), the pass is Y = M X with M the
+// real n_out x n_in matrix of the map.  Here M X runs as a GEMM on tcgen05
+// with FP32 accumulation in tensor memory, the operands split into BF16
+// pairs (v = v_hi + v_lo, v_hi = bf16(v), v_lo = bf16(v - v_hi)) and three
+// products M_hi X_hi + M_hi X_lo + M_lo X_hi, which keeps about 16
+// significant bits per product (the dropped M_lo X_lo term and the rounding
+// of the lo parts are O(2^-16) relative).
+//
+// Kernel structure (one CTA = 128 threads = one 128 x 128 output tile):
+//   - thread 0's warp allocates 128 TMEM columns (the FP32 accumulator);
+//   - per K chunk of 64: the operator's hi/lo rows are copied to shared
+//     memory and X's FP32 columns are split into hi/lo BF16 there, both in
+//     the K-major no-swizzle core-matrix layout (8 rows x 16 bytes per core
+//     matrix); one thread issues 4 x 3 tcgen05.mma (M = 128, N = 128, K =
+//     16) and commits them to an mbarrier that every thread waits on (with
+//     an iteration limit) before the next chunk reuses the buffers;
+//   - each warp reads its 32 accumulator lanes (rows) back with tcgen05.ld
+//     and stores them; the TMEM columns are freed.
+// No TMA and no multicast: the operand tiles are written by the threads.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "alfa_internal.cuh"
+
+namespace alfa {
+
+namespace tc {
+
+constexpr int BM = 128;   // output rows per tile (operator rows)
+constexpr int BN = 128;   // output columns per tile
+constexpr int BK = 64;    // K per staged chunk
+constexpr int NT = 128;   // threads
+constexpr int TILE_A = BM * BK * 2;  // bytes of one BF16 operator chunk
+constexpr int TILE_B = BN * BK * 2;  // bytes of one BF16 input chunk
+constexpr int SMEM = 2 * TILE_A + 2 * TILE_B + 64;
+constexpr unsigned long long SPIN_LIMIT = 1ull << 22;  // mbarrier polls before giving up
+
+// byte offset of element (row r, k) in a K-major no-swizzle operand tile of
+// `rows` rows: core matrices of 8 rows x 8 BF16 (128 contiguous bytes),
+// consecutive along the rows (stride 128 B), K blocks of 8 at stride
+// rows/8 * 128 B
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int rows) {
+  return (uint32_t)(((k >> 3) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory matrix descriptor (sm_100): start address, leading (K)
+// byte offset, stride (row-group) byte offset, all >> 4; version 1; no
+// swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;                // base offset 0, legacy LBO mode, SWIZZLE_NONE
+}
+
+// instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N = BN, M = BM
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+}
+
+// false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (unsigned long long i = 0; i < SPIN_LIMIT; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// Y[r][c] = scale-free sum_k M[r][k] X[k][c] for one 128 x 128 tile;
+// Mhi/Mlo: (n_out, n_in) BF16 row-major; X: (n_in, ncols) FP32; Y: (n_out,
+// ncols) FP32.  Requires n_out % 128 == 0, ncols % 128 == 0, n_in % 64 == 0.
+__global__ void __launch_bounds__(NT, 1)
+    k_line_gemm_bf16x3(const __nv_bfloat16* __restrict__ Mhi, const __nv_bfloat16* __restrict__ Mlo,
+                       const float* __restrict__ X, float* __restrict__ Y, int n_in, long long ncols,
+                       int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char* sAhi = sm;
+  unsigned char* sAlo = sm + TILE_A;
+  unsigned char* sBhi = sm + 2 * TILE_A;
+  unsigned char* sBlo = sm + 2 * TILE_A + TILE_B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * TILE_A + 2 * TILE_B);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + 2 * TILE_A + 2 * TILE_B + 16);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * BM;
+  const long long n0 = (long long)blockIdx.x * BN;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  bool ok = true;
+  const int nchunks = n_in / BK;
+  for (int ch = 0; ch < nchunks && ok; ch++) {
+    const int k0 = ch * BK;
+    // operator rows: 16-byte units (8 BF16 along K) of BM rows x BK;
+    // consecutive threads take consecutive rows (conflict-free stores)
+    for (int u = tid; u < BM * (BK / 8); u += NT) {
+      const int r = u % BM, kb = u / BM;
+      const size_t g = (size_t)(m0 + r) * n_in + k0 + kb * 8;
+      const uint4 vh = *reinterpret_cast<const uint4*>(Mhi + g);
+      const uint4 vl = *reinterpret_cast<const uint4*>(Mlo + g);
+      const uint32_t o = kmajor_off(r, kb * 8, BM);
+      *reinterpret_cast<uint4*>(sAhi + o) = vh;
+      *reinterpret_cast<uint4*>(sAlo + o) = vl;
+    }
+    // input columns: thread = column, 8 K values per 16-byte unit, split
+    for (int c = tid; c < BN; c += NT) {
+      for (int kb = 0; kb < BK / 8; kb++) {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+          const float x0 = __ldg(&X[(size_t)(k0 + kb * 8 + j) * ncols + n0 + c]);
+          const float x1 = __ldg(&X[(size_t)(k0 + kb * 8 + j + 1) * ncols + n0 + c]);
+          const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+          const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+          const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+          h[j / 2] = pack_bf16(h0, h1);
+          l[j / 2] = pack_bf16(l0, l1);
+        }
+        const uint32_t o = kmajor_off(c, kb * 8, BN);
+        *reinterpret_cast<uint4*>(sBhi + o) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(sBlo + o) = make_uint4(l[0], l[1], l[2], l[3]);
+      }
+    }
+    // the tensor cores read shared memory through the async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (tid == 0) {
+      const uint32_t lboA = (BM / 8) * 128, lboB = (BN / 8) * 128, sbo = 128;
+#pragma unroll
+      for (int ks = 0; ks < BK / 16; ks++) {
+        const uint32_t offA = ks * 2 * lboA, offB = ks * 2 * lboB;
+        const uint64_t ah = smem_desc(smem_u32(sAhi) + offA, lboA, sbo);
+        const uint64_t al = smem_desc(smem_u32(sAlo) + offA, lboA, sbo);
+        const uint64_t bh = smem_desc(smem_u32(sBhi) + offB, lboB, sbo);
+        const uint64_t bl = smem_desc(smem_u32(sBlo) + offB, lboB, sbo);
+        mma_bf16(tmem, ah, bh, (ch > 0 || ks > 0) ? 1u : 0u);
+        mma_bf16(tmem, ah, bl, 1u);
+        mma_bf16(tmem, al, bh, 1u);
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(bar))
+          : "memory");
+    }
+    // every thread waits for the chunk's products before the buffers are
+    // rewritten (and, after the last chunk, before the accumulator is read)
+    const bool mine = mbar_wait(smem_u32(bar), (uint32_t)(ch & 1));
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    ok = __syncthreads_and(mine) != 0;  // uniform across the CTA
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    // warp w holds accumulator lanes (rows) 32w .. 32w + 31
+    const int r = warp * 32 + lane;
+    float* yrow = Y + (size_t)(m0 + r) * ncols + n0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+          "%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; j += 4)
+        *reinterpret_cast<float4*>(yrow + c0 + j) =
+            make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                        __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+}
+
+}  // namespace tc
+
+// ---------------------------------------------------------------------------
+// host: the operator matrix of a line map, split into BF16 hi/lo
+// ---------------------------------------------------------------------------
+
+// the spectral map of line_map (alfa_line.cu) for output bin k of n_out from
+// an n_in-point spectrum: the source bin (or -1) and the multiplier
+static void map_bin(int map, int cut, int n_in, int n_out, int k, int* src, double* mul) {
+  *src = k;
+  *mul = 1.0;
+  const int n = n_in;
+  switch (map) {
+    case LM_IDENT:
+      return;
+    case LM_TRUNC:
+      if (!(k < cut || k >= n - cut + 1)) *src = -1;
+      return;
+    case LM_DERIV:
+    case LM_TRUNC_DERIV: {
+      if (map == LM_TRUNC_DERIV && !(k < cut || k >= n - cut + 1)) {
+        *src = -1;
+        return;
+      }
+      const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
+      *mul = (double)kk;  // times i
+      return;
+    }
+    case LM_PAD: {
+      const int h = n / 2, m = n_out;
+      if (k <= h) *src = k;
+      else if (k >= m - h) *src = k - m + n;
+      else *src = -1;
+      return;
+    }
+    default: {  // LM_UNPAD: n_in = m = 3 n_out / 2
+      const int h = n_out / 2;
+      if (k < h) *src = k;
+      else if (k == h) *src = -1;
+      else *src = k - n_out + n_in;
+      return;
+    }
+  }
+}
+
+// M[j][i] = scale * Re sum_k map(k) e^{+2 pi i k j / n_out} e^{-2 pi i src(k) i / n_in},
+// with the angles from per-length tables (long double, rounded once)
+static void operator_matrix(int map, int cut, int n_in, int n_out, double scale,
+                            std::vector<double>& M) {
+  M.assign((size_t)n_out * n_in, 0.0);
+  const long double two_pi = 6.283185307179586476925286766559L;
+  std::vector<double> co(n_out), so(n_out), ci(n_in), si(n_in);
+  for (int t = 0; t < n_out; t++) {
+    co[t] = (double)cosl(two_pi * t / n_out);
+    so[t] = (double)sinl(two_pi * t / n_out);
+  }
+  for (int t = 0; t < n_in; t++) {
+    ci[t] = (double)cosl(two_pi * t / n_in);
+    si[t] = (double)sinl(two_pi * t / n_in);
+  }
+  const bool deriv = (map == LM_DERIV || map == LM_TRUNC_DERIV);
+  for (int k = 0; k < n_out; k++) {
+    int src;
+    double mul;
+    map_bin(map, cut, n_in, n_out, k, &src, &mul);
+    if (src < 0 || mul == 0.0) continue;
+    for (int j = 0; j < n_out; j++) {
+      const int a = (int)((long long)k * j % n_out);
+      const double c1 = co[a], s1 = so[a];
+      double* row = M.data() + (size_t)j * n_in;
+      for (int i = 0; i < n_in; i++) {
+        const int b = (int)((long long)src * i % n_in);
+        const double c2 = ci[b], s2 = si[b];
+        // e^{i(t1 - t2)}: real c1 c2 + s1 s2, imaginary s1 c2 - c1 s2; the
+        // derivative multiplies by i k (real part -k * imaginary)
+        row[i] += deriv ? -mul * (s1 * c2 - c1 * s2) : (c1 * c2 + s1 * s2);
+      }
+    }
+  }
+  for (double& v : M) v *= scale;
+}
+
+int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale,
+                  long long ncols, const float* X, float* Y) {
+  if (n_out % tc::BM || ncols % tc::BN || n_in % tc::BK || ncols <= 0 || n_in <= 0)
+    return e.fail("tc_line_apply: n_out and ncols must be multiples of 128, n_in of 64",
+                  ALFA_E_SHAPE);
+  if ((map == LM_PAD && 2 * n_out != 3 * n_in) || (map == LM_UNPAD && 3 * n_out != 2 * n_in) ||
+      (map != LM_PAD && map != LM_UNPAD && n_in != n_out))
+    return e.fail("tc_line_apply: lengths do not match the map", ALFA_E_SHAPE);
+  // operators are built once per context and kept in its engine
+  Engine::TcOp* op = nullptr;
+  for (auto& o : e.tc_ops)
+    if (o.map == map && o.cut == cut && o.n_in == n_in && o.n_out == n_out && o.scale == scale)
+      op = &o;
+  if (!op) {
+    std::vector<double> M;
+    operator_matrix(map, cut, n_in, n_out, scale, M);
+    std::vector<__nv_bfloat16> hi(M.size()), lo(M.size());
+    for (size_t t = 0; t < M.size(); t++) {
+      const float f = (float)M[t];
+      hi[t] = __float2bfloat16_rn(f);
+      lo[t] = __float2bfloat16_rn(f - __bfloat162float(hi[t]));
+    }
+    Engine::TcOp o{map, cut, n_in, n_out, scale, nullptr, nullptr};
+    if (cudaMalloc(&o.hi, M.size() * 2) != cudaSuccess) return e.fail("tc: allocation failed", ALFA_E_CUDA);
+    e.allocs.push_back(o.hi);
+    if (cudaMalloc(&o.lo, M.size() * 2) != cudaSuccess) return e.fail("tc: allocation failed", ALFA_E_CUDA);
+    e.allocs.push_back(o.lo);
+    cudaMemcpy(o.hi, hi.data(), M.size() * 2, cudaMemcpyHostToDevice);
+    cudaMemcpy(o.lo, lo.data(), M.size() * 2, cudaMemcpyHostToDevice);
+    e.tc_ops.push_back(o);
+    op = &e.tc_ops.back();
+  }
+  if (!e.tc_err) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess)
+      return e.fail("tc_line_apply: flag allocation failed", ALFA_E_CUDA);
+    e.allocs.push_back(p);
+    e.tc_err = (int*)p;
+  }
+  int* d_err = e.tc_err;
+  cudaMemsetAsync(d_err, 0, sizeof(int), e.stream);
+  cudaFuncSetAttribute((const void*)tc::k_line_gemm_bf16x3,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
+  dim3 g((unsigned)(ncols / tc::BN), (unsigned)(n_out / tc::BM));
+  ::alfa::note_launch();
+  tc::k_line_gemm_bf16x3<<<g, tc::NT, tc::SMEM, e.stream>>>(
+      (const __nv_bfloat16*)op->hi, (const __nv_bfloat16*)op->lo, X, Y, n_in, ncols, d_err);
+  int h = 0;
+  cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
+  if (cudaStreamSynchronize(e.stream) != cudaSuccess)
+    return e.fail("tc_line_apply: kernel failed", ALFA_E_CUDA);
+  if (h) return e.fail("tc_line_apply: a bounded tensor-core wait gave up", ALFA_E_TIMEOUT);
+  return ALFA_OK;
+}
+
+}  // namespace alfa
