@@ -136,6 +136,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_bf16_peak():
+    """Dense BF16 TFLOP/s (burst) from MEASURED_PEAKS.json, else the
+    fallback figure of this pool."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
 def ncu_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/), or None."""
@@ -292,6 +304,20 @@ def run_alfa(args, rank, world, dist):
         if which in probes and chosen.get(shape, "default") != "default":
             probes[which]["kernel"] = (f"{shape} line pass, autotuned variant "
                                        f"'{chosen[shape]}'")
+    # the split-BF16 tensor-core line pass (FP32 x derivative of a field of
+    # this grid): issued tensor flops and bytes per launch
+    tc = None
+    if a.lib.alfa_time_kernel(a.ctx, 8, 20, ctypes.byref(t_ms), ctypes.byref(t_bytes)) == 0:
+        nx_, ny_, nz_ = grid
+        flops = 3 * 2.0 * nx_ * nx_ * ny_ * nz_
+        tflops = flops / (t_ms.value * 1e-3) / 1e12
+        bf16_peak, bf16_kind = measured_bf16_peak()
+        gbs = t_bytes.value / (t_ms.value * 1e-3) / 1e9
+        tc = {"kernel": "k_line_gemm_bf16x3 (x derivative, FP32 lines, split BF16 on tcgen05)",
+              "avg_launch_ms": t_ms.value, "alg_bytes_per_launch": t_bytes.value,
+              "achieved_gbs": gbs, "hbm_frac": gbs / peak, "issued_tflops": tflops,
+              "tensor_frac": tflops / bf16_peak,
+              "tensor_peak": f"{bf16_kind} {bf16_peak:.0f} TFLOP/s bf16 dense (burst)"}
     dom = 1  # the pad passes hold the largest share of the step (profiles/)
     if dom in probes:
         tr = ncu_traffic()
@@ -395,6 +421,7 @@ def run_alfa(args, rank, world, dist):
             "dtype": "f64", "data": "synthetic", "config": config_block(grid, world),
             "clocks": clk, "gpu_launches": int(n1 - n0), "roofline": roof,
             "cpu_baseline": cpu, "e2e": e2e, "e2e_per_function": e2e_pf,
+            "tensor_core_line_pass": tc,
             "autotune": [{k: c[k] for k in ("shape", "variant", "ms")} for c in tune
                          if c["chosen"]],
         }), flush=True)

@@ -410,6 +410,8 @@ unsigned long long alfa_launch_count(void);
  *   5 y-forward real -> half spectrum (2-D path)   (reads N, writes S)
  *   6 x-column: forward FFT + two i*k outputs      (reads S, writes 2 S)
  *   7 y-inverse half spectrum -> real (2-D path)   (reads S, writes N)
+ *   8 x derivative of an FP32 field on the tensor cores (alfa_tc_line_apply's
+ *     kernel; reads and writes N floats; 3 x 2 nx^2 ny nz issued BF16 flops)
  * (N, P, S: real, padded real and half-spectrum complex field sizes.)
  * ms = average duration of one launch; bytes = its algorithmic HBM bytes. */
 int alfa_time_kernel(alfa_ctx*, int which, int reps, double* ms /* host */,

@@ -1727,8 +1727,15 @@ unsigned long long alfa_launch_count(void) { return g_launches.load(); }
 
 int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes) {
   CTX_CHECK(c);
-  if (!ms || !bytes || reps < 1 || which < 0 || which > 7)
+  if (!ms || !bytes || reps < 1 || which < 0 || which > 8)
     return c->e.fail("time_kernel: bad arguments", ALFA_E_SHAPE);
+  Engine::TcOp* tcop = nullptr;
+  const long long tc_cols = (long long)c->e.ny * c->e.nz;
+  if (which == 8) {  // x derivative of an FP32 field on the tensor cores
+    const int st = tc_prepare(c->e, LM_DERIV, 0, c->e.nx, c->e.nx, 1.0 / c->e.nx, tc_cols, &tcop);
+    if (st) return st;
+    cudaMemsetAsync(c->e.tc_err, 0, sizeof(int), c->e.stream);
+  }
   Engine& e = c->e;
   Work& W = c->w;
   const double N8 = 8.0 * e.N(), Y8 = 8.0 * e.nx * e.my * e.nz, P8 = 8.0 * e.P();
@@ -1780,6 +1787,10 @@ int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes
       }
       case 5: launch_y_fwd(e, ld_field(e, W.u), e.nx, e.pny, e.nyh, e.T[0]); break;
       case 6: launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh); break;
+      case 8:  // FP32 in and out in two padded-field buffers (P doubles each)
+        tc_launch(e, tcop, tc_cols, reinterpret_cast<const float*>(W.Pb[6]),
+                  reinterpret_cast<float*>(W.Pb[7]));
+        break;
       default: launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, 1.0, e.W, 0); break;
     }
   };
@@ -1809,7 +1820,14 @@ int alfa_time_kernel(alfa_ctx* c, int which, int reps, double* ms, double* bytes
     case 4: *bytes = 2 * N8; break;
     case 5: *bytes = N8 + S16; break;
     case 6: *bytes = 3 * S16; break;
+    case 8: *bytes = N8; break;  // N floats in, N floats out
     default: *bytes = S16 + N8; break;
+  }
+  if (which == 8) {
+    int h = 0;
+    cudaMemcpyAsync(&h, e.tc_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
+    cudaStreamSynchronize(e.stream);
+    if (h) return e.fail("time_kernel: a bounded tensor-core wait gave up", ALFA_E_TIMEOUT);
   }
   return check_launch(e, "time_kernel");
 }

@@ -189,6 +189,11 @@ long long line_key(int axis, int n_in, int n_out, int map, int nout);
 // synchronises the stream
 int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale,
                   long long ncols, const float* X, float* Y);
+// the same in parts: the operator (built once, checks the shapes) and one
+// asynchronous launch
+int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, long long ncols,
+               Engine::TcOp** out);
+void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y);
 // separable spectral operators on real fields
 void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
                       double* scratch2);  // explicit filter and its x/y derivatives

@@ -311,8 +311,8 @@ static void operator_matrix(int map, int cut, int n_in, int n_out, double scale,
   for (double& v : M) v *= scale;
 }
 
-int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale,
-                  long long ncols, const float* X, float* Y) {
+int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, long long ncols,
+               Engine::TcOp** out) {
   if (n_out % tc::BM || ncols % tc::BN || n_in % tc::BK || ncols <= 0 || n_in <= 0)
     return e.fail("tc_line_apply: n_out and ncols must be multiples of 128, n_in of 64",
                   ALFA_E_SHAPE);
@@ -350,16 +350,30 @@ int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale
     e.allocs.push_back(p);
     e.tc_err = (int*)p;
   }
-  int* d_err = e.tc_err;
-  cudaMemsetAsync(d_err, 0, sizeof(int), e.stream);
   cudaFuncSetAttribute((const void*)tc::k_line_gemm_bf16x3,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
-  dim3 g((unsigned)(ncols / tc::BN), (unsigned)(n_out / tc::BM));
+  *out = op;
+  return ALFA_OK;
+}
+
+// one launch (asynchronous; a wait that gave up sets e.tc_err)
+void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y) {
+  dim3 g((unsigned)(ncols / tc::BN), (unsigned)(op->n_out / tc::BM));
   ::alfa::note_launch();
   tc::k_line_gemm_bf16x3<<<g, tc::NT, tc::SMEM, e.stream>>>(
-      (const __nv_bfloat16*)op->hi, (const __nv_bfloat16*)op->lo, X, Y, n_in, ncols, d_err);
+      (const __nv_bfloat16*)op->hi, (const __nv_bfloat16*)op->lo, X, Y, op->n_in, ncols,
+      e.tc_err);
+}
+
+int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale,
+                  long long ncols, const float* X, float* Y) {
+  Engine::TcOp* op = nullptr;
+  const int st = tc_prepare(e, map, cut, n_in, n_out, scale, ncols, &op);
+  if (st) return st;
+  cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
+  tc_launch(e, op, ncols, X, Y);
   int h = 0;
-  cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
+  cudaMemcpyAsync(&h, e.tc_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
   if (cudaStreamSynchronize(e.stream) != cudaSuccess)
     return e.fail("tc_line_apply: kernel failed", ALFA_E_CUDA);
   if (h) return e.fail("tc_line_apply: a bounded tensor-core wait gave up", ALFA_E_TIMEOUT);
