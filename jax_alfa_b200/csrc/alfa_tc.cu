@@ -43,6 +43,9 @@ constexpr int TILE_A = BM * BK * 2;  // bytes of one BF16 operator chunk
 constexpr int TILE_B = BN * BK * 2;  // bytes of one BF16 input chunk
 constexpr int SMEM = 2 * TILE_A + 2 * TILE_B + 64;
 constexpr unsigned long long SPIN_LIMIT = 1ull << 22;  // mbarrier polls before giving up
+constexpr int A_UNITS = BM * (BK / 8) / NT;  // 16-byte operator units per thread and chunk
+static_assert(NT == 128 && BN == 4 * 32 && BK / 8 == 2 * (NT / 32),
+              "input staging: 4 warps x 2 K blocks, 32 threads x 4 columns");
 
 // byte offset of element (row r, k) in a K-major no-swizzle operand tile of
 // `rows` rows: core matrices of 8 rows x 8 BF16 (128 contiguous bytes),
@@ -139,32 +142,51 @@ __global__ void __launch_bounds__(NT, 1)
   const int nchunks = n_in / BK;
   for (int ch = 0; ch < nchunks && ok; ch++) {
     const int k0 = ch * BK;
-    // operator rows: 16-byte units (8 BF16 along K) of BM rows x BK;
-    // consecutive threads take consecutive rows (conflict-free stores)
-    for (int u = tid; u < BM * (BK / 8); u += NT) {
+    // Every global load of the chunk is issued before any is used (the
+    // chunk is one memory round trip).  Operator: 16-byte units (8 BF16
+    // along K) of BM rows x BK, consecutive threads on consecutive rows.
+    uint4 ah[A_UNITS], al[A_UNITS];
+#pragma unroll
+    for (int q = 0; q < A_UNITS; q++) {
+      const int u = tid + q * NT;
       const int r = u % BM, kb = u / BM;
       const size_t g = (size_t)(m0 + r) * n_in + k0 + kb * 8;
-      const uint4 vh = *reinterpret_cast<const uint4*>(Mhi + g);
-      const uint4 vl = *reinterpret_cast<const uint4*>(Mlo + g);
-      const uint32_t o = kmajor_off(r, kb * 8, BM);
-      *reinterpret_cast<uint4*>(sAhi + o) = vh;
-      *reinterpret_cast<uint4*>(sAlo + o) = vl;
+      ah[q] = __ldg(reinterpret_cast<const uint4*>(Mhi + g));
+      al[q] = __ldg(reinterpret_cast<const uint4*>(Mlo + g));
     }
-    // input columns: thread = column, 8 K values per 16-byte unit, split
-    for (int c = tid; c < BN; c += NT) {
-      for (int kb = 0; kb < BK / 8; kb++) {
+    // input: thread (group grp, lane t4) reads 4 consecutive columns
+    // 4 t4 .. 4 t4 + 3 of the rows of K blocks 2 grp and 2 grp + 1
+    const int grp = tid >> 5, t4 = tid & 31;
+    float4 xv[2][8];
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        xv[b][j] = __ldg(reinterpret_cast<const float4*>(
+            X + (size_t)(k0 + (2 * grp + b) * 8 + j) * ncols + n0 + 4 * t4));
+#pragma unroll
+    for (int q = 0; q < A_UNITS; q++) {
+      const int u = tid + q * NT;
+      const uint32_t o = kmajor_off(u % BM, (u / BM) * 8, BM);
+      *reinterpret_cast<uint4*>(sAhi + o) = ah[q];
+      *reinterpret_cast<uint4*>(sAlo + o) = al[q];
+    }
+    // split each column's 8 K values into hi / lo BF16 units
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+#pragma unroll
+      for (int e4 = 0; e4 < 4; e4++) {
         uint32_t h[4], l[4];
 #pragma unroll
         for (int j = 0; j < 8; j += 2) {
-          const float x0 = __ldg(&X[(size_t)(k0 + kb * 8 + j) * ncols + n0 + c]);
-          const float x1 = __ldg(&X[(size_t)(k0 + kb * 8 + j + 1) * ncols + n0 + c]);
+          const float x0 = (&xv[b][j].x)[e4], x1 = (&xv[b][j + 1].x)[e4];
           const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
           const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
           const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
           h[j / 2] = pack_bf16(h0, h1);
           l[j / 2] = pack_bf16(l0, l1);
         }
-        const uint32_t o = kmajor_off(c, kb * 8, BN);
+        const uint32_t o = kmajor_off(4 * t4 + e4, (2 * grp + b) * 8, BN);
         *reinterpret_cast<uint4*>(sBhi + o) = make_uint4(h[0], h[1], h[2], h[3]);
         *reinterpret_cast<uint4*>(sBlo + o) = make_uint4(l[0], l[1], l[2], l[3]);
       }
