@@ -13,12 +13,14 @@
 //
 // Kernel structure (one CTA = 128 threads = one 128 x 128 output tile):
 //   - thread 0's warp allocates 128 TMEM columns (the FP32 accumulator);
-//   - per K chunk of 64: the operator's hi/lo rows are copied to shared
+//   - per K chunk of 32: the operator's hi/lo rows are copied to shared
 //     memory and X's FP32 columns are split into hi/lo BF16 there, both in
 //     the K-major no-swizzle core-matrix layout (8 rows x 16 bytes per core
-//     matrix); one thread issues 4 x 3 tcgen05.mma (M = 128, N = 128, K =
-//     16) and commits them to an mbarrier that every thread waits on (with
-//     an iteration limit) before the next chunk reuses the buffers;
+//     matrix), into one of two stages; one thread issues 2 x 3 tcgen05.mma
+//     (M = 128, N = 128, K = 16) and commits them to that stage's mbarrier,
+//     which every thread waits on (with an iteration limit) before the
+//     stage is rewritten two chunks later, so a chunk's loads overlap the
+//     previous chunk's products;
 //   - each warp reads its 32 accumulator lanes (rows) back with tcgen05.ld
 //     and stores them; the TMEM columns are freed.
 // No TMA and no multicast: the operand tiles are written by the threads.
@@ -37,15 +39,16 @@ namespace tc {
 
 constexpr int BM = 128;   // output rows per tile (operator rows)
 constexpr int BN = 128;   // output columns per tile
-constexpr int BK = 64;    // K per staged chunk
+constexpr int BK = 32;    // K per staged chunk (two chunks in flight: stages 0 and 1)
 constexpr int NT = 128;   // threads
 constexpr int TILE_A = BM * BK * 2;  // bytes of one BF16 operator chunk
 constexpr int TILE_B = BN * BK * 2;  // bytes of one BF16 input chunk
-constexpr int SMEM = 2 * TILE_A + 2 * TILE_B + 64;
+constexpr int STAGE = 2 * TILE_A + 2 * TILE_B;  // hi and lo of both operands
+constexpr int SMEM = 2 * STAGE + 64;
 constexpr unsigned long long SPIN_LIMIT = 1ull << 22;  // mbarrier polls before giving up
 constexpr int A_UNITS = BM * (BK / 8) / NT;  // 16-byte operator units per thread and chunk
-static_assert(NT == 128 && BN == 4 * 32 && BK / 8 == 2 * (NT / 32),
-              "input staging: 4 warps x 2 K blocks, 32 threads x 4 columns");
+static_assert(NT == 128 && BN == 4 * 32 && BK / 8 == NT / 32,
+              "input staging: one K block of 8 per warp, 32 threads x 4 columns");
 
 // byte offset of element (row r, k) in a K-major no-swizzle operand tile of
 // `rows` rows: core matrices of 8 rows x 8 BF16 (128 contiguous bytes),
@@ -104,24 +107,109 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) 
   return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
 
-// Y[r][c] = scale-free sum_k M[r][k] X[k][c] for one 128 x 128 tile;
-// Mhi/Mlo: (n_out, n_in) BF16 row-major; X: (n_in, ncols) FP32; Y: (n_out,
-// ncols) FP32.  Requires n_out % 128 == 0, ncols % 128 == 0, n_in % 64 == 0.
+// one chunk's global loads, all issued before any is used
+struct ChunkRegs {
+  uint4 ah[A_UNITS], al[A_UNITS];
+  float4 xv[8];
+};
+
+__device__ __forceinline__ void load_chunk(ChunkRegs& R, const __nv_bfloat16* __restrict__ Mhi,
+                                           const __nv_bfloat16* __restrict__ Mlo,
+                                           const float* __restrict__ X, int n_in,
+                                           long long ncols, int m0, long long n0, int k0,
+                                           int tid) {
+  // operator: 16-byte units (8 BF16 along K), consecutive threads on
+  // consecutive rows
+#pragma unroll
+  for (int q = 0; q < A_UNITS; q++) {
+    const int u = tid + q * NT;
+    const size_t g = (size_t)(m0 + u % BM) * n_in + k0 + (u / BM) * 8;
+    R.ah[q] = __ldg(reinterpret_cast<const uint4*>(Mhi + g));
+    R.al[q] = __ldg(reinterpret_cast<const uint4*>(Mlo + g));
+  }
+  // input: warp w reads the 8 rows of K block w, lane t4 the 4 consecutive
+  // columns 4 t4 .. 4 t4 + 3
+  const int w = tid >> 5, t4 = tid & 31;
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    R.xv[j] = __ldg(
+        reinterpret_cast<const float4*>(X + (size_t)(k0 + w * 8 + j) * ncols + n0 + 4 * t4));
+}
+
+// the chunk into a stage: operator units as they are, input columns split
+// into hi / lo BF16 units of 8 K values
+__device__ __forceinline__ void store_chunk(const ChunkRegs& R, unsigned char* stage, int tid) {
+  unsigned char* sAhi = stage;
+  unsigned char* sAlo = stage + TILE_A;
+  unsigned char* sBhi = stage + 2 * TILE_A;
+  unsigned char* sBlo = stage + 2 * TILE_A + TILE_B;
+#pragma unroll
+  for (int q = 0; q < A_UNITS; q++) {
+    const int u = tid + q * NT;
+    const uint32_t o = kmajor_off(u % BM, (u / BM) * 8, BM);
+    *reinterpret_cast<uint4*>(sAhi + o) = R.ah[q];
+    *reinterpret_cast<uint4*>(sAlo + o) = R.al[q];
+  }
+  const int w = tid >> 5, t4 = tid & 31;
+#pragma unroll
+  for (int e4 = 0; e4 < 4; e4++) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      const float x0 = (&R.xv[j].x)[e4], x1 = (&R.xv[j + 1].x)[e4];
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+      const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+      const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+      h[j / 2] = pack_bf16(h0, h1);
+      l[j / 2] = pack_bf16(l0, l1);
+    }
+    const uint32_t o = kmajor_off(4 * t4 + e4, w * 8, BN);
+    *reinterpret_cast<uint4*>(sBhi + o) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(sBlo + o) = make_uint4(l[0], l[1], l[2], l[3]);
+  }
+}
+
+// the three products of one staged chunk (one thread), committed to `bar`
+__device__ __forceinline__ void mma_chunk(uint32_t tmem, const unsigned char* stage, bool first,
+                                          uint32_t bar) {
+  const uint32_t lboA = (BM / 8) * 128, lboB = (BN / 8) * 128, sbo = 128;
+  const uint32_t a = smem_u32(stage), b = a + 2 * TILE_A;
+#pragma unroll
+  for (int ks = 0; ks < BK / 16; ks++) {
+    const uint32_t offA = ks * 2 * lboA, offB = ks * 2 * lboB;
+    const uint64_t ah = smem_desc(a + offA, lboA, sbo);
+    const uint64_t al = smem_desc(a + TILE_A + offA, lboA, sbo);
+    const uint64_t bh = smem_desc(b + offB, lboB, sbo);
+    const uint64_t bl = smem_desc(b + TILE_B + offB, lboB, sbo);
+    mma_bf16(tmem, ah, bh, (first && ks == 0) ? 0u : 1u);
+    mma_bf16(tmem, ah, bl, 1u);
+    mma_bf16(tmem, al, bh, 1u);
+  }
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+
+// Y[r][c] = sum_k M[r][k] X[k][c] for one 128 x 128 tile; Mhi/Mlo: (n_out,
+// n_in) BF16 row-major; X: (n_in, ncols) FP32; Y: (n_out, ncols) FP32.
+// Requires n_out % 128 == 0, ncols % 128 == 0, n_in % 32 == 0.  Two stages:
+// the loads of chunk ch are in flight while the products of chunk ch - 1
+// run; stage ch % 2 is rewritten once the products of chunk ch - 2 (the
+// barrier of that stage) have completed.
 __global__ void __launch_bounds__(NT, 1)
     k_line_gemm_bf16x3(const __nv_bfloat16* __restrict__ Mhi, const __nv_bfloat16* __restrict__ Mlo,
                        const float* __restrict__ X, float* __restrict__ Y, int n_in, long long ncols,
                        int* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  unsigned char* sAhi = sm;
-  unsigned char* sAlo = sm + TILE_A;
-  unsigned char* sBhi = sm + 2 * TILE_A;
-  unsigned char* sBlo = sm + 2 * TILE_A + TILE_B;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * TILE_A + 2 * TILE_B);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + 2 * TILE_A + 2 * TILE_B + 16);
+  unsigned char* stages[2] = {sm, sm + STAGE};
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * STAGE);  // bar[0], bar[1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + 2 * STAGE + 32);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.y * BM;
-  const long long n0 = (long long)blockIdx.x * BN;
+  // blockIdx.x runs over the operator's row tiles: the CTAs that read the
+  // same input columns are neighbours, so the second read comes from L2
+  const int m0 = blockIdx.x * BM;
+  const long long n0 = (long long)blockIdx.y * BN;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -131,6 +219,7 @@ __global__ void __launch_bounds__(NT, 1)
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar + 1)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -140,85 +229,29 @@ __global__ void __launch_bounds__(NT, 1)
 
   bool ok = true;
   const int nchunks = n_in / BK;
-  for (int ch = 0; ch < nchunks && ok; ch++) {
-    const int k0 = ch * BK;
-    // Every global load of the chunk is issued before any is used (the
-    // chunk is one memory round trip).  Operator: 16-byte units (8 BF16
-    // along K) of BM rows x BK, consecutive threads on consecutive rows.
-    uint4 ah[A_UNITS], al[A_UNITS];
-#pragma unroll
-    for (int q = 0; q < A_UNITS; q++) {
-      const int u = tid + q * NT;
-      const int r = u % BM, kb = u / BM;
-      const size_t g = (size_t)(m0 + r) * n_in + k0 + kb * 8;
-      ah[q] = __ldg(reinterpret_cast<const uint4*>(Mhi + g));
-      al[q] = __ldg(reinterpret_cast<const uint4*>(Mlo + g));
+  ChunkRegs R;
+  for (int ch = 0; ch < nchunks; ch++) {
+    const int s = ch & 1;
+    load_chunk(R, Mhi, Mlo, X, n_in, ncols, m0, n0, ch * BK, tid);
+    bool mine = true;
+    if (ch >= 2) {  // stage s still feeds the products of chunk ch - 2
+      mine = mbar_wait(smem_u32(bar + s), (uint32_t)(((ch - 2) >> 1) & 1));
+      asm volatile("tcgen05.fence::after_thread_sync;");
     }
-    // input: thread (group grp, lane t4) reads 4 consecutive columns
-    // 4 t4 .. 4 t4 + 3 of the rows of K blocks 2 grp and 2 grp + 1
-    const int grp = tid >> 5, t4 = tid & 31;
-    float4 xv[2][8];
-#pragma unroll
-    for (int b = 0; b < 2; b++)
-#pragma unroll
-      for (int j = 0; j < 8; j++)
-        xv[b][j] = __ldg(reinterpret_cast<const float4*>(
-            X + (size_t)(k0 + (2 * grp + b) * 8 + j) * ncols + n0 + 4 * t4));
-#pragma unroll
-    for (int q = 0; q < A_UNITS; q++) {
-      const int u = tid + q * NT;
-      const uint32_t o = kmajor_off(u % BM, (u / BM) * 8, BM);
-      *reinterpret_cast<uint4*>(sAhi + o) = ah[q];
-      *reinterpret_cast<uint4*>(sAlo + o) = al[q];
-    }
-    // split each column's 8 K values into hi / lo BF16 units
-#pragma unroll
-    for (int b = 0; b < 2; b++) {
-#pragma unroll
-      for (int e4 = 0; e4 < 4; e4++) {
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int j = 0; j < 8; j += 2) {
-          const float x0 = (&xv[b][j].x)[e4], x1 = (&xv[b][j + 1].x)[e4];
-          const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-          const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-          const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-          h[j / 2] = pack_bf16(h0, h1);
-          l[j / 2] = pack_bf16(l0, l1);
-        }
-        const uint32_t o = kmajor_off(4 * t4 + e4, (2 * grp + b) * 8, BN);
-        *reinterpret_cast<uint4*>(sBhi + o) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(sBlo + o) = make_uint4(l[0], l[1], l[2], l[3]);
-      }
-    }
+    store_chunk(R, stages[s], tid);
     // the tensor cores read shared memory through the async proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (tid == 0) {
-      const uint32_t lboA = (BM / 8) * 128, lboB = (BN / 8) * 128, sbo = 128;
-#pragma unroll
-      for (int ks = 0; ks < BK / 16; ks++) {
-        const uint32_t offA = ks * 2 * lboA, offB = ks * 2 * lboB;
-        const uint64_t ah = smem_desc(smem_u32(sAhi) + offA, lboA, sbo);
-        const uint64_t al = smem_desc(smem_u32(sAlo) + offA, lboA, sbo);
-        const uint64_t bh = smem_desc(smem_u32(sBhi) + offB, lboB, sbo);
-        const uint64_t bl = smem_desc(smem_u32(sBlo) + offB, lboB, sbo);
-        mma_bf16(tmem, ah, bh, (ch > 0 || ks > 0) ? 1u : 0u);
-        mma_bf16(tmem, ah, bl, 1u);
-        mma_bf16(tmem, al, bh, 1u);
-      }
-      asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(bar))
-          : "memory");
-    }
-    // every thread waits for the chunk's products before the buffers are
-    // rewritten (and, after the last chunk, before the accumulator is read)
-    const bool mine = mbar_wait(smem_u32(bar), (uint32_t)(ch & 1));
-    asm volatile("tcgen05.fence::after_thread_sync;");
     ok = __syncthreads_and(mine) != 0;  // uniform across the CTA
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok) break;
+    if (tid == 0) mma_chunk(tmem, stages[s], ch == 0, smem_u32(bar + s));
+  }
+  if (ok) {  // the last commit covers every product issued before it
+    const int L = nchunks - 1;
+    const bool mine = mbar_wait(smem_u32(bar + (L & 1)), (uint32_t)((L >> 1) & 1));
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    ok = __syncthreads_and(mine) != 0;
   }
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
@@ -336,7 +369,7 @@ static void operator_matrix(int map, int cut, int n_in, int n_out, double scale,
 int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, long long ncols,
                Engine::TcOp** out) {
   if (n_out % tc::BM || ncols % tc::BN || n_in % tc::BK || ncols <= 0 || n_in <= 0)
-    return e.fail("tc_line_apply: n_out and ncols must be multiples of 128, n_in of 64",
+    return e.fail("tc_line_apply: n_out and ncols must be multiples of 128, n_in of 32",
                   ALFA_E_SHAPE);
   if ((map == LM_PAD && 2 * n_out != 3 * n_in) || (map == LM_UNPAD && 3 * n_out != 2 * n_in) ||
       (map != LM_PAD && map != LM_UNPAD && n_in != n_out))
@@ -380,7 +413,7 @@ int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, l
 
 // one launch (asynchronous; a wait that gave up sets e.tc_err)
 void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y) {
-  dim3 g((unsigned)(ncols / tc::BN), (unsigned)(op->n_out / tc::BM));
+  dim3 g((unsigned)(op->n_out / tc::BM), (unsigned)(ncols / tc::BN));
   ::alfa::note_launch();
   tc::k_line_gemm_bf16x3<<<g, tc::NT, tc::SMEM, e.stream>>>(
       (const __nv_bfloat16*)op->hi, (const __nv_bfloat16*)op->lo, X, Y, op->n_in, ncols,
