@@ -44,7 +44,10 @@ constexpr int NT = 128;   // threads
 constexpr int TILE_A = BM * BK * 2;  // bytes of one BF16 operator chunk
 constexpr int TILE_B = BN * BK * 2;  // bytes of one BF16 input chunk
 constexpr int STAGE = 2 * TILE_A + 2 * TILE_B;  // hi and lo of both operands
-constexpr int SMEM = 2 * STAGE + 64;
+constexpr int TROW = BN + 4;  // epilogue tile row stride (floats): conflict-free writes
+constexpr int EPI = BM * TROW * 4;  // epilogue tile bytes (reuses the stages)
+constexpr int BARS = (EPI > 2 * STAGE ? EPI : 2 * STAGE);  // barriers after both
+constexpr int SMEM = BARS + 64;
 constexpr unsigned long long SPIN_LIMIT = 1ull << 22;  // mbarrier polls before giving up
 constexpr int A_UNITS = BM * (BK / 8) / NT;  // 16-byte operator units per thread and chunk
 static_assert(NT == 128 && BN == 4 * 32 && BK / 8 == NT / 32,
@@ -193,17 +196,17 @@ __device__ __forceinline__ void mma_chunk(uint32_t tmem, const unsigned char* st
 // Y[r][c] = sum_k M[r][k] X[k][c] for one 128 x 128 tile; Mhi/Mlo: (n_out,
 // n_in) BF16 row-major; X: (n_in, ncols) FP32; Y: (n_out, ncols) FP32.
 // Requires n_out % 128 == 0, ncols % 128 == 0, n_in % 32 == 0.  Two stages:
-// the loads of chunk ch are in flight while the products of chunk ch - 1
-// run; stage ch % 2 is rewritten once the products of chunk ch - 2 (the
-// barrier of that stage) have completed.
-__global__ void __launch_bounds__(NT, 1)
+// the loads of chunk ch + 1 are in flight while chunk ch is staged and its
+// products run; stage ch % 2 is rewritten once the products of chunk ch - 2
+// (the barrier of that stage) have completed.
+__global__ void __launch_bounds__(NT, 2)
     k_line_gemm_bf16x3(const __nv_bfloat16* __restrict__ Mhi, const __nv_bfloat16* __restrict__ Mlo,
                        const float* __restrict__ X, float* __restrict__ Y, int n_in, long long ncols,
                        int* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* stages[2] = {sm, sm + STAGE};
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * STAGE);  // bar[0], bar[1]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + 2 * STAGE + 32);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + BARS);  // bar[0], bar[1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + BARS + 32);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // blockIdx.x runs over the operator's row tiles: the CTAs that read the
@@ -229,10 +232,14 @@ __global__ void __launch_bounds__(NT, 1)
 
   bool ok = true;
   const int nchunks = n_in / BK;
-  ChunkRegs R;
-  for (int ch = 0; ch < nchunks; ch++) {
+  // two register sets: chunk ch + 1's loads are in flight while chunk ch is
+  // converted, stored and multiplied (the loop is unrolled by two so each
+  // set stays in registers)
+  ChunkRegs R0, R1;
+  load_chunk(R0, Mhi, Mlo, X, n_in, ncols, m0, n0, 0, tid);
+  if (nchunks > 1) load_chunk(R1, Mhi, Mlo, X, n_in, ncols, m0, n0, BK, tid);
+  auto step = [&](ChunkRegs& R, int ch) {
     const int s = ch & 1;
-    load_chunk(R, Mhi, Mlo, X, n_in, ncols, m0, n0, ch * BK, tid);
     bool mine = true;
     if (ch >= 2) {  // stage s still feeds the products of chunk ch - 2
       mine = mbar_wait(smem_u32(bar + s), (uint32_t)(((ch - 2) >> 1) & 1));
@@ -244,8 +251,13 @@ __global__ void __launch_bounds__(NT, 1)
     asm volatile("tcgen05.fence::before_thread_sync;");
     ok = __syncthreads_and(mine) != 0;  // uniform across the CTA
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (!ok) break;
+    if (!ok) return;
     if (tid == 0) mma_chunk(tmem, stages[s], ch == 0, smem_u32(bar + s));
+    if (ch + 2 < nchunks) load_chunk(R, Mhi, Mlo, X, n_in, ncols, m0, n0, (ch + 2) * BK, tid);
+  };
+  for (int ch = 0; ch < nchunks && ok; ch += 2) {
+    step(R0, ch);
+    if (ok && ch + 1 < nchunks) step(R1, ch + 1);
   }
   if (ok) {  // the last commit covers every product issued before it
     const int L = nchunks - 1;
@@ -256,9 +268,11 @@ __global__ void __launch_bounds__(NT, 1)
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
   } else {
-    // warp w holds accumulator lanes (rows) 32w .. 32w + 31
+    // warp w holds accumulator lanes (rows) 32w .. 32w + 31; the tile goes
+    // through shared memory (the stages are free now) so that the global
+    // stores are whole 512-byte row segments
     const int r = warp * 32 + lane;
-    float* yrow = Y + (size_t)(m0 + r) * ncols + n0;
+    float* T = reinterpret_cast<float*>(sm);
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
       uint32_t v[16];
@@ -273,9 +287,16 @@ __global__ void __launch_bounds__(NT, 1)
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
       for (int j = 0; j < 16; j += 4)
-        *reinterpret_cast<float4*>(yrow + c0 + j) =
+        *reinterpret_cast<float4*>(T + r * TROW + c0 + j) =
             make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
                         __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int it = 0; it < BM / 4; it++) {
+      const int row = it * 4 + warp;
+      *reinterpret_cast<float4*>(Y + (size_t)(m0 + row) * ncols + n0 + 4 * lane) =
+          *reinterpret_cast<const float4*>(T + row * TROW + 4 * lane);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
