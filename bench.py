@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--epochs", type=int, default=40,
+                    help="training epochs of the learned closure (--learned)")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the line-pass autotuner (default dispatch)")
     ap.add_argument("--learned", action="store_true",
@@ -505,7 +507,7 @@ def run_learned(args):
         net.collect(5000)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    loss = net.train(epochs=40, batch=1024, lr=2e-3)
+    loss = net.train(epochs=args.epochs, batch=1024, lr=2e-3)
     ev1.record()
     torch.cuda.synchronize()
     t_train = ev0.elapsed_time(ev1) / 1e3
@@ -547,7 +549,7 @@ def run_learned(args):
         "profile_errors_vs_dynamic": errs,
         "judge": {"every": 10, "tol": 0.05, "refresh": "20000 samples, 3 epochs per judge step",
                   "report": rep},
-        "training": {"samples": 200000, "after_spinup_steps": 160, "epochs": 40,
+        "training": {"samples": 200000, "after_spinup_steps": 160, "epochs": args.epochs,
                      "batch": 1024, "seconds": t_train,
                      "final_loss_normalised": loss},
         "dtype": "f64 step, f32 network (bf16 weights at inference)", "data": "synthetic",
