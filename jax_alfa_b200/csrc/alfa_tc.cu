@@ -236,6 +236,7 @@ __global__ void __launch_bounds__(NT, 2)
   // converted, stored and multiplied (the loop is unrolled by two so each
   // set stays in registers)
   ChunkRegs R0, R1;
+  int committed = -1;  // the last chunk whose products were issued
   load_chunk(R0, Mhi, Mlo, X, n_in, ncols, m0, n0, 0, tid);
   if (nchunks > 1) load_chunk(R1, Mhi, Mlo, X, n_in, ncols, m0, n0, BK, tid);
   auto step = [&](ChunkRegs& R, int ch) {
@@ -253,6 +254,7 @@ __global__ void __launch_bounds__(NT, 2)
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (!ok) return;
     if (tid == 0) mma_chunk(tmem, stages[s], ch == 0, smem_u32(bar + s));
+    committed = ch;
     if (ch + 2 < nchunks) load_chunk(R, Mhi, Mlo, X, n_in, ncols, m0, n0, (ch + 2) * BK, tid);
   };
   for (int ch = 0; ch < nchunks && ok; ch += 2) {
@@ -267,6 +269,10 @@ __global__ void __launch_bounds__(NT, 2)
   }
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
+    // a wait gave up: wait once more (bounded) for the products in flight
+    // before the accumulator columns are freed
+    if (committed >= 0)
+      mbar_wait(smem_u32(bar + (committed & 1)), (uint32_t)((committed >> 1) & 1));
   } else {
     // warp w holds accumulator lanes (rows) 32w .. 32w + 31; the tile goes
     // through shared memory (the stages are free now) so that the global
