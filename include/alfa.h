@@ -451,7 +451,7 @@ int alfa_autotune(alfa_ctx*, int reps, alfa_tune_entry* out /* host */, int max_
  * n; 0 identity) exactly as the FP64 line passes apply it.  Runs as a GEMM
  * on tcgen05 with BF16 hi/lo operand pairs (three products, FP32
  * accumulation in tensor memory): about 1e-5 relative accuracy.  n_out and
- * ncols multiples of 128, n_in of 32.  Synchronises the stream. */
+ * n_out a multiple of 128, ncols of 256, n_in of 32.  Synchronises the stream. */
 int alfa_tc_line_apply(alfa_ctx*, int map, int cut, int n_in, int n_out, double scale,
                        long long ncols, const float* X, float* Y);
 

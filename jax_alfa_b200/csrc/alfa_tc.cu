@@ -11,18 +11,19 @@
 // significant bits per product (the dropped M_lo X_lo term and the rounding
 // of the lo parts are O(2^-16) relative).
 //
-// Kernel structure (one CTA = 128 threads = one 128 x 128 output tile):
-//   - thread 0's warp allocates 128 TMEM columns (the FP32 accumulator);
+// Kernel structure (one CTA = 256 threads = one 128 x 256 output tile):
+//   - warp 0 allocates 256 TMEM columns (the FP32 accumulator);
 //   - per K chunk of 32: the operator's hi/lo rows are copied to shared
 //     memory and X's FP32 columns are split into hi/lo BF16 there, both in
 //     the K-major no-swizzle core-matrix layout (8 rows x 16 bytes per core
 //     matrix), into one of two stages; one thread issues 2 x 3 tcgen05.mma
-//     (M = 128, N = 128, K = 16) and commits them to that stage's mbarrier,
+//     (M = 128, N = 256, K = 16) and commits them to that stage's mbarrier,
 //     which every thread waits on (with an iteration limit) before the
 //     stage is rewritten two chunks later, so a chunk's loads overlap the
 //     previous chunk's products;
-//   - each warp reads its 32 accumulator lanes (rows) back with tcgen05.ld
-//     and stores them; the TMEM columns are freed.
+//   - the warps read the accumulator back with tcgen05.ld (32 lanes each)
+//     into a shared-memory tile, half the columns at a time, and store whole
+//     row segments; the TMEM columns are freed.
 // No TMA and no multicast: the operand tiles are written by the threads.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -38,20 +39,22 @@ namespace alfa {
 namespace tc {
 
 constexpr int BM = 128;   // output rows per tile (operator rows)
-constexpr int BN = 128;   // output columns per tile
+constexpr int BN = 256;   // output columns per tile
 constexpr int BK = 32;    // K per staged chunk (two chunks in flight: stages 0 and 1)
-constexpr int NT = 128;   // threads
+constexpr int NT = 256;   // threads
 constexpr int TILE_A = BM * BK * 2;  // bytes of one BF16 operator chunk
 constexpr int TILE_B = BN * BK * 2;  // bytes of one BF16 input chunk
 constexpr int STAGE = 2 * TILE_A + 2 * TILE_B;  // hi and lo of both operands
-constexpr int TROW = BN + 4;  // epilogue tile row stride (floats): conflict-free writes
+constexpr int EH = 128;        // epilogue columns per pass (two passes over BN)
+constexpr int TROW = EH + 4;   // epilogue tile row stride (floats): conflict-free writes
 constexpr int EPI = BM * TROW * 4;  // epilogue tile bytes (reuses the stages)
 constexpr int BARS = (EPI > 2 * STAGE ? EPI : 2 * STAGE);  // barriers after both
 constexpr int SMEM = BARS + 64;
 constexpr unsigned long long SPIN_LIMIT = 1ull << 22;  // mbarrier polls before giving up
 constexpr int A_UNITS = BM * (BK / 8) / NT;  // 16-byte operator units per thread and chunk
-static_assert(NT == 128 && BN == 4 * 32 && BK / 8 == NT / 32,
-              "input staging: one K block of 8 per warp, 32 threads x 4 columns");
+static_assert(NT == 256 && BN == 2 * 4 * 32 && BK / 8 == 4 && BN == 2 * EH,
+              "input staging: warp w takes K block w % 4 and column half w / 4, 32 threads x "
+              "4 columns; the epilogue runs in two halves");
 
 // byte offset of element (row r, k) in a K-major no-swizzle operand tile of
 // `rows` rows: core matrices of 8 rows x 8 BF16 (128 contiguous bytes),
@@ -130,13 +133,14 @@ __device__ __forceinline__ void load_chunk(ChunkRegs& R, const __nv_bfloat16* __
     R.ah[q] = __ldg(reinterpret_cast<const uint4*>(Mhi + g));
     R.al[q] = __ldg(reinterpret_cast<const uint4*>(Mlo + g));
   }
-  // input: warp w reads the 8 rows of K block w, lane t4 the 4 consecutive
-  // columns 4 t4 .. 4 t4 + 3
+  // input: warp w reads the 8 rows of K block w % 4 in column half w / 4,
+  // lane t4 the 4 consecutive columns 4 t4 .. 4 t4 + 3 of that half
   const int w = tid >> 5, t4 = tid & 31;
+  const int kbw = w & 3, col = (w >> 2) * 128 + 4 * t4;
 #pragma unroll
   for (int j = 0; j < 8; j++)
     R.xv[j] = __ldg(
-        reinterpret_cast<const float4*>(X + (size_t)(k0 + w * 8 + j) * ncols + n0 + 4 * t4));
+        reinterpret_cast<const float4*>(X + (size_t)(k0 + kbw * 8 + j) * ncols + n0 + col));
 }
 
 // the chunk into a stage: operator units as they are, input columns split
@@ -154,6 +158,7 @@ __device__ __forceinline__ void store_chunk(const ChunkRegs& R, unsigned char* s
     *reinterpret_cast<uint4*>(sAlo + o) = R.al[q];
   }
   const int w = tid >> 5, t4 = tid & 31;
+  const int kbw = w & 3, col = (w >> 2) * 128 + 4 * t4;
 #pragma unroll
   for (int e4 = 0; e4 < 4; e4++) {
     uint32_t h[4], l[4];
@@ -166,7 +171,7 @@ __device__ __forceinline__ void store_chunk(const ChunkRegs& R, unsigned char* s
       h[j / 2] = pack_bf16(h0, h1);
       l[j / 2] = pack_bf16(l0, l1);
     }
-    const uint32_t o = kmajor_off(4 * t4 + e4, w * 8, BN);
+    const uint32_t o = kmajor_off(col + e4, kbw * 8, BN);
     *reinterpret_cast<uint4*>(sBhi + o) = make_uint4(h[0], h[1], h[2], h[3]);
     *reinterpret_cast<uint4*>(sBlo + o) = make_uint4(l[0], l[1], l[2], l[3]);
   }
@@ -195,7 +200,7 @@ __device__ __forceinline__ void mma_chunk(uint32_t tmem, const unsigned char* st
 
 // Y[r][c] = sum_k M[r][k] X[k][c] for one 128 x 128 tile; Mhi/Mlo: (n_out,
 // n_in) BF16 row-major; X: (n_in, ncols) FP32; Y: (n_out, ncols) FP32.
-// Requires n_out % 128 == 0, ncols % 128 == 0, n_in % 32 == 0.  Two stages:
+// Requires n_out % 128 == 0, ncols % 256 == 0, n_in % 32 == 0.  Two stages:
 // the loads of chunk ch + 1 are in flight while chunk ch is staged and its
 // products run; stage ch % 2 is rewritten once the products of chunk ch - 2
 // (the barrier of that stage) have completed.
@@ -274,35 +279,43 @@ __global__ void __launch_bounds__(NT, 2)
     if (committed >= 0)
       mbar_wait(smem_u32(bar + (committed & 1)), (uint32_t)((committed >> 1) & 1));
   } else {
-    // warp w holds accumulator lanes (rows) 32w .. 32w + 31; the tile goes
-    // through shared memory (the stages are free now) so that the global
-    // stores are whole 512-byte row segments
-    const int r = warp * 32 + lane;
+    // warp w may read accumulator lanes (rows) 32 (w % 4) .. + 31; the tile
+    // goes through shared memory (the stages are free now), one half of the
+    // columns at a time, so that the global stores are whole 512-byte row
+    // segments
+    const int r = (warp & 3) * 32 + lane;
     float* T = reinterpret_cast<float*>(sm);
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-      uint32_t v[16];
-      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-          "%14,%15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(addr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    for (int h = 0; h < BN / EH; h++) {
+      if ((warp >> 2) == h) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < EH; c0 += 16) {
+          uint32_t v[16];
+          const uint32_t addr =
+              tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(h * EH + c0);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+              "%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+              : "r"(addr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int j = 0; j < 16; j += 4)
-        *reinterpret_cast<float4*>(T + r * TROW + c0 + j) =
-            make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
-                        __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
-    }
-    __syncthreads();
+          for (int j = 0; j < 16; j += 4)
+            *reinterpret_cast<float4*>(T + r * TROW + c0 + j) =
+                make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                            __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+        }
+      }
+      __syncthreads();
 #pragma unroll 4
-    for (int it = 0; it < BM / 4; it++) {
-      const int row = it * 4 + warp;
-      *reinterpret_cast<float4*>(Y + (size_t)(m0 + row) * ncols + n0 + 4 * lane) =
-          *reinterpret_cast<const float4*>(T + row * TROW + 4 * lane);
+      for (int it = 0; it < BM / (NT / 32); it++) {
+        const int row = it * (NT / 32) + warp;
+        *reinterpret_cast<float4*>(Y + (size_t)(m0 + row) * ncols + n0 + h * EH + 4 * lane) =
+            *reinterpret_cast<const float4*>(T + row * TROW + 4 * lane);
+      }
+      __syncthreads();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -396,7 +409,7 @@ static void operator_matrix(int map, int cut, int n_in, int n_out, double scale,
 int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, long long ncols,
                Engine::TcOp** out) {
   if (n_out % tc::BM || ncols % tc::BN || n_in % tc::BK || ncols <= 0 || n_in <= 0)
-    return e.fail("tc_line_apply: n_out and ncols must be multiples of 128, n_in of 32",
+    return e.fail("tc_line_apply: n_out must be a multiple of 128, ncols of 256, n_in of 32",
                   ALFA_E_SHAPE);
   if ((map == LM_PAD && 2 * n_out != 3 * n_in) || (map == LM_UNPAD && 3 * n_out != 2 * n_in) ||
       (map != LM_PAD && map != LM_UNPAD && n_in != n_out))
