@@ -390,8 +390,10 @@ int alfa_load_checkpoint(alfa_ctx*, const double* src);
  * Limit: nz <= 2048 (larger returns ALFA_E_NOALLOC_LIMIT before any launch).
  * The partial sums live in a fixed 4 MiB array inside the library, one per
  * device that loads it, kept until the process exits.  The first call on each
- * device looks that array's address up (with the device current); make that
- * first call before any stream capture.  All calls on a device share the
+ * device looks that array's address up (with the device current), and so
+ * does the first call after the device's context was replaced (for example
+ * by cudaDeviceReset); make such calls before any stream capture.  All calls
+ * on a device share the
  * array: calls that overlap on the GPU (different streams, no ordering)
  * race and must be serialised by the caller. */
 int alfa_PlanarMean_noalloc(const double* F, int nx, int ny, int nz, double* mean_nz,

@@ -11,6 +11,11 @@
 
 namespace alfa {
 
+// Partial-sum blocks of the plane mean behind alfa_PlanarMean_noalloc: the
+// launch (alfa_physics.cu) and the fixed partial-sum array it fills
+// (alfa_noalloc.cu) are both sized by this one constant.
+constexpr int NOALLOC_RED_BLOCKS = 256;
+
 // Process-wide count of kernel launches made by this library (every launch
 // site calls note_launch(); read through alfa_launch_count()).
 void note_launch();

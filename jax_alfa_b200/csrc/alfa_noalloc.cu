@@ -14,6 +14,8 @@
 // those partials live in a fixed array in the library's device image, so
 // nothing is allocated at call time.  Every device that loads the library
 // holds its own copy of the array until the process exits.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "alfa.h"
@@ -27,31 +29,74 @@ void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials
 
 namespace {
 
-constexpr int kBlocks = 256;       // partial sums per level (as plane_means)
-constexpr int kMaxLevels = 2048;   // largest nz accepted
+constexpr int kBlocks = alfa::NOALLOC_RED_BLOCKS;  // partial sums per level (the launch's blocks)
+constexpr int kMaxLevels = 2048;                   // largest nz accepted
 // 256 x 2048 doubles = 4 MiB per device
 static __device__ __align__(256) double g_partials[kBlocks * kMaxLevels];
 
+// Driver entry points that identify the current context, fetched through the
+// runtime (no link against the driver library).  Either may stay null on a
+// driver without it; the cache below is then bypassed.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+std::once_flag g_entry_once;
+
+// Id of the context current on this thread, 0 when none is current or the
+// id cannot be read.  Ids are unique within the process, so a device whose
+// primary context was destroyed (cudaDeviceReset) and re-created reports a
+// new one.
+unsigned long long current_context_id() {
+  std::call_once(g_entry_once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  });
+  if (!g_ctx_current || !g_ctx_id) return 0;
+  CUcontext c = nullptr;
+  if (g_ctx_current(&c) != CUDA_SUCCESS || c == nullptr) return 0;
+  unsigned long long id = 0;
+  if (g_ctx_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
 std::mutex g_mu;
 constexpr int kMaxDevices = 256;
-double* g_addr[kMaxDevices] = {};
+struct Cached {
+  unsigned long long ctx = 0;  // context the address belongs to
+  double* addr = nullptr;
+};
+Cached g_addr[kMaxDevices];
 
-// Device address of g_partials on the current device, looked up once per
-// device with that device current.  (In host code the name g_partials is a
-// host-side stand-in, not a device address, so it is never passed as is.)
+// Device address of g_partials on the current device, looked up with that
+// device current the first time and again whenever the device's context has
+// changed since (the old address died with the old context).  In host code
+// the name g_partials is a host-side stand-in, not a device address, so it is
+// never passed as is.
 int partials_on_current_device(double** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ALFA_E_CUDA;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (g_addr[dev] == nullptr) {
+  Cached& slot = g_addr[dev];
+  const unsigned long long ctx = current_context_id();
+  if (slot.addr == nullptr || ctx == 0 || slot.ctx != ctx) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_partials) != cudaSuccess || p == nullptr) {
       cudaGetLastError();
       return ALFA_E_CUDA;
     }
-    g_addr[dev] = static_cast<double*>(p);
+    slot.addr = static_cast<double*>(p);
+    slot.ctx = current_context_id();  // the lookup made the device's context current
   }
-  *out = g_addr[dev];
+  *out = slot.addr;
   return ALFA_OK;
 }
 

@@ -27,8 +27,6 @@ static inline int nblocks(size_t n, int tpb = TPB) {
 // latency-bound); e.red holds RED_BLOCKS x 18 x nz partials
 static constexpr int RED_BLOCKS = 1024;
 static constexpr int RED_MAXQ = 16;
-// the no-allocation entry's fixed partial array holds 256 x nz
-static constexpr int NOALLOC_RED_BLOCKS = 256;
 
 struct RedArgs {
   const double* f[RED_MAXQ];

@@ -198,7 +198,7 @@ __device__ __forceinline__ void mma_chunk(uint32_t tmem, const unsigned char* st
       : "memory");
 }
 
-// Y[r][c] = sum_k M[r][k] X[k][c] for one 128 x 128 tile; Mhi/Mlo: (n_out,
+// Y[r][c] = sum_k M[r][k] X[k][c] for one 128 x 256 tile (256 TMEM columns); Mhi/Mlo: (n_out,
 // n_in) BF16 row-major; X: (n_in, ncols) FP32; Y: (n_out, ncols) FP32.
 // Requires n_out % 128 == 0, ncols % 256 == 0, n_in % 32 == 0.  Two stages:
 // the loads of chunk ch + 1 are in flight while chunk ch is staged and its

@@ -20,7 +20,8 @@ result is one ``.npz`` per case:
   function's calls from the start of the run;
   ``final.<name>`` for the model state after the last step.
 
-Usage (from the repository root, with the reference checkout present):
+Usage (from the repository root; the reference checkout is given by --reference or
+$ALFA_REFERENCE_DIR):
     python tests/golden/make_golden.py --case neutral --grid 16 16 12 \
         --steps 2 --record 1 2 --out tests/golden/ref_neutral_16x16x12.npz
 """
@@ -35,7 +36,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("ALFA_REFERENCE_DIR", "/root/reference")
+# the reference checkout: --reference DIR, else $ALFA_REFERENCE_DIR (no default)
+REFERENCE = os.environ.get("ALFA_REFERENCE_DIR")
 
 TAPPED = {
     "src.operations.Filtering": ["Filtering_Explicit"],
@@ -159,6 +161,7 @@ def run(case, grid, steps, record, out_path, seed, overrides, final_names=FINAL_
 
 
 def main():
+    global REFERENCE
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default="neutral")
     ap.add_argument("--grid", type=int, nargs=3, default=[16, 16, 12])
@@ -170,7 +173,12 @@ def main():
     ap.add_argument("--final", nargs="*", default=FINAL_NAMES,
                     help="model-state names kept after the last step")
     ap.add_argument("--out", required=True)
+    ap.add_argument("--reference", default=REFERENCE,
+                    help="the JAX-ALFA checkout (default: $ALFA_REFERENCE_DIR)")
     a = ap.parse_args()
+    if not a.reference or not os.path.isdir(os.path.join(a.reference, "src")):
+        ap.error("give the JAX-ALFA checkout with --reference DIR or ALFA_REFERENCE_DIR")
+    REFERENCE = a.reference
     import ast
     over = {}
     for kv in a.set:

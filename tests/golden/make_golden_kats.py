@@ -20,7 +20,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("ALFA_REFERENCE_DIR", "/root/reference")
+# the reference checkout: --reference DIR, else $ALFA_REFERENCE_DIR (no default)
+REFERENCE = os.environ.get("ALFA_REFERENCE_DIR")
 
 TEST_ROOT_CASES = [([1.0, 0.0, -4.0], 1.0), ([1.0, 0.0, 0.0, -1.0], 0.5),
                    ([1.0, -3.0], 1.0), ([0.1, 0.3, 0.6, 0.1, 2.0, 1.0], 1.0)]
@@ -28,9 +29,15 @@ GUESSES = [0.5, 0.75, 1.0, 1.25, 1.5, 2.0, 3.0, 4.5]
 
 
 def main():
+    global REFERENCE
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
+    ap.add_argument("--reference", default=REFERENCE,
+                    help="the JAX-ALFA checkout (default: $ALFA_REFERENCE_DIR)")
     a = ap.parse_args()
+    if not a.reference or not os.path.isdir(os.path.join(a.reference, "src")):
+        ap.error("give the JAX-ALFA checkout with --reference DIR or ALFA_REFERENCE_DIR")
+    REFERENCE = a.reference
     sys.path.insert(0, os.path.join(HERE, "jaxshim"))
     sys.path.insert(0, REFERENCE)
     sys.path.insert(0, REPO)

@@ -20,7 +20,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("ALFA_REFERENCE_DIR", "/root/reference")
+# the reference checkout: --reference DIR, else $ALFA_REFERENCE_DIR (no default)
+REFERENCE = os.environ.get("ALFA_REFERENCE_DIR")
 
 GRID = (12, 16, 8)
 FIELDS = ("u", "v", "w", "TH", "dudz", "dvdz", "dTHdz", "txy", "txz", "tyz", "qz",
@@ -46,9 +47,15 @@ def sample_inputs(rng, nx, ny, nz):
 
 
 def main():
+    global REFERENCE
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
+    ap.add_argument("--reference", default=REFERENCE,
+                    help="the JAX-ALFA checkout (default: $ALFA_REFERENCE_DIR)")
     a = ap.parse_args()
+    if not a.reference or not os.path.isdir(os.path.join(a.reference, "src")):
+        ap.error("give the JAX-ALFA checkout with --reference DIR or ALFA_REFERENCE_DIR")
+    REFERENCE = a.reference
     sys.path.insert(0, os.path.join(HERE, "jaxshim"))
     sys.path.insert(0, REFERENCE)
     sys.path.insert(0, REPO)
