@@ -1,21 +1,32 @@
 """Throughput of the LES step on B200: grid-point-steps per second.
 
-Workload (default): the neutral ABL case at 256^3 (LASDD-SM dynamic SGS,
-3/2-rule dealiasing, Thomas pressure solve), FP64 -- the 256^3 LASDD-SM
-FP64 configuration of the reference's A100 benchmark table.  Synthetic
-seeded initial fields (log-law u with 0.5 % noise below 500 m); every field
-(134 MB) is larger than L2 (126 MB), so no L2 flush is needed between steps.
+Workload: the reference's own neutral-boundary-layer benchmark (NBL_A94,
+Andren et al. 1994) at 256^3: a neutral Ekman layer under a 5 m/s
+geostrophic wind in a 4000 m cube, Ugal = 3 m/s, LASDD-SM dynamic SGS every
+step, 3/2-rule dealiasing, Thomas pressure solve, AB2 at dt = 0.75 s
+(examples/NBL_A94/runs/256x256x256_LASDD_SM_DP/Config.py, the configuration
+of the reference's A100 figures).  Seeded synthetic initial fields of that
+case's form (u = 5 m/s, theta = 300 K, Gaussian noise below 200 m).  Every
+field (4 or 8 B x 16.8 M points) is larger than L2 (126 MB), so no flush is
+needed between steps.
 
-  value  : device-timed whole steps (alfa_step, state resident in HBM),
-           CUDA events on the launching stream, max over ranks.
-  e2e    : the same steps through the reference-facing per-function API
-           (jax_alfa_b200.driver.MainLoop, the Main.py loop on the C-ABI),
-           with the initial state copied in from pinned host memory, the
-           forcing row going in and the CFL check coming out every step, and
-           the final state copied back, all inside the timed region.
-  --impl reference : the reference's CPU implementation of the same step
-           (the NumPy FP64 port of it, scipy.fft with every host thread) on a
-           bounded sample: one step of the same physics on a 128^3 grid.
+The metric compares the mixed-precision step with the plain FP64 drop-in on
+the same GPU:
+  value   : the mixed-precision step (FP32 fields and transforms, split-BF16
+            tensor-core line passes where the autotuner measures them faster,
+            FP64 pressure tridiagonal solve, zero mode, plane means, beta
+            roots and surface layer), device-timed CUDA-graph steps with the
+            state resident in HBM, CUDA events on the launching stream, max
+            over ranks;
+  fp64    : the same for the FP64 drop-in, with the speed-up of the mixed
+            step over it and the mixed state's error against the FP64 state
+            after the same steps from the same initial fields;
+  e2e     : the mixed step through the whole-step C-ABI with the state from
+            and to pinned host memory and the CFL diagnostics read back every
+            step, all inside the timed region;
+  cpu_baseline / --impl reference : the reference's algorithm on the host
+            (the NumPy FP64 port of it, scipy.fft on every host thread) on
+            the same 256^3 workload, a bounded number of steps.
 
 Multi-GPU: ``replicas only`` -- each rank advances its own independent
 simulation (no data-path collective); scaling is weak.
@@ -33,8 +44,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-A100_BASELINE = 93.4e6   # gp-steps/s, 256^3 LASDD-SM FP64 on A100 (reference notebook)
-METRIC = "LES grid-point-steps/s at 256^3"
+# the reference's A100 JAX figures for NBL_A94 256^3 LASDD-SM
+A100_FP64 = 93.4e6   # gp-steps/s, FP64
+A100_FP32 = 166.8e6  # gp-steps/s, FP32
+METRIC = "LES grid-point-steps/s at 256^3: mixed-prec vs plain FP64 on B200, err vs FP64"
+DTYPES = {"mixed": "f32 fields + split-bf16 tensor-core line passes + f64 solves/means",
+          "fp32": "f32 fields + f64 solves/means", "fp64": "f64"}
 
 
 def parse():
@@ -44,8 +59,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="alfa", choices=["alfa", "reference"])
     ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"],
+                    help="the form timed as the headline value")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=60.0,
+                    help="seconds of host time for the cpu_baseline sample")
     ap.add_argument("--epochs", type=int, default=40,
                     help="training epochs of the learned closure (--learned)")
     ap.add_argument("--no-tune", action="store_true",
@@ -59,21 +79,34 @@ def parse():
     return ap.parse_args()
 
 
-def workload_config(grid, nsteps):
+def workload_config(grid, nsteps, precision="fp64"):
     from jax_alfa_b200 import cases
-    cfg = cases.neutral(*grid, nsteps=nsteps)
-    cfg["case"] = "neutral"
-    return cfg
+    return cases.nbl_a94(*grid, nsteps=nsteps, precision=precision)
 
 
-def config_block(grid, world):
-    return {"workload": f"neutral ABL {grid[0]}x{grid[1]}x{grid[2]}, LASDD-SM dynamic SGS, "
-                        "3/2-rule dealiasing, Thomas pressure, AB2, FP64",
+def config_block(grid, world, precision):
+    return {"workload": f"NBL_A94 neutral Ekman layer {grid[0]}x{grid[1]}x{grid[2]} (the "
+                        "reference's 256^3 benchmark case), LASDD-SM dynamic SGS, 3/2-rule "
+                        "dealiasing, Thomas pressure, AB2, dt 0.75 s",
             "grid": list(grid), "sgs": "LASDD-SM (optSgs=1, dynamic every step)",
-            "precision": "FP64 plain drop-in", "l2": "every field (8 B x N) exceeds L2; no flush",
+            "precision": precision, "l2": "every field exceeds L2 (126 MB); no flush",
             "step": "one CUDA graph replay per step (alfa_step_graph)",
             "parallelism": f"replicas x{world} (no sharding)",
-            "baseline": "A100 JAX 256^3 LASDD-SM FP64, 93.4 M gp-steps/s"}
+            "baseline": "A100 JAX NBL_A94 256^3 LASDD-SM: FP32 166.8 M, FP64 93.4 M gp-steps/s"}
+
+
+def cpu_info():
+    """Host threads and the CPU model (lscpu)."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return os.cpu_count() or 1, model
 
 
 class ClockSampler:
@@ -163,68 +196,62 @@ def ncu_traffic():
     return None
 
 
-def cpu_baseline(threads, grid=(128, 128, 128)):
-    """One step of the NumPy FP64 port of the reference on the host."""
+def oracle_steps(grid, threads, warmup, steps, budget_s):
+    """The NumPy FP64 port of the reference's step on the host: `warmup`
+    untimed steps, then timed steps until `steps` are done or the next one
+    would pass `budget_s` seconds.  Returns (timed steps, seconds)."""
     from jax_alfa_b200 import cases
     from oracle import alfa_oracle
-    from oracle.alfa_oracle import AlfaOracle, OracleRun
+    from oracle.alfa_oracle import OracleRun
     alfa_oracle.set_fft_workers(threads)
-    cfg = workload_config(grid, 2)
+    cfg = workload_config(grid, warmup + steps + 1)
     u, v, w, th = cases.initial_fields(cfg, 0)
-    o = AlfaOracle(cfg)
-    r = OracleRun(cfg, u, v, w, th, adv=o.adv_series(*cases.adv_forcing_series(cfg)))
-    t = time.perf_counter()
+    r = OracleRun(cfg, u, v, w, th)  # no forcing series: NBL_A94 has none
     with np.errstate(all="ignore"):
-        r.step()
-    dt = time.perf_counter() - t
-    n = grid[0] * grid[1] * grid[2]
-    return n / dt, dt
+        for _ in range(warmup):
+            r.step()
+        n, t0 = 0, time.perf_counter()
+        while n < steps:
+            r.step()
+            n += 1
+            el = time.perf_counter() - t0
+            if el * (n + 1) / n > budget_s:
+                break
+    return n, time.perf_counter() - t0
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    from jax_alfa_b200 import cases
-    from oracle import alfa_oracle
-    from oracle.alfa_oracle import AlfaOracle, OracleRun
-    alfa_oracle.set_fft_workers(threads)
-    grid = (128, 128, 128)
-    total = args.warmup + args.steps
-    cfg = workload_config(grid, total + 1)
-    u, v, w, th = cases.initial_fields(cfg, 0)
-    o = AlfaOracle(cfg)
-    r = OracleRun(cfg, u, v, w, th, adv=o.adv_series(*cases.adv_forcing_series(cfg)))
-    with np.errstate(all="ignore"):
-        for _ in range(args.warmup):
-            r.step()
-        t = time.perf_counter()
-        for _ in range(args.steps):
-            r.step()
-        dt = time.perf_counter() - t
-    n = grid[0] * grid[1] * grid[2]
-    value = n * args.steps / dt
-    sample = (f"{args.steps} steps of the same physics on a 128^3 grid (1/8 of the 256^3 "
-              f"points), {dt / args.steps:.2f} s/step, NumPy FP64 port of the reference with "
-              f"scipy.fft on {threads} threads")
+    threads, model = cpu_info()
+    grid = tuple(args.grid)
+    # one warm-up step (the first step allocates the port's temporaries), then
+    # as many of the requested steps as fit in about 150 s of host time
+    n, dt = oracle_steps(grid, threads, 1, args.steps, 150.0)
+    npts = grid[0] * grid[1] * grid[2]
+    value = npts * n / dt
+    sample = (f"{n} of the {args.steps} requested steps (after 1 warm-up step) of the same "
+              f"{grid[0]}x{grid[1]}x{grid[2]} workload, {dt / n:.2f} s/step: NumPy FP64 port of "
+              f"the reference's step with scipy.fft on {threads} host threads ({model})")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "gp-steps/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": value / A100_BASELINE, "dtype": "f64", "data": "synthetic",
-        "config": config_block(args.grid, world),
+        "n_gpus": world, "steps": n, "warmup": 1, "steps_requested": args.steps,
+        "ms_per_step": 1e3 * dt / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_block(grid, world, "FP64 reference algorithm on the host"),
         "cpu_baseline": {"value": value, "unit": "gp-steps/s", "cores": threads,
-                         "kind": "port", "sample": sample},
+                         "cpu_model": model, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "gp-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
 def run_alfa(args, rank, world, dist):
+    import ctypes
+
     import torch
     from jax_alfa_b200 import _lib, cases
     from jax_alfa_b200.api import Simulation
-    from jax_alfa_b200.driver import MainLoop
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -232,10 +259,9 @@ def run_alfa(args, rank, world, dist):
     grid = tuple(args.grid)
     n_gp = grid[0] * grid[1] * grid[2]
     total = args.warmup + args.steps + 2
-    cfg = workload_config(grid, total)
-    u, v, w, th = cases.initial_fields(cfg, rank)
-    adv = cases.adv_forcing_series(cfg)
+    u, v, w, th = cases.initial_fields(workload_config(grid, total), rank)
     lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
 
     def barrier():
         if dist is not None:
@@ -248,47 +274,79 @@ def run_alfa(args, rank, world, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident whole step -----------------------------------
-    sim = Simulation(cfg, u, v, w, th, adv_series=adv)
-    # warm-up: the bootstrap step, the line-pass autotuner (fastest variant
-    # whose outputs equal the default's), then graph captures of both
-    # iteration parities; the timed steps replay them (alfa_step_graph)
-    sim.step(1)
-    tune = sim.autotune(reps=3) if not args.no_tune else []
-    sim.step(max(args.warmup - 1, 2), graph=True)
-    stream = torch.cuda.current_stream(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = ClockSampler(local)
-    torch.cuda.synchronize(dev)
-    barrier()
-    torch.cuda.synchronize(dev)
-    clocks.start()
-    n0 = lib.alfa_launch_count()
-    e0.record(stream)
-    sim.step(args.steps, graph=True)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    n1 = lib.alfa_launch_count()
-    barrier()
-    torch.cuda.synchronize(dev)
-    clk = clocks.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    d = sim.diag()
-    if not np.isfinite(d["CFL"]):
-        raise RuntimeError("non-finite state in the timed run")
-    value = n_gp * args.steps * world / (ms / 1e3)
+    def timed(prec, keep=False):
+        """Warm-up (the bootstrap step, the line-pass autotuner, graph
+        captures of both iteration parities), then args.steps graph steps
+        timed with CUDA events on this stream, clocks sampled meanwhile."""
+        sim = Simulation(workload_config(grid, total, prec), u, v, w, th)
+        sim.step(1)
+        tune = sim.autotune(reps=3) if not args.no_tune else []
+        sim.step(max(args.warmup - 1, 2), graph=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(local)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        clocks.start()
+        n0 = lib.alfa_launch_count()
+        e0.record(stream)
+        sim.step(args.steps, graph=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        n1 = lib.alfa_launch_count()
+        barrier()
+        torch.cuda.synchronize(dev)
+        clk = clocks.stop()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        if not np.isfinite(sim.diag()["CFL"]):
+            raise RuntimeError(f"non-finite state in the timed {prec} run")
+        st = {k: t.cpu().numpy() for k, t in sim.state().items()}
+        out = {"ms": ms, "tune": tune, "launches": int(n1 - n0), "clocks": clk, "state": st}
+        if keep:
+            out["sim"] = sim
+        else:
+            del sim
+            torch.cuda.empty_cache()
+        return out
 
-    # ---- dominant kernel, live --------------------------------------------
-    import ctypes
+    head = timed(args.precision, keep=True)
+    sim = head["sim"]
+    ms = head["ms"]
+    value = n_gp * args.steps * world / (ms / 1e3)
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64:
+        sim_keep = sim
+        ref = timed("fp64")
+        st, rs = head["state"], ref["state"]
+        vmax = max(float(np.abs(rs[k]).max()) for k in ("u", "v", "w"))
+        err = {k: float(np.abs(st[k] - rs[k]).max()) / vmax for k in ("u", "v", "w")}
+        for k in ("TH", "p"):
+            err[k] = float(np.abs(st[k] - rs[k]).max()) / max(float(np.abs(rs[k]).max()), 1e-300)
+        fp64 = {"value": n_gp * args.steps * world / (ref["ms"] / 1e3),
+                "ms_per_step": ref["ms"] / args.steps,
+                "speedup": ref["ms"] / ms,
+                "vs_a100_fp64": n_gp * args.steps * world / (ref["ms"] / 1e3) / A100_FP64,
+                "err_vs_fp64": err,
+                "err_definition": (f"max |x - x_fp64| after {1 + max(args.warmup - 1, 2) + args.steps} "
+                                   "steps from the same initial fields: u, v, w relative to the "
+                                   "largest FP64 velocity component, TH and p relative to their "
+                                   "own largest FP64 value (TH is theta - T_0)"),
+                "gpu_launches": ref["launches"], "clocks": ref["clocks"]}
+        sim = sim_keep
+    del head["state"]
+    clk_head, launches_head, tune_head = head["clocks"], head["launches"], head["tune"]
+
+    # ---- dominant kernel and the other line passes, live ------------------
     roof = None
     peak, peak_kind = measured_peaks()
     t_ms, t_bytes = ctypes.c_double(), ctypes.c_double()
     a = sim.alfa
     a.lib.alfa_set_stream(a.ctx, ctypes.c_void_p(stream.cuda_stream))
-    names = {0: "k_pad3 (y pad pass 256 -> 384, phase-split 3/2 rule)",
-             1: "k_pad3 (x pad pass 256 -> 384, phase-split 3/2 rule)",
-             2: "k_unpad3 (x unpad pass 384 -> 256)",
-             3: "k_unpad3 (y unpad pass 384 -> 256)",
+    nx_, ny_, nz_ = grid
+    names = {0: f"k_pad3 (y pad pass {ny_} -> {3 * ny_ // 2}, phase-split 3/2 rule)",
+             1: f"k_pad3 (x pad pass {nx_} -> {3 * nx_ // 2}, phase-split 3/2 rule)",
+             2: f"k_unpad3 (x unpad pass {3 * nx_ // 2} -> {nx_})",
+             3: f"k_unpad3 (y unpad pass {3 * ny_ // 2} -> {ny_})",
              4: "k_line_rr (x derivative line pass)",
              5: "k_y_fwd (2-D path: real rows -> half spectrum)",
              6: "k_x (2-D path: x columns, forward FFT + two i*k outputs)",
@@ -300,7 +358,7 @@ def run_alfa(args, rank, world, dist):
             probes[which] = {"kernel": names[which], "avg_launch_ms": t_ms.value,
                              "alg_bytes_per_launch": t_bytes.value, "achieved_gbs": gbs,
                              "frac": gbs / peak}
-    chosen = {c["shape"]: c["variant"] for c in tune if c["chosen"]}
+    chosen = {c["shape"]: c["variant"] for c in head["tune"] if c["chosen"]}
     for which, shape in ((0, "y pad"), (1, "x pad"), (2, "x unpad"), (3, "y unpad"),
                          (4, "x derivative")):
         if which in probes and chosen.get(shape, "default") != "default":
@@ -310,7 +368,6 @@ def run_alfa(args, rank, world, dist):
     # this grid): issued tensor flops and bytes per launch
     tc = None
     if a.lib.alfa_time_kernel(a.ctx, 8, 20, ctypes.byref(t_ms), ctypes.byref(t_bytes)) == 0:
-        nx_, ny_, nz_ = grid
         flops = 3 * 2.0 * nx_ * nx_ * ny_ * nz_
         tflops = flops / (t_ms.value * 1e-3) / 1e12
         bf16_peak, bf16_kind = measured_bf16_peak()
@@ -320,7 +377,7 @@ def run_alfa(args, rank, world, dist):
               "achieved_gbs": gbs, "hbm_frac": gbs / peak, "issued_tflops": tflops,
               "tensor_frac": tflops / bf16_peak,
               "tensor_peak": f"{bf16_kind} {bf16_peak:.0f} TFLOP/s bf16 dense (burst)"}
-    dom = 1  # the pad passes hold the largest share of the step (profiles/)
+    dom = 1  # the x pad pass holds the largest share of the step (profiles/)
     if dom in probes:
         tr = ncu_traffic()
         p1 = probes[dom]
@@ -329,26 +386,26 @@ def run_alfa(args, rank, world, dist):
                 "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                 "alg_bytes_per_launch": p1["alg_bytes_per_launch"],
                 "avg_launch_ms": p1["avg_launch_ms"],
-                "traffic": None if tr is None else tr.get("dram_bytes_per_launch"),
+                "traffic": None if tr is None else tr.get(args.precision),
                 "other_kernels": [probes[k] for k in names if k in probes and k != dom]}
-    del sim
+    del sim, head
     torch.cuda.empty_cache()
 
     # ---- end to end through the C-ABI with host buffers -----------------
-    # e2e: the whole-step entry (alfa_init_state / alfa_step_graph /
-    # alfa_get_diag / alfa_get_state) on a context created beforehand: the
-    # state comes in from pinned host memory, every step reads its CFL
-    # diagnostics back to the host (Main.py:534-540 checks CFL every step),
-    # and the final state goes back to pinned host memory, all inside the
-    # timed region.  e2e_per_function: the same through the per-function ABI
-    # (MainLoop, the loop body of Main.py call for call).
-    e2e = e2e_pf = None
+    # The whole-step entry (alfa_init_state / alfa_step_graph / alfa_get_diag
+    # / alfa_get_state) on a context created beforehand: the state comes in
+    # from pinned host memory (FP64, as the reference's arrays), every step
+    # reads its CFL diagnostics back to the host (Main.py:534-540 checks CFL
+    # every step), and the final state goes back to pinned host memory, all
+    # inside the timed region.
+    e2e = None
     if not args.no_e2e:
         host = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in (u, v, w, th)]
         outs = [torch.empty(x.shape, dtype=torch.float64).pin_memory() for x in host]
-        sim_e = Simulation(cfg, u, v, w, th, adv_series=adv)
+        sim_e = Simulation(workload_config(grid, 2 * total, args.precision), u, v, w, th)
         if not args.no_tune:
             sim_e.autotune(reps=3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
         def run_e2e():
             sim_e.reset(*host)
@@ -374,57 +431,37 @@ def run_alfa(args, rank, world, dist):
                "h2d_bytes_per_step": state_bytes / args.steps,
                # per step: CFL (3), qz_sfc_avg (1) and the ustar plane of alfa_get_diag
                "d2h_bytes_per_step": state_bytes / args.steps + 8 * (4 + grid[0] * grid[1]),
-               "path": "whole-step C-ABI (alfa_init_state, alfa_step_graph, alfa_get_diag "
-                       "every step, alfa_get_state): state from and to pinned host memory "
-                       "inside the timed region",
+               "path": f"whole-step C-ABI, precision {args.precision} (alfa_init_state, "
+                       "alfa_step_graph, alfa_get_diag every step, alfa_get_state): FP64 state "
+                       "from and to pinned host memory inside the timed region",
                "host_wall_ms": 1e3 * (time.perf_counter() - t0)}
         del sim_e
         torch.cuda.empty_cache()
 
-        ml_warm = MainLoop(cfg, u, v, w, th, adv_series=adv)
-        for _ in range(args.warmup):
-            ml_warm.step()
-        api = ml_warm.a
-        if not args.no_tune:
-            api.autotune(reps=3)
-        del ml_warm
-        torch.cuda.synchronize(dev)
-        barrier()
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        e0.record(stream)
-        ml = MainLoop(cfg, *[h.numpy() for h in host], adv_series=adv, api=api)
-        for _ in range(args.steps):
-            ml.step()
-        outs2 = [x.to("cpu", non_blocking=True) for x in (ml.u, ml.v, ml.w, ml.TH)]
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        barrier()
-        pf_ms = max_over_ranks(e0.elapsed_time(e1))
-        e2e_pf = {"value": n_gp * args.steps * world / (pf_ms / 1e3), "unit": "gp-steps/s",
-                  "h2d_bytes_per_step": (state_bytes + ml.h2d_bytes) / args.steps,
-                  "d2h_bytes_per_step": (state_bytes + ml.d2h_bytes) / args.steps,
-                  "path": "MainLoop: Main.py loop body on the per-function C-ABI, state in/out "
-                          "from pinned host memory inside the timed region",
-                  "host_wall_ms": 1e3 * (time.perf_counter() - t0)}
-        del outs2, ml, api
-
     cpu = None
     if rank == 0 and not args.no_cpu:
-        v1, dt1 = cpu_baseline(1)
-        cpu = {"value": v1, "unit": "gp-steps/s", "cores": 1, "kind": "port",
-               "sample": f"1 step of the same physics on 128^3 (1/8 of the points), "
-                         f"{dt1:.1f} s, NumPy FP64 port of the reference, 1 thread"}
+        threads, model = cpu_info()
+        n, dt = oracle_steps(grid, threads, 1, 3, args.cpu_budget)
+        cpu = {"value": n_gp * n / dt, "unit": "gp-steps/s", "cores": threads, "cpu_model": model,
+               "kind": "port",
+               "sample": f"{n} step(s) after 1 warm-up of the same {grid[0]}x{grid[1]}x{grid[2]} "
+                         f"workload, {dt / n:.1f} s/step: NumPy FP64 port of the reference's "
+                         f"step, scipy.fft on {threads} threads"}
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "gp-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": value / A100_BASELINE,
-            "dtype": "f64", "data": "synthetic", "config": config_block(grid, world),
-            "clocks": clk, "gpu_launches": int(n1 - n0), "roofline": roof,
-            "cpu_baseline": cpu, "e2e": e2e, "e2e_per_function": e2e_pf,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / (A100_FP64 if args.precision == "fp64" else A100_FP32),
+            "vs_baseline_ref": ("A100 JAX NBL_A94 256^3 LASDD-SM "
+                                + ("FP64 93.4 M" if args.precision == "fp64" else "FP32 166.8 M")
+                                + " gp-steps/s (BASELINE.md)"),
+            "dtype": DTYPES[args.precision], "data": "synthetic",
+            "config": config_block(grid, world, args.precision),
+            "clocks": clk_head, "gpu_launches": launches_head,
+            "fp64": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "tensor_core_line_pass": tc,
-            "autotune": [{k: c[k] for k in ("shape", "variant", "ms")} for c in tune
+            "autotune": [{k: c[k] for k in ("shape", "variant", "ms")} for c in tune_head
                          if c["chosen"]],
         }), flush=True)
 
@@ -443,7 +480,7 @@ def run_ensemble(args):
     from jax_alfa_b200.api import Ensemble, Simulation
     grids = [(32, 32, 32)] * 32 + [(48, 48, 48)] * 16 + [(64, 64, 64)] * 16
     total = 2 * (args.warmup + args.steps) + 4
-    cfgs = [workload_config(g, total) for g in grids]
+    cfgs = [cases.neutral(*g, nsteps=total) for g in grids]
 
     def make(i, c):
         u, v, w, th = cases.initial_fields(c, i)

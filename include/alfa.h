@@ -1,6 +1,7 @@
 /*
- * libalfa: B200 (sm_100a) FP64 implementation of the JAX-ALFA per-timestep
- * LES hot path behind a plain C ABI.
+ * libalfa: B200 (sm_100a) implementation of the JAX-ALFA per-timestep LES
+ * hot path behind a plain C ABI: the FP64 drop-in, and FP32 / mixed-precision
+ * forms of the same step (alfa_config.precision).
  *
  * Conventions (identical to the reference's arrays, so no transposes at the
  * boundary):
@@ -73,7 +74,28 @@ typedef struct alfa_config {
   double MoistureFlux;           /* kg/kg m/s */
   double zMoisture;              /* m; reference height of the prescribed-Q flux (0: z0T) */
   double q_inversion;            /* kg/kg/m, Q lapse rate above the domain top */
+  /* Storage precision of the context's engine (no counterpart field in the
+   * reference's Config.py, whose use_double_precision switch,
+   * src/config/ConfigLoader.py:150-151 and src/initialization/Preprocess.py:
+   * 112-133, selects FP64 or FP32 for everything):
+   *   ALFA_FP64  fields, transforms and arithmetic in FP64 (the drop-in);
+   *   ALFA_FP32  fields and transforms in FP32; FP64 kept in the pressure
+   *              tridiagonal solve and its zero mode, the plane sums and means,
+   *              the beta quintic roots, the surface-layer (MOST) planes, the
+   *              profiles and series, and the arithmetic of the pointwise
+   *              kernels (values rounded to FP32 where they are stored);
+   *   ALFA_MIXED ALFA_FP32 plus the horizontal line transforms on the tensor
+   *              cores in split BF16 wherever the autotuner (alfa_autotune)
+   *              measures them faster than the FP32 transform.
+   * FP32 and mixed contexts serve the whole-step entry points (state as FP64
+   * device buffers, converted on import and export); the per-function entry
+   * points take FP64 arrays and return ALFA_E_CONFIG on them. */
+  int precision;
 } alfa_config;
+
+#define ALFA_FP64 0
+#define ALFA_FP32 1
+#define ALFA_MIXED 2
 
 /* Derived constants (src/config/DerivedVars.py:48-112, Preprocess.py:44-62). */
 typedef struct alfa_derived {
@@ -98,6 +120,8 @@ int alfa_create(const alfa_config* cfg, alfa_ctx** out);
 void alfa_destroy(alfa_ctx* ctx);
 const char* alfa_last_error(const alfa_ctx* ctx);
 int alfa_set_stream(alfa_ctx* ctx, void* cuda_stream);
+/* ALFA_FP64, ALFA_FP32 or ALFA_MIXED (no reference counterpart) */
+int alfa_get_precision(const alfa_ctx* ctx);
 int alfa_get_derived(const alfa_ctx* ctx, alfa_derived* out /* host */);
 size_t alfa_workspace_bytes(const alfa_ctx* ctx);
 

@@ -40,7 +40,12 @@ class AlfaConfig(ctypes.Structure):
         ("optMoisture", ctypes.c_int), ("optMoistureSurfBC", ctypes.c_int),
         ("MoistureFlux", ctypes.c_double), ("zMoisture", ctypes.c_double),
         ("q_inversion", ctypes.c_double),
+        ("precision", ctypes.c_int),
     ]
+
+
+# alfa_config.precision
+FP64, FP32, MIXED = 0, 1, 2
 
 
 class AlfaDerived(ctypes.Structure):
@@ -165,6 +170,8 @@ def load():
     lib.alfa_set_stream.restype = I
     lib.alfa_get_derived.argtypes = [CTX, ctypes.POINTER(AlfaDerived)]
     lib.alfa_get_derived.restype = I
+    lib.alfa_get_precision.argtypes = [CTX]
+    lib.alfa_get_precision.restype = I
     lib.alfa_workspace_bytes.argtypes = [CTX]
     lib.alfa_workspace_bytes.restype = ctypes.c_size_t
     lib.alfa_get_diag.argtypes = [CTX, ctypes.POINTER(AlfaDiag)]

@@ -28,6 +28,22 @@ C128 = torch.complex128
 CONFIG_KEYS = [f for f, _ in _lib.AlfaConfig._fields_]
 OPTIONAL_KEYS = ("optGeoWind", "optMoisture", "optMoistureSurfBC", "MoistureFlux", "zMoisture",
                  "q_inversion")
+PRECISIONS = {"fp64": _lib.FP64, "fp32": _lib.FP32, "mixed": _lib.MIXED}
+
+
+def precision_of(cfg):
+    """alfa_config.precision of a config: its "precision" entry ("fp64",
+    "fp32", "mixed" or the ALFA_* integer), else the reference's own switch
+    use_double_precision (ConfigLoader.py:150-151): True -> FP64, False ->
+    FP32."""
+    p = cfg.get("precision")
+    if p is None:
+        return _lib.FP64 if cfg.get("use_double_precision", True) else _lib.FP32
+    if isinstance(p, str):
+        if p.lower() not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, not {p!r}")
+        return PRECISIONS[p.lower()]
+    return int(p)
 
 
 def make_config(cfg):
@@ -35,6 +51,9 @@ def make_config(cfg):
     (optSgs 2, 4) start from Cwl / CwlPrRatio, as DerivedVars.py:101-103 does."""
     c = _lib.AlfaConfig()
     for k in CONFIG_KEYS:
+        if k == "precision":
+            c.precision = precision_of(cfg)
+            continue
         # options newer than the original Config.py default to off / zero
         # (ConfigLoader.py:77-124)
         v = cfg.get(k, 0) if k in OPTIONAL_KEYS else cfg[k]

@@ -8,10 +8,17 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalfa.so")
-SOURCES = ["alfa_line.cu", "alfa_spectral.cu", "alfa_physics.cu", "alfa_capi.cu",
-           "alfa_noalloc.cu", "alfa_mlp.cu", "alfa_tc.cu"]
-HEADERS = ["alfa_fft.cuh", "alfa_fft_ct.cuh", "alfa_internal.cuh", "alfa_physics.cuh",
-           "alfa_tile.cuh", "alfa_mlp.cuh"]
+# the engine, compiled once per storage precision (alfa_prec.cuh): FP64 into
+# alfa::f64, FP32 (-DALFA_BUILD_FP32) into alfa::f32
+ENGINE = ["alfa_line.cu", "alfa_spectral.cu", "alfa_physics.cu", "alfa_step.cu", "alfa_tc.cu"]
+# the C-ABI, the no-allocation entry and the learned-coefficient network (FP64)
+ONCE = ["alfa_capi.cu", "alfa_noalloc.cu", "alfa_mlp.cu"]
+SOURCES = ENGINE + ONCE
+HEADERS = ["alfa_prec.cuh", "alfa_fft.cuh", "alfa_fft_ct.cuh", "alfa_internal.cuh",
+           "alfa_physics.cuh", "alfa_tile.cuh", "alfa_mlp.cuh", "alfa_step.cuh", "alfa_iface.cuh"]
+# translation units: (source, extra flags, object suffix)
+UNITS = ([(s, [], "") for s in ENGINE] + [(s, ["-DALFA_BUILD_FP32"], "_f32") for s in ENGINE] +
+         [(s, [], "") for s in ONCE])
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -42,13 +49,13 @@ def build(force=False, verbose=False):
     if not force and not _stale():
         return LIB
     objs, procs = [], []
-    for src in SOURCES:  # translation units compile concurrently
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+    for src, extra, suffix in UNITS:  # translation units compile concurrently
+        obj = os.path.join(CSRC, src.replace(".cu", suffix + ".o"))
+        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+        procs.append((src + suffix, subprocess.Popen(cmd, stdout=subprocess.PIPE,
                                             stderr=subprocess.PIPE, text=True)))
         objs.append(obj)
     failed = []

@@ -13,7 +13,16 @@ Cases (all FP64, 3/2-rule dealiased, FGR=1):
               The large-scale forcing is the reference's advective tendency
               (optAdvection=1, ``src/pde/NSE_AllTerms.py:86-88``) held at
               Uadv = u*^2 / Lz.
-  neutral256  the same physics on 256^3 (the throughput workload).
+  nbl_a94     the reference's own neutral-boundary-layer benchmark after
+              Andren et al. (1994): a neutral Ekman layer under a 5 m/s
+              geostrophic wind, f = 1e-4 1/s, 4000 m cube, Ugal = 3 m/s,
+              z0 = 0.01 m, LASDD-SM, dt = 0.75 s, Rayleigh damping above
+              2500 m (examples/NBL_A94/runs/256x256x256_LASDD_SM_DP/
+              Config.py), the configuration of the reference's A100 256^3
+              throughput figures and this build's throughput workload.  (The
+              neutral case's own domain at 256^3 is not a usable workload:
+              its 7.8 m spacing at dt = 0.5 s puts the spectral CFL number
+              near 0.7, where AB2 is unstable.)
   convective  128^3 CBL: 0.24 K m/s surface flux, z0=0.16 m, inversion,
               0.03 m/s velocity noise below 200 m.
   stable      256x256x192 SBL: prescribed surface cooling 0.5 K/h from
@@ -54,9 +63,14 @@ def neutral(nx=32, ny=32, nz=32, nsteps=200, **over):
     return cfg
 
 
-def neutral256(nsteps=10, **over):
-    cfg = neutral(256, 256, 256, nsteps=nsteps, **over)
-    cfg["case"] = "neutral256"
+def nbl_a94(nx=256, ny=256, nz=256, nsteps=400000, **over):
+    cfg = dict(_BASE, l_x=4000.0, l_y=4000.0, l_z=4000.0, nx=nx, ny=ny, nz=nz,
+               dt=0.75, Ugal=3.0, optSgs=1, z0m=0.01, z0T=0.01, Ug2=5.0, Vg2=0.0,
+               f_coriolis=1.0e-4, inversion=0.0, optDamping=1, z_damping=2500.0,
+               RelaxTime=300.0, optAdvection=0)
+    cfg["SimTime"] = nsteps * cfg["dt"]
+    cfg["case"] = "nbl_a94"
+    cfg.update(over)
     return cfg
 
 
@@ -82,7 +96,7 @@ def stable(nx=256, ny=256, nz=192, nsteps=1000, **over):
     return cfg
 
 
-CASES = {"neutral": neutral, "neutral256": neutral256,
+CASES = {"neutral": neutral, "nbl_a94": nbl_a94,
          "convective": convective, "stable": stable}
 
 
@@ -110,7 +124,15 @@ def initial_fields(cfg, seed=0):
     w = np.zeros((nx, ny, nz))
     th = np.full((nx, ny, nz), float(cfg["T_0"]))
     case = cfg["case"]
-    if case in ("neutral", "neutral256"):
+    if case == "nbl_a94":
+        # CreateInputs_NBL_A94.py: u = Ug, v = w = 0, theta = T_0, with
+        # Gaussian noise of 0.03 m/s in u and 1e-3 K in theta below 200 m
+        u[:] = cfg["Ug2"]
+        for k in range(nz):
+            if z[k] <= 200.0:
+                u[:, :, k] += 0.03 * rng.standard_normal((nx, ny))
+                th[:, :, k] += 1.0e-3 * rng.standard_normal((nx, ny))
+    elif case == "neutral":
         prof = (USTAR_NEUTRAL / VONK) * np.log(z / cfg["z0m"])
         u[:] = prof[None, None, :]
         for k in range(nz):
@@ -273,7 +295,7 @@ def gp_per_step(cfg):
     return cfg["nx"] * cfg["ny"] * cfg["nz"]
 
 
-__all__ = ["CASES", "neutral", "neutral256", "convective", "stable",
+__all__ = ["CASES", "neutral", "nbl_a94", "convective", "stable",
            "initial_fields", "write_run_dir", "nsteps_of", "surface_bc_series",
            "adv_forcing_series", "geowind_series", "initial_moisture",
            "moisture_surface_series", "adv_moisture_series", "gp_per_step"]

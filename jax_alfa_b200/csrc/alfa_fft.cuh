@@ -1,9 +1,11 @@
-// FP64 batched FFT building blocks for sm_100a.
+// Batched FFT building blocks for sm_100a (complex of `real`: FP64 or FP32,
+// alfa_prec.cuh).
 //
 // A CTA transforms C independent columns at once: a tile of n rows x C
-// columns of complex doubles held in shared memory with the column index
+// columns of complex values held in shared memory with the column index
 // fastest (element (row, c) at row*C + c), which is exactly the layout of a
-// run of C consecutive z levels of a field stored z-fastest.  The transform
+// run of C consecutive z levels of a field stored z-fastest (complex doubles in
+// the FP64 build, complex floats in the FP32 build).  The transform
 // is a mixed-radix Stockham sweep: each pass, every thread takes R elements
 // of one column into registers, applies the inter-pass twiddles from a
 // per-length table, runs an R-point DFT in registers and writes the R
@@ -11,31 +13,30 @@
 // Radices 2, 3, 4, 8 and 16 cover every length 2^a 3^b used by the grids
 // (n, 3n/2 for the 3/2-rule padding).
 #pragma once
-#include <cuda_runtime.h>
+#include "alfa_prec.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
-typedef double2 cd;
-
-__device__ __forceinline__ cd cadd(cd a, cd b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ cd csub(cd a, cd b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cd cadd(cd a, cd b) { return mkc(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cd csub(cd a, cd b) { return mkc(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ cd cmul(cd a, cd b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ cd cscale(cd a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ cd cscale(cd a, real s) { return mkc(a.x * s, a.y * s); }
 // a * (S i): S = -1 forward (multiply by -i), S = +1 inverse (multiply by +i)
 template <int S>
 __device__ __forceinline__ cd rot90(cd a) {
-  return S < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+  return S < 0 ? mkc(a.y, -a.x) : mkc(-a.y, a.x);
 }
 
 // cos(m pi / 8) and sin(m pi / 8) for m = 0..15 (exact roots of unity of
-// order 16, correctly rounded).
+// order 16, correctly rounded to `real`).
 __device__ __forceinline__ cd w16(int m, int S) {
-  const double c1 = 0.92387953251128675613;  // cos(pi/8)
-  const double s1 = 0.38268343236508977173;  // sin(pi/8)
-  const double r2 = 0.70710678118654752440;  // sqrt(1/2)
-  double c, s;
+  const real c1 = (real)0.92387953251128675613;  // cos(pi/8)
+  const real s1 = (real)0.38268343236508977173;  // sin(pi/8)
+  const real r2 = (real)0.70710678118654752440;  // sqrt(1/2)
+  real c, s;
   switch (m & 15) {
     case 0: c = 1.0; s = 0.0; break;
     case 1: c = c1; s = s1; break;
@@ -54,7 +55,7 @@ __device__ __forceinline__ cd w16(int m, int S) {
     case 14: c = r2; s = -r2; break;
     default: c = c1; s = -s1; break;
   }
-  return make_double2(c, S * s);
+  return mkc(c, S * s);
 }
 
 template <int S>
@@ -66,9 +67,9 @@ __device__ __forceinline__ void dft2(cd& a, cd& b) {
 
 template <int S>
 __device__ __forceinline__ void dft3(cd& a, cd& b, cd& c) {
-  const double h = 0.86602540378443864676;  // sqrt(3)/2
+  const real h = (real)0.86602540378443864676;  // sqrt(3)/2
   cd t1 = cadd(b, c);
-  cd t2 = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  cd t2 = mkc(a.x - (real)0.5 * t1.x, a.y - (real)0.5 * t1.y);
   cd d = csub(b, c);
   cd t3 = rot90<S>(cscale(d, h));
   a = cadd(a, t1);
@@ -93,10 +94,10 @@ __device__ __forceinline__ void dft8(cd* v) {
   cd o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
   dft4<S>(e0, e1, e2, e3);
   dft4<S>(o0, o1, o2, o3);
-  const double r2 = 0.70710678118654752440;
-  o1 = cmul(o1, make_double2(r2, S * r2));
+  const real r2 = (real)0.70710678118654752440;
+  o1 = cmul(o1, mkc(r2, S * r2));
   o2 = rot90<S>(o2);
-  o3 = cmul(o3, make_double2(-r2, S * r2));
+  o3 = cmul(o3, mkc(-r2, S * r2));
   v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
   v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
   v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
@@ -300,4 +301,5 @@ inline int inplace_threads(int C, int n_max) {
   return t < 64 ? 64 : t;
 }
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

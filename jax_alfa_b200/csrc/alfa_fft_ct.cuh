@@ -1,4 +1,4 @@
-// Compile-time specialised FP64 Stockham FFT over an N x C shared-memory
+// Compile-time specialised Stockham FFT over an N x C shared-memory
 // tile (the same transform as fft_inplace in alfa_fft.cuh, with the radix
 // sequence, thread count and per-thread butterfly count all known to the
 // compiler: index arithmetic folds to shifts and constant multiplies, every
@@ -7,6 +7,7 @@
 #include "alfa_fft.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
 // radix taken for the remaining length m (the same greedy order as the
 // runtime plan: 16, 8, 4, 3, 2)
@@ -160,4 +161,5 @@ __device__ __forceinline__ void ct_last_reg(const cd* __restrict__ buf, const cd
   }
 }
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

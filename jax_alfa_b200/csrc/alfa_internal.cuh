@@ -1,4 +1,6 @@
 // Engine state and internal interfaces of libalfa (not part of the C-ABI).
+// The enums and the launch counter are shared; the engine, its loaders and
+// its operators are declared once per storage precision (alfa_prec.cuh).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -19,6 +21,9 @@ constexpr int NOALLOC_RED_BLOCKS = 256;
 // Process-wide count of kernel launches made by this library (every launch
 // site calls note_launch(); read through alfa_launch_count()).
 void note_launch();
+unsigned long long launch_count();
+// count n kernels that ran without passing a launch site (graph replays)
+void add_launches(unsigned long long n);
 
 // Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
 // current device (the attribute call is made once per kernel, device and
@@ -58,17 +63,30 @@ enum LoadKind {
   X(LD_SCALAR_ADV) X(LD_STRESS_UVP) X(LD_STRESS_W) X(LD_W_SXX) X(LD_THZ) X(LD_MUL_THZ) \
   X(LD_WL_UVP) X(LD_WL_W)
 
+// Output maps of the x-column stage.
+enum SpecMap { MAP_IDENT = 0, MAP_TRUNC, MAP_DX, MAP_DY, MAP_PAD, MAP_UNPAD };
+enum XOutKind { XO_SPEC = 0, XO_INV = 1 };
+
+// 1-D line operators (k_line): a transform along x or y of real fields,
+// two real z columns packed per complex line.  Maps act on the full packed
+// spectrum of length n_in and produce n_out entries.
+enum LineMap { LM_IDENT = 0, LM_TRUNC, LM_DERIV, LM_TRUNC_DERIV, LM_PAD, LM_UNPAD };
+
+}  // namespace alfa
+
+namespace alfa {
+namespace ALFA_PREC {
+
+// A loader's inputs are fields of the build's precision; its constants and
+// the arithmetic of its expression are FP64 (the value is rounded to `real`
+// once, where it enters a transform tile or a field).
 struct Loader {
   int kind;
   int sub;            // variant selector inside a kind
   int nz;
-  const double* a[10];
+  const real* a[10];
   double c[4];
 };
-
-// Output maps of the x-column stage.
-enum SpecMap { MAP_IDENT = 0, MAP_TRUNC, MAP_DX, MAP_DY, MAP_PAD, MAP_UNPAD };
-enum XOutKind { XO_SPEC = 0, XO_INV = 1 };
 
 struct XOut {
   int kind;   // XO_SPEC: write the mapped spectrum column (nx, nyh layout)
@@ -81,17 +99,12 @@ struct XOut {
   FftPlan inv;
 };
 
-// 1-D line operators (k_line): a transform along x or y of real fields,
-// two real z columns packed per complex line.  Maps act on the full packed
-// spectrum of length n_in and produce n_out entries.
-enum LineMap { LM_IDENT = 0, LM_TRUNC, LM_DERIV, LM_TRUNC_DERIV, LM_PAD, LM_UNPAD };
-
 struct LineOut {
   int map;
   int cut;          // LM_TRUNC / LM_TRUNC_DERIV: keep k < cut or k >= n - cut + 1
   double scale;     // applied to the inverse transform (1/n_out, times any extra factor)
   int accumulate;   // 1: dst += result
-  double* dst;
+  real* dst;
 };
 
 struct Engine;
@@ -134,13 +147,15 @@ struct Engine {
   // workspace (complex tiles and fields)
   cd* T[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t T_elems = 0;
-  double* red = nullptr;          // reduction partials
+  double* red = nullptr;          // reduction partials (FP64 in every build)
   size_t red_elems = 0;
   double* scal = nullptr;         // small device scalars / profiles
-  double* W = nullptr;            // field workspace arena
+  real* W = nullptr;              // one field of workspace
   size_t W_elems = 0;
-  double* mat = nullptr;          // a loader's expression, materialised (P elements)
+  real* mat = nullptr;            // a loader's expression, materialised (P elements)
   double* stat = nullptr;         // statistics scratch (24 nz)
+  double2* thomas_dm = nullptr;   // FP32 build: FP64 forward-sweep scratch of the Thomas
+                                  // solve (nx, nyh, nz); the FP64 build uses the output
 
   // Line-pass variants chosen by the autotuner (alfa_autotune), by pass
   // shape (line_key): 0 the default dispatch, 1 the compile-time transform
@@ -180,7 +195,7 @@ void launch_y_fwd(Engine& e, const Loader& L, int rows, const FftPlan& p, int K,
 void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const FftPlan& fwd,
               int nout, const XOut* outs, int Kgrid);
 void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
-                  double* out, int accumulate);
+                  real* out, int accumulate);
 
 // 1-D line passes (alfa_spectral.cu).  axis 0: lines along x of a field
 // (X, Y, nz); axis 1: lines along y.  X/Y of the input field; the output
@@ -200,27 +215,28 @@ int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, l
                Engine::TcOp** out);
 void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y);
 // separable spectral operators on real fields
-void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
-                      double* scratch2);  // explicit filter and its x/y derivatives
-void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int accy);
-void op2_pad(Engine& e, const Loader& L, double* out_pad, double* scratch);
-void op2_unpad(Engine& e, const Loader& L_pad, double* out, double* scratch);
+void op2_filter_deriv(Engine& e, const Loader& L, real* f, real* dx, real* dy,
+                      real* scratch2);  // explicit filter and its x/y derivatives
+void op2_deriv(Engine& e, const Loader& L, real* dx, int accx, real* dy, int accy);
+void op2_pad(Engine& e, const Loader& L, real* out_pad, real* scratch);
+void op2_unpad(Engine& e, const Loader& L_pad, real* out, real* scratch);
 // value of a loader at every point of its n-element domain, written to out
-void materialize(Engine& e, const Loader& L, size_t n, double* out);
+void materialize(Engine& e, const Loader& L, size_t n, real* out);
 
 // composite transforms on regular/padded grids
-Loader ld_field(const Engine& e, const double* a);
+Loader ld_field(const Engine& e, const real* a);
 void op_rfft2(Engine& e, const Loader& L, cd* spec);                       // FFT
-void op_filter_explicit(Engine& e, const Loader& L, double* out, cd* spec); // Filtering_Explicit(FFT(.))
-void op_filter12(Engine& e, const Loader& L, double* out1, double* out2);   // Level1/Level2 of FFT(.)
-void op_deriv_spec(Engine& e, const cd* spec, double* dx, double* dy);      // Derivxy x/y of a spectrum
-void op_deriv_field(Engine& e, const Loader& L, double* dx, double* dy);    // Derivxy(FFT(.)) x/y
-void op_pad(Engine& e, const Loader& L, double* out_pad);                   // Dealias1(FFT(.))
-void op_unpad(Engine& e, const Loader& L_pad, double* out);                 // Dealias2(FFT_pad(.))
-void op_irfft2(Engine& e, const cd* spec, double* out);                     // irfft2 of a spectrum
-void op_pad_spec(Engine& e, const cd* spec, double* out_pad);               // Dealias1(spec)
-void op_unpad_spec(Engine& e, const cd* spec_pad, double* out);             // Dealias2(spec_pad)
+void op_filter_explicit(Engine& e, const Loader& L, real* out, cd* spec); // Filtering_Explicit(FFT(.))
+void op_filter12(Engine& e, const Loader& L, real* out1, real* out2);   // Level1/Level2 of FFT(.)
+void op_deriv_spec(Engine& e, const cd* spec, real* dx, real* dy);      // Derivxy x/y of a spectrum
+void op_deriv_field(Engine& e, const Loader& L, real* dx, real* dy);    // Derivxy(FFT(.)) x/y
+void op_pad(Engine& e, const Loader& L, real* out_pad);                   // Dealias1(FFT(.))
+void op_unpad(Engine& e, const Loader& L_pad, real* out);                 // Dealias2(FFT_pad(.))
+void op_irfft2(Engine& e, const cd* spec, real* out);                     // irfft2 of a spectrum
+void op_pad_spec(Engine& e, const cd* spec, real* out_pad);               // Dealias1(spec)
+void op_unpad_spec(Engine& e, const cd* spec_pad, real* out);             // Dealias2(spec_pad)
 void op_rfft2_pad(Engine& e, const Loader& L, cd* spec_pad);                // FFT_pad
-void op_filter1_spec(Engine& e, const cd* spec, int level, double* out);    // Filtering_Level1/2(spec)
+void op_filter1_spec(Engine& e, const cd* spec, int level, real* out);    // Filtering_Level1/2(spec)
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

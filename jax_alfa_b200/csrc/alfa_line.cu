@@ -1,17 +1,19 @@
 // 1-D line passes along x or y of z-fastest real fields: the separable
 // forms of the reference's spectral operators (explicit filter with its
 // derivatives, derivatives, 3/2-rule pad and unpad), each a forward
-// transform of 16-level z runs, a map, and an inverse transform.
+// transform of runs of 2 YC z levels (a 128-byte row segment), a map, and an
+// inverse transform.
 #include <cmath>
 
 #include "alfa_tile.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
 // ---------------------------------------------------------------------------
 // k_line: 1-D spectral operator along x or y on real fields.  A CTA takes one
-// line index f (an x row for y lines, a y column for x lines) and 16
-// consecutive z levels packed as 8 complex lines, transforms them forward,
+// line index f (an x row for y lines, a y column for x lines) and 2 YC
+// consecutive z levels packed as YC complex lines, transforms them forward,
 // and for each output applies a map to the full packed spectrum, transforms
 // back and stores the real pair.  Packing two real lines in one complex
 // transform is exact for these maps because each is a real operator
@@ -39,16 +41,16 @@ __device__ __forceinline__ void line_load(const LineArgs& a, long long f, int z0
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * blockDim.x;
-      v[u] = make_double2(0.0, 0.0);
+      v[u] = mkc(0, 0);
       if (t < total) {
         const int r = t / YC, c = t % YC;
         const int z = z0 + 2 * c;
         const size_t i = (size_t)(f * a.fs_in + r * a.rs_in) + z;
         if (vec && z + 1 < nz) {
-          v[u] = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+          v[u] = __ldg(reinterpret_cast<const cd*>(L.a[0] + i));
         } else {
-          if (z < nz) v[u].x = ldv<KIND>(L, i, z);
-          if (z + 1 < nz) v[u].y = ldv<KIND>(L, i + 1, z + 1);
+          if (z < nz) v[u].x = (real)ldv<KIND>(L, i, z);
+          if (z + 1 < nz) v[u].y = (real)ldv<KIND>(L, i + 1, z + 1);
         }
       }
     }
@@ -63,28 +65,28 @@ __device__ __forceinline__ void line_load(const LineArgs& a, long long f, int z0
 __device__ __forceinline__ cd line_map(const LineOut& o, const cd* S, int k, int c, int n, int m) {
   auto deriv = [&](cd v) -> cd {
     const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
-    const double q = (double)kk;
-    return make_double2(-(q * v.y), q * v.x);
+    const real q = (real)kk;
+    return mkc(-(q * v.y), q * v.x);
   };
   switch (o.map) {
     case LM_IDENT:
       return S[k * YC + c];
     case LM_TRUNC:
-      return (k < o.cut || k >= n - o.cut + 1) ? S[k * YC + c] : make_double2(0.0, 0.0);
+      return (k < o.cut || k >= n - o.cut + 1) ? S[k * YC + c] : mkc(0, 0);
     case LM_DERIV:
       return deriv(S[k * YC + c]);
     case LM_TRUNC_DERIV:
-      return (k < o.cut || k >= n - o.cut + 1) ? deriv(S[k * YC + c]) : make_double2(0.0, 0.0);
+      return (k < o.cut || k >= n - o.cut + 1) ? deriv(S[k * YC + c]) : mkc(0, 0);
     case LM_PAD: {  // n -> m = 3n/2, Nyquist row repeated (Dealiasing.py:67-73)
       const int h = n / 2;
       if (k <= h) return S[k * YC + c];
       if (k >= m - h) return S[(k - m + n) * YC + c];
-      return make_double2(0.0, 0.0);
+      return mkc(0, 0);
     }
     default: {  // LM_UNPAD: n = 3m/2 -> m, Nyquist dropped (Dealiasing.py:102-109)
       const int h = m / 2;
       if (k < h) return S[k * YC + c];
-      if (k == h) return make_double2(0.0, 0.0);
+      if (k == h) return mkc(0, 0);
       return S[(k - m + n) * YC + c];
     }
   }
@@ -118,20 +120,20 @@ __global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(),
       W[t] = line_map(o, S, k, c, n, m);
     }
     tile_fft<+1, YC, NOUT, NT>(W, a.pout);
-    const double sc = o.scale;
+    const real sc = (real)o.scale;
     if (o.accumulate) {
       for (int t0 = threadIdx.x; t0 < m * YC; t0 += U * blockDim.x) {
-        double2 prev[U];
+        cd prev[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
           const int t = t0 + u * blockDim.x;
           const int r = t / YC, c = t % YC;
           const int z = z0 + 2 * c;
           const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
-          prev[u] = make_double2(0.0, 0.0);
+          prev[u] = mkc(0, 0);
           if (t < m * YC) {
             if (pair && z < nz) {
-              prev[u] = *reinterpret_cast<const double2*>(o.dst + i);
+              prev[u] = *reinterpret_cast<const cd*>(o.dst + i);
             } else {
               if (z < nz) prev[u].x = o.dst[i];
               if (z + 1 < nz) prev[u].y = o.dst[i + 1];
@@ -146,9 +148,9 @@ __global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(),
           const int z = z0 + 2 * c;
           const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
           const cd v = W[t];
-          const double2 w = make_double2(prev[u].x + sc * v.x, prev[u].y + sc * v.y);
+          const cd w = mkc(prev[u].x + sc * v.x, prev[u].y + sc * v.y);
           if (pair && z < nz) {
-            *reinterpret_cast<double2*>(o.dst + i) = w;
+            *reinterpret_cast<cd*>(o.dst + i) = w;
           } else {
             if (z < nz) o.dst[i] = w.x;
             if (z + 1 < nz) o.dst[i + 1] = w.y;
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(tile_threads<YC, (NIN > NOUT ? NIN : NOUT)>(),
         const size_t i = (size_t)(f * a.fs_out + r * a.rs_out) + z;
         const cd v = W[t];
         if (pair && z < nz) {
-          *reinterpret_cast<double2*>(o.dst + i) = make_double2(sc * v.x, sc * v.y);
+          *reinterpret_cast<cd*>(o.dst + i) = mkc(sc * v.x, sc * v.y);
         } else {
           if (z < nz) o.dst[i] = sc * v.x;
           if (z + 1 < nz) o.dst[i + 1] = sc * v.y;
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
 #pragma unroll
         for (int r = 0; r < R; r++)
           v[q * R + r] = (B % NT == 0 || b < B) ? line_map(o, S, j + r * NR, c, NIN, NOUT)
-                                                : make_double2(0.0, 0.0);
+                                                : mkc(0, 0);
       }
       if constexpr (R == NOUT) {
 #pragma unroll
@@ -321,7 +323,7 @@ __host__ __device__ constexpr bool pad3_ok() {
          ct_mb(YC, N, 1, ct_threads(YC, N)) == 1;
 }
 
-__device__ __forceinline__ cd cconj(cd a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ cd cconj(cd a) { return mkc(a.x, -a.y); }
 
 template <int KIND, int C, int N, int NT>
 __device__ __forceinline__ void line_gather_sel(const LineArgs& a, long long f, int z0, cd* v) {
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
       const cd lo = X[r], hi = X[r + RA];
       cd t;
       if (p == 0) {
-        t = (k == 0) ? make_double2(lo.x + 2.0 * hi.x, lo.y + 2.0 * hi.y) : cadd(lo, hi);
+        t = (k == 0) ? mkc(lo.x + (real)2 * hi.x, lo.y + (real)2 * hi.y) : cadd(lo, hi);
       } else if (k == 0) {
         t = csub(lo, hi);
       } else {
@@ -432,7 +434,7 @@ __device__ __forceinline__ void phase_gather(const LineArgs& a, long long f, int
       if (KIND != LD_FIELD && (a.nz & 1) == 0)
         v[q * RB + r] = eval_pair<KIND, C>(a.L, i, z, a.nz, c, ok);
       else
-        v[q * RB + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : make_double2(0.0, 0.0);
+        v[q * RB + r] = ok ? load_pair<KIND>(a.L, i, z, a.nz) : mkc(0, 0);
     }
   }
 }
@@ -509,7 +511,7 @@ __global__ void __launch_bounds__(ct_threads(YC, N), 3) k_unpad3(LineArgs a) {
       const cd g1 = cmul(F[1][r], __ldg(&twM[k]));
       const cd g2 = cmul(F[2][r], __ldg(&twM[2 * k]));
       out[r] = cadd(cadd(g0, g1), g2);
-      out[r + RA] = (k == 0) ? make_double2(0.0, 0.0)
+      out[r + RA] = (k == 0) ? mkc(0, 0)
                              : cadd(cadd(g0, cmul(w3a, g1)), cmul(w3b, g2));
     }
   }
@@ -649,7 +651,7 @@ long long line_key(int axis, int n_in, int n_out, int map, int nout) {
   return ((((long long)axis * 8192 + n_in) * 8192 + n_out) * 4 + cls) * 4 + nout;
 }
 
-static LineOut lo(int map, double* dst, double scale, int cut = 0, int acc = 0) {
+static LineOut lo(int map, real* dst, double scale, int cut = 0, int acc = 0) {
   LineOut o;
   o.map = map;
   o.cut = cut;
@@ -662,10 +664,10 @@ static LineOut lo(int map, double* dst, double scale, int cut = 0, int acc = 0) 
 // Filtering_Explicit followed by Derivxy in x and y (Filtering.py:50-89,
 // Derivatives.py:161-182), as separable passes: x pass (filter, and filter +
 // d/dx), then y passes.  scratch2: two N-sized fields.
-void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double* dy,
-                      double* scratch2) {
-  double* sx = scratch2;
-  double* sdx = scratch2 + e.N();
+void op2_filter_deriv(Engine& e, const Loader& L, real* f, real* dx, real* dy,
+                      real* scratch2) {
+  real* sx = scratch2;
+  real* sdx = scratch2 + e.N();
   const double ix = 1.0 / e.nx, iy = 1.0 / e.ny;
   LineOut ox[2] = {lo(LM_TRUNC, sx, ix, e.cut_e[0]), lo(LM_TRUNC_DERIV, sdx, ix, e.cut_e[0])};
   launch_line(e, 0, L, e.nx, e.ny, e.nx, e.nx, dx ? 2 : 1, ox);
@@ -678,7 +680,7 @@ void op2_filter_deriv(Engine& e, const Loader& L, double* f, double* dx, double*
 }
 
 // Derivxy(FFT(field), kx2) and (.., ky2) as one x pass and one y pass
-void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int accy) {
+void op2_deriv(Engine& e, const Loader& L, real* dx, int accx, real* dy, int accy) {
   if (dx) {
     LineOut o = lo(LM_DERIV, dx, 1.0 / e.nx, 0, accx);
     launch_line(e, 0, L, e.nx, e.ny, e.nx, e.nx, 1, &o);
@@ -696,14 +698,14 @@ void op2_deriv(Engine& e, const Loader& L, double* dx, int accx, double* dy, int
 // inputs per element inside the transform kernel limits the loads a thread
 // keeps in flight and measured slower than the two passes.
 template <int KIND>
-__global__ void __launch_bounds__(256) k_materialize(Loader L, size_t n, double* __restrict__ out) {
+__global__ void __launch_bounds__(256) k_materialize(Loader L, size_t n, real* __restrict__ out) {
   const int nz = L.nz;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    out[i] = ldv<KIND>(L, i, (int)(i % nz));
+    out[i] = (real)ldv<KIND>(L, i, (int)(i % nz));
 }
 
-void materialize(Engine& e, const Loader& L, size_t n, double* out) {
+void materialize(Engine& e, const Loader& L, size_t n, real* out) {
   const size_t want = (n + 255) / 256;
   const unsigned blocks = (unsigned)(want < (size_t)e.sms * 16 ? want : (size_t)e.sms * 16);
   ::alfa::note_launch();
@@ -718,7 +720,7 @@ void materialize(Engine& e, const Loader& L, size_t n, double* out) {
 
 // Dealias1(FFT(field)): y pad (ny -> my) into scratch (nx, my, nz), then x
 // pad; a non-field loader is first materialised
-void op2_pad(Engine& e, const Loader& L0, double* out_pad, double* scratch) {
+void op2_pad(Engine& e, const Loader& L0, real* out_pad, real* scratch) {
   Loader L = L0;
   if (L.kind != LD_FIELD) {
     materialize(e, L, e.N(), e.mat);
@@ -733,7 +735,7 @@ void op2_pad(Engine& e, const Loader& L0, double* out_pad, double* scratch) {
 // Dealias2(FFT_pad(padded field)): x unpad (mx -> nx) into scratch
 // (nx, my, nz), then y unpad with the 9/4 factor; a non-field loader is
 // first materialised
-void op2_unpad(Engine& e, const Loader& L0, double* out, double* scratch) {
+void op2_unpad(Engine& e, const Loader& L0, real* out, real* scratch) {
   Loader L = L0;
   if (L.kind != LD_FIELD) {
     materialize(e, L, e.P(), e.mat);
@@ -745,4 +747,5 @@ void op2_unpad(Engine& e, const Loader& L0, double* out, double* scratch) {
   launch_line(e, 1, ld_field(e, scratch), e.nx, e.my, e.my, e.ny, 1, &oy);
 }
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

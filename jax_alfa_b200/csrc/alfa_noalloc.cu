@@ -21,11 +21,7 @@
 #include "alfa.h"
 #include "alfa_internal.cuh"
 
-namespace alfa {
-// alfa_physics.cu: the reduction kernels of plane_means, fed explicit scratch
-void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials, double* mean,
-                             cudaStream_t s);
-}  // namespace alfa
+#include "alfa_physics.cuh"
 
 namespace {
 
@@ -111,7 +107,7 @@ extern "C" int alfa_PlanarMean_noalloc(const double* F, int nx, int ny, int nz, 
   if (st != ALFA_OK) return st;
   // Every partial read by the final sum is written by this call's first
   // kernel, so the array needs no clearing; it keeps the last call's values.
-  alfa::plane_mean_with_scratch(F, (size_t)nx * (size_t)ny, nz, partials, mean_nz,
+  alfa::f64::plane_mean_with_scratch(F, (size_t)nx * (size_t)ny, nz, partials, mean_nz,
                                 static_cast<cudaStream_t>(cuda_stream));
   return cudaGetLastError() == cudaSuccess ? ALFA_OK : ALFA_E_CUDA;
 }

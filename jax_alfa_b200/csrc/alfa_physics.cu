@@ -7,6 +7,7 @@
 #include "alfa_physics.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
 static constexpr int TPB = 256;
 
@@ -29,7 +30,7 @@ static constexpr int RED_BLOCKS = 1024;
 static constexpr int RED_MAXQ = 16;
 
 struct RedArgs {
-  const double* f[RED_MAXQ];
+  const real* f[RED_MAXQ];
   int nq;
 };
 
@@ -73,7 +74,7 @@ static int red_blocks(const Engine& e) {
   return (int)(e.H() < (size_t)RED_BLOCKS ? e.H() : RED_BLOCKS);
 }
 
-void plane_sums(Engine& e, const double* const* fields, int nq, double* sums) {
+void plane_sums(Engine& e, const real* const* fields, int nq, double* sums) {
   RedArgs a{};
   a.nq = nq;
   for (int q = 0; q < nq; q++) a.f[q] = fields[q];
@@ -85,7 +86,7 @@ void plane_sums(Engine& e, const double* const* fields, int nq, double* sums) {
 
 // The plane mean of one field with caller-provided partial-sum storage
 // (NOALLOC_RED_BLOCKS x nz doubles); the same kernels as plane_means.
-void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials, double* mean,
+void plane_mean_with_scratch(const real* F, size_t H, int nz, double* partials, double* mean,
                              cudaStream_t s) {
   RedArgs a{};
   a.nq = 1;
@@ -96,7 +97,7 @@ void plane_mean_with_scratch(const double* F, size_t H, int nz, double* partials
       partials, nb, 1, nz, 1.0 / (double)H, mean);
 }
 
-void plane_means(Engine& e, const double* const* fields, int nq, double* means) {
+void plane_means(Engine& e, const real* const* fields, int nq, double* means) {
   RedArgs a{};
   a.nq = nq;
   for (int q = 0; q < nq; q++) a.f[q] = fields[q];
@@ -153,9 +154,9 @@ __device__ void most_fn(double zL, bool stable, double* psi_m, double* psi_h, do
 }
 
 struct SurfPtr {
-  const double* u;
-  const double* v;
-  const double* TH;
+  const real* u;
+  const real* v;
+  const real* TH;
   const double* mi[6];
   double* M;
   double* ustar;
@@ -284,10 +285,10 @@ int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io,
 // ---------------------------------------------------------------------------
 // vertical derivatives: Derivatives.py:190-362
 // ---------------------------------------------------------------------------
-__global__ void k_derivz_M(const double* __restrict__ u, const double* __restrict__ v,
-                           const double* __restrict__ w, const double* __restrict__ ustar,
+__global__ void k_derivz_M(const real* __restrict__ u, const real* __restrict__ v,
+                           const real* __restrict__ w, const double* __restrict__ ustar,
                            const double* __restrict__ M, const double* __restrict__ fi,
-                           double* dudz, double* dvdz, double* dwdz, size_t n, int nz,
+                           real* dudz, real* dvdz, real* dwdz, size_t n, int nz,
                            double idz, double Ugal, double den_c) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
@@ -297,76 +298,76 @@ __global__ void k_derivz_M(const double* __restrict__ u, const double* __restric
       dudz[i] = fi[r] * ustar[r] * (u[i] + Ugal) / den;
       dvdz[i] = fi[r] * ustar[r] * v[i] / den;
     } else if (z < nz - 1) {
-      dudz[i] = (u[i] - u[i - 1]) * idz;
-      dvdz[i] = (v[i] - v[i - 1]) * idz;
+      dudz[i] = ((double)u[i] - (double)u[i - 1]) * idz;
+      dvdz[i] = ((double)v[i] - (double)v[i - 1]) * idz;
     } else {
       dudz[i] = 0.0;
       dvdz[i] = 0.0;
     }
-    dwdz[i] = (z < nz - 1) ? (w[i + 1] - w[i]) * idz : 0.0;
+    dwdz[i] = (z < nz - 1) ? ((double)w[i + 1] - (double)w[i]) * idz : 0.0;
   }
 }
 
-void derivz_M(Engine& e, const double* u, const double* v, const double* w, const double* ustar,
-              const double* M, const double* fi_m, double* dudz, double* dvdz, double* dwdz) {
+void derivz_M(Engine& e, const real* u, const real* v, const real* w, const double* ustar,
+              const double* M, const double* fi_m, real* dudz, real* dvdz, real* dwdz) {
   ::alfa::note_launch(); k_derivz_M<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, v, w, ustar, M, fi_m, dudz, dvdz, dwdz,
                                                     e.N(), e.nz, e.idz, e.cfg.Ugal, e.dz);
 }
 
-__global__ void k_derivz_TH(const double* __restrict__ T, const double* __restrict__ ustar,
+__global__ void k_derivz_TH(const real* __restrict__ T, const double* __restrict__ ustar,
                             const double* __restrict__ qz, const double* __restrict__ fi,
-                            double* out, size_t n, int nz, double idz, double den) {
+                            real* out, size_t n, int nz, double idz, double den) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     const size_t r = i / nz;
     if (z == 0) {
       out[i] = fi[r] * (-qz[r] / ustar[r]) / den;
     } else {
-      out[i] = (T[i] - T[i - 1]) * idz;
+      out[i] = ((double)T[i] - (double)T[i - 1]) * idz;
     }
   }
 }
 
-void derivz_TH(Engine& e, const double* TH, const double* ustar, const double* qz,
-               const double* fi_h, double* dTHdz) {
+void derivz_TH(Engine& e, const real* TH, const double* ustar, const double* qz,
+               const double* fi_h, real* dTHdz) {
   ::alfa::note_launch(); k_derivz_TH<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, ustar, qz, fi_h, dTHdz, e.N(), e.nz,
                                                      e.idz, 0.4 * 0.5 * e.dz);
 }
 
-__device__ __forceinline__ double dz_generic(const double* F, size_t i, int z, int nz, int w,
+__device__ __forceinline__ double dz_generic(const real* F, size_t i, int z, int nz, int w,
                                              double idz) {
-  if (w) return (z < nz - 1) ? (F[i + 1] - F[i]) * idz : 0.0;  // Derivz_Generic_w
-  return (z > 0) ? (F[i] - F[i - 1]) * idz : 0.0;              // Derivz_Generic_uvp
+  if (w) return (z < nz - 1) ? ((double)F[i + 1] - (double)F[i]) * idz : 0.0;  // Derivz_Generic_w
+  return (z > 0) ? ((double)F[i] - (double)F[i - 1]) * idz : 0.0;              // Derivz_Generic_uvp
 }
 
-__global__ void k_derivz_generic(const double* __restrict__ F, double* out, size_t n, int nz,
+__global__ void k_derivz_generic(const real* __restrict__ F, real* out, size_t n, int nz,
                                  int w, double idz) {
   GRID_STRIDE(i, n) { out[i] = dz_generic(F, i, (int)(i % nz), nz, w, idz); }
 }
 
-void derivz_generic(Engine& e, const double* F, int w_nodes, double* out) {
+void derivz_generic(Engine& e, const real* F, int w_nodes, real* out) {
   ::alfa::note_launch(); k_derivz_generic<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nz, w_nodes, e.idz);
 }
 
-__global__ void k_div_finish(double* div, const double* __restrict__ f, size_t n, int nz, int w,
+__global__ void k_div_finish(real* div, const real* __restrict__ f, size_t n, int nz, int w,
                              double idz) {
-  GRID_STRIDE(i, n) { div[i] = div[i] + dz_generic(f, i, (int)(i % nz), nz, w, idz); }
+  GRID_STRIDE(i, n) { div[i] = (double)div[i] + dz_generic(f, i, (int)(i % nz), nz, w, idz); }
 }
 
-void divergence_finish(Engine& e, double* div, const double* fz, int w_nodes) {
+void divergence_finish(Engine& e, real* div, const real* fz, int w_nodes) {
   ::alfa::note_launch(); k_div_finish<<<nblocks(e.N()), TPB, 0, e.stream>>>(div, fz, e.N(), e.nz, w_nodes, e.idz);
 }
 
 // ---------------------------------------------------------------------------
 // buoyancy: NSE_BuoyancyTerms.py:49-150 (dry, H = 0)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double thv_of(const double* __restrict__ TH,
-                                        const double* __restrict__ H, size_t i, double T0) {
-  return (TH[i] + T0) * (H ? __dadd_rn(1.0, __dmul_rn(0.61, H[i])) : 1.0);
+__device__ __forceinline__ double thv_of(const real* __restrict__ TH,
+                                        const real* __restrict__ H, size_t i, double T0) {
+  return ((double)TH[i] + T0) * (H ? __dadd_rn(1.0, __dmul_rn(0.61, (double)H[i])) : 1.0);
 }
 
-__global__ void k_buoy(const double* __restrict__ TH, const double* __restrict__ H,
-                       const double* __restrict__ bar, double* out, size_t n, int nz, double T0,
+__global__ void k_buoy(const real* __restrict__ TH, const real* __restrict__ H,
+                       const double* __restrict__ bar, real* out, size_t n, int nz, double T0,
                        int by_mean, double hg) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
@@ -382,16 +383,16 @@ __global__ void k_buoy(const double* __restrict__ TH, const double* __restrict__
   }
 }
 
-__global__ void k_thv(const double* __restrict__ TH, const double* __restrict__ H, double T0,
-                      double* out, size_t n) {
+__global__ void k_thv(const real* __restrict__ TH, const real* __restrict__ H, double T0,
+                      real* out, size_t n) {
   GRID_STRIDE(i, n) { out[i] = thv_of(TH, H, i, T0); }
 }
 
-void buoyancy(Engine& e, const double* TH, const double* H, int opt, double* out) {
+void buoyancy(Engine& e, const real* TH, const real* H, int opt, real* out) {
   // THv = (TH + T_0)(1 + 0.61 H) and its plane mean
-  double* thv = e.W;  // first workspace field
+  real* thv = e.W;  // first workspace field
   ::alfa::note_launch(); k_thv<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, H, e.T0_nondim, thv, e.N());
-  const double* f[1] = {thv};
+  const real* f[1] = {thv};
   plane_means(e, f, 1, e.scal);
   ::alfa::note_launch(); k_buoy<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, H, e.scal, out, e.N(), e.nz,
                                                                       e.T0_nondim, opt,
@@ -400,7 +401,7 @@ void buoyancy(Engine& e, const double* TH, const double* H, int opt, double* out
 
 // surface moisture flux (Main.py:253-267; SurfaceFlux.py:447-504):
 // qm = ustar vonk (Q_s - Q_air) / (log(0.5 dz z_scale / z_ref) + psi_h - psi_h0)
-__global__ void k_moisture_surface(int mode, int het, const double* __restrict__ Q,
+__global__ void k_moisture_surface(int mode, int het, const real* __restrict__ Q,
                                    const double* __restrict__ ustar,
                                    const double* __restrict__ psi_h,
                                    const double* __restrict__ psi_h0,
@@ -418,7 +419,7 @@ __global__ void k_moisture_surface(int mode, int het, const double* __restrict__
   }
 }
 
-void moisture_surface(Engine& e, int mode, int het, const double* Q, const double* ustar,
+void moisture_surface(Engine& e, int mode, int het, const real* Q, const double* ustar,
                       const double* psi_h, const double* psi_h0, const double* series,
                       const int* itp, double q_host, const double* qbar0, double* qm) {
   ::alfa::note_launch();
@@ -431,7 +432,7 @@ void moisture_surface(Engine& e, int mode, int het, const double* Q, const doubl
 // strain rates: StrainRates.py:56-141 (uvp), 219-299 (w)
 // ---------------------------------------------------------------------------
 struct G9 {
-  const double* g[9];
+  const real* g[9];
 };
 
 __device__ __forceinline__ double smag_of(double s11, double s22, double s33, double s12,
@@ -440,12 +441,12 @@ __device__ __forceinline__ double smag_of(double s11, double s22, double s33, do
                      2.0 * (s13 * s13) + 2.0 * (s23 * s23)));
 }
 
-__global__ void k_strains_uvp(G9 G, double* S12, double* S13, double* S23, double* S, size_t n,
+__global__ void k_strains_uvp(G9 G, real* S12, real* S13, real* S23, real* S, size_t n,
                               int nz) {
   // g: dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
-    const double* const* g = G.g;
+    const real* const* g = G.g;
     double uz, vz, wx, wy;
     if (z == 0) {
       uz = g[6][i];
@@ -458,13 +459,13 @@ __global__ void k_strains_uvp(G9 G, double* S12, double* S13, double* S23, doubl
       wx = g[2][i];
       wy = g[5][i];
     } else {
-      uz = 0.5 * (g[6][i] + g[6][i + 1]);
-      vz = 0.5 * (g[7][i] + g[7][i + 1]);
-      wx = 0.5 * (g[2][i] + g[2][i + 1]);
-      wy = 0.5 * (g[5][i] + g[5][i + 1]);
+      uz = 0.5 * ((double)g[6][i] + (double)g[6][i + 1]);
+      vz = 0.5 * ((double)g[7][i] + (double)g[7][i + 1]);
+      wx = 0.5 * ((double)g[2][i] + (double)g[2][i + 1]);
+      wy = 0.5 * ((double)g[5][i] + (double)g[5][i + 1]);
     }
     const double s11 = g[0][i], s22 = g[4][i], s33 = g[8][i];
-    const double s12 = 0.5 * (g[3][i] + g[1][i]);
+    const double s12 = 0.5 * ((double)g[3][i] + (double)g[1][i]);
     const double s13 = 0.5 * (uz + wx);
     const double s23 = 0.5 * (vz + wy);
     S12[i] = s12;
@@ -474,67 +475,66 @@ __global__ void k_strains_uvp(G9 G, double* S12, double* S13, double* S23, doubl
   }
 }
 
-void strains_uvp(Engine& e, const double* const g[9], double* S12, double* S13, double* S23,
-                 double* S) {
+void strains_uvp(Engine& e, const real* const g[9], real* S12, real* S13, real* S23, real* S) {
   G9 G;
   for (int i = 0; i < 9; i++) G.g[i] = g[i];
   ::alfa::note_launch(); k_strains_uvp<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, S12, S13, S23, S, e.N(), e.nz);
 }
 
-__global__ void k_smag_w(G9 G, double* Sw, size_t n, int nz) {
+__global__ void k_smag_w(G9 G, real* Sw, size_t n, int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
-    const double* const* g = G.g;
-    auto stag = [&](const double* d) -> double {
+    const real* const* g = G.g;
+    auto stag = [&](const real* d) -> double {
       if (z == 0) return d[i];
       if (z == nz - 1) return 0.0;
-      return 0.5 * (d[i - 1] + d[i]);
+      return 0.5 * ((double)d[i - 1] + (double)d[i]);
     };
     const double s11 = stag(g[0]), s22 = stag(g[4]), s33 = stag(g[8]);
     const double s12 = 0.5 * (stag(g[3]) + stag(g[1]));
-    const double wx = (z == 0) ? 0.5 * (g[2][i] + g[2][i + 1]) : g[2][i];
-    const double wy = (z == 0) ? 0.5 * (g[5][i] + g[5][i + 1]) : g[5][i];
-    const double s13 = 0.5 * (g[6][i] + wx);
-    const double s23 = 0.5 * (g[7][i] + wy);
+    const double wx = (z == 0) ? 0.5 * ((double)g[2][i] + (double)g[2][i + 1]) : (double)g[2][i];
+    const double wy = (z == 0) ? 0.5 * ((double)g[5][i] + (double)g[5][i + 1]) : (double)g[5][i];
+    const double s13 = 0.5 * ((double)g[6][i] + wx);
+    const double s23 = 0.5 * ((double)g[7][i] + wy);
     Sw[i] = smag_of(s11, s22, s33, s12, s13, s23);
   }
 }
 
-void smag_w(Engine& e, const double* const g[9], double* Sw) {
+void smag_w(Engine& e, const real* const g[9], real* Sw) {
   G9 G;
   for (int i = 0; i < 9; i++) G.g[i] = g[i];
   ::alfa::note_launch(); k_smag_w<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, Sw, e.N(), e.nz);
 }
 
 struct P6 {
-  const double* s[6];
+  const real* s[6];
 };
 
-__global__ void k_smag6(P6 P, double* out, size_t n) {
+__global__ void k_smag6(P6 P, real* out, size_t n) {
   GRID_STRIDE(i, n) {
     out[i] = smag_of(P.s[0][i], P.s[1][i], P.s[2][i], P.s[3][i], P.s[4][i], P.s[5][i]);
   }
 }
 
-void smag6(Engine& e, const double* const s[6], size_t n, double* out) {
+void smag6(Engine& e, const real* const s[6], size_t n, real* out) {
   P6 P;
   for (int i = 0; i < 6; i++) P.s[i] = s[i];
   ::alfa::note_launch(); k_smag6<<<nblocks(n), TPB, 0, e.stream>>>(P, out, n);
 }
 
-void smag6_n(Engine& e, const double* const s[6], double* out) { smag6(e, s, e.N(), out); }
+void smag6_n(Engine& e, const real* const s[6], real* out) { smag6(e, s, e.N(), out); }
 
 // w_ of DynamicSGS_LASDD_SM.py:180-183
-__global__ void k_wstar(const double* __restrict__ w, double* out, size_t n, int nz) {
+__global__ void k_wstar(const real* __restrict__ w, real* out, size_t n, int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
-    if (z == 0) out[i] = 0.5 * w[i + 1];
+    if (z == 0) out[i] = 0.5 * (double)w[i + 1];
     else if (z == nz - 1) out[i] = w[i - 1];
-    else out[i] = 0.5 * (w[i] + w[i + 1]);
+    else out[i] = 0.5 * ((double)w[i] + (double)w[i + 1]);
   }
 }
 
-void wstar(Engine& e, const double* w, double* w_) {
+void wstar(Engine& e, const real* w, real* w_) {
   ::alfa::note_launch(); k_wstar<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, w_, e.N(), e.nz);
 }
 
@@ -552,15 +552,15 @@ __device__ __forceinline__ double sq6(const double* A) {
   return A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + 2.0 * (A[3] * A[3] + A[4] * A[4] + A[5] * A[5]);
 }
 
-__device__ __forceinline__ void leonard(const double* const* ph, const double* const* hat, size_t i,
+__device__ __forceinline__ void leonard(const real* const* ph, const real* const* hat, size_t i,
                                         double* Lo) {
   const double u = hat[0][i], v = hat[1][i], w = hat[2][i];
-  Lo[0] = ph[0][i] - u * u;
-  Lo[1] = ph[1][i] - v * v;
-  Lo[2] = ph[2][i] - w * w;
-  Lo[3] = ph[3][i] - u * v;
-  Lo[4] = ph[4][i] - u * w;
-  Lo[5] = ph[5][i] - v * w;
+  Lo[0] = (double)ph[0][i] - u * u;
+  Lo[1] = (double)ph[1][i] - v * v;
+  Lo[2] = (double)ph[2][i] - w * w;
+  Lo[3] = (double)ph[3][i] - u * v;
+  Lo[4] = (double)ph[4][i] - u * w;
+  Lo[5] = (double)ph[5][i] - v * w;
 }
 
 __global__ void k_lasdd_partial(LasddFields f, LasddConst c, size_t H, int nz,
@@ -749,8 +749,8 @@ __global__ void k_ones(double* p, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 1.0;
 }
 
-__global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ beta, double* LM,
-                        double* MM, size_t n, int nz) {
+__global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ beta, real* LM,
+                        real* MM, size_t n, int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     double Lm[6], Mm[6];
@@ -758,14 +758,14 @@ __global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ 
     const double b = beta[z];
     const double Sh = f.S_hat[i];
 #pragma unroll
-    for (int q = 0; q < 6; q++) Mm[q] = c.T1 * f.SSh[q][i] - c.T2 * b * Sh * f.Sh[q][i];
+    for (int q = 0; q < 6; q++) Mm[q] = c.T1 * (double)f.SSh[q][i] - c.T2 * b * Sh * (double)f.Sh[q][i];
     LM[i] = (Lm[0] * Mm[0] + Lm[1] * Mm[1] + Lm[2] * Mm[2]) +
             2.0 * (Lm[3] * Mm[3] + Lm[4] * Mm[4] + Lm[5] * Mm[5]);
     MM[i] = sq6(Mm);
   }
 }
 
-void lasdd_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM) {
+void lasdd_LM_MM(Engine& e, const LasddFields& f, const double* beta, real* LM, real* MM) {
   ::alfa::note_launch(); k_LM_MM<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, lasdd_const(e), beta, LM, MM, e.N(), e.nz);
 }
 
@@ -841,21 +841,21 @@ void wl_poly(Engine& e, const double* sums4, double* coeffs6) {
 }
 
 __global__ void k_LM_MM_wl(LasddFields f, double T1, double T2, const double* __restrict__ beta,
-                           double* LM, double* MM, size_t n, int nz) {
+                           real* LM, real* MM, size_t n, int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     double Lm[6], Mm[6];
     leonard(f.ph, f.hat, i, Lm);
     const double b = beta[z];
 #pragma unroll
-    for (int q = 0; q < 6; q++) Mm[q] = T1 * f.Sh[q][i] - T2 * b * f.Sd[q][i];
+    for (int q = 0; q < 6; q++) Mm[q] = T1 * (double)f.Sh[q][i] - T2 * b * (double)f.Sd[q][i];
     LM[i] = (Lm[0] * Mm[0] + Lm[1] * Mm[1] + Lm[2] * Mm[2]) +
             2.0 * (Lm[3] * Mm[3] + Lm[4] * Mm[4] + Lm[5] * Mm[5]);
     MM[i] = sq6(Mm);
   }
 }
 
-void lasdd_wl_LM_MM(Engine& e, const LasddFields& f, const double* beta, double* LM, double* MM) {
+void lasdd_wl_LM_MM(Engine& e, const LasddFields& f, const double* beta, real* LM, real* MM) {
   const double T1 = 2 * std::pow(e.L, 4.0 / 3.0);
   const double T2 = 2 * std::pow(e.TFR * e.L, 4.0 / 3.0);
   ::alfa::note_launch(); k_LM_MM_wl<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, T1, T2, beta, LM, MM, e.N(), e.nz);
@@ -870,8 +870,8 @@ __device__ __forceinline__ WLScalarTerms wl_scalar_terms(const ScalarLasddFields
   double LT[3], QT[3], G1[3], G2[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    LT[q] = f.uTh[q][i] - f.hat[q][i] * T1;
-    QT[q] = f.uTd[q][i] - f.hatd[q][i] * T2;
+    LT[q] = (double)f.uTh[q][i] - (double)f.hat[q][i] * T1;
+    QT[q] = (double)f.uTd[q][i] - (double)f.hatd[q][i] * T2;
     G1[q] = f.Gh[q][i];
     G2[q] = f.Gd[q][i];
   }
@@ -911,7 +911,7 @@ void scalar_lasdd_wl_sums(Engine& e, const ScalarLasddFields& f, double* sums4) 
 }
 
 __global__ void k_slwl_TupTdn(ScalarLasddFields f, double L43, double L83, WLPow P,
-                              const double* __restrict__ beta, double* Tup, double* Tdn, size_t n,
+                              const double* __restrict__ beta, real* Tup, real* Tdn, size_t n,
                               int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
@@ -922,8 +922,8 @@ __global__ void k_slwl_TupTdn(ScalarLasddFields f, double L43, double L83, WLPow
   }
 }
 
-void scalar_wl_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
-                       double* Tdn) {
+void scalar_wl_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, real* Tup,
+                       real* Tdn) {
   const double L43 = std::pow(e.L, 4.0 / 3.0), L83 = std::pow(e.L, 8.0 / 3.0);
   ::alfa::note_launch(); k_slwl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, L43, L83, wl_pow(e), beta, Tup, Tdn, e.N(), e.nz);
 }
@@ -970,16 +970,16 @@ __global__ void k_stats_mean_partial(StatsIn a, size_t H, int nz, double* __rest
         s[12] += v;
         s[13] += T;
       } else {
-        s[11] += 0.5 * (a.u[i - 1] + u);
-        s[12] += 0.5 * (a.v[i - 1] + v);
-        s[13] += 0.5 * (a.TH[i - 1] + T);
+        s[11] += 0.5 * ((double)a.u[i - 1] + u);
+        s[12] += 0.5 * ((double)a.v[i - 1] + v);
+        s[13] += 0.5 * ((double)a.TH[i - 1] + T);
       }
       if (a.Q) {
         const double q = a.Q[i];
         s[14] += q;
         s[15] += a.dQdz[i];
         s[16] += a.qHz[i];
-        s[17] += (z == 0) ? q : 0.5 * (a.Q[i - 1] + q);
+        s[17] += (z == 0) ? q : 0.5 * ((double)a.Q[i - 1] + q);
       }
     }
 #pragma unroll
@@ -1017,9 +1017,9 @@ __global__ void k_stats_var_partial(StatsIn a, const double* __restrict__ m, siz
         vS = v;
         TS = T;
       } else {
-        uS = 0.5 * (a.u[i - 1] + u);
-        vS = 0.5 * (a.v[i - 1] + v);
-        TS = 0.5 * (a.TH[i - 1] + T);
+        uS = 0.5 * ((double)a.u[i - 1] + u);
+        vS = 0.5 * ((double)a.v[i - 1] + v);
+        TS = 0.5 * ((double)a.TH[i - 1] + T);
       }
       const double usf = uS + Ug - muS, vsf = vS - mvS, wsf = wf, Tsf = TS - mTS;
       s[7] += usf * wsf;
@@ -1028,7 +1028,7 @@ __global__ void k_stats_var_partial(StatsIn a, const double* __restrict__ m, siz
       if (a.Q) {
         const double q = a.Q[i];
         const double Qf = q - mQ;
-        const double QS = (z == 0) ? q : 0.5 * (a.Q[i - 1] + q);
+        const double QS = (z == 0) ? q : 0.5 * ((double)a.Q[i - 1] + q);
         s[10] += Qf * Qf;
         s[11] += wsf * (QS - mQS);
       }
@@ -1127,7 +1127,7 @@ void compute_stats(Engine& e, const StatsIn& a, double* acc) {
 }
 
 // 3x3 periodic box mean (Utilities.py:87-115) at (x, y, z)
-__device__ __forceinline__ double box9(const double* F, int x, int y, int z, int nx, int ny,
+__device__ __forceinline__ double box9(const real* F, int x, int y, int z, int nx, int ny,
                                        int nz) {
   double s = 0.0;
   const double w = 1.0 / 9.0;
@@ -1135,14 +1135,14 @@ __device__ __forceinline__ double box9(const double* F, int x, int y, int z, int
     const int xx = (x + a - 1 + nx) % nx;
     for (int b = 0; b < 3; b++) {
       const int yy = (y + b - 1 + ny) % ny;
-      s = s + F[((size_t)xx * ny + yy) * nz + z] * w;
+      s = s + (double)F[((size_t)xx * ny + yy) * nz + z] * w;
     }
   }
   return s;
 }
 
-__global__ void k_clip_ratio(const double* __restrict__ num, const double* __restrict__ den,
-                             double* out, size_t n, int nx, int ny, int nz) {
+__global__ void k_clip_ratio(const real* __restrict__ num, const real* __restrict__ den,
+                             real* out, size_t n, int nx, int ny, int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     const size_t r = i / nz;
@@ -1155,11 +1155,11 @@ __global__ void k_clip_ratio(const double* __restrict__ num, const double* __res
   }
 }
 
-void clip_ratio(Engine& e, const double* num, const double* den, double* out) {
+void clip_ratio(Engine& e, const real* num, const real* den, real* out) {
   ::alfa::note_launch(); k_clip_ratio<<<nblocks(e.N()), TPB, 0, e.stream>>>(num, den, out, e.N(), e.nx, e.ny, e.nz);
 }
 
-__global__ void k_imfilter(const double* __restrict__ F, double* out, size_t n, int nx, int ny,
+__global__ void k_imfilter(const real* __restrict__ F, real* out, size_t n, int nx, int ny,
                            int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
@@ -1168,11 +1168,11 @@ __global__ void k_imfilter(const double* __restrict__ F, double* out, size_t n, 
   }
 }
 
-void imfilter(Engine& e, const double* F, double* out) {
+void imfilter(Engine& e, const real* F, real* out) {
   ::alfa::note_launch(); k_imfilter<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nx, e.ny, e.nz);
 }
 
-__global__ void k_cs2_partial(const double* __restrict__ C, size_t H, int nz, double* part) {
+__global__ void k_cs2_partial(const real* __restrict__ C, size_t H, int nz, double* part) {
   const size_t rpb = (H + gridDim.x - 1) / gridDim.x;
   const size_t r0 = blockIdx.x * rpb;
   const size_t r1 = (r0 + rpb < H) ? r0 + rpb : H;
@@ -1196,7 +1196,7 @@ __global__ void k_cs2_finish(const double* __restrict__ m, int nz, double* avg1,
   }
 }
 
-void cs2_profiles(Engine& e, const double* Cs2, double* avg1, double* avg2) {
+void cs2_profiles(Engine& e, const real* Cs2, double* avg1, double* avg2) {
   const int nb = red_blocks(e);
   ::alfa::note_launch(); k_cs2_partial<<<nb, 128, 0, e.stream>>>(Cs2, e.H(), e.nz, e.red);
   double* m = e.scal + 64;
@@ -1230,14 +1230,14 @@ struct SLTerms {
   double a, b, c, d, e;
 };
 
-__device__ __forceinline__ SLTerms sl_terms(const double* const* uT, const double* const* hat,
-                                            const double* Tf, const double* const* SG,
-                                            const double* const* G, const double* S, size_t i) {
+__device__ __forceinline__ SLTerms sl_terms(const real* const* uT, const real* const* hat,
+                                            const real* Tf, const real* const* SG,
+                                            const real* const* G, const real* S, size_t i) {
   const double T = Tf[i], s = S[i];
   double LT[3], sg[3], g[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    LT[q] = uT[q][i] - hat[q][i] * T;
+    LT[q] = (double)uT[q][i] - (double)hat[q][i] * T;
     sg[q] = SG[q][i];
     g[q] = G[q][i];
   }
@@ -1285,7 +1285,7 @@ void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10) {
 }
 
 __global__ void k_sl_TupTdn(ScalarLasddFields f, SLConst c, const double* __restrict__ beta,
-                            double* Tup, double* Tdn, size_t n, int nz) {
+                            real* Tup, real* Tdn, size_t n, int nz) {
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     const SLTerms t = sl_terms(f.uTh, f.hat, f.Th, f.SGh, f.Gh, f.S_hat, i);
@@ -1295,39 +1295,39 @@ __global__ void k_sl_TupTdn(ScalarLasddFields f, SLConst c, const double* __rest
   }
 }
 
-void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, double* Tup,
-                    double* Tdn) {
+void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, real* Tup,
+                    real* Tdn) {
   ::alfa::note_launch(); k_sl_TupTdn<<<nblocks(e.N()), TPB, 0, e.stream>>>(f, sl_const(e), beta, Tup, Tdn, e.N(), e.nz);
 }
 
 // ---------------------------------------------------------------------------
 // wall stresses (SGSStresses_SM.py:63-90, 238-241) and plane-0 overrides
 // ---------------------------------------------------------------------------
-__global__ void k_wall(const double* __restrict__ u, const double* __restrict__ v,
+__global__ void k_wall(const real* __restrict__ u, const real* __restrict__ v,
                        const double* __restrict__ M, const double* __restrict__ pm,
-                       const double* __restrict__ pm0, double* txz, double* tyz, size_t H, int nz,
+                       const double* __restrict__ pm0, real* txz, real* tyz, size_t H, int nz,
                        double log_m, double Ugal) {
   GRID_STRIDE(r, H) {
     const double denom = log_m + pm[r] - pm0[r];
     const double us = 0.4 * M[r] / denom;
     const size_t i = r * nz;
-    txz[i] = -(us * us) * (u[i] + Ugal) / M[r];
+    txz[i] = -(us * us) * ((double)u[i] + Ugal) / M[r];
     tyz[i] = -(us * us) * v[i] / M[r];
   }
 }
 
-void wall_override(Engine& e, const double* u, const double* v, const double* M,
-                   const double* psi_m, const double* psi_m0, double* txz, double* tyz) {
+void wall_override(Engine& e, const real* u, const real* v, const double* M,
+                   const double* psi_m, const double* psi_m0, real* txz, real* tyz) {
   const double log_m = std::log(0.5 * e.dz * e.z_scale / e.cfg.z0m);
   ::alfa::note_launch(); k_wall<<<nblocks(e.H()), TPB, 0, e.stream>>>(u, v, M, psi_m, psi_m0, txz, tyz, e.H(), e.nz,
                                                 log_m, e.cfg.Ugal);
 }
 
-__global__ void k_set_plane0(const double* __restrict__ p, double* f, size_t H, int nz) {
+__global__ void k_set_plane0(const double* __restrict__ p, real* f, size_t H, int nz) {
   GRID_STRIDE(r, H) { f[r * nz] = p[r]; }
 }
 
-void set_plane0(Engine& e, const double* plane, double* field) {
+void set_plane0(Engine& e, const double* plane, real* field) {
   ::alfa::note_launch(); k_set_plane0<<<nblocks(e.H()), TPB, 0, e.stream>>>(plane, field, e.H(), e.nz);
 }
 
@@ -1335,9 +1335,11 @@ void set_plane0(Engine& e, const double* plane, double* field) {
 // RHS assembly: NSE_AllTerms.py:82-102, SCL_AllTerms.py:68-80
 // ---------------------------------------------------------------------------
 struct RhsM {
-  const double *u, *v, *w, *Ug, *Vg, *Cx, *Cy, *Cz, *b, *dx, *dy, *dz, *Uadv, *Vadv, *ubar, *vbar,
-      *rd, *rds;
-  double *Ru, *Rv, *Rw;
+  const real *u, *v, *w;
+  const double *Ug, *Vg;
+  const real *Cx, *Cy, *Cz, *b, *dx, *dy, *dz;
+  const double *Uadv, *Vadv, *ubar, *vbar, *rd, *rds;
+  real *Ru, *Rv, *Rw;
   double f, Ugal;
   int adv, damp;
   const int* itp;   // non-null: the forcing profiles are row (*itp - 1) of a series
@@ -1350,18 +1352,18 @@ __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
   const size_t grow = a.gtp ? (size_t)(*a.gtp - 1) * a.grs : 0;
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
-    double ru = -a.Cx[i] - a.dx[i] - a.f * (a.Vg[grow + z] - a.v[i]);
-    double rv = -a.Cy[i] - a.dy[i] + a.f * (a.Ug[grow + z] - a.Ugal - a.u[i]);
-    double rw = -a.Cz[i] - a.dz[i] + a.b[i];
+    double ru = -(double)a.Cx[i] - (double)a.dx[i] - a.f * (a.Vg[grow + z] - (double)a.v[i]);
+    double rv = -(double)a.Cy[i] - (double)a.dy[i] + a.f * (a.Ug[grow + z] - a.Ugal - (double)a.u[i]);
+    double rw = -(double)a.Cz[i] - (double)a.dz[i] + (double)a.b[i];
     if (a.adv) {
       const size_t row = a.itp ? (size_t)(*a.itp - 1) * a.rs : 0;
       ru = ru + a.Uadv[row + z];
       rv = rv + a.Vadv[row + z];
     }
     if (a.damp) {
-      ru = ru - a.rds[z] * (a.u[i] - a.ubar[z]);
-      rv = rv - a.rds[z] * (a.v[i] - a.vbar[z]);
-      rw = rw - a.rd[z] * a.w[i];
+      ru = ru - a.rds[z] * ((double)a.u[i] - a.ubar[z]);
+      rv = rv - a.rds[z] * ((double)a.v[i] - a.vbar[z]);
+      rw = rw - a.rd[z] * (double)a.w[i];
     }
     a.Ru[i] = ru;
     a.Rv[i] = rv;
@@ -1369,11 +1371,11 @@ __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
   }
 }
 
-void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
-                  const double* Ug, const double* Vg, const double* Cx, const double* Cy,
-                  const double* Cz, const double* b, const double* dx, const double* dy,
-                  const double* dz, const double* Uadv, const double* Vadv, const double* ubar,
-                  const double* vbar, double* Ru, double* Rv, double* Rw, const int* itp,
+void rhs_momentum(Engine& e, const real* u, const real* v, const real* w,
+                  const double* Ug, const double* Vg, const real* Cx, const real* Cy,
+                  const real* Cz, const real* b, const real* dx, const real* dy,
+                  const real* dz, const double* Uadv, const double* Vadv, const double* ubar,
+                  const double* vbar, real* Ru, real* Rv, real* Rw, const int* itp,
                   long long rs, const int* gtp, long long grs) {
   RhsM a{u, v, w, Ug, Vg, Cx, Cy, Cz, b, dx, dy, dz, Uadv, Vadv, ubar, vbar, e.d_rd, e.d_rd_stag,
          Ru, Rv, Rw, e.f_nondim, e.cfg.Ugal, e.cfg.optAdvection >= 1, e.cfg.optDamping == 1, itp,
@@ -1381,22 +1383,22 @@ void rhs_momentum(Engine& e, const double* u, const double* v, const double* w,
   ::alfa::note_launch(); k_rhs_m<<<nblocks(e.N()), TPB, 0, e.stream>>>(a, e.N(), e.nz);
 }
 
-__global__ void k_rhs_s(const double* __restrict__ TH, const double* __restrict__ adv,
-                        const double* __restrict__ dq, const double* __restrict__ THadv,
-                        const double* __restrict__ bar, const double* __restrict__ rds, double* R,
+__global__ void k_rhs_s(const real* __restrict__ TH, const real* __restrict__ adv,
+                        const real* __restrict__ dq, const double* __restrict__ THadv,
+                        const double* __restrict__ bar, const double* __restrict__ rds, real* R,
                         size_t n, int nz, int doadv, int damp, const int* itp, long long rs) {
   const size_t row = (doadv && itp) ? (size_t)(*itp - 1) * rs : 0;
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
-    double r = -adv[i] - dq[i];
+    double r = -(double)adv[i] - (double)dq[i];
     if (doadv) r = r + THadv[row + z];
-    if (damp) r = r - rds[z] * (TH[i] - bar[z]);
+    if (damp) r = r - rds[z] * ((double)TH[i] - bar[z]);
     R[i] = r;
   }
 }
 
-void rhs_scalar(Engine& e, const double* TH, const double* adv, const double* divq,
-                const double* THadv, const double* THbar, double* R, const int* itp,
+void rhs_scalar(Engine& e, const real* TH, const real* adv, const real* divq,
+                const double* THadv, const double* THbar, real* R, const int* itp,
                 long long rs, int always_adv) {
   ::alfa::note_launch(); k_rhs_s<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, adv, divq, THadv, THbar, e.d_rd_stag, R,
                                                  e.N(), e.nz,
@@ -1428,12 +1430,12 @@ __global__ void k_rc(const cd* __restrict__ fRx, const cd* __restrict__ fRy,
     } else {
       const size_t a = m * nz + (k - 1);
       const double q = kr[i], c = (double)j;
-      double hr = -q * fRx[a].y;
-      hr = hr - c * fRy[a].y;
-      double hi = q * fRx[a].x;
-      hi = hi + c * fRy[a].x;
-      RCr[t] = hr + (fRz[a + 1].x - fRz[a].x) / dz;
-      RCi[t] = hi + (fRz[a + 1].y - fRz[a].y) / dz;
+      double hr = -q * (double)fRx[a].y;
+      hr = hr - c * (double)fRy[a].y;
+      double hi = q * (double)fRx[a].x;
+      hi = hi + c * (double)fRy[a].x;
+      RCr[t] = hr + ((double)fRz[a + 1].x - (double)fRz[a].x) / dz;
+      RCi[t] = hi + ((double)fRz[a + 1].y - (double)fRz[a].y) / dz;
     }
     if (k < nz) fRzr[m * nz + k] = fRz[m * nz + k].x;
   }
@@ -1445,63 +1447,71 @@ void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const c
       fRx, fRy, fRz, fb2, e.d_kr, RCr, RCi, fRz_real, e.nx, e.nyh, e.nz, e.dz);
 }
 
+// Forward elimination and back substitution per mode with the factors of
+// engine_init.  The forward sweep's modified right-hand side is kept in dm
+// (FP64): in the FP64 build dm is the output spectrum itself (overwritten in
+// the back substitution, element by element after it is read), in the FP32
+// build a separate FP64 buffer, so the whole solve runs in FP64.
 __global__ void k_thomas(const double* __restrict__ RCr, const double* __restrict__ RCi,
                          const double* __restrict__ fRzr, const double* __restrict__ bt,
                          const double* __restrict__ mt, const double* __restrict__ cp, cd* fp,
-                         int nx, int nyh, int nz, double dz) {
+                         double2* dm_all, int nx, int nyh, int nz, double dz) {
   const size_t nm = (size_t)nx * nyh;
   GRID_STRIDE(m, nm) {
     const int j = (int)(m % nyh), i = (int)(m / nyh);
     const size_t base = m * (nz + 1);
     cd* out = fp + m * nz;
+    double2* dm = dm_all + m * nz;
     if (i == 0 && j == 0) {
       // zero mode by direct integration (Thomas.py:271-275)
       const double z0 = RCr[0];
-      out[0] = make_double2(z0, 0.0);
+      out[0] = mkc(z0, 0);
       double s = 0.0;
       for (int k = 1; k < nz; k++) {
         s = s + fRzr[k] * dz;
-        out[k] = make_double2(z0 + s, 0.0);
+        out[k] = mkc(z0 + s, 0);
       }
       continue;
     }
     if (i == nx / 2 || j == nyh - 1) {  // x- and y-Nyquist rows masked
-      for (int k = 0; k < nz; k++) out[k] = make_double2(0.0, 0.0);
+      for (int k = 0; k < nz; k++) out[k] = mkc(0, 0);
       continue;
     }
-    // forward sweep (d_mod stored in out[k-1] for k >= 1)
+    // forward sweep (d_mod stored in dm[k-1] for k >= 1)
     double dr = RCr[base], di = RCi[base];
-    const double d0r = dr, d0i = di;
     for (int k = 1; k <= nz; k++) {
       const double mk = mt[(size_t)(k - 1) * nm + m];
       dr = RCr[base + k] - mk * dr;
       di = RCi[base + k] - mk * di;
-      out[k - 1] = make_double2(dr, di);
+      dm[k - 1] = make_double2(dr, di);
     }
-    (void)d0r;
-    (void)d0i;
     // back substitution, x[k] for k = nz .. 1 (x[0] is not used)
     double xr = dr / bt[base + nz], xi = di / bt[base + nz];
-    out[nz - 1] = make_double2(xr, xi);
+    out[nz - 1] = mkc(xr, xi);
     for (int k = nz - 1; k >= 1; k--) {
-      const cd dm = out[k - 1];
+      const double2 d = dm[k - 1];
       const double b = bt[base + k], c = cp[k];
-      xr = (dm.x - c * xr) / b;
-      xi = (dm.y - c * xi) / b;
-      out[k - 1] = make_double2(xr, xi);
+      xr = (d.x - c * xr) / b;
+      xi = (d.y - c * xi) / b;
+      out[k - 1] = mkc(xr, xi);
     }
   }
 }
 
 void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double* fRz_real, cd* fp) {
   const size_t nm = (size_t)e.nx * e.nyh;
+#ifdef ALFA_BUILD_FP32
+  double2* dm = e.thomas_dm;
+#else
+  double2* dm = fp;
+#endif
   ::alfa::note_launch(); k_thomas<<<(int)((nm + 127) / 128), 128, 0, e.stream>>>(RCr, RCi, fRz_real, e.d_b_thomas,
-                                                          e.d_m_thomas, e.d_c_p, fp, e.nx, e.nyh,
+                                                          e.d_m_thomas, e.d_c_p, fp, dm, e.nx, e.nyh,
                                                           e.nz, e.dz);
 }
 
-__global__ void k_sub3(double* a, double* b, double* c, const double* __restrict__ x,
-                       const double* __restrict__ y, const double* __restrict__ z, size_t n) {
+__global__ void k_sub3(real* a, real* b, real* c, const real* __restrict__ x,
+                       const real* __restrict__ y, const real* __restrict__ z, size_t n) {
   GRID_STRIDE(i, n) {
     a[i] = a[i] - x[i];
     b[i] = b[i] - y[i];
@@ -1509,8 +1519,8 @@ __global__ void k_sub3(double* a, double* b, double* c, const double* __restrict
   }
 }
 
-void subtract3(Engine& e, double* Ru, double* Rv, double* Rw, const double* a, const double* b,
-               const double* c) {
+void subtract3(Engine& e, real* Ru, real* Rv, real* Rw, const real* a, const real* b,
+               const real* c) {
   ::alfa::note_launch(); k_sub3<<<nblocks(e.N()), TPB, 0, e.stream>>>(Ru, Rv, Rw, a, b, c, e.N());
 }
 
@@ -1518,13 +1528,13 @@ void subtract3(Engine& e, double* Ru, double* Rv, double* Rw, const double* a, c
 // AB2: NSE_TimeAdvancement.py:66-74, SCL_TimeAdvancement.py:64-69.  The
 // thread of level nz-2 also writes level nz-1, so in-place update is safe.
 // ---------------------------------------------------------------------------
-__global__ void k_ab2(const double* u, const double* __restrict__ R, const double* __restrict__ Rp,
-                      double* un, size_t n, int nz, double dt, int mode, double top_add) {
+__global__ void k_ab2(const real* u, const real* __restrict__ R, const real* __restrict__ Rp,
+                      real* un, size_t n, int nz, double dt, int mode, double top_add) {
   // mode 0: u/v (top copies nz-2), 1: w (top and bottom 0), 2: TH (top = nz-2 + c)
   GRID_STRIDE(i, n) {
     const int z = (int)(i % nz);
     if (z == nz - 1) continue;
-    const double val = u[i] + dt * (1.5 * R[i] - 0.5 * Rp[i]);
+    const double val = (double)u[i] + dt * (1.5 * (double)R[i] - 0.5 * (double)Rp[i]);
     if (mode == 1) {
       un[i] = (z == 0) ? 0.0 : val;
       if (z == nz - 2) un[i + 1] = 0.0;
@@ -1535,33 +1545,33 @@ __global__ void k_ab2(const double* u, const double* __restrict__ R, const doubl
   }
 }
 
-void ab2_uvw(Engine& e, const double* u, const double* v, const double* w, const double* Ru,
-             const double* Rup, const double* Rv, const double* Rvp, const double* Rw,
-             const double* Rwp, double* un, double* vn, double* wn) {
+void ab2_uvw(Engine& e, const real* u, const real* v, const real* w, const real* Ru,
+             const real* Rup, const real* Rv, const real* Rvp, const real* Rw,
+             const real* Rwp, real* un, real* vn, real* wn) {
   ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(u, Ru, Rup, un, e.N(), e.nz, e.dt_nondim, 0, 0.0);
   ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(v, Rv, Rvp, vn, e.N(), e.nz, e.dt_nondim, 0, 0.0);
   ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(w, Rw, Rwp, wn, e.N(), e.nz, e.dt_nondim, 1, 0.0);
 }
 
-void ab2_th(Engine& e, const double* TH, const double* R, const double* Rp, double* out) {
+void ab2_th(Engine& e, const real* TH, const real* R, const real* Rp, real* out) {
   ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(TH, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
                                                e.inversion_nondim * e.dz);
 }
 
-void ab2_q(Engine& e, const double* Q, const double* R, const double* Rp, double* out) {
+void ab2_q(Engine& e, const real* Q, const real* R, const real* Rp, real* out) {
   ::alfa::note_launch(); k_ab2<<<nblocks(e.N()), TPB, 0, e.stream>>>(Q, R, Rp, out, e.N(), e.nz, e.dt_nondim, 2,
                                                e.q_inversion_nondim * e.dz);
 }
 
 // max |u|, |v|, |w| (Main.py:534-537)
-__global__ void k_absmax_partial(const double* __restrict__ a, const double* __restrict__ b,
-                                 const double* __restrict__ c, size_t n, double* part) {
+__global__ void k_absmax_partial(const real* __restrict__ a, const real* __restrict__ b,
+                                 const real* __restrict__ c, size_t n, double* part) {
   __shared__ double sh[3][256];
   double m0 = 0.0, m1 = 0.0, m2 = 0.0;
   GRID_STRIDE(i, n) {
-    m0 = fmax(m0, fabs(a[i]));
-    m1 = fmax(m1, fabs(b[i]));
-    m2 = fmax(m2, fabs(c[i]));
+    m0 = fmax(m0, fabs((double)a[i]));
+    m1 = fmax(m1, fabs((double)b[i]));
+    m2 = fmax(m2, fabs((double)c[i]));
   }
   sh[0][threadIdx.x] = m0;
   sh[1][threadIdx.x] = m1;
@@ -1584,14 +1594,14 @@ __global__ void k_absmax_finish(const double* part, int nb, double* out) {
   }
 }
 
-void cfl_max(Engine& e, const double* u, const double* v, const double* w, double* out3) {
+void cfl_max(Engine& e, const real* u, const real* v, const real* w, double* out3) {
   const int nb = 256;
   ::alfa::note_launch(); k_absmax_partial<<<nb, 256, 0, e.stream>>>(u, v, w, e.N(), e.red);
   ::alfa::note_launch(); k_absmax_finish<<<1, 32, 0, e.stream>>>(e.red, nb, out3);
 }
 
 // copy z-planes k0 and k1 of F into a (nx, ny, 2) field
-__global__ void k_planes(const double* __restrict__ F, int k0, int k1, double* out, size_t H,
+__global__ void k_planes(const real* __restrict__ F, int k0, int k1, real* out, size_t H,
                          int nz) {
   GRID_STRIDE(r, H) {
     out[r * 2 + 0] = F[r * nz + k0];
@@ -1599,8 +1609,9 @@ __global__ void k_planes(const double* __restrict__ F, int k0, int k1, double* o
   }
 }
 
-void copy_planes_z(Engine& e, const double* F, int k0, int k1, double* out2) {
+void copy_planes_z(Engine& e, const real* F, int k0, int k1, real* out2) {
   ::alfa::note_launch(); k_planes<<<nblocks(e.H()), TPB, 0, e.stream>>>(F, k0, k1, out2, e.H(), e.nz);
 }
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

@@ -24,8 +24,9 @@
 #include "alfa_tile.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
-// Load the (n x 16 z) real tile of row `row` into b0 as n x 8 complex
+// Load the (n x 2 YC z) real tile of row `row` into b0 as n x YC complex
 // (z pairs), U elements per thread in flight.
 template <int KIND>
 __device__ __forceinline__ void y_fwd_load(const Loader& L, int row, int n, int z0, cd* b0) {
@@ -37,16 +38,16 @@ __device__ __forceinline__ void y_fwd_load(const Loader& L, int row, int n, int 
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * blockDim.x;
-      v[u] = make_double2(0.0, 0.0);
+      v[u] = mkc(0, 0);
       if (t < total) {
         const int y = t / YC, c = t % YC;
         const int z = z0 + 2 * c;
         const size_t i = ((size_t)row * n + y) * nz + z;
         if (vec && z + 1 < nz) {
-          v[u] = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+          v[u] = __ldg(reinterpret_cast<const cd*>(L.a[0] + i));
         } else {
-          if (z < nz) v[u].x = ldv<KIND>(L, i, z);
-          if (z + 1 < nz) v[u].y = ldv<KIND>(L, i + 1, z + 1);
+          if (z < nz) v[u].x = (real)ldv<KIND>(L, i, z);
+          if (z + 1 < nz) v[u].y = (real)ldv<KIND>(L, i + 1, z + 1);
         }
       }
     }
@@ -62,7 +63,7 @@ __device__ __forceinline__ void y_fwd_load(const Loader& L, int row, int n, int 
 // k_y_fwd: rows x n(y) x nz real -> T (rows, K, nz) complex, ky < K
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() == 128 ? 4 : 1))
+__global__ void __launch_bounds__(tile_threads<YC, N>(), (N == 256 ? Y_MINBLOCKS : 1))
     k_y_fwd(Loader L, FftPlan p, int K, cd* __restrict__ T) {
   extern __shared__ cd sm[];
   const int n = (N > 0) ? N : p.n;
@@ -110,8 +111,9 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
     const int z = z0 + 2 * c;
     const cd zk = Z[k * YC + c];
     const cd zn = Z[((n - k) % n) * YC + c];
-    const cd A = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y - zn.y));
-    const cd B = make_double2(0.5 * (zk.y + zn.y), -0.5 * (zk.x - zn.x));
+    const real h = (real)0.5;
+    const cd A = mkc(h * (zk.x + zn.x), h * (zk.y - zn.y));
+    const cd B = mkc(h * (zk.y + zn.y), -h * (zk.x - zn.x));
     const size_t o = ((size_t)row * K + k) * nz + z;
     if (z < nz) T[o] = A;
     if (z + 1 < nz) T[o + 1] = B;
@@ -122,9 +124,9 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
 // k_y_inv: T (rows, K, nz), ky < K nonzero -> rows x n(y) x nz real
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() == 128 ? 4 : 1))
+__global__ void __launch_bounds__(tile_threads<YC, N>(), (N == 256 ? Y_MINBLOCKS : 1))
     k_y_inv(const cd* __restrict__ T, int K, FftPlan p, int nz, double scale,
-            double* __restrict__ out, int accumulate) {
+            real* __restrict__ out, int accumulate) {
   extern __shared__ cd sm[];
   const int n = (N > 0) ? N : p.n;
   const int h = n / 2;
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
       for (int r = 0; r < R; r++) {
         const int k = j + r * NR;
         const int src = k <= h ? k : N - k;
-        cd a = make_double2(0.0, 0.0), bb = make_double2(0.0, 0.0);
+        cd a = mkc(0, 0), bb = mkc(0, 0);
         if (ok && src < K) {
           const size_t o = ((size_t)row * K + src) * nz + z;
           a = __ldg(T + o);
@@ -162,8 +164,8 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
           a.y = 0.0;
           bb.y = 0.0;
         }
-        v[q * R + r] = k <= h ? make_double2(a.x - bb.y, a.y + bb.x)
-                              : make_double2(a.x + bb.y, bb.x - a.y);
+        v[q * R + r] = k <= h ? mkc(a.x - bb.y, a.y + bb.x)
+                              : mkc(a.x + bb.y, bb.x - a.y);
       }
     }
     const size_t base = (size_t)row * N * nz;
@@ -206,8 +208,8 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int t = t0 + u * blockDim.x;
-      A[u] = make_double2(0.0, 0.0);
-      B[u] = make_double2(0.0, 0.0);
+      A[u] = mkc(0, 0);
+      B[u] = mkc(0, 0);
       const int k = t / YC, c = t % YC;
       const int z = z0 + 2 * c;
       if (t < total && k < K) {
@@ -231,25 +233,26 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
         a.y = 0.0;
         b.y = 0.0;
       }
-      b0[k * YC + c] = make_double2(a.x - b.y, a.y + b.x);
-      if (k > 0 && k < h) b0[(n - k) * YC + c] = make_double2(a.x + b.y, b.x - a.y);
+      b0[k * YC + c] = mkc(a.x - b.y, a.y + b.x);
+      if (k > 0 && k < h) b0[(n - k) * YC + c] = mkc(a.x + b.y, b.x - a.y);
     }
   }
   tile_fft<+1, YC, N, tile_threads<YC, N>()>(b0, p);
   const cd* Z = b0;
+  const real sc = (real)scale;
   if (accumulate) {
     for (int t0 = threadIdx.x; t0 < n * YC; t0 += U * blockDim.x) {
-      double2 prev[U];
+      cd prev[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int t = t0 + u * blockDim.x;
         const int y = t / YC, c = t % YC;
         const int z = z0 + 2 * c;
         const size_t o = ((size_t)row * n + y) * nz + z;
-        prev[u] = make_double2(0.0, 0.0);
+        prev[u] = mkc(0, 0);
         if (t < n * YC) {
           if (pair && z < nz) {
-            prev[u] = *reinterpret_cast<const double2*>(out + o);
+            prev[u] = *reinterpret_cast<const cd*>(out + o);
           } else {
             if (z < nz) prev[u].x = out[o];
             if (z + 1 < nz) prev[u].y = out[o + 1];
@@ -264,9 +267,9 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
         const int z = z0 + 2 * c;
         const size_t o = ((size_t)row * n + y) * nz + z;
         const cd v = Z[t];
-        const double2 w = make_double2(prev[u].x + scale * v.x, prev[u].y + scale * v.y);
+        const cd w = mkc(prev[u].x + sc * v.x, prev[u].y + sc * v.y);
         if (pair && z < nz) {
-          *reinterpret_cast<double2*>(out + o) = w;
+          *reinterpret_cast<cd*>(out + o) = w;
         } else {
           if (z < nz) out[o] = w.x;
           if (z + 1 < nz) out[o + 1] = w.y;
@@ -280,10 +283,10 @@ __global__ void __launch_bounds__(tile_threads<YC, N>(), (tile_threads<YC, N>() 
       const size_t o = ((size_t)row * n + y) * nz + z;
       const cd v = Z[t];
       if (pair && z < nz) {
-        *reinterpret_cast<double2*>(out + o) = make_double2(scale * v.x, scale * v.y);
+        *reinterpret_cast<cd*>(out + o) = mkc(sc * v.x, sc * v.y);
       } else {
-        if (z < nz) out[o] = scale * v.x;
-        if (z + 1 < nz) out[o + 1] = scale * v.y;
+        if (z < nz) out[o] = sc * v.x;
+        if (z + 1 < nz) out[o + 1] = sc * v.y;
       }
     }
   }
@@ -312,28 +315,28 @@ __device__ __forceinline__ cd map_value(const XArgs& a, const XOut& o, const cd*
       return S[k * C + c];
     case MAP_TRUNC: {
       const bool keep = (k < o.cx || k >= a.nx - o.cx + 1) && ky < o.cy;
-      return keep ? S[k * C + c] : make_double2(0.0, 0.0);
+      return keep ? S[k * C + c] : mkc(0, 0);
     }
     case MAP_DX: {
       const cd v = S[k * C + c];
-      const double q = a.kx[k];
-      return make_double2(-(q * v.y), q * v.x);
+      const real q = (real)a.kx[k];
+      return mkc(-(q * v.y), q * v.x);
     }
     case MAP_DY: {
       const cd v = S[k * C + c];
-      const double q = a.ky[ky];
-      return make_double2(-(q * v.y), q * v.x);
+      const real q = (real)a.ky[ky];
+      return mkc(-(q * v.y), q * v.x);
     }
     case MAP_PAD: {  // Dealiasing.py:67-73 (rows nx -> mx)
       const int h = a.nx / 2;
       if (k <= h) return S[k * C + c];
       if (k >= a.mx - h) return S[(k - a.mx + a.nx) * C + c];
-      return make_double2(0.0, 0.0);
+      return mkc(0, 0);
     }
     default: {  // MAP_UNPAD, Dealiasing.py:102-109 (rows mx -> nx)
       const int h = a.nx / 2;
       if (k < h) return S[k * C + c];
-      if (k == h) return make_double2(0.0, 0.0);
+      if (k == h) return mkc(0, 0);
       return S[(k - a.nx + a.mx) * C + c];
     }
   }
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x
 #pragma unroll
         for (int r = 0; r < R; r++)
           v[q * R + r] = ok ? __ldg(&a.src[((size_t)(j + r * NR) * a.Kin + ky) * nz + z])
-                            : make_double2(0.0, 0.0);
+                            : mkc(0, 0);
       }
       if constexpr (R == NI) {
         if (threadIdx.x < C) {
@@ -410,7 +413,7 @@ __global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x
 #pragma unroll
           for (int r = 0; r < RO; r++)
             w[q * RO + r] = (BO % NT == 0 || b < BO) ? map_value<C>(a, o, S, j + r * NRO, ky, c)
-                                                      : make_double2(0.0, 0.0);
+                                                      : mkc(0, 0);
         }
         if constexpr (RO == NO) {
           if (threadIdx.x < C) {
@@ -458,7 +461,7 @@ __global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x
       const int t = t0 + u * blockDim.x;
       const int r = t / C, c = t % C;
       const int z = z0 + c;
-      v[u] = make_double2(0.0, 0.0);
+      v[u] = mkc(0, 0);
       if (have && t < total && z < nz) v[u] = __ldg(&a.src[((size_t)r * a.Kin + ky) * nz + z]);
     }
 #pragma unroll
@@ -515,7 +518,7 @@ static void y_fwd_n(Engine& e, const Loader& L, int rows, const FftPlan& p, int 
 
 template <int N>
 static void y_inv_n(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
-                    double* out, int accumulate) {
+                    real* out, int accumulate) {
   const size_t smem = (size_t)p.n * YC * sizeof(cd);
   set_smem((const void*)k_y_inv<N>, smem);
   dim3 g((e.nz + 2 * YC - 1) / (2 * YC), rows);
@@ -535,7 +538,7 @@ void launch_y_fwd(Engine& e, const Loader& L, int rows, const FftPlan& p, int K,
 }
 
 void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
-                  double* out, int accumulate) {
+                  real* out, int accumulate) {
   ::alfa::note_launch();
   switch (p.n) {
 #define ALFA_CASE(n) \
@@ -587,21 +590,21 @@ void launch_x(Engine& e, const cd* src, int in_spec, int rows_in, int Kin, const
   if (same_inv) {
 #define ALFA_CASE(p, q)                                        \
   if (ni == p && ninv == q) {                                  \
-    if ((p > q ? p : q) <= 256) x_n<8, p, q>(e, a, Kgrid);     \
-    else x_n<4, p, q>(e, a, Kgrid);                            \
+    if ((p > q ? p : q) <= 256) x_n<YC, p, q>(e, a, Kgrid);    \
+    else x_n<YC / 2, p, q>(e, a, Kgrid);                       \
     return;                                                    \
   }
     ALFA_X_PAIRS(ALFA_CASE)
 #undef ALFA_CASE
   }
-  if (maxrows <= 256) x_n<8, 0, 0>(e, a, Kgrid);
-  else x_n<4, 0, 0>(e, a, Kgrid);
+  if (maxrows <= 256) x_n<YC, 0, 0>(e, a, Kgrid);
+  else x_n<YC / 2, 0, 0>(e, a, Kgrid);
 }
 
 // ---------------------------------------------------------------------------
 // composite operators
 // ---------------------------------------------------------------------------
-Loader ld_field(const Engine& e, const double* a) {
+Loader ld_field(const Engine& e, const real* a) {
   Loader L{};
   L.kind = LD_FIELD;
   L.nz = e.nz;
@@ -657,7 +660,7 @@ void op_rfft2_pad(Engine& e, const Loader& L, cd* spec_pad) {
 }
 
 // Filtering.py:50-89 applied to FFT(field)
-void op_filter_explicit(Engine& e, const Loader& L, double* out, cd* spec) {
+void op_filter_explicit(Engine& e, const Loader& L, real* out, cd* spec) {
   const int cx = e.cut_e[0], cy = e.cut_e[1];
   launch_y_fwd(e, L, e.nx, e.pny, e.nyh, e.T[0]);
   XOut o[2] = {xo_spec(e, MAP_TRUNC, spec, cx, cy),
@@ -667,7 +670,7 @@ void op_filter_explicit(Engine& e, const Loader& L, double* out, cd* spec) {
 }
 
 // Filtering_Level1 / Level2 (Filtering.py:97-165) of one FFT(field)
-void op_filter12(Engine& e, const Loader& L, double* out1, double* out2) {
+void op_filter12(Engine& e, const Loader& L, real* out1, real* out2) {
   const int c1x = e.cut_1[0], c1y = e.cut_1[1], c2x = e.cut_2[0], c2y = e.cut_2[1];
   const int K = c1y > c2y ? c1y : c2y;
   launch_y_fwd(e, L, e.nx, e.pny, K, e.T[0]);
@@ -679,7 +682,7 @@ void op_filter12(Engine& e, const Loader& L, double* out1, double* out2) {
 }
 
 // one filter level of a given spectrum
-void op_filter1_spec(Engine& e, const cd* spec, int level, double* out) {
+void op_filter1_spec(Engine& e, const cd* spec, int level, real* out) {
   const int* cut = level == 1 ? e.cut_1 : e.cut_2;
   XOut o = xo_inv(MAP_TRUNC, e.T[1], e.nx, cut[1], e.pnx, cut[0], cut[1]);
   launch_x(e, spec, 1, e.nx, e.nyh, e.pnx, 1, &o, cut[1]);
@@ -687,7 +690,7 @@ void op_filter1_spec(Engine& e, const cd* spec, int level, double* out) {
 }
 
 // Derivxy (Derivatives.py:161-182) in x and/or y of a spectrum
-void op_deriv_spec(Engine& e, const cd* spec, double* dx, double* dy) {
+void op_deriv_spec(Engine& e, const cd* spec, real* dx, real* dy) {
   XOut o[2];
   int n = 0;
   if (dx) o[n++] = xo_inv(MAP_DX, e.T[1], e.nx, e.nyh, e.pnx);
@@ -698,7 +701,7 @@ void op_deriv_spec(Engine& e, const cd* spec, double* dx, double* dy) {
 }
 
 // Derivxy(FFT(field)) in x and/or y
-void op_deriv_field(Engine& e, const Loader& L, double* dx, double* dy) {
+void op_deriv_field(Engine& e, const Loader& L, real* dx, real* dy) {
   launch_y_fwd(e, L, e.nx, e.pny, e.nyh, e.T[0]);
   XOut o[2];
   int n = 0;
@@ -710,7 +713,7 @@ void op_deriv_field(Engine& e, const Loader& L, double* dx, double* dy) {
 }
 
 // Dealias1(FFT(field)) (Dealiasing.py:51-78)
-void op_pad(Engine& e, const Loader& L, double* out_pad) {
+void op_pad(Engine& e, const Loader& L, real* out_pad) {
   launch_y_fwd(e, L, e.nx, e.pny, e.nyh, e.T[0]);
   XOut o = xo_inv(MAP_PAD, e.T[1], e.mx, e.nyh, e.pmx);
   launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 1, &o, e.nyh);
@@ -718,7 +721,7 @@ void op_pad(Engine& e, const Loader& L, double* out_pad) {
 }
 
 // Dealias1(spectrum)
-void op_pad_spec(Engine& e, const cd* spec, double* out_pad) {
+void op_pad_spec(Engine& e, const cd* spec, real* out_pad) {
   XOut o = xo_inv(MAP_PAD, e.T[1], e.mx, e.nyh, e.pmx);
   launch_x(e, spec, 1, e.nx, e.nyh, e.pnx, 1, &o, e.nyh);
   launch_y_inv(e, e.T[1], e.mx, e.nyh, e.pmy, inv_scale(e.mx, e.my), out_pad, 0);
@@ -726,7 +729,7 @@ void op_pad_spec(Engine& e, const cd* spec, double* out_pad) {
 
 // Dealias2(FFT_pad(padded field)) (Dealiasing.py:86-114): keeps ky < ny/2,
 // drops the x Nyquist row, rescales by 9/4.
-void op_unpad(Engine& e, const Loader& L_pad, double* out) {
+void op_unpad(Engine& e, const Loader& L_pad, real* out) {
   const int K = e.nyh - 1;
   launch_y_fwd(e, L_pad, e.mx, e.pmy, K, e.T[0]);
   XOut o = xo_inv(MAP_UNPAD, e.T[1], e.nx, K, e.pnx);
@@ -735,7 +738,7 @@ void op_unpad(Engine& e, const Loader& L_pad, double* out) {
 }
 
 // Dealias2(padded spectrum (mx, myh, nz))
-void op_unpad_spec(Engine& e, const cd* spec_pad, double* out) {
+void op_unpad_spec(Engine& e, const cd* spec_pad, real* out) {
   const int K = e.nyh - 1;
   XOut o = xo_inv(MAP_UNPAD, e.T[1], e.nx, K, e.pnx);
   launch_x(e, spec_pad, 1, e.mx, e.myh, e.pmx, 1, &o, K);
@@ -743,10 +746,11 @@ void op_unpad_spec(Engine& e, const cd* spec_pad, double* out) {
 }
 
 // irfft2(spectrum, s=(nx, ny))
-void op_irfft2(Engine& e, const cd* spec, double* out) {
+void op_irfft2(Engine& e, const cd* spec, real* out) {
   XOut o = xo_inv(MAP_IDENT, e.T[1], e.nx, e.nyh, e.pnx);
   launch_x(e, spec, 1, e.nx, e.nyh, e.pnx, 1, &o, e.nyh);
   launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, inv_scale(e.nx, e.ny), out, 0);
 }
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

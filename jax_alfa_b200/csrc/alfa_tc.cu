@@ -35,6 +35,7 @@
 #include "alfa_internal.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
 namespace tc {
 
@@ -475,4 +476,5 @@ int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale
   return ALFA_OK;
 }
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

@@ -5,9 +5,18 @@
 #include "alfa_internal.cuh"
 
 namespace alfa {
+namespace ALFA_PREC {
 
-static constexpr int YC = 8;    // complex columns (= 16 real z levels) per y tile
-static constexpr int MAXTHREADS = 384;  // in-place sweeps need C*n/16 threads
+// Complex columns per tile: one 128-byte row segment (8 complex doubles = 16
+// z levels in the FP64 build, 16 complex floats = 32 z levels in the FP32
+// build).  The transform kernels are latency bound, so the FP32 build keeps
+// the FP64 build's shared-memory tile and bytes in flight per SM (twice the
+// threads of half the width) rather than halving them.
+static constexpr int YC = (int)(128 / sizeof(cd));
+static constexpr int MAXTHREADS = 48 * YC;  // in-place sweeps need C*n/16 threads (n <= 768)
+// resident CTAs per SM asked of the 2-D y-transform kernels at n = 256
+// (512 threads per SM in both builds)
+static constexpr int Y_MINBLOCKS = 512 / (YC * 256 / 16);
 static constexpr int U = 8;     // loads in flight per thread
 
 // ---------------------------------------------------------------------------
@@ -15,6 +24,7 @@ static constexpr int U = 8;     // loads in flight per thread
 // accessor at(k, d) = input k at level z + d (d = -1, 0, +1); ldv evaluates
 // it at one linear index i, eval_pair at the two levels (z, z+1) of a packed
 // complex column.  The kind is a compile-time constant in the tile kernels.
+// The expressions are evaluated in FP64 whatever the storage precision.
 // ---------------------------------------------------------------------------
 template <int KIND, class At>
 __device__ __forceinline__ double ev_kind(const Loader& L, const At& at, int z, int nz) {
@@ -98,30 +108,30 @@ __device__ __forceinline__ double ldv(const Loader& L, size_t i, int z) {
 
 // Input k around a packed column: levels z-1, z, z+1, z+2.
 struct Q4 {
-  double m, x, y, p;
+  real m, x, y, p;
 };
 
-// One 16-byte load per input for the pair (z, z+1); the z-1 and z+2
+// One two-value vector load per input for the pair (z, z+1); the z-1 and z+2
 // neighbours (NM, NP) come from the adjacent columns of the same row, which
 // sit in adjacent lanes (lane % C == column), by warp shuffles, and from a
 // scalar load at the tile's edge columns.  Every lane of the warp must call
 // it; lanes with ok == false contribute zeros.
 template <int C, bool NM, bool NP>
-__device__ __forceinline__ Q4 fetch_q4(const double* a, size_t i, int z, int nz, int c, bool ok) {
-  Q4 q{0.0, 0.0, 0.0, 0.0};
+__device__ __forceinline__ Q4 fetch_q4(const real* a, size_t i, int z, int nz, int c, bool ok) {
+  Q4 q{0, 0, 0, 0};
   const bool in = ok && z < nz;
   if (in) {
-    const double2 v = __ldg(reinterpret_cast<const double2*>(a + i));
+    const cd v = __ldg(reinterpret_cast<const cd*>(a + i));
     q.x = v.x;
     q.y = v.y;
   }
   if constexpr (NM) {
-    const double t = __shfl_up_sync(0xffffffffu, q.y, 1);
-    q.m = (c == 0) ? ((in && z > 0) ? __ldg(a + i - 1) : 0.0) : t;
+    const real t = __shfl_up_sync(0xffffffffu, q.y, 1);
+    q.m = (c == 0) ? ((in && z > 0) ? __ldg(a + i - 1) : (real)0) : t;
   }
   if constexpr (NP) {
-    const double t = __shfl_down_sync(0xffffffffu, q.x, 1);
-    q.p = (c == C - 1) ? ((in && z + 2 < nz) ? __ldg(a + i + 2) : 0.0) : t;
+    const real t = __shfl_down_sync(0xffffffffu, q.x, 1);
+    q.p = (c == C - 1) ? ((in && z + 2 < nz) ? __ldg(a + i + 2) : (real)0) : t;
   }
   return q;
 }
@@ -140,7 +150,7 @@ __device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz
   Q4 q[NIN];
   if constexpr (KIND == LD_W_SXX) {
 #pragma unroll
-    for (int k = 0; k < NIN; k++) q[k] = Q4{0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < NIN; k++) q[k] = Q4{0, 0, 0, 0};
     switch (L.sub) {  // uniform over the launch
       case 0: q[0] = fetch_q4<C, true, false>(L.a[0], i, z, nz, c, ok); break;
       case 1: q[4] = fetch_q4<C, true, false>(L.a[4], i, z, nz, c, ok); break;
@@ -176,31 +186,32 @@ __device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz
   }
   auto at0 = [&](int k, int d) -> double { return d < 0 ? q[k].m : (d == 0 ? q[k].x : q[k].y); };
   auto at1 = [&](int k, int d) -> double { return d < 0 ? q[k].x : (d == 0 ? q[k].y : q[k].p); };
-  return make_double2(ev_kind<KIND>(L, at0, z, nz), ev_kind<KIND>(L, at1, z + 1, nz));
+  return mkc((real)ev_kind<KIND>(L, at0, z, nz), (real)ev_kind<KIND>(L, at1, z + 1, nz));
 }
 
 // value pair (z, z+1) of the loader at linear index i
 template <int KIND>
 __device__ __forceinline__ cd load_pair(const Loader& L, size_t i, int z, int nz) {
-  cd t = make_double2(0.0, 0.0);
+  cd t = mkc(0, 0);
   if (KIND == LD_FIELD && (nz & 1) == 0) {
-    if (z < nz) t = __ldg(reinterpret_cast<const double2*>(L.a[0] + i));
+    if (z < nz) t = __ldg(reinterpret_cast<const cd*>(L.a[0] + i));
   } else {
-    if (z < nz) t.x = ldv<KIND>(L, i, z);
-    if (z + 1 < nz) t.y = ldv<KIND>(L, i + 1, z + 1);
+    if (z < nz) t.x = (real)ldv<KIND>(L, i, z);
+    if (z + 1 < nz) t.y = (real)ldv<KIND>(L, i + 1, z + 1);
   }
   return t;
 }
 
 // store (or accumulate) a scaled value pair at linear index i of dst
-__device__ __forceinline__ void store_pair2(double* __restrict__ dst, double scale, int accumulate,
+__device__ __forceinline__ void store_pair2(real* __restrict__ dst, double scale, int accumulate,
                                             size_t i, int z, int nz, cd v) {
   if (z >= nz) return;
-  double2 w = make_double2(scale * v.x, scale * v.y);
+  const real s = (real)scale;
+  cd w = mkc(s * v.x, s * v.y);
   if ((nz & 1) == 0) {
-    double2* p = reinterpret_cast<double2*>(dst + i);
+    cd* p = reinterpret_cast<cd*>(dst + i);
     if (accumulate) {
-      const double2 pv = *p;
+      const cd pv = *p;
       w.x += pv.x;
       w.y += pv.y;
     }
@@ -243,7 +254,7 @@ __device__ __forceinline__ void gather_rows(const Loader& L, int nz, size_t base
       if (KIND != LD_FIELD && (nz & 1) == 0)
         v[q * R + r] = eval_pair<KIND, C>(L, i, z, nz, c, ok);
       else
-        v[q * R + r] = ok ? load_pair<KIND>(L, i, z, nz) : make_double2(0.0, 0.0);
+        v[q * R + r] = ok ? load_pair<KIND>(L, i, z, nz) : mkc(0, 0);
     }
   }
 }
@@ -274,4 +285,5 @@ static inline void set_smem(const void* f, size_t bytes) { raise_smem_limit(f, b
   X(48, 48) X(64, 64) X(64, 96) X(96, 64) X(96, 96) X(128, 128) X(128, 192) X(192, 128)         \
   X(192, 192) X(256, 256) X(256, 384) X(384, 256) X(384, 384)
 
+}  // namespace ALFA_PREC
 }  // namespace alfa

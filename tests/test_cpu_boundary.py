@@ -19,7 +19,7 @@ def test_library_exports_every_declared_symbol():
 def test_signature_table_covers_header():
     declared = set(_lib.exported_symbols())
     bound = set(_lib.SIGNATURES) | {"alfa_create", "alfa_destroy", "alfa_last_error",
-                                    "alfa_set_stream", "alfa_get_derived",
+                                    "alfa_set_stream", "alfa_get_derived", "alfa_get_precision",
                                     "alfa_workspace_bytes", "alfa_get_diag",
                                     "alfa_launch_count", "alfa_time_kernel", "alfa_autotune",
                                     "alfa_tc_line_apply",
@@ -38,8 +38,27 @@ def test_config_struct_carries_every_case_option():
     from jax_alfa_b200.api import CONFIG_KEYS
     for make in cases.CASES.values():
         cfg = make()
-        missing = [k for k in CONFIG_KEYS if k not in cfg]
+        # precision follows the reference's use_double_precision switch
+        missing = [k for k in CONFIG_KEYS if k not in cfg and k != "precision"]
         assert not missing, missing
+
+
+def test_precision_follows_the_reference_switch():
+    from jax_alfa_b200.api import make_config
+    assert make_config(cases.neutral()).precision == _lib.FP64
+    assert make_config(cases.neutral(use_double_precision=False)).precision == _lib.FP32
+    assert make_config(cases.neutral(precision="mixed")).precision == _lib.MIXED
+    assert make_config(cases.neutral(precision="fp32")).precision == _lib.FP32
+
+
+def test_create_rejects_unknown_precision_without_gpu():
+    from jax_alfa_b200.api import make_config
+    lib = _lib.load()
+    c = make_config(cases.neutral())
+    c.precision = 7
+    ctx = ctypes.c_void_p()
+    assert lib.alfa_create(ctypes.byref(c), ctypes.byref(ctx)) == -1
+    assert b"precision" in lib.alfa_last_error(None)
 
 
 def test_create_rejects_bad_config_without_gpu():
