@@ -220,8 +220,25 @@ def oracle_steps(grid, threads, warmup, steps, budget_s):
     return n, time.perf_counter() - t0
 
 
+def rank_max(x, dist, device=None):
+    """The largest of x over the ranks of the process group (x itself when
+    there is none): the device time of a replicated step is the slowest
+    rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank):
+    """Each rank's replica starts from its own seeded initial fields."""
+    return rank
+
+
 def run_reference(args, rank, world):
-    if rank != 0:
+    if rank != 0:  # the host arm runs once, on rank 0; the other ranks do no work
         return
     threads, model = cpu_info()
     grid = tuple(args.grid)
@@ -259,7 +276,7 @@ def run_alfa(args, rank, world, dist):
     grid = tuple(args.grid)
     n_gp = grid[0] * grid[1] * grid[2]
     total = args.warmup + args.steps + 2
-    u, v, w, th = cases.initial_fields(workload_config(grid, total), rank)
+    u, v, w, th = cases.initial_fields(workload_config(grid, total), replica_seed(rank))
     lib = _lib.load()
     stream = torch.cuda.current_stream(dev)
 
@@ -268,11 +285,7 @@ def run_alfa(args, rank, world, dist):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, dev)
 
     def timed(prec, keep=False):
         """Warm-up (the bootstrap step, the line-pass autotuner, graph
@@ -461,8 +474,10 @@ def run_alfa(args, rank, world, dist):
             "clocks": clk_head, "gpu_launches": launches_head,
             "fp64": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "tensor_core_line_pass": tc,
-            "autotune": [{k: c[k] for k in ("shape", "variant", "ms")} for c in tune_head
-                         if c["chosen"]],
+            # the chosen variant of each pass shape, and the tensor-core
+            # candidate's time beside it (mixed precision)
+            "autotune": [{k: c[k] for k in ("shape", "variant", "ms", "equal", "chosen")}
+                         for c in tune_head if c["chosen"] or c["variant"] == "tensor-core"],
         }), flush=True)
 
 
@@ -610,7 +625,8 @@ def main():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        if args.impl == "alfa":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl" if args.impl == "alfa" else "gloo",
                                 timeout=datetime.timedelta(seconds=120))
     try:

@@ -481,6 +481,13 @@ int alfa_autotune(alfa_ctx*, int reps, alfa_tune_entry* out /* host */, int max_
 int alfa_tc_line_apply(alfa_ctx*, int map, int cut, int n_in, int n_out, double scale,
                        long long ncols, const float* X, float* Y);
 
+/* No counterpart in the reference.  The number of mbarrier polls after which
+ * a wait of the tensor-core line pass (alfa_tc_line_apply, the split-BF16
+ * passes of ALFA_MIXED) gives up; the call then returns ALFA_E_TIMEOUT after
+ * waiting (at the full limit) for the products already issued, so the
+ * context stays usable.  0 restores the default (2^22 polls). */
+int alfa_set_tc_spin_limit(alfa_ctx* ctx, unsigned long long polls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -185,6 +185,8 @@ def load():
     lib.alfa_autotune.restype = I
     lib.alfa_tc_line_apply.argtypes = [CTX, I, I, I, I, D, ctypes.c_longlong, P, P]
     lib.alfa_tc_line_apply.restype = I
+    lib.alfa_set_tc_spin_limit.argtypes = [CTX, ctypes.c_ulonglong]
+    lib.alfa_set_tc_spin_limit.restype = I
     lib.alfa_PlanarMean_noalloc.argtypes = [P, I, I, I, P, c_void_p]
     lib.alfa_PlanarMean_noalloc.restype = I
     lib.alfa_checkpoint_doubles.argtypes = [CTX]

@@ -98,11 +98,14 @@ class Alfa:
 
     TUNE_SHAPES = ("y pad", "x pad", "x unpad", "y unpad", "x derivative", "y derivative",
                    "x filter+derivative", "y filter+derivative")
-    TUNE_VARIANTS = ("default", "compile-time", "radix-8", "radix-4", "ascending")
+    TUNE_VARIANTS = ("default", "compile-time", "radix-8", "radix-4", "ascending",
+                     "tensor-core")
 
     def autotune(self, reps=5):
         """Time every line-pass variant of the step's pass shapes and keep the
-        fastest one whose outputs equal the default's (alfa_autotune).
+        fastest one whose outputs equal the default's (alfa_autotune); for a
+        mixed-precision context the split-BF16 tensor-core pass is a candidate
+        too, at a tolerance of 5e-5 of the output's largest value.
         Returns a list of dicts, one per candidate."""
         cap = 64
         buf = (_lib.AlfaTuneEntry * cap)()

@@ -3,6 +3,7 @@ extension machinery: the library is a plain C-ABI shared object)."""
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -35,47 +36,60 @@ def nvcc():
     return "nvcc"
 
 
-def _stale():
-    if not os.path.exists(LIB):
+OBJ_DIR = os.path.join(ROOT, "_build")
+
+
+def _unit_stale(src, obj):
+    """An object is rebuilt when it is missing or older than its source, any
+    header of the library, this script or the C header."""
+    if not os.path.exists(obj):
         return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps.append(os.path.join(ROOT, "include", "alfa.h"))
+    t = os.path.getmtime(obj)
+    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS]
+    deps += [os.path.join(ROOT, "include", "alfa.h"), os.path.abspath(__file__)]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
 def build(force=False, verbose=False):
-    """Compile every CUDA source into jax_alfa_b200/libalfa.so."""
-    if not force and not _stale():
-        return LIB
+    """Compile every CUDA source into jax_alfa_b200/libalfa.so (objects kept
+    in _build/ so that an edit recompiles only the units it touches)."""
+    os.makedirs(OBJ_DIR, exist_ok=True)
     objs, procs = [], []
     for src, extra, suffix in UNITS:  # translation units compile concurrently
-        obj = os.path.join(CSRC, src.replace(".cu", suffix + ".o"))
+        obj = os.path.join(OBJ_DIR, src.replace(".cu", suffix + ".o"))
+        objs.append(obj)
+        if not force and not _unit_stale(src, obj):
+            continue
         cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        procs.append((src + suffix, subprocess.Popen(cmd, stdout=subprocess.PIPE,
-                                            stderr=subprocess.PIPE, text=True)))
-        objs.append(obj)
+        procs.append((src + suffix, obj, time.time(),
+                      subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                       text=True)))
     failed = []
-    for src, pr in procs:
+    for src, obj, t0, pr in procs:
         _, err = pr.communicate()
         if pr.returncode != 0:
             failed.append(f"nvcc failed on {src}:\n{err}")
-        elif verbose:
+            continue
+        # the object describes the sources as they were when its compile
+        # started: an edit made meanwhile leaves it stale
+        os.utime(obj, (t0, t0))
+        if verbose:
             sys.stderr.write(err)
     if failed:
         raise RuntimeError("\n".join(failed))
+    if not procs and os.path.exists(LIB) and all(
+            os.path.getmtime(o) <= os.path.getmtime(LIB) for o in objs):
+        return LIB  # every object current and already linked
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs,
            "-o", LIB, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
-    for o in objs:
-        os.remove(o)
     return LIB
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build(force="--force" in sys.argv or "--all" in sys.argv, verbose="-v" in sys.argv))

@@ -226,6 +226,12 @@ int alfa_tc_line_apply(alfa_ctx* c, int map, int cut, int n_in, int n_out, doubl
   return DISPATCH(c, tc_line_apply, map, cut, n_in, n_out, scale, ncols, X, Y);
 }
 
+int alfa_set_tc_spin_limit(alfa_ctx* c, unsigned long long polls) {
+  CTX_CHECK(c);
+  DISPATCH(c, ctx_set_tc_spin, polls);
+  return ALFA_OK;
+}
+
 unsigned long long alfa_launch_count(void) { return g_launches.load(); }
 
 }  // extern "C"

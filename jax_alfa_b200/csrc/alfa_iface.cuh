@@ -39,6 +39,7 @@
   int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out);              \
   int tc_line_apply(Ctx* c, int map, int cut, int n_in, int n_out, double scale,              \
                     long long ncols, const float* X, float* Y);                               \
+  void ctx_set_tc_spin(Ctx* c, unsigned long long polls);                                     \
   int ens_create(Ctx* const* members, int n, Ens** out);                                      \
   int ens_step(Ens* E, int nsteps);                                                           \
   int ens_sync(Ens* E);                                                                       \

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <deque>
 #include <map>
 #include <string>
 #include <vector>
@@ -137,7 +138,7 @@ struct Engine {
   double* d_ky = nullptr;   // (nyh) with Nyquist zeroed
   double* d_kr = nullptr;   // (nx) pressure x wavenumbers (Nyquist kept)
   double* d_b_thomas = nullptr;  // (nx, nyh, nz+1)
-  double* d_m_thomas = nullptr;  // (nz, nx, nyh)
+  double* d_m_thomas = nullptr;  // (nx, nyh, nz+1) elimination multipliers, row 0 unused
   double* d_c_p = nullptr;       // (nz+1)
   double* d_rd = nullptr;        // Rayleigh damping profile, full levels (nz)
   double* d_rd_stag = nullptr;   // half levels (nz)
@@ -168,11 +169,16 @@ struct Engine {
   struct TcOp {
     int map, cut, n_in, n_out;
     double scale;
+    int map2, cut2;  // a second map stacked below the first (map2 < 0: none)
+    double scale2;
     void *hi, *lo;
   };
-  std::vector<TcOp> tc_ops;
+  std::deque<TcOp> tc_ops;  // a deque: prepared operators keep their addresses
   int* tc_err = nullptr;
+  unsigned long long tc_spin = 0;  // mbarrier polls of the main loop's waits (0: default)
   static constexpr int N_SCHED = 3;
+  // the tensor-core (split-BF16) variant of a line pass: ALFA_MIXED contexts
+  // only, where the autotuner measured it faster and within its tolerance
   FftPlan alt_plans[4][N_SCHED];  // for nx, ny, mx, my
 
   size_t N() const { return (size_t)nx * ny * nz; }
@@ -202,6 +208,9 @@ void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, dou
 // field has n_out in place of the transformed extent.
 void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
                  int nout, const LineOut* outs);
+// the line-pass variant that runs on the tensor cores (after the default, the
+// compile-time transform and the N_SCHED runtime radix schedules)
+constexpr int TC_VARIANT = 2 + Engine::N_SCHED;
 // the autotuner's key of a line pass
 long long line_key(int axis, int n_in, int n_out, int map, int nout);
 // Y (n_out, ncols) = M X (X: (n_in, ncols) FP32) for the line map's
@@ -212,8 +221,10 @@ int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale
 // the same in parts: the operator (built once, checks the shapes) and one
 // asynchronous launch
 int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, long long ncols,
-               Engine::TcOp** out);
-void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y);
+               Engine::TcOp** out, int map2 = -1, int cut2 = 0, double scale2 = 0.0);
+void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y0,
+               float* Y1, int batch, long long xbs, long long ybs);
+bool tc_shape_ok(int n_in, int n_out, long long ncols);
 // separable spectral operators on real fields
 void op2_filter_deriv(Engine& e, const Loader& L, real* f, real* dx, real* dy,
                       real* scratch2);  // explicit filter and its x/y derivatives

@@ -587,6 +587,36 @@ static const FftPlan& plan_for(const Engine& e, int n) {
   return e.pmy;
 }
 
+#ifdef ALFA_BUILD_FP32
+// The pass as a split-BF16 tensor-core GEMM (alfa_tc.cu) of the stacked
+// operators of its outputs: x lines as one (n_in, Y nz) slab, y lines as X
+// slabs of (n_in, nz).  Only for a plain-field input, outputs that are
+// written (not accumulated) and an operator the autotuner has built already
+// (a step being captured into a graph builds nothing); returns false when the
+// pass does not qualify.
+static bool tc_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
+                    int nout, const LineOut* outs) {
+  if (L.kind != LD_FIELD || nout < 1 || nout > 2) return false;
+  for (int q = 0; q < nout; q++)
+    if (outs[q].accumulate) return false;
+  const long long nz = L.nz;
+  const long long ncols = axis == 0 ? (long long)Y * nz : nz;
+  if (!tc_shape_ok(n_in, n_out, ncols)) return false;
+  const int map2 = nout > 1 ? outs[1].map : -1;
+  const Engine::TcOp* op = nullptr;
+  for (const auto& o : e.tc_ops)
+    if (o.map == outs[0].map && o.cut == outs[0].cut && o.n_in == n_in && o.n_out == n_out &&
+        o.scale == outs[0].scale && o.map2 == map2 &&
+        (map2 < 0 || (o.cut2 == outs[1].cut && o.scale2 == outs[1].scale)))
+      op = &o;
+  if (!op || !e.tc_err) return false;
+  tc_launch(e, op, ncols, L.a[0], outs[0].dst, nout > 1 ? outs[1].dst : nullptr,
+            axis == 0 ? 1 : X, axis == 0 ? 0 : (long long)n_in * nz,
+            axis == 0 ? 0 : (long long)n_out * nz);
+  return true;
+}
+#endif
+
 void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, int n_out,
                  int nout, const LineOut* outs) {
   LineArgs a;
@@ -613,13 +643,16 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
   for (int i = 0; i < nout; i++) a.out[i] = outs[i];
   a.pin = plan_for(e, n_in);
   a.pout = plan_for(e, n_out);
-  ::alfa::note_launch();
   int variant = 0;
   if (!e.line_variant.empty()) {
     auto it = e.line_variant.find(line_key(axis, n_in, n_out, outs[0].map, nout));
     if (it != e.line_variant.end()) variant = it->second;
   }
-  if (variant >= 2) {  // runtime plans with an alternative radix schedule
+#ifdef ALFA_BUILD_FP32
+  if (variant == TC_VARIANT && tc_line(e, axis, L, X, Y, n_in, n_out, nout, outs)) return;
+#endif
+  ::alfa::note_launch();
+  if (variant >= 2 && variant < TC_VARIANT) {  // runtime plans, alternative radix schedule
     const int r = variant - 2;
     a.pin = alt_plan_for(e, n_in, r);
     a.pout = alt_plan_for(e, n_out, r);
@@ -700,9 +733,10 @@ void op2_deriv(Engine& e, const Loader& L, real* dx, int accx, real* dy, int acc
 template <int KIND>
 __global__ void __launch_bounds__(256) k_materialize(Loader L, size_t n, real* __restrict__ out) {
   const int nz = L.nz;
+#pragma unroll 4
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    out[i] = (real)ldv<KIND>(L, i, (int)(i % nz));
+    out[i] = (real)ldv<KIND>(L, i, zof(i, nz));
 }
 
 void materialize(Engine& e, const Loader& L, size_t n, real* out) {

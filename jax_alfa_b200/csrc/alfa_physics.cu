@@ -16,7 +16,12 @@ static inline int nblocks(size_t n, int tpb = TPB) {
   return (int)(b > 148 * 16 ? 148 * 16 : b);
 }
 
-#define GRID_STRIDE(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); \
+// Grid-stride loop over n elements.  (Unrolling it for more loads in flight
+// measured slower for the many-input kernels: their register budgets grew and
+// their occupancy fell; the few-input in-place AB2 batches two elements
+// explicitly instead.)
+#define GRID_STRIDE(i, n) \
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); \
                                i += (size_t)gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------------------
@@ -288,11 +293,11 @@ int surface_flux(Engine& e, int variant, double sfc_val, const SurfaceIO& io,
 __global__ void k_derivz_M(const real* __restrict__ u, const real* __restrict__ v,
                            const real* __restrict__ w, const double* __restrict__ ustar,
                            const double* __restrict__ M, const double* __restrict__ fi,
-                           real* dudz, real* dvdz, real* dwdz, size_t n, int nz,
+                           real* __restrict__ dudz, real* __restrict__ dvdz, real* __restrict__ dwdz, size_t n, int nz,
                            double idz, double Ugal, double den_c) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
-    const size_t r = i / nz;
+    const int z = zof(i, nz);
+    const size_t r = rof(i, nz);
     if (z == 0) {
       const double den = M[r] * 0.4 * 0.5 * den_c;
       dudz[i] = fi[r] * ustar[r] * (u[i] + Ugal) / den;
@@ -316,10 +321,10 @@ void derivz_M(Engine& e, const real* u, const real* v, const real* w, const doub
 
 __global__ void k_derivz_TH(const real* __restrict__ T, const double* __restrict__ ustar,
                             const double* __restrict__ qz, const double* __restrict__ fi,
-                            real* out, size_t n, int nz, double idz, double den) {
+                            real* __restrict__ out, size_t n, int nz, double idz, double den) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
-    const size_t r = i / nz;
+    const int z = zof(i, nz);
+    const size_t r = rof(i, nz);
     if (z == 0) {
       out[i] = fi[r] * (-qz[r] / ustar[r]) / den;
     } else {
@@ -340,18 +345,18 @@ __device__ __forceinline__ double dz_generic(const real* F, size_t i, int z, int
   return (z > 0) ? ((double)F[i] - (double)F[i - 1]) * idz : 0.0;              // Derivz_Generic_uvp
 }
 
-__global__ void k_derivz_generic(const real* __restrict__ F, real* out, size_t n, int nz,
+__global__ void k_derivz_generic(const real* __restrict__ F, real* __restrict__ out, size_t n, int nz,
                                  int w, double idz) {
-  GRID_STRIDE(i, n) { out[i] = dz_generic(F, i, (int)(i % nz), nz, w, idz); }
+  GRID_STRIDE(i, n) { out[i] = dz_generic(F, i, zof(i, nz), nz, w, idz); }
 }
 
 void derivz_generic(Engine& e, const real* F, int w_nodes, real* out) {
   ::alfa::note_launch(); k_derivz_generic<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nz, w_nodes, e.idz);
 }
 
-__global__ void k_div_finish(real* div, const real* __restrict__ f, size_t n, int nz, int w,
+__global__ void k_div_finish(real* __restrict__ div, const real* __restrict__ f, size_t n, int nz, int w,
                              double idz) {
-  GRID_STRIDE(i, n) { div[i] = (double)div[i] + dz_generic(f, i, (int)(i % nz), nz, w, idz); }
+  GRID_STRIDE(i, n) { div[i] = (double)div[i] + dz_generic(f, i, zof(i, nz), nz, w, idz); }
 }
 
 void divergence_finish(Engine& e, real* div, const real* fz, int w_nodes) {
@@ -367,10 +372,10 @@ __device__ __forceinline__ double thv_of(const real* __restrict__ TH,
 }
 
 __global__ void k_buoy(const real* __restrict__ TH, const real* __restrict__ H,
-                       const double* __restrict__ bar, real* out, size_t n, int nz, double T0,
+                       const double* __restrict__ bar, real* __restrict__ out, size_t n, int nz, double T0,
                        int by_mean, double hg) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     if (z == 0) {
       out[i] = 0.0;
     } else {
@@ -384,7 +389,7 @@ __global__ void k_buoy(const real* __restrict__ TH, const real* __restrict__ H,
 }
 
 __global__ void k_thv(const real* __restrict__ TH, const real* __restrict__ H, double T0,
-                      real* out, size_t n) {
+                      real* __restrict__ out, size_t n) {
   GRID_STRIDE(i, n) { out[i] = thv_of(TH, H, i, T0); }
 }
 
@@ -441,11 +446,12 @@ __device__ __forceinline__ double smag_of(double s11, double s22, double s33, do
                      2.0 * (s13 * s13) + 2.0 * (s23 * s23)));
 }
 
-__global__ void k_strains_uvp(G9 G, real* S12, real* S13, real* S23, real* S, size_t n,
+__global__ void k_strains_uvp(G9 G, real* __restrict__ S12, real* __restrict__ S13,
+                              real* __restrict__ S23, real* __restrict__ S, size_t n,
                               int nz) {
   // g: dudx dvdx dwdx dudy dvdy dwdy dudz dvdz dwdz
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     const real* const* g = G.g;
     double uz, vz, wx, wy;
     if (z == 0) {
@@ -481,9 +487,9 @@ void strains_uvp(Engine& e, const real* const g[9], real* S12, real* S13, real* 
   ::alfa::note_launch(); k_strains_uvp<<<nblocks(e.N()), TPB, 0, e.stream>>>(G, S12, S13, S23, S, e.N(), e.nz);
 }
 
-__global__ void k_smag_w(G9 G, real* Sw, size_t n, int nz) {
+__global__ void k_smag_w(G9 G, real* __restrict__ Sw, size_t n, int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     const real* const* g = G.g;
     auto stag = [&](const real* d) -> double {
       if (z == 0) return d[i];
@@ -510,7 +516,7 @@ struct P6 {
   const real* s[6];
 };
 
-__global__ void k_smag6(P6 P, real* out, size_t n) {
+__global__ void k_smag6(P6 P, real* __restrict__ out, size_t n) {
   GRID_STRIDE(i, n) {
     out[i] = smag_of(P.s[0][i], P.s[1][i], P.s[2][i], P.s[3][i], P.s[4][i], P.s[5][i]);
   }
@@ -525,9 +531,9 @@ void smag6(Engine& e, const real* const s[6], size_t n, real* out) {
 void smag6_n(Engine& e, const real* const s[6], real* out) { smag6(e, s, e.N(), out); }
 
 // w_ of DynamicSGS_LASDD_SM.py:180-183
-__global__ void k_wstar(const real* __restrict__ w, real* out, size_t n, int nz) {
+__global__ void k_wstar(const real* __restrict__ w, real* __restrict__ out, size_t n, int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     if (z == 0) out[i] = 0.5 * (double)w[i + 1];
     else if (z == nz - 1) out[i] = w[i - 1];
     else out[i] = 0.5 * ((double)w[i] + (double)w[i + 1]);
@@ -749,10 +755,10 @@ __global__ void k_ones(double* p, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 1.0;
 }
 
-__global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ beta, real* LM,
-                        real* MM, size_t n, int nz) {
+__global__ void k_LM_MM(LasddFields f, LasddConst c, const double* __restrict__ beta,
+                        real* __restrict__ LM, real* __restrict__ MM, size_t n, int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     double Lm[6], Mm[6];
     leonard(f.ph, f.hat, i, Lm);
     const double b = beta[z];
@@ -841,9 +847,9 @@ void wl_poly(Engine& e, const double* sums4, double* coeffs6) {
 }
 
 __global__ void k_LM_MM_wl(LasddFields f, double T1, double T2, const double* __restrict__ beta,
-                           real* LM, real* MM, size_t n, int nz) {
+                           real* __restrict__ LM, real* __restrict__ MM, size_t n, int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     double Lm[6], Mm[6];
     leonard(f.ph, f.hat, i, Lm);
     const double b = beta[z];
@@ -911,10 +917,11 @@ void scalar_lasdd_wl_sums(Engine& e, const ScalarLasddFields& f, double* sums4) 
 }
 
 __global__ void k_slwl_TupTdn(ScalarLasddFields f, double L43, double L83, WLPow P,
-                              const double* __restrict__ beta, real* Tup, real* Tdn, size_t n,
+                              const double* __restrict__ beta, real* __restrict__ Tup,
+                              real* __restrict__ Tdn, size_t n,
                               int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     const WLScalarTerms t = wl_scalar_terms(f, i);
     const double b = beta[z];
     Tup[i] = L43 * (t.a6 - P.p43 * b * t.b6);
@@ -1142,11 +1149,11 @@ __device__ __forceinline__ double box9(const real* F, int x, int y, int z, int n
 }
 
 __global__ void k_clip_ratio(const real* __restrict__ num, const real* __restrict__ den,
-                             real* out, size_t n, int nx, int ny, int nz) {
+                             real* __restrict__ out, size_t n, int nx, int ny, int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
-    const size_t r = i / nz;
-    const int y = (int)(r % ny), x = (int)(r / ny);
+    const int z = zof(i, nz);
+    const size_t r = rof(i, nz);
+    const int y = zof(r, ny), x = (int)rof(r, ny);
     const double nf = box9(num, x, y, z, nx, ny, nz);
     const double df = box9(den, x, y, z, nx, ny, nz);
     const double q = nf / df;
@@ -1159,12 +1166,12 @@ void clip_ratio(Engine& e, const real* num, const real* den, real* out) {
   ::alfa::note_launch(); k_clip_ratio<<<nblocks(e.N()), TPB, 0, e.stream>>>(num, den, out, e.N(), e.nx, e.ny, e.nz);
 }
 
-__global__ void k_imfilter(const real* __restrict__ F, real* out, size_t n, int nx, int ny,
+__global__ void k_imfilter(const real* __restrict__ F, real* __restrict__ out, size_t n, int nx, int ny,
                            int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
-    const size_t r = i / nz;
-    out[i] = box9(F, (int)(r / ny), (int)(r % ny), z, nx, ny, nz);
+    const int z = zof(i, nz);
+    const size_t r = rof(i, nz);
+    out[i] = box9(F, (int)rof(r, ny), zof(r, ny), z, nx, ny, nz);
   }
 }
 
@@ -1285,9 +1292,9 @@ void scalar_lasdd_sums(Engine& e, const ScalarLasddFields& f, double* sums10) {
 }
 
 __global__ void k_sl_TupTdn(ScalarLasddFields f, SLConst c, const double* __restrict__ beta,
-                            real* Tup, real* Tdn, size_t n, int nz) {
+                            real* __restrict__ Tup, real* __restrict__ Tdn, size_t n, int nz) {
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     const SLTerms t = sl_terms(f.uTh, f.hat, f.Th, f.SGh, f.Gh, f.S_hat, i);
     const double b = beta[z];
     Tup[i] = c.cL2 * t.a + c.cb2 * t.b * b;
@@ -1305,7 +1312,8 @@ void scalar_Tup_Tdn(Engine& e, const ScalarLasddFields& f, const double* beta, r
 // ---------------------------------------------------------------------------
 __global__ void k_wall(const real* __restrict__ u, const real* __restrict__ v,
                        const double* __restrict__ M, const double* __restrict__ pm,
-                       const double* __restrict__ pm0, real* txz, real* tyz, size_t H, int nz,
+                       const double* __restrict__ pm0, real* __restrict__ txz,
+                       real* __restrict__ tyz, size_t H, int nz,
                        double log_m, double Ugal) {
   GRID_STRIDE(r, H) {
     const double denom = log_m + pm[r] - pm0[r];
@@ -1323,7 +1331,7 @@ void wall_override(Engine& e, const real* u, const real* v, const double* M,
                                                 log_m, e.cfg.Ugal);
 }
 
-__global__ void k_set_plane0(const double* __restrict__ p, real* f, size_t H, int nz) {
+__global__ void k_set_plane0(const double* __restrict__ p, real* __restrict__ f, size_t H, int nz) {
   GRID_STRIDE(r, H) { f[r * nz] = p[r]; }
 }
 
@@ -1350,8 +1358,11 @@ struct RhsM {
 
 __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
   const size_t grow = a.gtp ? (size_t)(*a.gtp - 1) * a.grs : 0;
+  real* __restrict__ Ru = a.Ru;
+  real* __restrict__ Rv = a.Rv;
+  real* __restrict__ Rw = a.Rw;
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     double ru = -(double)a.Cx[i] - (double)a.dx[i] - a.f * (a.Vg[grow + z] - (double)a.v[i]);
     double rv = -(double)a.Cy[i] - (double)a.dy[i] + a.f * (a.Ug[grow + z] - a.Ugal - (double)a.u[i]);
     double rw = -(double)a.Cz[i] - (double)a.dz[i] + (double)a.b[i];
@@ -1365,9 +1376,9 @@ __global__ void k_rhs_m(RhsM a, size_t n, int nz) {
       rv = rv - a.rds[z] * ((double)a.v[i] - a.vbar[z]);
       rw = rw - a.rd[z] * (double)a.w[i];
     }
-    a.Ru[i] = ru;
-    a.Rv[i] = rv;
-    a.Rw[i] = rw;
+    Ru[i] = ru;
+    Rv[i] = rv;
+    Rw[i] = rw;
   }
 }
 
@@ -1385,11 +1396,12 @@ void rhs_momentum(Engine& e, const real* u, const real* v, const real* w,
 
 __global__ void k_rhs_s(const real* __restrict__ TH, const real* __restrict__ adv,
                         const real* __restrict__ dq, const double* __restrict__ THadv,
-                        const double* __restrict__ bar, const double* __restrict__ rds, real* R,
+                        const double* __restrict__ bar, const double* __restrict__ rds,
+                        real* __restrict__ R,
                         size_t n, int nz, int doadv, int damp, const int* itp, long long rs) {
   const size_t row = (doadv && itp) ? (size_t)(*itp - 1) * rs : 0;
   GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
+    const int z = zof(i, nz);
     double r = -(double)adv[i] - (double)dq[i];
     if (doadv) r = r + THadv[row + z];
     if (damp) r = r - rds[z] * ((double)TH[i] - bar[z]);
@@ -1412,13 +1424,14 @@ void rhs_scalar(Engine& e, const real* TH, const real* adv, const real* divq,
 // ---------------------------------------------------------------------------
 __global__ void k_rc(const cd* __restrict__ fRx, const cd* __restrict__ fRy,
                      const cd* __restrict__ fRz, const cd* __restrict__ fb2,
-                     const double* __restrict__ kr, double* RCr, double* RCi, double* fRzr,
+                     const double* __restrict__ kr, double* __restrict__ RCr,
+                     double* __restrict__ RCi, double* __restrict__ fRzr,
                      int nx, int nyh, int nz, double dz) {
   const size_t n = (size_t)nx * nyh * (nz + 1);
   GRID_STRIDE(t, n) {
-    const int k = (int)(t % (nz + 1));
-    const size_t m = t / (nz + 1);  // mode (i, j)
-    const int j = (int)(m % nyh), i = (int)(m / nyh);
+    const int k = zof(t, nz + 1);
+    const size_t m = rof(t, nz + 1);  // mode (i, j)
+    const int j = zof(m, nyh), i = (int)rof(m, nyh);
     if (k == 0) {
       const cd f = fb2[m * 2 + 0];
       RCr[t] = -dz * f.x;
@@ -1448,17 +1461,31 @@ void pressure_rc(Engine& e, const cd* fRx, const cd* fRy, const cd* fRz, const c
 }
 
 // Forward elimination and back substitution per mode with the factors of
-// engine_init.  The forward sweep's modified right-hand side is kept in dm
-// (FP64): in the FP64 build dm is the output spectrum itself (overwritten in
-// the back substitution, element by element after it is read), in the FP32
-// build a separate FP64 buffer, so the whole solve runs in FP64.
-__global__ void k_thomas(const double* __restrict__ RCr, const double* __restrict__ RCi,
-                         const double* __restrict__ fRzr, const double* __restrict__ bt,
-                         const double* __restrict__ mt, const double* __restrict__ cp, cd* fp,
-                         double2* dm_all, int nx, int nyh, int nz, double dz) {
+// engine_init, in the reference's order (NSE_PressureTerms_Thomas.py:99-143):
+// the solution depends on the order of its operations at ~1e-8 relative in
+// the low-wavenumber modes (condition ~(2/dz^2)/k^2), so the recurrences stay
+// sequential per mode.  What limited the kernel was memory latency (one
+// thread per mode, ~7 warps per SM at 256^3, every row's load waiting on the
+// previous row's arithmetic): each thread now issues the loads of RB rows
+// (RC, the multipliers and diagonals, all stored mode major, contiguous per
+// thread) before it runs them, so RB rows of every thread are in flight.
+// The forward sweep's modified right-hand side goes to dm (FP64): the output
+// spectrum itself in the FP64 build (each element read before it is
+// overwritten), a separate FP64 buffer in the FP32 build.
+static constexpr int RB = 8;
+
+__global__ void __launch_bounds__(64) k_thomas(const double* __restrict__ RCr,
+                                               const double* __restrict__ RCi,
+                                               const double* __restrict__ fRzr,
+                                               const double* __restrict__ bt,
+                                               const double* __restrict__ mt,
+                                               const double* __restrict__ cp, cd* fp,
+                                               double2* dm_all, int nx, int nyh, int nz,
+                                               double dz) {
   const size_t nm = (size_t)nx * nyh;
-  GRID_STRIDE(m, nm) {
-    const int j = (int)(m % nyh), i = (int)(m / nyh);
+  for (size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x; m < nm;
+       m += (size_t)gridDim.x * blockDim.x) {
+    const int j = zof(m, nyh), i = (int)rof(m, nyh);
     const size_t base = m * (nz + 1);
     cd* out = fp + m * nz;
     double2* dm = dm_all + m * nz;
@@ -1477,23 +1504,53 @@ __global__ void k_thomas(const double* __restrict__ RCr, const double* __restric
       for (int k = 0; k < nz; k++) out[k] = mkc(0, 0);
       continue;
     }
-    // forward sweep (d_mod stored in dm[k-1] for k >= 1)
+    // forward sweep (d_mod of row k in dm[k-1] for k >= 1)
     double dr = RCr[base], di = RCi[base];
-    for (int k = 1; k <= nz; k++) {
-      const double mk = mt[(size_t)(k - 1) * nm + m];
-      dr = RCr[base + k] - mk * dr;
-      di = RCi[base + k] - mk * di;
-      dm[k - 1] = make_double2(dr, di);
+    for (int k0 = 1; k0 <= nz; k0 += RB) {
+      double rr[RB], ri[RB], mk[RB];
+#pragma unroll
+      for (int t = 0; t < RB; t++) {
+        const int k = k0 + t;
+        if (k <= nz) {
+          rr[t] = __ldg(RCr + base + k);
+          ri[t] = __ldg(RCi + base + k);
+          mk[t] = __ldg(mt + base + k);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < RB; t++) {
+        const int k = k0 + t;
+        if (k <= nz) {
+          dr = rr[t] - mk[t] * dr;
+          di = ri[t] - mk[t] * di;
+          dm[k - 1] = make_double2(dr, di);
+        }
+      }
     }
     // back substitution, x[k] for k = nz .. 1 (x[0] is not used)
     double xr = dr / bt[base + nz], xi = di / bt[base + nz];
     out[nz - 1] = mkc(xr, xi);
-    for (int k = nz - 1; k >= 1; k--) {
-      const double2 d = dm[k - 1];
-      const double b = bt[base + k], c = cp[k];
-      xr = (d.x - c * xr) / b;
-      xi = (d.y - c * xi) / b;
-      out[k - 1] = mkc(xr, xi);
+    for (int k1 = nz - 1; k1 >= 1; k1 -= RB) {
+      double2 d[RB];
+      double b[RB], c[RB];
+#pragma unroll
+      for (int t = 0; t < RB; t++) {
+        const int k = k1 - t;
+        if (k >= 1) {
+          d[t] = dm[k - 1];
+          b[t] = __ldg(bt + base + k);
+          c[t] = __ldg(cp + k);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < RB; t++) {
+        const int k = k1 - t;
+        if (k >= 1) {
+          xr = (d[t].x - c[t] * xr) / b[t];
+          xi = (d[t].y - c[t] * xi) / b[t];
+          out[k - 1] = mkc(xr, xi);
+        }
+      }
     }
   }
 }
@@ -1505,12 +1562,14 @@ void thomas_solve(Engine& e, const double* RCr, const double* RCi, const double*
 #else
   double2* dm = fp;
 #endif
-  ::alfa::note_launch(); k_thomas<<<(int)((nm + 127) / 128), 128, 0, e.stream>>>(RCr, RCi, fRz_real, e.d_b_thomas,
-                                                          e.d_m_thomas, e.d_c_p, fp, dm, e.nx, e.nyh,
-                                                          e.nz, e.dz);
+  ::alfa::note_launch();
+  k_thomas<<<(unsigned)((nm + 63) / 64), 64, 0, e.stream>>>(RCr, RCi, fRz_real, e.d_b_thomas,
+                                                            e.d_m_thomas, e.d_c_p, fp, dm, e.nx,
+                                                            e.nyh, e.nz, e.dz);
 }
 
-__global__ void k_sub3(real* a, real* b, real* c, const real* __restrict__ x,
+__global__ void k_sub3(real* __restrict__ a, real* __restrict__ b, real* __restrict__ c,
+                       const real* __restrict__ x,
                        const real* __restrict__ y, const real* __restrict__ z, size_t n) {
   GRID_STRIDE(i, n) {
     a[i] = a[i] - x[i];
@@ -1530,17 +1589,31 @@ void subtract3(Engine& e, real* Ru, real* Rv, real* Rw, const real* a, const rea
 // ---------------------------------------------------------------------------
 __global__ void k_ab2(const real* u, const real* __restrict__ R, const real* __restrict__ Rp,
                       real* un, size_t n, int nz, double dt, int mode, double top_add) {
-  // mode 0: u/v (top copies nz-2), 1: w (top and bottom 0), 2: TH (top = nz-2 + c)
-  GRID_STRIDE(i, n) {
-    const int z = (int)(i % nz);
-    if (z == nz - 1) continue;
-    const double val = (double)u[i] + dt * (1.5 * (double)R[i] - 0.5 * (double)Rp[i]);
-    if (mode == 1) {
-      un[i] = (z == 0) ? 0.0 : val;
-      if (z == nz - 2) un[i + 1] = 0.0;
-    } else {
-      un[i] = val;
-      if (z == nz - 2) un[i + 1] = (mode == 2) ? val + top_add : val;
+  // mode 0: u/v (top copies nz-2), 1: w (top and bottom 0), 2: TH (top = nz-2 + c).
+  // u and un may be the same field (the step advances in place), so the two
+  // elements a thread takes per iteration are loaded explicitly before either
+  // is stored; no element reads what another writes (level nz-1 is only
+  // written, by the thread of level nz-2).
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i0 < n; i0 += 2 * stride) {
+    const size_t i1 = i0 + stride;
+    const int z0 = zof(i0, nz), z1 = i1 < n ? zof(i1, nz) : nz - 1;
+    double v0 = 0.0, v1 = 0.0;
+    if (z0 != nz - 1) v0 = (double)u[i0] + dt * (1.5 * (double)R[i0] - 0.5 * (double)Rp[i0]);
+    if (z1 != nz - 1) v1 = (double)u[i1] + dt * (1.5 * (double)R[i1] - 0.5 * (double)Rp[i1]);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const size_t i = q ? i1 : i0;
+      const int z = q ? z1 : z0;
+      const double val = q ? v1 : v0;
+      if (z == nz - 1) continue;
+      if (mode == 1) {
+        un[i] = (z == 0) ? 0.0 : val;
+        if (z == nz - 2) un[i + 1] = 0.0;
+      } else {
+        un[i] = val;
+        if (z == nz - 2) un[i + 1] = (mode == 2) ? val + top_add : val;
+      }
     }
   }
 }
@@ -1563,15 +1636,21 @@ void ab2_q(Engine& e, const real* Q, const real* R, const real* Rp, real* out) {
                                                e.q_inversion_nondim * e.dz);
 }
 
-// max |u|, |v|, |w| (Main.py:534-537)
+// max |u|, |v|, |w| (Main.py:534-537).  The maximum propagates NaN (as the
+// reference's jnp.max does; fmax would drop it), so a non-finite state shows
+// in the CFL number that alfa_get_diag checks.
+__device__ __forceinline__ double nanmax(double m, double a) {
+  return (a > m || a != a) ? a : m;
+}
+
 __global__ void k_absmax_partial(const real* __restrict__ a, const real* __restrict__ b,
                                  const real* __restrict__ c, size_t n, double* part) {
   __shared__ double sh[3][256];
   double m0 = 0.0, m1 = 0.0, m2 = 0.0;
   GRID_STRIDE(i, n) {
-    m0 = fmax(m0, fabs((double)a[i]));
-    m1 = fmax(m1, fabs((double)b[i]));
-    m2 = fmax(m2, fabs((double)c[i]));
+    m0 = nanmax(m0, fabs((double)a[i]));
+    m1 = nanmax(m1, fabs((double)b[i]));
+    m2 = nanmax(m2, fabs((double)c[i]));
   }
   sh[0][threadIdx.x] = m0;
   sh[1][threadIdx.x] = m1;
@@ -1579,7 +1658,7 @@ __global__ void k_absmax_partial(const real* __restrict__ a, const real* __restr
   __syncthreads();
   for (int s = blockDim.x / 2; s > 0; s >>= 1) {
     if (threadIdx.x < s)
-      for (int q = 0; q < 3; q++) sh[q][threadIdx.x] = fmax(sh[q][threadIdx.x], sh[q][threadIdx.x + s]);
+      for (int q = 0; q < 3; q++) sh[q][threadIdx.x] = nanmax(sh[q][threadIdx.x], sh[q][threadIdx.x + s]);
     __syncthreads();
   }
   if (threadIdx.x == 0)
@@ -1589,19 +1668,19 @@ __global__ void k_absmax_partial(const real* __restrict__ a, const real* __restr
 __global__ void k_absmax_finish(const double* part, int nb, double* out) {
   if (threadIdx.x < 3) {
     double m = 0.0;
-    for (int b = 0; b < nb; b++) m = fmax(m, part[b * 3 + threadIdx.x]);
+    for (int b = 0; b < nb; b++) m = nanmax(m, part[b * 3 + threadIdx.x]);
     out[threadIdx.x] = m;
   }
 }
 
 void cfl_max(Engine& e, const real* u, const real* v, const real* w, double* out3) {
-  const int nb = 256;
+  const int nb = 4 * e.sms < 1024 ? 4 * e.sms : 1024;  // e.red holds >= 3 x 1024 partials
   ::alfa::note_launch(); k_absmax_partial<<<nb, 256, 0, e.stream>>>(u, v, w, e.N(), e.red);
   ::alfa::note_launch(); k_absmax_finish<<<1, 32, 0, e.stream>>>(e.red, nb, out3);
 }
 
 // copy z-planes k0 and k1 of F into a (nx, ny, 2) field
-__global__ void k_planes(const real* __restrict__ F, int k0, int k1, real* out, size_t H,
+__global__ void k_planes(const real* __restrict__ F, int k0, int k1, real* __restrict__ out, size_t H,
                          int nz) {
   GRID_STRIDE(r, H) {
     out[r * 2 + 0] = F[r * nz + k0];

@@ -30,5 +30,16 @@ typedef double2 cd;
 __host__ __device__ __forceinline__ cd mkc(real x, real y) { return make_double2(x, y); }
 #endif
 
+// Level and row of linear index i of a field whose fastest extent is n:
+// 32-bit unsigned division (engine_init keeps every padded field below 2^32
+// elements; a 64-bit division costs ~10x the instructions of the kernels'
+// memory traffic per element).
+__host__ __device__ __forceinline__ int zof(size_t i, int n) {
+  return (int)((unsigned)i % (unsigned)n);
+}
+__host__ __device__ __forceinline__ size_t rof(size_t i, int n) {
+  return (size_t)((unsigned)i / (unsigned)n);
+}
+
 }  // namespace ALFA_PREC
 }  // namespace alfa

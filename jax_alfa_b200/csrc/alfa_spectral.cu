@@ -343,8 +343,10 @@ __device__ __forceinline__ cd map_value(const XArgs& a, const XOut& o, const cd*
 }
 
 // NI / NO: compile-time forward / inverse lengths (0: runtime plans)
+// two resident CTAs per SM at least (the register budget of the FP32
+// build's 256-thread tiles would otherwise leave one)
 template <int C, int NI, int NO>
-__global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 1) k_x(XArgs a) {
+__global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 2) k_x(XArgs a) {
   constexpr int NT = tile_threads<C, (NI > NO ? NI : NO)>();
   extern __shared__ cd sm[];
   const int nz = a.nz;

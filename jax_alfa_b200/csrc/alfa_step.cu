@@ -110,6 +110,9 @@ int engine_init(Engine& e, const alfa_config& c) {
   e.my = (int)(1.5 * c.ny);
   if (c.ny > 512 || c.nx > 1024)
     return e.fail("grid too large for the FFT tiles (ny <= 512, nx <= 1024)", ALFA_E_CONFIG);
+  if ((size_t)e.mx * (size_t)e.my * (size_t)(c.nz + 1) >= ((size_t)1 << 32))
+    return e.fail("grid too large: 1.5 nx x 1.5 ny x (nz + 1) must stay below 2^32 points",
+                  ALFA_E_CONFIG);
   e.nxh = c.nx / 2 + 1;
   e.nyh = c.ny / 2 + 1;
   e.mxh = e.mx / 2 + 1;
@@ -188,7 +191,7 @@ int engine_init(Engine& e, const alfa_config& c) {
   cc[0] = 1;
   cc[nz] = 0;
   const size_t nm = (size_t)c.nx * e.nyh;
-  std::vector<double> bt(nm * N1), mt((size_t)nz * nm);
+  std::vector<double> bt(nm * N1), mt(nm * N1, 0.0);  // both (nx, nyh, nz+1)
   for (int i = 0; i < c.nx; i++) {
     for (int j = 0; j < e.nyh; j++) {
       const size_t m = (size_t)i * e.nyh + j;
@@ -202,7 +205,7 @@ int engine_init(Engine& e, const alfa_config& c) {
         for (int k = 1; k < nz; k++) b[k] = -(1.0 + 2.0 / (dz * dz));
       for (int k = 1; k < N1; k++) {
         const double mk = a[k] / b[k - 1];
-        mt[(size_t)(k - 1) * nm + m] = mk;
+        mt[m * N1 + k] = mk;
         b[k] = b[k] - mk * cc[k - 1];
       }
     }
@@ -1282,7 +1285,16 @@ int get_diag(Ctx* c, alfa_diag* o) {
   cudaMemcpyAsync(&q, W.d_qavg, 8, cudaMemcpyDeviceToHost, e.stream);
   std::vector<double> us(e.H());
   cudaMemcpyAsync(us.data(), W.ustar, e.H() * 8, cudaMemcpyDeviceToHost, e.stream);
+  int tc_flag = 0;  // a bounded wait of a tensor-core line pass gave up
+  if (e.tc_err) {
+    cudaMemcpyAsync(&tc_flag, e.tc_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
+    cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
+  }
   if (cudaStreamSynchronize(e.stream) != cudaSuccess) return e.fail("diag sync failed", ALFA_E_CUDA);
+  if (tc_flag)
+    return e.fail("a bounded tensor-core wait of a line pass gave up; the step's fields are "
+                  "not valid",
+                  ALFA_E_TIMEOUT);
   const double cfl = std::max(std::max(m[0] * e.dt_nondim / e.dx, m[1] * e.dt_nondim / e.dy),
                               m[2] * e.dt_nondim / e.dz);
   W.CFL = cfl;
@@ -1456,7 +1468,7 @@ int time_kernel(Ctx* c, int which, int reps, double* ms, double* bytes) {
       case 6: launch_x(e, e.T[0], 0, e.nx, e.nyh, e.pnx, 2, o, e.nyh); break;
       case 8:  // FP32 in and out in two padded-field buffers (P values each)
         tc_launch(e, tcop, tc_cols, reinterpret_cast<const float*>(W.Pb[6]),
-                  reinterpret_cast<float*>(W.Pb[7]));
+                  reinterpret_cast<float*>(W.Pb[7]), nullptr, 1, 0, 0);
         break;
       default: launch_y_inv(e, e.T[1], e.nx, e.nyh, e.pny, 1.0, e.W, 0); break;
     }
@@ -1533,8 +1545,11 @@ __global__ void k_maxdiff(const real* __restrict__ a, const real* __restrict__ b
 }
 
 // A variant is a candidate only if its outputs equal the default's to the
-// round-off of the build's precision (relative to the output's largest value).
+// round-off of the build's precision (relative to the output's largest value);
+// the split-BF16 tensor-core variant (hi/lo operand pairs, three products,
+// about 2^-16 relative per operator entry) to its own accuracy.
 static constexpr double kTuneTol = sizeof(real) == 8 ? 1e-12 : 1e-5;
+static constexpr double kTcTuneTol = 5e-5;
 
 int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
   Engine& e = c->e;
@@ -1594,11 +1609,26 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
     for (int q = 0; q < sh.nout; q++)
       cudaMemcpyAsync(ref[q], sh.dst[q], sh.len * sizeof(real), cudaMemcpyDeviceToDevice,
                       e.stream);
+    std::vector<int> cand;
+    for (int v = 0; v < 2 + Engine::N_SCHED; v++)
+      if (v != 1 || phase) cand.push_back(v);
+#ifdef ALFA_BUILD_FP32
+    if (e.cfg.precision == ALFA_MIXED) {  // operators are built here, never inside a capture
+      const long long ncols = sh.axis == 0 ? (long long)sh.Y * e.nz : (long long)e.nz;
+      Engine::TcOp* op = nullptr;
+      if (tc_shape_ok(sh.n_in, sh.n_out, ncols)) {
+        if ((rc = tc_prepare(e, sh.map[0], sh.cut, sh.n_in, sh.n_out, sh.scale, ncols, &op,
+                             sh.nout > 1 ? sh.map[1] : -1, sh.cut, sh.scale)) != ALFA_OK)
+          break;
+        cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
+        cand.push_back(TC_VARIANT);
+      }
+    }
+#endif
     int best = -1;
     double best_ms = 0.0;
     const int first = n;
-    for (int v = 0; v < 2 + Engine::N_SCHED; v++) {
-      if (v == 1 && !phase) continue;
+    for (int v : cand) {
       e.line_variant[key] = v;
       run();
       bool same = true;
@@ -1611,7 +1641,7 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
         double dd, mm;
         std::memcpy(&dd, &h[0], 8);
         std::memcpy(&mm, &h[1], 8);
-        if (!(dd <= kTuneTol * mm)) same = false;
+        if (!(dd <= (v == TC_VARIANT ? kTcTuneTol : kTuneTol) * mm)) same = false;
       }
       run();  // warm
       cudaEventRecord(ea, e.stream);
@@ -1638,6 +1668,16 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
         te.ms = ms;
       }
       n++;
+    }
+    if (e.tc_err) {  // a tensor-core candidate whose wait gave up is not chosen
+      int h = 0;
+      cudaMemcpyAsync(&h, e.tc_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
+      cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
+      cudaStreamSynchronize(e.stream);
+      if (h && best == TC_VARIANT) best = -1;
+      if (h)
+        for (int i = first; i < n && i < max_out; i++)
+          if (out[i].variant == TC_VARIANT) out[i].equal = 0;
     }
     if (best < 0) best = 0;
     e.line_variant[key] = best;
@@ -1914,6 +1954,8 @@ void ctx_derived(const Ctx* c, alfa_derived* o) {
     o->cut_level2[i] = e.cut_2[i];
   }
 }
+
+void ctx_set_tc_spin(Ctx* c, unsigned long long polls) { c->e.tc_spin = polls; }
 
 int tc_line_apply(Ctx* c, int map, int cut, int n_in, int n_out, double scale, long long ncols,
                   const float* X, float* Y) {

@@ -51,7 +51,12 @@ constexpr int TROW = EH + 4;   // epilogue tile row stride (floats): conflict-fr
 constexpr int EPI = BM * TROW * 4;  // epilogue tile bytes (reuses the stages)
 constexpr int BARS = (EPI > 2 * STAGE ? EPI : 2 * STAGE);  // barriers after both
 constexpr int SMEM = BARS + 64;
-constexpr unsigned long long SPIN_LIMIT = 1ull << 22;  // mbarrier polls before giving up
+// mbarrier polls before a wait gives up (the default of the main loop's
+// waits; a context can lower it, alfa_set_tc_spin_limit)
+constexpr unsigned long long SPIN_LIMIT = 1ull << 22;
+// after a wait gave up, the waits for the products still in flight, each of
+// SPIN_LIMIT polls, before the accumulator is freed regardless
+constexpr int CLEANUP_WAITS = 16;
 constexpr int A_UNITS = BM * (BK / 8) / NT;  // 16-byte operator units per thread and chunk
 static_assert(NT == 256 && BN == 2 * 4 * 32 && BK / 8 == 4 && BN == 2 * EH,
               "input staging: warp w takes K block w % 4 and column half w / 4, 32 threads x "
@@ -94,17 +99,33 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t 
       "l"(da), "l"(db), "r"(IDESC), "r"(acc));
 }
 
-// false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (unsigned long long i = 0; i < SPIN_LIMIT; i++) {
+// false when the limit ran out.  try_wait may suspend the thread for a
+// while inside one poll, so a small limit (a test's) polls with the
+// non-blocking test_wait instead and gives up as soon as its polls find the
+// phase incomplete.
+constexpr unsigned long long SMALL_LIMIT = 64;
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          unsigned long long limit) {
+  for (unsigned long long i = 0; i < limit; i++) {
     uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
+    if (limit <= SMALL_LIMIT) {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\t"
+          "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t}\n"
+          : "=r"(done)
+          : "r"(bar), "r"(parity)
+          : "memory");
+    } else {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t}\n"
+          : "=r"(done)
+          : "r"(bar), "r"(parity)
+          : "memory");
+    }
     if (done) return true;
   }
   return false;
@@ -207,8 +228,14 @@ __device__ __forceinline__ void mma_chunk(uint32_t tmem, const unsigned char* st
 // (the barrier of that stage) have completed.
 __global__ void __launch_bounds__(NT, 2)
     k_line_gemm_bf16x3(const __nv_bfloat16* __restrict__ Mhi, const __nv_bfloat16* __restrict__ Mlo,
-                       const float* __restrict__ X, float* __restrict__ Y, int n_in, long long ncols,
-                       int* err) {
+                       const float* __restrict__ X, float* __restrict__ Y0, float* __restrict__ Y1,
+                       int split, int n_in, long long ncols, long long xbs, long long ybs,
+                       int* err, unsigned long long spin) {
+  // batch blockIdx.z: the slab of lines at X + z xbs; output rows below
+  // `split` go to Y0, the others to Y1 (two stacked maps), both + z ybs
+  X += (size_t)blockIdx.z * xbs;
+  Y0 += (size_t)blockIdx.z * ybs;
+  Y1 += (size_t)blockIdx.z * ybs;
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* stages[2] = {sm, sm + STAGE};
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + BARS);  // bar[0], bar[1]
@@ -249,7 +276,7 @@ __global__ void __launch_bounds__(NT, 2)
     const int s = ch & 1;
     bool mine = true;
     if (ch >= 2) {  // stage s still feeds the products of chunk ch - 2
-      mine = mbar_wait(smem_u32(bar + s), (uint32_t)(((ch - 2) >> 1) & 1));
+      mine = mbar_wait(smem_u32(bar + s), (uint32_t)(((ch - 2) >> 1) & 1), spin);
       asm volatile("tcgen05.fence::after_thread_sync;");
     }
     store_chunk(R, stages[s], tid);
@@ -269,16 +296,23 @@ __global__ void __launch_bounds__(NT, 2)
   }
   if (ok) {  // the last commit covers every product issued before it
     const int L = nchunks - 1;
-    const bool mine = mbar_wait(smem_u32(bar + (L & 1)), (uint32_t)((L >> 1) & 1));
+    const bool mine = mbar_wait(smem_u32(bar + (L & 1)), (uint32_t)((L >> 1) & 1), spin);
     asm volatile("tcgen05.fence::after_thread_sync;");
     ok = __syncthreads_and(mine) != 0;
   }
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
-    // a wait gave up: wait once more (bounded) for the products in flight
-    // before the accumulator columns are freed
-    if (committed >= 0)
-      mbar_wait(smem_u32(bar + (committed & 1)), (uint32_t)((committed >> 1) & 1));
+    // a wait gave up: wait (bounded, at the full limit) for the products in
+    // flight before the accumulator columns are freed; the last commit
+    // covers every product issued before it.  Should even that run out, the
+    // flag says so (2) and the columns are freed anyway.
+    if (committed >= 0) {
+      bool done = false;
+      for (int k = 0; k < CLEANUP_WAITS && !done; k++)
+        done = mbar_wait(smem_u32(bar + (committed & 1)), (uint32_t)((committed >> 1) & 1),
+                         SPIN_LIMIT);
+      if (!done && tid == 0) atomicExch(err, 2);
+    }
   } else {
     // warp w may read accumulator lanes (rows) 32 (w % 4) .. + 31; the tile
     // goes through shared memory (the stages are free now), one half of the
@@ -313,7 +347,9 @@ __global__ void __launch_bounds__(NT, 2)
 #pragma unroll 4
       for (int it = 0; it < BM / (NT / 32); it++) {
         const int row = it * (NT / 32) + warp;
-        *reinterpret_cast<float4*>(Y + (size_t)(m0 + row) * ncols + n0 + h * EH + 4 * lane) =
+        const int R = m0 + row;  // a tile's rows all lie below or above split
+        float* Yr = R < split ? Y0 + (size_t)R * ncols : Y1 + (size_t)(R - split) * ncols;
+        *reinterpret_cast<float4*>(Yr + n0 + h * EH + 4 * lane) =
             *reinterpret_cast<const float4*>(T + row * TROW + 4 * lane);
       }
       __syncthreads();
@@ -407,29 +443,44 @@ static void operator_matrix(int map, int cut, int n_in, int n_out, double scale,
   for (double& v : M) v *= scale;
 }
 
+// whether a line pass of these lengths and column count fits the kernel
+bool tc_shape_ok(int n_in, int n_out, long long ncols) {
+  return n_out % tc::BM == 0 && ncols % tc::BN == 0 && n_in % tc::BK == 0 && ncols > 0 &&
+         n_in > 0;
+}
+
 int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, long long ncols,
-               Engine::TcOp** out) {
-  if (n_out % tc::BM || ncols % tc::BN || n_in % tc::BK || ncols <= 0 || n_in <= 0)
+               Engine::TcOp** out, int map2, int cut2, double scale2) {
+  if (!tc_shape_ok(n_in, n_out, ncols))
     return e.fail("tc_line_apply: n_out must be a multiple of 128, ncols of 256, n_in of 32",
                   ALFA_E_SHAPE);
-  if ((map == LM_PAD && 2 * n_out != 3 * n_in) || (map == LM_UNPAD && 3 * n_out != 2 * n_in) ||
-      (map != LM_PAD && map != LM_UNPAD && n_in != n_out))
-    return e.fail("tc_line_apply: lengths do not match the map", ALFA_E_SHAPE);
+  for (int m : {map, map2}) {
+    if (m < 0) continue;
+    if ((m == LM_PAD && 2 * n_out != 3 * n_in) || (m == LM_UNPAD && 3 * n_out != 2 * n_in) ||
+        (m != LM_PAD && m != LM_UNPAD && n_in != n_out))
+      return e.fail("tc_line_apply: lengths do not match the map", ALFA_E_SHAPE);
+  }
   // operators are built once per context and kept in its engine
   Engine::TcOp* op = nullptr;
   for (auto& o : e.tc_ops)
-    if (o.map == map && o.cut == cut && o.n_in == n_in && o.n_out == n_out && o.scale == scale)
+    if (o.map == map && o.cut == cut && o.n_in == n_in && o.n_out == n_out && o.scale == scale &&
+        o.map2 == map2 && (map2 < 0 || (o.cut2 == cut2 && o.scale2 == scale2)))
       op = &o;
   if (!op) {
     std::vector<double> M;
     operator_matrix(map, cut, n_in, n_out, scale, M);
+    if (map2 >= 0) {  // a second map stacked below the first
+      std::vector<double> M2;
+      operator_matrix(map2, cut2, n_in, n_out, scale2, M2);
+      M.insert(M.end(), M2.begin(), M2.end());
+    }
     std::vector<__nv_bfloat16> hi(M.size()), lo(M.size());
     for (size_t t = 0; t < M.size(); t++) {
       const float f = (float)M[t];
       hi[t] = __float2bfloat16_rn(f);
       lo[t] = __float2bfloat16_rn(f - __bfloat162float(hi[t]));
     }
-    Engine::TcOp o{map, cut, n_in, n_out, scale, nullptr, nullptr};
+    Engine::TcOp o{map, cut, n_in, n_out, scale, map2, cut2, scale2, nullptr, nullptr};
     if (cudaMalloc(&o.hi, M.size() * 2) != cudaSuccess) return e.fail("tc: allocation failed", ALFA_E_CUDA);
     e.allocs.push_back(o.hi);
     if (cudaMalloc(&o.lo, M.size() * 2) != cudaSuccess) return e.fail("tc: allocation failed", ALFA_E_CUDA);
@@ -452,13 +503,17 @@ int tc_prepare(Engine& e, int map, int cut, int n_in, int n_out, double scale, l
   return ALFA_OK;
 }
 
-// one launch (asynchronous; a wait that gave up sets e.tc_err)
-void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y) {
-  dim3 g((unsigned)(op->n_out / tc::BM), (unsigned)(ncols / tc::BN));
+// one launch (asynchronous; a wait that gave up sets e.tc_err): `batch`
+// slabs of (n_in, ncols) lines at X + b xbs; the first map's rows to Y0 +
+// b ybs, a stacked second map's rows to Y1 + b ybs
+void tc_launch(Engine& e, const Engine::TcOp* op, long long ncols, const float* X, float* Y0,
+               float* Y1, int batch, long long xbs, long long ybs) {
+  const int rows = op->n_out * (op->map2 >= 0 ? 2 : 1);
+  dim3 g((unsigned)(rows / tc::BM), (unsigned)(ncols / tc::BN), (unsigned)batch);
   ::alfa::note_launch();
   tc::k_line_gemm_bf16x3<<<g, tc::NT, tc::SMEM, e.stream>>>(
-      (const __nv_bfloat16*)op->hi, (const __nv_bfloat16*)op->lo, X, Y, op->n_in, ncols,
-      e.tc_err);
+      (const __nv_bfloat16*)op->hi, (const __nv_bfloat16*)op->lo, X, Y0, Y1 ? Y1 : Y0,
+      op->n_out, op->n_in, ncols, xbs, ybs, e.tc_err, e.tc_spin ? e.tc_spin : tc::SPIN_LIMIT);
 }
 
 int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale,
@@ -467,11 +522,15 @@ int tc_line_apply(Engine& e, int map, int cut, int n_in, int n_out, double scale
   const int st = tc_prepare(e, map, cut, n_in, n_out, scale, ncols, &op);
   if (st) return st;
   cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
-  tc_launch(e, op, ncols, X, Y);
+  tc_launch(e, op, ncols, X, Y, nullptr, 1, 0, 0);
   int h = 0;
   cudaMemcpyAsync(&h, e.tc_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
   if (cudaStreamSynchronize(e.stream) != cudaSuccess)
     return e.fail("tc_line_apply: kernel failed", ALFA_E_CUDA);
+  if (h == 2)
+    return e.fail("tc_line_apply: a bounded tensor-core wait gave up and the products in flight "
+                  "did not complete within the cleanup limit",
+                  ALFA_E_TIMEOUT);
   if (h) return e.fail("tc_line_apply: a bounded tensor-core wait gave up", ALFA_E_TIMEOUT);
   return ALFA_OK;
 }

@@ -85,13 +85,16 @@ def _err(a, b):
 
 
 @pytest.mark.parametrize("prec", PRECISIONS)
-def test_one_step_matches_oracle(prec):
+def test_one_step_matches_oracle(prec, report_line):
     cfg = cases.neutral(32, 32, 32, nsteps=1, precision=prec)
     sim = _sim(cfg)
     assert sim.alfa.lib.alfa_get_precision(sim.alfa.ctx) == {"fp32": 1, "mixed": 2}[prec]
     st = _state(sim.step(1))
     ref = _oracle(cases.neutral(32, 32, 32, nsteps=1), 1)
-    for k, err in _errs(st, ref).items():
+    errs = _errs(st, ref)
+    report_line(f"{prec} vs oracle, neutral 32^3, 1 step: "
+                + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+    for k, err in errs.items():
         print(f"{prec} neutral 32^3, 1 step, {k}: {err:.2e} "
               f"(relative to its own maximum {_err(st[k], ref[k]):.2e})")
         assert err <= 1e-5, (k, err)
@@ -105,11 +108,14 @@ def test_one_step_matches_oracle(prec):
     ("convective", (24, 24, 16), 10, {"optSgs": 2}),
     ("stable", (24, 24, 16), 10, {"optSgs": 4, "FGR": 2}),
 ])
-def test_fp32_steps_match_oracle(case, grid, steps, over):
+def test_fp32_steps_match_oracle(case, grid, steps, over, report_line):
     cfg = cases.CASES[case](*grid, nsteps=steps, precision="fp32", **over)
     st = _state(_sim(cfg).step(steps))
     ref = _oracle(cases.CASES[case](*grid, nsteps=steps, **over), steps)
-    for k, err in _errs(st, ref).items():
+    errs = _errs(st, ref)
+    report_line(f"fp32 vs oracle, {case} {over} {steps} steps: "
+                + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+    for k, err in errs.items():
         print(f"fp32 {case} {over} {steps} steps {k}: {err:.2e}")
         assert err <= (5e-3 if k == "p" else 1e-4), (k, err)
 
@@ -146,7 +152,7 @@ def test_per_function_entry_needs_fp64_context():
 
 
 @pytest.mark.parametrize("prec", PRECISIONS)
-def test_reduced_precision_against_fp64_after_many_steps(prec):
+def test_reduced_precision_against_fp64_after_many_steps(prec, report_line):
     """The convective case (C2 physics) at 32x32x24 for 1000 steps in FP64
     and in the reduced form from the same initial fields: the errors of the
     plane-averaged <u>, <theta>, <w'theta'> and <w'w'> profiles (the
@@ -167,8 +173,10 @@ def test_reduced_precision_against_fp64_after_many_steps(prec):
         assert np.isfinite(sim.diag()["CFL"])
         out[p] = stats_to_dict(acc, 24, cfg["Ugal"])
     errs = {k: _err(out[prec][k], out["fp64"][k]) for k in ("U", "TH", "wTH", "w2")}
-    print(f"{prec} vs fp64, 1000 steps, profile errors: "
-          + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+    line = (f"{prec} vs fp64, convective 32x32x24, 1000 steps, profile errors: "
+            + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
+    report_line(line)
+    print(line)
     # measured: U 3.0e-4, TH 7.4e-8, wTH 4.3e-5, w2 8.1e-5
     assert errs["U"] <= 2e-3 and errs["TH"] <= 1e-6, errs
     assert errs["wTH"] <= 1e-3 and errs["w2"] <= 1e-3, errs

@@ -70,3 +70,27 @@ def test_tc_line_pass_rejects_unaligned_shapes():
     with pytest.raises(_lib.AlfaError):
         a.tc_line_apply(X, "derivative")
     a.close()
+
+
+def test_tc_wait_limit_returns_timeout_and_context_recovers():
+    """A wait limit of one mbarrier poll makes the kernel's waits for its own
+    products give up: the call returns ALFA_E_TIMEOUT (the kernel waited at
+    the full limit for the products in flight and freed its tensor memory).
+    With the default limit restored, the same context computes the operator
+    correctly."""
+    from jax_alfa_b200 import _lib
+    from jax_alfa_b200.api import Alfa
+    a = Alfa(cases.neutral(16, 16, 8, nsteps=1))
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((256, 4, 128)).astype(np.float32)
+    Xd = torch.from_numpy(X).cuda()
+    assert a.lib.alfa_set_tc_spin_limit(a.ctx, 1) == 0
+    with pytest.raises(_lib.AlfaError) as ei:
+        a.tc_line_apply(Xd, "derivative")
+    assert "(-5)" in str(ei.value) and "gave up" in str(ei.value)
+    assert a.lib.alfa_set_tc_spin_limit(a.ctx, 0) == 0
+    Y = a.tc_line_apply(Xd, "derivative")
+    got = Y.cpu().numpy().astype(np.float64).reshape(256, -1)
+    ref = operator("derivative", 256, 256, 0) @ X.astype(np.float64).reshape(256, -1)
+    assert float(np.abs(got - ref).max() / np.abs(ref).max()) <= TOL
+    a.close()
