@@ -55,7 +55,8 @@ DTYPES = {"mixed": "f32 fields + split-bf16 tensor-core line passes + f64 solves
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 20; 500 with --ensemble)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="alfa", choices=["alfa", "reference"])
     ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
@@ -76,7 +77,12 @@ def parse():
     ap.add_argument("--ensemble", action="store_true",
                     help="time the 64-member uneven ensemble (32x32^3, 16x48^3, 16x64^3) "
                          "against its members stepped one at a time")
-    return ap.parse_args()
+    ap.add_argument("--ens-precision", default="fp32", choices=["fp32", "fp64"],
+                    help="storage precision of the ensemble members")
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 500 if args.ensemble else 20
+    return args
 
 
 def workload_config(grid, nsteps, precision="fp64"):
@@ -482,54 +488,83 @@ def run_alfa(args, rank, world, dist):
 
 
 def run_ensemble(args):
-    """The ensemble form: 64 independent neutral members of uneven sizes, each
-    with its own seed, stepped together (one CUDA graph launch per step)
-    against the same members stepped one after another.  Host wall clock
-    around synchronised calls (the ensemble's streams are internal)."""
-    import time
-
-    import numpy as np
+    """The ensemble form: 64 independent neutral members of uneven sizes (32 of
+    32^3, 16 of 48^3, 16 of 64^3), each with its own seed, u* ~ U[0.3, 0.6]
+    m/s and z0 log-uniform in [0.01, 0.5] m (cases.ensemble_members), in FP32
+    with the FP64 tridiagonal solve, stepped together (one CUDA graph launch
+    per step across the members' streams) against the same members stepped
+    one after another.  Both timed with CUDA events on this stream (the
+    ensemble's steps are ordered on it, alfa_ensemble_set_stream); every
+    member's final state is compared with the same member run alone."""
     import torch
 
     from jax_alfa_b200 import cases
     from jax_alfa_b200.api import Ensemble, Simulation
-    grids = [(32, 32, 32)] * 32 + [(48, 48, 48)] * 16 + [(64, 64, 64)] * 16
-    total = 2 * (args.warmup + args.steps) + 4
-    cfgs = [cases.neutral(*g, nsteps=total) for g in grids]
+    total = args.warmup + args.steps + 2
+    members = cases.ensemble_members(nsteps=total, precision=args.ens_precision)
+    n_gp = int(sum(c["nx"] * c["ny"] * c["nz"] for c, _ in members))
+    stream = torch.cuda.current_stream()
 
-    def make(i, c):
-        u, v, w, th = cases.initial_fields(c, i)
+    def make(c, seed):
+        u, v, w, th = cases.initial_fields(c, seed)
         return Simulation(c, u, v, w, th, adv_series=cases.adv_forcing_series(c))
 
-    n_gp = int(sum(np.prod(g) for g in grids))
-    sims = [make(i, c) for i, c in enumerate(cfgs)]
-    for s_ in sims:
-        s_.step(args.warmup, graph=True)
+    def state(sim):
+        return {k: t.cpu().numpy() for k, t in sim.state().items()}
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sims = [make(c, seed) for c, seed in members]
+    for s_ in sims:  # the bootstrap step, then graph captures of both parities
+        s_.step(1)
+        s_.step(max(args.warmup - 1, 2), graph=True)
     torch.cuda.synchronize()
-    t = time.perf_counter()
+    e0.record(stream)
     for _ in range(args.steps):
         for s_ in sims:
             s_.step(1, graph=True)
+    e1.record(stream)
     torch.cuda.synchronize()
-    t_seq = (time.perf_counter() - t) / args.steps
+    t_seq = e0.elapsed_time(e1) / args.steps
+    alone = [state(s_) for s_ in sims]
     del sims
     torch.cuda.empty_cache()
-    ens = Ensemble([make(i, c) for i, c in enumerate(cfgs)])
-    ens.step(args.warmup).sync()
-    t = time.perf_counter()
-    ens.step(args.steps).sync()
-    t_ens = (time.perf_counter() - t) / args.steps
+
+    ens = Ensemble([make(c, seed) for c, seed in members]).set_stream(stream)
+    ens.step(1 + max(args.warmup - 1, 2))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ens.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_ens = e0.elapsed_time(e1) / args.steps
+    errs, exact = [], 0
+    for st, ref in zip(ens.states(), alone):
+        got = {k: t.cpu().numpy() for k, t in st.items()}
+        e = max(float(np.abs(got[k] - ref[k]).max()) / max(float(np.abs(ref[k]).max()), 1e-300)
+                for k in ref)
+        errs.append(e)
+        exact += all(np.array_equal(got[k], ref[k]) for k in ref)
     ens.close()
     print(json.dumps({
         "metric": "ensemble LES grid-point-steps/s (64 members: 32x32^3, 16x48^3, 16x64^3)",
-        "value": n_gp / t_ens, "unit": "gp-steps/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t_ens, "higher_is_better": True,
-        "sequential": {"value": n_gp / t_seq, "ms_per_step": 1e3 * t_seq,
+        "value": n_gp / (t_ens / 1e3), "unit": "gp-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": 1 + max(args.warmup - 1, 2),
+        "ms_per_step": t_ens, "higher_is_better": True,
+        "sequential": {"value": n_gp / (t_seq / 1e3), "ms_per_step": t_seq,
                        "how": "the same members, one graph step each, one after another"},
-        "speedup_vs_sequential": t_seq / t_ens, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "neutral ABL members (C1 physics), LASDD-SM, FP64",
-                   "members": len(grids), "grid_points": n_gp,
-                   "timing": "host wall clock around synchronised calls"}}), flush=True)
+        "speedup_vs_sequential": t_seq / t_ens,
+        "members_vs_alone": {"max_rel_err": max(errs), "bit_identical": exact,
+                             "members": len(errs), "bar": 1e-6,
+                             "after_steps": 1 + max(args.warmup - 1, 2) + args.steps},
+        "dtype": DTYPES[args.ens_precision], "data": "synthetic",
+        "config": {"workload": "neutral ABL members (C1 physics), LASDD-SM, per-member seed, "
+                               "u* ~ U[0.3, 0.6] m/s, z0 log-uniform [0.01, 0.5] m",
+                   "members": len(members), "grid_points": n_gp,
+                   "precision": args.ens_precision,
+                   "timing": "CUDA events on the stream the steps are ordered on"}}),
+        flush=True)
+    if max(errs) > 1e-6:
+        raise SystemExit(f"ensemble member differs from its run alone: {max(errs):.2e}")
 
 
 def run_learned(args):

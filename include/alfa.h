@@ -348,6 +348,11 @@ typedef struct alfa_ensemble alfa_ensemble;
 int alfa_ensemble_create(alfa_ctx* const* members, int n, alfa_ensemble** out);
 int alfa_ensemble_step(alfa_ensemble*, int nsteps);
 int alfa_ensemble_sync(alfa_ensemble*);
+/* Orders later alfa_ensemble_step calls on `stream` (a cudaStream_t; NULL
+ * to stop): each call's steps start after the work already queued on it,
+ * and work queued on it afterwards starts after the steps, so events
+ * recorded on it time them. */
+int alfa_ensemble_set_stream(alfa_ensemble*, void* stream);
 const char* alfa_ensemble_error(const alfa_ensemble*);
 void alfa_ensemble_destroy(alfa_ensemble*);
 
@@ -449,9 +454,10 @@ int alfa_time_kernel(alfa_ctx*, int which, int reps, double* ms /* host */,
  * run with `variant` (0 the default dispatch, 1 the compile-time transform
  * in place of a phase-split pad/unpad, 2/3/4 the runtime-plan transform
  * with radix schedule "largest radix 8" / "largest radix 4" / "default
- * factors in ascending order"), its average launch time, whether its
- * outputs equal the default's to 1e-12 of their maximum, and whether it was
- * chosen. */
+ * factors in ascending order", 5 the split-BF16 tensor-core pass of an
+ * ALFA_MIXED context), its average launch time, whether its outputs equal
+ * the default's to the precision's round-off of their maximum (1e-12 FP64,
+ * 1e-5 FP32, 5e-5 for the tensor-core pass), and whether it was chosen. */
 typedef struct alfa_tune_entry {
   int axis, n_in, n_out, outputs, map, variant, chosen, equal;
   double ms;
@@ -468,6 +474,17 @@ typedef struct alfa_tune_entry {
 int alfa_autotune(alfa_ctx*, int reps, alfa_tune_entry* out /* host */, int max_out,
                   int* n_out /* host */);
 
+/* No counterpart in the reference.  Makes `variant` (numbered as in
+ * alfa_tune_entry) the one the step uses for the line passes of one of the
+ * eight autotuned shapes, without timing: (axis, n_in, n_out, map, outputs)
+ * as in alfa_tune_entry.  Variant 5 (tensor cores) needs an ALFA_MIXED
+ * context and a shape the GEMM tiles (n_out a multiple of 128, n_in of 32,
+ * the pass's columns of 256) and builds the pass's operator here.  Returns
+ * ALFA_E_SHAPE when no autotuned shape matches or the variant does not apply
+ * to it.  Captured step graphs are released. */
+int alfa_set_line_variant(alfa_ctx*, int axis, int n_in, int n_out, int map, int outputs,
+                          int variant);
+
 /* ---- split-BF16 tensor-core line pass (FP32; no counterpart in the
  * reference, whose FFT passes run in the run's precision) -----------------
  * Y (n_out, ncols) = scale * M X for X (n_in, ncols) FP32 row-major (the x
@@ -476,8 +493,8 @@ int alfa_autotune(alfa_ctx*, int reps, alfa_tune_entry* out /* host */, int max_
  * Nyquist mode zeroed, 3 both, 4 the 3/2 pad n -> 3n/2, 5 the unpad 3n/2 ->
  * n; 0 identity) exactly as the FP64 line passes apply it.  Runs as a GEMM
  * on tcgen05 with BF16 hi/lo operand pairs (three products, FP32
- * accumulation in tensor memory): about 1e-5 relative accuracy.  n_out and
- * n_out a multiple of 128, ncols of 256, n_in of 32.  Synchronises the stream. */
+ * accumulation in tensor memory): about 1e-5 relative accuracy.  n_out a
+ * multiple of 128, ncols of 256, n_in of 32.  Synchronises the stream. */
 int alfa_tc_line_apply(alfa_ctx*, int map, int cut, int n_in, int n_out, double scale,
                        long long ncols, const float* X, float* Y);
 

@@ -183,6 +183,8 @@ def load():
     lib.alfa_autotune.argtypes = [CTX, I, ctypes.POINTER(AlfaTuneEntry), I,
                                   ctypes.POINTER(ctypes.c_int)]
     lib.alfa_autotune.restype = I
+    lib.alfa_set_line_variant.argtypes = [CTX, I, I, I, I, I, I]
+    lib.alfa_set_line_variant.restype = I
     lib.alfa_tc_line_apply.argtypes = [CTX, I, I, I, I, D, ctypes.c_longlong, P, P]
     lib.alfa_tc_line_apply.restype = I
     lib.alfa_set_tc_spin_limit.argtypes = [CTX, ctypes.c_ulonglong]
@@ -197,6 +199,8 @@ def load():
     lib.alfa_ensemble_step.restype = I
     lib.alfa_ensemble_sync.argtypes = [c_void_p]
     lib.alfa_ensemble_sync.restype = I
+    lib.alfa_ensemble_set_stream.argtypes = [c_void_p, c_void_p]
+    lib.alfa_ensemble_set_stream.restype = I
     lib.alfa_ensemble_error.argtypes = [c_void_p]
     lib.alfa_ensemble_error.restype = ctypes.c_char_p
     lib.alfa_ensemble_destroy.argtypes = [c_void_p]

@@ -123,6 +123,14 @@ class Alfa:
                         "equal": bool(e.equal), "chosen": bool(e.chosen)})
         return out
 
+    def set_line_variant(self, shape, variant):
+        """Make `variant` (a TUNE_VARIANTS name) the one the step uses for a
+        pass shape of autotune's list (a dict with axis, n_in, n_out, map
+        and outputs), without timing (alfa_set_line_variant)."""
+        self._call("alfa_set_line_variant", int(shape["axis"]), int(shape["n_in"]),
+                   int(shape["n_out"]), int(shape["map"]), int(shape["outputs"]),
+                   self.TUNE_VARIANTS.index(variant))
+
     TC_MAPS = {"identity": 0, "truncate": 1, "derivative": 2, "truncate+derivative": 3,
                "pad": 4, "unpad": 5}
 
@@ -697,6 +705,14 @@ class Ensemble:
                                  f"{self.lib.alfa_ensemble_error(self.h).decode()}")
         return self
 
+    def set_stream(self, stream):
+        """Order later steps on a torch CUDA stream (alfa_ensemble_set_stream),
+        so that events recorded on it time them; None stops."""
+        h = ctypes.c_void_p(stream.cuda_stream if stream is not None else None)
+        if self.lib.alfa_ensemble_set_stream(self.h, h) != 0:
+            raise _lib.AlfaError("alfa_ensemble_set_stream failed")
+        return self
+
     def sync(self):
         if self.lib.alfa_ensemble_sync(self.h) != 0:
             raise _lib.AlfaError("ensemble synchronisation failed")
@@ -887,6 +903,11 @@ class Simulation:
     def autotune(self, reps=5):
         """Alfa.autotune on this simulation's context (between steps)."""
         return self.alfa.autotune(reps)
+
+    def set_line_variant(self, shape, variant):
+        """Alfa.set_line_variant on this simulation's context."""
+        self.alfa.set_line_variant(shape, variant)
+        return self
 
     def reset(self, u, v, w, th, Q=None):
         """Start again from new initial fields (dimensional, as the

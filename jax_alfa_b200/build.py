@@ -39,15 +39,34 @@ def nvcc():
 OBJ_DIR = os.path.join(ROOT, "_build")
 
 
-def _unit_stale(src, obj):
-    """An object is rebuilt when it is missing or older than its source, any
-    header of the library, this script or the C header."""
+def _deps(src, obj):
+    """The files an object was compiled from: nvcc's dependency list of its
+    last compile (obj.d), else the source and every header of the library."""
+    try:
+        with open(obj + ".d") as f:
+            text = f.read().replace("\\\n", " ")
+        files = [t for t in text.split(":", 1)[1].split() if os.path.exists(t)]
+        if files:
+            return files
+    except (OSError, IndexError):
+        pass
+    return ([os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS]
+            + [os.path.join(ROOT, "include", "alfa.h")])
+
+
+def _unit_stale(src, obj, cmd):
+    """An object is rebuilt when it is missing, was compiled with another
+    recorded command line, or is older than a file it was compiled from."""
     if not os.path.exists(obj):
         return True
+    try:
+        with open(obj + ".cmd") as f:
+            if f.read() != " ".join(cmd):
+                return True
+    except OSError:  # compiled before command lines were recorded
+        pass
     t = os.path.getmtime(obj)
-    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS]
-    deps += [os.path.join(ROOT, "include", "alfa.h"), os.path.abspath(__file__)]
-    return any(os.path.getmtime(d) > t for d in deps)
+    return any(os.path.getmtime(d) > t for d in _deps(src, obj))
 
 
 def build(force=False, verbose=False):
@@ -58,10 +77,13 @@ def build(force=False, verbose=False):
     for src, extra, suffix in UNITS:  # translation units compile concurrently
         obj = os.path.join(OBJ_DIR, src.replace(".cu", suffix + ".o"))
         objs.append(obj)
-        if not force and not _unit_stale(src, obj):
-            continue
         cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                "-c", os.path.join(CSRC, src), "-o", obj]
+        if not force and not _unit_stale(src, obj, cmd):
+            continue
+        with open(obj + ".cmd", "w") as f:
+            f.write(" ".join(cmd))
+        cmd += ["-MD", "-MF", obj + ".d"]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((src + suffix, obj, time.time(),

@@ -53,14 +53,35 @@ USTAR_NEUTRAL = 0.45
 
 
 def neutral(nx=32, ny=32, nz=32, nsteps=200, **over):
+    """The neutral channel-like ABL driven by a constant pressure-gradient
+    forcing u*^2 / l_z (``ustar``, default 0.45 m/s), log-law initial wind
+    over roughness z0m."""
     cfg = dict(_BASE, l_x=2000.0, l_y=2000.0, l_z=1000.0, nx=nx, ny=ny, nz=nz,
                dt=0.5, optSgs=1, z0m=0.1, z0T=0.1, optAdvection=1,
-               z_damping=800.0, optDamping=0)
+               z_damping=800.0, optDamping=0, ustar=USTAR_NEUTRAL)
     cfg["SimTime"] = nsteps * cfg["dt"]
-    cfg["Uadv_const"] = USTAR_NEUTRAL ** 2 / cfg["l_z"]   # m s^-2
     cfg["case"] = "neutral"
     cfg.update(over)
+    cfg.setdefault("Uadv_const", cfg["ustar"] ** 2 / cfg["l_z"])   # m s^-2
     return cfg
+
+
+def ensemble_members(nsteps=500, precision="fp32", seed=2024):
+    """The ensemble workload: 64 independent neutral members of uneven sizes
+    (32 of 32^3, 16 of 48^3, 16 of 64^3), each with its own seed for the
+    initial perturbation, friction velocity u* ~ U[0.3, 0.6] m/s (forcing
+    and initial log law) and roughness z0 (= z0m = z0T) log-uniform in
+    [0.01, 0.5] m, drawn from one seeded generator.  Returns a list of
+    (config, initial-field seed)."""
+    rng = np.random.default_rng(seed)
+    grids = [(32, 32, 32)] * 32 + [(48, 48, 48)] * 16 + [(64, 64, 64)] * 16
+    out = []
+    for i, g in enumerate(grids):
+        ustar = float(rng.uniform(0.3, 0.6))
+        z0 = float(np.exp(rng.uniform(np.log(0.01), np.log(0.5))))
+        out.append((neutral(*g, nsteps=nsteps, ustar=ustar, z0m=z0, z0T=z0,
+                            precision=precision), 1000 + i))
+    return out
 
 
 def nbl_a94(nx=256, ny=256, nz=256, nsteps=400000, **over):
@@ -133,7 +154,7 @@ def initial_fields(cfg, seed=0):
                 u[:, :, k] += 0.03 * rng.standard_normal((nx, ny))
                 th[:, :, k] += 1.0e-3 * rng.standard_normal((nx, ny))
     elif case == "neutral":
-        prof = (USTAR_NEUTRAL / VONK) * np.log(z / cfg["z0m"])
+        prof = (cfg.get("ustar", USTAR_NEUTRAL) / VONK) * np.log(z / cfg["z0m"])
         u[:] = prof[None, None, :]
         for k in range(nz):
             if z[k] < 500.0:

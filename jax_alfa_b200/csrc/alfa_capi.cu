@@ -220,6 +220,12 @@ int alfa_autotune(alfa_ctx* c, int reps, alfa_tune_entry* out, int max_out, int*
   return DISPATCH(c, autotune, reps, out, max_out, n_out);
 }
 
+int alfa_set_line_variant(alfa_ctx* c, int axis, int n_in, int n_out, int map, int outputs,
+                          int variant) {
+  CTX_CHECK(c);
+  return DISPATCH(c, set_line_variant, axis, n_in, n_out, map, outputs, variant);
+}
+
 int alfa_tc_line_apply(alfa_ctx* c, int map, int cut, int n_in, int n_out, double scale,
                        long long ncols, const float* X, float* Y) {
   CTX_CHECK(c);
@@ -772,6 +778,12 @@ int alfa_ensemble_step(alfa_ensemble* E, int nsteps) {
 int alfa_ensemble_sync(alfa_ensemble* E) {
   if (!E) return ALFA_E_STATE;
   return E->d ? f64::ens_sync(E->d) : alfa::f32::ens_sync(E->f);
+}
+
+int alfa_ensemble_set_stream(alfa_ensemble* E, void* stream) {
+  if (!E) return ALFA_E_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  return E->d ? f64::ens_set_stream(E->d, s) : alfa::f32::ens_set_stream(E->f, s);
 }
 
 const char* alfa_ensemble_error(const alfa_ensemble* E) {

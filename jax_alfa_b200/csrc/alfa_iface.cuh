@@ -37,12 +37,14 @@
   int load_checkpoint(Ctx* c, const double* src);                                             \
   int time_kernel(Ctx* c, int which, int reps, double* ms, double* bytes);                    \
   int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out);              \
+  int set_line_variant(Ctx* c, int axis, int n_in, int n_out, int map, int nout, int variant); \
   int tc_line_apply(Ctx* c, int map, int cut, int n_in, int n_out, double scale,              \
                     long long ncols, const float* X, float* Y);                               \
   void ctx_set_tc_spin(Ctx* c, unsigned long long polls);                                     \
   int ens_create(Ctx* const* members, int n, Ens** out);                                      \
   int ens_step(Ens* E, int nsteps);                                                           \
   int ens_sync(Ens* E);                                                                       \
+  int ens_set_stream(Ens* E, cudaStream_t s);                                                 \
   const char* ens_error(const Ens* E);                                                        \
   void ens_destroy(Ens* E);
 

@@ -1551,27 +1551,24 @@ __global__ void k_maxdiff(const real* __restrict__ a, const real* __restrict__ b
 static constexpr double kTuneTol = sizeof(real) == 8 ? 1e-12 : 1e-5;
 static constexpr double kTcTuneTol = 5e-5;
 
-int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
+// the eight line-pass shapes of a step the autotuner times: (X, Y) are the
+// input's x and y extents; `in` a synthetic input, `dst` step scratch
+struct TuneShape {
+  int axis, X, Y, n_in, n_out, nout, map[2];
+  const real* in;
+  real* dst[2];
+  size_t len;
+  double scale;
+  int cut;
+};
+
+static void tune_shapes(Ctx* c, const real* src, TuneShape sh[8]) {
   Engine& e = c->e;
-  if (reps < 1 || (max_out > 0 && !out)) return e.fail("autotune: bad arguments", ALFA_E_SHAPE);
   Work& W = c->w;
   const size_t N = e.N(), Y = (size_t)e.nx * e.my * e.nz, P = e.P();
-  real* src = W.Pb[4];
-  real* ref[2] = {W.Pb[2], W.Pb[3]};
-  unsigned long long* dmax = reinterpret_cast<unsigned long long*>(W.Pb[5]);
-  k_fill_hash<<<4 * 148, 256, 0, e.stream>>>(src, N);
-  // the pass shapes of a step: (X, Y) are the input's x and y extents
-  struct Shape {
-    int axis, X, Y, n_in, n_out, nout, map[2];
-    const real* in;
-    real* dst[2];
-    size_t len;
-    double scale;
-    int cut;
-  };
   const real* Lp = W.Lpad;
   const int nx = e.nx, ny = e.ny, mx = e.mx, my = e.my;
-  const Shape shapes[8] = {
+  const TuneShape t[8] = {
       {1, nx, ny, ny, my, 1, {LM_PAD, 0}, src, {W.Lpad, nullptr}, Y, 1.0 / my, 0},
       {0, nx, my, nx, mx, 1, {LM_PAD, 0}, Lp, {W.Pb[0], nullptr}, P, 1.0 / mx, 0},
       {0, mx, my, mx, nx, 1, {LM_UNPAD, 0}, W.Pb[0], {W.Lpad, nullptr}, Y, 1.0 / nx, 0},
@@ -1583,12 +1580,81 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
       {1, nx, ny, ny, ny, 2, {LM_TRUNC, LM_TRUNC_DERIV}, src, {W.L2, W.L2 + N}, N, 1.0 / ny,
        e.cut_e[1]},
   };
+  for (int i = 0; i < 8; i++) sh[i] = t[i];
+}
+
+// whether a shape's pass can take the phase-split (1) variant's alternative
+static bool tune_phase(const TuneShape& sh) {
+  return sh.nout == 1 && ((sh.map[0] == LM_PAD && sh.n_in == 256 && sh.n_out == 384) ||
+                          (sh.map[0] == LM_UNPAD && sh.n_in == 384 && sh.n_out == 256));
+}
+
+// the GEMM columns of a shape's pass on the tensor cores: x lines as one
+// (n_in, Y nz) slab, y lines as X slabs of (n_in, nz)
+static long long tune_tc_cols(const Engine& e, const TuneShape& sh) {
+  return sh.axis == 0 ? (long long)sh.Y * e.nz : (long long)e.nz;
+}
+
+#ifdef ALFA_BUILD_FP32
+// builds the tensor-core operator of a shape's pass (ALFA_MIXED only)
+static int tune_tc_prepare(Engine& e, const TuneShape& sh) {
+  Engine::TcOp* op = nullptr;
+  return tc_prepare(e, sh.map[0], sh.cut, sh.n_in, sh.n_out, sh.scale, tune_tc_cols(e, sh), &op,
+                    sh.nout > 1 ? sh.map[1] : -1, sh.cut, sh.scale);
+}
+#endif
+
+int set_line_variant(Ctx* c, int axis, int n_in, int n_out, int map, int nout, int variant) {
+  Engine& e = c->e;
+  if (variant < 0 || variant > TC_VARIANT)
+    return e.fail("alfa_set_line_variant: variant must be 0..5", ALFA_E_SHAPE);
+  TuneShape shapes[8];
+  tune_shapes(c, c->w.Pb[4], shapes);
+  for (const TuneShape& sh : shapes) {
+    if (sh.axis != axis || sh.n_in != n_in || sh.n_out != n_out || sh.map[0] != map ||
+        sh.nout != nout)
+      continue;
+    if (variant == 1 && !tune_phase(sh))
+      return e.fail("alfa_set_line_variant: variant 1 applies to the 256 <-> 384 pad and unpad",
+                    ALFA_E_SHAPE);
+    if (variant == TC_VARIANT) {
+#ifdef ALFA_BUILD_FP32
+      if (e.cfg.precision != ALFA_MIXED || !tc_shape_ok(n_in, n_out, tune_tc_cols(e, sh)))
+        return e.fail("alfa_set_line_variant: the tensor-core pass needs an ALFA_MIXED context "
+                      "and n_out % 128 == 0, n_in % 32 == 0, the pass's columns % 256 == 0",
+                      ALFA_E_SHAPE);
+      const int rc = tune_tc_prepare(e, sh);
+      if (rc) return rc;
+      cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
+#else
+      return e.fail("alfa_set_line_variant: the tensor-core pass needs an ALFA_MIXED context",
+                    ALFA_E_SHAPE);
+#endif
+    }
+    e.line_variant[line_key(axis, n_in, n_out, map, nout)] = variant;
+    release_graphs(c);  // captured steps hold the old choice
+    return check_launch(e, "alfa_set_line_variant");
+  }
+  return e.fail("alfa_set_line_variant: no autotuned line-pass shape matches", ALFA_E_SHAPE);
+}
+
+int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
+  Engine& e = c->e;
+  if (reps < 1 || (max_out > 0 && !out)) return e.fail("autotune: bad arguments", ALFA_E_SHAPE);
+  Work& W = c->w;
+  const size_t N = e.N();
+  real* src = W.Pb[4];
+  real* ref[2] = {W.Pb[2], W.Pb[3]};
+  unsigned long long* dmax = reinterpret_cast<unsigned long long*>(W.Pb[5]);
+  k_fill_hash<<<4 * 148, 256, 0, e.stream>>>(src, N);
+  TuneShape shapes[8];
+  tune_shapes(c, src, shapes);
   cudaEvent_t ea, eb;
   cudaEventCreate(&ea);
   cudaEventCreate(&eb);
   int n = 0;
   int rc = ALFA_OK;
-  for (const Shape& sh : shapes) {
+  for (const TuneShape& sh : shapes) {
     LineOut o[2];
     for (int q = 0; q < sh.nout; q++) {
       o[q] = LineOut{};
@@ -1598,9 +1664,7 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
       o[q].dst = sh.dst[q];
     }
     const long long key = line_key(sh.axis, sh.n_in, sh.n_out, sh.map[0], sh.nout);
-    const bool phase = sh.nout == 1 &&
-                       ((sh.map[0] == LM_PAD && sh.n_in == 256 && sh.n_out == 384) ||
-                        (sh.map[0] == LM_UNPAD && sh.n_in == 384 && sh.n_out == 256));
+    const bool phase = tune_phase(sh);
     auto run = [&] {
       launch_line(e, sh.axis, ld_field(e, sh.in), sh.X, sh.Y, sh.n_in, sh.n_out, sh.nout, o);
     };
@@ -1614,12 +1678,8 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
       if (v != 1 || phase) cand.push_back(v);
 #ifdef ALFA_BUILD_FP32
     if (e.cfg.precision == ALFA_MIXED) {  // operators are built here, never inside a capture
-      const long long ncols = sh.axis == 0 ? (long long)sh.Y * e.nz : (long long)e.nz;
-      Engine::TcOp* op = nullptr;
-      if (tc_shape_ok(sh.n_in, sh.n_out, ncols)) {
-        if ((rc = tc_prepare(e, sh.map[0], sh.cut, sh.n_in, sh.n_out, sh.scale, ncols, &op,
-                             sh.nout > 1 ? sh.map[1] : -1, sh.cut, sh.scale)) != ALFA_OK)
-          break;
+      if (tc_shape_ok(sh.n_in, sh.n_out, tune_tc_cols(e, sh))) {
+        if ((rc = tune_tc_prepare(e, sh)) != ALFA_OK) break;
         cudaMemsetAsync(e.tc_err, 0, sizeof(int), e.stream);
         cand.push_back(TC_VARIANT);
       }
@@ -1698,6 +1758,8 @@ struct Ens {
   std::vector<cudaEvent_t> done;  // member i finished its part of the graph
   cudaStream_t master = nullptr;
   cudaEvent_t start = nullptr;
+  cudaStream_t user = nullptr;   // the caller's stream the steps are ordered on
+  cudaEvent_t fence = nullptr;
   struct G {
     cudaGraphExec_t exec = nullptr;
     std::vector<StepPtrs> before, after;
@@ -1825,8 +1887,32 @@ int ens_create(Ctx* const* members, int n, Ens** out) {
   return ALFA_OK;
 }
 
+static int ens_steps(Ens* E, int nsteps);
+
 int ens_step(Ens* E, int nsteps) {
   if (!E) return ALFA_E_STATE;
+  if (E->user) {  // after the work already queued on the caller's stream
+    cudaEventRecord(E->fence, E->user);
+    cudaStreamWaitEvent(E->master, E->fence, 0);
+  }
+  const int st = ens_steps(E, nsteps);
+  if (E->user) {  // and before the work queued on it next
+    cudaEventRecord(E->fence, E->master);
+    cudaStreamWaitEvent(E->user, E->fence, 0);
+  }
+  return st;
+}
+
+int ens_set_stream(Ens* E, cudaStream_t s) {
+  if (!E) return ALFA_E_STATE;
+  if (s && !E->fence &&
+      cudaEventCreateWithFlags(&E->fence, cudaEventDisableTiming) != cudaSuccess)
+    return ALFA_E_CUDA;
+  E->user = s;
+  return ALFA_OK;
+}
+
+static int ens_steps(Ens* E, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
     int st = ens_graph_step(E);
     if (st == ALFA_OK) continue;
@@ -1871,6 +1957,7 @@ void ens_destroy(Ens* E) {
     if (E->done[i]) cudaEventDestroy(E->done[i]);
   }
   if (E->start) cudaEventDestroy(E->start);
+  if (E->fence) cudaEventDestroy(E->fence);
   if (E->master) cudaStreamDestroy(E->master);
   delete E;
 }

@@ -22,10 +22,11 @@ def test_signature_table_covers_header():
                                     "alfa_set_stream", "alfa_get_derived", "alfa_get_precision",
                                     "alfa_workspace_bytes", "alfa_get_diag",
                                     "alfa_launch_count", "alfa_time_kernel", "alfa_autotune",
-                                    "alfa_tc_line_apply", "alfa_set_tc_spin_limit",
+                                    "alfa_set_line_variant", "alfa_tc_line_apply", "alfa_set_tc_spin_limit",
                                     "alfa_PlanarMean_noalloc", "alfa_checkpoint_doubles",
                                     "alfa_ensemble_create", "alfa_ensemble_step",
-                                    "alfa_ensemble_sync", "alfa_ensemble_error",
+                                    "alfa_ensemble_sync", "alfa_ensemble_set_stream",
+                                    "alfa_ensemble_error",
                                     "alfa_ensemble_destroy", "alfa_mlp_create",
                                     "alfa_mlp_destroy", "alfa_mlp_collect", "alfa_mlp_train",
                                     "alfa_mlp_loss_grad", "alfa_mlp_get_params",

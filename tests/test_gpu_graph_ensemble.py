@@ -106,3 +106,26 @@ def test_reset_restarts_the_run_bitwise():
     again = _state(s.step(5, graph=True))
     for k in fresh:
         assert np.array_equal(fresh[k], again[k]), k
+
+
+def test_fp32_ensemble_with_member_draws_equals_members_alone():
+    """Members of the ensemble workload (cases.ensemble_members: own seed,
+    u* ~ U[0.3, 0.6] m/s, z0 log-uniform in [0.01, 0.5] m; FP32 with the FP64
+    tridiagonal solve), two of each size, 100 steps together against each
+    run alone: bit for bit (the bar of the workload is 1e-6 relative)."""
+    import torch
+
+    from jax_alfa_b200.api import Ensemble
+    steps = 100
+    pick = [0, 1, 32, 33, 48, 49]
+    members = [cases.ensemble_members(nsteps=steps + 1)[i] for i in pick]
+    assert len({round(c["ustar"], 6) for c, _ in members}) == len(pick)
+    alone = [_state(_sim(c, seed=s).step(1).step(steps - 1, graph=True)) for c, s in members]
+    ens = Ensemble([_sim(c, seed=s) for c, s in members])
+    ens.set_stream(torch.cuda.current_stream())
+    ens.step(steps)
+    for i, st in enumerate(ens.states()):
+        got = {k: t.cpu().numpy() for k, t in st.items()}
+        for k in got:
+            assert np.array_equal(got[k], alone[i][k]), (i, k)
+    ens.close()

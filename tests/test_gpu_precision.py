@@ -180,3 +180,59 @@ def test_reduced_precision_against_fp64_after_many_steps(prec, report_line):
     # measured: U 3.0e-4, TH 7.4e-8, wTH 4.3e-5, w2 8.1e-5
     assert errs["U"] <= 2e-3 and errs["TH"] <= 1e-6, errs
     assert errs["wTH"] <= 1e-3 and errs["w2"] <= 1e-3, errs
+
+
+def test_mixed_step_with_tensor_core_passes(report_line):
+    """The mixed form with every line pass the tensor cores can tile forced
+    onto them (alfa_set_line_variant 'tensor-core', whatever the autotuner
+    would pick): the reference's NBL_A94 case at 256^3, where every x and y
+    pass qualifies, stepped 5 times from the same initial fields as the FP64
+    drop-in and the plain FP32 form.  The split-BF16 products (about 2^-16
+    relative per operator entry) must keep the velocity within 1e-4 of the
+    FP64 state (relative to the largest velocity component) and theta within
+    1e-4 of its own largest value; pressure within 5e-3.  Errors of both
+    reduced forms are printed."""
+    from jax_alfa_b200.api import Simulation
+    grid, steps = (256, 256, 256), 5
+    u, v, w, th = cases.initial_fields(cases.nbl_a94(*grid, nsteps=steps + 1), 0)
+    states, forced = {}, []
+    for p in ("fp64", "fp32", "mixed"):
+        sim = Simulation(cases.nbl_a94(*grid, nsteps=steps + 1, precision=p), u, v, w, th)
+        if p == "mixed":
+            tune = sim.autotune(reps=1)
+            for c in tune:
+                if c["variant"] == "tensor-core":
+                    sim.set_line_variant(c, "tensor-core")
+                    forced.append((c["shape"], c["equal"]))
+        sim.step(steps, graph=True)
+        assert np.isfinite(sim.diag()["CFL"])
+        states[p] = _state(sim)
+        del sim
+        torch.cuda.empty_cache()
+    assert len(forced) == 8, forced  # every pass shape of the 256^3 step
+    report_line("tensor-core passes within the autotuner's 5e-5 of the FP32 pass: "
+                + ", ".join(f"{s} {'yes' if eq else 'no'}" for s, eq in forced))
+    for p in ("fp32", "mixed"):
+        errs = _errs(states[p], states["fp64"])
+        line = (f"{p} vs fp64, NBL_A94 256^3, {steps} steps"
+                + (" (tensor-core passes forced)" if p == "mixed" else "") + ": "
+                + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+        report_line(line)
+        print(line)
+        for k in ("u", "v", "w", "TH"):
+            assert errs[k] <= 1e-4, (p, k, errs[k])
+        assert errs["p"] <= 5e-3, (p, errs["p"])
+
+
+def test_set_line_variant_rejects_what_does_not_apply():
+    from jax_alfa_b200._lib import AlfaError
+    cfg = cases.neutral(32, 32, 32, nsteps=2, precision="fp32")
+    sim = _sim(cfg)
+    shape = {"axis": 0, "n_in": 32, "n_out": 32, "map": 2, "outputs": 1}
+    sim.set_line_variant(shape, "radix-4")  # applies in every precision
+    with pytest.raises(AlfaError):
+        sim.set_line_variant(shape, "tensor-core")  # not a mixed context
+    with pytest.raises(AlfaError):
+        sim.set_line_variant(dict(shape, n_in=30), "default")  # no such pass shape
+    sim.step(1)
+    assert np.isfinite(sim.diag()["CFL"])
