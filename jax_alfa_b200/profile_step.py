@@ -1,0 +1,37 @@
+"""A few whole steps of the NBL_A94 workload (the reference's neutral
+boundary-layer benchmark case) for profilers: the bootstrap step, then graph
+steps, nothing else on the device.  The kernel launch lists and ncu captures
+under profiles/ name this command.
+
+    python -m jax_alfa_b200.profile_step --precision mixed --grid 256 256 256 --steps 3
+"""
+import argparse
+import sys
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "fp32", "mixed"])
+    ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
+    ap.add_argument("--steps", type=int, default=3, help="graph steps after the bootstrap step")
+    ap.add_argument("--tune", action="store_true", help="run the line-pass autotuner first")
+    args = ap.parse_args(argv)
+    import torch
+
+    from jax_alfa_b200 import cases
+    from jax_alfa_b200.api import Simulation
+    cfg = cases.nbl_a94(*args.grid, nsteps=args.steps + 2, precision=args.precision)
+    u, v, w, th = cases.initial_fields(cfg, 0)
+    sim = Simulation(cfg, u, v, w, th)
+    sim.step(1)
+    if args.tune:
+        for c in sim.autotune(reps=3):
+            if c["chosen"]:
+                print(f"{c['shape']}: {c['variant']} {c['ms']:.4f} ms")
+    sim.step(args.steps, graph=True)
+    torch.cuda.synchronize()
+    print("ok", sim.diag(), flush=True)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
