@@ -455,7 +455,9 @@ int alfa_time_kernel(alfa_ctx*, int which, int reps, double* ms /* host */,
  * in place of a phase-split pad/unpad, 2/3/4 the runtime-plan transform
  * with radix schedule "largest radix 8" / "largest radix 4" / "default
  * factors in ascending order", 5 the split-BF16 tensor-core pass of an
- * ALFA_MIXED context), its average launch time, whether its outputs equal
+ * ALFA_MIXED context, 6 the FP32 transform on two-lane elements: two packed
+ * columns per thread in paired FP32 instructions, for plain-field inputs
+ * with nz a multiple of 4), its average launch time, whether its outputs equal
  * the default's to the precision's round-off of their maximum (1e-12 FP64,
  * 1e-5 FP32, 5e-5 for the tensor-core pass), and whether it was chosen. */
 typedef struct alfa_tune_entry {

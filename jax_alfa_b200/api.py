@@ -99,7 +99,7 @@ class Alfa:
     TUNE_SHAPES = ("y pad", "x pad", "x unpad", "y unpad", "x derivative", "y derivative",
                    "x filter+derivative", "y filter+derivative")
     TUNE_VARIANTS = ("default", "compile-time", "radix-8", "radix-4", "ascending",
-                     "tensor-core")
+                     "tensor-core", "two-lane")
 
     def autotune(self, reps=5):
         """Time every line-pass variant of the step's pass shapes and keep the

@@ -58,40 +58,74 @@ __device__ __forceinline__ cd w16(int m, int S) {
   return mkc(c, S * s);
 }
 
+#ifdef ALFA_BUILD_FP32
+// Two complex values in the same position of two adjacent packed columns
+// (lanes A and B: levels z, z+1 and z+2, z+3 of a z-fastest FP32 field),
+// held as real and imaginary lane pairs so that every operation of a
+// butterfly is one paired FP32 instruction (FADD2 / FMUL2 / FFMA2 on sm_100)
+// for both lanes.  The codelets below run unchanged on it.
+struct cv {
+  float2 re, im;
+};
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ cv cadd(cv a, cv b) {
+  return cv{__fadd2_rn(a.re, b.re), __fadd2_rn(a.im, b.im)};
+}
+__device__ __forceinline__ cv csub(cv a, cv b) {
+  return cv{__fadd2_rn(a.re, neg2(b.re)), __fadd2_rn(a.im, neg2(b.im))};
+}
+// a * w, w one complex value for both lanes
+__device__ __forceinline__ cv cmul(cv a, cd w) {
+  return cv{__ffma2_rn(a.re, dup2(w.x), __fmul2_rn(a.im, dup2(-w.y))),
+            __ffma2_rn(a.re, dup2(w.y), __fmul2_rn(a.im, dup2(w.x)))};
+}
+__device__ __forceinline__ cv cmul(cd w, cv a) { return cmul(a, w); }
+__device__ __forceinline__ cv cscale(cv a, real s) {
+  return cv{__fmul2_rn(a.re, dup2(s)), __fmul2_rn(a.im, dup2(s))};
+}
 template <int S>
-__device__ __forceinline__ void dft2(cd& a, cd& b) {
-  cd t = a;
+__device__ __forceinline__ cv rot90(cv a) {
+  return S < 0 ? cv{a.im, neg2(a.re)} : cv{neg2(a.im), a.re};
+}
+#endif
+
+// R-point DFTs in registers over elements of type V: cd (one complex
+// value) or, in the FP32 build, cv (two lanes)
+template <int S, class V>
+__device__ __forceinline__ void dft2(V& a, V& b) {
+  V t = a;
   a = cadd(t, b);
   b = csub(t, b);
 }
 
-template <int S>
-__device__ __forceinline__ void dft3(cd& a, cd& b, cd& c) {
+template <int S, class V>
+__device__ __forceinline__ void dft3(V& a, V& b, V& c) {
   const real h = (real)0.86602540378443864676;  // sqrt(3)/2
-  cd t1 = cadd(b, c);
-  cd t2 = mkc(a.x - (real)0.5 * t1.x, a.y - (real)0.5 * t1.y);
-  cd d = csub(b, c);
-  cd t3 = rot90<S>(cscale(d, h));
+  V t1 = cadd(b, c);
+  V t2 = csub(a, cscale(t1, (real)0.5));
+  V d = csub(b, c);
+  V t3 = rot90<S>(cscale(d, h));
   a = cadd(a, t1);
   b = cadd(t2, t3);
   c = csub(t2, t3);
 }
 
-template <int S>
-__device__ __forceinline__ void dft4(cd& v0, cd& v1, cd& v2, cd& v3) {
-  cd t0 = cadd(v0, v2), t1 = csub(v0, v2);
-  cd t2 = cadd(v1, v3), t3 = rot90<S>(csub(v1, v3));
+template <int S, class V>
+__device__ __forceinline__ void dft4(V& v0, V& v1, V& v2, V& v3) {
+  V t0 = cadd(v0, v2), t1 = csub(v0, v2);
+  V t2 = cadd(v1, v3), t3 = rot90<S>(csub(v1, v3));
   v0 = cadd(t0, t2);
   v2 = csub(t0, t2);
   v1 = cadd(t1, t3);
   v3 = csub(t1, t3);
 }
 
-template <int S>
-__device__ __forceinline__ void dft8(cd* v) {
+template <int S, class V>
+__device__ __forceinline__ void dft8(V* v) {
   // radix-2 over two 4-point DFTs (even and odd inputs)
-  cd e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-  cd o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  V e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  V o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
   dft4<S>(e0, e1, e2, e3);
   dft4<S>(o0, o1, o2, o3);
   const real r2 = (real)0.70710678118654752440;
@@ -104,8 +138,8 @@ __device__ __forceinline__ void dft8(cd* v) {
   v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 
-template <int S>
-__device__ __forceinline__ void dft16(cd* v) {
+template <int S, class V>
+__device__ __forceinline__ void dft16(V* v) {
   // 4 x 4: inner 4-point DFTs over n2 (stride 4), twiddle W16^(n1 k2),
   // outer 4-point DFTs over n1.
 #pragma unroll
@@ -115,10 +149,10 @@ __device__ __forceinline__ void dft16(cd* v) {
 #pragma unroll
     for (int k2 = 1; k2 < 4; k2++) v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], w16(n1 * k2, S));
   }
-  cd o[16];
+  V o[16];
 #pragma unroll
   for (int k2 = 0; k2 < 4; k2++) {
-    cd a = v[4 * k2], b = v[4 * k2 + 1], c = v[4 * k2 + 2], d = v[4 * k2 + 3];
+    V a = v[4 * k2], b = v[4 * k2 + 1], c = v[4 * k2 + 2], d = v[4 * k2 + 3];
     dft4<S>(a, b, c, d);
     o[k2] = a; o[k2 + 4] = b; o[k2 + 8] = c; o[k2 + 12] = d;
   }
@@ -126,8 +160,8 @@ __device__ __forceinline__ void dft16(cd* v) {
   for (int i = 0; i < 16; i++) v[i] = o[i];
 }
 
-template <int R, int S>
-__device__ __forceinline__ void dftR(cd* v) {
+template <int R, int S, class V>
+__device__ __forceinline__ void dftR(V* v) {
   if (R == 2) dft2<S>(v[0], v[1]);
   else if (R == 3) dft3<S>(v[0], v[1], v[2]);
   else if (R == 4) dft4<S>(v[0], v[1], v[2], v[3]);

@@ -23,13 +23,15 @@ __host__ __device__ constexpr int ct_threads(int C, int N) {
   return t < 64 ? 64 : t;
 }
 
-template <int R, int S, int C, int N, int NS, int NT>
-__device__ __forceinline__ void ct_pass(cd* __restrict__ buf, const cd* __restrict__ tw) {
+// Element type V: cd, or the two-lane cv of the FP32 build (alfa_fft.cuh);
+// C counts elements of V per tile row.
+template <int R, int S, int C, int N, int NS, int NT, class V>
+__device__ __forceinline__ void ct_pass(V* __restrict__ buf, const cd* __restrict__ tw) {
   constexpr int NR = N / R;
   constexpr int B = NR * C;
   constexpr int MB = (B + NT - 1) / NT;
   constexpr int STRIDE = N / (NS * R);
-  cd v[MB * R];
+  V v[MB * R];
 #pragma unroll
   for (int q = 0; q < MB; q++) {
     const int b = threadIdx.x + q * NT;
@@ -65,8 +67,8 @@ __device__ __forceinline__ void ct_pass(cd* __restrict__ buf, const cd* __restri
   }
 }
 
-template <int S, int C, int N, int NS, int NT>
-__device__ __forceinline__ void ct_passes(cd* buf, const cd* tw) {
+template <int S, int C, int N, int NS, int NT, class V>
+__device__ __forceinline__ void ct_passes(V* buf, const cd* tw) {
   if constexpr (NS < N) {
     constexpr int R = ct_radix(N / NS);
     __syncthreads();
@@ -77,8 +79,8 @@ __device__ __forceinline__ void ct_passes(cd* buf, const cd* tw) {
 
 // Unnormalised in-place transform of the N x C tile; blockDim.x must be NT.
 // Leaves a __syncthreads() behind.
-template <int S, int C, int N, int NT>
-__device__ __forceinline__ void fft_ct(cd* buf, const cd* tw) {
+template <int S, int C, int N, int NT, class V>
+__device__ __forceinline__ void fft_ct(V* buf, const cd* tw) {
   ct_passes<S, C, N, 1, NT>(buf, tw);
   __syncthreads();
 }
@@ -104,8 +106,8 @@ __host__ __device__ constexpr int ct_mb(int C, int N, int NS, int NT) {
 
 // First pass from registers v[q*R + r]; outputs go to buf.  The caller makes
 // sure no thread still reads buf.  Requires more than one pass.
-template <int S, int C, int N, int NT>
-__device__ __forceinline__ void ct_first_reg(cd* v, cd* __restrict__ buf) {
+template <int S, int C, int N, int NT, class V>
+__device__ __forceinline__ void ct_first_reg(V* v, V* __restrict__ buf) {
   constexpr int R = ct_radix(N);
   constexpr int B = (N / R) * C;
   constexpr int MB = (B + NT - 1) / NT;
@@ -123,8 +125,8 @@ __device__ __forceinline__ void ct_first_reg(cd* v, cd* __restrict__ buf) {
 }
 
 // Passes that start at NS, up to but excluding the last one, in buf.
-template <int S, int C, int N, int NS, int NT>
-__device__ __forceinline__ void ct_mid_passes(cd* buf, const cd* tw) {
+template <int S, int C, int N, int NS, int NT, class V>
+__device__ __forceinline__ void ct_mid_passes(V* buf, const cd* tw) {
   if constexpr (NS < ct_last_ns(N)) {
     constexpr int R = ct_radix(N / NS);
     __syncthreads();
@@ -135,9 +137,9 @@ __device__ __forceinline__ void ct_mid_passes(cd* buf, const cd* tw) {
 
 // Last pass from buf into registers v[q*R + r] = X[j + r*NS] (the caller
 // synchronises before).  Requires more than one pass.
-template <int S, int C, int N, int NT>
-__device__ __forceinline__ void ct_last_reg(const cd* __restrict__ buf, const cd* __restrict__ tw,
-                                            cd* v) {
+template <int S, int C, int N, int NT, class V>
+__device__ __forceinline__ void ct_last_reg(const V* __restrict__ buf, const cd* __restrict__ tw,
+                                            V* v) {
   constexpr int NS = ct_last_ns(N);
   constexpr int R = N / NS;
   constexpr int B = NS * C;

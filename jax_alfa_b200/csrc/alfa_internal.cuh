@@ -211,6 +211,12 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
 // the line-pass variant that runs on the tensor cores (after the default, the
 // compile-time transform and the N_SCHED runtime radix schedules)
 constexpr int TC_VARIANT = 2 + Engine::N_SCHED;
+// the FP32 line-pass variant on two-lane elements (two packed columns per
+// thread, paired FP32 instructions)
+constexpr int CV_VARIANT = TC_VARIANT + 1;
+#ifdef ALFA_BUILD_FP32
+bool cv_line_ok(const Loader& L, int n_in, int n_out, int nout, const LineOut* outs);
+#endif
 // the autotuner's key of a line pass
 long long line_key(int axis, int n_in, int n_out, int map, int nout);
 // Y (n_out, ncols) = M X (X: (n_in, ncols) FP32) for the line map's

@@ -4,6 +4,7 @@
 // transform of runs of 2 YC z levels (a 128-byte row segment), a map, and an
 // inverse transform.
 #include <cmath>
+#include <type_traits>
 
 #include "alfa_tile.cuh"
 
@@ -62,32 +63,34 @@ __device__ __forceinline__ void line_load(const LineArgs& a, long long f, int z0
   }
 }
 
-__device__ __forceinline__ cd line_map(const LineOut& o, const cd* S, int k, int c, int n, int m) {
-  auto deriv = [&](cd v) -> cd {
+// bin k of output map o applied to the spectrum S (n bins, C elements per
+// row) for an m-point output
+template <int C = YC, class V = cd>
+__device__ __forceinline__ V line_map(const LineOut& o, const V* S, int k, int c, int n, int m) {
+  auto deriv = [&](V v) -> V {
     const int kk = (k < n / 2) ? k : (k == n / 2 ? 0 : k - n);
-    const real q = (real)kk;
-    return mkc(-(q * v.y), q * v.x);
+    return mul_ik(v, (real)kk);
   };
   switch (o.map) {
     case LM_IDENT:
-      return S[k * YC + c];
+      return S[k * C + c];
     case LM_TRUNC:
-      return (k < o.cut || k >= n - o.cut + 1) ? S[k * YC + c] : mkc(0, 0);
+      return (k < o.cut || k >= n - o.cut + 1) ? S[k * C + c] : vzero<V>();
     case LM_DERIV:
-      return deriv(S[k * YC + c]);
+      return deriv(S[k * C + c]);
     case LM_TRUNC_DERIV:
-      return (k < o.cut || k >= n - o.cut + 1) ? deriv(S[k * YC + c]) : mkc(0, 0);
+      return (k < o.cut || k >= n - o.cut + 1) ? deriv(S[k * C + c]) : vzero<V>();
     case LM_PAD: {  // n -> m = 3n/2, Nyquist row repeated (Dealiasing.py:67-73)
       const int h = n / 2;
-      if (k <= h) return S[k * YC + c];
-      if (k >= m - h) return S[(k - m + n) * YC + c];
-      return mkc(0, 0);
+      if (k <= h) return S[k * C + c];
+      if (k >= m - h) return S[(k - m + n) * C + c];
+      return vzero<V>();
     }
     default: {  // LM_UNPAD: n = 3m/2 -> m, Nyquist dropped (Dealiasing.py:102-109)
       const int h = m / 2;
-      if (k < h) return S[k * YC + c];
-      if (k == h) return mkc(0, 0);
-      return S[(k - m + n) * YC + c];
+      if (k < h) return S[k * C + c];
+      if (k == h) return vzero<V>();
+      return S[(k - m + n) * C + c];
     }
   }
 }
@@ -209,9 +212,9 @@ __device__ __forceinline__ void line_gather_any(const LineArgs& a, long long f, 
 }
 
 // store (or accumulate) v[q*R + r] = value at row j + r*STEP of line c
-template <int C, int R, int STEP, int B, int NT>
+template <int C, int R, int STEP, int B, int NT, class V>
 __device__ __forceinline__ void line_scatter(const LineArgs& a, const LineOut& o, long long f,
-                                             int z0, const cd* v) {
+                                             int z0, const V* v) {
   constexpr int MB = (B + NT - 1) / NT;
 #pragma unroll
   for (int q = 0; q < MB; q++) {
@@ -219,34 +222,73 @@ __device__ __forceinline__ void line_scatter(const LineArgs& a, const LineOut& o
     if (!(B % NT == 0 || b < B)) continue;
     const int c = b % C;
     const int j = b / C;
-    const int z = z0 + 2 * c;
+    const int z = z0 + zp_of<V>() * c;
 #pragma unroll
     for (int r = 0; r < R; r++) {
       const size_t i = (size_t)(f * a.fs_out + (long long)(j + r * STEP) * a.rs_out) + z;
-      store_pair(o, i, z, a.nz, v[q * R + r]);
+      store_elem(o, i, z, a.nz, v[q * R + r]);
     }
   }
 }
 
-template <int NIN, int NOUT, bool GEN>
-__global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
+#ifdef ALFA_BUILD_FP32
+// first-pass gather of a plain FP32 field in two-lane elements:
+// v[q*R + r] = levels z .. z+3 at row j + r*(N/R) of element column c
+template <int C, int N, int NT>
+__device__ __forceinline__ void gather_rows_cv(const real* a0, int nz, size_t base, size_t rs,
+                                               int z0, cv* v) {
+  constexpr int R = ct_radix(N);
+  constexpr int NR = N / R;
+  constexpr int B = NR * C;
+  constexpr int MB = (B + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 4 * c;
+    const bool ok = (B % NT == 0 || b < B) && z < nz;
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      v[q * R + r] = ok ? ld_cv(a0 + base + (size_t)(j + r * NR) * rs + z) : vzero<cv>();
+  }
+}
+#endif
+
+// elements of type V per tile row: one 128-byte row segment
+template <class V>
+__host__ __device__ constexpr int tile_cols() { return (int)(128 / sizeof(V)); }
+
+// V: cd, or (FP32 build, plain-field input, nz a multiple of 4) the two-lane
+// cv, which takes 4 z levels per element and half the threads per tile
+template <int NIN, int NOUT, bool GEN, class V = cd>
+__global__ void __launch_bounds__(line_threads<tile_cols<V>(), NIN, NOUT>())
     k_line_rr(LineArgs a) {
-  constexpr int C = YC;
+  constexpr int C = tile_cols<V>();
   constexpr int NT = line_threads<C, NIN, NOUT>();
   constexpr int NMAX = NIN > NOUT ? NIN : NOUT;
-  extern __shared__ cd sm[];
-  cd* S = sm;
-  const int z0 = blockIdx.x * (2 * C);
+  extern __shared__ __align__(16) unsigned char sm_line[];
+  V* sm = reinterpret_cast<V*>(sm_line);
+  V* S = sm;
+  const int z0 = blockIdx.x * (zp_of<V>() * C);
   const long long f = blockIdx.y;
   {
-    cd* Wb = a.nouts > 1 ? sm + NMAX * C : sm;
+    V* Wb = a.nouts > 1 ? sm + NMAX * C : sm;
     // forward transform of the NIN-line tile into S
     {
       constexpr int R = ct_radix(NIN);
       constexpr int MB = ct_mb(C, NIN, 1, NT);
-      cd v[MB * R];
-      if constexpr (GEN) line_gather_any<C, NIN, NT>(a, f, z0, v);
-      else line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v);
+      V v[MB * R];
+      if constexpr (!std::is_same<V, cd>::value) {
+#ifdef ALFA_BUILD_FP32
+        static_assert(!GEN, "two-lane tiles take plain fields only");
+        gather_rows_cv<C, NIN, NT>(a.L.a[0], a.nz, (size_t)(f * a.fs_in), (size_t)a.rs_in, z0, v);
+#endif
+      } else if constexpr (GEN) {
+        line_gather_any<C, NIN, NT>(a, f, z0, v);
+      } else {
+        line_gather<LD_FIELD, C, NIN, NT>(a, f, z0, v);
+      }
       if constexpr (R == NIN) {
         if (threadIdx.x < C) {
           dftR<R, -1>(v);
@@ -266,7 +308,7 @@ __global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
       constexpr int NR = NOUT / R;
       constexpr int B = NR * C;
       constexpr int MB = ct_mb(C, NOUT, 1, NT);
-      cd v[MB * R];
+      V v[MB * R];
 #pragma unroll
       for (int q = 0; q < MB; q++) {
         const int b = threadIdx.x + q * NT;
@@ -274,8 +316,9 @@ __global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
         const int j = b / C;
 #pragma unroll
         for (int r = 0; r < R; r++)
-          v[q * R + r] = (B % NT == 0 || b < B) ? line_map(o, S, j + r * NR, c, NIN, NOUT)
-                                                : mkc(0, 0);
+          v[q * R + r] = (B % NT == 0 || b < B)
+                             ? line_map<C>(o, (const V*)S, j + r * NR, c, NIN, NOUT)
+                             : vzero<V>();
       }
       if constexpr (R == NOUT) {
 #pragma unroll
@@ -289,7 +332,7 @@ __global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
         constexpr int NSL = ct_last_ns(NOUT);
         constexpr int RL = NOUT / NSL;
         constexpr int ML = ct_mb(C, NOUT, NSL, NT);
-        cd u[ML * RL];
+        V u[ML * RL];
         ct_last_reg<+1, C, NOUT, NT>(Wb, a.pout.tw, u);
         line_scatter<C, RL, NSL, NSL * C, NT>(a, o, f, z0, u);
       }
@@ -317,10 +360,10 @@ __global__ void __launch_bounds__(line_threads<YC, NIN, NOUT>())
 // is one radix-8 pass in registers, one shared-memory exchange and one
 // radix-16 pass.  The length-m transform and its radix-3 pass disappear.
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, int C = YC>
 __host__ __device__ constexpr bool pad3_ok() {
   return ct_last_ns(N) == ct_radix(N) && ct_radix(N) * ct_radix(N) == N && ct_radix(N) >= 4 &&
-         ct_mb(YC, N, 1, ct_threads(YC, N)) == 1;
+         ct_mb(C, N, 1, ct_threads(C, N)) == 1;
 }
 
 __device__ __forceinline__ cd cconj(cd a) { return mkc(a.x, -a.y); }
@@ -331,29 +374,37 @@ __device__ __forceinline__ void line_gather_sel(const LineArgs& a, long long f, 
   else line_gather_any<C, N, NT>(a, f, z0, v);
 }
 
-// KIND: the loader kind, or -1 for any kind (chosen at run time)
-template <int N, int KIND>
-__global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
-  constexpr int C = YC;
+// KIND: the loader kind, or -1 for any kind (chosen at run time); V as in
+// k_line_rr (the two-lane cv for plain fields only)
+template <int N, int KIND, class V = cd>
+__global__ void __launch_bounds__(ct_threads(tile_cols<V>(), N)) k_pad3(LineArgs a) {
+  constexpr int C = tile_cols<V>();
   constexpr int NT = ct_threads(C, N);
   constexpr int R = ct_radix(N);   // both passes of the length-N transform
   constexpr int L = N / 2;
   constexpr int RA = R / 2;        // first radix of the length-L phase transforms
   constexpr int RB = L / RA;       // their second radix (= R)
-  static_assert(pad3_ok<N>() && RB == R, "pad3 layout");
-  extern __shared__ cd sm[];
-  cd* S = sm;  // forward exchange, then three phase tiles of L x C
-  const int z0 = blockIdx.x * (2 * C);
+  static_assert(pad3_ok<N, C>() && RB == R, "pad3 layout");
+  extern __shared__ __align__(16) unsigned char sm_pad[];
+  V* S = reinterpret_cast<V*>(sm_pad);  // forward exchange, then three phase tiles of L x C
+  const int z0 = blockIdx.x * (zp_of<V>() * C);
   const long long f = blockIdx.y;
   const LineOut& o = a.out[0];
   const cd* twN = a.pin.tw;   // exp(-2 pi i q / N)
   const cd* twM = a.pout.tw;  // exp(-2 pi i q / 3L)
   const int c = threadIdx.x % C;
   const int j = threadIdx.x / C;  // 0 .. R-1
-  cd X[R];
+  V X[R];
   {
-    cd v[R];
-    line_gather_sel<KIND, C, N, NT>(a, f, z0, v);
+    V v[R];
+    if constexpr (!std::is_same<V, cd>::value) {
+#ifdef ALFA_BUILD_FP32
+      static_assert(KIND == LD_FIELD, "two-lane tiles take plain fields only");
+      gather_rows_cv<C, N, NT>(a.L.a[0], a.nz, (size_t)(f * a.fs_in), (size_t)a.rs_in, z0, v);
+#endif
+    } else {
+      line_gather_sel<KIND, C, N, NT>(a, f, z0, v);
+    }
     ct_first_reg<-1, C, N, NT>(v, S);
     __syncthreads();
     ct_last_reg<-1, C, N, NT>(S, twN, X);  // X[r] = bin j + R r
@@ -363,14 +414,14 @@ __global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
   const cd w3b = cconj(__ldg(&twM[L]));      // w_3^{4} = w_3
 #pragma unroll
   for (int p = 0; p < 3; p++) {
-    cd z[RA];
+    V z[RA];
 #pragma unroll
     for (int r = 0; r < RA; r++) {
       const int k = j + R * r;
-      const cd lo = X[r], hi = X[r + RA];
-      cd t;
+      const V lo = X[r], hi = X[r + RA];
+      V t;
       if (p == 0) {
-        t = (k == 0) ? mkc(lo.x + (real)2 * hi.x, lo.y + (real)2 * hi.y) : cadd(lo, hi);
+        t = (k == 0) ? cadd(lo, cscale(hi, (real)2)) : cadd(lo, hi);
       } else if (k == 0) {
         t = csub(lo, hi);
       } else {
@@ -379,7 +430,7 @@ __global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
       z[r] = t;
     }
     dftR<RA, +1>(z);
-    cd* P = S + p * L * C;
+    V* P = S + p * L * C;
 #pragma unroll
     for (int r = 0; r < RA; r++) P[(j * RA + r) * C + c] = z[r];
   }
@@ -395,19 +446,19 @@ __global__ void __launch_bounds__(ct_threads(YC, N)) k_pad3(LineArgs a) {
     const int bb = b % (RA * C);
     const int cc = bb % C;
     const int jj = bb / C;  // 0 .. RA-1
-    const cd* P = S + p * L * C;
-    cd v[RB];
+    const V* P = S + p * L * C;
+    V v[RB];
 #pragma unroll
     for (int r = 0; r < RB; r++) v[r] = P[(jj + r * RA) * C + cc];
 #pragma unroll
     for (int r = 1; r < RB; r++) v[r] = cmul(v[r], cconj(__ldg(&twM[3 * jj * r])));
     dftR<RB, +1>(v);
-    const int z = z0 + 2 * cc;
+    const int z = z0 + zp_of<V>() * cc;
 #pragma unroll
     for (int r = 0; r < RB; r++) {
       const int row = 3 * (jj + RA * r) + p;
       const size_t i = (size_t)(f * a.fs_out + (long long)row * a.rs_out) + z;
-      store_pair(o, i, z, nz, v[r]);
+      store_elem(o, i, z, nz, v[r]);
     }
   }
 }
@@ -439,6 +490,31 @@ __device__ __forceinline__ void phase_gather(const LineArgs& a, long long f, int
   }
 }
 
+#ifdef ALFA_BUILD_FP32
+// phase_gather for a plain FP32 field in two-lane elements (4 levels each)
+template <int C, int RA, int RB, int NT>
+__device__ __forceinline__ void phase_gather_cv(const LineArgs& a, long long f, int z0, cv* v) {
+  constexpr int BB = 3 * RA * C;
+  constexpr int MBB = (BB + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < MBB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const int p = b / (RA * C);
+    const int bb = b % (RA * C);
+    const int c = bb % C;
+    const int jj = bb / C;
+    const int z = z0 + 4 * c;
+    const bool ok = (BB % NT == 0 || b < BB) && z < a.nz;
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      const long long row = 3 * (jj + RA * r) + p;
+      v[q * RB + r] = ok ? ld_cv(a.L.a[0] + (size_t)(f * a.fs_in + row * a.rs_in) + z)
+                         : vzero<cv>();
+    }
+  }
+}
+#endif
+
 template <int C, int RA, int RB, int NT>
 __device__ __forceinline__ void phase_gather_any(const LineArgs& a, long long f, int z0, cd* v) {
   switch (a.L.kind) {
@@ -451,28 +527,39 @@ __device__ __forceinline__ void phase_gather_any(const LineArgs& a, long long f,
 }
 
 // three CTAs per SM measured faster than the unconstrained register budget
-template <int N, int KIND>
-__global__ void __launch_bounds__(ct_threads(YC, N), 3) k_unpad3(LineArgs a) {
-  constexpr int C = YC;
+// (one-lane elements)
+template <int N, int KIND, class V = cd>
+__global__ void __launch_bounds__(ct_threads(tile_cols<V>(), N),
+                                  (std::is_same<V, cd>::value ? 3 : 4))
+    k_unpad3(LineArgs a) {
+  constexpr int C = tile_cols<V>();
   constexpr int NT = ct_threads(C, N);
   constexpr int R = ct_radix(N);   // both passes of the length-N inverse
   constexpr int L = N / 2;
   constexpr int RA = R / 2;        // last radix of the length-L phase transforms
   constexpr int RB = L / RA;       // their first radix (= R)
-  static_assert(pad3_ok<N>() && RB == R, "unpad3 layout");
+  static_assert(pad3_ok<N, C>() && RB == R, "unpad3 layout");
   constexpr int BB = 3 * RA * C;
   constexpr int MBB = (BB + NT - 1) / NT;
-  extern __shared__ cd sm[];
-  cd* S = sm;  // three phase tiles of L x C, then the inverse exchange
-  const int z0 = blockIdx.x * (2 * C);
+  extern __shared__ __align__(16) unsigned char sm_unpad[];
+  V* S = reinterpret_cast<V*>(sm_unpad);  // three phase tiles of L x C, then the exchange
+  const int z0 = blockIdx.x * (zp_of<V>() * C);
   const long long f = blockIdx.y;
   const LineOut& o = a.out[0];
   const cd* twM = a.pin.tw;   // exp(-2 pi i q / 3L)
   const cd* twN = a.pout.tw;  // exp(-2 pi i q / N)
   {
-    cd v[MBB * RB];
-    if constexpr (KIND >= 0) phase_gather<KIND, C, RA, RB, NT>(a, f, z0, v);
-    else phase_gather_any<C, RA, RB, NT>(a, f, z0, v);
+    V v[MBB * RB];
+    if constexpr (!std::is_same<V, cd>::value) {
+#ifdef ALFA_BUILD_FP32
+      static_assert(KIND == LD_FIELD, "two-lane tiles take plain fields only");
+      phase_gather_cv<C, RA, RB, NT>(a, f, z0, v);
+#endif
+    } else if constexpr (KIND >= 0) {
+      phase_gather<KIND, C, RA, RB, NT>(a, f, z0, v);
+    } else {
+      phase_gather_any<C, RA, RB, NT>(a, f, z0, v);
+    }
 #pragma unroll
     for (int q = 0; q < MBB; q++) {
       const int b = threadIdx.x + q * NT;
@@ -482,7 +569,7 @@ __global__ void __launch_bounds__(ct_threads(YC, N), 3) k_unpad3(LineArgs a) {
       const int cc = bb % C;
       const int jj = bb / C;
       dftR<RB, -1>(v + q * RB);
-      cd* P = S + p * L * C;
+      V* P = S + p * L * C;
 #pragma unroll
       for (int r = 0; r < RB; r++) P[(jj * RB + r) * C + cc] = v[q * RB + r];
     }
@@ -490,12 +577,12 @@ __global__ void __launch_bounds__(ct_threads(YC, N), 3) k_unpad3(LineArgs a) {
   __syncthreads();
   const int c = threadIdx.x % C;
   const int j = threadIdx.x / C;  // 0 .. R-1
-  cd out[R];
+  V out[R];
   {
-    cd F[3][RA];
+    V F[3][RA];
 #pragma unroll
     for (int p = 0; p < 3; p++) {
-      const cd* P = S + p * L * C;
+      const V* P = S + p * L * C;
 #pragma unroll
       for (int r = 0; r < RA; r++) F[p][r] = P[(j + r * RB) * C + c];
 #pragma unroll
@@ -507,18 +594,18 @@ __global__ void __launch_bounds__(ct_threads(YC, N), 3) k_unpad3(LineArgs a) {
 #pragma unroll
     for (int r = 0; r < RA; r++) {
       const int k = j + R * r;
-      const cd g0 = F[0][r];
-      const cd g1 = cmul(F[1][r], __ldg(&twM[k]));
-      const cd g2 = cmul(F[2][r], __ldg(&twM[2 * k]));
+      const V g0 = F[0][r];
+      const V g1 = cmul(F[1][r], __ldg(&twM[k]));
+      const V g2 = cmul(F[2][r], __ldg(&twM[2 * k]));
       out[r] = cadd(cadd(g0, g1), g2);
-      out[r + RA] = (k == 0) ? mkc(0, 0)
+      out[r + RA] = (k == 0) ? vzero<V>()
                              : cadd(cadd(g0, cmul(w3a, g1)), cmul(w3b, g2));
     }
   }
   __syncthreads();  // phase tiles fully read
   ct_first_reg<+1, C, N, NT>(out, S);
   __syncthreads();
-  cd u[R];
+  V u[R];
   ct_last_reg<+1, C, N, NT>(S, twN, u);
   line_scatter<C, R, R, R * C, NT>(a, o, f, z0, u);
 }
@@ -572,6 +659,70 @@ static void phase_n(Engine& e, const LineArgs& a, int F) {
     else unpad3_k<N, -1>(e, a, g, smem);
   }
 }
+
+#ifdef ALFA_BUILD_FP32
+// The two-lane (cv) kernels: 4 z levels per element, paired FP32
+// instructions for two packed columns at once.  Plain-field inputs with nz a
+// multiple of 4, the phase-split 256 <-> 384 pad and unpad and the
+// same-length compile-time passes of the bench-class grids.
+template <int NIN, int NOUT>
+static void line_n_cv(Engine& e, const LineArgs& a, int F) {
+  constexpr int C = tile_cols<cv>();
+  dim3 g((a.nz + 4 * C - 1) / (4 * C), F);
+  constexpr int nmax = NIN > NOUT ? NIN : NOUT;
+  constexpr int nt = line_threads<C, NIN, NOUT>();
+  const size_t smem = (size_t)(nmax + (a.nouts > 1 ? NOUT : 0)) * C * sizeof(cv);
+  set_smem((const void*)k_line_rr<NIN, NOUT, false, cv>, smem);
+  k_line_rr<NIN, NOUT, false, cv><<<g, nt, smem, e.stream>>>(a);
+}
+
+template <int N, bool PAD>
+static void phase_n_cv(Engine& e, const LineArgs& a, int F) {
+  constexpr int C = tile_cols<cv>();
+  dim3 g((a.nz + 4 * C - 1) / (4 * C), F);
+  const size_t smem = (size_t)(3 * N / 2) * C * sizeof(cv);
+  if (PAD) {
+    set_smem((const void*)k_pad3<N, LD_FIELD, cv>, smem);
+    k_pad3<N, LD_FIELD, cv><<<g, ct_threads(C, N), smem, e.stream>>>(a);
+  } else {
+    set_smem((const void*)k_unpad3<N, LD_FIELD, cv>, smem);
+    k_unpad3<N, LD_FIELD, cv><<<g, ct_threads(C, N), smem, e.stream>>>(a);
+  }
+}
+
+#define ALFA_CV_PAIRS(X) X(128, 128) X(192, 192) X(256, 256) X(384, 384)
+
+// whether the pass has a two-lane kernel
+bool cv_line_ok(const Loader& L, int n_in, int n_out, int nout, const LineOut* outs) {
+  if (L.kind != LD_FIELD || (L.nz & 3) != 0) return false;
+  if (nout == 1 && ((outs[0].map == LM_PAD && n_in == 256 && n_out == 384) ||
+                    (outs[0].map == LM_UNPAD && n_in == 384 && n_out == 256)))
+    return true;
+#define ALFA_CASE(p, q) \
+  if (n_in == p && n_out == q) return true;
+  ALFA_CV_PAIRS(ALFA_CASE)
+#undef ALFA_CASE
+  return false;
+}
+
+static void cv_line(Engine& e, const LineArgs& a, int F, int nout, const LineOut* outs) {
+  if (nout == 1 && outs[0].map == LM_PAD && a.n_in == 256 && a.n_out == 384) {
+    phase_n_cv<256, true>(e, a, F);
+    return;
+  }
+  if (nout == 1 && outs[0].map == LM_UNPAD && a.n_in == 384 && a.n_out == 256) {
+    phase_n_cv<256, false>(e, a, F);
+    return;
+  }
+#define ALFA_CASE(p, q)                  \
+  if (a.n_in == p && a.n_out == q) {     \
+    line_n_cv<p, q>(e, a, F);            \
+    return;                              \
+  }
+  ALFA_CV_PAIRS(ALFA_CASE)
+#undef ALFA_CASE
+}
+#endif
 
 static const FftPlan& alt_plan_for(const Engine& e, int n, int r) {
   if (n == e.nx) return e.alt_plans[0][r];
@@ -652,6 +803,12 @@ void launch_line(Engine& e, int axis, const Loader& L, int X, int Y, int n_in, i
   if (variant == TC_VARIANT && tc_line(e, axis, L, X, Y, n_in, n_out, nout, outs)) return;
 #endif
   ::alfa::note_launch();
+#ifdef ALFA_BUILD_FP32
+  if (variant == CV_VARIANT && cv_line_ok(L, n_in, n_out, nout, outs)) {
+    cv_line(e, a, F, nout, outs);
+    return;
+  }
+#endif
   if (variant >= 2 && variant < TC_VARIANT) {  // runtime plans, alternative radix schedule
     const int r = variant - 2;
     a.pin = alt_plan_for(e, n_in, r);

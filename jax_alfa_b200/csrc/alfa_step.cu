@@ -1606,8 +1606,8 @@ static int tune_tc_prepare(Engine& e, const TuneShape& sh) {
 
 int set_line_variant(Ctx* c, int axis, int n_in, int n_out, int map, int nout, int variant) {
   Engine& e = c->e;
-  if (variant < 0 || variant > TC_VARIANT)
-    return e.fail("alfa_set_line_variant: variant must be 0..5", ALFA_E_SHAPE);
+  if (variant < 0 || variant > CV_VARIANT)
+    return e.fail("alfa_set_line_variant: variant must be 0..6", ALFA_E_SHAPE);
   TuneShape shapes[8];
   tune_shapes(c, c->w.Pb[4], shapes);
   for (const TuneShape& sh : shapes) {
@@ -1617,6 +1617,19 @@ int set_line_variant(Ctx* c, int axis, int n_in, int n_out, int map, int nout, i
     if (variant == 1 && !tune_phase(sh))
       return e.fail("alfa_set_line_variant: variant 1 applies to the 256 <-> 384 pad and unpad",
                     ALFA_E_SHAPE);
+    if (variant == CV_VARIANT) {
+#ifdef ALFA_BUILD_FP32
+      LineOut o[2];
+      for (int q = 0; q < sh.nout; q++) {
+        o[q] = LineOut{};
+        o[q].map = sh.map[q];
+      }
+      if (!cv_line_ok(ld_field(e, sh.in), n_in, n_out, nout, o))
+#endif
+        return e.fail("alfa_set_line_variant: the two-lane pass needs an FP32 or mixed context, "
+                      "nz % 4 == 0 and a pass length it is built for",
+                      ALFA_E_SHAPE);
+    }
     if (variant == TC_VARIANT) {
 #ifdef ALFA_BUILD_FP32
       if (e.cfg.precision != ALFA_MIXED || !tc_shape_ok(n_in, n_out, tune_tc_cols(e, sh)))
@@ -1677,6 +1690,10 @@ int autotune(Ctx* c, int reps, alfa_tune_entry* out, int max_out, int* n_out) {
     for (int v = 0; v < 2 + Engine::N_SCHED; v++)
       if (v != 1 || phase) cand.push_back(v);
 #ifdef ALFA_BUILD_FP32
+    {
+      const Loader L = ld_field(e, sh.in);
+      if (cv_line_ok(L, sh.n_in, sh.n_out, sh.nout, o)) cand.push_back(CV_VARIANT);
+    }
     if (e.cfg.precision == ALFA_MIXED) {  // operators are built here, never inside a capture
       if (tc_shape_ok(sh.n_in, sh.n_out, tune_tc_cols(e, sh))) {
         if ((rc = tune_tc_prepare(e, sh)) != ALFA_OK) break;

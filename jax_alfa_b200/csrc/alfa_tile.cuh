@@ -230,6 +230,49 @@ __device__ __forceinline__ void store_pair(const LineOut& o, size_t i, int z, in
   store_pair2(o.dst, o.scale, o.accumulate, i, z, nz, v);
 }
 
+// Tile elements of type V (cd: one packed complex column, two z levels; cv:
+// two packed columns, four z levels): the zero, i q times an element, and
+// the store of a scaled element at linear index i (level z) of an output.
+template <class V>
+__device__ __forceinline__ V vzero();
+template <>
+__device__ __forceinline__ cd vzero<cd>() { return mkc(0, 0); }
+__device__ __forceinline__ cd mul_ik(cd v, real q) { return mkc(-(q * v.y), q * v.x); }
+__device__ __forceinline__ void store_elem(const LineOut& o, size_t i, int z, int nz, cd v) {
+  store_pair(o, i, z, nz, v);
+}
+// z levels per element
+template <class V>
+__host__ __device__ constexpr int zp_of() { return (int)(sizeof(V) / sizeof(real)); }
+
+#ifdef ALFA_BUILD_FP32
+template <>
+__device__ __forceinline__ cv vzero<cv>() { return cv{dup2(0.f), dup2(0.f)}; }
+__device__ __forceinline__ cv mul_ik(cv v, real q) {
+  return cv{__fmul2_rn(v.im, dup2(-q)), __fmul2_rn(v.re, dup2(q))};
+}
+// levels z .. z+3 of a plain FP32 field (nz a multiple of 4: an element is
+// wholly inside or wholly outside the field)
+__device__ __forceinline__ cv ld_cv(const real* p) {
+  const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+  return cv{make_float2(q.x, q.z), make_float2(q.y, q.w)};
+}
+__device__ __forceinline__ void store_elem(const LineOut& o, size_t i, int z, int nz, cv v) {
+  if (z >= nz) return;
+  const float s = (float)o.scale;
+  float4 w = make_float4(s * v.re.x, s * v.im.x, s * v.re.y, s * v.im.y);
+  float4* p = reinterpret_cast<float4*>(o.dst + i);
+  if (o.accumulate) {
+    const float4 pv = *p;
+    w.x += pv.x;
+    w.y += pv.y;
+    w.z += pv.z;
+    w.w += pv.w;
+  }
+  *p = w;
+}
+#endif
+
 // First-pass gather of a length-N transform over C packed columns:
 // v[q*R + r] = loader pair at row j + r*(N/R) of column c, for butterfly
 // b = threadIdx.x + q*NT (c = b % C, j = b / C); element index
