@@ -373,17 +373,28 @@ void alfa_ensemble_destroy(alfa_ensemble*);
  *   (ALFA_MLP_NPARAM floats) and loss (one float).
  * params: W1 (64 x 10), b1, W2 (64 x 64), b2, W3 (2 x 64), b3, FP32.
  * step_learned: steps whose Cs^2 comes from the network (static stresses and
- *   fluxes with it); every judge_every-th step runs the dynamic procedure
- *   instead and compares the network's plane-averaged Cs^2 on that state
- *   with the procedure's (relative L2 difference of the two profiles):
- *   a drift above tol reverts to the dynamic procedure for good; otherwise
- *   refresh_points samples of that step are collected and the network trains
- *   refresh_epochs more epochs (0, 0: no refresh). */
+ *   fluxes with it); the first step of a run with no judge step yet, and
+ *   then every judge_every-th step, runs the dynamic procedure instead (the
+ *   judge) and compares the network's plane-averaged Cs^2 on that state with
+ *   the procedure's: last_drift is the relative L2 difference of the two
+ *   profiles of that step, window_drift the same for the two profiles
+ *   averaged over the last ALFA_MLP_JUDGE_WINDOW judge steps (the
+ *   procedure's single-step plane means jump between steps where its
+ *   clipping switches on or off, so one step's profile is not a stable
+ *   reference).  Once the window is full, a window_drift above tol reverts
+ *   to the dynamic procedure for good.  Otherwise each judge step
+ *   recalibrates the network per level: its Cs^2 at level z is scaled by
+ *   the running ratio of the procedure's plane mean to the network's
+ *   (held within [0.1, 10]), so the network supplies the horizontal pattern
+ *   and the last judge the level means; then refresh_points samples of the
+ *   judge step are collected and the network trains refresh_epochs more
+ *   epochs (0, 0: no refresh).  alfa_mlp_infer applies the same scaling. */
 #define ALFA_MLP_NPARAM 4994
+#define ALFA_MLP_JUDGE_WINDOW 8
 typedef struct alfa_mlp alfa_mlp;
 typedef struct {
   int steps, learned_steps, judged, reverted, reverted_at;
-  double last_drift, max_drift;
+  double last_drift, max_drift, window_drift, max_window_drift;
 } alfa_mlp_report;
 int alfa_mlp_create(alfa_ctx*, int capacity, unsigned long long seed, alfa_mlp** out);
 void alfa_mlp_destroy(alfa_mlp*);

@@ -141,7 +141,8 @@ class AlfaTuneEntry(ctypes.Structure):
 
 class AlfaMlpReport(ctypes.Structure):
     _fields_ = [("steps", I), ("learned_steps", I), ("judged", I), ("reverted", I),
-                ("reverted_at", I), ("last_drift", D), ("max_drift", D)]
+                ("reverted_at", I), ("last_drift", D), ("max_drift", D),
+                ("window_drift", D), ("max_window_drift", D)]
 
 
 _lib = None

@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <deque>
 #include <vector>
 
 #include "alfa_iface.cuh"
@@ -62,6 +63,13 @@ struct alfa_mlp {
   double* scratch = nullptr;  // N: the network's Cs^2 on a judge step
   double* means = nullptr;    // 2 nz plane means
   int trained = 0;
+  // the judge's window: the network's and the procedure's plane-mean Cs^2
+  // profiles of the last ALFA_MLP_JUDGE_WINDOW judge steps (2 nz each)
+  std::deque<std::vector<double>> window;
+  // per-level calibration of the network's Cs^2 (nz): the ratio of the
+  // procedure's plane mean to the network's at the last judge step
+  double* calib = nullptr;
+  std::vector<double> calib_h;
 };
 
 #define CTX_CHECK(c)                                  \
@@ -820,7 +828,8 @@ static MlpFeatIn feat_in(alfa_ctx* c) {
 
 static void learned_cs2(alfa_ctx* c, double* Cs2_out) {
   alfa_mlp* m = c->mlp;
-  mlp_infer(c->d->e.stream, c->d->e.sms, feat_in(c), m->Pb, m->norm, c->d->e.N(), Cs2_out, nullptr);
+  mlp_infer(c->d->e.stream, c->d->e.sms, feat_in(c), m->Pb, m->norm, c->d->e.N(), m->calib,
+            Cs2_out, nullptr);
 }
 
 extern "C" {
@@ -833,7 +842,7 @@ void alfa_mlp_destroy(alfa_mlp* m) {
   }
   for (void* p : {(void*)m->X, (void*)m->T, (void*)m->norm, (void*)m->P, (void*)m->G,
                   (void*)m->M, (void*)m->V, (void*)m->loss, (void*)m->perm, (void*)m->Pb,
-                  (void*)m->scratch, (void*)m->means})
+                  (void*)m->scratch, (void*)m->means, (void*)m->calib})
     if (p) cudaFree(p);
   delete m;
 }
@@ -862,6 +871,7 @@ int alfa_mlp_create(alfa_ctx* c, int capacity, unsigned long long seed, alfa_mlp
   al((void**)&m->Pb, MLP_NPARAM * 2);
   al((void**)&m->scratch, N * 8);
   al((void**)&m->means, (size_t)2 * c->d->e.nz * 8);
+  al((void**)&m->calib, (size_t)c->d->e.nz * 8);
   if (!ok) {
     alfa_mlp_destroy(m);
     return c->d->e.fail("mlp_create: device allocation failed", ALFA_E_CUDA);
@@ -884,6 +894,8 @@ int alfa_mlp_create(alfa_ctx* c, int capacity, unsigned long long seed, alfa_mlp
   fill(OW3, 2, MLP_H);
   std::vector<float> nm(2 * (MLP_IN + 2), 0.0f);
   for (int q = MLP_IN + 2; q < 2 * (MLP_IN + 2); q++) nm[q] = 1.0f;
+  m->calib_h.assign(c->d->e.nz, 1.0);
+  cudaMemcpy(m->calib, m->calib_h.data(), c->d->e.nz * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(m->P, p.data(), MLP_NPARAM * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(m->norm, nm.data(), nm.size() * 4, cudaMemcpyHostToDevice);
   cudaMemset(m->G, 0, MLP_NPARAM * 4);
@@ -989,7 +1001,8 @@ int alfa_mlp_infer(alfa_mlp* m, double* Cs2, double* beta) {
   if (!m || !m->c) return ALFA_E_STATE;
   alfa_ctx* c = m->c;
   NN(Cs2);
-  mlp_infer(m->c->d->e.stream, m->c->d->e.sms, feat_in(m->c), m->Pb, m->norm, m->c->d->e.N(), Cs2, beta);
+  mlp_infer(m->c->d->e.stream, m->c->d->e.sms, feat_in(m->c), m->Pb, m->norm, m->c->d->e.N(),
+            m->calib, Cs2, beta);
   return check_launch(m->c->d->e, "mlp_infer");
 }
 
@@ -1006,7 +1019,8 @@ int alfa_step_learned(alfa_mlp* m, int nsteps, int judge_every, double tol, int 
   const int nz = e.nz;
   for (int s = 0; s < nsteps; s++) {
     const int it = W.iteration;
-    const bool judge = rep->reverted || it == e.cfg.istep || it % judge_every == 0;
+    const bool judge =
+        rep->reverted || rep->judged == 0 || it == e.cfg.istep || it % judge_every == 0;
     int st = f64::step(c->d, 1, judge ? 2 : 1);
     if (st) return st;
     rep->steps++;
@@ -1031,10 +1045,39 @@ int alfa_step_learned(alfa_mlp* m, int nsteps, int judge_every, double tol, int 
     rep->judged++;
     rep->last_drift = drift;
     rep->max_drift = std::max(rep->max_drift, drift);
-    if (drift > tol) {
+    // the windowed drift: relative L2 difference of the two profiles
+    // averaged over the last ALFA_MLP_JUDGE_WINDOW judge steps
+    m->window.push_back(h);
+    if ((int)m->window.size() > ALFA_MLP_JUDGE_WINDOW) m->window.pop_front();
+    bool full = (int)m->window.size() == ALFA_MLP_JUDGE_WINDOW;
+    if (full) {
+      double wn = 0.0, wd = 0.0;
+      for (int z = 0; z < nz; z++) {
+        double a = 0.0, b = 0.0;
+        for (const auto& v : m->window) {
+          a += v[z];
+          b += v[nz + z];
+        }
+        wn += (a - b) * (a - b);
+        wd += b * b;
+      }
+      rep->window_drift = wd > 0 ? std::sqrt(wn / wd) : 0.0;
+      rep->max_window_drift = std::max(rep->max_window_drift, rep->window_drift);
+    }
+    if (full && rep->window_drift > tol) {
       rep->reverted = 1;
       rep->reverted_at = it;
-    } else if (refresh_points > 0 && refresh_epochs > 0) {
+      continue;
+    }
+    // recalibrate the levels to this step's procedure profile (ratios held
+    // within [0.1, 10]; levels where either mean is ~0 keep their factor)
+    for (int z = 0; z < nz; z++) {
+      const double net = h[z], dyn = h[nz + z];
+      if (net > 1e-12 && dyn > 1e-12)
+        m->calib_h[z] = std::min(10.0, std::max(0.1, m->calib_h[z] * dyn / net));
+    }
+    cudaMemcpyAsync(m->calib, m->calib_h.data(), nz * 8, cudaMemcpyHostToDevice, e.stream);
+    if (refresh_points > 0 && refresh_epochs > 0) {
       // keep learning from the procedure's own fields of this judge step
       st = alfa_mlp_collect(m, std::min(refresh_points, m->cap));
       if (!st && m->count >= 1024) st = alfa_mlp_train(m, refresh_epochs, 1024, 1e-3, nullptr);

@@ -297,11 +297,13 @@ void mlp_to_bf16(cudaStream_t st, const float* P, __nv_bfloat16* Pb) {
   k_to_bf16<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(P, Pb, MLP_NPARAM);
 }
 
-// Inference at every uvp node: Cs^2 = clip(y0, 0, 1) (the dynamic procedure's
-// range), beta = y1 (diagnostic), BF16 weights, FP32 accumulation
+// Inference at every uvp node: Cs^2 = clip(y0 s_z, 0, 1) (the dynamic
+// procedure's range; s_z the per-level calibration, 1 without one), beta = y1
+// (diagnostic), BF16 weights, FP32 accumulation
 __global__ void __launch_bounds__(TPB_MLP) k_mlp_infer(MlpFeatIn a,
                                                        const __nv_bfloat16* __restrict__ Pb,
                                                        const float* __restrict__ norm, size_t N,
+                                                       const double* __restrict__ level_scale,
                                                        double* Cs2, double* beta) {
   __shared__ float W[MLP_NPARAM];
   __shared__ float nm[2 * (MLP_IN + 2)];
@@ -330,18 +332,20 @@ __global__ void __launch_bounds__(TPB_MLP) k_mlp_infer(MlpFeatIn a,
       y0 += W[OW3 + k] * h;
       y1 += W[OW3 + MLP_H + k] * h;
     }
-    const double c = (double)(y0 * nm[2 * MLP_IN + 2] + nm[MLP_IN]);
+    double c = (double)(y0 * nm[2 * MLP_IN + 2] + nm[MLP_IN]);
+    if (level_scale) c *= level_scale[i % a.nz];
     Cs2[i] = c < 0.0 ? 0.0 : (c > 1.0 ? 1.0 : c);
     if (beta) beta[i] = (double)(y1 * nm[2 * MLP_IN + 3] + nm[MLP_IN + 1]);
   }
 }
 
 void mlp_infer(cudaStream_t st, int sms, const MlpFeatIn& a, const __nv_bfloat16* Pb,
-               const float* norm, size_t N, double* Cs2, double* beta) {
+               const float* norm, size_t N, const double* level_scale, double* Cs2,
+               double* beta) {
   const size_t want = (N + TPB_MLP - 1) / TPB_MLP;
   const unsigned blocks = (unsigned)(want < (size_t)sms * 8 ? want : (size_t)sms * 8);
   ::alfa::note_launch();
-  k_mlp_infer<<<blocks, TPB_MLP, 0, st>>>(a, Pb, norm, N, Cs2, beta);
+  k_mlp_infer<<<blocks, TPB_MLP, 0, st>>>(a, Pb, norm, N, level_scale, Cs2, beta);
 }
 
 // features of every point into X (N x 10), for tests and diagnostics

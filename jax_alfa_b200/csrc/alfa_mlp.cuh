@@ -29,8 +29,10 @@ void mlp_grad(cudaStream_t st, const float* P, const float* X, const float* T, c
 void mlp_adam(cudaStream_t st, float* P, float* G, float* M, float* V, __nv_bfloat16* Pb,
               float lr, int t);
 void mlp_to_bf16(cudaStream_t st, const float* P, __nv_bfloat16* Pb);
+// level_scale: nz per-level factors of the Cs^2 output, or null
 void mlp_infer(cudaStream_t st, int sms, const MlpFeatIn& a, const __nv_bfloat16* Pb,
-               const float* norm, size_t N, double* Cs2, double* beta);
+               const float* norm, size_t N, const double* level_scale, double* Cs2,
+               double* beta);
 void mlp_features_all(cudaStream_t st, const MlpFeatIn& a, size_t N, float* X);
 
 }  // namespace alfa
