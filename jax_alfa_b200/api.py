@@ -123,6 +123,16 @@ class Alfa:
                         "equal": bool(e.equal), "chosen": bool(e.chosen)})
         return out
 
+    def tune_shapes(self):
+        """The eight line-pass shapes of a step, in autotune's order, as the
+        dicts set_line_variant takes."""
+        nx, ny = int(self.cfg["nx"]), int(self.cfg["ny"])
+        mx, my = 3 * nx // 2, 3 * ny // 2
+        rows = [(1, ny, my, 4, 1), (0, nx, mx, 4, 1), (0, mx, nx, 5, 1), (1, my, ny, 5, 1),
+                (0, nx, nx, 2, 1), (1, ny, ny, 2, 1), (0, nx, nx, 1, 2), (1, ny, ny, 1, 2)]
+        return [{"shape": name, "axis": a, "n_in": i, "n_out": o, "map": m, "outputs": n}
+                for name, (a, i, o, m, n) in zip(self.TUNE_SHAPES, rows)]
+
     def set_line_variant(self, shape, variant):
         """Make `variant` (a TUNE_VARIANTS name) the one the step uses for a
         pass shape of autotune's list (a dict with axis, n_in, n_out, map

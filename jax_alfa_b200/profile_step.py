@@ -3,7 +3,8 @@ boundary-layer benchmark case) for profilers: the bootstrap step, then graph
 steps, nothing else on the device.  The kernel launch lists and ncu captures
 under profiles/ name this command.
 
-    python -m jax_alfa_b200.profile_step --precision mixed --grid 256 256 256 --steps 3
+    python -m jax_alfa_b200.profile_step --precision mixed --grid 256 256 256 --steps 3 \
+        --variant two-lane
 """
 import argparse
 import sys
@@ -15,6 +16,9 @@ def main(argv=None):
     ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
     ap.add_argument("--steps", type=int, default=3, help="graph steps after the bootstrap step")
     ap.add_argument("--tune", action="store_true", help="run the line-pass autotuner first")
+    ap.add_argument("--variant", default=None,
+                    help="set this line-pass variant (a TUNE_VARIANTS name) on every pass "
+                         "shape that takes it, without timing")
     args = ap.parse_args(argv)
     import torch
 
@@ -24,6 +28,14 @@ def main(argv=None):
     u, v, w, th = cases.initial_fields(cfg, 0)
     sim = Simulation(cfg, u, v, w, th)
     sim.step(1)
+    if args.variant:
+        from jax_alfa_b200._lib import AlfaError
+        for shape in sim.alfa.tune_shapes():
+            try:
+                sim.set_line_variant(shape, args.variant)
+                print(f"{shape['shape']}: {args.variant}")
+            except AlfaError:
+                print(f"{shape['shape']}: default ({args.variant} does not apply)")
     if args.tune:
         for c in sim.autotune(reps=3):
             if c["chosen"]:
