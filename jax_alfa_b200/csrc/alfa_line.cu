@@ -255,10 +255,6 @@ __device__ __forceinline__ void gather_rows_cv(const real* a0, int nz, size_t ba
 }
 #endif
 
-// elements of type V per tile row: one 128-byte row segment
-template <class V>
-__host__ __device__ constexpr int tile_cols() { return (int)(128 / sizeof(V)); }
-
 // V: cd, or (FP32 build, plain-field input, nz a multiple of 4) the two-lane
 // cv, which takes 4 z levels per element and half the threads per tile
 template <int NIN, int NOUT, bool GEN, class V = cd>

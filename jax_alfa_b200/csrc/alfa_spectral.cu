@@ -506,6 +506,249 @@ __global__ void __launch_bounds__(tile_threads<C, (NI > NO ? NI : NO)>(), 2) k_x
   }
 }
 
+#ifdef ALFA_BUILD_FP32
+// ---------------------------------------------------------------------------
+// k_y_inv_cv: k_y_inv (compile-time length) on two-lane elements: a thread
+// takes two packed column pairs, four z levels (two 16-byte spectrum loads,
+// one 16-byte store per row), and runs their inverse transforms in paired
+// FP32 instructions.  nz a multiple of 4.
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N))
+    k_y_inv_cv(const cd* __restrict__ T, int K, FftPlan p, int nz, double scale,
+               real* __restrict__ out, int accumulate) {
+  constexpr int C = tile_cols<cv>();
+  constexpr int NT = ct_threads(C, N);
+  constexpr int R = ct_radix(N);
+  constexpr int NR = N / R;
+  constexpr int B = NR * C;
+  constexpr int MB = ct_mb(C, N, 1, NT);
+  constexpr int h = N / 2;
+  extern __shared__ __align__(16) unsigned char sm_yinv[];
+  cv* b0 = reinterpret_cast<cv*>(sm_yinv);
+  const int z0 = blockIdx.x * (4 * C);
+  const int row = blockIdx.y;
+  // Hermitian expansion of the packed columns (z, z+1) and (z+2, z+3)
+  cv v[MB * R];
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 4 * c;
+    const bool ok = (B % NT == 0 || b < B) && z < nz;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int k = j + r * NR;
+      const int src = k <= h ? k : N - k;
+      float4 a = make_float4(0.f, 0.f, 0.f, 0.f), bq = a;  // (a, bb) of lane A, of lane B
+      if (ok && src < K) {
+        const float4* t = reinterpret_cast<const float4*>(T + ((size_t)row * K + src) * nz + z);
+        a = __ldg(t);
+        bq = __ldg(t + 1);
+      }
+      if (k == 0 || k == h) {
+        a.y = 0.f;
+        a.w = 0.f;
+        bq.y = 0.f;
+        bq.w = 0.f;
+      }
+      v[q * R + r] = k <= h ? cv{make_float2(a.x - a.w, bq.x - bq.w),
+                                 make_float2(a.y + a.z, bq.y + bq.z)}
+                            : cv{make_float2(a.x + a.w, bq.x + bq.w),
+                                 make_float2(a.z - a.y, bq.z - bq.y)};
+    }
+  }
+  const size_t base = (size_t)row * N * nz;
+  ct_first_reg<+1, C, N, NT>(v, b0);
+  ct_mid_passes<+1, C, N, R, NT>(b0, p.tw);
+  __syncthreads();
+  constexpr int NSL = ct_last_ns(N);
+  constexpr int RL = N / NSL;
+  constexpr int BL = NSL * C;
+  constexpr int ML = ct_mb(C, N, NSL, NT);
+  cv u[ML * RL];
+  ct_last_reg<+1, C, N, NT>(b0, p.tw, u);
+  LineOut o{};
+  o.scale = scale;
+  o.accumulate = accumulate;
+  o.dst = out;
+#pragma unroll
+  for (int q = 0; q < ML; q++) {
+    const int b = threadIdx.x + q * NT;
+    if (!(BL % NT == 0 || b < BL)) continue;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 4 * c;
+#pragma unroll
+    for (int r = 0; r < RL; r++)
+      store_elem(o, base + (size_t)(j + r * NSL) * nz + z, z, nz, u[q * RL + r]);
+  }
+}
+
+// store a two-lane element as the complex values at z and z+1 of a spectrum
+__device__ __forceinline__ void st_cv(cd* p, cv v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v.re.x, v.im.x, v.re.y, v.im.y);
+}
+
+// map_value on two-lane elements (two consecutive z levels of a spectrum)
+template <int C>
+__device__ __forceinline__ cv map_value_cv(const XArgs& a, const XOut& o, const cv* S, int k,
+                                           int ky, int c) {
+  switch (o.map) {
+    case MAP_IDENT:
+      return S[k * C + c];
+    case MAP_TRUNC: {
+      const bool keep = (k < o.cx || k >= a.nx - o.cx + 1) && ky < o.cy;
+      return keep ? S[k * C + c] : vzero<cv>();
+    }
+    case MAP_DX:
+      return mul_ik(S[k * C + c], (real)a.kx[k]);
+    case MAP_DY:
+      return mul_ik(S[k * C + c], (real)a.ky[ky]);
+    case MAP_PAD: {
+      const int h = a.nx / 2;
+      if (k <= h) return S[k * C + c];
+      if (k >= a.mx - h) return S[(k - a.mx + a.nx) * C + c];
+      return vzero<cv>();
+    }
+    default: {
+      const int h = a.nx / 2;
+      if (k < h) return S[k * C + c];
+      if (k == h) return vzero<cv>();
+      return S[(k - a.nx + a.mx) * C + c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_x_cv: the compile-time forward-and-outputs path of k_x on two-lane
+// elements (two consecutive z levels of the y half spectrum per element, one
+// 16-byte load or store, paired FP32 instructions).  nz even.
+// ---------------------------------------------------------------------------
+template <int NI, int NO>
+__global__ void __launch_bounds__(tile_threads<tile_cols<cv>(), (NI > NO ? NI : NO)>(), 2)
+    k_x_cv(XArgs a) {
+  constexpr int C = tile_cols<cv>();
+  constexpr int NT = tile_threads<C, (NI > NO ? NI : NO)>();
+  extern __shared__ __align__(16) unsigned char sm_x[];
+  cv* sm = reinterpret_cast<cv*>(sm_x);
+  const int nz = a.nz;
+  const int z0 = blockIdx.x * (2 * C);
+  const int ky = blockIdx.y;
+  const int M = a.maxrows * C;
+  cv* buf0 = sm;
+  cv* f0 = sm + M;
+  const bool have = ky < a.Kin;
+  {
+    constexpr int R = ct_radix(NI);
+    constexpr int NR = NI / R;
+    constexpr int B = NR * C;
+    constexpr int MB = ct_mb(C, NI, 1, NT);
+    cv v[MB * R];
+#pragma unroll
+    for (int q = 0; q < MB; q++) {
+      const int b = threadIdx.x + q * NT;
+      const int c = b % C;
+      const int j = b / C;
+      const int z = z0 + 2 * c;
+      const bool ok = have && (B % NT == 0 || b < B) && z < nz;
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        v[q * R + r] =
+            ok ? ld_cv(reinterpret_cast<const real*>(a.src + ((size_t)(j + r * NR) * a.Kin + ky) *
+                                                                  nz + z))
+               : vzero<cv>();
+    }
+    ct_first_reg<-1, C, NI, NT>(v, buf0);
+    ct_passes<-1, C, NI, R, NT>(buf0, a.fwd.tw);
+    __syncthreads();
+  }
+  const cv* S = buf0;
+  for (int oi = 0; oi < a.nout; oi++) {
+    const XOut& o = a.out[oi];
+    if (o.kind == XO_SPEC) {
+      for (int t = threadIdx.x; t < o.rows * C; t += blockDim.x) {
+        const int k = t / C, c = t % C;
+        const int z = z0 + 2 * c;
+        if (z < nz) st_cv(o.dst + ((size_t)k * o.K + ky) * nz + z, map_value_cv<C>(a, o, S, k, ky, c));
+      }
+      continue;
+    }
+    if (ky >= o.K) continue;  // column not stored: zero by convention
+    constexpr int RO = ct_radix(NO);
+    constexpr int NRO = NO / RO;
+    constexpr int BO = NRO * C;
+    constexpr int MBO = ct_mb(C, NO, 1, NT);
+    cv w[MBO * RO];
+#pragma unroll
+    for (int q = 0; q < MBO; q++) {
+      const int b = threadIdx.x + q * NT;
+      const int c = b % C;
+      const int j = b / C;
+#pragma unroll
+      for (int r = 0; r < RO; r++)
+        w[q * RO + r] = (BO % NT == 0 || b < BO) ? map_value_cv<C>(a, o, S, j + r * NRO, ky, c)
+                                                  : vzero<cv>();
+    }
+    ct_first_reg<+1, C, NO, NT>(w, f0);
+    ct_mid_passes<+1, C, NO, RO, NT>(f0, o.inv.tw);
+    __syncthreads();
+    constexpr int NSL = ct_last_ns(NO);
+    constexpr int RL = NO / NSL;
+    constexpr int BL = NSL * C;
+    constexpr int ML = ct_mb(C, NO, NSL, NT);
+    cv u[ML * RL];
+    ct_last_reg<+1, C, NO, NT>(f0, o.inv.tw, u);
+#pragma unroll
+    for (int q = 0; q < ML; q++) {
+      const int b = threadIdx.x + q * NT;
+      if (!(BL % NT == 0 || b < BL)) continue;
+      const int c = b % C;
+      const int j = b / C;
+      const int z = z0 + 2 * c;
+      if (z >= nz) continue;
+#pragma unroll
+      for (int r = 0; r < RL; r++)
+        st_cv(o.dst + ((size_t)(j + r * NSL) * o.K + ky) * nz + z, u[q * RL + r]);
+    }
+    __syncthreads();
+  }
+}
+
+// the two-lane k_x where it is built: plain forward transform from a y half
+// spectrum, same-length inverses, nz even
+template <int NI, int NO>
+static bool x_cv(Engine& e, const XArgs& a, int Kgrid) {
+  if constexpr ((NI == 128 || NI == 256) && NO == NI) {
+    if (a.in_spec || (e.nz & 1) != 0) return false;
+    constexpr int C = tile_cols<cv>();
+    const size_t smem = 2 * (size_t)a.maxrows * C * sizeof(cv);
+    set_smem((const void*)k_x_cv<NI, NO>, smem);
+    dim3 g((e.nz + 2 * C - 1) / (2 * C), Kgrid);
+    k_x_cv<NI, NO><<<g, tile_threads<C, NI>(), smem, e.stream>>>(a);
+    return true;
+  }
+  return false;
+}
+
+template <int N>
+static bool y_inv_cv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
+                     real* out, int accumulate) {
+  if constexpr (N == 128 || N == 256 || N == 384) {
+    if (e.nz % 4 != 0 || ct_radix(N) == N) return false;
+    constexpr int C = tile_cols<cv>();
+    const size_t smem = (size_t)N * C * sizeof(cv);
+    set_smem((const void*)k_y_inv_cv<N>, smem);
+    dim3 g((e.nz + 4 * C - 1) / (4 * C), rows);
+    k_y_inv_cv<N><<<g, ct_threads(C, N), smem, e.stream>>>(T, K, p, e.nz, scale, out,
+                                                            accumulate);
+    return true;
+  }
+  return false;
+}
+#endif
+
 // ---------------------------------------------------------------------------
 // launchers (dispatch to the specialised lengths)
 // ---------------------------------------------------------------------------
@@ -521,6 +764,9 @@ static void y_fwd_n(Engine& e, const Loader& L, int rows, const FftPlan& p, int 
 template <int N>
 static void y_inv_n(Engine& e, const cd* T, int rows, int K, const FftPlan& p, double scale,
                     real* out, int accumulate) {
+#ifdef ALFA_BUILD_FP32
+  if (y_inv_cv<N>(e, T, rows, K, p, scale, out, accumulate)) return;
+#endif
   const size_t smem = (size_t)p.n * YC * sizeof(cd);
   set_smem((const void*)k_y_inv<N>, smem);
   dim3 g((e.nz + 2 * YC - 1) / (2 * YC), rows);
@@ -553,6 +799,11 @@ void launch_y_inv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, dou
 
 template <int C, int NI, int NO>
 static void x_n(Engine& e, const XArgs& a, int Kgrid) {
+#ifdef ALFA_BUILD_FP32
+  if constexpr (C == YC) {
+    if (x_cv<NI, NO>(e, a, Kgrid)) return;
+  }
+#endif
   const size_t smem = 2 * (size_t)a.maxrows * C * sizeof(cd);
   set_smem((const void*)k_x<C, NI, NO>, smem);
   dim3 g((e.nz + C - 1) / C, Kgrid);

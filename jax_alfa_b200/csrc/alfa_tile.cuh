@@ -244,6 +244,9 @@ __device__ __forceinline__ void store_elem(const LineOut& o, size_t i, int z, in
 // z levels per element
 template <class V>
 __host__ __device__ constexpr int zp_of() { return (int)(sizeof(V) / sizeof(real)); }
+// elements of type V per tile row: one 128-byte row segment
+template <class V>
+__host__ __device__ constexpr int tile_cols() { return (int)(128 / sizeof(V)); }
 
 #ifdef ALFA_BUILD_FP32
 template <>

