@@ -277,7 +277,7 @@ def run_alfa(args, rank, world, dist):
 
     import torch
     from jax_alfa_b200 import _lib, cases
-    from jax_alfa_b200.api import Simulation
+    from jax_alfa_b200.api import Simulation, stats_to_dict
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -323,6 +323,9 @@ def run_alfa(args, rank, world, dist):
         if not np.isfinite(sim.diag()["CFL"]):
             raise RuntimeError(f"non-finite state in the timed {prec} run")
         st = {k: t.cpu().numpy() for k, t in sim.state().items()}
+        # the beta profiles of the last step (the dynamic procedure's quintic roots)
+        prof = stats_to_dict(sim.stats_sample(None), grid[2], sim.alfa.cfg["Ugal"])
+        st["beta"] = np.stack([prof["Beta1"], prof["Beta2"]])
         out = {"ms": ms, "tune": tune, "launches": int(n1 - n0), "clocks": clk, "state": st}
         if keep:
             out["sim"] = sim
@@ -344,11 +347,20 @@ def run_alfa(args, rank, world, dist):
         err = {k: float(np.abs(st[k] - rs[k]).max()) / vmax for k in ("u", "v", "w")}
         for k in ("TH", "p"):
             err[k] = float(np.abs(st[k] - rs[k]).max()) / max(float(np.abs(rs[k]).max()), 1e-300)
+        # the same per level: the median over levels shows the round-off floor,
+        # the maximum the levels where the beta root selection went the other way
+        lev = np.max(np.stack([np.abs(st[k] - rs[k]).max(axis=(0, 1)) for k in ("u", "v", "w")]),
+                     axis=0) / vmax
+        beta_flips = int(np.sum(np.any(np.abs(st["beta"] - rs["beta"]) > 0.1, axis=0)))
         fp64 = {"value": n_gp * args.steps * world / (ref["ms"] / 1e3),
                 "ms_per_step": ref["ms"] / args.steps,
                 "speedup": ref["ms"] / ms,
                 "vs_a100_fp64": n_gp * args.steps * world / (ref["ms"] / 1e3) / A100_FP64,
                 "err_vs_fp64": err,
+                "velocity_err_per_level": {"median": float(np.median(lev)),
+                                           "max": float(lev.max()),
+                                           "worst_level": int(np.argmax(lev))},
+                "levels_with_other_beta_root": beta_flips,
                 "err_definition": (f"max |x - x_fp64| after {1 + max(args.warmup - 1, 2) + args.steps} "
                                    "steps from the same initial fields: u, v, w relative to the "
                                    "largest FP64 velocity component, TH and p relative to their "

@@ -586,6 +586,103 @@ __global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N))
   }
 }
 
+// levels z .. z+3 of a loader without z neighbours (a plain field, a
+// product, the pressure source R_i) as a two-lane element: one 16-byte load
+// per input, each level evaluated by the loader's own FP64 expression
+template <int KIND>
+__device__ __forceinline__ cv ld_elem_cv(const Loader& L, size_t i, int z, int nz) {
+  static_assert(KIND == LD_FIELD || KIND == LD_MUL || KIND == LD_PRESSURE_R,
+                "two-lane loaders: no z neighbours");
+  constexpr int NI = KIND == LD_FIELD ? 1 : (KIND == LD_MUL ? 2 : 3);
+  float4 q[NI];
+#pragma unroll
+  for (int k = 0; k < NI; k++) q[k] = __ldg(reinterpret_cast<const float4*>(L.a[k] + i));
+  float r[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+    r[m] = (float)ev_kind<KIND>(
+        L, [&](int k, int) { return (double)(&q[k].x)[m]; }, z + m, nz);
+  return cv{make_float2(r[0], r[2]), make_float2(r[1], r[3])};
+}
+
+// ---------------------------------------------------------------------------
+// k_y_fwd_cv: k_y_fwd (compile-time length) on two-lane elements for the
+// loaders without z neighbours: four z levels per element, the Hermitian
+// split of both packed columns written as two 16-byte stores.  nz a
+// multiple of 4.
+// ---------------------------------------------------------------------------
+template <int N, int KIND>
+__global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N), 4)
+    k_y_fwd_cv(Loader L, FftPlan p, int K, cd* __restrict__ T) {
+  constexpr int C = tile_cols<cv>();
+  constexpr int NT = ct_threads(C, N);
+  constexpr int R = ct_radix(N);
+  constexpr int NR = N / R;
+  constexpr int B = NR * C;
+  constexpr int MB = ct_mb(C, N, 1, NT);
+  extern __shared__ __align__(16) unsigned char sm_yfwd[];
+  cv* b0 = reinterpret_cast<cv*>(sm_yfwd);
+  const int nz = L.nz;
+  const int z0 = blockIdx.x * (4 * C);
+  const int row = blockIdx.y;
+  const size_t base = (size_t)row * N * nz;
+  cv v[MB * R];
+#pragma unroll
+  for (int q = 0; q < MB; q++) {
+    const int b = threadIdx.x + q * NT;
+    const int c = b % C;
+    const int j = b / C;
+    const int z = z0 + 4 * c;
+    const bool ok = (B % NT == 0 || b < B) && z < nz;
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      v[q * R + r] = ok ? ld_elem_cv<KIND>(L, base + (size_t)(j + r * NR) * nz + z, z, nz)
+                        : vzero<cv>();
+  }
+  ct_first_reg<-1, C, N, NT>(v, b0);
+  ct_passes<-1, C, N, R, NT>(b0, p.tw);
+  __syncthreads();
+  const float2 h = dup2(0.5f);
+  for (int t = threadIdx.x; t < K * C; t += blockDim.x) {
+    const int k = t / C, c = t % C;
+    const int z = z0 + 4 * c;
+    if (z >= nz) continue;
+    const cv zk = b0[k * C + c];
+    const cv zn = b0[((N - k) % N) * C + c];
+    const float2 Ar = __fmul2_rn(h, __fadd2_rn(zk.re, zn.re));
+    const float2 Ai = __fmul2_rn(h, __fadd2_rn(zk.im, neg2(zn.im)));
+    const float2 Br = __fmul2_rn(h, __fadd2_rn(zk.im, zn.im));
+    const float2 Bi = neg2(__fmul2_rn(h, __fadd2_rn(zk.re, neg2(zn.re))));
+    float4* o = reinterpret_cast<float4*>(T + ((size_t)row * K + k) * nz + z);
+    o[0] = make_float4(Ar.x, Ai.x, Br.x, Bi.x);
+    o[1] = make_float4(Ar.y, Ai.y, Br.y, Bi.y);
+  }
+}
+
+template <int N>
+static bool y_fwd_cv(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T) {
+  if constexpr (N == 128 || N == 256) {
+    if (L.nz % 4 != 0) return false;
+    constexpr int C = tile_cols<cv>();
+    const size_t smem = (size_t)N * C * sizeof(cv);
+    dim3 g((L.nz + 4 * C - 1) / (4 * C), rows);
+    switch (L.kind) {
+#define ALFA_YF(KD)                                                               \
+  case KD:                                                                        \
+    set_smem((const void*)k_y_fwd_cv<N, KD>, smem);                               \
+    k_y_fwd_cv<N, KD><<<g, ct_threads(C, N), smem, e.stream>>>(L, p, K, T);       \
+    return true;
+      ALFA_YF(LD_FIELD)
+      ALFA_YF(LD_MUL)
+      ALFA_YF(LD_PRESSURE_R)
+#undef ALFA_YF
+      default:
+        return false;
+    }
+  }
+  return false;
+}
+
 // store a two-lane element as the complex values at z and z+1 of a spectrum
 __device__ __forceinline__ void st_cv(cd* p, cv v) {
   *reinterpret_cast<float4*>(p) = make_float4(v.re.x, v.im.x, v.re.y, v.im.y);
@@ -754,6 +851,9 @@ static bool y_inv_cv(Engine& e, const cd* T, int rows, int K, const FftPlan& p, 
 // ---------------------------------------------------------------------------
 template <int N>
 static void y_fwd_n(Engine& e, const Loader& L, int rows, const FftPlan& p, int K, cd* T) {
+#ifdef ALFA_BUILD_FP32
+  if (y_fwd_cv<N>(e, L, rows, p, K, T)) return;
+#endif
   const size_t smem = (size_t)p.n * YC * sizeof(cd);
   set_smem((const void*)k_y_fwd<N>, smem);
   dim3 g((L.nz + 2 * YC - 1) / (2 * YC), rows);
