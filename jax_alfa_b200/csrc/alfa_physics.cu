@@ -1152,35 +1152,43 @@ __device__ __forceinline__ double box9(const real* F, int x, int y, int z, int n
   return s;
 }
 
+// The box-filtered kernels run one CTA per (x, y) column (blockIdx.x = y,
+// blockIdx.y = x) and loop over its z levels, so the nine neighbour columns'
+// offsets are computed once per thread instead of dividing the linear index
+// by nz and ny for every element (the index arithmetic was most of these
+// kernels' instructions).
+static inline dim3 column_grid(const Engine& e) { return dim3((unsigned)e.ny, (unsigned)e.nx); }
+static inline int column_threads(int nz) { return nz >= 256 ? 256 : (nz + 31) / 32 * 32; }
+
 __global__ void k_clip_ratio(const real* __restrict__ num, const real* __restrict__ den,
-                             real* __restrict__ out, size_t n, int nx, int ny, int nz) {
-  GRID_STRIDE(i, n) {
-    const int z = zof(i, nz);
-    const size_t r = rof(i, nz);
-    const int y = zof(r, ny), x = (int)rof(r, ny);
+                             real* __restrict__ out, int nx, int ny, int nz) {
+  const int y = blockIdx.x, x = blockIdx.y;
+  const size_t col = ((size_t)x * ny + y) * nz;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
     const double nf = box9(num, x, y, z, nx, ny, nz);
     const double df = box9(den, x, y, z, nx, ny, nz);
     const double q = nf / df;
     const bool bad = (fabs(df) < 1e-10) || (q < 0.0) || (q > 1.0);
-    out[i] = bad ? 0.0 : q;
+    out[col + z] = bad ? 0.0 : q;
   }
 }
 
 void clip_ratio(Engine& e, const real* num, const real* den, real* out) {
-  ::alfa::note_launch(); k_clip_ratio<<<nblocks(e.N()), TPB, 0, e.stream>>>(num, den, out, e.N(), e.nx, e.ny, e.nz);
+  ::alfa::note_launch();
+  k_clip_ratio<<<column_grid(e), column_threads(e.nz), 0, e.stream>>>(num, den, out, e.nx, e.ny,
+                                                                      e.nz);
 }
 
-__global__ void k_imfilter(const real* __restrict__ F, real* __restrict__ out, size_t n, int nx, int ny,
+__global__ void k_imfilter(const real* __restrict__ F, real* __restrict__ out, int nx, int ny,
                            int nz) {
-  GRID_STRIDE(i, n) {
-    const int z = zof(i, nz);
-    const size_t r = rof(i, nz);
-    out[i] = box9(F, (int)rof(r, ny), zof(r, ny), z, nx, ny, nz);
-  }
+  const int y = blockIdx.x, x = blockIdx.y;
+  const size_t col = ((size_t)x * ny + y) * nz;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) out[col + z] = box9(F, x, y, z, nx, ny, nz);
 }
 
 void imfilter(Engine& e, const real* F, real* out) {
-  ::alfa::note_launch(); k_imfilter<<<nblocks(e.N()), TPB, 0, e.stream>>>(F, out, e.N(), e.nx, e.ny, e.nz);
+  ::alfa::note_launch();
+  k_imfilter<<<column_grid(e), column_threads(e.nz), 0, e.stream>>>(F, out, e.nx, e.ny, e.nz);
 }
 
 __global__ void k_cs2_partial(const real* __restrict__ C, size_t H, int nz, double* part) {
