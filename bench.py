@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--ensemble", action="store_true",
                     help="time the 64-member uneven ensemble (32x32^3, 16x48^3, 16x64^3) "
                          "against its members stepped one at a time")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the short ensemble run of the default line")
     ap.add_argument("--ens-precision", default="fp32", choices=["fp32", "fp64"],
                     help="storage precision of the ensemble members")
     ap.add_argument("--spinup", type=int, default=3000,
@@ -473,6 +475,12 @@ def run_alfa(args, rank, world, dist):
         del sim_e
         torch.cuda.empty_cache()
 
+    # the ensemble workload, a short run beside the headline (`--ensemble`
+    # gives its full 500-step line)
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_measure(50, args.warmup, "fp32")
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads, model = cpu_info()
@@ -496,6 +504,7 @@ def run_alfa(args, rank, world, dist):
             "clocks": clk_head, "gpu_launches": launches_head,
             "fp64": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "tensor_core_line_pass": tc,
+            "ensemble": ens,
             # the chosen variant of each pass shape, and the tensor-core
             # candidate's time beside it (mixed precision)
             "autotune": [{k: c[k] for k in ("shape", "variant", "ms", "equal", "chosen")}
@@ -503,23 +512,24 @@ def run_alfa(args, rank, world, dist):
         }), flush=True)
 
 
-def run_ensemble(args):
-    """The ensemble form: 64 independent neutral members of uneven sizes (32 of
-    32^3, 16 of 48^3, 16 of 64^3), each with its own seed, u* ~ U[0.3, 0.6]
-    m/s and z0 log-uniform in [0.01, 0.5] m (cases.ensemble_members), in FP32
-    with the FP64 tridiagonal solve, stepped together (one CUDA graph launch
-    per step across the members' streams) against the same members stepped
-    one after another.  Both timed with CUDA events on this stream (the
-    ensemble's steps are ordered on it, alfa_ensemble_set_stream); every
-    member's final state is compared with the same member run alone."""
+def ensemble_measure(steps, warmup, precision):
+    """The ensemble workload (cases.ensemble_members: 64 independent neutral
+    members of uneven sizes, 32 of 32^3, 16 of 48^3, 16 of 64^3, each with its
+    own seed, u* ~ U[0.3, 0.6] m/s and z0 log-uniform in [0.01, 0.5] m) stepped
+    together (one CUDA graph launch per step across the members' streams)
+    against the same members stepped one after another.  Both timed with CUDA
+    events on this stream (the ensemble's steps are ordered on it,
+    alfa_ensemble_set_stream); every member's final state is compared with
+    the same member run alone."""
     import torch
 
     from jax_alfa_b200 import cases
     from jax_alfa_b200.api import Ensemble, Simulation
-    total = args.warmup + args.steps + 2
-    members = cases.ensemble_members(nsteps=total, precision=args.ens_precision)
+    total = warmup + steps + 2
+    members = cases.ensemble_members(nsteps=total, precision=precision)
     n_gp = int(sum(c["nx"] * c["ny"] * c["nz"] for c, _ in members))
     stream = torch.cuda.current_stream()
+    n_warm = 1 + max(warmup - 1, 2)
 
     def make(c, seed):
         u, v, w, th = cases.initial_fields(c, seed)
@@ -532,27 +542,27 @@ def run_ensemble(args):
     sims = [make(c, seed) for c, seed in members]
     for s_ in sims:  # the bootstrap step, then graph captures of both parities
         s_.step(1)
-        s_.step(max(args.warmup - 1, 2), graph=True)
+        s_.step(n_warm - 1, graph=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         for s_ in sims:
             s_.step(1, graph=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1) / args.steps
+    t_seq = e0.elapsed_time(e1) / steps
     alone = [state(s_) for s_ in sims]
     del sims
     torch.cuda.empty_cache()
 
     ens = Ensemble([make(c, seed) for c, seed in members]).set_stream(stream)
-    ens.step(1 + max(args.warmup - 1, 2))
+    ens.step(n_warm)
     torch.cuda.synchronize()
     e0.record(stream)
-    ens.step(args.steps)
+    ens.step(steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_ens = e0.elapsed_time(e1) / args.steps
+    t_ens = e0.elapsed_time(e1) / steps
     errs, exact = [], 0
     finite = sum(all(np.isfinite(r[k]).all() for k in r) for r in alone)
     for st, ref in zip(ens.states(), alone):
@@ -562,28 +572,35 @@ def run_ensemble(args):
         errs.append(e)
         exact += all(np.array_equal(got[k], ref[k]) for k in ref)
     ens.close()
-    print(json.dumps({
+    del ens
+    torch.cuda.empty_cache()
+    return {
         "metric": "ensemble LES grid-point-steps/s (64 members: 32x32^3, 16x48^3, 16x64^3)",
-        "value": n_gp / (t_ens / 1e3), "unit": "gp-steps/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": 1 + max(args.warmup - 1, 2),
-        "ms_per_step": t_ens, "higher_is_better": True,
+        "value": n_gp / (t_ens / 1e3), "unit": "gp-steps/s", "steps": steps, "warmup": n_warm,
+        "ms_per_step": t_ens,
         "sequential": {"value": n_gp / (t_seq / 1e3), "ms_per_step": t_seq,
                        "how": "the same members, one graph step each, one after another"},
         "speedup_vs_sequential": t_seq / t_ens,
         "members_vs_alone": {"max_rel_err": max(errs), "bit_identical": exact,
-                             "finite_members": finite,
-                             "members": len(errs), "bar": 1e-6,
-                             "after_steps": 1 + max(args.warmup - 1, 2) + args.steps},
-        "dtype": DTYPES[args.ens_precision], "data": "synthetic",
+                             "finite_members": finite, "members": len(errs), "bar": 1e-6,
+                             "after_steps": n_warm + steps},
+        "dtype": DTYPES[precision],
         "config": {"workload": "neutral ABL members (C1 physics), LASDD-SM, per-member seed, "
-                               "u* ~ U[0.3, 0.6] m/s, z0 log-uniform [0.01, 0.5] m",
-                   "members": len(members), "grid_points": n_gp,
-                   "precision": args.ens_precision,
-                   "timing": "CUDA events on the stream the steps are ordered on"}}),
-        flush=True)
-    if not (max(errs) <= 1e-6) or finite != len(members):
-        raise SystemExit(f"ensemble members: max error {max(errs):.2e}, "
-                         f"{finite} of {len(members)} finite")
+                               "u* ~ U[0.3, 0.6] m/s, z0 log-uniform [0.01, 0.5] m, dt scaled "
+                               "to the grid",
+                   "members": len(members), "grid_points": n_gp, "precision": precision,
+                   "timing": "CUDA events on the stream the steps are ordered on"}}
+
+
+def run_ensemble(args):
+    """The ensemble form on its own line (`--ensemble`, 500 steps by default)."""
+    out = ensemble_measure(args.steps, args.warmup, args.ens_precision)
+    out.update({"n_gpus": 1, "higher_is_better": True, "data": "synthetic"})
+    print(json.dumps(out), flush=True)
+    m = out["members_vs_alone"]
+    if not (m["max_rel_err"] <= 1e-6) or m["finite_members"] != m["members"]:
+        raise SystemExit(f"ensemble members: max error {m['max_rel_err']:.2e}, "
+                         f"{m['finite_members']} of {m['members']} finite")
 
 
 def run_learned(args):

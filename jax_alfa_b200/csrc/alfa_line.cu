@@ -924,11 +924,11 @@ void op2_pad(Engine& e, const Loader& L0, real* out_pad, real* scratch) {
 // first materialised
 void op2_unpad(Engine& e, const Loader& L0, real* out, real* scratch) {
   Loader L = L0;
+  LineOut ox = lo(LM_UNPAD, scratch, 1.0 / e.nx);
   if (L.kind != LD_FIELD) {
     materialize(e, L, e.P(), e.mat);
     L = ld_field(e, e.mat);
   }
-  LineOut ox = lo(LM_UNPAD, scratch, 1.0 / e.nx);
   launch_line(e, 0, L, e.mx, e.my, e.mx, e.nx, 1, &ox);
   LineOut oy = lo(LM_UNPAD, out, (9.0 / 4.0) * (1.0 / e.ny));
   launch_line(e, 1, ld_field(e, scratch), e.nx, e.my, e.my, e.ny, 1, &oy);

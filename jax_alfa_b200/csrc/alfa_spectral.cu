@@ -586,25 +586,6 @@ __global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N))
   }
 }
 
-// levels z .. z+3 of a loader without z neighbours (a plain field, a
-// product, the pressure source R_i) as a two-lane element: one 16-byte load
-// per input, each level evaluated by the loader's own FP64 expression
-template <int KIND>
-__device__ __forceinline__ cv ld_elem_cv(const Loader& L, size_t i, int z, int nz) {
-  static_assert(KIND == LD_FIELD || KIND == LD_MUL || KIND == LD_PRESSURE_R,
-                "two-lane loaders: no z neighbours");
-  constexpr int NI = KIND == LD_FIELD ? 1 : (KIND == LD_MUL ? 2 : 3);
-  float4 q[NI];
-#pragma unroll
-  for (int k = 0; k < NI; k++) q[k] = __ldg(reinterpret_cast<const float4*>(L.a[k] + i));
-  float r[4];
-#pragma unroll
-  for (int m = 0; m < 4; m++)
-    r[m] = (float)ev_kind<KIND>(
-        L, [&](int k, int) { return (double)(&q[k].x)[m]; }, z + m, nz);
-  return cv{make_float2(r[0], r[2]), make_float2(r[1], r[3])};
-}
-
 // ---------------------------------------------------------------------------
 // k_y_fwd_cv: k_y_fwd (compile-time length) on two-lane elements for the
 // loaders without z neighbours: four z levels per element, the Hermitian

@@ -260,6 +260,38 @@ __device__ __forceinline__ cv ld_cv(const real* p) {
   const float4 q = __ldg(reinterpret_cast<const float4*>(p));
   return cv{make_float2(q.x, q.z), make_float2(q.y, q.w)};
 }
+// the loader kinds a two-lane kernel evaluates inline: no z neighbours
+__host__ __device__ constexpr bool cv_inline_kind(int kind) {
+  return kind == LD_FIELD || kind == LD_MUL || kind == LD_MUL3 || kind == LD_PRESSURE_R ||
+         kind == LD_STRESS_UVP || kind == LD_WL_UVP;
+}
+
+// levels z .. z+3 of such a loader as a two-lane element: one 16-byte load
+// per input, each level evaluated by the loader's own FP64 expression (a
+// plain field is taken as loaded).  Evaluating the multi-input kinds inside
+// a transform kernel is worth it only where the expression is cheap: the
+// 3/2-rule unpad with the three-factor stress product inline measured 234 us
+// per x pass against 117 + 62 us for the materialising pass and the
+// plain-field unpad, so the line passes keep materialising.
+template <int KIND>
+__device__ __forceinline__ cv ld_elem_cv(const Loader& L, size_t i, int z, int nz) {
+  static_assert(cv_inline_kind(KIND), "two-lane loaders: no z neighbours");
+  if constexpr (KIND == LD_FIELD) {
+    return ld_cv(L.a[0] + i);
+  } else {
+    constexpr int NI = (KIND == LD_MUL || KIND == LD_WL_UVP) ? 2 : 3;
+    float4 q[NI];
+#pragma unroll
+    for (int k = 0; k < NI; k++) q[k] = __ldg(reinterpret_cast<const float4*>(L.a[k] + i));
+    float r[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+      r[m] = (float)ev_kind<KIND>(
+          L, [&](int k, int) { return (double)(&q[k].x)[m]; }, z + m, nz);
+    return cv{make_float2(r[0], r[2]), make_float2(r[1], r[3])};
+  }
+}
+
 __device__ __forceinline__ void store_elem(const LineOut& o, size_t i, int z, int nz, cv v) {
   if (z >= nz) return;
   const float s = (float)o.scale;

@@ -129,6 +129,21 @@ def test_learned_closure_trains_and_steps(report_line):
                 f"{rep['max_window_drift']:.3f}; profile error vs dynamic (learned / fixed): "
                 + ", ".join(f"{k} {a:.1e}/{b:.1e}" for k, (a, b) in errs.items()))
     assert t_lrn < t_dyn
+    # the same run judged at the 5 % tolerance: either the network is
+    # accepted throughout (its windowed drift never above 0.05) or the judge
+    # records the revert at the step where it went above
+    s5 = _sim(cfg).restore(ck)
+    n5 = Learned(s5, capacity=1024)
+    n5.set_params(P, norm)
+    r5 = n5.step(steps, judge_every=10, tol=0.05)
+    if r5["reverted"]:
+        assert r5["window_drift"] > 0.05 and r5["reverted_at"] > 0
+        assert r5["learned_steps"] + r5["judged"] <= steps  # dynamic steps after the revert
+    else:
+        assert r5["max_window_drift"] <= 0.05 and r5["learned_steps"] == steps - r5["judged"]
+    report_line(f"learned closure at tol 0.05: {'reverted at iteration ' + str(r5['reverted_at']) if r5['reverted'] else 'accepted'}"
+                f" (windowed drift last {r5['window_drift']:.3f}, max {r5['max_window_drift']:.3f}, "
+                f"{r5['learned_steps']} of {steps} steps learned)")
 
 
 def test_judge_reverts_to_the_dynamic_procedure():

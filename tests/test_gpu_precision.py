@@ -258,3 +258,21 @@ def test_two_lane_fp32_kernels_match_oracle(report_line):
                 + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
     for k, err in errs.items():
         assert err <= (1e-4 if k == "p" else 1e-5), (k, err)
+
+
+def test_two_lane_step_at_256_matches_fp64(report_line):
+    """Every line pass on the two-lane kernels at the 256^2 NBL_A94 shapes
+    (the phase-split pad and unpad, the same-length passes) and the 2-D
+    path's two-lane kernels: one step against the FP64 drop-in, velocity
+    within 1e-5 of its largest component."""
+    cfg = cases.nbl_a94(256, 256, 64, nsteps=2)
+    ref = _state(_sim(cfg).step(1))
+    sim = _sim(dict(cfg, precision="fp32"))
+    for shape in sim.alfa.tune_shapes():
+        sim.set_line_variant(shape, "two-lane")
+    st = _state(sim.step(1))
+    errs = _errs(st, ref)
+    report_line("fp32 two-lane vs fp64, NBL_A94 256x256x64, 1 step: "
+                + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+    for k in ("u", "v", "w"):
+        assert errs[k] <= 1e-5, (k, errs[k])
