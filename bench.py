@@ -555,12 +555,15 @@ def ensemble_measure(steps, warmup, precision):
     del sims
     torch.cuda.empty_cache()
 
-    ens = Ensemble([make(c, seed) for c, seed in members]).set_stream(stream)
+    # the ensemble's steps ordered on a stream of their own (the legacy
+    # default stream cannot be handed over: its handle is the null stream)
+    tstream = torch.cuda.Stream()
+    ens = Ensemble([make(c, seed) for c, seed in members]).set_stream(tstream)
     ens.step(n_warm)
     torch.cuda.synchronize()
-    e0.record(stream)
+    e0.record(tstream)
     ens.step(steps)
-    e1.record(stream)
+    e1.record(tstream)
     torch.cuda.synchronize()
     t_ens = e0.elapsed_time(e1) / steps
     errs, exact = [], 0

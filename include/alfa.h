@@ -348,10 +348,11 @@ typedef struct alfa_ensemble alfa_ensemble;
 int alfa_ensemble_create(alfa_ctx* const* members, int n, alfa_ensemble** out);
 int alfa_ensemble_step(alfa_ensemble*, int nsteps);
 int alfa_ensemble_sync(alfa_ensemble*);
-/* Orders later alfa_ensemble_step calls on `stream` (a cudaStream_t; NULL
- * to stop): each call's steps start after the work already queued on it,
- * and work queued on it afterwards starts after the steps, so events
- * recorded on it time them. */
+/* Orders later alfa_ensemble_step calls on `stream` (a created
+ * cudaStream_t; NULL, which is also the legacy default stream's handle,
+ * stops): each call's steps start after the work already queued on it, and
+ * work queued on it afterwards starts after the steps, so events recorded on
+ * it time them. */
 int alfa_ensemble_set_stream(alfa_ensemble*, void* stream);
 const char* alfa_ensemble_error(const alfa_ensemble*);
 void alfa_ensemble_destroy(alfa_ensemble*);

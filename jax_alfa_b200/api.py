@@ -717,7 +717,10 @@ class Ensemble:
 
     def set_stream(self, stream):
         """Order later steps on a torch CUDA stream (alfa_ensemble_set_stream),
-        so that events recorded on it time them; None stops."""
+        so that events recorded on it time them; None stops.  The stream must
+        not be the legacy default stream (its null handle means stop)."""
+        if stream is not None and stream.cuda_stream == 0:
+            raise ValueError("Ensemble.set_stream needs a created stream, not the default one")
         h = ctypes.c_void_p(stream.cuda_stream if stream is not None else None)
         if self.lib.alfa_ensemble_set_stream(self.h, h) != 0:
             raise _lib.AlfaError("alfa_ensemble_set_stream failed")

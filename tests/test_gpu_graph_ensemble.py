@@ -122,8 +122,16 @@ def test_fp32_ensemble_with_member_draws_equals_members_alone():
     assert len({round(c["ustar"], 6) for c, _ in members}) == len(pick)
     alone = [_state(_sim(c, seed=s).step(1).step(steps - 1, graph=True)) for c, s in members]
     ens = Ensemble([_sim(c, seed=s) for c, s in members])
-    ens.set_stream(torch.cuda.current_stream())
+    ts = torch.cuda.Stream()
+    ens.set_stream(ts)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(ts)
     ens.step(steps)
+    ev1.record(ts)
+    torch.cuda.synchronize()
+    # events on the ordering stream bracket the steps: at least a few
+    # microseconds of device time per step of 6 members
+    assert ev0.elapsed_time(ev1) / steps > 0.05
     for i, st in enumerate(ens.states()):
         got = {k: t.cpu().numpy() for k, t in st.items()}
         for k in got:
