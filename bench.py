@@ -80,6 +80,9 @@ def parse():
                          "against its members stepped one at a time")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the short ensemble run of the default line")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the convective 128^3 and stable 256x256x192 runs of the "
+                         "default line")
     ap.add_argument("--ens-precision", default="fp32", choices=["fp32", "fp64"],
                     help="storage precision of the ensemble members")
     ap.add_argument("--spinup", type=int, default=3000,
@@ -480,6 +483,10 @@ def run_alfa(args, rank, world, dist):
     ens = None
     if not args.no_ensemble:
         ens = ensemble_measure(50, args.warmup, "fp32")
+    # the convective and stable configurations, short
+    wl = None
+    if not args.no_workloads:
+        wl = workloads_measure()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -505,6 +512,7 @@ def run_alfa(args, rank, world, dist):
             "fp64": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "tensor_core_line_pass": tc,
             "ensemble": ens,
+            "workloads": wl,
             # the chosen variant of each pass shape, and the tensor-core
             # candidate's time beside it (mixed precision)
             "autotune": [{k: c[k] for k in ("shape", "variant", "ms", "equal", "chosen")}
@@ -593,6 +601,83 @@ def ensemble_measure(steps, warmup, precision):
                                "to the grid",
                    "members": len(members), "grid_points": n_gp, "precision": precision,
                    "timing": "CUDA events on the stream the steps are ordered on"}}
+
+
+def workloads_measure():
+    """The other two configurations of the benchmark matrix, short, beside
+    the headline: the convective ABL at 128^3 (mixed and FP64 from the same
+    initial fields, 1500 steps of spin-up then 500 steps with the statistics
+    accumulated every step; the plane-averaged <u>, <theta>, <w'theta'> and
+    <w'w'> profiles of the two compared) and the stable ABL at 256x256x192
+    (LAD-SM, 20 graph steps of each precision).  CUDA events on this
+    stream."""
+    import torch
+
+    from jax_alfa_b200 import cases
+    from jax_alfa_b200.api import Simulation, stats_to_dict
+
+    def sim_of(cfg):
+        u, v, w, th = cases.initial_fields(cfg, 0)
+        sfc = cases.surface_bc_series(cfg) if cfg["optSurfBC"] else None
+        return Simulation(cfg, u, v, w, th, surface_series=sfc)
+
+    def timed(sim, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.step(n, graph=True)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {}
+    # convective 128^3
+    spin, avg = 1500, 500
+    prof, ms = {}, {}
+    for p in ("mixed", "fp64"):
+        cfg = cases.convective(128, 128, 128, nsteps=spin + avg + 2, precision=p)
+        sim = sim_of(cfg)
+        sim.step(1)
+        if p == "mixed":
+            sim.autotune(reps=2)
+        ms[p] = timed(sim, spin - 1)
+        acc = None
+        for _ in range(avg):
+            sim.step(1, graph=True)
+            acc = sim.stats_sample(acc)
+        prof[p] = stats_to_dict(acc, 128, cfg["Ugal"])
+        del sim
+        torch.cuda.empty_cache()
+    n_gp = 128 ** 3
+    out["convective_128"] = {
+        "workload": "convective ABL 128^3 (CBL_N91 physics), LASDD-SM, 2000 steps",
+        "mixed": {"ms_per_step": ms["mixed"], "value": n_gp / (ms["mixed"] / 1e3)},
+        "fp64": {"ms_per_step": ms["fp64"], "value": n_gp / (ms["fp64"] / 1e3)},
+        "speedup": ms["fp64"] / ms["mixed"],
+        "profile_err_vs_fp64": {
+            k: float(np.abs(prof["mixed"][k] - prof["fp64"][k]).max()
+                     / max(float(np.abs(prof["fp64"][k]).max()), 1e-300))
+            for k in ("U", "TH", "wTH", "w2")},
+        "profile_definition": "Statistics.py profiles accumulated over steps 1501-2000, max "
+                              "|mixed - fp64| / max |fp64|"}
+    # stable 256x256x192
+    ms = {}
+    for p in ("mixed", "fp64"):
+        cfg = cases.stable(256, 256, 192, nsteps=30, precision=p)
+        sim = sim_of(cfg)
+        sim.step(1)
+        if p == "mixed":
+            sim.autotune(reps=2)
+        sim.step(3, graph=True)
+        ms[p] = timed(sim, 20)
+        del sim
+        torch.cuda.empty_cache()
+    n_gp = 256 * 256 * 192
+    out["stable_256x256x192"] = {
+        "workload": "stable ABL 256x256x192 (GABLS1-like), LAD-SM, 20 timed steps",
+        "mixed": {"ms_per_step": ms["mixed"], "value": n_gp / (ms["mixed"] / 1e3)},
+        "fp64": {"ms_per_step": ms["fp64"], "value": n_gp / (ms["fp64"] / 1e3)},
+        "speedup": ms["fp64"] / ms["mixed"]}
+    return out
 
 
 def run_ensemble(args):
