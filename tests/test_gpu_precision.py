@@ -276,3 +276,28 @@ def test_two_lane_step_at_256_matches_fp64(report_line):
                 + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
     for k in ("u", "v", "w"):
         assert errs[k] <= 1e-5, (k, errs[k])
+
+
+def test_fp32_odd_depth_falls_back_where_two_lane_does_not_fit(report_line):
+    """nz = 30 (even, not a multiple of 4): the 2-D path's k_x_cv still runs
+    (two complex levels per element, a partial last tile) while the y
+    transforms and the line passes keep their one-lane kernels (the two-lane
+    variant is refused for the line shapes); one step of the convective case
+    at 128x128x30 against the FP64 oracle within the FP32 bar."""
+    from jax_alfa_b200._lib import AlfaError
+    cfg = cases.convective(128, 128, 30, nsteps=1, precision="fp32")
+    sim = _sim(cfg)
+    refused = 0
+    for shape in sim.alfa.tune_shapes():
+        try:
+            sim.set_line_variant(shape, "two-lane")
+        except AlfaError:
+            refused += 1
+    assert refused == 8
+    st = _state(sim.step(1))
+    ref = _oracle(cases.convective(128, 128, 30, nsteps=1), 1)
+    errs = _errs(st, ref)
+    report_line("fp32 vs oracle, convective 128x128x30 (odd depth), 1 step: "
+                + ", ".join(f"{k} {v:.1e}" for k, v in errs.items()))
+    for k, err in errs.items():
+        assert err <= (1e-4 if k == "p" else 1e-5), (k, err)
