@@ -480,12 +480,13 @@ def run_alfa(args, rank, world, dist):
 
     # the ensemble workload, a short run beside the headline (`--ensemble`
     # gives its full 500-step line)
+    # (rank 0 only: no collective follows, the line is rank 0's)
     ens = None
-    if not args.no_ensemble:
+    if not args.no_ensemble and rank == 0:
         ens = ensemble_measure(50, args.warmup, "fp32")
     # the convective and stable configurations, short
     wl = None
-    if not args.no_workloads:
+    if not args.no_workloads and rank == 0:
         wl = workloads_measure()
 
     cpu = None
