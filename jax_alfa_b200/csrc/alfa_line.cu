@@ -2,7 +2,9 @@
 // forms of the reference's spectral operators (explicit filter with its
 // derivatives, derivatives, 3/2-rule pad and unpad), each a forward
 // transform of runs of 2 YC z levels (a 128-byte row segment), a map, and an
-// inverse transform.
+// inverse transform.  The FP32 build also has each compile-time pass on
+// two-lane elements (cv: two packed columns, four z levels, per thread), a
+// variant the autotuner chooses per pass shape.
 #include <cmath>
 #include <type_traits>
 

@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N))
 // multiple of 4.
 // ---------------------------------------------------------------------------
 template <int N, int KIND>
-__global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N), 4)
+__global__ void __launch_bounds__(ct_threads(tile_cols<cv>(), N), 5)
     k_y_fwd_cv(Loader L, FftPlan p, int K, cd* __restrict__ T) {
   constexpr int C = tile_cols<cv>();
   constexpr int NT = ct_threads(C, N);
