@@ -826,10 +826,11 @@ static MlpFeatIn feat_in(alfa_ctx* c) {
   return a;
 }
 
+// the network's Cs^2 for a step (the hidden layer on the tensor cores)
 static void learned_cs2(alfa_ctx* c, double* Cs2_out) {
   alfa_mlp* m = c->mlp;
-  mlp_infer(c->d->e.stream, c->d->e.sms, feat_in(c), m->Pb, m->norm, c->d->e.N(), m->calib,
-            Cs2_out, nullptr);
+  mlp_infer_tc(c->d->e.stream, c->d->e.sms, feat_in(c), m->Pb, m->norm, c->d->e.N(), m->calib,
+               Cs2_out);
 }
 
 extern "C" {

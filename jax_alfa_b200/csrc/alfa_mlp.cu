@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstdint>
 
 #include "alfa_mlp.cuh"
 
@@ -346,6 +347,239 @@ void mlp_infer(cudaStream_t st, int sms, const MlpFeatIn& a, const __nv_bfloat16
   const unsigned blocks = (unsigned)(want < (size_t)sms * 8 ? want : (size_t)sms * 8);
   ::alfa::note_launch();
   k_mlp_infer<<<blocks, TPB_MLP, 0, st>>>(a, Pb, norm, N, level_scale, Cs2, beta);
+}
+
+// ---------------------------------------------------------------------------
+// The same inference with the 64 x 64 hidden layer on the tensor cores
+// (tcgen05): a CTA of 128 threads takes tiles of 128 points, one point per
+// thread.  Each thread computes its point's features and first layer and
+// writes the 64 activations, rounded to BF16, as row `tid` of the A operand
+// (K-major, no swizzle: core matrices of 8 rows x 16 bytes); the BF16 second-
+// layer weights are the B operand (64 outputs x 64 inputs, K-major).  One
+// thread issues the four K = 16 MMAs (M = 128, N = 64, FP32 accumulation in
+// 64 tensor-memory columns) and commits them to an mbarrier; after the
+// (bounded) wait each warp reads its 32 rows back with tcgen05.ld, so every
+// thread gets its own point's 64 pre-activations for the tanh and the
+// output layer.  Differs from k_mlp_infer by the BF16 rounding of the first
+// layer's activations.  A wait that gives up writes NaN for the tile's
+// points (a step using them then reports a non-finite state) and waits,
+// bounded, for the products in flight before the columns are freed.
+// ---------------------------------------------------------------------------
+namespace umma {
+
+constexpr int TM = 128;  // points per tile (the MMA's M), threads per CTA
+constexpr int TN = MLP_H;  // hidden units (the MMA's N and K)
+constexpr int A_BYTES = TM * TN * 2;
+constexpr int B_BYTES = TN * TN * 2;
+constexpr int F_OFF = A_BYTES + B_BYTES;  // FP32 weights of the other layers
+constexpr int NF = MLP_H * MLP_IN + MLP_H + MLP_H + 2 * MLP_H + 2 + 2 * (MLP_IN + 2);
+constexpr int BAR_OFF = F_OFF + ((NF * 4 + 15) / 16) * 16;
+constexpr int SMEM = BAR_OFF + 32;
+constexpr unsigned long long SPIN = 1ull << 22;
+constexpr int CLEANUP_WAITS = 16;
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, N = 64, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                           ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// byte offset of element (row r, k) in a K-major no-swizzle tile of `rows` rows
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int rows) {
+  return (uint32_t)(((k >> 3) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity,
+                                         unsigned long long limit) {
+  for (unsigned long long i = 0; i < limit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+}  // namespace umma
+
+__global__ void __launch_bounds__(umma::TM) k_mlp_infer_tc(MlpFeatIn a,
+                                                           const __nv_bfloat16* __restrict__ Pb,
+                                                           const float* __restrict__ norm,
+                                                           size_t N,
+                                                           const double* __restrict__ level_scale,
+                                                           double* Cs2) {
+  using namespace umma;
+  extern __shared__ __align__(1024) unsigned char sm_mlp[];
+  unsigned char* At = sm_mlp;
+  unsigned char* Bt = sm_mlp + A_BYTES;
+  float* F = reinterpret_cast<float*>(sm_mlp + F_OFF);
+  float* W1 = F;                          // 64 x 10
+  float* B1 = W1 + MLP_H * MLP_IN;        // 64
+  float* B2 = B1 + MLP_H;                 // 64
+  float* W3 = B2 + MLP_H;                 // 2 x 64
+  float* B3 = W3 + 2 * MLP_H;             // 2
+  float* NM = B3 + 2;                     // 24
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm_mlp + BAR_OFF);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm_mlp + BAR_OFF + 16);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  for (int q = tid; q < MLP_H * MLP_IN; q += TM) W1[q] = __bfloat162float(Pb[OW1 + q]);
+  for (int q = tid; q < MLP_H; q += TM) {
+    B1[q] = __bfloat162float(Pb[OB1 + q]);
+    B2[q] = __bfloat162float(Pb[OB2 + q]);
+  }
+  for (int q = tid; q < 2 * MLP_H; q += TM) W3[q] = __bfloat162float(Pb[OW3 + q]);
+  if (tid < 2) B3[tid] = __bfloat162float(Pb[OB3 + tid]);
+  for (int q = tid; q < 2 * (MLP_IN + 2); q += TM) NM[q] = norm[q];
+  // B operand: row n = hidden unit of the second layer, K = its 64 inputs
+  for (int q = tid; q < TN * (TN / 8); q += TM) {
+    const int n = q / (TN / 8), kb = q % (TN / 8);
+    *reinterpret_cast<uint4*>(Bt + kmajor_off(n, kb * 8, TN)) =
+        *reinterpret_cast<const uint4*>(Pb + OW2 + n * MLP_H + kb * 8);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t aA = smem_u32(At), aB = smem_u32(Bt);
+  const uint32_t lboA = (TM / 8) * 128, lboB = (TN / 8) * 128, sbo = 128;
+
+  uint32_t phase = 0;
+  bool issued = false;  // products of this CTA issued and not yet waited for
+  const size_t ntiles = (N + TM - 1) / TM;
+  for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const size_t i = tile * TM + tid;
+    const bool valid = i < N;
+    float x[MLP_IN];
+    if (valid) {
+      mlp_features(a, i, x);
+    } else {
+#pragma unroll
+      for (int f = 0; f < MLP_IN; f++) x[f] = NM[f];
+    }
+#pragma unroll
+    for (int f = 0; f < MLP_IN; f++) x[f] = (x[f] - NM[f]) / NM[MLP_IN + 2 + f];
+    // first layer, written as row tid of A in BF16, 8 K values per 16 bytes
+#pragma unroll
+    for (int kb = 0; kb < TN / 8; kb++) {
+      uint32_t pk[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        float h[2];
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          const int k = kb * 8 + 2 * e + t;
+          float acc = B1[k];
+#pragma unroll
+          for (int f = 0; f < MLP_IN; f++) acc += W1[k * MLP_IN + f] * x[f];
+          h[t] = tanhf(acc);
+        }
+        pk[e] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(h[0])) |
+                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(h[1])) << 16);
+      }
+      *reinterpret_cast<uint4*>(At + kmajor_off(tid, kb * 8, TM)) =
+          make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (tid == 0) {
+#pragma unroll
+      for (int ks = 0; ks < TN / 16; ks++) {
+        const uint64_t da = smem_desc(aA + ks * 2 * lboA, lboA, sbo);
+        const uint64_t db = smem_desc(aB + ks * 2 * lboB, lboB, sbo);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(IDESC), "r"(ks > 0 ? 1u : 0u));
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(bar))
+          : "memory");
+    }
+    issued = true;
+    const bool mine = bar_wait(smem_u32(bar), phase, SPIN);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const bool ok = __syncthreads_and(mine) != 0;
+    if (!ok) {
+      if (valid) Cs2[i] = __longlong_as_double(0x7FF8000000000000ll);  // NaN: the tile failed
+      break;
+    }
+    issued = false;
+    phase ^= 1u;
+    // this thread's row of the accumulator, 16 columns at a time (the step
+    // uses the Cs^2 output only)
+    float y0 = B3[0];
+#pragma unroll
+    for (int c0 = 0; c0 < TN; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+          "%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+            "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+            "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        y0 += W3[c0 + j] * tanhf(__uint_as_float(v[j]) + B2[c0 + j]);
+      }
+    }
+    if (valid) {
+      double c = (double)(y0 * NM[2 * MLP_IN + 2] + NM[MLP_IN]);
+      if (level_scale) c *= level_scale[i % a.nz];
+      Cs2[i] = c < 0.0 ? 0.0 : (c > 1.0 ? 1.0 : c);
+    }
+    // the A tile and the accumulator are rewritten by the next tile
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+  }
+  if (issued) {  // a wait gave up: let the products in flight finish (bounded)
+    bool done = false;
+    for (int k = 0; k < CLEANUP_WAITS && !done; k++) done = bar_wait(smem_u32(bar), phase, SPIN);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+}
+
+void mlp_infer_tc(cudaStream_t st, int sms, const MlpFeatIn& a, const __nv_bfloat16* Pb,
+                  const float* norm, size_t N, const double* level_scale, double* Cs2) {
+  static_assert(umma::SMEM <= 48 * 1024, "dynamic shared memory within the default limit");
+  const size_t tiles = (N + umma::TM - 1) / umma::TM;
+  const unsigned blocks = (unsigned)(tiles < (size_t)sms * 4 ? tiles : (size_t)sms * 4);
+  ::alfa::note_launch();
+  k_mlp_infer_tc<<<blocks, umma::TM, umma::SMEM, st>>>(a, Pb, norm, N, level_scale, Cs2);
 }
 
 // features of every point into X (N x 10), for tests and diagnostics

@@ -33,6 +33,10 @@ void mlp_to_bf16(cudaStream_t st, const float* P, __nv_bfloat16* Pb);
 void mlp_infer(cudaStream_t st, int sms, const MlpFeatIn& a, const __nv_bfloat16* Pb,
                const float* norm, size_t N, const double* level_scale, double* Cs2,
                double* beta);
+// Cs^2 only, the hidden layer on the tensor cores (BF16 activations); a
+// tensor-core wait that gives up leaves NaN in the affected points
+void mlp_infer_tc(cudaStream_t st, int sms, const MlpFeatIn& a, const __nv_bfloat16* Pb,
+                  const float* norm, size_t N, const double* level_scale, double* Cs2);
 void mlp_features_all(cudaStream_t st, const MlpFeatIn& a, size_t N, float* X);
 
 }  // namespace alfa

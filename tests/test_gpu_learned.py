@@ -165,3 +165,34 @@ def test_judge_reverts_to_the_dynamic_procedure():
     more = net.step(10, judge_every=10, tol=1e-9)
     assert more["learned_steps"] == rep["learned_steps"]  # no learned step after the revert
     assert first == more["reverted_at"]
+
+
+def test_tensor_core_inference_matches_cuda_core_inference(report_line):
+    """The learned step evaluates the network with its 64 x 64 hidden layer
+    on the tensor cores (tcgen05, BF16 activations, FP32 accumulation in
+    tensor memory); alfa_mlp_infer evaluates it on the CUDA cores with FP32
+    activations.  On the state of a learned step the two Cs^2 fields agree
+    to the BF16 rounding of the activations: within 1 % of the field's
+    largest value everywhere and 1e-3 on average."""
+    from jax_alfa_b200.api import Learned
+    cfg = cases.convective(32, 32, 24, nsteps=60)
+    sim = _sim(cfg)
+    sim.step(1)
+    sim.step(29, graph=True)
+    net = Learned(sim, capacity=20_000, seed=4)
+    for _ in range(5):
+        sim.step(1)
+        net.collect(4000)
+    net.train(epochs=20, batch=1024, lr=2e-3)
+    rep = net.step(2, judge_every=1000, tol=1e9)  # the first step judges, the second is learned
+    assert rep["learned_steps"] == 1
+    n = 32 * 32 * 24
+    tc = sim.checkpoint().cpu().numpy()[9 * n:10 * n]  # the step's Cs^2 (checkpoint field 9)
+    cuda_core, _ = net.infer()
+    cc = cuda_core.cpu().numpy().reshape(-1)
+    scale = float(np.abs(cc).max())
+    err_max = float(np.abs(tc - cc).max()) / scale
+    err_mean = float(np.abs(tc - cc).mean()) / scale
+    report_line(f"learned Cs^2, tensor-core vs CUDA-core inference: max {err_max:.1e}, "
+                f"mean {err_mean:.1e} of the largest value")
+    assert err_max <= 1e-2 and err_mean <= 1e-3
