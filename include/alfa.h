@@ -363,7 +363,9 @@ void alfa_ensemble_destroy(alfa_ensemble*);
  * Delta^2 |S|, the six S_ij / |S|, dtheta/dz, z / Delta and the gradient
  * Richardson number Ri as Ri / (1 + |Ri|).  Hand-written kernels train it (FP32 master weights,
  * Adam) on samples of the dynamic procedure's Cs^2 and beta, and infer it
- * with BF16 weights and FP32 accumulation.
+ * with BF16 weights and FP32 accumulation: alfa_mlp_infer on the CUDA cores
+ * with FP32 activations, the learned step with the 64 x 64 hidden layer on
+ * the tensor cores (BF16 activations of the first layer).
  * collect: npoints random samples of the context's last step, which must
  *   have run the dynamic procedure, into a ring of `capacity` samples.
  * train: epochs over the collected samples (shuffled), batch, learning rate;
