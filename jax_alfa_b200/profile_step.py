@@ -16,6 +16,10 @@ def main(argv=None):
     ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 256])
     ap.add_argument("--steps", type=int, default=3, help="graph steps after the bootstrap step")
     ap.add_argument("--tune", action="store_true", help="run the line-pass autotuner first")
+    ap.add_argument("--learned", action="store_true",
+                    help="instead: the convective case at --grid in FP64, one dynamic step, a "
+                         "network trained one epoch on it, then two learned steps (the "
+                         "tensor-core inference of alfa_step_learned)")
     ap.add_argument("--variant", default=None,
                     help="set this line-pass variant (a TUNE_VARIANTS name) on every pass "
                          "shape that takes it, without timing")
@@ -23,7 +27,19 @@ def main(argv=None):
     import torch
 
     from jax_alfa_b200 import cases
-    from jax_alfa_b200.api import Simulation
+    from jax_alfa_b200.api import Learned, Simulation
+    if args.learned:
+        cfg = cases.convective(*args.grid, nsteps=8)
+        u, v, w, th = cases.initial_fields(cfg, 0)
+        sim = Simulation(cfg, u, v, w, th)
+        sim.step(1)
+        net = Learned(sim, capacity=8192, seed=1)
+        net.collect(8192)
+        net.train(epochs=1, batch=1024, lr=1e-3)
+        rep = net.step(2, judge_every=1000, tol=1e9)
+        torch.cuda.synchronize()
+        print("ok", rep, flush=True)
+        return 0
     cfg = cases.nbl_a94(*args.grid, nsteps=args.steps + 2, precision=args.precision)
     u, v, w, th = cases.initial_fields(cfg, 0)
     sim = Simulation(cfg, u, v, w, th)
