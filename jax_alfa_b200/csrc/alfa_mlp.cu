@@ -397,6 +397,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   d |= (uint64_t)1 << 46;
   return d;
 }
+// the hardware's single-instruction tanh (tanh.approx.f32, relative error
+// ~2^-11): the tensor-core inference rounds the activations to BF16 (2^-9)
+// anyway, and the multi-instruction tanhf held the SFU pipe at half its
+// throughput
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity,
                                          unsigned long long limit) {
   for (unsigned long long i = 0; i < limit; i++) {
@@ -496,7 +506,7 @@ __global__ void __launch_bounds__(umma::TM) k_mlp_infer_tc(MlpFeatIn a,
           float acc = B1[k];
 #pragma unroll
           for (int f = 0; f < MLP_IN; f++) acc += W1[k * MLP_IN + f] * x[f];
-          h[t] = tanhf(acc);
+          h[t] = tanh_hw(acc);
         }
         pk[e] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(h[0])) |
                 ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(h[1])) << 16);
@@ -550,7 +560,7 @@ __global__ void __launch_bounds__(umma::TM) k_mlp_infer_tc(MlpFeatIn a,
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
       for (int j = 0; j < 16; j++) {
-        y0 += W3[c0 + j] * tanhf(__uint_as_float(v[j]) + B2[c0 + j]);
+        y0 += W3[c0 + j] * tanh_hw(__uint_as_float(v[j]) + B2[c0 + j]);
       }
     }
     if (valid) {
