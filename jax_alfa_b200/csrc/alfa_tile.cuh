@@ -106,6 +106,38 @@ __device__ __forceinline__ double ldv(const Loader& L, size_t i, int z) {
   return ev_kind<KIND>(L, [&](int k, int d) { return L.a[k][i + d]; }, z, L.nz);
 }
 
+// Inputs a loader kind has, and for input k whether ev_kind reads it at all
+// (in), at level z-1 (m) or at level z+1 (p); `sub` selects the strain
+// component of LD_W_SXX and is uniform over a launch.
+__host__ __device__ constexpr int loader_nin(int kind) {
+  return (kind == LD_FIELD || kind == LD_THZ) ? 1
+         : (kind == LD_MUL || kind == LD_MUL_THZ || kind == LD_WL_UVP || kind == LD_WL_W) ? 2
+         : (kind == LD_MUL3 || kind == LD_PRESSURE_R || kind == LD_STRESS_UVP ||
+            kind == LD_STRESS_W) ? 3
+         : (kind == LD_W_SXX) ? 9 : 6;
+}
+struct InUse {
+  bool in, m, p;
+};
+__host__ __device__ __forceinline__ InUse loader_use(int kind, int sub, int k) {
+  if (kind == LD_W_SXX) {
+    switch (sub) {
+      case 0: return {k == 0, k == 0, false};
+      case 1: return {k == 4, k == 4, false};
+      case 2: return {k == 8, k == 8, false};
+      case 3: return {k == 3 || k == 1, k == 3 || k == 1, false};
+      case 4: return {k == 6 || k == 2, false, k == 2};
+      default: return {k == 7 || k == 5, false, k == 5};
+    }
+  }
+  const bool m = (kind == LD_ADV_Z && k < 2) || (kind == LD_STRESS_W && k == 0) ||
+                 (kind == LD_WL_W && k == 0);
+  const bool p = (kind == LD_ADV_XY && k >= 3) ||
+                 (kind == LD_SCALAR_ADV && (k == 2 || k == 5)) || kind == LD_THZ ||
+                 (kind == LD_MUL_THZ && k == 1);
+  return {true, m, p};
+}
+
 // Input k around a packed column: levels z-1, z, z+1, z+2.
 struct Q4 {
   real m, x, y, p;
@@ -141,12 +173,7 @@ __device__ __forceinline__ Q4 fetch_q4(const real* a, size_t i, int z, int nz, i
 template <int KIND, int C>
 __device__ __forceinline__ cd eval_pair(const Loader& L, size_t i, int z, int nz, int c,
                                         bool ok) {
-  constexpr int NIN = (KIND == LD_FIELD || KIND == LD_THZ) ? 1
-                      : (KIND == LD_MUL || KIND == LD_MUL_THZ || KIND == LD_WL_UVP ||
-                         KIND == LD_WL_W) ? 2
-                      : (KIND == LD_MUL3 || KIND == LD_PRESSURE_R || KIND == LD_STRESS_UVP ||
-                         KIND == LD_STRESS_W) ? 3
-                      : (KIND == LD_W_SXX) ? 9 : 6;
+  constexpr int NIN = loader_nin(KIND);
   Q4 q[NIN];
   if constexpr (KIND == LD_W_SXX) {
 #pragma unroll
