@@ -24,7 +24,10 @@ static constexpr int U = 8;     // loads in flight per thread
 // accessor at(k, d) = input k at level z + d (d = -1, 0, +1); ldv evaluates
 // it at one linear index i, eval_pair at the two levels (z, z+1) of a packed
 // complex column.  The kind is a compile-time constant in the tile kernels.
-// The expressions are evaluated in FP64 whatever the storage precision.
+// The expressions are evaluated in FP64 whatever the storage precision, except
+// where the accessor returns the stored type (ldv and the materialising
+// pass): there a sub-expression of inputs alone, such as a difference of two
+// FP32 inputs, is computed in FP32 before it meets an FP64 operand.
 // ---------------------------------------------------------------------------
 template <int KIND, class At>
 __device__ __forceinline__ double ev_kind(const Loader& L, const At& at, int z, int nz) {
